@@ -1,0 +1,182 @@
+/*
+ * mb2.h -- the C ABI of the B200-native dense statevector engine for MENOS.
+ *
+ * Plain C types only (no CUDA, torch or C++ types cross this boundary), so
+ * MENOS's C++ SimulationEngine adapter, a ctypes binding or any other FFI can
+ * bind it.  Every function returns an int status (MB2_OK == 0); the message of
+ * the most recent failure on a context is read with mb2_last_error().
+ *
+ * Conventions are the reference's dense-kernel contract
+ * (src/kernels/dense_kernels.h:25-58):
+ *   - little-endian qubits: bit j of an amplitude index is qubit j;
+ *   - operand order: bit j of a gate matrix's row/column index is operand j;
+ *   - amplitudes are interleaved (re, im) pairs; complex128 for the plain
+ *     path (MB2_C128), complex64 for the precision path (MB2_C64);
+ *   - the global phase is part of the state: init writes exp(i*phase)|0..0>;
+ *   - Pauli strings use Y = i*X*Z (x/z bit masks, one 64-bit word).
+ *
+ * The plain complex128 path is bitwise identical to the reference's generic
+ * CPU kernel (src/kernels/cpu/dense_kernels.cpp:465-524): every output
+ * amplitude is (+0) + sum_in m[out][in]*a[in] in increasing `in`, each
+ * product and sum rounded separately (no FMA).
+ */
+#ifndef MENOS_B200_MB2_ABI_H
+#define MENOS_B200_MB2_ABI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    MB2_OK = 0,
+    MB2_ERR_INVALID = 1,       /* a malformed argument (reference: InternalError from ensure) */
+    MB2_ERR_RESOURCE = 2,      /* over budget / out of device memory (reference: ResourceExceeded) */
+    MB2_ERR_CUDA = 3,          /* a CUDA runtime failure (reference: ensure_cuda -> InternalError) */
+    MB2_ERR_NO_DEVICE = 4,     /* no usable sm_100 device */
+    MB2_ERR_TIMEOUT = 5,       /* a bounded wait ran out (serving loop polls) */
+    MB2_ERR_UNSUPPORTED = 6,   /* an operation this engine refuses (e.g. a noise channel) */
+    MB2_ERR_ABANDONED = 7      /* the execution monitor asked to abandon */
+};
+
+/* ---- precisions -------------------------------------------------------- */
+enum { MB2_C128 = 0, MB2_C64 = 1 };
+
+/* ---- opcodes: the reference's menos::Opcode order (include/menos/circuit.h:17-41) */
+enum {
+    MB2_X = 0, MB2_Y, MB2_Z, MB2_H, MB2_S, MB2_SDG, MB2_T, MB2_TDG, MB2_SX, MB2_SXDG,
+    MB2_RX, MB2_RY, MB2_RZ, MB2_P, MB2_U, MB2_CX, MB2_CZ, MB2_SWAP, MB2_CP, MB2_RZZ,
+    MB2_CCX, MB2_UNITARY, MB2_MEASURE
+};
+
+/* The widest operation carried: the reference caps UnitaryOp at 5 qubits
+ * (kMaxUnitaryQubits, include/menos/circuit.h:46); fused blocks reach 6. */
+#define MB2_MAX_OP_QUBITS 6
+
+/* One KIR operation, the flat form of the reference's Operation variant
+ * (GateOp / UnitaryOp / MeasureOp, include/menos/circuit.h:50-90). */
+typedef struct mb2_op {
+    int32_t opcode;                      /* MB2_X .. MB2_MEASURE */
+    uint32_t num_qubits;                 /* operands used in qubits[] */
+    uint32_t qubits[MB2_MAX_OP_QUBITS];  /* operand j = matrix bit j */
+    double params[3];                    /* gate parameters (RX/RY/RZ/P/CP/RZZ: 1, U: 3) */
+    const double* matrix;                /* MB2_UNITARY: 2*4^k doubles, row-major (re, im); else NULL */
+    uint32_t clbit;                      /* MB2_MEASURE: classical bit written */
+    uint32_t reserved;
+} mb2_op;
+
+/* Opaque handles. */
+typedef struct mb2_context mb2_context;
+typedef struct mb2_state mb2_state;
+
+/* ---- context ----------------------------------------------------------- */
+/* Replaces: kernels::cuda::device_info()/DevicePool set-up
+ * (src/kernels/cuda/device_info.h:14-55, device_pool.h:34-75). */
+int mb2_context_create(int device, mb2_context** out);
+int mb2_context_destroy(mb2_context* ctx);
+/* Copies the last error message of ctx (NUL-terminated, truncated to len). */
+int mb2_last_error(const mb2_context* ctx, char* buf, size_t len);
+/* Device facts: SM count, total and free bytes. */
+int mb2_device_info(mb2_context* ctx, int* sm_count, uint64_t* total_bytes, uint64_t* free_bytes);
+
+/* ---- state ------------------------------------------------------------- */
+/* Replaces: DeviceBuffer(num_amplitudes, budget) (src/kernels/cuda/device_buffer.h:25-55);
+ * fails with MB2_ERR_RESOURCE before allocating when 2^n amplitudes exceed
+ * budget_bytes, as the reference does (device_buffer.cpp:23). */
+int mb2_state_alloc(mb2_context* ctx, uint32_t num_qubits, int precision, uint64_t budget_bytes,
+                    mb2_state** out);
+int mb2_state_free(mb2_state* state);
+/* Replaces: kernels::cuda::initialize (src/kernels/cuda/dense_kernels.cu:273-286). */
+int mb2_init(mb2_state* state, double global_phase);
+/* Device pointer of the amplitudes (interleaved re/im), for in-process callers. */
+int mb2_state_device_ptr(mb2_state* state, void** out);
+/* The CUDA stream (cudaStream_t) every call on this state is queued on, for
+ * in-process callers that time or order work against it. */
+int mb2_state_stream(mb2_state* state, void** out);
+
+/* ---- gate application -------------------------------------------------- */
+/* One matrix on one operand list.  Replaces: kernels::cuda::apply_matrix
+ * (src/kernels/cuda/dense_kernels.cu:288-328; contract dense_kernels.h:211-225).
+ * matrix: 2*4^k doubles, row-major, interleaved.  Asynchronous on the
+ * state's stream; the host matrix is staged before return. */
+int mb2_apply_matrix(mb2_state* state, const double* matrix, const uint32_t* operands, uint32_t k);
+/* The generic kernel, kept as the device oracle of the specialised ones.
+ * Replaces: kernels::cuda::apply_matrix_generic (dense_kernels.cu:330-365). */
+int mb2_apply_matrix_generic(mb2_state* state, const double* matrix, const uint32_t* operands,
+                             uint32_t k);
+
+/* Execution options of a program sweep. */
+typedef struct mb2_sweep_options {
+    int32_t fuse_gates;      /* 1: the reference's containment fusion (fuse_gates.cpp:190-283) */
+    int32_t fuse_width;      /* >0: the wide fusion pass up to this many qubits (<= 6); 0 = off */
+    int32_t tile_qubits;     /* qubits per multi-gate tile pass; 0 = autotuned */
+    int32_t per_gate;        /* 1: one launch per block, no tiling (the reference's sweep shape) */
+} mb2_sweep_options;
+
+/* Applies a whole operation list (MeasureOps skipped) as a sequence of
+ * multi-gate tiled passes.  Bitwise identical to applying the same blocks
+ * one by one with mb2_apply_matrix.  Replaces: apply_blocks / apply_operations
+ * in CudaDenseEngine::execute (src/engines/dense_cuda/cuda_dense_engine.cpp:58-87,
+ * 337-355).  opts may be NULL (defaults: reference fusion on, autotuned tile). */
+int mb2_apply_program(mb2_state* state, const mb2_op* ops, uint32_t num_ops,
+                      const mb2_sweep_options* opts);
+/* Statistics of the last mb2_apply_program on this state. */
+typedef struct mb2_sweep_stats {
+    uint64_t blocks;         /* blocks applied (after fusion) */
+    uint64_t passes;         /* state passes launched */
+    uint64_t launches;       /* kernels launched */
+    uint64_t fp64_ops_per_amp; /* FP64 instructions per amplitude summed over the sweep (model) */
+} mb2_sweep_stats;
+int mb2_last_sweep_stats(mb2_state* state, mb2_sweep_stats* out);
+
+/* ---- outputs ----------------------------------------------------------- */
+/* <psi|P_t|psi> for each term (coefficient not applied), out[2t] = re,
+ * out[2t+1] = im.  Replaces: kernels::cuda::expectation_of_term per term
+ * (src/kernels/cuda/dense_kernels.cu:367-409); terms sharing passes.
+ * Synchronous. */
+int mb2_expectation(mb2_state* state, const uint64_t* x_masks, const uint64_t* z_masks,
+                    uint32_t num_terms, double* out);
+/* sum |a|^2, accumulated in FP64.  Synchronous. */
+int mb2_norm(mb2_state* state, double* out);
+/* Counts by the reference's sort-then-walk sampler (src/engines/dense/sample.cpp:24-75):
+ * seed -> mt19937_64 -> (w>>11)*2^-53 uniforms, sorted, walked against the
+ * sequential FP64 cumulative sum of |a|^2 (identical counts).  Outcomes are
+ * the measured bits mapped through targets (pairs qubit, clbit; width <= 64),
+ * returned in ascending outcome order.  *num_outcomes in: capacity of
+ * outcomes/counts, out: distinct outcomes written.  Synchronous. */
+int mb2_sample(mb2_state* state, uint64_t shots, uint64_t seed, const uint32_t* targets,
+               uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes);
+/* Copies the amplitudes to host memory (interleaved; 2 doubles or 2 floats
+ * per amplitude by precision).  Replaces: DeviceBuffer::copy_to_host
+ * (src/kernels/cuda/device_buffer.cpp:60-63).  Synchronous. */
+int mb2_copy_out(mb2_state* state, void* host, uint64_t num_amplitudes);
+/* Copies amplitudes from host memory into the state. Synchronous. */
+int mb2_copy_in(mb2_state* state, const void* host, uint64_t num_amplitudes);
+/* Waits for all work queued on the state's stream. */
+int mb2_synchronize(mb2_state* state);
+
+/* ---- host-side reference pieces (no device work) ----------------------- */
+/* Gate matrix, bitwise ir::generate_matrix (src/ir/gate_table.cpp:260).
+ * out: 2*4^k doubles; returns MB2_ERR_INVALID for UNITARY/MEASURE. */
+int mb2_gate_matrix(int32_t opcode, const double* params, double* out, uint32_t out_len);
+
+/* ---- diagnostics (no device work) ------------------------------------- */
+/* The block schedule mb2_apply_program would run for these ops on a
+ * num_qubits state: for each applied block, in application order, its pass
+ * index, operand count, operands (6 slots) and matrix (2*4^k doubles,
+ * appended to `matrices`).  *num_blocks in: capacity of pass/k/qubits,
+ * out: blocks written; *matrix_len in: capacity of matrices (doubles), out:
+ * doubles written.  Lets tests check the tiled schedule's reordering on the
+ * CPU oracle.  Has no counterpart in the reference (its sweep is in op order). */
+int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
+                       uint32_t num_qubits, uint32_t* pass, uint32_t* k, uint32_t* qubits,
+                       double* matrices, uint64_t* num_blocks, uint64_t* matrix_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MENOS_B200_MB2_ABI_H */

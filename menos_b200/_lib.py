@@ -1,0 +1,98 @@
+"""ctypes binding of libmenos_b200.so (the C ABI in include/mb2.h).
+
+The library is built in-tree (``python -m menos_b200.build``); importing this
+module without it raises, so no caller can silently run without the CUDA
+path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .circuit import MB2Op
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libmenos_b200.so")
+
+MB2_OK = 0
+ERRORS = {1: "invalid argument", 2: "resource exceeded", 3: "CUDA error", 4: "no sm_100 device",
+          5: "timeout", 6: "unsupported", 7: "abandoned"}
+C128, C64 = 0, 1
+
+
+class SweepOptions(C.Structure):
+    _fields_ = [("fuse_gates", C.c_int32), ("fuse_width", C.c_int32), ("tile_qubits", C.c_int32),
+                ("per_gate", C.c_int32)]
+
+
+class SweepStats(C.Structure):
+    _fields_ = [("blocks", C.c_uint64), ("passes", C.c_uint64), ("launches", C.c_uint64),
+                ("fp64_ops_per_amp", C.c_uint64)]
+
+
+# Exported symbol -> (restype, argtypes); the list the C-ABI tests check
+# against include/mb2.h.
+_VP = C.c_void_p
+SIGNATURES = {
+    "mb2_context_create": (C.c_int, [C.c_int, C.POINTER(_VP)]),
+    "mb2_context_destroy": (C.c_int, [_VP]),
+    "mb2_last_error": (C.c_int, [_VP, C.c_char_p, C.c_size_t]),
+    "mb2_device_info": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "mb2_state_alloc": (C.c_int, [_VP, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(_VP)]),
+    "mb2_state_free": (C.c_int, [_VP]),
+    "mb2_init": (C.c_int, [_VP, C.c_double]),
+    "mb2_state_device_ptr": (C.c_int, [_VP, C.POINTER(_VP)]),
+    "mb2_state_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
+    "mb2_apply_matrix": (C.c_int, [_VP, _VP, _VP, C.c_uint32]),
+    "mb2_apply_matrix_generic": (C.c_int, [_VP, _VP, _VP, C.c_uint32]),
+    "mb2_apply_program": (C.c_int, [_VP, C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions)]),
+    "mb2_last_sweep_stats": (C.c_int, [_VP, C.POINTER(SweepStats)]),
+    "mb2_expectation": (C.c_int, [_VP, _VP, _VP, C.c_uint32, _VP]),
+    "mb2_norm": (C.c_int, [_VP, C.POINTER(C.c_double)]),
+    "mb2_sample": (C.c_int, [_VP, C.c_uint64, C.c_uint64, _VP, C.c_uint32, _VP, _VP, C.POINTER(C.c_uint64)]),
+    "mb2_copy_out": (C.c_int, [_VP, _VP, C.c_uint64]),
+    "mb2_copy_in": (C.c_int, [_VP, _VP, C.c_uint64]),
+    "mb2_synchronize": (C.c_int, [_VP]),
+    "mb2_gate_matrix": (C.c_int, [C.c_int32, _VP, _VP, C.c_uint32]),
+    "mb2_debug_schedule": (C.c_int, [C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions), C.c_uint32, _VP, _VP,
+                                     _VP, _VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libmenos_b200.so is not built ({LIB_PATH}); run python -m menos_b200.build")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class MB2Error(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class ResourceExceeded(MB2Error):
+    """The reference's common::ResourceExceeded (src/common/error.h:29-43)."""
+
+
+def check(rc: int, ctx=None, what: str = "") -> None:
+    if rc == MB2_OK:
+        return
+    msg = what
+    if ctx is not None:
+        buf = C.create_string_buffer(512)
+        lib().mb2_last_error(ctx, buf, 512)
+        msg = f"{what}: {buf.value.decode(errors='replace')}"
+    if rc == 2:
+        raise ResourceExceeded(rc, msg)
+    raise MB2Error(rc, msg)

@@ -1,0 +1,92 @@
+"""KIR operations on the Python side of the C ABI.
+
+``Circuit`` mirrors the reference's ``menos::Circuit`` operation list
+(include/menos/circuit.h:50-150): named gates by opcode (the reference's
+``menos::Opcode`` order), explicit unitaries, and measurements.  ``ops`` is a
+list of ``(opcode, qubits, params, matrix, clbit)`` tuples; ``to_mb2_ops``
+packs it into the C ABI's ``mb2_op`` array.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+OPCODES = ["x", "y", "z", "h", "s", "sdg", "t", "tdg", "sx", "sxdg", "rx", "ry", "rz", "p",
+           "u", "cx", "cz", "swap", "cp", "rzz", "ccx", "unitary", "measure"]
+OP = {name: i for i, name in enumerate(OPCODES)}
+NUM_QUBITS = {**{i: 1 for i in range(15)}, 15: 2, 16: 2, 17: 2, 18: 2, 19: 2, 20: 3}
+NUM_PARAMS = {10: 1, 11: 1, 12: 1, 13: 1, 14: 3, 18: 1, 19: 1}
+MAX_OP_QUBITS = 6
+
+
+class MB2Op(C.Structure):
+    """``mb2_op`` (include/mb2.h)."""
+    _fields_ = [("opcode", C.c_int32), ("num_qubits", C.c_uint32), ("qubits", C.c_uint32 * 6),
+                ("params", C.c_double * 3), ("matrix", C.POINTER(C.c_double)),
+                ("clbit", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Circuit:
+    def __init__(self, num_qubits: int, num_clbits: int = 0, global_phase: float = 0.0):
+        self.num_qubits = int(num_qubits)
+        self.num_clbits = int(num_clbits)
+        self.global_phase = float(global_phase)
+        self.ops: list[tuple] = []
+
+    def gate(self, name: str, qubits, params=()) -> "Circuit":
+        oc = OP[name]
+        qs = tuple(int(q) for q in qubits)
+        if len(qs) != NUM_QUBITS[oc]:
+            raise ValueError(f"{name} takes {NUM_QUBITS[oc]} qubits")
+        ps = tuple(float(p) for p in params)
+        if len(ps) != NUM_PARAMS.get(oc, 0):
+            raise ValueError(f"{name} takes {NUM_PARAMS.get(oc, 0)} parameters")
+        self.ops.append((oc, qs, ps, None, 0))
+        return self
+
+    def unitary(self, qubits, matrix) -> "Circuit":
+        qs = tuple(int(q) for q in qubits)
+        m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128))
+        if m.shape != (1 << len(qs), 1 << len(qs)) or len(qs) > MAX_OP_QUBITS:
+            raise ValueError("unitary shape does not match its operands")
+        self.ops.append((OP["unitary"], qs, (), m, 0))
+        return self
+
+    def measure(self, qubit: int, clbit: int) -> "Circuit":
+        self.ops.append((OP["measure"], (int(qubit),), (), None, int(clbit)))
+        self.num_clbits = max(self.num_clbits, int(clbit) + 1)
+        return self
+
+    def __len__(self) -> int:
+        return len(self.ops)
+
+    def measure_targets(self):
+        """Last-write-wins (qubit, clbit) pairs, as the reference's runtime
+        resolves them before the engine sees them."""
+        by_clbit = {}
+        for oc, qs, _ps, _m, cl in self.ops:
+            if oc == OP["measure"]:
+                by_clbit[cl] = qs[0]
+        return [(q, c) for c, q in sorted(by_clbit.items())]
+
+
+def to_mb2_ops(circ: Circuit):
+    """Returns (array of MB2Op, keep-alive list of matrix buffers)."""
+    n = len(circ.ops)
+    arr = (MB2Op * max(n, 1))()
+    keep = []
+    for i, (oc, qs, ps, m, cl) in enumerate(circ.ops):
+        o = arr[i]
+        o.opcode = oc
+        o.num_qubits = len(qs)
+        for j, q in enumerate(qs):
+            o.qubits[j] = q
+        for j, p in enumerate(ps):
+            o.params[j] = p
+        if m is not None:
+            buf = np.ascontiguousarray(m.view(np.float64).ravel())
+            keep.append(buf)
+            o.matrix = buf.ctypes.data_as(C.POINTER(C.c_double))
+        o.clbit = cl
+    return arr, keep

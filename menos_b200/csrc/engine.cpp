@@ -1,0 +1,491 @@
+// The C ABI (include/mb2.h) over the sm_100a kernels: contexts, device
+// states, gate application (per block or as multi-gate tiled passes),
+// expectation, norm, sampling and copies.
+//
+// Error conventions follow the reference's CUDA backend
+// (src/kernels/cuda/cuda_error.h:23-30, device_buffer.cpp:23,
+// device_pool.cpp:73-86): a request over budget fails before anything is
+// allocated (MB2_ERR_RESOURCE), an out-of-memory allocation is reported as
+// MB2_ERR_RESOURCE with the CUDA error cleared, any other CUDA failure is
+// MB2_ERR_CUDA with its message kept on the context.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mb2_internal.h"
+
+struct mb2_context {
+    int device = 0;
+    int sm_count = 0;
+    std::mutex mu;
+    std::string last_error;
+};
+
+struct mb2_state {
+    mb2_context* ctx = nullptr;
+    uint32_t n = 0;
+    int precision = MB2_C128;
+    void* amps = nullptr;
+    cudaStream_t stream = nullptr;
+    void* scratch = nullptr;  // staging: program, matrices, masks, partials
+    size_t scratch_bytes = 0;
+    mb2_sweep_stats stats{};
+};
+
+namespace {
+
+int fail(mb2_context* ctx, int code, const std::string& msg) {
+    if (ctx != nullptr) {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        ctx->last_error = msg;
+    }
+    return code;
+}
+
+int cuda_fail(mb2_context* ctx, cudaError_t e, const char* what) {
+    const std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();  // clear the sticky-free allocation error
+        return fail(ctx, MB2_ERR_RESOURCE, msg);
+    }
+    return fail(ctx, MB2_ERR_CUDA, msg);
+}
+
+#define MB2_CUDA(ctx, call)                                    \
+    do {                                                       \
+        const cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+size_t amp_bytes(int precision) { return precision == MB2_C64 ? 8 : 16; }
+
+// Grow-only device staging buffer of the state.  Freed buffers may still be
+// read by queued kernels, so the stream is drained first.
+int ensure_scratch(mb2_state* s, size_t bytes) {
+    if (bytes <= s->scratch_bytes) return MB2_OK;
+    MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+    if (s->scratch != nullptr) MB2_CUDA(s->ctx, cudaFree(s->scratch));
+    s->scratch = nullptr;
+    s->scratch_bytes = 0;
+    size_t want = 1 << 20;
+    while (want < bytes) want <<= 1;
+    MB2_CUDA(s->ctx, cudaMalloc(&s->scratch, want));
+    s->scratch_bytes = want;
+    return MB2_OK;
+}
+
+int check_operands(mb2_state* s, const uint32_t* q, uint32_t k) {
+    if (k == 0 || k > MB2_MAX_OP_QUBITS) return fail(s->ctx, MB2_ERR_INVALID, "operand count must be 1..6");
+    uint64_t seen = 0;
+    for (uint32_t j = 0; j < k; ++j) {
+        if (q[j] >= s->n) return fail(s->ctx, MB2_ERR_INVALID, "operand out of range");
+        if (seen & (uint64_t{1} << q[j])) return fail(s->ctx, MB2_ERR_INVALID, "repeated operand");
+        seen |= uint64_t{1} << q[j];
+    }
+    return MB2_OK;
+}
+
+// One block through the per-gate kernels (the reference's apply_matrix
+// dispatch, src/kernels/cpu/dense_kernels.cpp:427-463: diagonal, 1q, 2q,
+// generic).
+int apply_block(mb2_state* s, const mb2::Cd* m, const uint32_t* q, uint32_t k, bool force_generic) {
+    const uint32_t dim = 1u << k;
+    std::vector<mb2::Cd> mv(m, m + size_t{dim} * dim);
+    const double* md = reinterpret_cast<const double*>(mv.data());
+    int rc;
+    if (!force_generic && mb2::is_diagonal(mv, dim)) {
+        std::vector<double> d(2 * dim);
+        for (uint32_t i = 0; i < dim; ++i) {
+            d[2 * i] = mv[size_t{i} * dim + i].real();
+            d[2 * i + 1] = mv[size_t{i} * dim + i].imag();
+        }
+        rc = mb2::launch_apply_diag(s->amps, s->n, q, k, d.data(), s->stream);
+    } else if (!force_generic && k == 1) {
+        rc = mb2::launch_apply_1q(s->amps, s->n, q[0], md, s->stream);
+    } else if (!force_generic && k == 2) {
+        rc = mb2::launch_apply_2q(s->amps, s->n, q[0], q[1], md, s->stream);
+    } else {
+        const size_t bytes = size_t{dim} * dim * sizeof(mb2::Cd);
+        if (int e = ensure_scratch(s, bytes); e != MB2_OK) return e;
+        MB2_CUDA(s->ctx, cudaMemcpyAsync(s->scratch, md, bytes, cudaMemcpyHostToDevice, s->stream));
+        rc = mb2::launch_apply_generic(s->amps, s->n, q, k, static_cast<const double*>(s->scratch), s->stream);
+    }
+    if (rc != MB2_OK) return fail(s->ctx, rc, std::string("kernel launch: ") + mb2::last_cuda_error_string());
+    s->stats.launches += 1;
+    return MB2_OK;
+}
+
+uint32_t default_tile_qubits(uint32_t n) { return std::min<uint32_t>(12, n); }
+
+// The tile width a sweep runs at: the requested (or default) width, raised
+// to hold the widest block, within the kernel's limits.
+uint32_t tile_width(uint32_t requested, uint32_t n, const std::vector<mb2::Block>& blocks) {
+    uint32_t m = requested > 0 ? requested : default_tile_qubits(n);
+    for (const mb2::Block& b : blocks) m = std::max(m, b.k);
+    m = std::max(m, mb2::kMinTileQubits);
+    return std::min(m, mb2::kMaxTileQubits);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mb2_context_create(int device, mb2_context** out) {
+    if (out == nullptr) return MB2_ERR_INVALID;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) {
+        cudaGetLastError();
+        return MB2_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return MB2_ERR_NO_DEVICE;
+    if (prop.major < 10) return MB2_ERR_NO_DEVICE;  // sm_100a kernels only
+    if (cudaSetDevice(device) != cudaSuccess) return MB2_ERR_NO_DEVICE;
+    auto* ctx = new mb2_context;
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    *out = ctx;
+    return MB2_OK;
+}
+
+int mb2_context_destroy(mb2_context* ctx) {
+    delete ctx;
+    return MB2_OK;
+}
+
+int mb2_last_error(const mb2_context* ctx, char* buf, size_t len) {
+    if (ctx == nullptr || buf == nullptr || len == 0) return MB2_ERR_INVALID;
+    auto* c = const_cast<mb2_context*>(ctx);
+    std::lock_guard<std::mutex> lock(c->mu);
+    const size_t n = std::min(len - 1, c->last_error.size());
+    std::memcpy(buf, c->last_error.data(), n);
+    buf[n] = '\0';
+    return MB2_OK;
+}
+
+int mb2_device_info(mb2_context* ctx, int* sm_count, uint64_t* total_bytes, uint64_t* free_bytes) {
+    if (ctx == nullptr) return MB2_ERR_INVALID;
+    MB2_CUDA(ctx, cudaSetDevice(ctx->device));
+    size_t fr = 0, tot = 0;
+    MB2_CUDA(ctx, cudaMemGetInfo(&fr, &tot));
+    if (sm_count) *sm_count = ctx->sm_count;
+    if (total_bytes) *total_bytes = tot;
+    if (free_bytes) *free_bytes = fr;
+    return MB2_OK;
+}
+
+int mb2_state_alloc(mb2_context* ctx, uint32_t num_qubits, int precision, uint64_t budget_bytes, mb2_state** out) {
+    if (ctx == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    *out = nullptr;
+    if (precision != MB2_C128 && precision != MB2_C64) return fail(ctx, MB2_ERR_INVALID, "unknown precision");
+    if (num_qubits < 1 || num_qubits > 40) return fail(ctx, MB2_ERR_INVALID, "num_qubits must be 1..40");
+    const uint64_t bytes = (uint64_t{1} << num_qubits) * amp_bytes(precision);
+    if (bytes > budget_bytes)
+        return fail(ctx, MB2_ERR_RESOURCE,
+                    "state needs " + std::to_string(bytes) + " bytes, budget is " + std::to_string(budget_bytes));
+    MB2_CUDA(ctx, cudaSetDevice(ctx->device));
+    auto* s = new mb2_state;
+    s->ctx = ctx;
+    s->n = num_qubits;
+    s->precision = precision;
+    cudaError_t e = cudaMalloc(&s->amps, bytes);
+    if (e != cudaSuccess) {
+        delete s;
+        return cuda_fail(ctx, e, "cudaMalloc(state)");
+    }
+    e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cudaFree(s->amps);
+        delete s;
+        return cuda_fail(ctx, e, "cudaStreamCreate");
+    }
+    *out = s;
+    return MB2_OK;
+}
+
+int mb2_state_free(mb2_state* s) {
+    if (s == nullptr) return MB2_OK;
+    cudaStreamSynchronize(s->stream);
+    if (s->scratch) cudaFree(s->scratch);
+    cudaFree(s->amps);
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return MB2_OK;
+}
+
+int mb2_state_device_ptr(mb2_state* s, void** out) {
+    if (s == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    *out = s->amps;
+    return MB2_OK;
+}
+
+int mb2_state_stream(mb2_state* s, void** out) {
+    if (s == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    *out = s->stream;
+    return MB2_OK;
+}
+
+int mb2_init(mb2_state* s, double global_phase) {
+    if (s == nullptr) return MB2_ERR_INVALID;
+    const mb2::Cd ph = mb2::initial_phase(global_phase);
+    const int rc = mb2::launch_init(s->amps, uint64_t{1} << s->n, s->precision, ph.real(), ph.imag(), s->stream);
+    if (rc != MB2_OK) return fail(s->ctx, rc, std::string("init: ") + mb2::last_cuda_error_string());
+    return MB2_OK;
+}
+
+int mb2_apply_matrix(mb2_state* s, const double* matrix, const uint32_t* operands, uint32_t k) {
+    if (s == nullptr || matrix == nullptr || operands == nullptr) return MB2_ERR_INVALID;
+    if (s->precision != MB2_C128) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "mb2_apply_matrix: complex128 states only");
+    if (int e = check_operands(s, operands, k); e != MB2_OK) return e;
+    return apply_block(s, reinterpret_cast<const mb2::Cd*>(matrix), operands, k, false);
+}
+
+int mb2_apply_matrix_generic(mb2_state* s, const double* matrix, const uint32_t* operands, uint32_t k) {
+    if (s == nullptr || matrix == nullptr || operands == nullptr) return MB2_ERR_INVALID;
+    if (s->precision != MB2_C128) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "complex128 states only");
+    if (int e = check_operands(s, operands, k); e != MB2_OK) return e;
+    return apply_block(s, reinterpret_cast<const mb2::Cd*>(matrix), operands, k, true);
+}
+
+int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts) {
+    if (s == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
+    if (s->precision != MB2_C128) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "mb2_apply_program: complex128 states only");
+    mb2_sweep_options o{1, 0, 0, 0};
+    if (opts != nullptr) o = *opts;
+    for (uint32_t i = 0; i < num_ops; ++i) {
+        if (ops[i].opcode == MB2_MEASURE) continue;
+        if (ops[i].num_qubits == 0 || ops[i].num_qubits > MB2_MAX_OP_QUBITS)
+            return fail(s->ctx, MB2_ERR_INVALID, "operation " + std::to_string(i) + ": operand count");
+        if (int e = check_operands(s, ops[i].qubits, ops[i].num_qubits); e != MB2_OK) return e;
+    }
+    std::vector<mb2::Block> blocks;
+    try {
+        blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+    } catch (const std::exception& e) {
+        return fail(s->ctx, MB2_ERR_INVALID, e.what());
+    }
+    s->stats = mb2_sweep_stats{};
+    s->stats.blocks = blocks.size();
+    if (blocks.empty()) return MB2_OK;
+    const uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, s->n, blocks);
+    if (o.per_gate != 0 || s->n < mb2::kMinTileQubits) {
+        for (const mb2::Block& b : blocks) {
+            if (int e = apply_block(s, b.m.data(), b.q, b.k, false); e != MB2_OK) return e;
+            s->stats.passes += 1;
+        }
+        return MB2_OK;
+    }
+    mb2::TileProgram prog;
+    try {
+        prog = mb2::plan_tile_program(blocks, s->n, m);
+    } catch (const std::exception& e) {
+        return fail(s->ctx, MB2_ERR_INVALID, e.what());
+    }
+    const size_t ibytes = prog.instrs.size() * sizeof(mb2::TileInstr);
+    const size_t dbytes = prog.data.size() * sizeof(double);
+    if (int e = ensure_scratch(s, ibytes + dbytes + 256); e != MB2_OK) return e;
+    // One upload: instructions, then the data block (256-byte aligned).
+    const size_t doff = (ibytes + 255) & ~size_t{255};
+    std::vector<unsigned char> host(doff + dbytes);
+    std::memcpy(host.data(), prog.instrs.data(), ibytes);
+    std::memcpy(host.data() + doff, prog.data.data(), dbytes);
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(s->scratch, host.data(), host.size(), cudaMemcpyHostToDevice, s->stream));
+    const auto* dev_instrs = static_cast<const mb2::TileInstr*>(s->scratch);
+    const auto* dev_data = reinterpret_cast<const double*>(static_cast<unsigned char*>(s->scratch) + doff);
+    for (const mb2::TilePass& pass : prog.passes) {
+        const int rc = mb2::launch_tile_pass(s->amps, s->n, pass, dev_instrs, dev_data, s->ctx->sm_count, s->stream);
+        if (rc != MB2_OK) return fail(s->ctx, rc, std::string("tile pass launch: ") + mb2::last_cuda_error_string());
+    }
+    s->stats.passes = prog.passes.size();
+    s->stats.launches = prog.passes.size();
+    s->stats.fp64_ops_per_amp = prog.fp64_per_amp;
+    return MB2_OK;
+}
+
+int mb2_last_sweep_stats(mb2_state* s, mb2_sweep_stats* out) {
+    if (s == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    *out = s->stats;
+    return MB2_OK;
+}
+
+int mb2_expectation(mb2_state* s, const uint64_t* x_masks, const uint64_t* z_masks, uint32_t num_terms, double* out) {
+    if (s == nullptr || (num_terms != 0 && (x_masks == nullptr || z_masks == nullptr || out == nullptr)))
+        return MB2_ERR_INVALID;
+    if (num_terms == 0) return MB2_OK;
+    if (s->precision != MB2_C128) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "mb2_expectation: complex128 states only");
+    const uint64_t lim = (s->n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << s->n) - 1);
+    for (uint32_t t = 0; t < num_terms; ++t)
+        if ((x_masks[t] | z_masks[t]) & ~lim) return fail(s->ctx, MB2_ERR_INVALID, "Pauli mask beyond the state's qubits");
+    const size_t mask_bytes = size_t{num_terms} * 8;
+    const size_t part_bytes = size_t{num_terms} * mb2::kExpBlocks * 16;
+    const size_t out_bytes = size_t{num_terms} * 16;
+    const size_t off_z = (mask_bytes + 255) & ~size_t{255};
+    const size_t off_p = off_z + ((mask_bytes + 255) & ~size_t{255});
+    const size_t off_o = off_p + part_bytes;
+    if (int e = ensure_scratch(s, off_o + out_bytes); e != MB2_OK) return e;
+    auto* base = static_cast<unsigned char*>(s->scratch);
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(base, x_masks, mask_bytes, cudaMemcpyHostToDevice, s->stream));
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(base + off_z, z_masks, mask_bytes, cudaMemcpyHostToDevice, s->stream));
+    const int rc = mb2::launch_expectation(s->amps, s->n, reinterpret_cast<const uint64_t*>(base),
+                                           reinterpret_cast<const uint64_t*>(base + off_z), num_terms,
+                                           reinterpret_cast<double*>(base + off_p),
+                                           reinterpret_cast<double*>(base + off_o), s->stream);
+    if (rc != MB2_OK) return fail(s->ctx, rc, std::string("expectation launch: ") + mb2::last_cuda_error_string());
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(out, base + off_o, out_bytes, cudaMemcpyDeviceToHost, s->stream));
+    MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+    return MB2_OK;
+}
+
+int mb2_norm(mb2_state* s, double* out) {
+    if (s == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    const uint64_t zero = 0;
+    double v[2];
+    if (int e = mb2_expectation(s, &zero, &zero, 1, v); e != MB2_OK) return e;
+    *out = v[0];
+    return MB2_OK;
+}
+
+int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targets, uint32_t num_targets,
+               uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes) {
+    if (s == nullptr || num_outcomes == nullptr) return MB2_ERR_INVALID;
+    if (s->precision != MB2_C128) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "mb2_sample: complex128 states only");
+    for (uint32_t t = 0; t < num_targets; ++t)
+        if (targets[2 * t] >= s->n || targets[2 * t + 1] >= 64)
+            return fail(s->ctx, MB2_ERR_INVALID, "measure target out of range");
+    if (shots == 0) {
+        *num_outcomes = 0;
+        return MB2_OK;
+    }
+    // Uniforms exactly as common::Rng (src/common/rng.cpp:176-186), sorted
+    // (src/engines/dense/sample.cpp:37-42).
+    std::vector<double> u(shots);
+    {
+        std::mt19937_64 eng(seed);
+        for (uint64_t i = 0; i < shots; ++i) u[i] = static_cast<double>(eng() >> 11) * (1.0 / 9007199254740992.0);
+    }
+    std::sort(u.begin(), u.end());
+    // The sequential walk (sample.cpp:55-69) over the state, streamed back
+    // in chunks through a pinned buffer.
+    const uint64_t na = uint64_t{1} << s->n;
+    const uint64_t chunk = std::min<uint64_t>(na, uint64_t{1} << 22);
+    double* pinned = nullptr;
+    MB2_CUDA(s->ctx, cudaMallocHost(reinterpret_cast<void**>(&pinned), chunk * 16));
+    std::vector<uint64_t> basis(shots);
+    double cumulative = 0.0;
+    uint64_t shot = 0;
+    int rc = MB2_OK;
+    for (uint64_t c0 = 0; c0 < na && shot < shots; c0 += chunk) {
+        const cudaError_t e1 = cudaMemcpyAsync(pinned, static_cast<const unsigned char*>(s->amps) + c0 * 16,
+                                               chunk * 16, cudaMemcpyDeviceToHost, s->stream);
+        const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamSynchronize(s->stream) : e1;
+        if (e2 != cudaSuccess) {
+            rc = cuda_fail(s->ctx, e2, "sample copy");
+            break;
+        }
+        for (uint64_t i = 0; i < chunk && shot < shots; ++i) {
+            const double re = pinned[2 * i], im = pinned[2 * i + 1];
+            cumulative += re * re + im * im;
+            while (shot < shots && u[shot] < cumulative) basis[shot++] = c0 + i;
+        }
+    }
+    cudaFreeHost(pinned);
+    if (rc != MB2_OK) return rc;
+    while (shot < shots) basis[shot++] = na - 1;
+    // Outcomes through the measure targets, ascending, with counts.
+    std::vector<uint64_t> oc(shots);
+    for (uint64_t i = 0; i < shots; ++i) {
+        uint64_t o = 0;
+        for (uint32_t t = 0; t < num_targets; ++t)
+            if ((basis[i] >> targets[2 * t]) & 1u) o |= uint64_t{1} << targets[2 * t + 1];
+        oc[i] = o;
+    }
+    std::sort(oc.begin(), oc.end());
+    uint64_t d = 0;
+    for (uint64_t i = 0; i < shots; ++i) {
+        if (d > 0 && outcomes[d - 1] == oc[i]) {
+            counts[d - 1] += 1;
+            continue;
+        }
+        if (d >= *num_outcomes) return fail(s->ctx, MB2_ERR_INVALID, "outcome capacity too small");
+        outcomes[d] = oc[i];
+        counts[d] = 1;
+        ++d;
+    }
+    *num_outcomes = d;
+    return MB2_OK;
+}
+
+int mb2_copy_out(mb2_state* s, void* host, uint64_t num_amplitudes) {
+    if (s == nullptr || host == nullptr) return MB2_ERR_INVALID;
+    if (num_amplitudes > (uint64_t{1} << s->n)) return fail(s->ctx, MB2_ERR_INVALID, "copy beyond the state");
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(host, s->amps, num_amplitudes * amp_bytes(s->precision), cudaMemcpyDeviceToHost,
+                                     s->stream));
+    MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+    return MB2_OK;
+}
+
+int mb2_copy_in(mb2_state* s, const void* host, uint64_t num_amplitudes) {
+    if (s == nullptr || host == nullptr) return MB2_ERR_INVALID;
+    if (num_amplitudes > (uint64_t{1} << s->n)) return fail(s->ctx, MB2_ERR_INVALID, "copy beyond the state");
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(s->amps, host, num_amplitudes * amp_bytes(s->precision), cudaMemcpyHostToDevice,
+                                     s->stream));
+    MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+    return MB2_OK;
+}
+
+int mb2_synchronize(mb2_state* s) {
+    if (s == nullptr) return MB2_ERR_INVALID;
+    MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+    return MB2_OK;
+}
+
+int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
+                       uint32_t* pass, uint32_t* k, uint32_t* qubits, double* matrices, uint64_t* num_blocks,
+                       uint64_t* matrix_len) {
+    if (num_blocks == nullptr || matrix_len == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
+    if (num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
+    mb2_sweep_options o{1, 0, 0, 0};
+    if (opts != nullptr) o = *opts;
+    std::vector<mb2::Block> blocks;
+    std::vector<uint32_t> order, order_pass;
+    try {
+        blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+        const uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, num_qubits, blocks);
+        if (o.per_gate != 0 || num_qubits < mb2::kMinTileQubits || blocks.empty()) {
+            for (uint32_t i = 0; i < blocks.size(); ++i) {
+                order.push_back(i);
+                order_pass.push_back(i);
+            }
+        } else {
+            const mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m);
+            order = prog.order;
+            order_pass = prog.order_pass;
+        }
+    } catch (const std::exception&) {
+        return MB2_ERR_INVALID;
+    }
+    if (order.size() > *num_blocks) return MB2_ERR_INVALID;
+    uint64_t mlen = 0;
+    for (size_t i = 0; i < order.size(); ++i) {
+        const mb2::Block& b = blocks[order[i]];
+        const uint64_t need = 2ull << (2 * b.k);
+        if (mlen + need > *matrix_len) return MB2_ERR_INVALID;
+        pass[i] = order_pass[i];
+        k[i] = b.k;
+        for (uint32_t j = 0; j < 6; ++j) qubits[6 * i + j] = j < b.k ? b.q[j] : 0;
+        std::memcpy(matrices + mlen, b.m.data(), need * sizeof(double));
+        mlen += need;
+    }
+    *num_blocks = order.size();
+    *matrix_len = mlen;
+    return MB2_OK;
+}
+
+}  // extern "C"

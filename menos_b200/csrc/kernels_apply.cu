@@ -1,0 +1,582 @@
+// sm_100a gate kernels of the plain complex128 path.
+//
+// Bitwise contract (the reference's generic kernel,
+// src/kernels/cpu/dense_kernels.cpp:465-524): each output amplitude is
+//     (+0) + m[out][0]*a[0] + m[out][1]*a[1] + ...   (increasing `in`)
+// with the product (mr*ar - mi*ai, mr*ai + mi*ar), every multiply and add
+// rounded on its own (built with -fmad=false and written with __dmul_rn /
+// __dadd_rn / __dsub_rn, which are never contracted).  Two rewrites keep the
+// result identical and save FP64 issue slots:
+//   * the leading "(+0) +" only turns a -0.0 into +0.0, and the sign of a
+//     zero never changes a later non-zero sum, so it is dropped inside the
+//     arithmetic and applied once, as canon(), where an amplitude is stored;
+//   * a product term whose matrix entry is exactly zero (either sign) is a
+//     signed zero and changes nothing but a zero's sign, so it is skipped;
+//     an entry with zero imaginary part contributes (mr*ar, mr*ai).
+// Both hold for finite amplitudes, the reference kernels' own precondition
+// (src/kernels/dense_kernels.h:105-124).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mb2_internal.h"
+
+namespace mb2 {
+namespace {
+
+// ---------------------------------------------------------------- arithmetic
+__device__ __forceinline__ double2 cmul(double mr, double mi, double2 x) {
+    return make_double2(__dsub_rn(__dmul_rn(mr, x.x), __dmul_rn(mi, x.y)),
+                        __dadd_rn(__dmul_rn(mr, x.y), __dmul_rn(mi, x.x)));
+}
+__device__ __forceinline__ double2 cmul_re(double mr, double2 x) {
+    return make_double2(__dmul_rn(mr, x.x), __dmul_rn(mr, x.y));
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+    return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y));
+}
+// -0.0 -> +0.0, everything else unchanged (integer compare, no FP64 issue).
+__device__ __forceinline__ double canon1(double v) {
+    const long long b = __double_as_longlong(v);
+    return __longlong_as_double(b == static_cast<long long>(0x8000000000000000ULL) ? 0LL : b);
+}
+__device__ __forceinline__ double2 canon(double2 v) { return make_double2(canon1(v.x), canon1(v.y)); }
+__device__ __forceinline__ double2 cneg(double2 v) {
+    return make_double2(__longlong_as_double(__double_as_longlong(v.x) ^ static_cast<long long>(0x8000000000000000ULL)),
+                        __longlong_as_double(__double_as_longlong(v.y) ^ static_cast<long long>(0x8000000000000000ULL)));
+}
+// d * a for one diagonal / monomial entry, exact up to a zero's sign:
+// (1, 0) -> a, (-1, 0) -> -a, else the full product.
+__device__ __forceinline__ double2 scale_entry(double dr, double di, double2 a) {
+    if (di == 0.0) {
+        if (dr == 1.0) return a;
+        if (dr == -1.0) return cneg(a);
+    }
+    return cmul(dr, di, a);
+}
+
+__device__ __forceinline__ uint64_t insert_zero(uint64_t i, uint32_t pos) {
+    const uint64_t low = (uint64_t{1} << pos) - 1;
+    return ((i & ~low) << 1) | (i & low);
+}
+
+// Scatters the low bits of v onto the set bits of mask (ascending).
+__device__ __forceinline__ uint64_t pdep64(uint64_t v, uint64_t mask) {
+    uint64_t r = 0;
+    while (mask != 0) {
+        const uint64_t low = mask & (~mask + 1);
+        if (v & 1) r |= low;
+        v >>= 1;
+        mask ^= low;
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------- init
+__global__ void k_init_c128(double2* st, uint64_t n_amps, double re, double im) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_amps; i += stride)
+        st[i] = (i == 0) ? make_double2(re, im) : make_double2(0.0, 0.0);
+}
+__global__ void k_init_c64(float2* st, uint64_t n_amps, float re, float im) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_amps; i += stride)
+        st[i] = (i == 0) ? make_float2(re, im) : make_float2(0.0f, 0.0f);
+}
+
+// ---------------------------------------------------------------- per-gate kernels
+struct M8 {
+    double v[8];
+};
+struct M32 {
+    double v[32];
+};
+struct D128 {
+    double v[128];
+};
+
+// One pair (i0, i0 | 2^q) per thread iteration: the reference's 1-qubit
+// contract (dense_kernels.cpp:227-273).
+__global__ void __launch_bounds__(256) k_apply_1q(double2* __restrict__ st, uint64_t npairs, uint32_t q, M8 m) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t bit = uint64_t{1} << q;
+    for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < npairs; p += stride) {
+        const uint64_t i0 = insert_zero(p, q);
+        const double2 a0 = st[i0];
+        const double2 a1 = st[i0 | bit];
+        st[i0] = canon(cadd(cmul(m.v[0], m.v[1], a0), cmul(m.v[2], m.v[3], a1)));
+        st[i0 | bit] = canon(cadd(cmul(m.v[4], m.v[5], a0), cmul(m.v[6], m.v[7], a1)));
+    }
+}
+
+// One group of four per thread iteration; local bit j = operand j
+// (dense_kernels.cpp:275-297).
+__global__ void __launch_bounds__(256) k_apply_2q(double2* __restrict__ st, uint64_t ngroups, uint32_t q0,
+                                                  uint32_t q1, M32 m) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint32_t lo = q0 < q1 ? q0 : q1;
+    const uint32_t hi = q0 < q1 ? q1 : q0;
+    const uint64_t b0 = uint64_t{1} << q0, b1 = uint64_t{1} << q1;
+    for (uint64_t g = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < ngroups; g += stride) {
+        const uint64_t base = insert_zero(insert_zero(g, lo), hi);
+        const uint64_t idx[4] = {base, base | b0, base | b1, base | b0 | b1};
+        double2 a[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = st[idx[i]];
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            double2 s = cmul(m.v[8 * o], m.v[8 * o + 1], a[0]);
+#pragma unroll
+            for (int i = 1; i < 4; ++i) s = cadd(s, cmul(m.v[8 * o + 2 * i], m.v[8 * o + 2 * i + 1], a[i]));
+            st[idx[o]] = canon(s);
+        }
+    }
+}
+
+// Diagonal matrices: each amplitude times its entry (dense_kernels.cpp:299-363).
+__global__ void __launch_bounds__(256) k_apply_diag(double2* __restrict__ st, uint64_t n_amps, uint32_t k,
+                                                    uint32_t q0, uint32_t q1, uint32_t q2, uint32_t q3,
+                                                    uint32_t q4, uint32_t q5, D128 d) {
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint32_t q[6] = {q0, q1, q2, q3, q4, q5};
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n_amps; i += stride) {
+        uint32_t e = 0;
+        for (uint32_t j = 0; j < k; ++j) e |= static_cast<uint32_t>((i >> q[j]) & 1u) << j;
+        st[i] = canon(scale_entry(d.v[2 * e], d.v[2 * e + 1], st[i]));
+    }
+}
+
+// The generic k-operand kernel (dense_kernels.cpp:465-524), cooperative per
+// CTA: a batch of groups is gathered into shared memory, each thread then
+// forms whole outputs (sum over `in` in increasing order) and stores them.
+// Dynamic shared memory: the matrix (dim^2) then the batch (kGenBatch amps).
+constexpr uint32_t kGenBatch = 1024;
+__global__ void __launch_bounds__(256) k_apply_generic(double2* __restrict__ st, uint32_t n, uint32_t k,
+                                                       uint32_t q0, uint32_t q1, uint32_t q2, uint32_t q3,
+                                                       uint32_t q4, uint32_t q5,
+                                                       const double2* __restrict__ matrix) {
+    extern __shared__ double2 smem[];
+    const uint32_t dim = 1u << k;
+    double2* mat = smem;
+    double2* buf = smem + dim * dim;
+    const uint32_t q[6] = {q0, q1, q2, q3, q4, q5};
+    uint64_t opmask = 0;
+    for (uint32_t j = 0; j < k; ++j) opmask |= uint64_t{1} << q[j];
+    const uint64_t rest = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~opmask;
+    for (uint32_t i = threadIdx.x; i < dim * dim; i += blockDim.x) mat[i] = matrix[i];
+    const uint64_t ngroups = (uint64_t{1} << n) >> k;
+    const uint32_t per_batch = kGenBatch >> k;  // groups per batch (k <= 6 -> >= 16)
+    const uint64_t nbatches = (ngroups + per_batch - 1) / per_batch;
+    for (uint64_t bt = blockIdx.x; bt < nbatches; bt += gridDim.x) {
+        __syncthreads();
+        // gather
+        for (uint32_t s = threadIdx.x; s < kGenBatch; s += blockDim.x) {
+            const uint64_t g = bt * per_batch + (s >> k);
+            if (g >= ngroups) continue;
+            const uint32_t local = s & (dim - 1);
+            uint64_t idx = pdep64(g, rest);
+            for (uint32_t j = 0; j < k; ++j)
+                if ((local >> j) & 1u) idx |= uint64_t{1} << q[j];
+            buf[s] = st[idx];
+        }
+        __syncthreads();
+        for (uint32_t s = threadIdx.x; s < kGenBatch; s += blockDim.x) {
+            const uint64_t g = bt * per_batch + (s >> k);
+            if (g >= ngroups) continue;
+            const uint32_t out = s & (dim - 1);
+            const double2* grp = buf + (s & ~(dim - 1));
+            double2 acc = cmul(mat[out * dim].x, mat[out * dim].y, grp[0]);
+            for (uint32_t in = 1; in < dim; ++in) acc = cadd(acc, cmul(mat[out * dim + in].x, mat[out * dim + in].y, grp[in]));
+            uint64_t idx = pdep64(g, rest);
+            for (uint32_t j = 0; j < k; ++j)
+                if ((out >> j) & 1u) idx |= uint64_t{1} << q[j];
+            st[idx] = canon(acc);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- tile pass
+// Shared-memory slot of tile-local index l: the low three bits XOR-folded
+// with every higher 3-bit group, so quarter-warps whose eight threads vary
+// three tile bits of distinct residue mod 3 hit eight distinct 16-byte bank
+// groups.
+__device__ __forceinline__ uint32_t swz(uint32_t l) {
+    const uint32_t h = l >> 3;
+    return l ^ ((h ^ (h >> 3) ^ (h >> 6) ^ (h >> 9)) & 7u);
+}
+
+// A TileInstr read as four 64-bit words (fields extracted by shifts, so no
+// field is ever indexed dynamically in local memory).  Layout: bytes 0-3 op,
+// k, kind, nthread; 4-11 pos[8]; 12-15 data; 16-27 tperm[12]; 28-31 aux.
+struct DI {
+    uint64_t w0, w1, w2, w3;
+    __device__ __forceinline__ uint32_t op() const { return static_cast<uint32_t>(w0 & 0xffu); }
+    __device__ __forceinline__ uint32_t k() const { return static_cast<uint32_t>((w0 >> 8) & 0xffu); }
+    __device__ __forceinline__ uint32_t kind() const { return static_cast<uint32_t>((w0 >> 16) & 0xffu); }
+    __device__ __forceinline__ uint32_t nthread() const { return static_cast<uint32_t>((w0 >> 24) & 0xffu); }
+    __device__ __forceinline__ uint32_t pos(uint32_t b) const {
+        return static_cast<uint32_t>((b < 4 ? (w0 >> (32 + 8 * b)) : (w1 >> (8 * (b - 4)))) & 0xffu);
+    }
+    __device__ __forceinline__ uint32_t data() const { return static_cast<uint32_t>(w1 >> 32); }
+    __device__ __forceinline__ uint32_t tperm(uint32_t i) const {
+        return static_cast<uint32_t>((i < 8 ? (w2 >> (8 * i)) : (w3 >> (8 * (i - 8)))) & 0xffu);
+    }
+    __device__ __forceinline__ uint32_t aux() const { return static_cast<uint32_t>(w3 >> 32); }
+};
+
+__device__ __forceinline__ DI load_instr(const TileInstr* p) {
+    const ulonglong2* s = reinterpret_cast<const ulonglong2*>(p);
+    const ulonglong2 a = __ldg(s), b = __ldg(s + 1);
+    return DI{a.x, a.y, b.x, b.y};
+}
+
+template <int P, int KIND>
+__device__ __forceinline__ void g1(double2 (&a)[16], const double* __restrict__ md, uint32_t aux) {
+    const double m00r = __ldg(md + 0), m00i = __ldg(md + 1), m01r = __ldg(md + 2), m01i = __ldg(md + 3);
+    const double m10r = __ldg(md + 4), m10i = __ldg(md + 5), m11r = __ldg(md + 6), m11i = __ldg(md + 7);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if (j & (1 << P)) continue;
+        const double2 x = a[j];
+        const double2 y = a[j | (1 << P)];
+        double2 o0, o1;
+        if (KIND == TK_GEN) {
+            o0 = cadd(cmul(m00r, m00i, x), cmul(m01r, m01i, y));
+            o1 = cadd(cmul(m10r, m10i, x), cmul(m11r, m11i, y));
+        } else if (KIND == TK_U3) {
+            o0 = cadd(cmul_re(m00r, x), cmul(m01r, m01i, y));
+            o1 = cadd(cmul(m10r, m10i, x), cmul(m11r, m11i, y));
+        } else if (KIND == TK_REAL) {
+            o0 = cadd(cmul_re(m00r, x), cmul_re(m01r, y));
+            o1 = cadd(cmul_re(m10r, x), cmul_re(m11r, y));
+        } else {  // TK_MONO: row r takes entry (r, src_r) of column src_r, or is zero
+            const uint32_t s0 = aux & 7u, s1 = (aux >> 3) & 7u;
+            o0 = s0 == 7u ? make_double2(0.0, 0.0)
+                          : scale_entry(s0 ? m01r : m00r, s0 ? m01i : m00i, s0 ? y : x);
+            o1 = s1 == 7u ? make_double2(0.0, 0.0)
+                          : scale_entry(s1 ? m11r : m10r, s1 ? m11i : m10i, s1 ? y : x);
+        }
+        a[j] = o0;
+        a[j | (1 << P)] = o1;
+    }
+}
+
+template <int P0, int P1, int KIND>
+__device__ __forceinline__ void g2(double2 (&a)[16], const double* __restrict__ md, uint32_t aux) {
+    if constexpr (P0 == P1) {
+        return;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            if (j & ((1 << P0) | (1 << P1))) continue;
+            const int idx[4] = {j, j | (1 << P0), j | (1 << P1), j | (1 << P0) | (1 << P1)};
+            const double2 in[4] = {a[idx[0]], a[idx[1]], a[idx[2]], a[idx[3]]};
+            double2 out[4];
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+                if (KIND == TK_MONO) {
+                    const uint32_t s = (aux >> (3 * o)) & 7u;
+                    if (s == 7u) {
+                        out[o] = make_double2(0.0, 0.0);
+                    } else {
+                        const double2 src = s == 0 ? in[0] : s == 1 ? in[1] : s == 2 ? in[2] : in[3];
+                        out[o] = scale_entry(__ldg(md + 8 * o + 2 * s), __ldg(md + 8 * o + 2 * s + 1), src);
+                    }
+                } else {
+                    double2 acc = cmul(__ldg(md + 8 * o), __ldg(md + 8 * o + 1), in[0]);
+#pragma unroll
+                    for (int i = 1; i < 4; ++i)
+                        acc = cadd(acc, cmul(__ldg(md + 8 * o + 2 * i), __ldg(md + 8 * o + 2 * i + 1), in[i]));
+                    out[o] = acc;
+                }
+            }
+#pragma unroll
+            for (int o = 0; o < 4; ++o) a[idx[o]] = out[o];
+        }
+    }
+}
+
+template <int KIND>
+__device__ __forceinline__ void dispatch_g1(int p, double2 (&a)[16], const double* md, uint32_t aux) {
+    switch (p) {
+        case 0: g1<0, KIND>(a, md, aux); break;
+        case 1: g1<1, KIND>(a, md, aux); break;
+        case 2: g1<2, KIND>(a, md, aux); break;
+        default: g1<3, KIND>(a, md, aux); break;
+    }
+}
+
+template <int P0, int KIND>
+__device__ __forceinline__ void dispatch_g2b(int p1, double2 (&a)[16], const double* md, uint32_t aux) {
+    switch (p1) {
+        case 0: g2<P0, 0, KIND>(a, md, aux); break;
+        case 1: g2<P0, 1, KIND>(a, md, aux); break;
+        case 2: g2<P0, 2, KIND>(a, md, aux); break;
+        default: g2<P0, 3, KIND>(a, md, aux); break;
+    }
+}
+
+template <int KIND>
+__device__ __forceinline__ void dispatch_g2(int p0, int p1, double2 (&a)[16], const double* md, uint32_t aux) {
+    switch (p0) {
+        case 0: dispatch_g2b<0, KIND>(p1, a, md, aux); break;
+        case 1: dispatch_g2b<1, KIND>(p1, a, md, aux); break;
+        case 2: dispatch_g2b<2, KIND>(p1, a, md, aux); break;
+        default: dispatch_g2b<3, KIND>(p1, a, md, aux); break;
+    }
+}
+
+__device__ __forceinline__ uint32_t reg_local(uint32_t tb, int j, uint32_t r0, uint32_t r1, uint32_t r2,
+                                              uint32_t r3) {
+    return tb | ((j & 1) ? r0 : 0u) | ((j & 2) ? r1 : 0u) | ((j & 4) ? r2 : 0u) | ((j & 8) ? r3 : 0u);
+}
+
+// cp.async of one 16-byte amplitude, global -> shared (L2 only, no L1).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// One pass of the tiled sweep.  blockDim.x == 2^(m-4) <= 256; each thread
+// owns 16 amplitudes.  Persistent CTAs take tiles round-robin; the next
+// tile is gathered into the second shared-memory buffer with cp.async while
+// the current one is computed, so HBM traffic overlaps the FP64 work.
+__global__ void __launch_bounds__(256, 1)
+    k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m, uint64_t smask, const TileInstr* __restrict__ prog,
+                uint32_t nprog, const double* __restrict__ data, uint64_t ntiles) {
+    extern __shared__ double2 smem_tiles[];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t tbits = m - kRegQubits;
+    const uint32_t tile_amps = 1u << m;
+    // Canonical (load/store) mapping: thread bits = tile bits 0..tbits-1,
+    // register bits = tile bits tbits..m-1.
+    uint64_t off_lo = 0, hib0 = 0, hib1 = 0, hib2 = 0, hib3 = 0;
+    {
+        uint32_t b = 0;
+        for (uint32_t p = 0; p < n; ++p) {
+            if (!((smask >> p) & 1u)) continue;
+            if (b < tbits) {
+                off_lo |= static_cast<uint64_t>((tid >> b) & 1u) << p;
+            } else {
+                const uint64_t v = uint64_t{1} << p;
+                const uint32_t r = b - tbits;
+                if (r == 0) hib0 = v;
+                else if (r == 1) hib1 = v;
+                else if (r == 2) hib2 = v;
+                else hib3 = v;
+            }
+            ++b;
+        }
+    }
+    const uint64_t nmask = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~smask;
+
+    auto prefetch = [&](uint64_t t, double2* buf) {
+        const uint64_t base = pdep64(t, nmask) | off_lo;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const uint64_t off = ((j & 1) ? hib0 : 0) | ((j & 2) ? hib1 : 0) | ((j & 4) ? hib2 : 0) | ((j & 8) ? hib3 : 0);
+            cp_async16(buf + swz(tid | (static_cast<uint32_t>(j) << tbits)), st + (base | off));
+        }
+        cp_async_commit();
+    };
+
+    uint64_t t = blockIdx.x;
+    if (t < ntiles) prefetch(t, smem_tiles);
+    for (uint32_t it = 0; t < ntiles; t += gridDim.x, ++it) {
+        double2* tile = smem_tiles + (it & 1u) * tile_amps;
+        const uint64_t tn = t + gridDim.x;
+        if (tn < ntiles) {
+            prefetch(tn, smem_tiles + ((it + 1) & 1u) * tile_amps);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+
+        double2 a[16];
+        uint32_t pc = 0;
+        while (pc < nprog) {
+            const DI I = load_instr(prog + pc);
+            ++pc;
+            if (I.op() == TOP_PHASE) {
+                uint32_t tb = 0;
+                for (uint32_t i = 0; i < I.nthread(); ++i) tb |= ((tid >> i) & 1u) << I.tperm(i);
+                const uint32_t r0 = 1u << I.pos(0), r1 = 1u << I.pos(1), r2 = 1u << I.pos(2), r3 = 1u << I.pos(3);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) a[j] = tile[swz(reg_local(tb, j, r0, r1, r2, r3))];
+                for (;;) {
+                    const DI G = load_instr(prog + pc);
+                    ++pc;
+                    if (G.op() == TOP_END) break;
+                    const double* md = data + G.data();
+                    if (G.op() == TOP_G1) {
+                        switch (G.kind()) {
+                            case TK_GEN: dispatch_g1<TK_GEN>(G.pos(0), a, md, G.aux()); break;
+                            case TK_U3: dispatch_g1<TK_U3>(G.pos(0), a, md, G.aux()); break;
+                            case TK_REAL: dispatch_g1<TK_REAL>(G.pos(0), a, md, G.aux()); break;
+                            default: dispatch_g1<TK_MONO>(G.pos(0), a, md, G.aux()); break;
+                        }
+                    } else if (G.op() == TOP_G2) {
+                        if (G.kind() == TK_MONO) dispatch_g2<TK_MONO>(G.pos(0), G.pos(1), a, md, G.aux());
+                        else dispatch_g2<TK_GEN>(G.pos(0), G.pos(1), a, md, G.aux());
+                    } else {  // TOP_DIAG
+                        // Entry index bits: from the thread part once, from
+                        // the register part per amplitude.
+                        const uint32_t k = G.k();
+                        uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+                        for (uint32_t b = 0; b < k; ++b) {
+                            const uint32_t pb = G.pos(b);
+                            const uint32_t bit = 1u << pb;
+                            et |= ((tb >> pb) & 1u) << b;
+                            if (bit == r0) e0 = 1u << b;
+                            if (bit == r1) e1 = 1u << b;
+                            if (bit == r2) e2 = 1u << b;
+                            if (bit == r3) e3 = 1u << b;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) | ((j & 4) ? e2 : 0u) |
+                                               ((j & 8) ? e3 : 0u);
+                            a[j] = scale_entry(__ldg(md + 2 * e), __ldg(md + 2 * e + 1), a[j]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 16; ++j) tile[swz(reg_local(tb, j, r0, r1, r2, r3))] = a[j];
+                __syncthreads();
+            } else if (I.op() == TOP_SMEM) {
+                // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
+                const uint32_t k = I.k(), dim = 1u << k;
+                uint32_t opm = 0;
+                for (uint32_t b = 0; b < k; ++b) opm |= 1u << I.pos(b);
+                const double* md = data + I.data();
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const uint32_t l = tid | (static_cast<uint32_t>(j) << tbits);
+                    uint32_t out = 0;
+                    for (uint32_t b = 0; b < k; ++b) out |= ((l >> I.pos(b)) & 1u) << b;
+                    const uint32_t gbase = l & ~opm;
+                    double2 acc = make_double2(0.0, 0.0);
+                    for (uint32_t in = 0; in < dim; ++in) {
+                        uint32_t li = gbase;
+                        for (uint32_t b = 0; b < k; ++b)
+                            if ((in >> b) & 1u) li |= 1u << I.pos(b);
+                        const double2 p = cmul(__ldg(md + 2 * (out * dim + in)), __ldg(md + 2 * (out * dim + in) + 1),
+                                               tile[swz(li)]);
+                        acc = (in == 0) ? p : cadd(acc, p);
+                    }
+                    a[j] = acc;
+                }
+                __syncthreads();
+#pragma unroll
+                for (int j = 0; j < 16; ++j) tile[swz(tid | (static_cast<uint32_t>(j) << tbits))] = a[j];
+                __syncthreads();
+            }
+        }
+
+        // Store: canonical mapping, -0.0 normalised.
+        const uint64_t base = pdep64(t, nmask) | off_lo;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const uint64_t off = ((j & 1) ? hib0 : 0) | ((j & 2) ? hib1 : 0) | ((j & 4) ? hib2 : 0) | ((j & 8) ? hib3 : 0);
+            st[base | off] = canon(tile[swz(tid | (static_cast<uint32_t>(j) << tbits))]);
+        }
+        __syncthreads();  // the buffer is the target of the prefetch two tiles on
+    }
+}
+
+int grid_for(uint64_t work, int threads) {
+    const uint64_t blocks = (work + threads - 1) / threads;
+    return static_cast<int>(blocks < 148ull * 16 ? (blocks == 0 ? 1 : blocks) : 148ull * 16);
+}
+
+int status_of(cudaError_t e) { return e == cudaSuccess ? MB2_OK : MB2_ERR_CUDA; }
+
+}  // namespace
+
+int launch_init(void* amps, uint64_t n_amps, int precision, double re, double im, void* stream) {
+    const auto s = static_cast<cudaStream_t>(stream);
+    if (precision == MB2_C64)
+        k_init_c64<<<grid_for(n_amps, 256), 256, 0, s>>>(static_cast<float2*>(amps), n_amps, static_cast<float>(re),
+                                                        static_cast<float>(im));
+    else
+        k_init_c128<<<grid_for(n_amps, 256), 256, 0, s>>>(static_cast<double2*>(amps), n_amps, re, im);
+    return status_of(cudaGetLastError());
+}
+
+int launch_apply_1q(void* amps, uint32_t n, uint32_t q, const double* m8, void* stream) {
+    M8 m;
+    for (int i = 0; i < 8; ++i) m.v[i] = m8[i];
+    const uint64_t npairs = (uint64_t{1} << n) >> 1;
+    k_apply_1q<<<grid_for(npairs, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<double2*>(amps),
+                                                                                    npairs, q, m);
+    return status_of(cudaGetLastError());
+}
+
+int launch_apply_2q(void* amps, uint32_t n, uint32_t q0, uint32_t q1, const double* m32, void* stream) {
+    M32 m;
+    for (int i = 0; i < 32; ++i) m.v[i] = m32[i];
+    const uint64_t ng = (uint64_t{1} << n) >> 2;
+    k_apply_2q<<<grid_for(ng, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<double2*>(amps), ng, q0,
+                                                                                q1, m);
+    return status_of(cudaGetLastError());
+}
+
+int launch_apply_diag(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* diag, void* stream) {
+    D128 d;
+    const uint32_t dim = 1u << k;
+    for (uint32_t i = 0; i < 2 * dim; ++i) d.v[i] = diag[i];
+    uint32_t qq[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t j = 0; j < k; ++j) qq[j] = q[j];
+    const uint64_t na = uint64_t{1} << n;
+    k_apply_diag<<<grid_for(na, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<double2*>(amps), na, k, qq[0], qq[1], qq[2], qq[3], qq[4], qq[5], d);
+    return status_of(cudaGetLastError());
+}
+
+int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* dev_matrix,
+                         void* stream) {
+    uint32_t qq[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t j = 0; j < k; ++j) qq[j] = q[j];
+    const uint32_t dim = 1u << k;
+    const size_t smem = (size_t{dim} * dim + kGenBatch) * sizeof(double2);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_apply_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        attr_set = true;
+    }
+    const uint64_t ngroups = (uint64_t{1} << n) >> k;
+    const uint64_t nb = (ngroups + (kGenBatch >> k) - 1) / (kGenBatch >> k);
+    const int grid = static_cast<int>(nb < 148ull * 4 ? nb : 148ull * 4);
+    k_apply_generic<<<grid, 256, smem, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<double2*>(amps), n, k, qq[0], qq[1], qq[2], qq[3], qq[4], qq[5],
+        reinterpret_cast<const double2*>(dev_matrix));
+    return status_of(cudaGetLastError());
+}
+
+int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs, const double* dev_data,
+                     int sm_count, void* stream) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_tile_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(2 * (size_t{1} << kMaxTileQubits) * sizeof(double2)));
+        attr_set = true;
+    }
+    if (pass.m > kMaxTileQubits || pass.m < kMinTileQubits) return MB2_ERR_INVALID;
+    const uint32_t threads = 1u << (pass.m - kRegQubits);
+    const size_t smem = 2 * (size_t{1} << pass.m) * sizeof(double2);
+    const uint64_t ntiles = (uint64_t{1} << n) >> pass.m;
+    const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m <= 11 ? 2u : 1u);
+    const int grid = static_cast<int>(ntiles < cap ? ntiles : cap);
+    k_tile_pass<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<double2*>(amps), n, pass.m, pass.smask, dev_instrs + pass.prog_begin, pass.prog_count, dev_data,
+        ntiles);
+    return status_of(cudaGetLastError());
+}
+
+const char* last_cuda_error_string() { return cudaGetErrorString(cudaGetLastError()); }
+
+}  // namespace mb2

@@ -1,0 +1,133 @@
+// Pauli-string expectation and norm reductions (FP64), fixed-order.
+//
+// <psi|P|psi> = i^popcount(x&z) * sum_m conj(psi[m]) psi[m^x] (-1)^popcount(z & (m^x))
+// (src/kernels/cpu/dense_kernels.cpp:544-569).  The pair (m, m^x) is visited
+// once, from the member whose bit h (the highest bit of x) is clear:
+//     t = conj(a_m) a_m'                 (m' = m ^ x)
+//     contribution = t s(m') + conj(t) s(m)
+// so each amplitude is read once per term.  Partial sums land in a fixed
+// number of blocks and are added in block order by one thread per term, so
+// the value does not depend on the GPU's SM count or on what else runs.
+// Like the reference's CUDA reduction (dense_kernels.h:237-246) it is not
+// bitwise the CPU's sequential sum; the parity tests bound the difference.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mb2_internal.h"
+
+namespace mb2 {
+namespace {
+
+__device__ __forceinline__ uint64_t insert_zero(uint64_t i, uint32_t pos) {
+    const uint64_t low = (uint64_t{1} << pos) - 1;
+    return ((i & ~low) << 1) | (i & low);
+}
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ void block_reduce2(double& re, double& im) {
+    __shared__ double sre[kThreads / 32], sim[kThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_down_sync(0xffffffffu, re, o);
+        im += __shfl_down_sync(0xffffffffu, im, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        sre[w] = re;
+        sim[w] = im;
+    }
+    __syncthreads();
+    if (w == 0) {
+        re = l < kThreads / 32 ? sre[l] : 0.0;
+        im = l < kThreads / 32 ? sim[l] : 0.0;
+        for (int o = 4; o > 0; o >>= 1) {
+            re += __shfl_down_sync(0xffffffffu, re, o);
+            im += __shfl_down_sync(0xffffffffu, im, o);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_expectation(const double2* __restrict__ st, uint32_t n, const uint64_t* __restrict__ xs,
+                  const uint64_t* __restrict__ zs, double* __restrict__ partials) {
+    const uint32_t term = blockIdx.y;
+    const uint64_t x = xs[term], z = zs[term];
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    const uint64_t first = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    double re = 0.0, im = 0.0;
+    if (x == 0) {
+        const uint64_t na = uint64_t{1} << n;
+        for (uint64_t m = first; m < na; m += stride) {
+            const double2 a = st[m];
+            const double p = __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
+            re = (__popcll(z & m) & 1) ? __dsub_rn(re, p) : __dadd_rn(re, p);
+        }
+    } else {
+        const uint32_t h = 63 - __clzll(static_cast<long long>(x));
+        const uint64_t np = (uint64_t{1} << n) >> 1;
+        for (uint64_t c = first; c < np; c += stride) {
+            const uint64_t m = insert_zero(c, h);
+            const uint64_t m2 = m ^ x;
+            const double2 a = st[m], b = st[m2];
+            // t = conj(a) * b
+            const double tr = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
+            const double ti = __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x));
+            const bool neg2 = __popcll(z & m2) & 1;  // sign of the (m, m') term
+            const bool neg1 = __popcll(z & m) & 1;   // sign of the (m', m) term, conj(t)
+            re = neg2 ? __dsub_rn(re, tr) : __dadd_rn(re, tr);
+            im = neg2 ? __dsub_rn(im, ti) : __dadd_rn(im, ti);
+            re = neg1 ? __dsub_rn(re, tr) : __dadd_rn(re, tr);
+            im = neg1 ? __dadd_rn(im, ti) : __dsub_rn(im, ti);
+        }
+    }
+    block_reduce2(re, im);
+    if (threadIdx.x == 0) {
+        double* p = partials + 2 * (static_cast<uint64_t>(term) * gridDim.x + blockIdx.x);
+        p[0] = re;
+        p[1] = im;
+    }
+}
+
+// One thread per term: the partials in block order, then i^popcount(x&z).
+__global__ void k_expectation_finish(const double* __restrict__ partials, uint32_t blocks,
+                                     const uint64_t* __restrict__ xs, const uint64_t* __restrict__ zs,
+                                     uint32_t num_terms, double* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= num_terms) return;
+    double re = 0.0, im = 0.0;
+    const double* p = partials + 2 * static_cast<uint64_t>(t) * blocks;
+    for (uint32_t b = 0; b < blocks; ++b) {
+        re = __dadd_rn(re, p[2 * b]);
+        im = __dadd_rn(im, p[2 * b + 1]);
+    }
+    const int ph = __popcll(xs[t] & zs[t]) & 3;
+    double orr = re, oi = im;
+    if (ph == 1) {
+        orr = -im;
+        oi = re;
+    } else if (ph == 2) {
+        orr = -re;
+        oi = -im;
+    } else if (ph == 3) {
+        orr = im;
+        oi = -re;
+    }
+    out[2 * t] = orr;
+    out[2 * t + 1] = oi;
+}
+
+}  // namespace
+
+int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
+                       uint32_t num_terms, double* dev_partials, double* dev_out, void* stream) {
+    if (num_terms == 0) return MB2_OK;
+    const auto s = static_cast<cudaStream_t>(stream);
+    const dim3 grid(kExpBlocks, num_terms);
+    k_expectation<<<grid, kThreads, 0, s>>>(static_cast<const double2*>(amps), n, dev_x, dev_z, dev_partials);
+    k_expectation_finish<<<(num_terms + 127) / 128, 128, 0, s>>>(dev_partials, kExpBlocks, dev_x, dev_z, num_terms,
+                                                                  dev_out);
+    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+}
+
+}  // namespace mb2

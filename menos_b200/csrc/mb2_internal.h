@@ -1,0 +1,129 @@
+// Internal declarations shared by the host C++ and the CUDA translation
+// units of the B200 dense engine.  Nothing here crosses the C ABI.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mb2.h"
+
+namespace mb2 {
+
+using Cd = std::complex<double>;
+
+// ---- gate table (gate_table.cpp) -------------------------------------------
+int gate_num_qubits(int opcode);
+int gate_num_params(int opcode);
+int gate_matrix(int opcode, const double* params, std::vector<Cd>& m);
+Cd initial_phase(double global_phase);
+
+// ---- one block to apply: a matrix on an operand list ----------------------
+// Operand j is bit j of the matrix's row/column index (the reference's
+// operand-order rule, src/kernels/dense_kernels.h:32-37).
+struct Block {
+    uint32_t k = 0;
+    uint32_t q[MB2_MAX_OP_QUBITS] = {0, 0, 0, 0, 0, 0};
+    std::vector<Cd> m;  // (2^k)^2 entries, row-major
+    bool diagonal = false;
+    uint32_t members = 1;  // gates fused into it
+    uint64_t mask() const {
+        uint64_t v = 0;
+        for (uint32_t j = 0; j < k; ++j) v |= uint64_t{1} << q[j];
+        return v;
+    }
+};
+
+// All off-diagonal entries exactly zero (either sign): the reference's
+// is_diagonal (src/kernels/cpu/dense_kernels.cpp:314-324).
+bool is_diagonal(const std::vector<Cd>& m, uint32_t dim);
+
+// ---- fusion (fusion.cpp) ----------------------------------------------------
+// The operations as blocks: with fuse_gates, the reference's containment plan
+// (src/ir/fuse_gates.cpp:190-283) and its block matrices
+// (src/engines/dense/fused_block.cpp:61-99); without, one block per gate.
+// MeasureOps are dropped (they apply nothing).  Throws std::invalid_argument
+// on a malformed op.
+std::vector<Block> build_blocks(const mb2_op* ops, uint32_t n_ops, bool fuse_gates);
+
+// The generic kernel on a host vector (the fused-matrix builder's tool):
+// bitwise kernels::cpu::apply_matrix_generic.
+void host_apply_generic(Cd* state, uint64_t n_amps, const Cd* matrix, const uint32_t* operands,
+                        uint32_t k);
+
+// ---- tiled multi-gate passes (tile_plan.cpp) -------------------------------
+// One device instruction of a tile pass (32 bytes).
+enum TileOp : uint8_t {
+    TOP_PHASE = 1,    // load the registers with the mapping in pos[0..3] / tperm
+    TOP_END = 2,      // write the registers back, barrier
+    TOP_G1 = 3,       // 1-qubit dense gate on register slot pos[0]
+    TOP_G2 = 4,       // 2-qubit dense gate on register slots (pos[0], pos[1])
+    TOP_DIAG = 5,     // diagonal on tile bits pos[0..k-1]
+    TOP_SMEM = 6      // k-qubit dense gate applied from shared memory (own phase)
+};
+enum TileKind : uint8_t {
+    TK_GEN = 0,   // every entry general
+    TK_U3 = 1,    // 1q: entry (0,0) real, the others general
+    TK_REAL = 2,  // 1q: every entry real
+    TK_MONO = 3   // 1 nonzero entry per row: a permutation up to per-row factors
+};
+struct TileInstr {
+    uint8_t op;
+    uint8_t k;
+    uint8_t kind;
+    uint8_t nthread;   // PHASE: number of thread bits in tperm
+    uint8_t pos[8];
+    uint32_t data;     // offset (doubles) of the gate's data in the data block
+    uint8_t tperm[12];
+    uint32_t aux;      // MONO: per-row source slots (2 bits each)
+};
+static_assert(sizeof(TileInstr) == 32, "TileInstr is 32 bytes");
+
+struct TilePass {
+    uint32_t m = 0;          // tile qubits
+    uint64_t smask = 0;      // global qubits in the tile
+    uint32_t prog_begin = 0; // first instruction
+    uint32_t prog_count = 0;
+    uint32_t gates = 0;      // blocks applied in this pass
+};
+
+struct TileProgram {
+    std::vector<TilePass> passes;
+    std::vector<uint32_t> order;       // block indices in application order
+    std::vector<uint32_t> order_pass;  // the pass of each entry of `order`
+    std::vector<TileInstr> instrs;
+    std::vector<double> data;
+    uint64_t fp64_per_amp = 0;  // modelled FP64 instructions per amplitude
+};
+
+// Register qubits per thread in the tile kernel (16 amplitudes per thread).
+constexpr uint32_t kRegQubits = 4;
+constexpr uint32_t kMaxTileQubits = 12;
+constexpr uint32_t kMinTileQubits = 4;
+
+// Low qubits every tile holds by default (runs of 2^3 amplitudes, 128 bytes).
+constexpr uint32_t kDefaultFixedLow = 3;
+TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint32_t m,
+                              uint32_t fixed_low = kDefaultFixedLow);
+
+// ---- device launches (kernels_*.cu) ----------------------------------------
+struct DevCtx;  // forward (engine.cpp)
+int launch_init(void* amps, uint64_t n_amps, int precision, double re, double im, void* stream);
+int launch_apply_1q(void* amps, uint32_t n, uint32_t q, const double* m8, void* stream);
+int launch_apply_2q(void* amps, uint32_t n, uint32_t q0, uint32_t q1, const double* m32, void* stream);
+int launch_apply_diag(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* dev_diag,
+                      void* stream);
+int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* dev_matrix,
+                         void* stream);
+int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
+                     const double* dev_data, int sm_count, void* stream);
+// Expectation of num_terms Pauli terms: partials (num_terms * kExpBlocks * 2
+// doubles) then the fixed-order finish into out (num_terms * 2 doubles), all
+// device pointers.
+constexpr uint32_t kExpBlocks = 512;
+int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
+                       uint32_t num_terms, double* dev_partials, double* dev_out, void* stream);
+const char* last_cuda_error_string();
+
+}  // namespace mb2

@@ -1,0 +1,263 @@
+// Host planner of the multi-gate tiled sweep.
+//
+// A pass loads every tile of 2^m amplitudes -- the amplitudes that share
+// their bits outside a set S of m qubits -- into shared memory once, applies
+// a run of blocks whose operands lie in S, and writes the tile back once.
+// A pass applies a run of consecutive blocks, in their order, and per
+// amplitude the arithmetic of every block is exactly the per-gate kernel's,
+// so the state after the sweep is bitwise the one the reference's
+// block-by-block sweep gives
+// (src/engines/dense/fused_block.h:60-101, src/engines/dense/dense_engine.cpp:65-112).
+//
+// Inside a pass each thread holds 16 amplitudes in registers (4 "register
+// qubits"); a PHASE instruction picks which 4 tile qubits those are, and the
+// blocks of the phase act on registers only.  Diagonal blocks need no pairing
+// and run in any phase.  Blocks wider than 2 dense qubits run from shared
+// memory (TOP_SMEM).
+#include <algorithm>
+#include <bit>
+#include <stdexcept>
+
+#include "mb2_internal.h"
+
+namespace mb2 {
+namespace {
+
+
+uint32_t local_pos(uint64_t smask, uint32_t q) {
+    return static_cast<uint32_t>(std::popcount(smask & ((uint64_t{1} << q) - 1)));
+}
+
+bool is_real(const Cd& c) { return c.imag() == 0.0; }
+bool is_zero(const Cd& c) { return c.real() == 0.0 && c.imag() == 0.0; }
+
+// Row r's single nonzero column, -1 for an all-zero row, -2 if the row has more.
+int mono_src(const std::vector<Cd>& m, uint32_t dim, uint32_t r) {
+    int src = -1;
+    for (uint32_t c = 0; c < dim; ++c) {
+        if (!is_zero(m[r * dim + c])) {
+            if (src != -1) return -2;
+            src = static_cast<int>(c);
+        }
+    }
+    return src;
+}
+
+struct PassSel {
+    uint64_t smask;
+    std::vector<uint32_t> gates;  // block indices in application order
+};
+
+// Passes are maximal runs of CONSECUTIVE blocks whose operands fit one
+// tile.  Blocks are never reordered, not even commuting ones: two gates on
+// disjoint qubits applied in the other order give the same state only up to
+// rounding, and the plain path is bitwise the reference's sweep, which
+// applies the blocks in plan order.
+std::vector<PassSel> select_passes(const std::vector<Block>& blocks, uint32_t n, uint32_t m, uint32_t fixed_low) {
+    std::vector<PassSel> passes;
+    uint32_t widest = 1;
+    for (const Block& b : blocks) widest = std::max(widest, b.k);
+    const uint32_t mt = std::min(m, n);
+    if (widest > mt) throw std::invalid_argument("a block is wider than the tile");
+    // Low qubits kept in every tile so that tiles gather contiguous runs,
+    // leaving room for the widest block.
+    const uint32_t fixed = std::min(fixed_low, mt - widest);
+    size_t i = 0;
+    while (i < blocks.size()) {
+        uint64_t smask = 0;
+        for (uint32_t q = 0; q < fixed; ++q) smask |= uint64_t{1} << q;
+        PassSel sel;
+        while (i < blocks.size()) {
+            const uint64_t grown = smask | blocks[i].mask();
+            if (static_cast<uint32_t>(std::popcount(grown)) > mt) break;
+            smask = grown;
+            sel.gates.push_back(static_cast<uint32_t>(i));
+            ++i;
+        }
+        // Pad the tile to exactly mt qubits with the lowest unused ones.
+        for (uint32_t q = 0; q < n && static_cast<uint32_t>(std::popcount(smask)) < mt; ++q)
+            smask |= uint64_t{1} << q;
+        sel.smask = smask;
+        passes.push_back(std::move(sel));
+    }
+    return passes;
+}
+
+// Thread-bit order for a phase whose register bits are `reg` (tile-local
+// positions): the first three thread bits get distinct residues mod 3 when
+// possible, so that the eight threads of a quarter warp hit eight distinct
+// 16-byte bank groups under the kernel's XOR-fold swizzle.
+void thread_order(uint32_t m, const uint32_t* reg, uint32_t nreg, uint8_t* tperm, uint8_t& nthread) {
+    std::vector<uint32_t> free_pos;
+    for (uint32_t p = 0; p < m; ++p)
+        if (std::find(reg, reg + nreg, p) == reg + nreg) free_pos.push_back(p);
+    std::vector<uint32_t> order;
+    for (uint32_t res = 0; res < 3; ++res) {
+        for (uint32_t p : free_pos)
+            if (p % 3 == res && std::find(order.begin(), order.end(), p) == order.end()) {
+                order.push_back(p);
+                break;
+            }
+    }
+    if (order.size() < 3) order.clear();
+    for (uint32_t p : free_pos)
+        if (std::find(order.begin(), order.end(), p) == order.end()) order.push_back(p);
+    nthread = static_cast<uint8_t>(order.size());
+    for (size_t i = 0; i < order.size(); ++i) tperm[i] = static_cast<uint8_t>(order[i]);
+}
+
+uint32_t push_matrix(std::vector<double>& data, const std::vector<Cd>& m) {
+    const uint32_t off = static_cast<uint32_t>(data.size());
+    for (const Cd& c : m) {
+        data.push_back(c.real());
+        data.push_back(c.imag());
+    }
+    return off;
+}
+
+}  // namespace
+
+TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint32_t m, uint32_t fixed_low) {
+    if (m < kMinTileQubits || m > kMaxTileQubits) throw std::invalid_argument("tile width out of range");
+    TileProgram prog;
+    const uint32_t mt = std::min(m, n);
+    if (mt < kRegQubits) throw std::invalid_argument("state too small for the tile kernel");
+    const std::vector<PassSel> sels = select_passes(blocks, n, mt, fixed_low);
+    for (const PassSel& sel : sels) {
+        TilePass pass;
+        pass.m = mt;
+        pass.smask = sel.smask;
+        pass.prog_begin = static_cast<uint32_t>(prog.instrs.size());
+        pass.gates = static_cast<uint32_t>(sel.gates.size());
+
+        bool open = false;
+        uint32_t reg[kRegQubits] = {0, 1, 2, 3};
+        auto in_reg = [&](uint32_t p) -> int {
+            for (uint32_t s = 0; s < kRegQubits; ++s)
+                if (reg[s] == p) return static_cast<int>(s);
+            return -1;
+        };
+        auto close_phase = [&]() {
+            if (open) {
+                TileInstr e{};
+                e.op = TOP_END;
+                prog.instrs.push_back(e);
+                open = false;
+            }
+        };
+        // Opens a phase whose registers hold `first` (in order), filled from
+        // the dense 1q/2q blocks that follow position `from` in this pass.
+        auto open_phase = [&](const std::vector<uint32_t>& first, size_t from) {
+            close_phase();
+            std::vector<uint32_t> r(first);
+            for (size_t j = from; j < sel.gates.size() && r.size() < kRegQubits; ++j) {
+                const Block& b = blocks[sel.gates[j]];
+                if (b.diagonal || b.k > 2) continue;
+                bool fits = true;
+                uint32_t extra = 0;
+                for (uint32_t t = 0; t < b.k; ++t)
+                    if (std::find(r.begin(), r.end(), local_pos(sel.smask, b.q[t])) == r.end()) ++extra;
+                if (r.size() + extra > kRegQubits) fits = false;
+                if (!fits) continue;
+                for (uint32_t t = 0; t < b.k; ++t) {
+                    const uint32_t p = local_pos(sel.smask, b.q[t]);
+                    if (std::find(r.begin(), r.end(), p) == r.end()) r.push_back(p);
+                }
+            }
+            for (uint32_t p = 0; p < mt && r.size() < kRegQubits; ++p)
+                if (std::find(r.begin(), r.end(), p) == r.end()) r.push_back(p);
+            for (uint32_t s = 0; s < kRegQubits; ++s) reg[s] = r[s];
+            TileInstr ph{};
+            ph.op = TOP_PHASE;
+            for (uint32_t s = 0; s < kRegQubits; ++s) ph.pos[s] = static_cast<uint8_t>(reg[s]);
+            thread_order(mt, reg, kRegQubits, ph.tperm, ph.nthread);
+            prog.instrs.push_back(ph);
+            open = true;
+        };
+
+        for (size_t j = 0; j < sel.gates.size(); ++j) {
+            const Block& b = blocks[sel.gates[j]];
+            const uint32_t dim = 1u << b.k;
+            prog.order.push_back(sel.gates[j]);
+            prog.order_pass.push_back(static_cast<uint32_t>(prog.passes.size()));
+            TileInstr g{};
+            g.k = static_cast<uint8_t>(b.k);
+            if (b.diagonal) {
+                if (!open) open_phase({}, j + 1);
+                g.op = TOP_DIAG;
+                for (uint32_t t = 0; t < b.k; ++t) g.pos[t] = static_cast<uint8_t>(local_pos(sel.smask, b.q[t]));
+                std::vector<Cd> d(dim);
+                for (uint32_t i = 0; i < dim; ++i) d[i] = b.m[i * dim + i];
+                g.data = push_matrix(prog.data, d);
+                prog.instrs.push_back(g);
+                prog.fp64_per_amp += 6;
+                continue;
+            }
+            if (b.k <= 2) {
+                int slot[2] = {-1, -1};
+                bool have = open;
+                for (uint32_t t = 0; t < b.k && have; ++t) {
+                    slot[t] = in_reg(local_pos(sel.smask, b.q[t]));
+                    if (slot[t] < 0) have = false;
+                }
+                if (!have) {
+                    std::vector<uint32_t> first;
+                    for (uint32_t t = 0; t < b.k; ++t) first.push_back(local_pos(sel.smask, b.q[t]));
+                    open_phase(first, j + 1);
+                    for (uint32_t t = 0; t < b.k; ++t) slot[t] = in_reg(local_pos(sel.smask, b.q[t]));
+                }
+                g.op = b.k == 1 ? TOP_G1 : TOP_G2;
+                g.pos[0] = static_cast<uint8_t>(slot[0]);
+                if (b.k == 2) g.pos[1] = static_cast<uint8_t>(slot[1]);
+                // Specialisations, each exact up to the sign of zero results
+                // (normalised at the store): monomial rows, real entries.
+                bool mono = true;
+                uint32_t aux = 0;
+                for (uint32_t r = 0; r < dim; ++r) {
+                    const int s = mono_src(b.m, dim, r);
+                    if (s == -2) {
+                        mono = false;
+                        break;
+                    }
+                    aux |= static_cast<uint32_t>(s < 0 ? 7 : s) << (3 * r);
+                }
+                if (mono) {
+                    g.kind = TK_MONO;
+                    g.aux = aux;
+                    prog.fp64_per_amp += 6;
+                } else if (b.k == 1) {
+                    const bool all_real = is_real(b.m[0]) && is_real(b.m[1]) && is_real(b.m[2]) && is_real(b.m[3]);
+                    if (all_real) {
+                        g.kind = TK_REAL;
+                        prog.fp64_per_amp += 6;
+                    } else if (is_real(b.m[0])) {
+                        g.kind = TK_U3;
+                        prog.fp64_per_amp += 12;
+                    } else {
+                        g.kind = TK_GEN;
+                        prog.fp64_per_amp += 14;
+                    }
+                } else {
+                    g.kind = TK_GEN;
+                    prog.fp64_per_amp += 30;
+                }
+                g.data = push_matrix(prog.data, b.m);
+                prog.instrs.push_back(g);
+                continue;
+            }
+            // Wider dense block: from shared memory, as a phase of its own.
+            close_phase();
+            g.op = TOP_SMEM;
+            for (uint32_t t = 0; t < b.k; ++t) g.pos[t] = static_cast<uint8_t>(local_pos(sel.smask, b.q[t]));
+            g.data = push_matrix(prog.data, b.m);
+            prog.instrs.push_back(g);
+            prog.fp64_per_amp += 8ull * dim - 2;
+        }
+        close_phase();
+        pass.prog_count = static_cast<uint32_t>(prog.instrs.size()) - pass.prog_begin;
+        prog.passes.push_back(pass);
+    }
+    return prog;
+}
+
+}  // namespace mb2

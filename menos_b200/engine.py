@@ -1,0 +1,232 @@
+"""Python side of the engine: device contexts, device states and the
+``B200DenseEngine`` that mirrors the reference's ``SimulationEngine``
+interface for the dense statevector path
+(include/menos/simulation_engine.h:322-367; request/result fields :141-234).
+
+Everything computes through libmenos_b200.so; nothing here has a CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import C128, C64, SweepOptions, SweepStats, check, lib
+from .circuit import Circuit, to_mb2_ops
+
+
+class Context:
+    """One device (reference: DeviceInfo + DevicePool set-up,
+    src/kernels/cuda/device_info.h:14-55)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        rc = lib().mb2_context_create(device, C.byref(h))
+        if rc != _lib.MB2_OK:
+            raise _lib.MB2Error(rc, f"mb2_context_create(device={device})")
+        self.h = h
+        self.device = device
+
+    def close(self) -> None:
+        if self.h:
+            lib().mb2_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        sm, tot, fr = C.c_int(), C.c_uint64(), C.c_uint64()
+        check(lib().mb2_device_info(self.h, C.byref(sm), C.byref(tot), C.byref(fr)), self.h, "device_info")
+        return {"sm_count": sm.value, "total_bytes": tot.value, "free_bytes": fr.value}
+
+
+class DeviceState:
+    """A statevector in device memory (reference: DeviceBuffer,
+    src/kernels/cuda/device_buffer.h:25-55)."""
+
+    def __init__(self, ctx: Context, num_qubits: int, precision: int = C128, budget_bytes: int = 2 ** 64 - 1):
+        h = C.c_void_p()
+        check(lib().mb2_state_alloc(ctx.h, num_qubits, precision, min(budget_bytes, 2 ** 64 - 1), C.byref(h)),
+              ctx.h, "mb2_state_alloc")
+        self.ctx = ctx
+        self.h = h
+        self.n = num_qubits
+        self.precision = precision
+
+    def free(self) -> None:
+        if self.h:
+            lib().mb2_state_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t this state's work is queued on (as an int)."""
+        h = C.c_void_p()
+        self._chk(lib().mb2_state_stream(self.h, C.byref(h)), "mb2_state_stream")
+        return h.value or 0
+
+    def _chk(self, rc, what):
+        check(rc, self.ctx.h, what)
+
+    def init(self, global_phase: float = 0.0) -> None:
+        self._chk(lib().mb2_init(self.h, global_phase), "mb2_init")
+
+    def apply_matrix(self, matrix, operands, generic: bool = False) -> None:
+        m = np.ascontiguousarray(np.asarray(matrix, np.complex128)).view(np.float64).ravel()
+        q = np.ascontiguousarray(np.asarray(operands, np.uint32))
+        f = lib().mb2_apply_matrix_generic if generic else lib().mb2_apply_matrix
+        self._chk(f(self.h, m.ctypes.data, q.ctypes.data, len(q)), "mb2_apply_matrix")
+
+    def apply_program(self, circ: Circuit, fuse_gates: bool = True, tile_qubits: int = 0,
+                      per_gate: bool = False) -> SweepStats:
+        arr, keep = to_mb2_ops(circ)
+        opts = SweepOptions(1 if fuse_gates else 0, 0, tile_qubits, 1 if per_gate else 0)
+        self._chk(lib().mb2_apply_program(self.h, arr, len(circ.ops), C.byref(opts)), "mb2_apply_program")
+        del keep
+        return self.stats()
+
+    def stats(self) -> SweepStats:
+        s = SweepStats()
+        self._chk(lib().mb2_last_sweep_stats(self.h, C.byref(s)), "stats")
+        return s
+
+    def expectation(self, paulis: Sequence[tuple]) -> np.ndarray:
+        """paulis: (x_mask, z_mask) pairs -> complex128 array (coefficients not applied)."""
+        if len(paulis) == 0:
+            return np.zeros(0, np.complex128)
+        xs = np.ascontiguousarray([int(p[0]) for p in paulis], dtype=np.uint64)
+        zs = np.ascontiguousarray([int(p[1]) for p in paulis], dtype=np.uint64)
+        out = np.zeros(2 * len(paulis), np.float64)
+        self._chk(lib().mb2_expectation(self.h, xs.ctypes.data, zs.ctypes.data, len(paulis), out.ctypes.data),
+                  "mb2_expectation")
+        return out.view(np.complex128).copy()
+
+    def norm(self) -> float:
+        v = C.c_double()
+        self._chk(lib().mb2_norm(self.h, C.byref(v)), "mb2_norm")
+        return v.value
+
+    def sample(self, shots: int, seed: int, targets) -> dict:
+        t = np.ascontiguousarray(np.asarray(targets, np.uint32).ravel())
+        cap = max(int(shots), 1)
+        outc = np.zeros(cap, np.uint64)
+        cnt = np.zeros(cap, np.uint64)
+        nout = C.c_uint64(cap)
+        self._chk(lib().mb2_sample(self.h, shots, seed, t.ctypes.data if len(t) else None, len(t) // 2,
+                                   outc.ctypes.data, cnt.ctypes.data, C.byref(nout)), "mb2_sample")
+        d = nout.value
+        return {int(o): int(c) for o, c in zip(outc[:d], cnt[:d])}
+
+    def copy_out(self) -> np.ndarray:
+        dt = np.complex128 if self.precision == C128 else np.complex64
+        out = np.zeros(1 << self.n, dt)
+        self._chk(lib().mb2_copy_out(self.h, out.ctypes.data, out.size), "mb2_copy_out")
+        return out
+
+    def copy_in(self, amps: np.ndarray) -> None:
+        dt = np.complex128 if self.precision == C128 else np.complex64
+        a = np.ascontiguousarray(amps, dtype=dt)
+        self._chk(lib().mb2_copy_in(self.h, a.ctypes.data, a.size), "mb2_copy_in")
+
+    def synchronize(self) -> None:
+        self._chk(lib().mb2_synchronize(self.h), "mb2_synchronize")
+
+
+# ---------------------------------------------------------------------------
+# The SimulationEngine mirror.
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass
+class PauliTerm:
+    x_mask: int
+    z_mask: int
+    coefficient: complex = 1.0
+
+
+@dataclasses.dataclass
+class EngineExecutionRequest:
+    """menos::EngineExecutionRequest (include/menos/simulation_engine.h:141-198),
+    the fields a dense engine reads."""
+    num_qubits: int
+    operations: Circuit
+    want_statevector: bool = False
+    want_counts: bool = False
+    want_expectation: bool = False
+    shots: int = 0
+    measure_targets: Sequence[tuple] = ()
+    bitstring_width: int = 0
+    seed: int = 0
+    global_phase: float = 0.0
+    budget_bytes: int = 2 ** 64 - 1
+    is_sole_region: bool = True
+    observable: Optional[Sequence[PauliTerm]] = None
+    fuse_gates: bool = True
+
+
+@dataclasses.dataclass
+class EngineExecutionResult:
+    """menos::EngineExecutionResult (simulation_engine.h:227-236)."""
+    statevector: Optional[np.ndarray] = None
+    counts: Optional[dict] = None
+    expectation_terms: Optional[np.ndarray] = None
+    actual_bytes: int = 0
+    sweep: Optional[dict] = None
+
+
+class B200DenseEngine:
+    """The dense statevector engine on one B200: {Dense, Cuda, InMemory}
+    (the triple src/plan/execution_engines.cpp:37-45 resolves)."""
+
+    def __init__(self, device: int = 0, tile_qubits: int = 0):
+        self.ctx = Context(device)
+        self.tile_qubits = tile_qubits
+
+    def name(self) -> str:
+        return "dense_b200"
+
+    def engine_id(self) -> str:
+        return "dense"
+
+    def backend(self) -> str:
+        return "cuda"
+
+    def tier(self) -> str:
+        return "in_memory"
+
+    def capabilities(self) -> dict:
+        return {"counts": True, "statevector": True, "expectation": True}
+
+    def execute(self, req: EngineExecutionRequest) -> EngineExecutionResult:
+        """CudaDenseEngine::execute's contract
+        (src/engines/dense_cuda/cuda_dense_engine.cpp:325-412)."""
+        for oc, *_ in req.operations.ops:
+            if oc > 22 or oc < 0:
+                raise _lib.MB2Error(6, "unsupported operation")
+        st = DeviceState(self.ctx, req.num_qubits, C128, req.budget_bytes)
+        try:
+            st.init(req.global_phase)
+            stats = st.apply_program(req.operations, fuse_gates=req.fuse_gates, tile_qubits=self.tile_qubits)
+            res = EngineExecutionResult(actual_bytes=16 << req.num_qubits,
+                                        sweep={"blocks": stats.blocks, "passes": stats.passes,
+                                               "launches": stats.launches})
+            if req.want_expectation:
+                terms = list(req.observable or [])
+                res.expectation_terms = st.expectation([(t.x_mask, t.z_mask) for t in terms])
+            if req.want_counts:
+                res.counts = st.sample(req.shots, req.seed, list(req.measure_targets))
+            if req.want_statevector:
+                res.statevector = st.copy_out()
+            return res
+        finally:
+            st.free()

@@ -1,0 +1,146 @@
+"""Seeded synthetic workloads of the dense statevector path.
+
+No public benchmark suite stands behind these; they are the circuit families
+the engine is measured on, generated from a fixed seeding convention:
+  * angles come from std::mt19937_64(seed), each uniform as the reference's
+    common::Rng maps a word, (w >> 11) * 2^-53 (src/common/rng.cpp:184-186),
+    scaled to the stated interval;
+  * a Pauli string takes one word per qubit, w % 4 -> I / X / Y / Z;
+  * weights are N(0, 1) by Box-Muller from the same stream.
+
+Families:
+  brick(n, depth, seed)       U3(theta, phi, lambda in [0, 2pi)) on every qubit, then CZ on
+                              (0,1),(2,3),... on even layers, (1,2),(3,4),... on odd layers
+  qft(n)                      H(j), CP(2pi / 2^(k-j+1)) on (k, j) for k > j, then the final swaps
+  hea(n, layers, seed)        RY(theta) RZ(phi) on every qubit (angles in [-pi, pi)) + CX(q, q+1) ladder
+  pauli_strings(n, count, seed), weights(count, seed)
+"""
+from __future__ import annotations
+
+import math
+
+from .circuit import Circuit
+
+_MASK64 = (1 << 64) - 1
+
+
+class MT19937_64:
+    """The 64-bit Mersenne Twister (Matsumoto & Nishimura), with the
+    parameters the C++ standard fixes for std::mt19937_64."""
+
+    def __init__(self, seed: int):
+        mt = [0] * 312
+        mt[0] = seed & _MASK64
+        for i in range(1, 312):
+            mt[i] = (6364136223846793005 * (mt[i - 1] ^ (mt[i - 1] >> 62)) + i) & _MASK64
+        self.mt = mt
+        self.idx = 312
+
+    def _twist(self):
+        mt = self.mt
+        for i in range(312):
+            y = (mt[i] & 0xFFFFFFFF80000000) | (mt[(i + 1) % 312] & 0x7FFFFFFF)
+            v = mt[(i + 156) % 312] ^ (y >> 1)
+            if y & 1:
+                v ^= 0xB5026F5AA96619E9
+            mt[i] = v
+        self.idx = 0
+
+    def next_word(self) -> int:
+        if self.idx >= 312:
+            self._twist()
+        x = self.mt[self.idx]
+        self.idx += 1
+        x ^= (x >> 29) & 0x5555555555555555
+        x ^= (x << 17) & 0x71D67FFFEDA60000
+        x ^= (x << 37) & 0xFFF7EEE000000000
+        x ^= x >> 43
+        return x & _MASK64
+
+    def uniform(self) -> float:
+        """(w >> 11) * 2^-53, exactly as common::Rng::word_to_uniform."""
+        return float(self.next_word() >> 11) * (1.0 / 9007199254740992.0)
+
+
+TWO_PI = 2.0 * math.pi
+
+
+def brick(n: int, depth: int, seed: int, circ: Circuit | None = None) -> Circuit:
+    c = circ if circ is not None else Circuit(n)
+    rng = MT19937_64(seed)
+    for layer in range(depth):
+        for q in range(n):
+            theta = TWO_PI * rng.uniform()
+            phi = TWO_PI * rng.uniform()
+            lam = TWO_PI * rng.uniform()
+            c.gate("u", [q], [theta, phi, lam])
+        start = 0 if layer % 2 == 0 else 1
+        for q in range(start, n - 1, 2):
+            c.gate("cz", [q, q + 1])
+    return c
+
+
+def qft(n: int, circ: Circuit | None = None) -> Circuit:
+    c = circ if circ is not None else Circuit(n)
+    for j in range(n):
+        c.gate("h", [j])
+        for k in range(j + 1, n):
+            c.gate("cp", [k, j], [TWO_PI / float(1 << (k - j + 1))])
+    for i in range(n // 2):
+        c.gate("swap", [i, n - 1 - i])
+    return c
+
+
+def hea(n: int, layers: int, seed: int, circ: Circuit | None = None) -> Circuit:
+    c = circ if circ is not None else Circuit(n)
+    rng = MT19937_64(seed)
+    for _ in range(layers):
+        for q in range(n):
+            theta = -math.pi + TWO_PI * rng.uniform()
+            phi = -math.pi + TWO_PI * rng.uniform()
+            c.gate("ry", [q], [theta])
+            c.gate("rz", [q], [phi])
+        for q in range(n - 1):
+            c.gate("cx", [q, q + 1])
+    return c
+
+
+def pauli_strings(n: int, count: int, seed: int):
+    """(x_mask, z_mask) pairs; per qubit w % 4 -> I, X, Y, Z."""
+    rng = MT19937_64(seed)
+    out = []
+    for _ in range(count):
+        x = z = 0
+        for q in range(n):
+            r = rng.next_word() % 4
+            if r == 1:
+                x |= 1 << q
+            elif r == 2:
+                x |= 1 << q
+                z |= 1 << q
+            elif r == 3:
+                z |= 1 << q
+        out.append((x, z))
+    return out
+
+
+def weights(count: int, seed: int):
+    """N(0,1) by Box-Muller on (1 - u1, u2)."""
+    rng = MT19937_64(seed)
+    out = []
+    for _ in range(count):
+        u1 = 1.0 - rng.uniform()
+        u2 = rng.uniform()
+        out.append(math.sqrt(-2.0 * math.log(u1)) * math.cos(TWO_PI * u2))
+    return out
+
+
+def config_c1(seed: int = 20260929) -> Circuit:
+    """20 qubits, 20 brick layers (statevector + 4096 shots)."""
+    return brick(20, 20, seed)
+
+
+def config_c2(n: int = 30, depth: int = 40, seed: int = 20260929) -> Circuit:
+    """The 30-qubit complex128 workload: brick depth 40, then a full QFT."""
+    c = brick(n, depth, seed)
+    return qft(n, c)

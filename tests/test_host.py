@@ -1,0 +1,136 @@
+"""Host-side product checks that need no GPU: the C ABI's exports, the gate
+table, the seeded workloads, and the tiled sweep's block schedule (its
+reordering applied on the CPU oracle must be bitwise the plain sweep)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from menos_b200 import _lib, workloads
+from menos_b200.circuit import OP, Circuit, to_mb2_ops
+from test_oracle_pin import bits_equal, random_circuit
+
+
+def declared_functions():
+    with open(os.path.join(ROOT, "include", "mb2.h")) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"^int\s+(mb2_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_every_declared_symbol_is_exported():
+    L = C.CDLL(_lib.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(L, name), name
+        assert name in _lib.SIGNATURES, name
+
+
+def test_no_device_is_reported_cleanly():
+    # On a machine without a GPU the context refuses loudly; with one it opens.
+    h = C.c_void_p()
+    rc = _lib.lib().mb2_context_create(0, C.byref(h))
+    if rc == 0:
+        _lib.lib().mb2_context_destroy(h)
+    else:
+        assert rc == 4
+
+
+@pytest.mark.parametrize("opcode", range(21))
+def test_gate_table_bitwise(oracle, opcode):
+    rng = np.random.default_rng(opcode)
+    for _ in range(8):
+        p = np.zeros(3)
+        p[:] = rng.uniform(-9, 9, size=3)
+        out = np.zeros(128, np.float64)
+        assert _lib.lib().mb2_gate_matrix(opcode, p.ctypes.data, out.ctypes.data, 128) == 0
+        ref = oracle.gate_matrix(opcode, p)
+        assert bits_equal(out[:2 * ref.size], ref.view(np.float64).ravel())
+
+
+def test_gate_table_rejects_non_gates():
+    out = np.zeros(128, np.float64)
+    assert _lib.lib().mb2_gate_matrix(OP["unitary"], None, out.ctypes.data, 128) == 1
+    assert _lib.lib().mb2_gate_matrix(OP["measure"], None, out.ctypes.data, 128) == 1
+
+
+def test_workload_rng_is_mt19937_64(oracle):
+    for seed in (0, 5, 20260929):
+        rng = workloads.MT19937_64(seed)
+        ours = [rng.next_word() for _ in range(700)]
+        assert ours == [int(w) for w in oracle.words(seed, 700)]
+
+
+def test_workload_shapes():
+    c1 = workloads.config_c1()
+    assert sum(1 for o in c1.ops if o[0] == OP["u"]) == 400
+    assert sum(1 for o in c1.ops if o[0] == OP["cz"]) == 190
+    c2 = workloads.config_c2()
+    assert sum(1 for o in c2.ops if o[0] == OP["u"]) == 1200
+    assert sum(1 for o in c2.ops if o[0] == OP["cz"]) == 580
+    assert sum(1 for o in c2.ops if o[0] == OP["cp"]) == 435
+    assert sum(1 for o in c2.ops if o[0] == OP["swap"]) == 15
+    h = workloads.hea(16, 8, 1)
+    assert sum(1 for o in h.ops if o[0] == OP["cx"]) == 8 * 15
+    ps = workloads.pauli_strings(30, 64, 3)
+    assert len(ps) == 64 and all(x < (1 << 30) and z < (1 << 30) for x, z in ps)
+
+
+def schedule(circ, n, fuse=True, tile=0, per_gate=False):
+    arr, keep = to_mb2_ops(circ)
+    opts = _lib.SweepOptions(1 if fuse else 0, 0, tile, 1 if per_gate else 0)
+    cap = 4 * len(circ.ops) + 4
+    pas = np.zeros(cap, np.uint32)
+    ks = np.zeros(cap, np.uint32)
+    qs = np.zeros(6 * cap, np.uint32)
+    mats = np.zeros(cap * 2 * 4096, np.float64)
+    nb = C.c_uint64(cap)
+    ml = C.c_uint64(mats.size)
+    rc = _lib.lib().mb2_debug_schedule(arr, len(circ.ops), C.byref(opts), n, pas.ctypes.data, ks.ctypes.data,
+                                       qs.ctypes.data, mats.ctypes.data, C.byref(nb), C.byref(ml))
+    assert rc == 0
+    out, off = [], 0
+    for i in range(nb.value):
+        k = int(ks[i])
+        d = 1 << k
+        m = mats[off:off + 2 * d * d].view(np.complex128).reshape(d, d)
+        off += 2 * d * d
+        out.append((int(pas[i]), list(qs[6 * i:6 * i + k]), m))
+    return out
+
+
+def as_oracle_circuit(c):
+    import pyoracle
+    oc = pyoracle.Circuit(c.num_qubits, c.global_phase)
+    oc.ops = list(c.ops)
+    return oc
+
+
+@pytest.mark.parametrize("tile", [4, 5, 7, 12])
+def test_tiled_schedule_is_bitwise_the_plain_sweep(oracle, tile):
+    rng = np.random.default_rng(tile)
+    for n in (4, 6, 9, 11, 13):
+        for fuse in (True, False):
+            c = random_circuit(n, 80, rng)
+            c.num_clbits = 0
+            sched = schedule(c, n, fuse=fuse, tile=tile)
+            state = oracle.initialize(n, c.global_phase)
+            passes = [p for p, _, _ in sched]
+            assert passes == sorted(passes)
+            for _p, qs, m in sched:
+                oracle.apply_generic(state, m, qs)
+            expect = oracle.run(as_oracle_circuit(c), fuse_gates=fuse)
+            assert bits_equal(state, expect), (n, fuse, tile)
+
+
+def test_brick_schedule_pass_count():
+    c = workloads.brick(30, 40, 1)
+    workloads.qft(30, c)
+    sched = schedule(c, 30, fuse=True, tile=12)
+    passes = max(p for p, _, _ in sched) + 1
+    # runs of consecutive blocks (never reordered): ~300 passes instead of
+    # one per block (2260 blocks)
+    assert passes < 400, passes
