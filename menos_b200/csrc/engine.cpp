@@ -371,33 +371,19 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
         for (uint64_t i = 0; i < shots; ++i) u[i] = static_cast<double>(eng() >> 11) * (1.0 / 9007199254740992.0);
     }
     std::sort(u.begin(), u.end());
-    // The sequential walk (sample.cpp:55-69) over the state, streamed back
-    // in chunks through a pinned buffer.
-    const uint64_t na = uint64_t{1} << s->n;
-    const uint64_t chunk = std::min<uint64_t>(na, uint64_t{1} << 22);
-    double* pinned = nullptr;
-    MB2_CUDA(s->ctx, cudaMallocHost(reinterpret_cast<void**>(&pinned), chunk * 16));
+    // The walk (sample.cpp:55-69), reproduced exactly on the device.
+    const size_t al_u = (shots * 8 + 255) & ~size_t{255};
+    const size_t need = 2 * al_u + mb2::sample_scratch_bytes(s->n, shots);
+    if (int e = ensure_scratch(s, need); e != MB2_OK) return e;
+    auto* base = static_cast<unsigned char*>(s->scratch);
+    auto* dev_u = reinterpret_cast<double*>(base);
+    auto* dev_basis = reinterpret_cast<uint64_t*>(base + al_u);
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(dev_u, u.data(), shots * 8, cudaMemcpyHostToDevice, s->stream));
+    const int rc = mb2::launch_sample(s->amps, s->n, dev_u, shots, base + 2 * al_u, dev_basis, s->stream);
+    if (rc != MB2_OK) return fail(s->ctx, rc, std::string("sample launch: ") + mb2::last_cuda_error_string());
     std::vector<uint64_t> basis(shots);
-    double cumulative = 0.0;
-    uint64_t shot = 0;
-    int rc = MB2_OK;
-    for (uint64_t c0 = 0; c0 < na && shot < shots; c0 += chunk) {
-        const cudaError_t e1 = cudaMemcpyAsync(pinned, static_cast<const unsigned char*>(s->amps) + c0 * 16,
-                                               chunk * 16, cudaMemcpyDeviceToHost, s->stream);
-        const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamSynchronize(s->stream) : e1;
-        if (e2 != cudaSuccess) {
-            rc = cuda_fail(s->ctx, e2, "sample copy");
-            break;
-        }
-        for (uint64_t i = 0; i < chunk && shot < shots; ++i) {
-            const double re = pinned[2 * i], im = pinned[2 * i + 1];
-            cumulative += re * re + im * im;
-            while (shot < shots && u[shot] < cumulative) basis[shot++] = c0 + i;
-        }
-    }
-    cudaFreeHost(pinned);
-    if (rc != MB2_OK) return rc;
-    while (shot < shots) basis[shot++] = na - 1;
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(basis.data(), dev_basis, shots * 8, cudaMemcpyDeviceToHost, s->stream));
+    MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
     // Outcomes through the measure targets, ascending, with counts.
     std::vector<uint64_t> oc(shots);
     for (uint64_t i = 0; i < shots; ++i) {

@@ -124,6 +124,14 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileIns
 constexpr uint32_t kExpBlocks = 512;
 int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
                        uint32_t num_terms, double* dev_partials, double* dev_out, void* stream);
+// Exact device sampler (kernels_sample.cu): the chunk size of its scan, the
+// scratch its internals need (beyond the sorted uniforms and the per-shot
+// basis output), and the launch.  dev_basis[s] receives the basis state of
+// the s-th smallest uniform.
+constexpr uint32_t kSampleChunk = 4096;
+size_t sample_scratch_bytes(uint32_t n, uint64_t shots);
+int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
+                  uint64_t* dev_basis, void* stream);
 const char* last_cuda_error_string();
 
 }  // namespace mb2
