@@ -198,6 +198,7 @@ def main():
         counts = st.sample(args.shots, 1234, targets)
         return stats, norm, terms, counts
 
+    fp64_peak, copy_peak = ctx.probe_rates()
     for _ in range(args.warmup):
         stats, norm, terms, counts = step()
     assert abs(norm - 1.0) < 1e-9, norm
@@ -275,6 +276,11 @@ def main():
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": 2 * state_bytes},
+        "fp64": {"kernel": "k_tile_pass", "achieved_ops_per_s": round(stats.fp64_ops_per_amp * (1 << n) /
+                                                                     (sweep_avg * 1e-3), 1),
+                 "peak_ops_per_s": round(fp64_peak, 1), "peak_source": "measured (mb2_probe_rates)",
+                 "frac": round(stats.fp64_ops_per_amp * (1 << n) / (sweep_avg * 1e-3) / fp64_peak, 4),
+                 "model_ops_per_amp": int(stats.fp64_ops_per_amp), "copy_gbs_probe": round(copy_peak, 1)},
         "e2e": {"value": round(world * args.steps / e2e_s, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": args.steps * (passes + 1 + 2 + 2),

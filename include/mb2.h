@@ -158,6 +158,14 @@ int mb2_copy_in(mb2_state* state, const void* host, uint64_t num_amplitudes);
 /* Waits for all work queued on the state's stream. */
 int mb2_synchronize(mb2_state* state);
 
+/* ---- calibration ------------------------------------------------------- */
+/* Measures the device's FP64 multiply/add issue rate (instructions per
+ * second) and its device-to-device copy bandwidth (read+write GB/s), for the
+ * planner's CUDA time model and the roofline.  Replaces the reference's
+ * device microbenchmarks (src/kernels/cuda/device_benchmarks.h:30-67) feeding
+ * CudaCalibration (src/plan/cuda_calibration.h:9-48). */
+int mb2_probe_rates(mb2_context* ctx, double* fp64_ops_per_s, double* copy_gbs);
+
 /* ---- host-side reference pieces (no device work) ----------------------- */
 /* Gate matrix, bitwise ir::generate_matrix (src/ir/gate_table.cpp:260).
  * out: 2*4^k doubles; returns MB2_ERR_INVALID for UNITARY/MEASURE. */

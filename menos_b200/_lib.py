@@ -37,6 +37,7 @@ SIGNATURES = {
     "mb2_context_destroy": (C.c_int, [_VP]),
     "mb2_last_error": (C.c_int, [_VP, C.c_char_p, C.c_size_t]),
     "mb2_device_info": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "mb2_probe_rates": (C.c_int, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mb2_state_alloc": (C.c_int, [_VP, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(_VP)]),
     "mb2_state_free": (C.c_int, [_VP]),
     "mb2_init": (C.c_int, [_VP, C.c_double]),

@@ -181,6 +181,14 @@ int mb2_device_info(mb2_context* ctx, int* sm_count, uint64_t* total_bytes, uint
     return MB2_OK;
 }
 
+int mb2_probe_rates(mb2_context* ctx, double* fp64_ops_per_s, double* copy_gbs) {
+    if (ctx == nullptr || fp64_ops_per_s == nullptr || copy_gbs == nullptr) return MB2_ERR_INVALID;
+    MB2_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int rc = mb2::probe_rates(ctx->sm_count, fp64_ops_per_s, copy_gbs);
+    if (rc != MB2_OK) return fail(ctx, rc, "probe_rates failed");
+    return MB2_OK;
+}
+
 int mb2_state_alloc(mb2_context* ctx, uint32_t num_qubits, int precision, uint64_t budget_bytes, mb2_state** out) {
     if (ctx == nullptr || out == nullptr) return MB2_ERR_INVALID;
     *out = nullptr;

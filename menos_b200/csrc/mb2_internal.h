@@ -132,6 +132,9 @@ constexpr uint32_t kSampleChunk = 4096;
 size_t sample_scratch_bytes(uint32_t n, uint64_t shots);
 int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
                   uint64_t* dev_basis, void* stream);
+// Calibration probes (kernels_probe.cu): FP64 instructions per second and
+// device-to-device copy GB/s (read + write bytes), on the current device.
+int probe_rates(int sm_count, double* fp64_per_s, double* copy_gbs);
 const char* last_cuda_error_string();
 
 }  // namespace mb2

@@ -41,6 +41,12 @@ class Context:
         except Exception:
             pass
 
+    def probe_rates(self):
+        """(FP64 instructions/s, device copy GB/s) measured on this device."""
+        f, c = C.c_double(), C.c_double()
+        check(lib().mb2_probe_rates(self.h, C.byref(f), C.byref(c)), self.h, "probe_rates")
+        return f.value, c.value
+
     def info(self):
         sm, tot, fr = C.c_int(), C.c_uint64(), C.c_uint64()
         check(lib().mb2_device_info(self.h, C.byref(sm), C.byref(tot), C.byref(fr)), self.h, "device_info")
