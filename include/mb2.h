@@ -123,6 +123,30 @@ typedef struct mb2_sweep_options {
  * 337-355).  opts may be NULL (defaults: reference fusion on, autotuned tile). */
 int mb2_apply_program(mb2_state* state, const mb2_op* ops, uint32_t num_ops,
                       const mb2_sweep_options* opts);
+/* As mb2_apply_program, calling `boundary(user, blocks_done)` on the host
+ * after each pass has completed on the device: the state is then complete
+ * and consistent, the reference's safe boundary (ExecutionMonitor::
+ * at_safe_boundary, include/menos/simulation_engine.h:94-116).  A nonzero
+ * return abandons the sweep: MB2_ERR_ABANDONED, the state as of that pass. */
+typedef int (*mb2_boundary_fn)(void* user, uint64_t blocks_done);
+int mb2_apply_program_monitored(mb2_state* state, const mb2_op* ops, uint32_t num_ops,
+                                const mb2_sweep_options* opts, mb2_boundary_fn boundary, void* user);
+
+/* What a sweep of these ops on a num_qubits state costs the device, without
+ * running it: the planner's DeviceCost (include/menos/plan.h:117-122) and the
+ * dense work units of DenseEngine::estimate (src/engines/dense/dense_engine.cpp:309-331). */
+typedef struct mb2_sweep_estimate {
+    uint64_t blocks;
+    uint64_t passes;
+    uint64_t launches;
+    uint64_t device_bytes;     /* state + staging */
+    uint64_t h2d_bytes;        /* program upload */
+    uint64_t work_units;       /* 2^n + sum over blocks of 2^(n+k) */
+    uint64_t fp64_ops_per_amp;
+} mb2_sweep_estimate;
+int mb2_estimate_sweep(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
+                       uint32_t num_qubits, mb2_sweep_estimate* out);
+
 /* Statistics of the last mb2_apply_program on this state. */
 typedef struct mb2_sweep_stats {
     uint64_t blocks;         /* blocks applied (after fusion) */

@@ -24,6 +24,15 @@ class SweepOptions(C.Structure):
                 ("per_gate", C.c_int32)]
 
 
+class SweepEstimate(C.Structure):
+    _fields_ = [("blocks", C.c_uint64), ("passes", C.c_uint64), ("launches", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("h2d_bytes", C.c_uint64), ("work_units", C.c_uint64),
+                ("fp64_ops_per_amp", C.c_uint64)]
+
+
+BOUNDARY_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64)
+
+
 class SweepStats(C.Structure):
     _fields_ = [("blocks", C.c_uint64), ("passes", C.c_uint64), ("launches", C.c_uint64),
                 ("fp64_ops_per_amp", C.c_uint64)]
@@ -46,6 +55,10 @@ SIGNATURES = {
     "mb2_apply_matrix": (C.c_int, [_VP, _VP, _VP, C.c_uint32]),
     "mb2_apply_matrix_generic": (C.c_int, [_VP, _VP, _VP, C.c_uint32]),
     "mb2_apply_program": (C.c_int, [_VP, C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions)]),
+    "mb2_apply_program_monitored": (C.c_int, [_VP, C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions),
+                                              BOUNDARY_FN, _VP]),
+    "mb2_estimate_sweep": (C.c_int, [C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions), C.c_uint32,
+                                     C.POINTER(SweepEstimate)]),
     "mb2_last_sweep_stats": (C.c_int, [_VP, C.POINTER(SweepStats)]),
     "mb2_expectation": (C.c_int, [_VP, _VP, _VP, C.c_uint32, _VP]),
     "mb2_norm": (C.c_int, [_VP, C.POINTER(C.c_double)]),

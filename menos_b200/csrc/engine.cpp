@@ -262,7 +262,8 @@ int mb2_apply_matrix_generic(mb2_state* s, const double* matrix, const uint32_t*
     return apply_block(s, reinterpret_cast<const mb2::Cd*>(matrix), operands, k, true);
 }
 
-int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts) {
+int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
+                                mb2_boundary_fn boundary, void* user) {
     if (s == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
     if (s->precision != MB2_C128) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "mb2_apply_program: complex128 states only");
     mb2_sweep_options o{1, 0, 0, 0};
@@ -287,6 +288,10 @@ int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const m
         for (const mb2::Block& b : blocks) {
             if (int e = apply_block(s, b.m.data(), b.q, b.k, false); e != MB2_OK) return e;
             s->stats.passes += 1;
+            if (boundary != nullptr) {
+                MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+                if (boundary(user, s->stats.passes) != 0) return fail(s->ctx, MB2_ERR_ABANDONED, "sweep abandoned");
+            }
         }
         return MB2_OK;
     }
@@ -307,13 +312,55 @@ int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const m
     MB2_CUDA(s->ctx, cudaMemcpyAsync(s->scratch, host.data(), host.size(), cudaMemcpyHostToDevice, s->stream));
     const auto* dev_instrs = static_cast<const mb2::TileInstr*>(s->scratch);
     const auto* dev_data = reinterpret_cast<const double*>(static_cast<unsigned char*>(s->scratch) + doff);
+    s->stats.fp64_ops_per_amp = prog.fp64_per_amp;
+    uint64_t done = 0;
     for (const mb2::TilePass& pass : prog.passes) {
         const int rc = mb2::launch_tile_pass(s->amps, s->n, pass, dev_instrs, dev_data, s->ctx->sm_count, s->stream);
         if (rc != MB2_OK) return fail(s->ctx, rc, std::string("tile pass launch: ") + mb2::last_cuda_error_string());
+        s->stats.passes += 1;
+        s->stats.launches += 1;
+        done += pass.gates;
+        if (boundary != nullptr) {
+            MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+            if (boundary(user, done) != 0) return fail(s->ctx, MB2_ERR_ABANDONED, "sweep abandoned");
+        }
     }
-    s->stats.passes = prog.passes.size();
-    s->stats.launches = prog.passes.size();
-    s->stats.fp64_ops_per_amp = prog.fp64_per_amp;
+    return MB2_OK;
+}
+
+int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts) {
+    return mb2_apply_program_monitored(s, ops, num_ops, opts, nullptr, nullptr);
+}
+
+int mb2_estimate_sweep(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
+                       mb2_sweep_estimate* out) {
+    if (out == nullptr || (ops == nullptr && num_ops != 0) || num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
+    mb2_sweep_options o{1, 0, 0, 0};
+    if (opts != nullptr) o = *opts;
+    *out = mb2_sweep_estimate{};
+    try {
+        const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+        out->blocks = blocks.size();
+        out->work_units = uint64_t{1} << num_qubits;
+        for (const mb2::Block& b : blocks) out->work_units += uint64_t{1} << (num_qubits + b.k);
+        out->device_bytes = (uint64_t{1} << num_qubits) * 16;
+        if (o.per_gate != 0 || num_qubits < mb2::kMinTileQubits || blocks.empty()) {
+            out->passes = blocks.size();
+            out->launches = blocks.size() + 1;
+            for (const mb2::Block& b : blocks) out->h2d_bytes += 16ull << (2 * b.k);
+        } else {
+            const uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, num_qubits,
+                                          blocks);
+            const mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m);
+            out->passes = prog.passes.size();
+            out->launches = prog.passes.size() + 1;
+            out->h2d_bytes = prog.instrs.size() * sizeof(mb2::TileInstr) + prog.data.size() * sizeof(double);
+            out->fp64_ops_per_amp = prog.fp64_per_amp;
+        }
+        out->device_bytes += out->h2d_bytes;
+    } catch (const std::exception&) {
+        return MB2_ERR_INVALID;
+    }
     return MB2_OK;
 }
 

@@ -230,12 +230,15 @@ __device__ __forceinline__ DI load_instr(const TileInstr* p) {
     return DI{a.x, a.y, b.x, b.y};
 }
 
+constexpr int kR = static_cast<int>(kRegQubits);  // register qubits per thread
+constexpr int kNA = 1 << kR;                         // amplitudes per thread
+
 template <int P, int KIND>
-__device__ __forceinline__ void g1(double2 (&a)[16], const double* __restrict__ md, uint32_t aux) {
-    const double m00r = __ldg(md + 0), m00i = __ldg(md + 1), m01r = __ldg(md + 2), m01i = __ldg(md + 3);
-    const double m10r = __ldg(md + 4), m10i = __ldg(md + 5), m11r = __ldg(md + 6), m11i = __ldg(md + 7);
+__device__ __forceinline__ void g1(double2 (&a)[kNA], const double* __restrict__ md, uint32_t aux) {
+    const double m00r = md[0], m00i = md[1], m01r = md[2], m01i = md[3];
+    const double m10r = md[4], m10i = md[5], m11r = md[6], m11i = md[7];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
+    for (int j = 0; j < kNA; ++j) {
         if (j & (1 << P)) continue;
         const double2 x = a[j];
         const double2 y = a[j | (1 << P)];
@@ -262,12 +265,12 @@ __device__ __forceinline__ void g1(double2 (&a)[16], const double* __restrict__ 
 }
 
 template <int P0, int P1, int KIND>
-__device__ __forceinline__ void g2(double2 (&a)[16], const double* __restrict__ md, uint32_t aux) {
+__device__ __forceinline__ void g2(double2 (&a)[kNA], const double* __restrict__ md, uint32_t aux) {
     if constexpr (P0 == P1) {
         return;
     } else {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < kNA; ++j) {
             if (j & ((1 << P0) | (1 << P1))) continue;
             const int idx[4] = {j, j | (1 << P0), j | (1 << P1), j | (1 << P0) | (1 << P1)};
             const double2 in[4] = {a[idx[0]], a[idx[1]], a[idx[2]], a[idx[3]]};
@@ -280,13 +283,12 @@ __device__ __forceinline__ void g2(double2 (&a)[16], const double* __restrict__ 
                         out[o] = make_double2(0.0, 0.0);
                     } else {
                         const double2 src = s == 0 ? in[0] : s == 1 ? in[1] : s == 2 ? in[2] : in[3];
-                        out[o] = scale_entry(__ldg(md + 8 * o + 2 * s), __ldg(md + 8 * o + 2 * s + 1), src);
+                        out[o] = scale_entry(md[8 * o + 2 * s], md[8 * o + 2 * s + 1], src);
                     }
                 } else {
-                    double2 acc = cmul(__ldg(md + 8 * o), __ldg(md + 8 * o + 1), in[0]);
+                    double2 acc = cmul(md[8 * o], md[8 * o + 1], in[0]);
 #pragma unroll
-                    for (int i = 1; i < 4; ++i)
-                        acc = cadd(acc, cmul(__ldg(md + 8 * o + 2 * i), __ldg(md + 8 * o + 2 * i + 1), in[i]));
+                    for (int i = 1; i < 4; ++i) acc = cadd(acc, cmul(md[8 * o + 2 * i], md[8 * o + 2 * i + 1], in[i]));
                     out[o] = acc;
                 }
             }
@@ -297,38 +299,41 @@ __device__ __forceinline__ void g2(double2 (&a)[16], const double* __restrict__ 
 }
 
 template <int KIND>
-__device__ __forceinline__ void dispatch_g1(int p, double2 (&a)[16], const double* md, uint32_t aux) {
+__device__ __forceinline__ void dispatch_g1(int p, double2 (&a)[kNA], const double* md, uint32_t aux) {
+    static_assert(kR == 3, "dispatch written for 3 register qubits");
     switch (p) {
         case 0: g1<0, KIND>(a, md, aux); break;
         case 1: g1<1, KIND>(a, md, aux); break;
-        case 2: g1<2, KIND>(a, md, aux); break;
-        default: g1<3, KIND>(a, md, aux); break;
-    }
-}
-
-template <int P0, int KIND>
-__device__ __forceinline__ void dispatch_g2b(int p1, double2 (&a)[16], const double* md, uint32_t aux) {
-    switch (p1) {
-        case 0: g2<P0, 0, KIND>(a, md, aux); break;
-        case 1: g2<P0, 1, KIND>(a, md, aux); break;
-        case 2: g2<P0, 2, KIND>(a, md, aux); break;
-        default: g2<P0, 3, KIND>(a, md, aux); break;
+        default: g1<2, KIND>(a, md, aux); break;
     }
 }
 
 template <int KIND>
-__device__ __forceinline__ void dispatch_g2(int p0, int p1, double2 (&a)[16], const double* md, uint32_t aux) {
-    switch (p0) {
-        case 0: dispatch_g2b<0, KIND>(p1, a, md, aux); break;
-        case 1: dispatch_g2b<1, KIND>(p1, a, md, aux); break;
-        case 2: dispatch_g2b<2, KIND>(p1, a, md, aux); break;
-        default: dispatch_g2b<3, KIND>(p1, a, md, aux); break;
+__device__ __forceinline__ void dispatch_g2(int p0, int p1, double2 (&a)[kNA], const double* md, uint32_t aux) {
+    switch (p0 * 3 + p1) {
+        case 1: g2<0, 1, KIND>(a, md, aux); break;
+        case 2: g2<0, 2, KIND>(a, md, aux); break;
+        case 3: g2<1, 0, KIND>(a, md, aux); break;
+        case 5: g2<1, 2, KIND>(a, md, aux); break;
+        case 6: g2<2, 0, KIND>(a, md, aux); break;
+        case 7: g2<2, 1, KIND>(a, md, aux); break;
+        default: break;
     }
 }
 
-__device__ __forceinline__ uint32_t reg_local(uint32_t tb, int j, uint32_t r0, uint32_t r1, uint32_t r2,
-                                              uint32_t r3) {
-    return tb | ((j & 1) ? r0 : 0u) | ((j & 2) ? r1 : 0u) | ((j & 4) ? r2 : 0u) | ((j & 8) ? r3 : 0u);
+// Tile-local index of register slot j: thread part | the register bits.
+__device__ __forceinline__ uint32_t reg_local(uint32_t tb, int j, const uint32_t (&rb)[kR]) {
+    uint32_t l = tb;
+#pragma unroll
+    for (int b = 0; b < kR; ++b) l |= ((j >> b) & 1) ? rb[b] : 0u;
+    return l;
+}
+
+__device__ __forceinline__ uint64_t reg_offset(int j, const uint64_t (&hib)[kR]) {
+    uint64_t o = 0;
+#pragma unroll
+    for (int b = 0; b < kR; ++b) o |= ((j >> b) & 1) ? hib[b] : 0ull;
+    return o;
 }
 
 // cp.async of one 16-byte amplitude, global -> shared (L2 only, no L1).
@@ -340,20 +345,27 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// One pass of the tiled sweep.  blockDim.x == 2^(m-4) <= 256; each thread
-// owns 16 amplitudes.  Persistent CTAs take tiles round-robin; the next
+// One pass of the tiled sweep.  blockDim.x == 2^(m-3) <= 512; each thread
+// owns 8 amplitudes.  Persistent CTAs take tiles round-robin; the next
 // tile is gathered into the second shared-memory buffer with cp.async while
-// the current one is computed, so HBM traffic overlaps the FP64 work.
-__global__ void __launch_bounds__(256, 1)
+// the current one is computed, so HBM traffic overlaps the FP64 work.  The
+// pass's instructions are staged in shared memory once per CTA.
+__global__ void __launch_bounds__(512, 1)
     k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m, uint64_t smask, const TileInstr* __restrict__ prog,
                 uint32_t nprog, const double* __restrict__ data, uint64_t ntiles) {
     extern __shared__ double2 smem_tiles[];
     const uint32_t tid = threadIdx.x;
     const uint32_t tbits = m - kRegQubits;
     const uint32_t tile_amps = 1u << m;
+    TileInstr* sprog = reinterpret_cast<TileInstr*>(smem_tiles + 2 * tile_amps);
+    for (uint32_t i = tid; i < nprog * 2; i += blockDim.x)
+        reinterpret_cast<ulonglong2*>(sprog)[i] = __ldg(reinterpret_cast<const ulonglong2*>(prog) + i);
     // Canonical (load/store) mapping: thread bits = tile bits 0..tbits-1,
     // register bits = tile bits tbits..m-1.
-    uint64_t off_lo = 0, hib0 = 0, hib1 = 0, hib2 = 0, hib3 = 0;
+    uint64_t off_lo = 0;
+    uint64_t hib[kR];
+#pragma unroll
+    for (int b = 0; b < kR; ++b) hib[b] = 0;
     {
         uint32_t b = 0;
         for (uint32_t p = 0; p < n; ++p) {
@@ -361,12 +373,9 @@ __global__ void __launch_bounds__(256, 1)
             if (b < tbits) {
                 off_lo |= static_cast<uint64_t>((tid >> b) & 1u) << p;
             } else {
-                const uint64_t v = uint64_t{1} << p;
-                const uint32_t r = b - tbits;
-                if (r == 0) hib0 = v;
-                else if (r == 1) hib1 = v;
-                else if (r == 2) hib2 = v;
-                else hib3 = v;
+#pragma unroll
+                for (int r = 0; r < kR; ++r)
+                    if (static_cast<uint32_t>(r) == b - tbits) hib[r] = uint64_t{1} << p;
             }
             ++b;
         }
@@ -376,10 +385,8 @@ __global__ void __launch_bounds__(256, 1)
     auto prefetch = [&](uint64_t t, double2* buf) {
         const uint64_t base = pdep64(t, nmask) | off_lo;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const uint64_t off = ((j & 1) ? hib0 : 0) | ((j & 2) ? hib1 : 0) | ((j & 4) ? hib2 : 0) | ((j & 8) ? hib3 : 0);
-            cp_async16(buf + swz(tid | (static_cast<uint32_t>(j) << tbits)), st + (base | off));
-        }
+        for (int j = 0; j < kNA; ++j)
+            cp_async16(buf + swz(tid | (static_cast<uint32_t>(j) << tbits)), st + (base | reg_offset(j, hib)));
         cp_async_commit();
     };
 
@@ -396,19 +403,21 @@ __global__ void __launch_bounds__(256, 1)
         }
         __syncthreads();
 
-        double2 a[16];
+        double2 a[kNA];
         uint32_t pc = 0;
         while (pc < nprog) {
-            const DI I = load_instr(prog + pc);
+            const DI I = load_instr(sprog + pc);
             ++pc;
             if (I.op() == TOP_PHASE) {
                 uint32_t tb = 0;
                 for (uint32_t i = 0; i < I.nthread(); ++i) tb |= ((tid >> i) & 1u) << I.tperm(i);
-                const uint32_t r0 = 1u << I.pos(0), r1 = 1u << I.pos(1), r2 = 1u << I.pos(2), r3 = 1u << I.pos(3);
+                uint32_t rb[kR];
 #pragma unroll
-                for (int j = 0; j < 16; ++j) a[j] = tile[swz(reg_local(tb, j, r0, r1, r2, r3))];
+                for (int b = 0; b < kR; ++b) rb[b] = 1u << I.pos(b);
+#pragma unroll
+                for (int j = 0; j < kNA; ++j) a[j] = tile[swz(reg_local(tb, j, rb))];
                 for (;;) {
-                    const DI G = load_instr(prog + pc);
+                    const DI G = load_instr(sprog + pc);
                     ++pc;
                     if (G.op() == TOP_END) break;
                     const double* md = data + G.data();
@@ -426,26 +435,28 @@ __global__ void __launch_bounds__(256, 1)
                         // Entry index bits: from the thread part once, from
                         // the register part per amplitude.
                         const uint32_t k = G.k();
-                        uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+                        uint32_t et = 0;
+                        uint32_t er[kR];
+#pragma unroll
+                        for (int r = 0; r < kR; ++r) er[r] = 0;
                         for (uint32_t b = 0; b < k; ++b) {
-                            const uint32_t pb = G.pos(b);
-                            const uint32_t bit = 1u << pb;
-                            et |= ((tb >> pb) & 1u) << b;
-                            if (bit == r0) e0 = 1u << b;
-                            if (bit == r1) e1 = 1u << b;
-                            if (bit == r2) e2 = 1u << b;
-                            if (bit == r3) e3 = 1u << b;
+                            const uint32_t bit = 1u << G.pos(b);
+                            et |= ((tb & bit) ? 1u : 0u) << b;
+#pragma unroll
+                            for (int r = 0; r < kR; ++r)
+                                if (bit == rb[r]) er[r] = 1u << b;
                         }
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) | ((j & 4) ? e2 : 0u) |
-                                               ((j & 8) ? e3 : 0u);
-                            a[j] = scale_entry(__ldg(md + 2 * e), __ldg(md + 2 * e + 1), a[j]);
+                        for (int j = 0; j < kNA; ++j) {
+                            uint32_t e = et;
+#pragma unroll
+                            for (int r = 0; r < kR; ++r) e |= ((j >> r) & 1) ? er[r] : 0u;
+                            a[j] = scale_entry(md[2 * e], md[2 * e + 1], a[j]);
                         }
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < 16; ++j) tile[swz(reg_local(tb, j, r0, r1, r2, r3))] = a[j];
+                for (int j = 0; j < kNA; ++j) tile[swz(reg_local(tb, j, rb))] = a[j];
                 __syncthreads();
             } else if (I.op() == TOP_SMEM) {
                 // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
@@ -454,7 +465,7 @@ __global__ void __launch_bounds__(256, 1)
                 for (uint32_t b = 0; b < k; ++b) opm |= 1u << I.pos(b);
                 const double* md = data + I.data();
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
+                for (int j = 0; j < kNA; ++j) {
                     const uint32_t l = tid | (static_cast<uint32_t>(j) << tbits);
                     uint32_t out = 0;
                     for (uint32_t b = 0; b < k; ++b) out |= ((l >> I.pos(b)) & 1u) << b;
@@ -464,15 +475,14 @@ __global__ void __launch_bounds__(256, 1)
                         uint32_t li = gbase;
                         for (uint32_t b = 0; b < k; ++b)
                             if ((in >> b) & 1u) li |= 1u << I.pos(b);
-                        const double2 p = cmul(__ldg(md + 2 * (out * dim + in)), __ldg(md + 2 * (out * dim + in) + 1),
-                                               tile[swz(li)]);
+                        const double2 p = cmul(md[2 * (out * dim + in)], md[2 * (out * dim + in) + 1], tile[swz(li)]);
                         acc = (in == 0) ? p : cadd(acc, p);
                     }
                     a[j] = acc;
                 }
                 __syncthreads();
 #pragma unroll
-                for (int j = 0; j < 16; ++j) tile[swz(tid | (static_cast<uint32_t>(j) << tbits))] = a[j];
+                for (int j = 0; j < kNA; ++j) tile[swz(tid | (static_cast<uint32_t>(j) << tbits))] = a[j];
                 __syncthreads();
             }
         }
@@ -480,10 +490,8 @@ __global__ void __launch_bounds__(256, 1)
         // Store: canonical mapping, -0.0 normalised.
         const uint64_t base = pdep64(t, nmask) | off_lo;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const uint64_t off = ((j & 1) ? hib0 : 0) | ((j & 2) ? hib1 : 0) | ((j & 4) ? hib2 : 0) | ((j & 8) ? hib3 : 0);
-            st[base | off] = canon(tile[swz(tid | (static_cast<uint32_t>(j) << tbits))]);
-        }
+        for (int j = 0; j < kNA; ++j)
+            st[base | reg_offset(j, hib)] = canon(tile[swz(tid | (static_cast<uint32_t>(j) << tbits))]);
         __syncthreads();  // the buffer is the target of the prefetch two tiles on
     }
 }
@@ -559,15 +567,18 @@ int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, 
 
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs, const double* dev_data,
                      int sm_count, void* stream) {
+    constexpr size_t kMaxProgBytes = 32 * 1024;
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_tile_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(2 * (size_t{1} << kMaxTileQubits) * sizeof(double2)));
+                             static_cast<int>(2 * (size_t{1} << kMaxTileQubits) * sizeof(double2) + kMaxProgBytes));
         attr_set = true;
     }
     if (pass.m > kMaxTileQubits || pass.m < kMinTileQubits) return MB2_ERR_INVALID;
+    const size_t prog_bytes = size_t{pass.prog_count} * sizeof(TileInstr);
+    if (prog_bytes > kMaxProgBytes) return MB2_ERR_INVALID;
     const uint32_t threads = 1u << (pass.m - kRegQubits);
-    const size_t smem = 2 * (size_t{1} << pass.m) * sizeof(double2);
+    const size_t smem = 2 * (size_t{1} << pass.m) * sizeof(double2) + prog_bytes;
     const uint64_t ntiles = (uint64_t{1} << n) >> pass.m;
     const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m <= 11 ? 2u : 1u);
     const int grid = static_cast<int>(ntiles < cap ? ntiles : cap);

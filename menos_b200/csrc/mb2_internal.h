@@ -55,7 +55,7 @@ void host_apply_generic(Cd* state, uint64_t n_amps, const Cd* matrix, const uint
 // ---- tiled multi-gate passes (tile_plan.cpp) -------------------------------
 // One device instruction of a tile pass (32 bytes).
 enum TileOp : uint8_t {
-    TOP_PHASE = 1,    // load the registers with the mapping in pos[0..3] / tperm
+    TOP_PHASE = 1,    // load the registers with the mapping in pos[0..kRegQubits) / tperm
     TOP_END = 2,      // write the registers back, barrier
     TOP_G1 = 3,       // 1-qubit dense gate on register slot pos[0]
     TOP_G2 = 4,       // 2-qubit dense gate on register slots (pos[0], pos[1])
@@ -97,10 +97,10 @@ struct TileProgram {
     uint64_t fp64_per_amp = 0;  // modelled FP64 instructions per amplitude
 };
 
-// Register qubits per thread in the tile kernel (16 amplitudes per thread).
-constexpr uint32_t kRegQubits = 4;
+// Register qubits per thread in the tile kernel (8 amplitudes per thread).
+constexpr uint32_t kRegQubits = 3;
 constexpr uint32_t kMaxTileQubits = 12;
-constexpr uint32_t kMinTileQubits = 4;
+constexpr uint32_t kMinTileQubits = 3;
 
 // Low qubits every tile holds by default (runs of 2^3 amplitudes, 128 bytes).
 constexpr uint32_t kDefaultFixedLow = 3;

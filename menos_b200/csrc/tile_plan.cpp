@@ -9,8 +9,8 @@
 // block-by-block sweep gives
 // (src/engines/dense/fused_block.h:60-101, src/engines/dense/dense_engine.cpp:65-112).
 //
-// Inside a pass each thread holds 16 amplitudes in registers (4 "register
-// qubits"); a PHASE instruction picks which 4 tile qubits those are, and the
+// Inside a pass each thread holds 8 amplitudes in registers (3 "register
+// qubits"); a PHASE instruction picks which 3 tile qubits those are, and the
 // blocks of the phase act on registers only.  Diagonal blocks need no pairing
 // and run in any phase.  Blocks wider than 2 dense qubits run from shared
 // memory (TOP_SMEM).
@@ -22,6 +22,10 @@
 
 namespace mb2 {
 namespace {
+
+// A pass's instructions are staged in 32 KiB of shared memory (1024
+// records); a block costs at most three (phase, gate, end).
+constexpr size_t kMaxBlocksPerPass = 300;
 
 
 uint32_t local_pos(uint64_t smask, uint32_t q) {
@@ -67,7 +71,7 @@ std::vector<PassSel> select_passes(const std::vector<Block>& blocks, uint32_t n,
         uint64_t smask = 0;
         for (uint32_t q = 0; q < fixed; ++q) smask |= uint64_t{1} << q;
         PassSel sel;
-        while (i < blocks.size()) {
+        while (i < blocks.size() && sel.gates.size() < kMaxBlocksPerPass) {
             const uint64_t grown = smask | blocks[i].mask();
             if (static_cast<uint32_t>(std::popcount(grown)) > mt) break;
             smask = grown;
@@ -131,7 +135,8 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
         pass.gates = static_cast<uint32_t>(sel.gates.size());
 
         bool open = false;
-        uint32_t reg[kRegQubits] = {0, 1, 2, 3};
+        uint32_t reg[kRegQubits];
+        for (uint32_t r = 0; r < kRegQubits; ++r) reg[r] = r;
         auto in_reg = [&](uint32_t p) -> int {
             for (uint32_t s = 0; s < kRegQubits; ++s)
                 if (reg[s] == p) return static_cast<int>(s);

@@ -118,6 +118,18 @@ def test_tiled_program_bitwise(ctx, oracle, tile):
             assert bits_equal(st.copy_out(), expect), (n, fuse, tile)
 
 
+def test_long_program_splits_passes(ctx, oracle):
+    # More blocks than one pass may hold on a state that fits a single tile.
+    rng = np.random.default_rng(8)
+    n = 10
+    c = random_circuit(n, 800, rng, unitaries=False)
+    st = DeviceState(ctx, n)
+    st.init(c.global_phase)
+    stats = st.apply_program(c, fuse_gates=False)
+    assert stats.passes >= 3
+    assert bits_equal(st.copy_out(), oracle.run(as_oracle_circuit(c), fuse_gates=False))
+
+
 def test_per_gate_sweep_bitwise(ctx, oracle):
     rng = np.random.default_rng(77)
     for n in (3, 9, 13):
