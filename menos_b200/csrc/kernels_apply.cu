@@ -224,9 +224,11 @@ struct DI {
     __device__ __forceinline__ uint32_t aux() const { return static_cast<uint32_t>(w3 >> 32); }
 };
 
+// Reads one instruction from the pass program staged in shared memory
+// (a plain load: the program is not in the global address space).
 __device__ __forceinline__ DI load_instr(const TileInstr* p) {
     const ulonglong2* s = reinterpret_cast<const ulonglong2*>(p);
-    const ulonglong2 a = __ldg(s), b = __ldg(s + 1);
+    const ulonglong2 a = s[0], b = s[1];
     return DI{a.x, a.y, b.x, b.y};
 }
 
