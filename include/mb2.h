@@ -163,6 +163,24 @@ int mb2_last_sweep_stats(mb2_state* state, mb2_sweep_stats* out);
  * Synchronous. */
 int mb2_expectation(mb2_state* state, const uint64_t* x_masks, const uint64_t* z_masks,
                     uint32_t num_terms, double* out);
+/* The same reduction for callers that cannot allocate device memory: a
+ * serving process whose own allocator has reserved the GPU's memory, or code
+ * where a driver allocation must not happen.  It allocates nothing (no
+ * cudaMalloc, cudaFree or allocating library call): its scratch -- masks,
+ * partial sums, results -- is a file-scope __device__ array of 526,336
+ * bytes that every GPU loading this library holds until exit.  The caller
+ * passes the state (dev_amps: 2^num_qubits complex128 in device memory), the
+ * host masks, the host output (2 doubles per term) and the stream to run on.
+ * num_terms above MB2_NOALLOC_MAX_TERMS returns MB2_ERR_RESOURCE and does
+ * nothing.  The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress, with that device current); make it before any
+ * stream capture.  Calls share the one array: calls that overlap on the GPU
+ * (on different streams) race.  Synchronous.  No counterpart in the
+ * reference, which allocates its partial sums per term
+ * (src/kernels/cuda/dense_kernels.cu:378-399). */
+#define MB2_NOALLOC_MAX_TERMS 64
+int mb2_expectation_noalloc(const void* dev_amps, uint32_t num_qubits, const uint64_t* x_masks,
+                            const uint64_t* z_masks, uint32_t num_terms, double* out, void* stream);
 /* sum |a|^2, accumulated in FP64.  Synchronous. */
 int mb2_norm(mb2_state* state, double* out);
 /* Counts by the reference's sort-then-walk sampler (src/engines/dense/sample.cpp:24-75):

@@ -61,6 +61,7 @@ SIGNATURES = {
                                      C.POINTER(SweepEstimate)]),
     "mb2_last_sweep_stats": (C.c_int, [_VP, C.POINTER(SweepStats)]),
     "mb2_expectation": (C.c_int, [_VP, _VP, _VP, C.c_uint32, _VP]),
+    "mb2_expectation_noalloc": (C.c_int, [_VP, C.c_uint32, _VP, _VP, C.c_uint32, _VP, _VP]),
     "mb2_norm": (C.c_int, [_VP, C.POINTER(C.c_double)]),
     "mb2_sample": (C.c_int, [_VP, C.c_uint64, C.c_uint64, _VP, C.c_uint32, _VP, _VP, C.POINTER(C.c_uint64)]),
     "mb2_copy_out": (C.c_int, [_VP, _VP, C.c_uint64]),

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "mb2_internal.h"
 
@@ -131,3 +132,87 @@ int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, cons
 }
 
 }  // namespace mb2
+
+// ---------------------------------------------------------------------------
+// The expectation reduction for callers that cannot allocate device memory.
+//
+// Some callers of this library must not call cudaMalloc: a serving process
+// whose own pool allocator has reserved the GPU's memory up front (a
+// cudaMalloc from here would fail or fragment that pool), or code running
+// where allocation is not allowed at all (a latency-critical loop that must
+// not stall on the driver's allocator).  mb2_expectation_noalloc gives them
+// the Pauli-expectation reduction with every byte of scratch it needs --
+// the Pauli masks, the per-block partial sums and the finished terms -- in
+// the file-scope array below, a fixed 526,336 bytes that every GPU which
+// loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+namespace mb2 {
+namespace {
+
+constexpr uint32_t kNoAllocTerms = MB2_NOALLOC_MAX_TERMS;
+constexpr size_t kNoAllocMasks = kNoAllocTerms * sizeof(uint64_t);                 // x, then z
+constexpr size_t kNoAllocPartials = size_t{kNoAllocTerms} * kExpBlocks * 2 * sizeof(double);
+constexpr size_t kNoAllocOut = kNoAllocTerms * 2 * sizeof(double);
+constexpr size_t kNoAllocBytes = 2 * kNoAllocMasks + kNoAllocPartials + kNoAllocOut;
+static_assert(kNoAllocBytes == 526336, "the documented size");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+
+// The device address of g_noalloc_scratch on the current device.  In host
+// code the symbol names a host-side stand-in, not device memory, so the
+// address is looked up once per device (with that device current) and kept.
+int noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MB2_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
+            cudaGetLastError();
+            return MB2_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return MB2_OK;
+}
+
+}  // namespace
+
+}  // namespace mb2
+
+extern "C" int mb2_expectation_noalloc(const void* dev_amps, uint32_t num_qubits, const uint64_t* x_masks,
+                                       const uint64_t* z_masks, uint32_t num_terms, double* out, void* stream) {
+    using namespace mb2;
+    if (num_terms == 0) return MB2_OK;
+    if (num_terms > kNoAllocTerms) return MB2_ERR_RESOURCE;
+    if (dev_amps == nullptr || x_masks == nullptr || z_masks == nullptr || out == nullptr || num_qubits < 1 ||
+        num_qubits > 40)
+        return MB2_ERR_INVALID;
+    const uint64_t lim = (uint64_t{1} << num_qubits) - 1;
+    for (uint32_t t = 0; t < num_terms; ++t)
+        if ((x_masks[t] | z_masks[t]) & ~lim) return MB2_ERR_INVALID;
+    unsigned char* base = nullptr;
+    if (int rc = noalloc_scratch(&base); rc != MB2_OK) return rc;
+    auto* dx = reinterpret_cast<uint64_t*>(base);
+    auto* dz = reinterpret_cast<uint64_t*>(base + kNoAllocMasks);
+    auto* partials = reinterpret_cast<double*>(base + 2 * kNoAllocMasks);
+    auto* dout = reinterpret_cast<double*>(base + 2 * kNoAllocMasks + kNoAllocPartials);
+    const auto s = static_cast<cudaStream_t>(stream);
+    const size_t mb = size_t{num_terms} * sizeof(uint64_t);
+    if (cudaMemcpyAsync(dx, x_masks, mb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dz, z_masks, mb, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return MB2_ERR_CUDA;
+    // Every partial and every output slot is written before it is read, so
+    // nothing left in the array by an earlier call needs clearing.
+    if (launch_expectation(dev_amps, num_qubits, dx, dz, num_terms, partials, dout, stream) != MB2_OK)
+        return MB2_ERR_CUDA;
+    if (cudaMemcpyAsync(out, dout, size_t{num_terms} * 2 * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return MB2_ERR_CUDA;
+    return cudaStreamSynchronize(s) == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+}
+
