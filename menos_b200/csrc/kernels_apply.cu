@@ -234,11 +234,19 @@ __device__ __forceinline__ DI load_instr(const TileInstr* p) {
 
 constexpr int kR = static_cast<int>(kRegQubits);  // register qubits per thread
 constexpr int kNA = 1 << kR;                         // amplitudes per thread
+static_assert(kR == 4, "the register-slot dispatch below is written for 4 register qubits");
+
+// 16-bit masks of the register indices j whose bit s is set.
+__device__ __forceinline__ uint32_t slot_mask(uint32_t s) {
+    return s == 0 ? 0xAAAAu : s == 1 ? 0xCCCCu : s == 2 ? 0xF0F0u : 0xFF00u;
+}
 
 template <int P, int KIND>
-__device__ __forceinline__ void g1(double2 (&a)[kNA], const double* __restrict__ md, uint32_t aux) {
-    const double m00r = md[0], m00i = md[1], m01r = md[2], m01i = md[3];
-    const double m10r = md[4], m10i = md[5], m11r = md[6], m11i = md[7];
+__device__ __forceinline__ void g1(double2 (&a)[kNA], const double* md, uint32_t aux) {
+    const double2 e0 = reinterpret_cast<const double2*>(md)[0], e1 = reinterpret_cast<const double2*>(md)[1];
+    const double2 e2 = reinterpret_cast<const double2*>(md)[2], e3 = reinterpret_cast<const double2*>(md)[3];
+    const double m00r = e0.x, m00i = e0.y, m01r = e1.x, m01i = e1.y;
+    const double m10r = e2.x, m10i = e2.y, m11r = e3.x, m11i = e3.y;
 #pragma unroll
     for (int j = 0; j < kNA; ++j) {
         if (j & (1 << P)) continue;
@@ -267,7 +275,7 @@ __device__ __forceinline__ void g1(double2 (&a)[kNA], const double* __restrict__
 }
 
 template <int P0, int P1, int KIND>
-__device__ __forceinline__ void g2(double2 (&a)[kNA], const double* __restrict__ md, uint32_t aux) {
+__device__ __forceinline__ void g2(double2 (&a)[kNA], const double* md, uint32_t aux) {
     if constexpr (P0 == P1) {
         return;
     } else {
@@ -302,24 +310,54 @@ __device__ __forceinline__ void g2(double2 (&a)[kNA], const double* __restrict__
 
 template <int KIND>
 __device__ __forceinline__ void dispatch_g1(int p, double2 (&a)[kNA], const double* md, uint32_t aux) {
-    static_assert(kR == 3, "dispatch written for 3 register qubits");
     switch (p) {
         case 0: g1<0, KIND>(a, md, aux); break;
         case 1: g1<1, KIND>(a, md, aux); break;
-        default: g1<2, KIND>(a, md, aux); break;
+        case 2: g1<2, KIND>(a, md, aux); break;
+        default: g1<3, KIND>(a, md, aux); break;
+    }
+}
+
+template <int P0, int KIND>
+__device__ __forceinline__ void dispatch_g2b(int p1, double2 (&a)[kNA], const double* md, uint32_t aux) {
+    switch (p1) {
+        case 0: g2<P0, 0, KIND>(a, md, aux); break;
+        case 1: g2<P0, 1, KIND>(a, md, aux); break;
+        case 2: g2<P0, 2, KIND>(a, md, aux); break;
+        default: g2<P0, 3, KIND>(a, md, aux); break;
     }
 }
 
 template <int KIND>
 __device__ __forceinline__ void dispatch_g2(int p0, int p1, double2 (&a)[kNA], const double* md, uint32_t aux) {
-    switch (p0 * 3 + p1) {
-        case 1: g2<0, 1, KIND>(a, md, aux); break;
-        case 2: g2<0, 2, KIND>(a, md, aux); break;
-        case 3: g2<1, 0, KIND>(a, md, aux); break;
-        case 5: g2<1, 2, KIND>(a, md, aux); break;
-        case 6: g2<2, 0, KIND>(a, md, aux); break;
-        case 7: g2<2, 1, KIND>(a, md, aux); break;
-        default: break;
+    switch (p0) {
+        case 0: dispatch_g2b<0, KIND>(p1, a, md, aux); break;
+        case 1: dispatch_g2b<1, KIND>(p1, a, md, aux); break;
+        case 2: dispatch_g2b<2, KIND>(p1, a, md, aux); break;
+        default: dispatch_g2b<3, KIND>(p1, a, md, aux); break;
+    }
+}
+
+// A diagonal block of k <= 2 qubits in registers.  Operand b's bit over the
+// thread's 16 amplitudes is a 16-bit mask: a register slot's pattern, or all
+// ones / all zeros for a thread bit.  Entry e of amplitude j follows from the
+// masks; its class (aux, 2 bits per entry) picks copy, negate or multiply.
+__device__ __forceinline__ void diag_small(double2 (&a)[kNA], const double* md, uint32_t k, uint32_t aux, uint32_t m0,
+                                           uint32_t m1) {
+    const double2 d0 = reinterpret_cast<const double2*>(md)[0];
+    const double2 d1 = reinterpret_cast<const double2*>(md)[1];
+    const double2 d2 = k > 1 ? reinterpret_cast<const double2*>(md)[2] : d0;
+    const double2 d3 = k > 1 ? reinterpret_cast<const double2*>(md)[3] : d1;
+#pragma unroll
+    for (int j = 0; j < kNA; ++j) {
+        const uint32_t e = ((m0 >> j) & 1u) | (((m1 >> j) & 1u) << 1);
+        const uint32_t cls = (aux >> (2 * e)) & 3u;
+        if (cls == 1u) {
+            a[j] = cneg(a[j]);
+        } else if (cls == 2u) {
+            const double2 d = (e & 2u) ? ((e & 1u) ? d3 : d2) : ((e & 1u) ? d1 : d0);
+            a[j] = cmul(d.x, d.y, a[j]);
+        }
     }
 }
 
@@ -331,13 +369,6 @@ __device__ __forceinline__ uint32_t reg_local(uint32_t tb, int j, const uint32_t
     return l;
 }
 
-__device__ __forceinline__ uint64_t reg_offset(int j, const uint64_t (&hib)[kR]) {
-    uint64_t o = 0;
-#pragma unroll
-    for (int b = 0; b < kR; ++b) o |= ((j >> b) & 1) ? hib[b] : 0ull;
-    return o;
-}
-
 // cp.async of one 16-byte amplitude, global -> shared (L2 only, no L1).
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
@@ -347,27 +378,28 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// One pass of the tiled sweep.  blockDim.x == 2^(m-3) <= 512; each thread
-// owns 8 amplitudes.  Persistent CTAs take tiles round-robin; the next
+// One pass of the tiled sweep.  blockDim.x == 2^(m-4) <= 256; each thread
+// owns 16 amplitudes.  Persistent CTAs take tiles round-robin; the next
 // tile is gathered into the second shared-memory buffer with cp.async while
 // the current one is computed, so HBM traffic overlaps the FP64 work.  The
-// pass's instructions are staged in shared memory once per CTA.
-__global__ void __launch_bounds__(512, 1)
+// pass's instructions and small-matrix data are staged in shared memory once
+// per CTA.
+__global__ void __launch_bounds__(256, 1)
     k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m, uint64_t smask, const TileInstr* __restrict__ prog,
-                uint32_t nprog, const double* __restrict__ data, uint64_t ntiles) {
+                uint32_t nprog, const double* __restrict__ sdata, uint32_t nsdata, const double* __restrict__ gdata,
+                uint64_t ntiles) {
     extern __shared__ double2 smem_tiles[];
     const uint32_t tid = threadIdx.x;
     const uint32_t tbits = m - kRegQubits;
     const uint32_t tile_amps = 1u << m;
     TileInstr* sprog = reinterpret_cast<TileInstr*>(smem_tiles + 2 * tile_amps);
+    double* sd = reinterpret_cast<double*>(sprog + nprog);
     for (uint32_t i = tid; i < nprog * 2; i += blockDim.x)
         reinterpret_cast<ulonglong2*>(sprog)[i] = __ldg(reinterpret_cast<const ulonglong2*>(prog) + i);
+    for (uint32_t i = tid; i < nsdata; i += blockDim.x) sd[i] = __ldg(sdata + i);
     // Canonical (load/store) mapping: thread bits = tile bits 0..tbits-1,
     // register bits = tile bits tbits..m-1.
-    uint64_t off_lo = 0;
-    uint64_t hib[kR];
-#pragma unroll
-    for (int b = 0; b < kR; ++b) hib[b] = 0;
+    uint64_t off_lo = 0, hib0 = 0, hib1 = 0, hib2 = 0, hib3 = 0;
     {
         uint32_t b = 0;
         for (uint32_t p = 0; p < n; ++p) {
@@ -375,20 +407,25 @@ __global__ void __launch_bounds__(512, 1)
             if (b < tbits) {
                 off_lo |= static_cast<uint64_t>((tid >> b) & 1u) << p;
             } else {
-#pragma unroll
-                for (int r = 0; r < kR; ++r)
-                    if (static_cast<uint32_t>(r) == b - tbits) hib[r] = uint64_t{1} << p;
+                const uint64_t v = uint64_t{1} << p;
+                const uint32_t r = b - tbits;
+                if (r == 0) hib0 = v;
+                else if (r == 1) hib1 = v;
+                else if (r == 2) hib2 = v;
+                else hib3 = v;
             }
             ++b;
         }
     }
     const uint64_t nmask = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~smask;
-
+    auto reg_off = [&](int j) -> uint64_t {
+        return ((j & 1) ? hib0 : 0) | ((j & 2) ? hib1 : 0) | ((j & 4) ? hib2 : 0) | ((j & 8) ? hib3 : 0);
+    };
     auto prefetch = [&](uint64_t t, double2* buf) {
         const uint64_t base = pdep64(t, nmask) | off_lo;
 #pragma unroll
         for (int j = 0; j < kNA; ++j)
-            cp_async16(buf + swz(tid | (static_cast<uint32_t>(j) << tbits)), st + (base | reg_offset(j, hib)));
+            cp_async16(buf + swz(tid | (static_cast<uint32_t>(j) << tbits)), st + (base | reg_off(j)));
         cp_async_commit();
     };
 
@@ -422,7 +459,7 @@ __global__ void __launch_bounds__(512, 1)
                     const DI G = load_instr(sprog + pc);
                     ++pc;
                     if (G.op() == TOP_END) break;
-                    const double* md = data + G.data();
+                    const double* md = sd + G.data();
                     if (G.op() == TOP_G1) {
                         switch (G.kind()) {
                             case TK_GEN: dispatch_g1<TK_GEN>(G.pos(0), a, md, G.aux()); break;
@@ -433,26 +470,35 @@ __global__ void __launch_bounds__(512, 1)
                     } else if (G.op() == TOP_G2) {
                         if (G.kind() == TK_MONO) dispatch_g2<TK_MONO>(G.pos(0), G.pos(1), a, md, G.aux());
                         else dispatch_g2<TK_GEN>(G.pos(0), G.pos(1), a, md, G.aux());
-                    } else {  // TOP_DIAG
-                        // Entry index bits: from the thread part once, from
-                        // the register part per amplitude.
-                        const uint32_t k = G.k();
-                        uint32_t et = 0;
-                        uint32_t er[kR];
+                    } else if (G.kind() == TK_DSMALL) {
+                        // Operand masks over the 16 register slots.
+                        uint32_t msk[2] = {0u, 0u};
 #pragma unroll
-                        for (int r = 0; r < kR; ++r) er[r] = 0;
+                        for (int b = 0; b < 2; ++b) {
+                            if (static_cast<uint32_t>(b) >= G.k()) break;
+                            const uint32_t bit = 1u << G.pos(b);
+                            uint32_t mk = ((tb & bit) != 0u) ? 0xFFFFu : 0u;
+#pragma unroll
+                            for (int r = 0; r < kR; ++r)
+                                if (bit == rb[r]) mk = slot_mask(static_cast<uint32_t>(r));
+                            msk[b] = mk;
+                        }
+                        diag_small(a, md, G.k(), G.aux(), msk[0], msk[1]);
+                    } else {  // TOP_DIAG, any k: entry index per amplitude
+                        const uint32_t k = G.k();
+                        uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
                         for (uint32_t b = 0; b < k; ++b) {
                             const uint32_t bit = 1u << G.pos(b);
                             et |= ((tb & bit) ? 1u : 0u) << b;
-#pragma unroll
-                            for (int r = 0; r < kR; ++r)
-                                if (bit == rb[r]) er[r] = 1u << b;
+                            if (bit == rb[0]) e0 = 1u << b;
+                            if (bit == rb[1]) e1 = 1u << b;
+                            if (bit == rb[2]) e2 = 1u << b;
+                            if (bit == rb[3]) e3 = 1u << b;
                         }
 #pragma unroll
                         for (int j = 0; j < kNA; ++j) {
-                            uint32_t e = et;
-#pragma unroll
-                            for (int r = 0; r < kR; ++r) e |= ((j >> r) & 1) ? er[r] : 0u;
+                            const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) | ((j & 4) ? e2 : 0u) |
+                                               ((j & 8) ? e3 : 0u);
                             a[j] = scale_entry(md[2 * e], md[2 * e + 1], a[j]);
                         }
                     }
@@ -465,7 +511,7 @@ __global__ void __launch_bounds__(512, 1)
                 const uint32_t k = I.k(), dim = 1u << k;
                 uint32_t opm = 0;
                 for (uint32_t b = 0; b < k; ++b) opm |= 1u << I.pos(b);
-                const double* md = data + I.data();
+                const double* md = gdata + I.data();
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) {
                     const uint32_t l = tid | (static_cast<uint32_t>(j) << tbits);
@@ -477,7 +523,8 @@ __global__ void __launch_bounds__(512, 1)
                         uint32_t li = gbase;
                         for (uint32_t b = 0; b < k; ++b)
                             if ((in >> b) & 1u) li |= 1u << I.pos(b);
-                        const double2 p = cmul(md[2 * (out * dim + in)], md[2 * (out * dim + in) + 1], tile[swz(li)]);
+                        const double2 p = cmul(__ldg(md + 2 * (out * dim + in)), __ldg(md + 2 * (out * dim + in) + 1),
+                                               tile[swz(li)]);
                         acc = (in == 0) ? p : cadd(acc, p);
                     }
                     a[j] = acc;
@@ -493,7 +540,7 @@ __global__ void __launch_bounds__(512, 1)
         const uint64_t base = pdep64(t, nmask) | off_lo;
 #pragma unroll
         for (int j = 0; j < kNA; ++j)
-            st[base | reg_offset(j, hib)] = canon(tile[swz(tid | (static_cast<uint32_t>(j) << tbits))]);
+            st[base | reg_off(j)] = canon(tile[swz(tid | (static_cast<uint32_t>(j) << tbits))]);
         __syncthreads();  // the buffer is the target of the prefetch two tiles on
     }
 }
@@ -567,26 +614,25 @@ int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, 
     return status_of(cudaGetLastError());
 }
 
-int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs, const double* dev_data,
-                     int sm_count, void* stream) {
-    constexpr size_t kMaxProgBytes = 32 * 1024;
+int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
+                     const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream) {
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_tile_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(2 * (size_t{1} << kMaxTileQubits) * sizeof(double2) + kMaxProgBytes));
+                             static_cast<int>(2 * (size_t{1} << kMaxTileQubits) * sizeof(double2) + kMaxStagedBytes));
         attr_set = true;
     }
     if (pass.m > kMaxTileQubits || pass.m < kMinTileQubits) return MB2_ERR_INVALID;
-    const size_t prog_bytes = size_t{pass.prog_count} * sizeof(TileInstr);
-    if (prog_bytes > kMaxProgBytes) return MB2_ERR_INVALID;
+    const size_t staged = size_t{pass.prog_count} * sizeof(TileInstr) + size_t{pass.sdata_count} * sizeof(double);
+    if (staged > kMaxStagedBytes) return MB2_ERR_INVALID;
     const uint32_t threads = 1u << (pass.m - kRegQubits);
-    const size_t smem = 2 * (size_t{1} << pass.m) * sizeof(double2) + prog_bytes;
+    const size_t smem = 2 * (size_t{1} << pass.m) * sizeof(double2) + staged;
     const uint64_t ntiles = (uint64_t{1} << n) >> pass.m;
     const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m <= 11 ? 2u : 1u);
     const int grid = static_cast<int>(ntiles < cap ? ntiles : cap);
     k_tile_pass<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(
-        static_cast<double2*>(amps), n, pass.m, pass.smask, dev_instrs + pass.prog_begin, pass.prog_count, dev_data,
-        ntiles);
+        static_cast<double2*>(amps), n, pass.m, pass.smask, dev_instrs + pass.prog_begin, pass.prog_count,
+        dev_sdata + pass.sdata_begin, pass.sdata_count, dev_gdata, ntiles);
     return status_of(cudaGetLastError());
 }
 

@@ -196,34 +196,136 @@ __global__ void __launch_bounds__(kThreads) k_chunk_maps(const double2* __restri
     }
 }
 
-// Step D: the exact chain at every chunk start, one warp walking the chunks
-// in order.  Valid maps advance the chain in O(1) when the exact start lies
-// in the map's binade and the chunk does not leave it; every other chunk is
-// walked with the reference's FP64 adds (its elements staged in shared
-// memory by the warp).  cstart[j] = chain value before chunk j; cstart[nchunks]
-// = the final sum.  seq[j] = 1 when chunk j was walked.
-__global__ void __launch_bounds__(32) k_chain(const double2* __restrict__ st, uint64_t n_amps, uint32_t chunk,
-                                              uint64_t nchunks, const ChunkMap* __restrict__ maps,
-                                              double* __restrict__ cstart, unsigned char* __restrict__ seq) {
+// Step D: the exact chain at every chunk start.
+//
+// D1 (one CTA): chunks whose maps are valid for the same binade form
+// segments; a segmented scan gives each chunk the composition of the
+// segment's chunks before it (`excl`) and each segment head the whole
+// segment's map and length.
+// D2 (one warp): walks the segments in order with the exact running value
+// c.  A segment is crossed in O(1) when c lies in its binade and the
+// segment does not leave it; otherwise its chunks are taken one at a time
+// (O(1) per chunk under the same checks, or the reference's FP64 adds over
+// the chunk's elements).
+// D3 (all chunks): the start of every chunk inside a crossed segment,
+// exactly, from the segment's start value and `excl`.
+// cstart[j] = the chain before chunk j; cstart[nchunks] = the final sum;
+// seq[j] = 1 when chunk j was walked element by element.
+struct SMap {
+    long long inc0, inc1;
+    int par0, par1;
+    unsigned count;
+    unsigned pad;
+};
+
+__device__ __forceinline__ SMap sm_identity() { return SMap{0, 0, 0, 1, 0, 0}; }
+
+__device__ __forceinline__ SMap sm_compose(const SMap& a, const SMap& b) {
+    SMap r;
+    r.inc0 = a.inc0 + (a.par0 ? b.inc1 : b.inc0);
+    r.par0 = a.par0 ? b.par1 : b.par0;
+    r.inc1 = a.inc1 + (a.par1 ? b.inc1 : b.inc0);
+    r.par1 = a.par1 ? b.par1 : b.par0;
+    r.count = a.count + b.count;
+    r.pad = 0;
+    return r;
+}
+
+__device__ __forceinline__ bool seg_head(const ChunkMap* maps, uint64_t j) {
+    if (j == 0 || !maps[j].valid || !maps[j - 1].valid) return true;
+    return maps[j].e != maps[j - 1].e;
+}
+
+__device__ __forceinline__ SMap sm_of(const ChunkMap& m) {
+    return SMap{m.inc0, m.inc1, m.par0, m.par1, 1, 0};
+}
+
+__global__ void __launch_bounds__(1024) k_seg_scan(const ChunkMap* __restrict__ maps, uint64_t nchunks,
+                                                   SMap* __restrict__ excl, SMap* __restrict__ seg_total) {
+    __shared__ SMap agg[1024];
+    __shared__ unsigned char agg_head[1024];
+    const uint64_t per = (nchunks + 1023) / 1024;
+    const uint64_t b = threadIdx.x * per, e = b + per < nchunks ? b + per : nchunks;
+    // Pass 1: this range's segmented aggregate.
+    SMap v = sm_identity();
+    bool any_head = false;
+    for (uint64_t j = b; j < e; ++j) {
+        if (seg_head(maps, j)) {
+            v = sm_of(maps[j]);
+            any_head = true;
+        } else {
+            v = sm_compose(v, sm_of(maps[j]));
+        }
+    }
+    agg[threadIdx.x] = v;
+    agg_head[threadIdx.x] = any_head ? 1 : 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {  // exclusive segmented scan of the 1024 aggregates
+        SMap run = sm_identity();
+        for (int t = 0; t < 1024; ++t) {
+            const SMap a = agg[t];
+            const bool h = agg_head[t] != 0;
+            agg[t] = run;
+            run = h ? a : sm_compose(run, a);
+        }
+    }
+    __syncthreads();
+    // Pass 2: per chunk, within-segment exclusive prefix; segment totals at heads.
+    SMap run = agg[threadIdx.x];
+    for (uint64_t j = b; j < e; ++j) {
+        if (seg_head(maps, j)) run = sm_identity();
+        excl[j] = run;
+        run = sm_compose(run, sm_of(maps[j]));
+        const bool last = (j + 1 == nchunks) || seg_head(maps, j + 1);
+        if (last) seg_total[j + 1 - run.count] = run;
+    }
+}
+
+__device__ __forceinline__ bool advance_exact(double& c, int e, long long inc0, long long inc1) {
+    if (!(c > 0.0) || binade_of(c) != e) return false;
+    const double u = ldexp(1.0, e - 52);
+    const long long M = static_cast<long long>(c / u);  // exact: c is on the grid
+    const long long M2 = M + ((M & 1) ? inc1 : inc0);
+    if (M2 >= (1LL << 53)) return false;
+    c = static_cast<double>(M2) * u;  // exact: M2 < 2^53
+    return true;
+}
+
+__global__ void __launch_bounds__(32) k_seg_chain(const double2* __restrict__ st, uint64_t n_amps, uint32_t chunk,
+                                                  uint64_t nchunks, const ChunkMap* __restrict__ maps,
+                                                  const SMap* __restrict__ seg_total, double* __restrict__ cstart,
+                                                  unsigned char* __restrict__ seq, unsigned char* __restrict__ direct,
+                                                  double* __restrict__ seg_c) {
     __shared__ double buf[kSampleChunk];
     const int lane = threadIdx.x;
     double c = 0.0;
-    for (uint64_t j = 0; j < nchunks; ++j) {
+    uint64_t j = 0;
+    bool in_failed_segment = false;
+    while (j < nchunks) {
         const ChunkMap m = maps[j];
-        if (lane == 0) cstart[j] = c;
-        bool done = false;
-        if (m.valid && c > 0.0 && binade_of(c) == m.e) {
-            const double u = ldexp(1.0, m.e - 52);
-            const long long M = static_cast<long long>(c / u);  // exact: c is on the grid
-            const int par = static_cast<int>(M & 1);
-            const long long M2 = M + (par ? m.inc1 : m.inc0);
-            if (M2 < (1LL << 53)) {
-                c = static_cast<double>(M2) * u;  // exact: M2 < 2^53
-                done = true;
+        const bool head = seg_head(maps, j);
+        if (head) in_failed_segment = false;
+        if (head && m.valid) {
+            const SMap t = seg_total[j];
+            double c2 = c;
+            if (advance_exact(c2, m.e, t.inc0, t.inc1)) {
+                if (lane == 0) seg_c[j] = c;
+                c = c2;
+                j += t.count;
+                continue;
             }
+            in_failed_segment = true;
         }
-        if (lane == 0) seq[j] = done ? 0 : 1;
-        if (!done) {
+        // This chunk on its own.
+        if (lane == 0) {
+            cstart[j] = c;
+            direct[j] = 1;
+        }
+        double c2 = c;
+        if (m.valid && advance_exact(c2, m.e, m.inc0, m.inc1)) {
+            c = c2;
+            if (lane == 0) seq[j] = 0;
+        } else {
             const uint64_t base = j * chunk;
             for (uint32_t i = lane; i < chunk; i += 32) buf[i] = (base + i < n_amps) ? prob(st[base + i]) : 0.0;
             __syncwarp();
@@ -232,9 +334,28 @@ __global__ void __launch_bounds__(32) k_chain(const double2* __restrict__ st, ui
                 for (uint32_t i = 0; i < chunk; ++i) cc = __dadd_rn(cc, buf[i]);
             c = __shfl_sync(0xffffffffu, cc, 0);
             __syncwarp();
+            if (lane == 0) seq[j] = 1;
         }
+        (void)in_failed_segment;
+        ++j;
     }
     if (lane == 0) cstart[nchunks] = c;
+}
+
+__global__ void __launch_bounds__(kThreads) k_seg_fill(uint64_t nchunks, const ChunkMap* __restrict__ maps,
+                                                       const SMap* __restrict__ excl,
+                                                       const unsigned char* __restrict__ direct,
+                                                       const double* __restrict__ seg_c, double* __restrict__ cstart,
+                                                       unsigned char* __restrict__ seq) {
+    const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= nchunks || direct[j]) return;
+    const SMap x = excl[j];
+    const uint64_t h = j - x.count;
+    const double c = seg_c[h];
+    const double u = ldexp(1.0, maps[j].e - 52);
+    const long long M = static_cast<long long>(c / u);
+    cstart[j] = static_cast<double>(M + ((M & 1) ? x.inc1 : x.inc0)) * u;
+    seq[j] = 0;
 }
 
 // Number of sorted uniforms strictly below x.
@@ -348,7 +469,8 @@ size_t sample_scratch_bytes(uint32_t n, uint64_t shots) {
     const uint64_t nchunks = na / chunk;
     auto al = [](size_t b) { return (b + 255) & ~size_t{255}; };
     (void)shots;
-    return 2 * al(nchunks * 8) + al((nchunks + 1) * 8) + al(nchunks * sizeof(ChunkMap)) + al(nchunks);
+    return 2 * al(nchunks * 8) + al((nchunks + 1) * 8) + al(nchunks * sizeof(ChunkMap)) + al(nchunks) +
+           2 * al(nchunks * sizeof(SMap)) + al(nchunks) + al(nchunks * 8);
 }
 
 int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
@@ -369,10 +491,23 @@ int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorte
     auto* maps = reinterpret_cast<ChunkMap*>(p);
     p += al(nchunks * sizeof(ChunkMap));
     auto* seq = reinterpret_cast<unsigned char*>(p);
+    p += al(nchunks);
+    auto* excl = reinterpret_cast<SMap*>(p);
+    p += al(nchunks * sizeof(SMap));
+    auto* seg_total = reinterpret_cast<SMap*>(p);
+    p += al(nchunks * sizeof(SMap));
+    auto* direct = reinterpret_cast<unsigned char*>(p);
+    p += al(nchunks);
+    auto* seg_c = reinterpret_cast<double*>(p);
     k_chunk_sums<<<static_cast<unsigned>(nchunks), kThreads, 0, s>>>(st, na, chunk, sums);
     k_scan_sums<<<1, 1024, 0, s>>>(sums, nchunks, starts);
     k_chunk_maps<<<static_cast<unsigned>(nchunks), kThreads, 0, s>>>(st, na, chunk, starts, sums, maps);
-    k_chain<<<1, 32, 0, s>>>(st, na, chunk, nchunks, maps, cst, seq);
+    cudaMemsetAsync(direct, 0, nchunks, s);
+    k_seg_scan<<<1, 1024, 0, s>>>(maps, nchunks, excl, seg_total);
+    k_seg_chain<<<1, 32, 0, s>>>(st, na, chunk, nchunks, maps, seg_total, cst, seq, direct, seg_c);
+    k_seg_fill<<<static_cast<unsigned>((nchunks + kThreads - 1) / kThreads), kThreads, 0, s>>>(nchunks, maps, excl,
+                                                                                                direct, seg_c, cst,
+                                                                                                seq);
     k_assign<<<static_cast<unsigned>(nchunks), kThreads, 0, s>>>(st, na, chunk, maps, cst, seq,
                                                                  dev_uniforms_sorted, shots, dev_basis);
     k_leftover<<<1, 256, 0, s>>>(cst, nchunks, dev_uniforms_sorted, shots, na - 1, dev_basis);

@@ -66,7 +66,8 @@ enum TileKind : uint8_t {
     TK_GEN = 0,   // every entry general
     TK_U3 = 1,    // 1q: entry (0,0) real, the others general
     TK_REAL = 2,  // 1q: every entry real
-    TK_MONO = 3   // 1 nonzero entry per row: a permutation up to per-row factors
+    TK_MONO = 3,  // 1 nonzero entry per row: a permutation up to per-row factors
+    TK_DSMALL = 4 // diagonal, k <= 2: per-entry class in aux (2 bits each: 0 = (1,0), 1 = (-1,0), 2 = general)
 };
 struct TileInstr {
     uint8_t op;
@@ -85,11 +86,20 @@ struct TilePass {
     uint64_t smask = 0;      // global qubits in the tile
     uint32_t prog_begin = 0; // first instruction
     uint32_t prog_count = 0;
+    uint32_t sdata_begin = 0;  // this pass's staged data (doubles), copied to shared memory
+    uint32_t sdata_count = 0;
     uint32_t gates = 0;      // blocks applied in this pass
 };
 
+// Shared-memory budget of one pass's staged instructions + data.
+constexpr size_t kMaxStagedBytes = 48 * 1024;
+
+// TileInstr.data: for TOP_SMEM an offset into the program's global-only data
+// block (gdata); for every other instruction an offset into its pass's
+// staged data (sdata, relative to the pass's sdata_begin).
 struct TileProgram {
     std::vector<TilePass> passes;
+    std::vector<double> gdata;
     std::vector<uint32_t> order;       // block indices in application order
     std::vector<uint32_t> order_pass;  // the pass of each entry of `order`
     std::vector<TileInstr> instrs;
@@ -97,10 +107,10 @@ struct TileProgram {
     uint64_t fp64_per_amp = 0;  // modelled FP64 instructions per amplitude
 };
 
-// Register qubits per thread in the tile kernel (8 amplitudes per thread).
-constexpr uint32_t kRegQubits = 3;
+// Register qubits per thread in the tile kernel (16 amplitudes per thread).
+constexpr uint32_t kRegQubits = 4;
 constexpr uint32_t kMaxTileQubits = 12;
-constexpr uint32_t kMinTileQubits = 3;
+constexpr uint32_t kMinTileQubits = 4;
 
 // Low qubits every tile holds by default (runs of 2^3 amplitudes, 128 bytes).
 constexpr uint32_t kDefaultFixedLow = 3;
@@ -117,7 +127,7 @@ int launch_apply_diag(void* amps, uint32_t n, const uint32_t* q, uint32_t k, con
 int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* dev_matrix,
                          void* stream);
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
-                     const double* dev_data, int sm_count, void* stream);
+                     const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream);
 // Expectation of num_terms Pauli terms: partials (num_terms * kExpBlocks * 2
 // doubles) then the fixed-order finish into out (num_terms * 2 doubles), all
 // device pointers.

@@ -9,8 +9,8 @@
 // block-by-block sweep gives
 // (src/engines/dense/fused_block.h:60-101, src/engines/dense/dense_engine.cpp:65-112).
 //
-// Inside a pass each thread holds 8 amplitudes in registers (3 "register
-// qubits"); a PHASE instruction picks which 3 tile qubits those are, and the
+// Inside a pass each thread holds 16 amplitudes in registers (4 "register
+// qubits"); a PHASE instruction picks which 4 tile qubits those are, and the
 // blocks of the phase act on registers only.  Diagonal blocks need no pairing
 // and run in any phase.  Blocks wider than 2 dense qubits run from shared
 // memory (TOP_SMEM).
@@ -23,9 +23,16 @@
 namespace mb2 {
 namespace {
 
-// A pass's instructions are staged in 32 KiB of shared memory (1024
-// records); a block costs at most three (phase, gate, end).
+// A pass's instructions and small-matrix data are staged in shared memory
+// (kMaxStagedBytes); a block costs at most three records (phase, gate, end)
+// plus its staged entries.
 constexpr size_t kMaxBlocksPerPass = 300;
+
+size_t staged_bytes(const Block& b) {
+    const size_t dim = size_t{1} << b.k;
+    const size_t entries = b.diagonal ? dim : (b.k <= 2 ? dim * dim : 0);
+    return 3 * sizeof(TileInstr) + entries * 2 * sizeof(double);
+}
 
 
 uint32_t local_pos(uint64_t smask, uint32_t q) {
@@ -71,9 +78,12 @@ std::vector<PassSel> select_passes(const std::vector<Block>& blocks, uint32_t n,
         uint64_t smask = 0;
         for (uint32_t q = 0; q < fixed; ++q) smask |= uint64_t{1} << q;
         PassSel sel;
+        size_t staged = 0;
         while (i < blocks.size() && sel.gates.size() < kMaxBlocksPerPass) {
             const uint64_t grown = smask | blocks[i].mask();
             if (static_cast<uint32_t>(std::popcount(grown)) > mt) break;
+            if (staged + staged_bytes(blocks[i]) > kMaxStagedBytes && !sel.gates.empty()) break;
+            staged += staged_bytes(blocks[i]);
             smask = grown;
             sel.gates.push_back(static_cast<uint32_t>(i));
             ++i;
@@ -132,7 +142,11 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
         pass.m = mt;
         pass.smask = sel.smask;
         pass.prog_begin = static_cast<uint32_t>(prog.instrs.size());
+        pass.sdata_begin = static_cast<uint32_t>(prog.data.size());
         pass.gates = static_cast<uint32_t>(sel.gates.size());
+        auto push_staged = [&](const std::vector<Cd>& m) {
+            return push_matrix(prog.data, m) - pass.sdata_begin;
+        };
 
         bool open = false;
         uint32_t reg[kRegQubits];
@@ -193,9 +207,24 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
                 for (uint32_t t = 0; t < b.k; ++t) g.pos[t] = static_cast<uint8_t>(local_pos(sel.smask, b.q[t]));
                 std::vector<Cd> d(dim);
                 for (uint32_t i = 0; i < dim; ++i) d[i] = b.m[i * dim + i];
-                g.data = push_matrix(prog.data, d);
+                g.data = push_staged(d);
+                if (b.k <= 2) {
+                    // Entry classes: (1,0) copies, (-1,0) negates, the rest multiply.
+                    g.kind = TK_DSMALL;
+                    uint32_t gen = 0;
+                    for (uint32_t i = 0; i < dim; ++i) {
+                        uint32_t cls = 2;
+                        if (d[i].imag() == 0.0 && d[i].real() == 1.0) cls = 0;
+                        else if (d[i].imag() == 0.0 && d[i].real() == -1.0) cls = 1;
+                        if (cls == 2) ++gen;
+                        g.aux |= cls << (2 * i);
+                    }
+                    prog.fp64_per_amp += (6 * gen + dim - 1) / dim;
+                } else {
+                    g.kind = TK_GEN;
+                    prog.fp64_per_amp += 6;
+                }
                 prog.instrs.push_back(g);
-                prog.fp64_per_amp += 6;
                 continue;
             }
             if (b.k <= 2) {
@@ -246,7 +275,7 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
                     g.kind = TK_GEN;
                     prog.fp64_per_amp += 30;
                 }
-                g.data = push_matrix(prog.data, b.m);
+                g.data = push_staged(b.m);
                 prog.instrs.push_back(g);
                 continue;
             }
@@ -254,12 +283,13 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
             close_phase();
             g.op = TOP_SMEM;
             for (uint32_t t = 0; t < b.k; ++t) g.pos[t] = static_cast<uint8_t>(local_pos(sel.smask, b.q[t]));
-            g.data = push_matrix(prog.data, b.m);
+            g.data = push_matrix(prog.gdata, b.m);
             prog.instrs.push_back(g);
             prog.fp64_per_amp += 8ull * dim - 2;
         }
         close_phase();
         pass.prog_count = static_cast<uint32_t>(prog.instrs.size()) - pass.prog_begin;
+        pass.sdata_count = static_cast<uint32_t>(prog.data.size()) - pass.sdata_begin;
         prog.passes.push_back(pass);
     }
     return prog;
