@@ -236,6 +236,9 @@ constexpr int kR = static_cast<int>(kRegQubits);  // register qubits per thread
 constexpr int kNA = 1 << kR;                         // amplitudes per thread
 static_assert(kR == 4, "the register-slot dispatch below is written for 4 register qubits");
 
+// Index of the lowest set bit of a (compile-time) register index j > 0.
+__host__ __device__ constexpr int lowbit_index(int j) { return (j & 1) ? 0 : (j & 2) ? 1 : (j & 4) ? 2 : 3; }
+
 // 16-bit masks of the register indices j whose bit s is set.
 __device__ __forceinline__ uint32_t slot_mask(uint32_t s) {
     return s == 0 ? 0xAAAAu : s == 1 ? 0xCCCCu : s == 2 ? 0xF0F0u : 0xFF00u;
@@ -338,26 +341,102 @@ __device__ __forceinline__ void dispatch_g2(int p0, int p1, double2 (&a)[kNA], c
     }
 }
 
-// A diagonal block of k <= 2 qubits in registers.  Operand b's bit over the
-// thread's 16 amplitudes is a 16-bit mask: a register slot's pattern, or all
-// ones / all zeros for a thread bit.  Entry e of amplitude j follows from the
-// masks; its class (aux, 2 bits per entry) picks copy, negate or multiply.
-__device__ __forceinline__ void diag_small(double2 (&a)[kNA], const double* md, uint32_t k, uint32_t aux, uint32_t m0,
-                                           uint32_t m1) {
-    const double2 d0 = reinterpret_cast<const double2*>(md)[0];
-    const double2 d1 = reinterpret_cast<const double2*>(md)[1];
-    const double2 d2 = k > 1 ? reinterpret_cast<const double2*>(md)[2] : d0;
-    const double2 d3 = k > 1 ? reinterpret_cast<const double2*>(md)[3] : d1;
+// A diagonal block of k <= 2 qubits in registers.  Each operand is either
+// a register slot (its bit over j is known at compile time in the templates
+// below) or a thread bit (one value for all 16 amplitudes).  The entry of
+// amplitude j is e = bit0 | bit1 << 1; its class (aux, 2 bits per entry)
+// picks copy, negate or multiply -- a warp-uniform choice per entry.
+struct Diag4 {
+    double2 d[4];
+    uint32_t aux;
+};
+
+__device__ __forceinline__ void diag_apply(double2& x, const Diag4& D, uint32_t e) {
+    const uint32_t cls = (D.aux >> (2 * e)) & 3u;
+    if (cls == 1u) {
+        x = cneg(x);
+    } else if (cls == 2u) {
+        // A select tree, not an indexed load: e is often a run-time value.
+        const double2 d = (e & 2u) ? ((e & 1u) ? D.d[3] : D.d[2]) : ((e & 1u) ? D.d[1] : D.d[0]);
+        x = cmul(d.x, d.y, x);
+    }
+}
+
+// Operand 0 in register slot P0, operand 1 in slot P1 (k == 2), or k == 1 (P1 < 0).
+template <int P0, int P1>
+__device__ __forceinline__ void diag_rr(double2 (&a)[kNA], const Diag4& D) {
 #pragma unroll
     for (int j = 0; j < kNA; ++j) {
-        const uint32_t e = ((m0 >> j) & 1u) | (((m1 >> j) & 1u) << 1);
-        const uint32_t cls = (aux >> (2 * e)) & 3u;
-        if (cls == 1u) {
-            a[j] = cneg(a[j]);
-        } else if (cls == 2u) {
-            const double2 d = (e & 2u) ? ((e & 1u) ? d3 : d2) : ((e & 1u) ? d1 : d0);
-            a[j] = cmul(d.x, d.y, a[j]);
+        const uint32_t e = static_cast<uint32_t>((j >> P0) & 1) | (P1 >= 0 ? static_cast<uint32_t>((j >> (P1 < 0 ? 0 : P1)) & 1) << 1 : 0u);
+        diag_apply(a[j], D, e);
+    }
+}
+
+// One operand in register slot P (its bit is `shift` of e), the other a thread bit `tv` (at bit 1 - shift).
+template <int P>
+__device__ __forceinline__ void diag_rt(double2 (&a)[kNA], const Diag4& D, uint32_t shift, uint32_t tv) {
+#pragma unroll
+    for (int j = 0; j < kNA; ++j) {
+        const uint32_t e = (static_cast<uint32_t>((j >> P) & 1) << shift) | (tv << (1u - shift));
+        diag_apply(a[j], D, e);
+    }
+}
+
+__device__ __forceinline__ void diag_small(double2 (&a)[kNA], const double* md, uint32_t k, uint32_t aux, int s0,
+                                           int s1, uint32_t t0, uint32_t t1) {
+    // s0/s1: register slot of operand 0/1, or -1 for a thread bit of value t0/t1.
+    Diag4 D;
+    D.aux = aux;
+    D.d[0] = reinterpret_cast<const double2*>(md)[0];
+    D.d[1] = reinterpret_cast<const double2*>(md)[1];
+    D.d[2] = k > 1 ? reinterpret_cast<const double2*>(md)[2] : D.d[0];
+    D.d[3] = k > 1 ? reinterpret_cast<const double2*>(md)[3] : D.d[1];
+    if (k == 1) {
+        if (s0 < 0) {
+#pragma unroll
+            for (int j = 0; j < kNA; ++j) diag_apply(a[j], D, t0);
+            return;
         }
+        switch (s0) {
+            case 0: diag_rr<0, -1>(a, D); break;
+            case 1: diag_rr<1, -1>(a, D); break;
+            case 2: diag_rr<2, -1>(a, D); break;
+            default: diag_rr<3, -1>(a, D); break;
+        }
+        return;
+    }
+    if (s0 >= 0 && s1 >= 0) {
+        switch (s0 * 4 + s1) {
+            case 1: diag_rr<0, 1>(a, D); break;
+            case 2: diag_rr<0, 2>(a, D); break;
+            case 3: diag_rr<0, 3>(a, D); break;
+            case 4: diag_rr<1, 0>(a, D); break;
+            case 6: diag_rr<1, 2>(a, D); break;
+            case 7: diag_rr<1, 3>(a, D); break;
+            case 8: diag_rr<2, 0>(a, D); break;
+            case 9: diag_rr<2, 1>(a, D); break;
+            case 11: diag_rr<2, 3>(a, D); break;
+            case 12: diag_rr<3, 0>(a, D); break;
+            case 13: diag_rr<3, 1>(a, D); break;
+            case 14: diag_rr<3, 2>(a, D); break;
+            default: break;
+        }
+        return;
+    }
+    if (s0 < 0 && s1 < 0) {
+        const uint32_t e = t0 | (t1 << 1);
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) diag_apply(a[j], D, e);
+        return;
+    }
+    const int s = s0 >= 0 ? s0 : s1;
+    const uint32_t shift = s0 >= 0 ? 0u : 1u;
+    const uint32_t tv = s0 >= 0 ? t1 : t0;
+    switch (s) {
+        case 0: diag_rt<0>(a, D, shift, tv); break;
+        case 1: diag_rt<1>(a, D, shift, tv); break;
+        case 2: diag_rt<2>(a, D, shift, tv); break;
+        default: diag_rt<3>(a, D, shift, tv); break;
     }
 }
 
@@ -453,8 +532,14 @@ __global__ void __launch_bounds__(256, 1)
                 uint32_t rb[kR];
 #pragma unroll
                 for (int b = 0; b < kR; ++b) rb[b] = 1u << I.pos(b);
+                // swz is linear over XOR, so slot j's address is swz(tb) XOR the
+                // swizzled register bits of j.
+                uint32_t adr[kNA];
+                adr[0] = swz(tb);
 #pragma unroll
-                for (int j = 0; j < kNA; ++j) a[j] = tile[swz(reg_local(tb, j, rb))];
+                for (int j = 1; j < kNA; ++j) adr[j] = adr[j & (j - 1)] ^ swz(rb[lowbit_index(j)]);
+#pragma unroll
+                for (int j = 0; j < kNA; ++j) a[j] = tile[adr[j]];
                 for (;;) {
                     const DI G = load_instr(sprog + pc);
                     ++pc;
@@ -471,19 +556,18 @@ __global__ void __launch_bounds__(256, 1)
                         if (G.kind() == TK_MONO) dispatch_g2<TK_MONO>(G.pos(0), G.pos(1), a, md, G.aux());
                         else dispatch_g2<TK_GEN>(G.pos(0), G.pos(1), a, md, G.aux());
                     } else if (G.kind() == TK_DSMALL) {
-                        // Operand masks over the 16 register slots.
-                        uint32_t msk[2] = {0u, 0u};
+                        int sl[2] = {-1, -1};
+                        uint32_t tv[2] = {0u, 0u};
 #pragma unroll
                         for (int b = 0; b < 2; ++b) {
                             if (static_cast<uint32_t>(b) >= G.k()) break;
                             const uint32_t bit = 1u << G.pos(b);
-                            uint32_t mk = ((tb & bit) != 0u) ? 0xFFFFu : 0u;
+                            tv[b] = (tb & bit) ? 1u : 0u;
 #pragma unroll
                             for (int r = 0; r < kR; ++r)
-                                if (bit == rb[r]) mk = slot_mask(static_cast<uint32_t>(r));
-                            msk[b] = mk;
+                                if (bit == rb[r]) sl[b] = r;
                         }
-                        diag_small(a, md, G.k(), G.aux(), msk[0], msk[1]);
+                        diag_small(a, md, G.k(), G.aux(), sl[0], sl[1], tv[0], tv[1]);
                     } else {  // TOP_DIAG, any k: entry index per amplitude
                         const uint32_t k = G.k();
                         uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
@@ -504,7 +588,7 @@ __global__ void __launch_bounds__(256, 1)
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < kNA; ++j) tile[swz(reg_local(tb, j, rb))] = a[j];
+                for (int j = 0; j < kNA; ++j) tile[adr[j]] = a[j];
                 __syncthreads();
             } else if (I.op() == TOP_SMEM) {
                 // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
