@@ -200,6 +200,40 @@ int mb2_copy_in(mb2_state* state, const void* host, uint64_t num_amplitudes);
 /* Waits for all work queued on the state's stream. */
 int mb2_synchronize(mb2_state* state);
 
+/* ---- batched parameter sweep ------------------------------------------- */
+/* One circuit structure under many parameter bindings, in one device job:
+ * every binding's state lives in one buffer (binding b at b * 2^n), the
+ * tiled passes run once for all bindings, and <H> = sum_t coef_t <P_t> is
+ * returned per binding (out[b], real part).  Binding b's circuit is `ops`
+ * with each parameterised gate (RX RY RZ P U CP RZZ), in op order, taking
+ * its parameters from params[b * params_per_binding ...] (the ops' own
+ * params are ignored; params_per_binding must equal the slots the ops
+ * have).  complex128 results per binding are bitwise the state a single run
+ * of that binding computes; <H> within the expectation tolerance.  2^n
+ * amplitudes per binding with 4 <= n <= 16; at most MB2_BATCH_MAX_TERMS terms.
+ * states_out (optional): every binding's final amplitudes, 2 * 2^n doubles
+ * each.  Replaces: a run_batch loop of menos::run calls
+ * (src/api/batch.cpp:10-27) for a parameter sweep; no direct counterpart. */
+#define MB2_BATCH_MAX_TERMS 64
+typedef struct mb2_batch_options {
+    int32_t precision;   /* MB2_C128 */
+    int32_t fuse_gates;  /* 1: the reference's containment fusion per binding; 0: gate by gate */
+    int32_t tile_qubits; /* 0: default */
+    int32_t reserved;
+} mb2_batch_options;
+typedef struct mb2_batch_stats {
+    uint64_t passes;
+    uint64_t blocks;
+    uint64_t parametric_blocks;
+    uint64_t h2d_bytes;
+    uint64_t fp64_ops_per_amp;
+} mb2_batch_stats;
+int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num_ops, uint32_t num_qubits,
+                    const double* params, uint32_t params_per_binding, uint32_t num_bindings,
+                    const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs,
+                    uint32_t num_terms, const mb2_batch_options* opts, double* out,
+                    double* states_out, mb2_batch_stats* stats);
+
 /* ---- calibration ------------------------------------------------------- */
 /* Measures the device's FP64 multiply/add issue rate (instructions per
  * second) and its device-to-device copy bandwidth (read+write GB/s), for the

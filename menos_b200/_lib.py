@@ -33,6 +33,16 @@ class SweepEstimate(C.Structure):
 BOUNDARY_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64)
 
 
+class BatchOptions(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("fuse_gates", C.c_int32), ("tile_qubits", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("passes", C.c_uint64), ("blocks", C.c_uint64), ("parametric_blocks", C.c_uint64),
+                ("h2d_bytes", C.c_uint64), ("fp64_ops_per_amp", C.c_uint64)]
+
+
 class SweepStats(C.Structure):
     _fields_ = [("blocks", C.c_uint64), ("passes", C.c_uint64), ("launches", C.c_uint64),
                 ("fp64_ops_per_amp", C.c_uint64)]
@@ -46,6 +56,9 @@ SIGNATURES = {
     "mb2_context_destroy": (C.c_int, [_VP]),
     "mb2_last_error": (C.c_int, [_VP, C.c_char_p, C.c_size_t]),
     "mb2_device_info": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "mb2_sweep_batch": (C.c_int, [_VP, C.POINTER(MB2Op), C.c_uint32, C.c_uint32, _VP, C.c_uint32, C.c_uint32,
+                                  _VP, _VP, _VP, C.c_uint32, C.POINTER(BatchOptions), _VP, _VP,
+                                  C.POINTER(BatchStats)]),
     "mb2_probe_rates": (C.c_int, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mb2_state_alloc": (C.c_int, [_VP, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(_VP)]),
     "mb2_state_free": (C.c_int, [_VP]),

@@ -1,0 +1,235 @@
+// Batched parameter sweep (mb2_sweep_batch): one circuit structure under many
+// parameter bindings in one device job.
+//
+// Each binding's blocks are built on the host exactly as a single run builds
+// them (gate matrices from the same libm calls, the same fusion plan and
+// fused matrices), so every binding's state is bitwise the state the
+// reference computes for that binding alone.  All bindings share one tile
+// program; blocks whose matrices differ between bindings read their entries
+// from a per-binding record selected by the tile's binding index.  The
+// expectation runs one 8-CTA cluster per binding (kernels_batch.cu).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "mb2_internal.h"
+
+namespace mb2 {
+int launch_batch_init(void* amps, uint32_t n, uint64_t bindings, double re, double im, void* stream);
+int launch_batch_expect(const void* amps, uint32_t n, uint64_t bindings, const uint64_t* dev_x,
+                        const uint64_t* dev_z, const double* dev_coefs, uint32_t num_terms, double* dev_out,
+                        void* stream);
+}  // namespace mb2
+
+namespace {
+
+// The blocks of binding b: ops with their parameters taken, in op order,
+// from params.
+std::vector<mb2::Block> binding_blocks(const mb2_op* ops, uint32_t num_ops, const double* params, bool fuse) {
+    std::vector<mb2_op> mine(ops, ops + num_ops);
+    uint32_t k = 0;
+    for (mb2_op& o : mine) {
+        if (o.opcode == MB2_MEASURE || o.opcode == MB2_UNITARY) continue;
+        const int np = mb2::gate_num_params(o.opcode);
+        for (int p = 0; p < np; ++p) o.params[p] = params[k++];
+    }
+    return mb2::build_blocks(mine.data(), num_ops, fuse);
+}
+
+uint32_t param_slots(const mb2_op* ops, uint32_t num_ops) {
+    uint32_t k = 0;
+    for (uint32_t i = 0; i < num_ops; ++i)
+        if (ops[i].opcode != MB2_MEASURE && ops[i].opcode != MB2_UNITARY) k += mb2::gate_num_params(ops[i].opcode);
+    return k;
+}
+
+struct Runner {
+    int device;
+    cudaStream_t stream = nullptr;
+    void* state = nullptr;
+    void* work = nullptr;
+    ~Runner() {
+        if (stream) cudaStreamSynchronize(stream);
+        if (state) cudaFree(state);
+        if (work) cudaFree(work);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+}  // namespace
+
+extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num_ops, uint32_t num_qubits,
+                               const double* params, uint32_t params_per_binding, uint32_t num_bindings,
+                               const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs,
+                               uint32_t num_terms, const mb2_batch_options* opts, double* out,
+                               double* states_out, mb2_batch_stats* stats) {
+    if (ctx == nullptr || out == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
+    if (num_bindings == 0) return MB2_OK;
+    if (num_qubits < mb2::kMinTileQubits || num_qubits > 16) return MB2_ERR_INVALID;
+    if (num_terms > mb2::kMaxBatchTerms || (num_terms > 0 && (!x_masks || !z_masks || !coefs))) return MB2_ERR_INVALID;
+    if (param_slots(ops, num_ops) != params_per_binding || (params_per_binding > 0 && params == nullptr))
+        return MB2_ERR_INVALID;
+    for (uint32_t i = 0; i < num_ops; ++i) {
+        if (ops[i].opcode == MB2_MEASURE) continue;
+        if (ops[i].num_qubits == 0 || ops[i].num_qubits > MB2_MAX_OP_QUBITS) return MB2_ERR_INVALID;
+        for (uint32_t j = 0; j < ops[i].num_qubits; ++j)
+            if (ops[i].qubits[j] >= num_qubits) return MB2_ERR_INVALID;
+    }
+    const uint64_t lim = (uint64_t{1} << num_qubits) - 1;
+    for (uint32_t t = 0; t < num_terms; ++t)
+        if ((x_masks[t] | z_masks[t]) & ~lim) return MB2_ERR_INVALID;
+    mb2_batch_options o{MB2_C128, 0, 0, 0};
+    if (opts != nullptr) o = *opts;
+    if (o.precision != MB2_C128) return MB2_ERR_UNSUPPORTED;
+    const bool fuse = o.fuse_gates != 0;
+
+    // ---- host: every binding's blocks (threads), the shared structure, flags.
+    std::vector<std::vector<mb2::Block>> per(num_bindings);
+    try {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const unsigned nt = std::min<unsigned>(hw, num_bindings);
+        std::vector<std::thread> pool;
+        std::vector<std::string> errors(nt);
+        for (unsigned w = 0; w < nt; ++w) {
+            pool.emplace_back([&, w]() {
+                try {
+                    for (uint32_t b = w; b < num_bindings; b += nt)
+                        per[b] = binding_blocks(ops, num_ops, params + size_t{b} * params_per_binding, fuse);
+                } catch (const std::exception& e) {
+                    errors[w] = e.what();
+                }
+            });
+        }
+        for (auto& th : pool) th.join();
+        for (const auto& e : errors)
+            if (!e.empty()) throw std::invalid_argument(e);
+    } catch (const std::exception&) {
+        return MB2_ERR_INVALID;
+    }
+    std::vector<mb2::Block> shape = per[0];
+    const size_t nb = shape.size();
+    for (uint32_t b = 1; b < num_bindings; ++b) {  // one structure for every binding
+        if (per[b].size() != nb) return MB2_ERR_INVALID;
+        for (size_t i = 0; i < nb; ++i)
+            if (per[b][i].k != shape[i].k || per[b][i].mask() != shape[i].mask()) return MB2_ERR_INVALID;
+    }
+    std::vector<uint8_t> flags(nb, 0);
+    for (size_t i = 0; i < nb; ++i) {
+        const uint32_t dim = 1u << shape[i].k;
+        bool differs = false, all_real = true, m00_real = true, all_diag = true;
+        for (uint32_t b = 0; b < num_bindings; ++b) {
+            const auto& m = per[b][i].m;
+            if (std::memcmp(m.data(), shape[i].m.data(), m.size() * sizeof(mb2::Cd)) != 0) differs = true;
+            for (const mb2::Cd& c : m) all_real = all_real && c.imag() == 0.0;
+            m00_real = m00_real && m[0].imag() == 0.0;
+            all_diag = all_diag && per[b][i].diagonal;
+        }
+        shape[i].diagonal = all_diag;
+        if (differs) {
+            flags[i] = mb2::kParamBlock | (all_real ? mb2::kParamAllReal : 0) | (m00_real ? mb2::kParamM00Real : 0);
+            if (!all_diag && shape[i].k > 2) return MB2_ERR_UNSUPPORTED;  // parametric wide dense blocks
+        }
+        (void)dim;
+    }
+    uint32_t m = o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 12;
+    for (const auto& b : shape) m = std::max(m, b.k);
+    m = std::min(std::max(m, mb2::kMinTileQubits), std::min(mb2::kMaxTileQubits, num_qubits));
+    mb2::TileProgram prog;
+    try {
+        prog = mb2::plan_tile_program(shape, num_qubits, m, mb2::kDefaultFixedLow, &flags);
+    } catch (const std::exception&) {
+        return MB2_ERR_INVALID;
+    }
+    // Per-binding records of the parametric blocks, in the kernel's layout.
+    const size_t stride = prog.param_stride;
+    std::vector<double> pdata(std::max<size_t>(1, stride * num_bindings), 0.0);
+    for (uint32_t b = 0; b < num_bindings; ++b) {
+        for (size_t i = 0; i < nb; ++i) {
+            if (!(flags[i] & mb2::kParamBlock)) continue;
+            const mb2::Block& blk = per[b][i];
+            const uint32_t dim = 1u << blk.k;
+            double* dst = pdata.data() + size_t{b} * stride + prog.param_offsets[i];
+            if (shape[i].diagonal) {
+                for (uint32_t e = 0; e < dim; ++e) {
+                    dst[2 * e] = blk.m[size_t{e} * dim + e].real();
+                    dst[2 * e + 1] = blk.m[size_t{e} * dim + e].imag();
+                }
+            } else {
+                std::memcpy(dst, blk.m.data(), size_t{dim} * dim * sizeof(mb2::Cd));
+            }
+        }
+    }
+
+    // ---- device
+    Runner r{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaStreamCreateWithFlags(&r.stream, cudaStreamNonBlocking) != cudaSuccess) return MB2_ERR_CUDA;
+    const size_t state_bytes = (size_t{num_bindings} << num_qubits) * sizeof(mb2::Cd);
+    auto al = [](size_t v) { return (v + 255) & ~size_t{255}; };
+    const size_t ib = prog.instrs.size() * sizeof(mb2::TileInstr), sb = prog.data.size() * 8,
+                 gb = prog.gdata.size() * 8, pb = pdata.size() * 8, tb = size_t{num_terms} * 8;
+    const size_t o_s = al(ib), o_g = o_s + al(sb), o_p = o_g + al(gb), o_x = o_p + al(pb), o_z = o_x + al(tb),
+                 o_c = o_z + al(tb), o_o = o_c + al(tb), total = o_o + al(size_t{num_bindings} * 8);
+    if (cudaMalloc(&r.state, state_bytes) != cudaSuccess || cudaMalloc(&r.work, total) != cudaSuccess) {
+        cudaGetLastError();
+        return MB2_ERR_RESOURCE;
+    }
+    auto* w = static_cast<unsigned char*>(r.work);
+    std::vector<unsigned char> host(o_o, 0);
+    std::memcpy(host.data(), prog.instrs.data(), ib);
+    if (sb) std::memcpy(host.data() + o_s, prog.data.data(), sb);
+    if (gb) std::memcpy(host.data() + o_g, prog.gdata.data(), gb);
+    std::memcpy(host.data() + o_p, pdata.data(), pb);
+    if (tb) {
+        std::memcpy(host.data() + o_x, x_masks, tb);
+        std::memcpy(host.data() + o_z, z_masks, tb);
+        std::memcpy(host.data() + o_c, coefs, tb);
+    }
+    if (cudaMemcpyAsync(w, host.data(), host.size(), cudaMemcpyHostToDevice, r.stream) != cudaSuccess)
+        return MB2_ERR_CUDA;
+    const mb2::Cd ph = mb2::initial_phase(0.0);
+    if (mb2::launch_batch_init(r.state, num_qubits, num_bindings, ph.real(), ph.imag(), r.stream) != MB2_OK)
+        return MB2_ERR_CUDA;
+    int sm = 148;
+    cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+    mb2::BatchLayout layout;
+    layout.bindings = num_bindings;
+    layout.pdata = reinterpret_cast<const double*>(w + o_p);
+    layout.pstride = static_cast<uint32_t>(stride);
+    for (const mb2::TilePass& pass : prog.passes) {
+        if (mb2::launch_tile_pass(r.state, num_qubits, pass, reinterpret_cast<const mb2::TileInstr*>(w),
+                                  reinterpret_cast<const double*>(w + o_s), reinterpret_cast<const double*>(w + o_g),
+                                  sm, r.stream, &layout) != MB2_OK)
+            return MB2_ERR_CUDA;
+    }
+    if (num_terms > 0) {
+        if (mb2::launch_batch_expect(r.state, num_qubits, num_bindings, reinterpret_cast<const uint64_t*>(w + o_x),
+                                     reinterpret_cast<const uint64_t*>(w + o_z), reinterpret_cast<const double*>(w + o_c),
+                                     num_terms, reinterpret_cast<double*>(w + o_o), r.stream) != MB2_OK)
+            return MB2_ERR_CUDA;
+        if (cudaMemcpyAsync(out, w + o_o, size_t{num_bindings} * 8, cudaMemcpyDeviceToHost, r.stream) != cudaSuccess)
+            return MB2_ERR_CUDA;
+    } else {
+        std::fill(out, out + num_bindings, 0.0);
+    }
+    if (states_out != nullptr &&
+        cudaMemcpyAsync(states_out, r.state, state_bytes, cudaMemcpyDeviceToHost, r.stream) != cudaSuccess)
+        return MB2_ERR_CUDA;
+    if (cudaStreamSynchronize(r.stream) != cudaSuccess) return MB2_ERR_CUDA;
+    if (stats != nullptr) {
+        stats->passes = prog.passes.size();
+        stats->blocks = nb;
+        stats->parametric_blocks = static_cast<uint64_t>(std::count_if(flags.begin(), flags.end(), [](uint8_t f) {
+            return (f & mb2::kParamBlock) != 0;
+        }));
+        stats->h2d_bytes = host.size();
+        stats->fp64_ops_per_amp = prog.fp64_per_amp;
+    }
+    return MB2_OK;
+}

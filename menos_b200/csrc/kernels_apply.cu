@@ -239,11 +239,6 @@ static_assert(kR == 4, "the register-slot dispatch below is written for 4 regist
 // Index of the lowest set bit of a (compile-time) register index j > 0.
 __host__ __device__ constexpr int lowbit_index(int j) { return (j & 1) ? 0 : (j & 2) ? 1 : (j & 4) ? 2 : 3; }
 
-// 16-bit masks of the register indices j whose bit s is set.
-__device__ __forceinline__ uint32_t slot_mask(uint32_t s) {
-    return s == 0 ? 0xAAAAu : s == 1 ? 0xCCCCu : s == 2 ? 0xF0F0u : 0xFF00u;
-}
-
 template <int P, int KIND>
 __device__ __forceinline__ void g1(double2 (&a)[kNA], const double* md, uint32_t aux) {
     const double2 e0 = reinterpret_cast<const double2*>(md)[0], e1 = reinterpret_cast<const double2*>(md)[1];
@@ -440,14 +435,6 @@ __device__ __forceinline__ void diag_small(double2 (&a)[kNA], const double* md, 
     }
 }
 
-// Tile-local index of register slot j: thread part | the register bits.
-__device__ __forceinline__ uint32_t reg_local(uint32_t tb, int j, const uint32_t (&rb)[kR]) {
-    uint32_t l = tb;
-#pragma unroll
-    for (int b = 0; b < kR; ++b) l |= ((j >> b) & 1) ? rb[b] : 0u;
-    return l;
-}
-
 // cp.async of one 16-byte amplitude, global -> shared (L2 only, no L1).
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
@@ -466,7 +453,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 __global__ void __launch_bounds__(256, 1)
     k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m, uint64_t smask, const TileInstr* __restrict__ prog,
                 uint32_t nprog, const double* __restrict__ sdata, uint32_t nsdata, const double* __restrict__ gdata,
-                uint64_t ntiles) {
+                uint64_t ntiles, const double* __restrict__ pdata, uint32_t pstride, uint32_t bshift) {
     extern __shared__ double2 smem_tiles[];
     const uint32_t tid = threadIdx.x;
     const uint32_t tbits = m - kRegQubits;
@@ -544,7 +531,9 @@ __global__ void __launch_bounds__(256, 1)
                     const DI G = load_instr(sprog + pc);
                     ++pc;
                     if (G.op() == TOP_END) break;
-                    const double* md = sd + G.data();
+                    // Parametric blocks (a batched sweep) read the matrix of
+                    // this tile's binding: binding = tile >> bshift.
+                    const double* md = G.nthread() ? pdata + (t >> bshift) * pstride + G.data() : sd + G.data();
                     if (G.op() == TOP_G1) {
                         switch (G.kind()) {
                             case TK_GEN: dispatch_g1<TK_GEN>(G.pos(0), a, md, G.aux()); break;
@@ -699,7 +688,8 @@ int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, 
 }
 
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
-                     const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream) {
+                     const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
+                     const BatchLayout* batch) {
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_tile_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -711,12 +701,20 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileIns
     if (staged > kMaxStagedBytes) return MB2_ERR_INVALID;
     const uint32_t threads = 1u << (pass.m - kRegQubits);
     const size_t smem = 2 * (size_t{1} << pass.m) * sizeof(double2) + staged;
-    const uint64_t ntiles = (uint64_t{1} << n) >> pass.m;
+    // A batch adds the bindings above the n qubits: ntiles counts every
+    // binding's tiles, and n grows to the bits the binding index occupies.
+    uint64_t ntiles = (uint64_t{1} << n) >> pass.m;
+    uint32_t n_all = n;
+    if (batch != nullptr) {
+        ntiles *= batch->bindings;
+        while ((uint64_t{1} << (n_all - n)) < batch->bindings) ++n_all;
+    }
     const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m <= 11 ? 2u : 1u);
     const int grid = static_cast<int>(ntiles < cap ? ntiles : cap);
     k_tile_pass<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(
-        static_cast<double2*>(amps), n, pass.m, pass.smask, dev_instrs + pass.prog_begin, pass.prog_count,
-        dev_sdata + pass.sdata_begin, pass.sdata_count, dev_gdata, ntiles);
+        static_cast<double2*>(amps), n_all, pass.m, pass.smask, dev_instrs + pass.prog_begin, pass.prog_count,
+        dev_sdata + pass.sdata_begin, pass.sdata_count, dev_gdata, ntiles, batch ? batch->pdata : nullptr,
+        batch ? batch->pstride : 0u, n - pass.m);
     return status_of(cudaGetLastError());
 }
 

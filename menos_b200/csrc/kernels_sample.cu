@@ -300,11 +300,9 @@ __global__ void __launch_bounds__(32) k_seg_chain(const double2* __restrict__ st
     const int lane = threadIdx.x;
     double c = 0.0;
     uint64_t j = 0;
-    bool in_failed_segment = false;
     while (j < nchunks) {
         const ChunkMap m = maps[j];
         const bool head = seg_head(maps, j);
-        if (head) in_failed_segment = false;
         if (head && m.valid) {
             const SMap t = seg_total[j];
             double c2 = c;
@@ -314,7 +312,6 @@ __global__ void __launch_bounds__(32) k_seg_chain(const double2* __restrict__ st
                 j += t.count;
                 continue;
             }
-            in_failed_segment = true;
         }
         // This chunk on its own.
         if (lane == 0) {
@@ -336,7 +333,6 @@ __global__ void __launch_bounds__(32) k_seg_chain(const double2* __restrict__ st
             __syncwarp();
             if (lane == 0) seq[j] = 1;
         }
-        (void)in_failed_segment;
         ++j;
     }
     if (lane == 0) cstart[nchunks] = c;

@@ -102,6 +102,8 @@ struct TileProgram {
     std::vector<double> gdata;
     std::vector<uint32_t> order;       // block indices in application order
     std::vector<uint32_t> order_pass;  // the pass of each entry of `order`
+    std::vector<uint32_t> param_offsets;  // per block: offset in the per-binding record (parametric only)
+    uint32_t param_stride = 0;            // doubles per binding record
     std::vector<TileInstr> instrs;
     std::vector<double> data;
     uint64_t fp64_per_amp = 0;  // modelled FP64 instructions per amplitude
@@ -114,8 +116,17 @@ constexpr uint32_t kMinTileQubits = 4;
 
 // Low qubits every tile holds by default (runs of 2^3 amplitudes, 128 bytes).
 constexpr uint32_t kDefaultFixedLow = 3;
+// Flags of a block in a batched sweep.
+constexpr uint8_t kParamBlock = 1;     // its matrix differs between bindings
+constexpr uint8_t kParamAllReal = 2;   // ... but every entry is real in every binding
+constexpr uint8_t kParamM00Real = 4;   // ... entry (0,0) is real in every binding
+// parametric (optional, one flag per block): those blocks' data is not
+// staged; each gets an offset in a per-binding record instead
+// (param_offsets[block], record length param_stride doubles), and a kind
+// that holds for every parameter value.
 TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint32_t m,
-                              uint32_t fixed_low = kDefaultFixedLow);
+                              uint32_t fixed_low = kDefaultFixedLow,
+                              const std::vector<uint8_t>* parametric = nullptr);
 
 // ---- device launches (kernels_*.cu) ----------------------------------------
 struct DevCtx;  // forward (engine.cpp)
@@ -126,14 +137,26 @@ int launch_apply_diag(void* amps, uint32_t n, const uint32_t* q, uint32_t k, con
                       void* stream);
 int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* dev_matrix,
                          void* stream);
+// A batched sweep: `bindings` states of 2^n amplitudes back to back; the
+// data of a parametric instruction for binding b is at pdata + b * pstride
+// + instr.data (doubles).
+struct BatchLayout {
+    uint64_t bindings = 0;
+    const double* pdata = nullptr;
+    uint32_t pstride = 0;
+};
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
-                     const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream);
+                     const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
+                     const BatchLayout* batch = nullptr);
 // Expectation of num_terms Pauli terms: partials (num_terms * kExpBlocks * 2
 // doubles) then the fixed-order finish into out (num_terms * 2 doubles), all
 // device pointers.
 constexpr uint32_t kExpBlocks = 512;
 int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
                        uint32_t num_terms, double* dev_partials, double* dev_out, void* stream);
+// Batched sweep (batch.cpp, kernels_batch.cu).
+constexpr uint32_t kMaxBatchTerms = MB2_BATCH_MAX_TERMS;
+
 // Exact device sampler (kernels_sample.cu): the chunk size of its scan, the
 // scratch its internals need (beyond the sorted uniforms and the per-shot
 // basis output), and the launch.  dev_basis[s] receives the basis state of

@@ -131,12 +131,22 @@ uint32_t push_matrix(std::vector<double>& data, const std::vector<Cd>& m) {
 
 }  // namespace
 
-TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint32_t m, uint32_t fixed_low) {
+TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint32_t m, uint32_t fixed_low,
+                              const std::vector<uint8_t>* parametric) {
     if (m < kMinTileQubits || m > kMaxTileQubits) throw std::invalid_argument("tile width out of range");
     TileProgram prog;
     const uint32_t mt = std::min(m, n);
     if (mt < kRegQubits) throw std::invalid_argument("state too small for the tile kernel");
     const std::vector<PassSel> sels = select_passes(blocks, n, mt, fixed_low);
+    prog.param_offsets.assign(blocks.size(), 0);
+    auto param_flags = [&](uint32_t bi) -> uint8_t { return parametric ? (*parametric)[bi] : uint8_t{0}; };
+    // A parametric block's data goes to the per-binding record.
+    auto push_param = [&](uint32_t bi, uint32_t doubles) {
+        const uint32_t off = prog.param_stride;
+        prog.param_offsets[bi] = off;
+        prog.param_stride += (doubles + 1) & ~1u;  // keep 16-byte alignment
+        return off;
+    };
     for (const PassSel& sel : sels) {
         TilePass pass;
         pass.m = mt;
@@ -207,6 +217,16 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
                 for (uint32_t t = 0; t < b.k; ++t) g.pos[t] = static_cast<uint8_t>(local_pos(sel.smask, b.q[t]));
                 std::vector<Cd> d(dim);
                 for (uint32_t i = 0; i < dim; ++i) d[i] = b.m[i * dim + i];
+                if (param_flags(sel.gates[j]) & kParamBlock) {
+                    g.nthread = 1;
+                    g.data = push_param(sel.gates[j], 2 * dim);
+                    g.kind = b.k <= 2 ? TK_DSMALL : TK_GEN;
+                    if (b.k <= 2)
+                        for (uint32_t i = 0; i < dim; ++i) g.aux |= 2u << (2 * i);  // every entry multiplies
+                    prog.fp64_per_amp += 6;
+                    prog.instrs.push_back(g);
+                    continue;
+                }
                 g.data = push_staged(d);
                 if (b.k <= 2) {
                     // Entry classes: (1,0) copies, (-1,0) negates, the rest multiply.
@@ -245,9 +265,10 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
                 if (b.k == 2) g.pos[1] = static_cast<uint8_t>(slot[1]);
                 // Specialisations, each exact up to the sign of zero results
                 // (normalised at the store): monomial rows, real entries.
-                bool mono = true;
+                const uint8_t pf = param_flags(sel.gates[j]);
+                bool mono = (pf & kParamBlock) == 0;
                 uint32_t aux = 0;
-                for (uint32_t r = 0; r < dim; ++r) {
+                for (uint32_t r = 0; r < dim && mono; ++r) {
                     const int s = mono_src(b.m, dim, r);
                     if (s == -2) {
                         mono = false;
@@ -260,11 +281,16 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
                     g.aux = aux;
                     prog.fp64_per_amp += 6;
                 } else if (b.k == 1) {
-                    const bool all_real = is_real(b.m[0]) && is_real(b.m[1]) && is_real(b.m[2]) && is_real(b.m[3]);
+                    bool all_real = is_real(b.m[0]) && is_real(b.m[1]) && is_real(b.m[2]) && is_real(b.m[3]);
+                    bool m00_real = is_real(b.m[0]);
+                    if (pf & kParamBlock) {  // what holds for every binding
+                        all_real = (pf & kParamAllReal) != 0;
+                        m00_real = (pf & kParamM00Real) != 0;
+                    }
                     if (all_real) {
                         g.kind = TK_REAL;
                         prog.fp64_per_amp += 6;
-                    } else if (is_real(b.m[0])) {
+                    } else if (m00_real) {
                         g.kind = TK_U3;
                         prog.fp64_per_amp += 12;
                     } else {
@@ -275,7 +301,12 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
                     g.kind = TK_GEN;
                     prog.fp64_per_amp += 30;
                 }
-                g.data = push_staged(b.m);
+                if (pf & kParamBlock) {
+                    g.nthread = 1;
+                    g.data = push_param(sel.gates[j], 2 * dim * dim);
+                } else {
+                    g.data = push_staged(b.m);
+                }
                 prog.instrs.push_back(g);
                 continue;
             }
@@ -283,6 +314,8 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
             close_phase();
             g.op = TOP_SMEM;
             for (uint32_t t = 0; t < b.k; ++t) g.pos[t] = static_cast<uint8_t>(local_pos(sel.smask, b.q[t]));
+            if (param_flags(sel.gates[j]) & kParamBlock)
+                throw std::invalid_argument("parametric blocks wider than 2 qubits are not batched");
             g.data = push_matrix(prog.gdata, b.m);
             prog.instrs.push_back(g);
             prog.fp64_per_amp += 8ull * dim - 2;

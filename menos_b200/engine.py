@@ -150,6 +150,31 @@ class DeviceState:
         self._chk(lib().mb2_synchronize(self.h), "mb2_synchronize")
 
 
+def sweep_batch(ctx: Context, circ: Circuit, params, paulis, coefs, fuse_gates: bool = False, tile_qubits: int = 0,
+                want_states: bool = False):
+    """mb2_sweep_batch: <H> per binding for params[b] (one row per binding,
+    the circuit's parameter slots in op order).  Returns (values, states or
+    None, stats)."""
+    params = np.ascontiguousarray(np.asarray(params, np.float64))
+    if params.ndim == 1:
+        params = params.reshape(1, -1)
+    B, ppb = params.shape
+    arr, keep = to_mb2_ops(circ)
+    xs = np.ascontiguousarray([int(p[0]) for p in paulis] or [0], dtype=np.uint64)
+    zs = np.ascontiguousarray([int(p[1]) for p in paulis] or [0], dtype=np.uint64)
+    cs = np.ascontiguousarray(list(coefs) or [0.0], dtype=np.float64)
+    out = np.zeros(B, np.float64)
+    states = np.zeros((B, 1 << circ.num_qubits), np.complex128) if want_states else None
+    opts = _lib.BatchOptions(C128, 1 if fuse_gates else 0, tile_qubits, 0)
+    stats = _lib.BatchStats()
+    check(lib().mb2_sweep_batch(ctx.h, arr, len(circ.ops), circ.num_qubits, params.ctypes.data, ppb, B,
+                                xs.ctypes.data, zs.ctypes.data, cs.ctypes.data, len(paulis), C.byref(opts),
+                                out.ctypes.data, states.ctypes.data if want_states else None, C.byref(stats)),
+          ctx.h, "mb2_sweep_batch")
+    del keep
+    return out, states, stats
+
+
 # ---------------------------------------------------------------------------
 # The SimulationEngine mirror.
 # ---------------------------------------------------------------------------

@@ -105,6 +105,13 @@ def hea(n: int, layers: int, seed: int, circ: Circuit | None = None) -> Circuit:
     return c
 
 
+def hea_bindings(n: int, layers: int, count: int, seed: int):
+    """`count` parameter rows for hea(n, layers): per layer and qubit RY(theta)
+    then RZ(phi), angles in [-pi, pi) from mt19937_64(seed), in op order."""
+    rng = MT19937_64(seed)
+    return [[-math.pi + TWO_PI * rng.uniform() for _ in range(2 * n * layers)] for _ in range(count)]
+
+
 def pauli_strings(n: int, count: int, seed: int):
     """(x_mask, z_mask) pairs; per qubit w % 4 -> I, X, Y, Z."""
     rng = MT19937_64(seed)

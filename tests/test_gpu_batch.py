@@ -1,0 +1,57 @@
+"""The batched parameter sweep against single runs: every binding's state is
+bitwise the state the reference engine computes for that binding alone, and
+<H> agrees within the expectation tolerance."""
+import numpy as np
+import pytest
+
+from menos_b200 import workloads
+from menos_b200.engine import sweep_batch
+from test_host import as_oracle_circuit
+from test_oracle_pin import bits_equal
+
+pytestmark = pytest.mark.gpu
+
+
+def bound_circuit(n, layers, row):
+    c = workloads.hea(n, layers, 0)
+    k = 0
+    ops = []
+    for oc, qs, ps, m, cl in c.ops:
+        if ps:
+            ps = tuple(row[k:k + len(ps)])
+            k += len(ps)
+        ops.append((oc, qs, ps, m, cl))
+    c.ops = ops
+    return c
+
+
+@pytest.mark.parametrize("fuse", [False, True])
+def test_batch_matches_single_runs(ctx, ref, fuse):
+    n, layers, B = 10, 4, 13
+    rows = workloads.hea_bindings(n, layers, B, 99)
+    paulis = workloads.pauli_strings(n, 32, 5)
+    coefs = workloads.weights(32, 6)
+    vals, states, stats = sweep_batch(ctx, workloads.hea(n, layers, 0), rows, paulis, coefs, fuse_gates=fuse,
+                                      want_states=True)
+    assert stats.parametric_blocks > 0
+    for b in range(B):
+        c = as_oracle_circuit(bound_circuit(n, layers, rows[b]))
+        r = ref.run(c, fuse_gates=fuse, statevector=True, paulis=paulis)
+        assert bits_equal(states[b], r["statevector"]), b
+        h = sum(w * t for w, t in zip(coefs, r["terms"]))
+        assert abs(vals[b] - h.real) <= 1e-12 * max(1.0, sum(abs(w) for w in coefs)), (b, vals[b], h)
+
+
+def test_batch_hea16_subset(ctx, ref):
+    # The benchmark's shape (16 qubits, 8 layers, 32 terms) on a few bindings.
+    n, layers, B = 16, 8, 9
+    rows = workloads.hea_bindings(n, layers, B, 2026)
+    paulis = workloads.pauli_strings(n, 32, 7)
+    coefs = workloads.weights(32, 8)
+    vals, states, stats = sweep_batch(ctx, workloads.hea(n, layers, 0), rows, paulis, coefs, want_states=True)
+    for b in (0, 4, 8):
+        c = as_oracle_circuit(bound_circuit(n, layers, rows[b]))
+        r = ref.run(c, fuse_gates=False, statevector=True, paulis=paulis)
+        assert bits_equal(states[b], r["statevector"])
+        h = sum(w * t for w, t in zip(coefs, r["terms"]))
+        assert abs(vals[b] - h.real) <= 1e-11
