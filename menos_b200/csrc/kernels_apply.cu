@@ -339,41 +339,55 @@ __device__ __forceinline__ void dispatch_g2(int p0, int p1, double2 (&a)[kNA], c
 // A diagonal block of k <= 2 qubits in registers.  Each operand is either
 // a register slot (its bit over j is known at compile time in the templates
 // below) or a thread bit (one value for all 16 amplitudes).  The entry of
-// amplitude j is e = bit0 | bit1 << 1; its class (aux, 2 bits per entry)
-// picks copy, negate or multiply -- a warp-uniform choice per entry.
+// amplitude j is e = bit0 | bit1 << 1; its class (aux, 2 bits per entry:
+// 0 copy, 1 negate, 2 multiply) is resolved once per gate or per thread, and
+// each class runs its own loop, so an amplitude costs nothing (copy), two
+// integer ops (negate) or one complex product (multiply).
 struct Diag4 {
     double2 d[4];
     uint32_t aux;
 };
 
-__device__ __forceinline__ void diag_apply(double2& x, const Diag4& D, uint32_t e) {
-    const uint32_t cls = (D.aux >> (2 * e)) & 3u;
+__device__ __forceinline__ double2 diag_entry(const Diag4& D, uint32_t e) {
+    return (e & 2u) ? ((e & 1u) ? D.d[3] : D.d[2]) : ((e & 1u) ? D.d[1] : D.d[0]);
+}
+
+// Applies entry class `cls` with entry d to the amplitudes j whose selector
+// bits (j >> P0 & 1, j >> P1 & 1) equal (b0, b1); P < 0 means "no condition".
+template <int P0, int P1>
+__device__ __forceinline__ void diag_set(double2 (&a)[kNA], uint32_t cls, double2 d, int b0, int b1) {
     if (cls == 1u) {
-        x = cneg(x);
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) {
+            if (P0 >= 0 && ((j >> (P0 < 0 ? 0 : P0)) & 1) != b0) continue;
+            if (P1 >= 0 && ((j >> (P1 < 0 ? 0 : P1)) & 1) != b1) continue;
+            a[j] = cneg(a[j]);
+        }
     } else if (cls == 2u) {
-        // A select tree, not an indexed load: e is often a run-time value.
-        const double2 d = (e & 2u) ? ((e & 1u) ? D.d[3] : D.d[2]) : ((e & 1u) ? D.d[1] : D.d[0]);
-        x = cmul(d.x, d.y, x);
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) {
+            if (P0 >= 0 && ((j >> (P0 < 0 ? 0 : P0)) & 1) != b0) continue;
+            if (P1 >= 0 && ((j >> (P1 < 0 ? 0 : P1)) & 1) != b1) continue;
+            a[j] = cmul(d.x, d.y, a[j]);
+        }
     }
 }
 
-// Operand 0 in register slot P0, operand 1 in slot P1 (k == 2), or k == 1 (P1 < 0).
+// Both operands in register slots (P1 < 0: one operand).
 template <int P0, int P1>
 __device__ __forceinline__ void diag_rr(double2 (&a)[kNA], const Diag4& D) {
 #pragma unroll
-    for (int j = 0; j < kNA; ++j) {
-        const uint32_t e = static_cast<uint32_t>((j >> P0) & 1) | (P1 >= 0 ? static_cast<uint32_t>((j >> (P1 < 0 ? 0 : P1)) & 1) << 1 : 0u);
-        diag_apply(a[j], D, e);
-    }
+    for (int e = 0; e < (P1 >= 0 ? 4 : 2); ++e)
+        diag_set<P0, P1>(a, (D.aux >> (2 * e)) & 3u, D.d[e], e & 1, (e >> 1) & 1);
 }
 
-// One operand in register slot P (its bit is `shift` of e), the other a thread bit `tv` (at bit 1 - shift).
+// One operand in register slot P (bit `shift` of e), the other a thread bit tv.
 template <int P>
 __device__ __forceinline__ void diag_rt(double2 (&a)[kNA], const Diag4& D, uint32_t shift, uint32_t tv) {
 #pragma unroll
-    for (int j = 0; j < kNA; ++j) {
-        const uint32_t e = (static_cast<uint32_t>((j >> P) & 1) << shift) | (tv << (1u - shift));
-        diag_apply(a[j], D, e);
+    for (int b = 0; b < 2; ++b) {
+        const uint32_t e = (static_cast<uint32_t>(b) << shift) | (tv << (1u - shift));
+        diag_set<P, -1>(a, (D.aux >> (2 * e)) & 3u, diag_entry(D, e), b, 0);
     }
 }
 
@@ -388,8 +402,7 @@ __device__ __forceinline__ void diag_small(double2 (&a)[kNA], const double* md, 
     D.d[3] = k > 1 ? reinterpret_cast<const double2*>(md)[3] : D.d[1];
     if (k == 1) {
         if (s0 < 0) {
-#pragma unroll
-            for (int j = 0; j < kNA; ++j) diag_apply(a[j], D, t0);
+            diag_set<-1, -1>(a, (aux >> (2 * t0)) & 3u, diag_entry(D, t0), 0, 0);
             return;
         }
         switch (s0) {
@@ -420,8 +433,7 @@ __device__ __forceinline__ void diag_small(double2 (&a)[kNA], const double* md, 
     }
     if (s0 < 0 && s1 < 0) {
         const uint32_t e = t0 | (t1 << 1);
-#pragma unroll
-        for (int j = 0; j < kNA; ++j) diag_apply(a[j], D, e);
+        diag_set<-1, -1>(a, (aux >> (2 * e)) & 3u, diag_entry(D, e), 0, 0);
         return;
     }
     const int s = s0 >= 0 ? s0 : s1;
@@ -432,6 +444,58 @@ __device__ __forceinline__ void diag_small(double2 (&a)[kNA], const double* md, 
         case 1: diag_rt<1>(a, D, shift, tv); break;
         case 2: diag_rt<2>(a, D, shift, tv); break;
         default: diag_rt<3>(a, D, shift, tv); break;
+    }
+}
+
+// Exact permutations (every nonzero entry (1,0)): register moves only.
+// TK_X: 1q swap; TK_SW12 / TK_SW13 / TK_SW23: 2q, exchange local indices
+// (1,2) (SWAP), (1,3) (CX, control = operand 0), (2,3) (CX, control = operand 1).
+template <int P>
+__device__ __forceinline__ void perm1(double2 (&a)[kNA]) {
+#pragma unroll
+    for (int j = 0; j < kNA; ++j) {
+        if (j & (1 << P)) continue;
+        const double2 t = a[j];
+        a[j] = a[j | (1 << P)];
+        a[j | (1 << P)] = t;
+    }
+}
+
+template <int P0, int P1, int KIND>
+__device__ __forceinline__ void perm2(double2 (&a)[kNA]) {
+    if constexpr (P0 == P1) {
+        return;
+    } else {
+        constexpr int lo = KIND == TK_SW23 ? 2 : 1;
+        constexpr int hi = KIND == TK_SW12 ? 2 : 3;
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) {
+            if (j & ((1 << P0) | (1 << P1))) continue;
+            const int il = j | ((lo & 1) ? (1 << P0) : 0) | ((lo & 2) ? (1 << P1) : 0);
+            const int ih = j | ((hi & 1) ? (1 << P0) : 0) | ((hi & 2) ? (1 << P1) : 0);
+            const double2 t = a[il];
+            a[il] = a[ih];
+            a[ih] = t;
+        }
+    }
+}
+
+template <int KIND>
+__device__ __forceinline__ void dispatch_perm2(int p0, int p1, double2 (&a)[kNA]) {
+    switch (p0 * 4 + p1) {
+        case 1: perm2<0, 1, KIND>(a); break;
+        case 2: perm2<0, 2, KIND>(a); break;
+        case 3: perm2<0, 3, KIND>(a); break;
+        case 4: perm2<1, 0, KIND>(a); break;
+        case 6: perm2<1, 2, KIND>(a); break;
+        case 7: perm2<1, 3, KIND>(a); break;
+        case 8: perm2<2, 0, KIND>(a); break;
+        case 9: perm2<2, 1, KIND>(a); break;
+        case 11: perm2<2, 3, KIND>(a); break;
+        case 12: perm2<3, 0, KIND>(a); break;
+        case 13: perm2<3, 1, KIND>(a); break;
+        case 14: perm2<3, 2, KIND>(a); break;
+        default: break;
     }
 }
 
@@ -539,11 +603,24 @@ __global__ void __launch_bounds__(256, 1)
                             case TK_GEN: dispatch_g1<TK_GEN>(G.pos(0), a, md, G.aux()); break;
                             case TK_U3: dispatch_g1<TK_U3>(G.pos(0), a, md, G.aux()); break;
                             case TK_REAL: dispatch_g1<TK_REAL>(G.pos(0), a, md, G.aux()); break;
+                            case TK_X:
+                                switch (G.pos(0)) {
+                                    case 0: perm1<0>(a); break;
+                                    case 1: perm1<1>(a); break;
+                                    case 2: perm1<2>(a); break;
+                                    default: perm1<3>(a); break;
+                                }
+                                break;
                             default: dispatch_g1<TK_MONO>(G.pos(0), a, md, G.aux()); break;
                         }
                     } else if (G.op() == TOP_G2) {
-                        if (G.kind() == TK_MONO) dispatch_g2<TK_MONO>(G.pos(0), G.pos(1), a, md, G.aux());
-                        else dispatch_g2<TK_GEN>(G.pos(0), G.pos(1), a, md, G.aux());
+                        switch (G.kind()) {
+                            case TK_SW12: dispatch_perm2<TK_SW12>(G.pos(0), G.pos(1), a); break;
+                            case TK_SW13: dispatch_perm2<TK_SW13>(G.pos(0), G.pos(1), a); break;
+                            case TK_SW23: dispatch_perm2<TK_SW23>(G.pos(0), G.pos(1), a); break;
+                            case TK_MONO: dispatch_g2<TK_MONO>(G.pos(0), G.pos(1), a, md, G.aux()); break;
+                            default: dispatch_g2<TK_GEN>(G.pos(0), G.pos(1), a, md, G.aux()); break;
+                        }
                     } else if (G.kind() == TK_DSMALL) {
                         int sl[2] = {-1, -1};
                         uint32_t tv[2] = {0u, 0u};

@@ -67,7 +67,11 @@ enum TileKind : uint8_t {
     TK_U3 = 1,    // 1q: entry (0,0) real, the others general
     TK_REAL = 2,  // 1q: every entry real
     TK_MONO = 3,  // 1 nonzero entry per row: a permutation up to per-row factors
-    TK_DSMALL = 4 // diagonal, k <= 2: per-entry class in aux (2 bits each: 0 = (1,0), 1 = (-1,0), 2 = general)
+    TK_DSMALL = 4, // diagonal, k <= 2: per-entry class in aux (2 bits each: 0 = (1,0), 1 = (-1,0), 2 = general)
+    TK_X = 5,      // 1q exact swap of the pair (X)
+    TK_SW12 = 6,   // 2q exact exchange of local indices 1 and 2 (SWAP)
+    TK_SW13 = 7,   // 2q exact exchange of local indices 1 and 3 (CX, control = operand 0)
+    TK_SW23 = 8    // 2q exact exchange of local indices 2 and 3 (CX, control = operand 1)
 };
 struct TileInstr {
     uint8_t op;

@@ -16,6 +16,8 @@
 // memory (TOP_SMEM).
 #include <algorithm>
 #include <bit>
+#include <cmath>
+#include <initializer_list>
 #include <stdexcept>
 
 #include "mb2_internal.h"
@@ -279,7 +281,24 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
                 if (mono) {
                     g.kind = TK_MONO;
                     g.aux = aux;
-                    prog.fp64_per_amp += 6;
+                    // Exact permutations run as register moves.
+                    bool ones = true;
+                    for (uint32_t r = 0; r < dim; ++r) {
+                        const uint32_t src = (aux >> (3 * r)) & 7u;
+                        if (src == 7u || b.m[r * dim + src] != Cd(1.0, 0.0) || std::signbit(b.m[r * dim + src].imag()))
+                            ones = false;
+                    }
+                    auto is_perm = [&](std::initializer_list<uint32_t> srcs) {
+                        uint32_t r = 0;
+                        for (uint32_t v : srcs)
+                            if (((aux >> (3 * r++)) & 7u) != v) return false;
+                        return true;
+                    };
+                    if (ones && b.k == 1 && is_perm({1, 0})) g.kind = TK_X;
+                    else if (ones && b.k == 2 && is_perm({0, 2, 1, 3})) g.kind = TK_SW12;
+                    else if (ones && b.k == 2 && is_perm({0, 3, 2, 1})) g.kind = TK_SW13;
+                    else if (ones && b.k == 2 && is_perm({0, 1, 3, 2})) g.kind = TK_SW23;
+                    prog.fp64_per_amp += (g.kind == TK_MONO) ? 6 : 0;
                 } else if (b.k == 1) {
                     bool all_real = is_real(b.m[0]) && is_real(b.m[1]) && is_real(b.m[2]) && is_real(b.m[3]);
                     bool m00_real = is_real(b.m[0]);
