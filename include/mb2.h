@@ -234,6 +234,59 @@ int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num_ops, uint3
                     uint32_t num_terms, const mb2_batch_options* opts, double* out,
                     double* states_out, mb2_batch_stats* stats);
 
+/* ---- serving loop (continuous batching) -------------------------------- */
+/* A server takes circuit requests as they arrive and runs them on one GPU:
+ * `slots` requests at a time, each on its own stream, admitted against a
+ * device-memory budget (state + staging); a request that arrives while
+ * others run starts as soon as a slot and memory free up.  Results do not
+ * depend on what else runs.  New in this engine: the reference runs
+ * circuits one after another (src/api/batch.cpp:10-27). */
+enum { MB2_OUT_COUNTS = 1, MB2_OUT_EXPECTATION = 2 };
+typedef struct mb2_server mb2_server;
+typedef struct mb2_server_options {
+    uint64_t device_budget_bytes;  /* 0: 90% of the free device memory */
+    uint32_t slots;                /* concurrent requests; 0: 16 */
+    uint32_t reserved;
+} mb2_server_options;
+typedef struct mb2_request {
+    const mb2_op* ops;
+    uint32_t num_ops;
+    uint32_t num_qubits;
+    double global_phase;
+    int32_t fuse_gates;
+    int32_t output;                /* MB2_OUT_COUNTS or MB2_OUT_EXPECTATION */
+    uint64_t shots, seed;          /* counts */
+    const uint32_t* targets;       /* counts: (qubit, clbit) pairs */
+    uint32_t num_targets;
+    uint32_t num_terms;            /* expectation: <H> = sum_t coefs[t] <P_t> (real part) */
+    const uint64_t* x_masks;
+    const uint64_t* z_masks;
+    const double* coefs;
+} mb2_request;
+typedef struct mb2_completion {
+    uint64_t ticket;
+    int32_t status;                /* MB2_OK or the failing call's status */
+    uint32_t reserved;
+    double value;                  /* expectation requests */
+    uint64_t num_outcomes;         /* counts requests */
+    const uint64_t* outcomes;      /* ascending; owned by the server until mb2_server_release */
+    const uint64_t* counts;
+    double queue_seconds;          /* submit -> admission */
+    double latency_seconds;        /* submit -> completion */
+} mb2_completion;
+int mb2_server_create(mb2_context* ctx, const mb2_server_options* opts, mb2_server** out);
+/* Copies the request; MB2_ERR_RESOURCE if it could never fit the budget. */
+int mb2_server_submit(mb2_server* server, const mb2_request* request, uint64_t* ticket);
+/* Up to `capacity` completions; waits at most timeout_ms for the first.
+ * MB2_ERR_TIMEOUT when none arrived. */
+int mb2_server_poll(mb2_server* server, mb2_completion* out, uint32_t capacity, uint32_t* count,
+                    uint32_t timeout_ms);
+int mb2_server_release(mb2_server* server, uint64_t ticket);
+int mb2_server_stats(mb2_server* server, uint64_t* pending, uint64_t* in_flight, uint64_t* held_bytes,
+                     uint64_t* budget_bytes);
+/* Drops pending requests, waits for the running ones, frees everything. */
+int mb2_server_destroy(mb2_server* server);
+
 /* ---- calibration ------------------------------------------------------- */
 /* Measures the device's FP64 multiply/add issue rate (instructions per
  * second) and its device-to-device copy bandwidth (read+write GB/s), for the

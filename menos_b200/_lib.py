@@ -43,6 +43,28 @@ class BatchStats(C.Structure):
                 ("h2d_bytes", C.c_uint64), ("fp64_ops_per_amp", C.c_uint64)]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("device_budget_bytes", C.c_uint64), ("slots", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("ops", C.POINTER(MB2Op)), ("num_ops", C.c_uint32), ("num_qubits", C.c_uint32),
+                ("global_phase", C.c_double), ("fuse_gates", C.c_int32), ("output", C.c_int32),
+                ("shots", C.c_uint64), ("seed", C.c_uint64), ("targets", C.c_void_p), ("num_targets", C.c_uint32),
+                ("num_terms", C.c_uint32), ("x_masks", C.c_void_p), ("z_masks", C.c_void_p),
+                ("coefs", C.c_void_p)]
+
+
+class Completion(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("status", C.c_int32), ("reserved", C.c_uint32), ("value", C.c_double),
+                ("num_outcomes", C.c_uint64), ("outcomes", C.POINTER(C.c_uint64)),
+                ("counts", C.POINTER(C.c_uint64)), ("queue_seconds", C.c_double),
+                ("latency_seconds", C.c_double)]
+
+
+OUT_COUNTS, OUT_EXPECTATION = 1, 2
+
+
 class SweepStats(C.Structure):
     _fields_ = [("blocks", C.c_uint64), ("passes", C.c_uint64), ("launches", C.c_uint64),
                 ("fp64_ops_per_amp", C.c_uint64)]
@@ -59,6 +81,13 @@ SIGNATURES = {
     "mb2_sweep_batch": (C.c_int, [_VP, C.POINTER(MB2Op), C.c_uint32, C.c_uint32, _VP, C.c_uint32, C.c_uint32,
                                   _VP, _VP, _VP, C.c_uint32, C.POINTER(BatchOptions), _VP, _VP,
                                   C.POINTER(BatchStats)]),
+    "mb2_server_create": (C.c_int, [_VP, C.POINTER(ServerOptions), C.POINTER(_VP)]),
+    "mb2_server_submit": (C.c_int, [_VP, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "mb2_server_poll": (C.c_int, [_VP, C.POINTER(Completion), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32]),
+    "mb2_server_release": (C.c_int, [_VP, C.c_uint64]),
+    "mb2_server_stats": (C.c_int, [_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                   C.POINTER(C.c_uint64)]),
+    "mb2_server_destroy": (C.c_int, [_VP]),
     "mb2_probe_rates": (C.c_int, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mb2_state_alloc": (C.c_int, [_VP, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(_VP)]),
     "mb2_state_free": (C.c_int, [_VP]),

@@ -33,6 +33,7 @@ struct mb2_state {
     int precision = MB2_C128;
     void* amps = nullptr;
     cudaStream_t stream = nullptr;
+    bool owns_stream = true;
     void* scratch = nullptr;  // staging: program, matrices, masks, partials
     size_t scratch_bytes = 0;
     mb2_sweep_stats stats{};
@@ -65,17 +66,19 @@ int cuda_fail(mb2_context* ctx, cudaError_t e, const char* what) {
 
 size_t amp_bytes(int precision) { return precision == MB2_C64 ? 8 : 16; }
 
-// Grow-only device staging buffer of the state.  Freed buffers may still be
-// read by queued kernels, so the stream is drained first.
+// Grow-only device staging buffer of the state.  Allocations are
+// stream-ordered (cudaMallocAsync / cudaFreeAsync on the state's stream):
+// work queued before a free finishes before the memory is reused, and no
+// call synchronises the device, so states driven from other threads keep
+// running.
 int ensure_scratch(mb2_state* s, size_t bytes) {
     if (bytes <= s->scratch_bytes) return MB2_OK;
-    MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
-    if (s->scratch != nullptr) MB2_CUDA(s->ctx, cudaFree(s->scratch));
+    if (s->scratch != nullptr) MB2_CUDA(s->ctx, cudaFreeAsync(s->scratch, s->stream));
     s->scratch = nullptr;
     s->scratch_bytes = 0;
     size_t want = 1 << 20;
     while (want < bytes) want <<= 1;
-    MB2_CUDA(s->ctx, cudaMalloc(&s->scratch, want));
+    MB2_CUDA(s->ctx, cudaMallocAsync(&s->scratch, want, s->stream));
     s->scratch_bytes = want;
     return MB2_OK;
 }
@@ -134,6 +137,33 @@ uint32_t tile_width(uint32_t requested, uint32_t n, const std::vector<mb2::Block
 
 }  // namespace
 
+namespace mb2 {
+int context_device(const mb2_context* ctx) { return ctx == nullptr ? 0 : ctx->device; }
+
+// A state whose work is queued on a stream the caller owns (the serving
+// loop's worker streams); freed with mb2_state_free, which leaves the
+// stream alone.
+int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, void* stream, mb2_state** out) {
+    if (ctx == nullptr || out == nullptr || stream == nullptr) return MB2_ERR_INVALID;
+    *out = nullptr;
+    if (num_qubits < 1 || num_qubits > 40) return fail(ctx, MB2_ERR_INVALID, "num_qubits must be 1..40");
+    const uint64_t bytes = (uint64_t{1} << num_qubits) * 16;
+    if (bytes > budget_bytes) return fail(ctx, MB2_ERR_RESOURCE, "state over budget");
+    auto* s = new mb2_state;
+    s->ctx = ctx;
+    s->n = num_qubits;
+    s->stream = static_cast<cudaStream_t>(stream);
+    s->owns_stream = false;
+    const cudaError_t e = cudaMallocAsync(&s->amps, bytes, s->stream);
+    if (e != cudaSuccess) {
+        delete s;
+        return cuda_fail(ctx, e, "cudaMallocAsync(state)");
+    }
+    *out = s;
+    return MB2_OK;
+}
+}  // namespace mb2
+
 extern "C" {
 
 int mb2_context_create(int device, mb2_context** out) {
@@ -148,6 +178,12 @@ int mb2_context_create(int device, mb2_context** out) {
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return MB2_ERR_NO_DEVICE;
     if (prop.major < 10) return MB2_ERR_NO_DEVICE;  // sm_100a kernels only
     if (cudaSetDevice(device) != cudaSuccess) return MB2_ERR_NO_DEVICE;
+    // Freed states stay in the device's stream-ordered pool for reuse.
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~uint64_t{0};
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     auto* ctx = new mb2_context;
     ctx->device = device;
     ctx->sm_count = prop.multiProcessorCount;
@@ -203,16 +239,16 @@ int mb2_state_alloc(mb2_context* ctx, uint32_t num_qubits, int precision, uint64
     s->ctx = ctx;
     s->n = num_qubits;
     s->precision = precision;
-    cudaError_t e = cudaMalloc(&s->amps, bytes);
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
-        delete s;
-        return cuda_fail(ctx, e, "cudaMalloc(state)");
-    }
-    e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-        cudaFree(s->amps);
         delete s;
         return cuda_fail(ctx, e, "cudaStreamCreate");
+    }
+    e = cudaMallocAsync(&s->amps, bytes, s->stream);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return cuda_fail(ctx, e, "cudaMallocAsync(state)");
     }
     *out = s;
     return MB2_OK;
@@ -220,10 +256,10 @@ int mb2_state_alloc(mb2_context* ctx, uint32_t num_qubits, int precision, uint64
 
 int mb2_state_free(mb2_state* s) {
     if (s == nullptr) return MB2_OK;
+    if (s->scratch) cudaFreeAsync(s->scratch, s->stream);
+    cudaFreeAsync(s->amps, s->stream);
     cudaStreamSynchronize(s->stream);
-    if (s->scratch) cudaFree(s->scratch);
-    cudaFree(s->amps);
-    cudaStreamDestroy(s->stream);
+    if (s->owns_stream) cudaStreamDestroy(s->stream);
     delete s;
     return MB2_OK;
 }

@@ -169,6 +169,10 @@ constexpr uint32_t kSampleChunk = 4096;
 size_t sample_scratch_bytes(uint32_t n, uint64_t shots);
 int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
                   uint64_t* dev_basis, void* stream);
+int context_device(const mb2_context* ctx);
+// A complex128 state on a caller-owned stream (engine.cpp).
+int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, void* stream, mb2_state** out);
+
 // Calibration probes (kernels_probe.cu): FP64 instructions per second and
 // device-to-device copy GB/s (read + write bytes), on the current device.
 int probe_rates(int sm_count, double* fp64_per_s, double* copy_gbs);

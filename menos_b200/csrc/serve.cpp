@@ -1,0 +1,290 @@
+// The serving loop: continuous batching of circuit requests on one GPU.
+//
+// Requests (any qubit count and depth, counts or <H>) arrive through
+// mb2_server_submit at any time.  `slots` worker threads each own a CUDA
+// stream; a worker takes the oldest pending request whose device memory
+// (state + staging) fits what is left of the admission budget, runs it on
+// its stream -- init, the tiled sweep, then the device sampler or the Pauli
+// reduction -- and posts a completion.  Requests that arrive while others run
+// are admitted as soon as a slot and memory free up, and their kernels run
+// concurrently on the device.  Every kernel's result is independent of what
+// else runs (fixed grids, fixed reduction orders), so a request's result is
+// the same alone and in the mix.
+//
+// Admission mirrors the reference's two-level budget check: the job's own
+// budget (the state must fit, else MB2_ERR_RESOURCE, src/engines/dense/
+// state_vector.cpp:16-28) and a ledger of bytes currently held
+// (src/common/memory_ledger.h:37-117), here the device budget of the server.
+// An oldest request that has waited longer than the starvation limit stops
+// smaller ones from being admitted ahead of it until it fits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "mb2_internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t ticket = 0;
+    std::vector<mb2_op> ops;
+    std::vector<std::vector<double>> matrices;
+    uint32_t n = 0;
+    double global_phase = 0.0;
+    int32_t fuse = 1;
+    int32_t output = MB2_OUT_EXPECTATION;
+    uint64_t shots = 0, seed = 0;
+    std::vector<uint32_t> targets;
+    std::vector<uint64_t> xs, zs;
+    std::vector<double> coefs;
+    uint64_t bytes = 0;  // admission charge
+    Clock::time_point submitted;
+};
+
+struct Done {
+    mb2_completion c{};
+    std::vector<uint64_t> outcomes, counts;
+};
+
+uint64_t admission_bytes(const Request& r) {
+    const uint64_t state = (uint64_t{1} << r.n) * 16;
+    const uint64_t nchunks = std::max<uint64_t>(1, (uint64_t{1} << r.n) / mb2::kSampleChunk);
+    const uint64_t sampler = r.output == MB2_OUT_COUNTS ? 16 * r.shots + 128 * nchunks : 0;
+    const uint64_t expect = 16ull * mb2::kExpBlocks * std::max<size_t>(1, r.xs.size());
+    // program staging (instructions + matrices), rounded as the state rounds it
+    const uint64_t program = 128ull * r.ops.size() + (1ull << 20);
+    return state + std::max(sampler, expect) + program + (2ull << 20);
+}
+
+}  // namespace
+
+struct mb2_server {
+    mb2_context* ctx = nullptr;
+    uint64_t budget = 0;
+    uint64_t held = 0;
+    double starvation_s = 0.5;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request> pending;
+    std::deque<Done> done;
+    std::map<uint64_t, Done> released_wait;  // completions handed out, their arrays alive until release
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    uint32_t in_flight = 0;
+    std::vector<std::thread> workers;
+    std::vector<cudaStream_t> streams;
+};
+
+namespace {
+
+// The oldest pending request that fits the remaining budget; none if the
+// oldest has waited past the starvation limit and does not fit.
+bool pick(mb2_server* s, Request& out) {
+    if (s->pending.empty()) return false;
+    const Request& head = s->pending.front();
+    const bool head_fits = s->held + head.bytes <= s->budget;
+    const double head_wait = std::chrono::duration<double>(Clock::now() - head.submitted).count();
+    for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
+        if (s->held + it->bytes <= s->budget) {
+            if (it != s->pending.begin() && !head_fits && head_wait > s->starvation_s) return false;
+            out = std::move(*it);
+            s->pending.erase(it);
+            s->held += out.bytes;
+            return true;
+        }
+    }
+    return false;
+}
+
+void run_request(mb2_server* s, cudaStream_t stream, Request& r, Done& d) {
+    mb2_state* st = nullptr;
+    int rc = mb2::state_on_stream(s->ctx, r.n, ~uint64_t{0}, stream, &st);
+    if (rc == MB2_OK) rc = mb2_init(st, r.global_phase);
+    if (rc == MB2_OK) {
+        mb2_sweep_options o{r.fuse, 0, 0, 0};
+        rc = mb2_apply_program(st, r.ops.data(), static_cast<uint32_t>(r.ops.size()), &o);
+    }
+    if (rc == MB2_OK && r.output == MB2_OUT_EXPECTATION) {
+        std::vector<double> terms(2 * r.xs.size());
+        rc = mb2_expectation(st, r.xs.data(), r.zs.data(), static_cast<uint32_t>(r.xs.size()), terms.data());
+        double total = 0.0;
+        for (size_t t = 0; t < r.xs.size() && rc == MB2_OK; ++t) total += r.coefs[t] * terms[2 * t];
+        d.c.value = total;
+    } else if (rc == MB2_OK && r.output == MB2_OUT_COUNTS) {
+        d.outcomes.resize(std::max<uint64_t>(1, r.shots));
+        d.counts.resize(std::max<uint64_t>(1, r.shots));
+        uint64_t distinct = d.outcomes.size();
+        rc = mb2_sample(st, r.shots, r.seed, r.targets.data(), static_cast<uint32_t>(r.targets.size() / 2),
+                        d.outcomes.data(), d.counts.data(), &distinct);
+        d.outcomes.resize(rc == MB2_OK ? distinct : 0);
+        d.counts.resize(rc == MB2_OK ? distinct : 0);
+        d.c.num_outcomes = rc == MB2_OK ? distinct : 0;
+    }
+    if (st != nullptr) mb2_state_free(st);
+    d.c.status = rc;
+}
+
+void worker(mb2_server* s, uint32_t slot) {
+    cudaSetDevice(mb2::context_device(s->ctx));
+    for (;;) {
+        Request r;
+        Clock::time_point admitted;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait(lk, [&] { return s->stop || pick(s, r); });
+            if (r.ticket == 0) return;  // stopped with nothing picked
+            admitted = Clock::now();
+            ++s->in_flight;
+        }
+        Done d;
+        d.c.ticket = r.ticket;
+        run_request(s, s->streams[slot], r, d);
+        const auto finished = Clock::now();
+        d.c.queue_seconds = std::chrono::duration<double>(admitted - r.submitted).count();
+        d.c.latency_seconds = std::chrono::duration<double>(finished - r.submitted).count();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->held -= r.bytes;
+            --s->in_flight;
+            s->done.push_back(std::move(d));
+        }
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();  // memory freed: others may fit now
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int mb2_server_create(mb2_context* ctx, const mb2_server_options* opts, mb2_server** out) {
+    if (ctx == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    *out = nullptr;
+    mb2_server_options o{0, 0, 0};
+    if (opts != nullptr) o = *opts;
+    uint64_t free_b = 0, total_b = 0;
+    if (mb2_device_info(ctx, nullptr, &total_b, &free_b) != MB2_OK) return MB2_ERR_CUDA;
+    cudaSetDevice(mb2::context_device(ctx));
+    auto* s = new mb2_server;
+    s->ctx = ctx;
+    s->budget = o.device_budget_bytes != 0 ? std::min<uint64_t>(o.device_budget_bytes, free_b) : (free_b / 10) * 9;
+    const uint32_t slots = o.slots != 0 ? std::min<uint32_t>(o.slots, 64) : 16;
+    for (uint32_t i = 0; i < slots; ++i) {
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            for (cudaStream_t x : s->streams) cudaStreamDestroy(x);
+            delete s;
+            return MB2_ERR_CUDA;
+        }
+        s->streams.push_back(st);
+    }
+    for (uint32_t i = 0; i < slots; ++i) s->workers.emplace_back(worker, s, i);
+    *out = s;
+    return MB2_OK;
+}
+
+int mb2_server_submit(mb2_server* s, const mb2_request* q, uint64_t* ticket) {
+    if (s == nullptr || q == nullptr || ticket == nullptr || (q->ops == nullptr && q->num_ops != 0))
+        return MB2_ERR_INVALID;
+    if (q->num_qubits < 1 || q->num_qubits > 34) return MB2_ERR_INVALID;
+    if (q->output != MB2_OUT_COUNTS && q->output != MB2_OUT_EXPECTATION) return MB2_ERR_INVALID;
+    Request r;
+    r.n = q->num_qubits;
+    r.global_phase = q->global_phase;
+    r.fuse = q->fuse_gates;
+    r.output = q->output;
+    r.shots = q->shots;
+    r.seed = q->seed;
+    r.ops.assign(q->ops, q->ops + q->num_ops);
+    for (mb2_op& o : r.ops) {  // own the unitary matrices
+        if (o.opcode != MB2_UNITARY || o.matrix == nullptr) continue;
+        const size_t len = 2ull << (2 * o.num_qubits);
+        r.matrices.emplace_back(o.matrix, o.matrix + len);
+        o.matrix = r.matrices.back().data();
+    }
+    if (q->output == MB2_OUT_COUNTS) {
+        if (q->num_targets > 0 && q->targets == nullptr) return MB2_ERR_INVALID;
+        r.targets.assign(q->targets, q->targets + 2 * q->num_targets);
+    } else {
+        if (q->num_terms > 0 && (!q->x_masks || !q->z_masks || !q->coefs)) return MB2_ERR_INVALID;
+        r.xs.assign(q->x_masks, q->x_masks + q->num_terms);
+        r.zs.assign(q->z_masks, q->z_masks + q->num_terms);
+        r.coefs.assign(q->coefs, q->coefs + q->num_terms);
+    }
+    r.bytes = admission_bytes(r);
+    r.submitted = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (r.bytes > s->budget) return MB2_ERR_RESOURCE;  // can never be admitted
+        if (s->stop) return MB2_ERR_INVALID;
+        r.ticket = s->next_ticket++;
+        *ticket = r.ticket;
+        s->pending.push_back(std::move(r));
+    }
+    s->cv_work.notify_one();
+    return MB2_OK;
+}
+
+int mb2_server_poll(mb2_server* s, mb2_completion* out, uint32_t capacity, uint32_t* count, uint32_t timeout_ms) {
+    if (s == nullptr || count == nullptr || (capacity > 0 && out == nullptr)) return MB2_ERR_INVALID;
+    *count = 0;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->done.empty() && timeout_ms > 0)
+        s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return !s->done.empty(); });
+    while (!s->done.empty() && *count < capacity) {
+        Done d = std::move(s->done.front());
+        s->done.pop_front();
+        auto& kept = s->released_wait[d.c.ticket];
+        kept = std::move(d);
+        kept.c.outcomes = kept.outcomes.empty() ? nullptr : kept.outcomes.data();
+        kept.c.counts = kept.counts.empty() ? nullptr : kept.counts.data();
+        out[(*count)++] = kept.c;
+    }
+    return *count > 0 ? MB2_OK : MB2_ERR_TIMEOUT;
+}
+
+int mb2_server_release(mb2_server* s, uint64_t ticket) {
+    if (s == nullptr) return MB2_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    return s->released_wait.erase(ticket) ? MB2_OK : MB2_ERR_INVALID;
+}
+
+int mb2_server_stats(mb2_server* s, uint64_t* pending, uint64_t* in_flight, uint64_t* held_bytes,
+                     uint64_t* budget_bytes) {
+    if (s == nullptr) return MB2_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (pending) *pending = s->pending.size();
+    if (in_flight) *in_flight = s->in_flight;
+    if (held_bytes) *held_bytes = s->held;
+    if (budget_bytes) *budget_bytes = s->budget;
+    return MB2_OK;
+}
+
+int mb2_server_destroy(mb2_server* s) {
+    if (s == nullptr) return MB2_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->pending.clear();
+    }
+    s->cv_work.notify_all();
+    for (auto& w : s->workers) w.join();
+    for (cudaStream_t st : s->streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    delete s;
+    return MB2_OK;
+}
+
+}  // extern "C"

@@ -151,3 +151,31 @@ def config_c2(n: int = 30, depth: int = 40, seed: int = 20260929) -> Circuit:
     """The 30-qubit complex128 workload: brick depth 40, then a full QFT."""
     c = brick(n, depth, seed)
     return qft(n, c)
+
+
+def serving_stream(count: int, rate: float, seed: int, nmin: int = 12, nmax: int = 28, dmin: int = 4,
+                   dmax: int = 40, shots: int = 4096, terms: int = 32):
+    """Requests of the serving workload: Poisson arrivals at `rate` per
+    second; qubits uniform in [nmin, nmax], depth uniform in [dmin, dmax]
+    layers of the U3/CZ brick or the RY/RZ + CX ansatz; each asks for
+    `shots` counts or <H> over `terms` weighted Pauli strings.  Returns a
+    list of dicts (arrival_s, circuit, output, shots, seed, paulis, coefs)."""
+    rng = MT19937_64(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += -math.log(1.0 - rng.uniform()) / rate
+        n = nmin + int(rng.uniform() * (nmax - nmin + 1))
+        depth = dmin + int(rng.uniform() * (dmax - dmin + 1))
+        family = "brick" if rng.uniform() < 0.5 else "hea"
+        cseed = rng.next_word()
+        circ = brick(n, depth, cseed) if family == "brick" else hea(n, depth, cseed)
+        if rng.uniform() < 0.5:
+            out.append({"arrival_s": t, "circuit": circ, "output": "counts", "shots": shots,
+                        "seed": rng.next_word(), "paulis": (), "coefs": (), "family": family})
+        else:
+            ps = pauli_strings(n, terms, rng.next_word())
+            ws = weights(terms, rng.next_word())
+            out.append({"arrival_s": t, "circuit": circ, "output": "expectation", "shots": 0, "seed": 0,
+                        "paulis": ps, "coefs": ws, "family": family})
+    return out
