@@ -517,12 +517,13 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 __global__ void __launch_bounds__(256, 1)
     k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m, uint64_t smask, const TileInstr* __restrict__ prog,
                 uint32_t nprog, const double* __restrict__ sdata, uint32_t nsdata, const double* __restrict__ gdata,
-                uint64_t ntiles, const double* __restrict__ pdata, uint32_t pstride, uint32_t bshift) {
+                uint64_t ntiles, const double* __restrict__ pdata, uint32_t pstride, uint32_t bshift,
+                uint32_t stages) {
     extern __shared__ double2 smem_tiles[];
     const uint32_t tid = threadIdx.x;
     const uint32_t tbits = m - kRegQubits;
     const uint32_t tile_amps = 1u << m;
-    TileInstr* sprog = reinterpret_cast<TileInstr*>(smem_tiles + 2 * tile_amps);
+    TileInstr* sprog = reinterpret_cast<TileInstr*>(smem_tiles + stages * tile_amps);
     double* sd = reinterpret_cast<double*>(sprog + nprog);
     for (uint32_t i = tid; i < nprog * 2; i += blockDim.x)
         reinterpret_cast<ulonglong2*>(sprog)[i] = __ldg(reinterpret_cast<const ulonglong2*>(prog) + i);
@@ -559,17 +560,23 @@ __global__ void __launch_bounds__(256, 1)
         cp_async_commit();
     };
 
-    uint64_t t = blockIdx.x;
-    if (t < ntiles) prefetch(t, smem_tiles);
+    // `stages` tile buffers: the tiles `stages - 1` ahead are in flight
+    // while this one is computed (one commit group per tile, empty groups
+    // past the end keep the count uniform).
+    const uint64_t t0 = blockIdx.x;
+    for (uint32_t sg = 0; sg + 1 < stages; ++sg) {
+        const uint64_t tp = t0 + static_cast<uint64_t>(sg) * gridDim.x;
+        if (tp < ntiles) prefetch(tp, smem_tiles + sg * tile_amps);
+        else cp_async_commit();
+    }
+    uint64_t t = t0;
     for (uint32_t it = 0; t < ntiles; t += gridDim.x, ++it) {
-        double2* tile = smem_tiles + (it & 1u) * tile_amps;
-        const uint64_t tn = t + gridDim.x;
-        if (tn < ntiles) {
-            prefetch(tn, smem_tiles + ((it + 1) & 1u) * tile_amps);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        double2* tile = smem_tiles + (it % stages) * tile_amps;
+        const uint64_t tn = t + static_cast<uint64_t>(stages - 1) * gridDim.x;
+        if (tn < ntiles) prefetch(tn, smem_tiles + ((it + stages - 1) % stages) * tile_amps);
+        else cp_async_commit();
+        if (stages == 3) cp_async_wait<2>();
+        else cp_async_wait<1>();
         __syncthreads();
 
         double2 a[kNA];
@@ -622,18 +629,13 @@ __global__ void __launch_bounds__(256, 1)
                             default: dispatch_g2<TK_GEN>(G.pos(0), G.pos(1), a, md, G.aux()); break;
                         }
                     } else if (G.kind() == TK_DSMALL) {
-                        int sl[2] = {-1, -1};
-                        uint32_t tv[2] = {0u, 0u};
-#pragma unroll
-                        for (int b = 0; b < 2; ++b) {
-                            if (static_cast<uint32_t>(b) >= G.k()) break;
-                            const uint32_t bit = 1u << G.pos(b);
-                            tv[b] = (tb & bit) ? 1u : 0u;
-#pragma unroll
-                            for (int r = 0; r < kR; ++r)
-                                if (bit == rb[r]) sl[b] = r;
-                        }
-                        diag_small(a, md, G.k(), G.aux(), sl[0], sl[1], tv[0], tv[1]);
+                        // Operand sources decided on the host: 0x80 | slot, or a thread bit.
+                        const uint32_t c0 = G.pos(4), c1 = G.pos(5);
+                        const int s0 = (c0 & 0x80u) ? static_cast<int>(c0 & 3u) : -1;
+                        const int s1 = (c1 & 0x80u) ? static_cast<int>(c1 & 3u) : -1;
+                        const uint32_t t0 = (c0 & 0x80u) ? 0u : (tb >> c0) & 1u;
+                        const uint32_t t1 = (c1 & 0x80u) ? 0u : (tb >> c1) & 1u;
+                        diag_small(a, md, G.k(), G.aux(), s0, s1, t0, t1);
                     } else {  // TOP_DIAG, any k: entry index per amplitude
                         const uint32_t k = G.k();
                         uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
@@ -770,14 +772,17 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileIns
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_tile_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(2 * (size_t{1} << kMaxTileQubits) * sizeof(double2) + kMaxStagedBytes));
+                             static_cast<int>(3 * (size_t{1} << kMaxTileQubits) * sizeof(double2) + kMaxStagedBytes));
         attr_set = true;
     }
     if (pass.m > kMaxTileQubits || pass.m < kMinTileQubits) return MB2_ERR_INVALID;
     const size_t staged = size_t{pass.prog_count} * sizeof(TileInstr) + size_t{pass.sdata_count} * sizeof(double);
     if (staged > kMaxStagedBytes) return MB2_ERR_INVALID;
     const uint32_t threads = 1u << (pass.m - kRegQubits);
-    const size_t smem = 2 * (size_t{1} << pass.m) * sizeof(double2) + staged;
+    // 12-qubit tiles: one CTA per SM with three buffers (two tiles in
+    // flight); smaller tiles: two CTAs per SM with two buffers each.
+    const uint32_t stages = pass.m == kMaxTileQubits ? 3u : 2u;
+    const size_t smem = stages * (size_t{1} << pass.m) * sizeof(double2) + staged;
     // A batch adds the bindings above the n qubits: ntiles counts every
     // binding's tiles, and n grows to the bits the binding index occupies.
     uint64_t ntiles = (uint64_t{1} << n) >> pass.m;
@@ -791,7 +796,7 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileIns
     k_tile_pass<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(
         static_cast<double2*>(amps), n_all, pass.m, pass.smask, dev_instrs + pass.prog_begin, pass.prog_count,
         dev_sdata + pass.sdata_begin, pass.sdata_count, dev_gdata, ntiles, batch ? batch->pdata : nullptr,
-        batch ? batch->pstride : 0u, n - pass.m);
+        batch ? batch->pstride : 0u, n - pass.m, stages);
     return status_of(cudaGetLastError());
 }
 

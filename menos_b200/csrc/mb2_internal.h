@@ -96,7 +96,7 @@ struct TilePass {
 };
 
 // Shared-memory budget of one pass's staged instructions + data.
-constexpr size_t kMaxStagedBytes = 48 * 1024;
+constexpr size_t kMaxStagedBytes = 32 * 1024;
 
 // TileInstr.data: for TOP_SMEM an offset into the program's global-only data
 // block (gdata); for every other instruction an offset into its pass's

@@ -206,6 +206,14 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
             open = true;
         };
 
+        // A small diagonal's operand sources, decided here once: pos[4 + b]
+        // = 0x80 | register slot, or the operand's tile bit (a thread bit).
+        auto encode_sources = [&](TileInstr& g, uint32_t k) {
+            for (uint32_t t = 0; t < k; ++t) {
+                const int slot = in_reg(g.pos[t]);
+                g.pos[4 + t] = static_cast<uint8_t>(slot >= 0 ? (0x80u | static_cast<uint32_t>(slot)) : g.pos[t]);
+            }
+        };
         for (size_t j = 0; j < sel.gates.size(); ++j) {
             const Block& b = blocks[sel.gates[j]];
             const uint32_t dim = 1u << b.k;
@@ -223,8 +231,10 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
                     g.nthread = 1;
                     g.data = push_param(sel.gates[j], 2 * dim);
                     g.kind = b.k <= 2 ? TK_DSMALL : TK_GEN;
-                    if (b.k <= 2)
+                    if (b.k <= 2) {
                         for (uint32_t i = 0; i < dim; ++i) g.aux |= 2u << (2 * i);  // every entry multiplies
+                        encode_sources(g, b.k);
+                    }
                     prog.fp64_per_amp += 6;
                     prog.instrs.push_back(g);
                     continue;
@@ -242,6 +252,7 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
                         g.aux |= cls << (2 * i);
                     }
                     prog.fp64_per_amp += (6 * gen + dim - 1) / dim;
+                    encode_sources(g, b.k);
                 } else {
                     g.kind = TK_GEN;
                     prog.fp64_per_amp += 6;
