@@ -15,6 +15,10 @@
  *   - the global phase is part of the state: init writes exp(i*phase)|0..0>;
  *   - Pauli strings use Y = i*X*Z (x/z bit masks, one 64-bit word).
  *
+ * The complex64 precision path (MB2_C64 states) runs the same sweep with FP32
+ * fused multiply-adds on gate matrices composed in FP64; norms, expectations
+ * and sampling probabilities accumulate in FP64.
+ *
  * The plain complex128 path is bitwise identical to the reference's generic
  * CPU kernel (src/kernels/cpu/dense_kernels.cpp:465-524): every output
  * amplitude is (+0) + sum_in m[out][in]*a[in] in increasing `in`, each
@@ -111,7 +115,7 @@ int mb2_apply_matrix_generic(mb2_state* state, const double* matrix, const uint3
 /* Execution options of a program sweep. */
 typedef struct mb2_sweep_options {
     int32_t fuse_gates;      /* 1: the reference's containment fusion (fuse_gates.cpp:190-283) */
-    int32_t fuse_width;      /* >0: the wide fusion pass up to this many qubits (<= 6); 0 = off */
+    int32_t low_qubits;      /* qubits 0..low-1 held in every tile (contiguous runs); -1 = none, 0 = default 3 */
     int32_t tile_qubits;     /* qubits per multi-gate tile pass; 0 = autotuned */
     int32_t per_gate;        /* 1: one launch per block, no tiling (the reference's sweep shape) */
 } mb2_sweep_options;
@@ -183,6 +187,10 @@ int mb2_expectation_noalloc(const void* dev_amps, uint32_t num_qubits, const uin
                             const uint64_t* z_masks, uint32_t num_terms, double* out, void* stream);
 /* sum |a|^2, accumulated in FP64.  Synchronous. */
 int mb2_norm(mb2_state* state, double* out);
+/* Renormalises a complex64 state to unit norm (the norm in FP64, the scale
+ * applied in FP32); reports the norm before.  complex128 states are only
+ * measured, never rescaled (their bits are the reference's).  Synchronous. */
+int mb2_normalize(mb2_state* state, double* norm_before);
 /* Counts by the reference's sort-then-walk sampler (src/engines/dense/sample.cpp:24-75):
  * seed -> mt19937_64 -> (w>>11)*2^-53 uniforms, sorted, walked against the
  * sequential FP64 cumulative sum of |a|^2 (identical counts).  Outcomes are

@@ -20,7 +20,7 @@ C128, C64 = 0, 1
 
 
 class SweepOptions(C.Structure):
-    _fields_ = [("fuse_gates", C.c_int32), ("fuse_width", C.c_int32), ("tile_qubits", C.c_int32),
+    _fields_ = [("fuse_gates", C.c_int32), ("low_qubits", C.c_int32), ("tile_qubits", C.c_int32),
                 ("per_gate", C.c_int32)]
 
 
@@ -105,6 +105,7 @@ SIGNATURES = {
     "mb2_expectation": (C.c_int, [_VP, _VP, _VP, C.c_uint32, _VP]),
     "mb2_expectation_noalloc": (C.c_int, [_VP, C.c_uint32, _VP, _VP, C.c_uint32, _VP, _VP]),
     "mb2_norm": (C.c_int, [_VP, C.POINTER(C.c_double)]),
+    "mb2_normalize": (C.c_int, [_VP, C.POINTER(C.c_double)]),
     "mb2_sample": (C.c_int, [_VP, C.c_uint64, C.c_uint64, _VP, C.c_uint32, _VP, _VP, C.POINTER(C.c_uint64)]),
     "mb2_copy_out": (C.c_int, [_VP, _VP, C.c_uint64]),
     "mb2_copy_in": (C.c_int, [_VP, _VP, C.c_uint64]),

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <random>
@@ -301,7 +302,6 @@ int mb2_apply_matrix_generic(mb2_state* s, const double* matrix, const uint32_t*
 int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
                                 mb2_boundary_fn boundary, void* user) {
     if (s == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
-    if (s->precision != MB2_C128) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "mb2_apply_program: complex128 states only");
     mb2_sweep_options o{1, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     for (uint32_t i = 0; i < num_ops; ++i) {
@@ -319,8 +319,17 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     s->stats = mb2_sweep_stats{};
     s->stats.blocks = blocks.size();
     if (blocks.empty()) return MB2_OK;
-    const uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, s->n, blocks);
-    if (o.per_gate != 0 || s->n < mb2::kMinTileQubits) {
+    const bool c64 = s->precision == MB2_C64;
+    uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, s->n, blocks);
+    if (c64) {
+        // 8-byte amplitudes: 13-qubit tiles fit the same shared memory.
+        m = o.tile_qubits > 0 ? std::min<uint32_t>(static_cast<uint32_t>(o.tile_qubits), mb2::kMaxTileQubitsC64)
+                              : std::min<uint32_t>(mb2::kMaxTileQubitsC64, s->n);
+        for (const mb2::Block& b : blocks) m = std::max(m, b.k);
+        m = std::max(m, mb2::kMinTileQubits);
+        if (s->n < mb2::kMinTileQubits) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "complex64 states need >= 4 qubits");
+    }
+    if (!c64 && (o.per_gate != 0 || s->n < mb2::kMinTileQubits)) {
         for (const mb2::Block& b : blocks) {
             if (int e = apply_block(s, b.m.data(), b.q, b.k, false); e != MB2_OK) return e;
             s->stats.passes += 1;
@@ -333,7 +342,9 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     }
     mb2::TileProgram prog;
     try {
-        prog = mb2::plan_tile_program(blocks, s->n, m);
+        const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
+                                                                         : static_cast<uint32_t>(o.low_qubits));
+        prog = mb2::plan_tile_program(blocks, s->n, m, low);
     } catch (const std::exception& e) {
         return fail(s->ctx, MB2_ERR_INVALID, e.what());
     }
@@ -355,8 +366,10 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     s->stats.fp64_ops_per_amp = prog.fp64_per_amp;
     uint64_t done = 0;
     for (const mb2::TilePass& pass : prog.passes) {
-        const int rc = mb2::launch_tile_pass(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata, s->ctx->sm_count,
-                                             s->stream);
+        const int rc = c64 ? mb2::launch_tile_pass_c64(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata,
+                                                       s->ctx->sm_count, s->stream)
+                           : mb2::launch_tile_pass(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata,
+                                                   s->ctx->sm_count, s->stream);
         if (rc != MB2_OK) return fail(s->ctx, rc, std::string("tile pass launch: ") + mb2::last_cuda_error_string());
         s->stats.passes += 1;
         s->stats.launches += 1;
@@ -415,7 +428,6 @@ int mb2_expectation(mb2_state* s, const uint64_t* x_masks, const uint64_t* z_mas
     if (s == nullptr || (num_terms != 0 && (x_masks == nullptr || z_masks == nullptr || out == nullptr)))
         return MB2_ERR_INVALID;
     if (num_terms == 0) return MB2_OK;
-    if (s->precision != MB2_C128) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "mb2_expectation: complex128 states only");
     const uint64_t lim = (s->n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << s->n) - 1);
     for (uint32_t t = 0; t < num_terms; ++t)
         if ((x_masks[t] | z_masks[t]) & ~lim) return fail(s->ctx, MB2_ERR_INVALID, "Pauli mask beyond the state's qubits");
@@ -432,10 +444,23 @@ int mb2_expectation(mb2_state* s, const uint64_t* x_masks, const uint64_t* z_mas
     const int rc = mb2::launch_expectation(s->amps, s->n, reinterpret_cast<const uint64_t*>(base),
                                            reinterpret_cast<const uint64_t*>(base + off_z), num_terms,
                                            reinterpret_cast<double*>(base + off_p),
-                                           reinterpret_cast<double*>(base + off_o), s->stream);
+                                           reinterpret_cast<double*>(base + off_o), s->stream, s->precision);
     if (rc != MB2_OK) return fail(s->ctx, rc, std::string("expectation launch: ") + mb2::last_cuda_error_string());
     MB2_CUDA(s->ctx, cudaMemcpyAsync(out, base + off_o, out_bytes, cudaMemcpyDeviceToHost, s->stream));
     MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+    return MB2_OK;
+}
+
+int mb2_normalize(mb2_state* s, double* norm_before) {
+    if (s == nullptr) return MB2_ERR_INVALID;
+    double nrm = 0.0;
+    if (int e = mb2_norm(s, &nrm); e != MB2_OK) return e;
+    if (norm_before != nullptr) *norm_before = nrm;
+    if (!(nrm > 0.0)) return fail(s->ctx, MB2_ERR_INVALID, "cannot normalise a zero state");
+    if (s->precision != MB2_C64) return MB2_OK;  // complex128 states are left exactly as computed
+    const double scale = 1.0 / std::sqrt(nrm);
+    const int rc = mb2::launch_scale_c64(s->amps, uint64_t{1} << s->n, static_cast<float>(scale), s->stream);
+    if (rc != MB2_OK) return fail(s->ctx, rc, "normalise launch");
     return MB2_OK;
 }
 
@@ -451,7 +476,6 @@ int mb2_norm(mb2_state* s, double* out) {
 int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targets, uint32_t num_targets,
                uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes) {
     if (s == nullptr || num_outcomes == nullptr) return MB2_ERR_INVALID;
-    if (s->precision != MB2_C128) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "mb2_sample: complex128 states only");
     for (uint32_t t = 0; t < num_targets; ++t)
         if (targets[2 * t] >= s->n || targets[2 * t + 1] >= 64)
             return fail(s->ctx, MB2_ERR_INVALID, "measure target out of range");
@@ -475,7 +499,8 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
     auto* dev_u = reinterpret_cast<double*>(base);
     auto* dev_basis = reinterpret_cast<uint64_t*>(base + al_u);
     MB2_CUDA(s->ctx, cudaMemcpyAsync(dev_u, u.data(), shots * 8, cudaMemcpyHostToDevice, s->stream));
-    const int rc = mb2::launch_sample(s->amps, s->n, dev_u, shots, base + 2 * al_u, dev_basis, s->stream);
+    const int rc =
+        mb2::launch_sample(s->amps, s->n, dev_u, shots, base + 2 * al_u, dev_basis, s->stream, s->precision);
     if (rc != MB2_OK) return fail(s->ctx, rc, std::string("sample launch: ") + mb2::last_cuda_error_string());
     std::vector<uint64_t> basis(shots);
     MB2_CUDA(s->ctx, cudaMemcpyAsync(basis.data(), dev_basis, shots * 8, cudaMemcpyDeviceToHost, s->stream));
@@ -546,7 +571,9 @@ int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
                 order_pass.push_back(i);
             }
         } else {
-            const mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m);
+            const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
+                                                                             : static_cast<uint32_t>(o.low_qubits));
+            const mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m, low);
             order = prog.order;
             order_pass = prog.order_pass;
         }

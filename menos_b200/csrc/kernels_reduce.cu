@@ -49,8 +49,13 @@ __device__ __forceinline__ void block_reduce2(double& re, double& im) {
     }
 }
 
+__device__ __forceinline__ double2 as_d2(double2 a) { return a; }
+__device__ __forceinline__ double2 as_d2(float2 a) { return make_double2(a.x, a.y); }
+
+// A: double2 (complex128 state) or float2 (complex64 state, promoted to FP64).
+template <typename A>
 __global__ void __launch_bounds__(kThreads)
-    k_expectation(const double2* __restrict__ st, uint32_t n, const uint64_t* __restrict__ xs,
+    k_expectation(const A* __restrict__ st, uint32_t n, const uint64_t* __restrict__ xs,
                   const uint64_t* __restrict__ zs, double* __restrict__ partials) {
     const uint32_t term = blockIdx.y;
     const uint64_t x = xs[term], z = zs[term];
@@ -60,7 +65,7 @@ __global__ void __launch_bounds__(kThreads)
     if (x == 0) {
         const uint64_t na = uint64_t{1} << n;
         for (uint64_t m = first; m < na; m += stride) {
-            const double2 a = st[m];
+            const double2 a = as_d2(st[m]);
             const double p = __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
             re = (__popcll(z & m) & 1) ? __dsub_rn(re, p) : __dadd_rn(re, p);
         }
@@ -70,7 +75,7 @@ __global__ void __launch_bounds__(kThreads)
         for (uint64_t c = first; c < np; c += stride) {
             const uint64_t m = insert_zero(c, h);
             const uint64_t m2 = m ^ x;
-            const double2 a = st[m], b = st[m2];
+            const double2 a = as_d2(st[m]), b = as_d2(st[m2]);
             // t = conj(a) * b
             const double tr = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
             const double ti = __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x));
@@ -121,11 +126,15 @@ __global__ void k_expectation_finish(const double* __restrict__ partials, uint32
 }  // namespace
 
 int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
-                       uint32_t num_terms, double* dev_partials, double* dev_out, void* stream) {
+                       uint32_t num_terms, double* dev_partials, double* dev_out, void* stream, int precision) {
     if (num_terms == 0) return MB2_OK;
     const auto s = static_cast<cudaStream_t>(stream);
     const dim3 grid(kExpBlocks, num_terms);
-    k_expectation<<<grid, kThreads, 0, s>>>(static_cast<const double2*>(amps), n, dev_x, dev_z, dev_partials);
+    if (precision == MB2_C64)
+        k_expectation<float2><<<grid, kThreads, 0, s>>>(static_cast<const float2*>(amps), n, dev_x, dev_z, dev_partials);
+    else
+        k_expectation<double2><<<grid, kThreads, 0, s>>>(static_cast<const double2*>(amps), n, dev_x, dev_z,
+                                                         dev_partials);
     k_expectation_finish<<<(num_terms + 127) / 128, 128, 0, s>>>(dev_partials, kExpBlocks, dev_x, dev_z, num_terms,
                                                                   dev_out);
     return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;

@@ -36,9 +36,15 @@ constexpr int kThreads = 256;
 constexpr int kPerThread = kSampleChunk / kThreads;  // 16
 
 __device__ __forceinline__ double prob(double2 a) { return __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y)); }
+// A complex64 amplitude's probability in FP64 (the squares of FP32 values are exact).
+__device__ __forceinline__ double prob(float2 a) {
+    return __dadd_rn(__dmul_rn(static_cast<double>(a.x), static_cast<double>(a.x)),
+                     __dmul_rn(static_cast<double>(a.y), static_cast<double>(a.y)));
+}
 
 // Step A: approximate chunk sums (any order; only used to guess binades).
-__global__ void __launch_bounds__(kThreads) k_chunk_sums(const double2* __restrict__ st, uint64_t n_amps,
+template <typename A>
+__global__ void __launch_bounds__(kThreads) k_chunk_sums(const A* __restrict__ st, uint64_t n_amps,
                                                          uint32_t chunk, double* __restrict__ sums) {
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * chunk;
     double s = 0.0;
@@ -135,7 +141,8 @@ struct ChunkMap {
     int valid;  // 0: walk sequentially
 };
 
-__global__ void __launch_bounds__(kThreads) k_chunk_maps(const double2* __restrict__ st, uint64_t n_amps,
+template <typename A>
+__global__ void __launch_bounds__(kThreads) k_chunk_maps(const A* __restrict__ st, uint64_t n_amps,
                                                          uint32_t chunk, const double* __restrict__ starts,
                                                          const double* __restrict__ sums,
                                                          ChunkMap* __restrict__ maps) {
@@ -291,7 +298,8 @@ __device__ __forceinline__ bool advance_exact(double& c, int e, long long inc0, 
     return true;
 }
 
-__global__ void __launch_bounds__(32) k_seg_chain(const double2* __restrict__ st, uint64_t n_amps, uint32_t chunk,
+template <typename A>
+__global__ void __launch_bounds__(32) k_seg_chain(const A* __restrict__ st, uint64_t n_amps, uint32_t chunk,
                                                   uint64_t nchunks, const ChunkMap* __restrict__ maps,
                                                   const SMap* __restrict__ seg_total, double* __restrict__ cstart,
                                                   unsigned char* __restrict__ seq, unsigned char* __restrict__ direct,
@@ -367,7 +375,8 @@ __device__ __forceinline__ uint64_t count_below(const double* __restrict__ u, ui
 
 // Step E: per chunk, the exact running sums of its elements, then each of
 // its shots placed on the first element whose sum exceeds the uniform.
-__global__ void __launch_bounds__(kThreads) k_assign(const double2* __restrict__ st, uint64_t n_amps,
+template <typename A>
+__global__ void __launch_bounds__(kThreads) k_assign(const A* __restrict__ st, uint64_t n_amps,
                                                      uint32_t chunk, const ChunkMap* __restrict__ maps,
                                                      const double* __restrict__ cstart,
                                                      const unsigned char* __restrict__ seq,
@@ -469,10 +478,11 @@ size_t sample_scratch_bytes(uint32_t n, uint64_t shots) {
            2 * al(nchunks * sizeof(SMap)) + al(nchunks) + al(nchunks * 8);
 }
 
-int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
-                  uint64_t* dev_basis, void* stream) {
+template <typename A>
+int launch_sample_t(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
+                    uint64_t* dev_basis, void* stream) {
     const auto s = static_cast<cudaStream_t>(stream);
-    const auto* st = static_cast<const double2*>(amps);
+    const auto* st = static_cast<const A*>(amps);
     const uint64_t na = uint64_t{1} << n;
     const uint32_t chunk = static_cast<uint32_t>(na < kSampleChunk ? na : kSampleChunk);
     const uint64_t nchunks = na / chunk;
@@ -508,6 +518,13 @@ int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorte
                                                                  dev_uniforms_sorted, shots, dev_basis);
     k_leftover<<<1, 256, 0, s>>>(cst, nchunks, dev_uniforms_sorted, shots, na - 1, dev_basis);
     return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+}
+
+int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
+                  uint64_t* dev_basis, void* stream, int precision) {
+    return precision == MB2_C64
+               ? launch_sample_t<float2>(amps, n, dev_uniforms_sorted, shots, scratch, dev_basis, stream)
+               : launch_sample_t<double2>(amps, n, dev_uniforms_sorted, shots, scratch, dev_basis, stream);
 }
 
 }  // namespace mb2

@@ -157,7 +157,8 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileIns
 // device pointers.
 constexpr uint32_t kExpBlocks = 512;
 int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
-                       uint32_t num_terms, double* dev_partials, double* dev_out, void* stream);
+                       uint32_t num_terms, double* dev_partials, double* dev_out, void* stream,
+                       int precision = MB2_C128);
 // Batched sweep (batch.cpp, kernels_batch.cu).
 constexpr uint32_t kMaxBatchTerms = MB2_BATCH_MAX_TERMS;
 
@@ -168,7 +169,12 @@ constexpr uint32_t kMaxBatchTerms = MB2_BATCH_MAX_TERMS;
 constexpr uint32_t kSampleChunk = 4096;
 size_t sample_scratch_bytes(uint32_t n, uint64_t shots);
 int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
-                  uint64_t* dev_basis, void* stream);
+                  uint64_t* dev_basis, void* stream, int precision = MB2_C128);
+// complex64 precision path (kernels_c64.cu).
+constexpr uint32_t kMaxTileQubitsC64 = 13;
+int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
+                         const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream);
+int launch_scale_c64(void* amps, uint64_t n_amps, float s, void* stream);
 int context_device(const mb2_context* ctx);
 // A complex128 state on a caller-owned stream (engine.cpp).
 int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, void* stream, mb2_state** out);

@@ -135,7 +135,7 @@ uint32_t push_matrix(std::vector<double>& data, const std::vector<Cd>& m) {
 
 TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint32_t m, uint32_t fixed_low,
                               const std::vector<uint8_t>* parametric) {
-    if (m < kMinTileQubits || m > kMaxTileQubits) throw std::invalid_argument("tile width out of range");
+    if (m < kMinTileQubits || m > kMaxTileQubitsC64) throw std::invalid_argument("tile width out of range");
     TileProgram prog;
     const uint32_t mt = std::min(m, n);
     if (mt < kRegQubits) throw std::invalid_argument("state too small for the tile kernel");

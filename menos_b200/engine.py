@@ -96,9 +96,9 @@ class DeviceState:
         self._chk(f(self.h, m.ctypes.data, q.ctypes.data, len(q)), "mb2_apply_matrix")
 
     def apply_program(self, circ: Circuit, fuse_gates: bool = True, tile_qubits: int = 0,
-                      per_gate: bool = False) -> SweepStats:
+                      per_gate: bool = False, low_qubits: int = 0) -> SweepStats:
         arr, keep = to_mb2_ops(circ)
-        opts = SweepOptions(1 if fuse_gates else 0, 0, tile_qubits, 1 if per_gate else 0)
+        opts = SweepOptions(1 if fuse_gates else 0, low_qubits, tile_qubits, 1 if per_gate else 0)
         self._chk(lib().mb2_apply_program(self.h, arr, len(circ.ops), C.byref(opts)), "mb2_apply_program")
         del keep
         return self.stats()
@@ -118,6 +118,12 @@ class DeviceState:
         self._chk(lib().mb2_expectation(self.h, xs.ctypes.data, zs.ctypes.data, len(paulis), out.ctypes.data),
                   "mb2_expectation")
         return out.view(np.complex128).copy()
+
+    def normalize(self) -> float:
+        """complex64: rescale to unit norm (returns the norm before)."""
+        v = C.c_double()
+        self._chk(lib().mb2_normalize(self.h, C.byref(v)), "mb2_normalize")
+        return v.value
 
     def norm(self) -> float:
         v = C.c_double()
