@@ -271,7 +271,7 @@ def main():
                                f"fusion=containment, norm + {args.terms} Paulis + {args.shots} shots",
                    "qubits": n, "parallelism": f"replicas x{world}", "l2": "state 16 GiB >> L2 (no flush)",
                    "passes": passes, "blocks": int(stats.blocks), "sweep_ms": round(sweep_avg, 2),
-                   "tile_qubits": args.tile or 12},
+                   "tile_qubits": args.tile or 11},
         "roofline": {"bound": "hbm", "kernel": "k_tile_pass", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
                      "peak_source": peak_src,

@@ -118,6 +118,7 @@ typedef struct mb2_sweep_options {
     int32_t low_qubits;      /* qubits 0..low-1 held in every tile (contiguous runs); -1 = none, 0 = default 3 */
     int32_t tile_qubits;     /* qubits per multi-gate tile pass; 0 = autotuned */
     int32_t per_gate;        /* 1: one launch per block, no tiling (the reference's sweep shape) */
+    int32_t ctas_per_sm;     /* complex128 tiles below 12 qubits: resident CTAs per SM (2 or 3); 0 = 2 */
 } mb2_sweep_options;
 
 /* Applies a whole operation list (MeasureOps skipped) as a sequence of
@@ -303,6 +304,11 @@ int mb2_server_destroy(mb2_server* server);
  * CudaCalibration (src/plan/cuda_calibration.h:9-48). */
 int mb2_probe_rates(mb2_context* ctx, double* fp64_ops_per_s, double* copy_gbs);
 
+/* Kernels this library has launched since it was loaded, over all contexts
+ * and states (probes excluded).  Read before and after a region to count its
+ * device launches.  Has no counterpart in the reference. */
+int mb2_kernel_launches(uint64_t* out);
+
 /* ---- host-side reference pieces (no device work) ----------------------- */
 /* Gate matrix, bitwise ir::generate_matrix (src/ir/gate_table.cpp:260).
  * out: 2*4^k doubles; returns MB2_ERR_INVALID for UNITARY/MEASURE. */
@@ -319,6 +325,18 @@ int mb2_gate_matrix(int32_t opcode, const double* params, double* out, uint32_t 
 int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
                        uint32_t num_qubits, uint32_t* pass, uint32_t* k, uint32_t* qubits,
                        double* matrices, uint64_t* num_blocks, uint64_t* matrix_len);
+
+/* The grouping mb2_expectation uses for these terms on a num_qubits state,
+ * as 64-bit words: the group count, then per group c, d, free_mask, nterms,
+ * the 2^d span vectors (X-mask bits above c, span[k] = XOR of the basis
+ * vectors selected by k), and per term its index, kx (coordinates of its
+ * X mask above c) and xl (its low c X bits).  A group's tiles are the cosets
+ * of the span: chunk k of the tile at coset index i holds amplitudes
+ * ((deposit(i, free_mask) ^ span[k]) << c) | low, low < 2^c.  *out_words in:
+ * capacity, out: words needed.  Lets tests check on the CPU that every
+ * amplitude pair is visited once.  Has no counterpart in the reference. */
+int mb2_debug_pauli_groups(const uint64_t* x_masks, const uint64_t* z_masks, uint32_t num_terms,
+                           uint32_t num_qubits, uint64_t* out, uint64_t* out_words);
 
 #ifdef __cplusplus
 }

@@ -21,7 +21,7 @@ C128, C64 = 0, 1
 
 class SweepOptions(C.Structure):
     _fields_ = [("fuse_gates", C.c_int32), ("low_qubits", C.c_int32), ("tile_qubits", C.c_int32),
-                ("per_gate", C.c_int32)]
+                ("per_gate", C.c_int32), ("ctas_per_sm", C.c_int32)]
 
 
 class SweepEstimate(C.Structure):
@@ -89,6 +89,8 @@ SIGNATURES = {
                                    C.POINTER(C.c_uint64)]),
     "mb2_server_destroy": (C.c_int, [_VP]),
     "mb2_probe_rates": (C.c_int, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "mb2_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),
+    "mb2_debug_pauli_groups": (C.c_int, [_VP, _VP, C.c_uint32, C.c_uint32, _VP, C.POINTER(C.c_uint64)]),
     "mb2_state_alloc": (C.c_int, [_VP, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(_VP)]),
     "mb2_state_free": (C.c_int, [_VP]),
     "mb2_init": (C.c_int, [_VP, C.c_double]),

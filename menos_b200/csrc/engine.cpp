@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -125,7 +126,9 @@ int apply_block(mb2_state* s, const mb2::Cd* m, const uint32_t* q, uint32_t k, b
     return MB2_OK;
 }
 
-uint32_t default_tile_qubits(uint32_t n) { return std::min<uint32_t>(12, n); }
+// 11-qubit tiles: two (or three) CTAs per SM with double buffering stream
+// better than one 12-qubit CTA per SM, and that outweighs the extra passes.
+uint32_t default_tile_qubits(uint32_t n) { return std::min<uint32_t>(11, n); }
 
 // The tile width a sweep runs at: the requested (or default) width, raised
 // to hold the widest block, within the kernel's limits.
@@ -163,6 +166,13 @@ int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes
     *out = s;
     return MB2_OK;
 }
+}  // namespace mb2
+
+namespace mb2 {
+namespace {
+std::atomic<uint64_t> g_kernel_launches{0};
+}
+void note_launches(uint32_t k) { g_kernel_launches.fetch_add(k, std::memory_order_relaxed); }
 }  // namespace mb2
 
 extern "C" {
@@ -215,6 +225,12 @@ int mb2_device_info(mb2_context* ctx, int* sm_count, uint64_t* total_bytes, uint
     if (sm_count) *sm_count = ctx->sm_count;
     if (total_bytes) *total_bytes = tot;
     if (free_bytes) *free_bytes = fr;
+    return MB2_OK;
+}
+
+int mb2_kernel_launches(uint64_t* out) {
+    if (out == nullptr) return MB2_ERR_INVALID;
+    *out = mb2::g_kernel_launches.load(std::memory_order_relaxed);
     return MB2_OK;
 }
 
@@ -302,7 +318,7 @@ int mb2_apply_matrix_generic(mb2_state* s, const double* matrix, const uint32_t*
 int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
                                 mb2_boundary_fn boundary, void* user) {
     if (s == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     for (uint32_t i = 0; i < num_ops; ++i) {
         if (ops[i].opcode == MB2_MEASURE) continue;
@@ -369,7 +385,8 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
         const int rc = c64 ? mb2::launch_tile_pass_c64(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata,
                                                        s->ctx->sm_count, s->stream)
                            : mb2::launch_tile_pass(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata,
-                                                   s->ctx->sm_count, s->stream);
+                                                   s->ctx->sm_count, s->stream, nullptr,
+                                                   o.ctas_per_sm > 0 ? static_cast<uint32_t>(o.ctas_per_sm) : 0u);
         if (rc != MB2_OK) return fail(s->ctx, rc, std::string("tile pass launch: ") + mb2::last_cuda_error_string());
         s->stats.passes += 1;
         s->stats.launches += 1;
@@ -389,7 +406,7 @@ int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const m
 int mb2_estimate_sweep(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
                        mb2_sweep_estimate* out) {
     if (out == nullptr || (ops == nullptr && num_ops != 0) || num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     *out = mb2_sweep_estimate{};
     try {
@@ -431,20 +448,39 @@ int mb2_expectation(mb2_state* s, const uint64_t* x_masks, const uint64_t* z_mas
     const uint64_t lim = (s->n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << s->n) - 1);
     for (uint32_t t = 0; t < num_terms; ++t)
         if ((x_masks[t] | z_masks[t]) & ~lim) return fail(s->ctx, MB2_ERR_INVALID, "Pauli mask beyond the state's qubits");
+    // Terms are grouped so that each group reads the state once (one launch
+    // per group); the fixed-order finish then adds every term's partials.
+    const mb2::PauliPlan plan = mb2::plan_pauli_groups(x_masks, z_masks, num_terms, s->n);
     const size_t mask_bytes = size_t{num_terms} * 8;
     const size_t part_bytes = size_t{num_terms} * mb2::kExpBlocks * 16;
     const size_t out_bytes = size_t{num_terms} * 16;
-    const size_t off_z = (mask_bytes + 255) & ~size_t{255};
-    const size_t off_p = off_z + ((mask_bytes + 255) & ~size_t{255});
+    const size_t span_bytes = plan.spans.size() * 8;
+    const size_t term_bytes = plan.terms.size() * sizeof(mb2::PauliGroupTerm);
+    auto up = [](size_t v) { return (v + 255) & ~size_t{255}; };
+    const size_t off_z = up(mask_bytes);
+    const size_t off_p = off_z + up(mask_bytes);
     const size_t off_o = off_p + part_bytes;
-    if (int e = ensure_scratch(s, off_o + out_bytes); e != MB2_OK) return e;
+    const size_t off_s = up(off_o + out_bytes);
+    const size_t off_t = off_s + up(span_bytes);
+    if (int e = ensure_scratch(s, off_t + term_bytes); e != MB2_OK) return e;
     auto* base = static_cast<unsigned char*>(s->scratch);
+    std::vector<unsigned char> host(off_t + term_bytes - off_s);
+    std::memcpy(host.data(), plan.spans.data(), span_bytes);
+    std::memcpy(host.data() + (off_t - off_s), plan.terms.data(), term_bytes);
     MB2_CUDA(s->ctx, cudaMemcpyAsync(base, x_masks, mask_bytes, cudaMemcpyHostToDevice, s->stream));
     MB2_CUDA(s->ctx, cudaMemcpyAsync(base + off_z, z_masks, mask_bytes, cudaMemcpyHostToDevice, s->stream));
-    const int rc = mb2::launch_expectation(s->amps, s->n, reinterpret_cast<const uint64_t*>(base),
-                                           reinterpret_cast<const uint64_t*>(base + off_z), num_terms,
-                                           reinterpret_cast<double*>(base + off_p),
-                                           reinterpret_cast<double*>(base + off_o), s->stream, s->precision);
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(base + off_s, host.data(), host.size(), cudaMemcpyHostToDevice, s->stream));
+    auto* partials = reinterpret_cast<double*>(base + off_p);
+    for (const mb2::PauliGroupPlan& g : plan.groups) {
+        const int rc = mb2::launch_pauli_group(
+            s->amps, s->n, g.c, g.d, reinterpret_cast<const uint64_t*>(base + off_s) + g.span_off, g.free_mask,
+            base + off_t + size_t{g.term_off} * sizeof(mb2::PauliGroupTerm), g.nterms, partials, mb2::kExpBlocks,
+            s->stream, s->precision);
+        if (rc != MB2_OK) return fail(s->ctx, rc, std::string("expectation launch: ") + mb2::last_cuda_error_string());
+    }
+    const int rc = mb2::launch_expectation_finish(partials, mb2::kExpBlocks, reinterpret_cast<const uint64_t*>(base),
+                                                  reinterpret_cast<const uint64_t*>(base + off_z), num_terms,
+                                                  reinterpret_cast<double*>(base + off_o), s->stream);
     if (rc != MB2_OK) return fail(s->ctx, rc, std::string("expectation launch: ") + mb2::last_cuda_error_string());
     MB2_CUDA(s->ctx, cudaMemcpyAsync(out, base + off_o, out_bytes, cudaMemcpyDeviceToHost, s->stream));
     MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
@@ -558,7 +594,7 @@ int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
                        uint64_t* matrix_len) {
     if (num_blocks == nullptr || matrix_len == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
     if (num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     std::vector<mb2::Block> blocks;
     std::vector<uint32_t> order, order_pass;

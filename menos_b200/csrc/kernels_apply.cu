@@ -514,7 +514,8 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // the current one is computed, so HBM traffic overlaps the FP64 work.  The
 // pass's instructions and small-matrix data are staged in shared memory once
 // per CTA.
-__global__ void __launch_bounds__(256, 1)
+template <int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
     k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m, uint64_t smask, const TileInstr* __restrict__ prog,
                 uint32_t nprog, const double* __restrict__ sdata, uint32_t nsdata, const double* __restrict__ gdata,
                 uint64_t ntiles, const double* __restrict__ pdata, uint32_t pstride, uint32_t bshift,
@@ -598,10 +599,12 @@ __global__ void __launch_bounds__(256, 1)
                 for (int j = 1; j < kNA; ++j) adr[j] = adr[j & (j - 1)] ^ swz(rb[lowbit_index(j)]);
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) a[j] = tile[adr[j]];
-                for (;;) {
-                    const DI G = load_instr(sprog + pc);
-                    ++pc;
-                    if (G.op() == TOP_END) break;
+                // The next instruction is read while this one executes (every
+                // group ends with TOP_END, so the read stays in the program).
+                DI G = load_instr(sprog + pc);
+                ++pc;
+                for (; G.op() != TOP_END; ++pc) {
+                    const DI Gn = load_instr(sprog + pc);
                     // Parametric blocks (a batched sweep) read the matrix of
                     // this tile's binding: binding = tile >> bshift.
                     const double* md = G.nthread() ? pdata + (t >> bshift) * pstride + G.data() : sd + G.data();
@@ -654,6 +657,7 @@ __global__ void __launch_bounds__(256, 1)
                             a[j] = scale_entry(md[2 * e], md[2 * e + 1], a[j]);
                         }
                     }
+                    G = Gn;
                 }
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) tile[adr[j]] = a[j];
@@ -713,6 +717,7 @@ int launch_init(void* amps, uint64_t n_amps, int precision, double re, double im
                                                         static_cast<float>(im));
     else
         k_init_c128<<<grid_for(n_amps, 256), 256, 0, s>>>(static_cast<double2*>(amps), n_amps, re, im);
+    note_launches(1);
     return status_of(cudaGetLastError());
 }
 
@@ -722,6 +727,7 @@ int launch_apply_1q(void* amps, uint32_t n, uint32_t q, const double* m8, void* 
     const uint64_t npairs = (uint64_t{1} << n) >> 1;
     k_apply_1q<<<grid_for(npairs, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<double2*>(amps),
                                                                                     npairs, q, m);
+    note_launches(1);
     return status_of(cudaGetLastError());
 }
 
@@ -731,6 +737,7 @@ int launch_apply_2q(void* amps, uint32_t n, uint32_t q0, uint32_t q1, const doub
     const uint64_t ng = (uint64_t{1} << n) >> 2;
     k_apply_2q<<<grid_for(ng, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<double2*>(amps), ng, q0,
                                                                                 q1, m);
+    note_launches(1);
     return status_of(cudaGetLastError());
 }
 
@@ -743,6 +750,7 @@ int launch_apply_diag(void* amps, uint32_t n, const uint32_t* q, uint32_t k, con
     const uint64_t na = uint64_t{1} << n;
     k_apply_diag<<<grid_for(na, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<double2*>(amps), na, k, qq[0], qq[1], qq[2], qq[3], qq[4], qq[5], d);
+    note_launches(1);
     return status_of(cudaGetLastError());
 }
 
@@ -763,16 +771,19 @@ int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, 
     k_apply_generic<<<grid, 256, smem, static_cast<cudaStream_t>(stream)>>>(
         static_cast<double2*>(amps), n, k, qq[0], qq[1], qq[2], qq[3], qq[4], qq[5],
         reinterpret_cast<const double2*>(dev_matrix));
+    note_launches(1);
     return status_of(cudaGetLastError());
 }
 
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
                      const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
-                     const BatchLayout* batch) {
+                     const BatchLayout* batch, uint32_t ctas_per_sm) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_tile_pass, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(3 * (size_t{1} << kMaxTileQubits) * sizeof(double2) + kMaxStagedBytes));
+        const int most = static_cast<int>(3 * (size_t{1} << kMaxTileQubits) * sizeof(double2) + kMaxStagedBytes);
+        cudaFuncSetAttribute(k_tile_pass<256, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        cudaFuncSetAttribute(k_tile_pass<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        cudaFuncSetAttribute(k_tile_pass<128, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         attr_set = true;
     }
     if (pass.m > kMaxTileQubits || pass.m < kMinTileQubits) return MB2_ERR_INVALID;
@@ -780,9 +791,21 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileIns
     if (staged > kMaxStagedBytes) return MB2_ERR_INVALID;
     const uint32_t threads = 1u << (pass.m - kRegQubits);
     // 12-qubit tiles: one CTA per SM with three buffers (two tiles in
-    // flight); smaller tiles: two CTAs per SM with two buffers each.
+    // flight); smaller tiles: two buffers per CTA and two CTAs per SM, or
+    // three (168 registers a thread) when ctas_per_sm asks for it and the
+    // shared memory allows.
     const uint32_t stages = pass.m == kMaxTileQubits ? 3u : 2u;
     const size_t smem = stages * (size_t{1} << pass.m) * sizeof(double2) + staged;
+    auto kern = pass.m == kMaxTileQubits ? k_tile_pass<256, 1> : k_tile_pass<128, 2>;
+    uint32_t per_sm = pass.m == kMaxTileQubits ? 1u : 2u;
+    if (pass.m < kMaxTileQubits && ctas_per_sm >= 3) {
+        int resident = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_tile_pass<128, 3>, static_cast<int>(threads), smem);
+        if (resident >= 3) {
+            kern = k_tile_pass<128, 3>;
+            per_sm = 3;
+        }
+    }
     // A batch adds the bindings above the n qubits: ntiles counts every
     // binding's tiles, and n grows to the bits the binding index occupies.
     uint64_t ntiles = (uint64_t{1} << n) >> pass.m;
@@ -791,12 +814,13 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileIns
         ntiles *= batch->bindings;
         while ((uint64_t{1} << (n_all - n)) < batch->bindings) ++n_all;
     }
-    const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m <= 11 ? 2u : 1u);
+    const uint64_t cap = static_cast<uint64_t>(sm_count) * per_sm;
     const int grid = static_cast<int>(ntiles < cap ? ntiles : cap);
-    k_tile_pass<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(
+    kern<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(
         static_cast<double2*>(amps), n_all, pass.m, pass.smask, dev_instrs + pass.prog_begin, pass.prog_count,
         dev_sdata + pass.sdata_begin, pass.sdata_count, dev_gdata, ntiles, batch ? batch->pdata : nullptr,
         batch ? batch->pstride : 0u, n - pass.m, stages);
+    note_launches(1);
     return status_of(cudaGetLastError());
 }
 

@@ -123,7 +123,150 @@ __global__ void k_expectation_finish(const double* __restrict__ partials, uint32
     out[2 * t + 1] = oi;
 }
 
+// ---- grouped terms: one state read per group --------------------------------
+// A group's terms have high X parts (bits >= c) inside a subspace V of
+// dimension d.  A tile is a coset of V: 2^d chunks of 2^c contiguous
+// amplitudes (chunk k's high bits are rep ^ span[k]), so for every term the
+// partner m ^ x of each amplitude m is in the same tile: chunk k ^ kx, low
+// bits low ^ xl.  Each pair is visited once.  Partial sums go to fixed slots
+// (CTA, term) and are added in CTA order by the finish kernel.
+using GroupTerm = PauliGroupTerm;
+
+template <typename A>
+__global__ void __launch_bounds__(kThreads)
+    k_pauli_group(const A* __restrict__ st, uint32_t c, uint32_t d, const uint64_t* __restrict__ span,
+                  uint64_t free_mask, const GroupTerm* __restrict__ terms, uint32_t nterms, uint64_t ncosets,
+                  double* __restrict__ partials) {
+    extern __shared__ double2 gtile[];
+    __shared__ uint64_t sspan[1u << kPauliMaxSpan];
+    __shared__ GroupTerm sterm[kMaxGroupTerms];
+    __shared__ double red[2 * (kThreads / 32)];
+    const uint32_t tile_amps = 1u << (c + d);
+    const uint32_t lowmask = (1u << c) - 1;
+    for (uint32_t i = threadIdx.x; i < (1u << d); i += kThreads) sspan[i] = span[i];
+    for (uint32_t i = threadIdx.x; i < nterms; i += kThreads) sterm[i] = terms[i];
+    double re[kMaxGroupTerms], im[kMaxGroupTerms];
+#pragma unroll
+    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
+        re[t] = 0.0;
+        im[t] = 0.0;
+    }
+    for (uint64_t cs = blockIdx.x; cs < ncosets; cs += gridDim.x) {
+        // Coset representative: the bits of cs deposited on the free
+        // (non-pivot) high bits; the pivots stay zero.
+        uint64_t rep = 0;
+        {
+            uint64_t v = cs, mask = free_mask;
+            while (mask != 0) {
+                const uint64_t low = mask & (~mask + 1);
+                if (v & 1) rep |= low;
+                v >>= 1;
+                mask ^= low;
+            }
+        }
+        __syncthreads();  // the previous coset's reads are done (and the staging above)
+        for (uint32_t L = threadIdx.x; L < tile_amps; L += kThreads) {
+            const uint64_t m = ((rep ^ sspan[L >> c]) << c) | (L & lowmask);
+            gtile[L] = as_d2(st[m]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
+            if (t < nterms) {
+                const uint64_t z = sterm[t].z;
+                const uint32_t dl = (sterm[t].kx << c) | sterm[t].xl;  // tile-local XOR of the pair
+                if (dl == 0) {                                          // x = 0: a Z string
+                    for (uint32_t L = threadIdx.x; L < tile_amps; L += kThreads) {
+                        const uint64_t m = ((rep ^ sspan[L >> c]) << c) | (L & lowmask);
+                        const double2 a = gtile[L];
+                        const double p = __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
+                        re[t] = (__popcll(z & m) & 1) ? __dsub_rn(re[t], p) : __dadd_rn(re[t], p);
+                    }
+                } else {
+                    const uint32_t hb = 31 - __clz(dl);
+                    const uint32_t below = (1u << hb) - 1;
+                    for (uint32_t q = threadIdx.x; q < tile_amps / 2; q += kThreads) {
+                        const uint32_t L = ((q & ~below) << 1) | (q & below);
+                        const uint32_t L2 = L ^ dl;
+                        const uint64_t m = ((rep ^ sspan[L >> c]) << c) | (L & lowmask);
+                        const uint64_t m2 = ((rep ^ sspan[L2 >> c]) << c) | (L2 & lowmask);
+                        const double2 a = gtile[L], b = gtile[L2];
+                        const double tr = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
+                        const double ti = __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x));
+                        const bool neg2 = __popcll(z & m2) & 1;
+                        const bool neg1 = __popcll(z & m) & 1;
+                        re[t] = neg2 ? __dsub_rn(re[t], tr) : __dadd_rn(re[t], tr);
+                        im[t] = neg2 ? __dsub_rn(im[t], ti) : __dadd_rn(im[t], ti);
+                        re[t] = neg1 ? __dsub_rn(re[t], tr) : __dadd_rn(re[t], tr);
+                        im[t] = neg1 ? __dadd_rn(im[t], ti) : __dsub_rn(im[t], ti);
+                    }
+                }
+            }
+        }
+    }
+    // Per term: this CTA's sum in a fixed order (lanes, then warps).
+#pragma unroll
+    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
+        if (t < nterms) {
+            double r = re[t], i = im[t];
+            for (int o = 16; o > 0; o >>= 1) {
+                r += __shfl_down_sync(0xffffffffu, r, o);
+                i += __shfl_down_sync(0xffffffffu, i, o);
+            }
+            __syncthreads();
+            if ((threadIdx.x & 31) == 0) {
+                red[2 * (threadIdx.x >> 5)] = r;
+                red[2 * (threadIdx.x >> 5) + 1] = i;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double sr = 0.0, si = 0.0;
+                for (int w = 0; w < kThreads / 32; ++w) {
+                    sr += red[2 * w];
+                    si += red[2 * w + 1];
+                }
+                double* p = partials + 2 * (static_cast<uint64_t>(sterm[t].out) * gridDim.x + blockIdx.x);
+                p[0] = sr;
+                p[1] = si;
+            }
+        }
+    }
+}
+
 }  // namespace
+
+int launch_pauli_group(const void* amps, uint32_t n, uint32_t c, uint32_t d, const uint64_t* dev_span,
+                       uint64_t free_mask, const void* dev_terms, uint32_t nterms, double* dev_partials,
+                       uint32_t grid, void* stream, int precision) {
+    if (nterms == 0) return MB2_OK;
+    if (nterms > kMaxGroupTerms || c + d > kPauliTileQubits || d > kPauliMaxSpan) return MB2_ERR_INVALID;
+    const auto s = static_cast<cudaStream_t>(stream);
+    const uint64_t ncosets = uint64_t{1} << (n - c - d);
+    const size_t smem = (size_t{1} << (c + d)) * sizeof(double2);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_pauli_group<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        cudaFuncSetAttribute(k_pauli_group<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        attr = true;
+    }
+    const auto* terms = static_cast<const GroupTerm*>(dev_terms);
+    if (precision == MB2_C64)
+        k_pauli_group<float2><<<grid, kThreads, smem, s>>>(static_cast<const float2*>(amps), c, d, dev_span,
+                                                           free_mask, terms, nterms, ncosets, dev_partials);
+    else
+        k_pauli_group<double2><<<grid, kThreads, smem, s>>>(static_cast<const double2*>(amps), c, d, dev_span,
+                                                            free_mask, terms, nterms, ncosets, dev_partials);
+    note_launches(1);
+    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+}
+
+int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const uint64_t* dev_x,
+                              const uint64_t* dev_z, uint32_t num_terms, double* dev_out, void* stream) {
+    k_expectation_finish<<<(num_terms + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        dev_partials, blocks, dev_x, dev_z, num_terms, dev_out);
+    note_launches(1);
+    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+}
 
 int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
                        uint32_t num_terms, double* dev_partials, double* dev_out, void* stream, int precision) {
@@ -137,6 +280,7 @@ int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, cons
                                                          dev_partials);
     k_expectation_finish<<<(num_terms + 127) / 128, 128, 0, s>>>(dev_partials, kExpBlocks, dev_x, dev_z, num_terms,
                                                                   dev_out);
+    note_launches(2);
     return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
 }
 

@@ -522,6 +522,7 @@ int launch_sample_t(const void* amps, uint32_t n, const double* dev_uniforms_sor
 
 int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
                   uint64_t* dev_basis, void* stream, int precision) {
+    note_launches(8);
     return precision == MB2_C64
                ? launch_sample_t<float2>(amps, n, dev_uniforms_sorted, shots, scratch, dev_basis, stream)
                : launch_sample_t<double2>(amps, n, dev_uniforms_sorted, shots, scratch, dev_basis, stream);

@@ -151,7 +151,7 @@ struct BatchLayout {
 };
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
                      const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
-                     const BatchLayout* batch = nullptr);
+                     const BatchLayout* batch = nullptr, uint32_t ctas_per_sm = 0);
 // Expectation of num_terms Pauli terms: partials (num_terms * kExpBlocks * 2
 // doubles) then the fixed-order finish into out (num_terms * 2 doubles), all
 // device pointers.
@@ -182,6 +182,38 @@ int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes
 // Calibration probes (kernels_probe.cu): FP64 instructions per second and
 // device-to-device copy GB/s (read + write bytes), on the current device.
 int probe_rates(int sm_count, double* fp64_per_s, double* copy_gbs);
+// Grouped Pauli terms (pauli_groups.cpp plans, kernels_reduce.cu reduces):
+// terms whose X masks above the low c bits span a subspace of dimension d
+// share one read of the state, in tiles of 2^(c+d) <= 2^12 amplitudes.
+// Partials are written at (term.out * grid + CTA).
+constexpr uint32_t kMaxGroupTerms = 16;
+constexpr uint32_t kPauliTileQubits = 12;
+constexpr uint32_t kPauliMaxSpan = 9;
+struct PauliGroupTerm {
+    uint64_t x, z;
+    uint32_t kx;   // coordinates of x >> c in the group's basis
+    uint32_t xl;   // x's low c bits
+    uint32_t out;  // the term's index in the caller's list
+    uint32_t pad;
+};
+struct PauliGroupPlan {
+    uint32_t c = 0, d = 0;
+    uint64_t free_mask = 0;  // high bits (above c) that index the cosets
+    uint32_t span_off = 0, term_off = 0, nterms = 0;
+};
+struct PauliPlan {
+    std::vector<PauliGroupPlan> groups;
+    std::vector<uint64_t> spans;  // 2^d per group: span[k] = XOR of basis vectors in k
+    std::vector<PauliGroupTerm> terms;
+};
+PauliPlan plan_pauli_groups(const uint64_t* x, const uint64_t* z, uint32_t num_terms, uint32_t n);
+int launch_pauli_group(const void* amps, uint32_t n, uint32_t c, uint32_t d, const uint64_t* dev_span,
+                       uint64_t free_mask, const void* dev_terms, uint32_t nterms, double* dev_partials,
+                       uint32_t grid, void* stream, int precision);
+int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const uint64_t* dev_x,
+                              const uint64_t* dev_z, uint32_t num_terms, double* dev_out, void* stream);
 const char* last_cuda_error_string();
+// Counts kernels this library launched (process-wide; mb2_kernel_launches).
+void note_launches(uint32_t k);
 
 }  // namespace mb2
