@@ -701,6 +701,10 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
 }
 
+// Shared memory an SM gives its resident CTAs (228 KiB less the 1 KiB the
+// system reserves per CTA is accounted per CTA by the callers).
+constexpr size_t kSmemPerSm = 228 * 1024;
+
 int grid_for(uint64_t work, int threads) {
     const uint64_t blocks = (work + threads - 1) / threads;
     return static_cast<int>(blocks < 148ull * 16 ? (blocks == 0 ? 1 : blocks) : 148ull * 16);
@@ -777,7 +781,7 @@ int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, 
 
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
                      const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
-                     const BatchLayout* batch, uint32_t ctas_per_sm) {
+                     const BatchLayout* batch, uint32_t ctas_per_sm, uint32_t buffers) {
     static bool attr_set = false;
     if (!attr_set) {
         const int most = static_cast<int>(3 * (size_t{1} << kMaxTileQubits) * sizeof(double2) + kMaxStagedBytes);
@@ -790,15 +794,19 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileIns
     const size_t staged = size_t{pass.prog_count} * sizeof(TileInstr) + size_t{pass.sdata_count} * sizeof(double);
     if (staged > kMaxStagedBytes) return MB2_ERR_INVALID;
     const uint32_t threads = 1u << (pass.m - kRegQubits);
-    // 12-qubit tiles: one CTA per SM with three buffers (two tiles in
-    // flight); smaller tiles: two buffers per CTA and two CTAs per SM, or
+    // 12-qubit tiles: one CTA per SM; smaller tiles: two CTAs per SM, or
     // three (168 registers a thread) when ctas_per_sm asks for it and the
-    // shared memory allows.
-    const uint32_t stages = pass.m == kMaxTileQubits ? 3u : 2u;
-    const size_t smem = stages * (size_t{1} << pass.m) * sizeof(double2) + staged;
+    // shared memory allows.  Each CTA keeps `stages` tile buffers (tiles
+    // stages - 1 ahead in flight): three where they fit beside the other
+    // CTAs of the SM, else two.
+    const uint32_t want_per_sm = pass.m == kMaxTileQubits ? 1u : (ctas_per_sm >= 3 ? 3u : 2u);
+    const size_t tile_bytes = (size_t{1} << pass.m) * sizeof(double2);
+    uint32_t stages = buffers == 2 ? 2u : 3u;
+    if (stages == 3 && want_per_sm * (3 * tile_bytes + staged + 1024) > kSmemPerSm) stages = 2;
+    const size_t smem = stages * tile_bytes + staged;
     auto kern = pass.m == kMaxTileQubits ? k_tile_pass<256, 1> : k_tile_pass<128, 2>;
     uint32_t per_sm = pass.m == kMaxTileQubits ? 1u : 2u;
-    if (pass.m < kMaxTileQubits && ctas_per_sm >= 3) {
+    if (want_per_sm >= 3) {
         int resident = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_tile_pass<128, 3>, static_cast<int>(threads), smem);
         if (resident >= 3) {

@@ -124,13 +124,23 @@ __global__ void k_expectation_finish(const double* __restrict__ partials, uint32
 }
 
 // ---- grouped terms: one state read per group --------------------------------
-// A group's terms have high X parts (bits >= c) inside a subspace V of
+// A group's terms have X masks whose bits above c lie in a subspace V of
 // dimension d.  A tile is a coset of V: 2^d chunks of 2^c contiguous
 // amplitudes (chunk k's high bits are rep ^ span[k]), so for every term the
-// partner m ^ x of each amplitude m is in the same tile: chunk k ^ kx, low
-// bits low ^ xl.  Each pair is visited once.  Partial sums go to fixed slots
-// (CTA, term) and are added in CTA order by the finish kernel.
+// partner m ^ x of each amplitude m is in the same tile, at tile index
+// L ^ dl with dl = (kx << c) | xl.  Each pair is visited once, from the
+// member whose bit hb (the highest bit of dl) is clear.
+//
+// With s(m) = (-1)^popcount(z & m) and s(m ^ x) = s(m) (-1)^popcount(z & x),
+// the pair's share t s(m') + conj(t) s(m), t = conj(a_m) a_m', is
+// 2 s(m) Re t when popcount(z & x) is even and -2i s(m) Im t when it is odd,
+// so one real accumulator per term suffices.  s(m) splits over the parts of
+// m: the coset representative (one parity per term and coset), the chunk
+// (a per-term table over the 2^d chunks) and the low c bits.
+// Partial sums go to fixed slots (term, CTA) and are added in CTA order by
+// the finish kernel.
 using GroupTerm = PauliGroupTerm;
+constexpr uint32_t kChunkWords = (1u << kPauliMaxSpan) / 32;
 
 template <typename A>
 __global__ void __launch_bounds__(kThreads)
@@ -139,18 +149,35 @@ __global__ void __launch_bounds__(kThreads)
                   double* __restrict__ partials) {
     extern __shared__ double2 gtile[];
     __shared__ uint64_t sspan[1u << kPauliMaxSpan];
-    __shared__ GroupTerm sterm[kMaxGroupTerms];
-    __shared__ double red[2 * (kThreads / 32)];
+    __shared__ uint32_t cpar[kMaxGroupTerms][kChunkWords];  // parity of z_hi & span[k], bit k
+    __shared__ uint32_t rpar[kMaxGroupTerms];               // parity of z_hi & rep, this coset
+    __shared__ uint32_t tdl[kMaxGroupTerms], tzl[kMaxGroupTerms], tmode[kMaxGroupTerms];
+    __shared__ uint64_t tzh[kMaxGroupTerms];
+    __shared__ double red[kThreads / 32];
     const uint32_t tile_amps = 1u << (c + d);
-    const uint32_t lowmask = (1u << c) - 1;
-    for (uint32_t i = threadIdx.x; i < (1u << d); i += kThreads) sspan[i] = span[i];
-    for (uint32_t i = threadIdx.x; i < nterms; i += kThreads) sterm[i] = terms[i];
-    double re[kMaxGroupTerms], im[kMaxGroupTerms];
-#pragma unroll
-    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
-        re[t] = 0.0;
-        im[t] = 0.0;
+    const uint32_t nchunks = 1u << d;
+    for (uint32_t i = threadIdx.x; i < nchunks; i += kThreads) sspan[i] = span[i];
+    for (uint32_t t = threadIdx.x; t < nterms; t += kThreads) {
+        const GroupTerm T = terms[t];
+        tdl[t] = (T.kx << c) | T.xl;
+        tzl[t] = static_cast<uint32_t>(T.z & ((uint64_t{1} << c) - 1));
+        tzh[t] = T.z >> c;
+        // 0: a Z string (x = 0); 1: real pair sum; 2: imaginary pair sum
+        tmode[t] = T.x == 0 ? 0u : ((__popcll(T.x & T.z) & 1) ? 2u : 1u);
     }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kMaxGroupTerms * kChunkWords; i += kThreads) {
+        const uint32_t t = i / kChunkWords, w = i % kChunkWords;
+        uint32_t bits = 0;
+        if (t < nterms)
+            for (uint32_t b = 0; b < 32 && w * 32 + b < nchunks; ++b)
+                bits |= static_cast<uint32_t>(__popcll(tzh[t] & sspan[w * 32 + b]) & 1) << b;
+        cpar[t][w] = bits;
+    }
+    double acc[kMaxGroupTerms];
+#pragma unroll
+    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) acc[t] = 0.0;
+    const uint32_t lowmask = (1u << c) - 1;
     for (uint64_t cs = blockIdx.x; cs < ncosets; cs += gridDim.x) {
         // Coset representative: the bits of cs deposited on the free
         // (non-pivot) high bits; the pivots stay zero.
@@ -164,70 +191,59 @@ __global__ void __launch_bounds__(kThreads)
                 mask ^= low;
             }
         }
-        __syncthreads();  // the previous coset's reads are done (and the staging above)
+        __syncthreads();  // the previous coset's reads are done
         for (uint32_t L = threadIdx.x; L < tile_amps; L += kThreads) {
             const uint64_t m = ((rep ^ sspan[L >> c]) << c) | (L & lowmask);
             gtile[L] = as_d2(st[m]);
         }
+        if (threadIdx.x < nterms) rpar[threadIdx.x] = __popcll(tzh[threadIdx.x] & rep) & 1;
         __syncthreads();
 #pragma unroll
         for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
             if (t < nterms) {
-                const uint64_t z = sterm[t].z;
-                const uint32_t dl = (sterm[t].kx << c) | sterm[t].xl;  // tile-local XOR of the pair
-                if (dl == 0) {                                          // x = 0: a Z string
+                const uint32_t dl = tdl[t], zl = tzl[t], mode = tmode[t], rp = rpar[t];
+                const uint32_t* cp = cpar[t];
+                if (mode == 0) {
                     for (uint32_t L = threadIdx.x; L < tile_amps; L += kThreads) {
-                        const uint64_t m = ((rep ^ sspan[L >> c]) << c) | (L & lowmask);
+                        const uint32_t k = L >> c;
+                        const uint32_t neg = rp ^ (cp[k >> 5] >> (k & 31)) ^ __popc(zl & L);
                         const double2 a = gtile[L];
                         const double p = __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
-                        re[t] = (__popcll(z & m) & 1) ? __dsub_rn(re[t], p) : __dadd_rn(re[t], p);
+                        acc[t] = (neg & 1) ? __dsub_rn(acc[t], p) : __dadd_rn(acc[t], p);
                     }
                 } else {
                     const uint32_t hb = 31 - __clz(dl);
                     const uint32_t below = (1u << hb) - 1;
                     for (uint32_t q = threadIdx.x; q < tile_amps / 2; q += kThreads) {
                         const uint32_t L = ((q & ~below) << 1) | (q & below);
-                        const uint32_t L2 = L ^ dl;
-                        const uint64_t m = ((rep ^ sspan[L >> c]) << c) | (L & lowmask);
-                        const uint64_t m2 = ((rep ^ sspan[L2 >> c]) << c) | (L2 & lowmask);
-                        const double2 a = gtile[L], b = gtile[L2];
-                        const double tr = __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y));
-                        const double ti = __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x));
-                        const bool neg2 = __popcll(z & m2) & 1;
-                        const bool neg1 = __popcll(z & m) & 1;
-                        re[t] = neg2 ? __dsub_rn(re[t], tr) : __dadd_rn(re[t], tr);
-                        im[t] = neg2 ? __dsub_rn(im[t], ti) : __dadd_rn(im[t], ti);
-                        re[t] = neg1 ? __dsub_rn(re[t], tr) : __dadd_rn(re[t], tr);
-                        im[t] = neg1 ? __dadd_rn(im[t], ti) : __dsub_rn(im[t], ti);
+                        const uint32_t k = L >> c;
+                        const uint32_t neg = rp ^ (cp[k >> 5] >> (k & 31)) ^ __popc(zl & L);
+                        const double2 a = gtile[L], b = gtile[L ^ dl];
+                        const double v = mode == 1 ? __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y))
+                                                   : __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x));
+                        acc[t] = (neg & 1) ? __dsub_rn(acc[t], v) : __dadd_rn(acc[t], v);
                     }
                 }
             }
         }
     }
-    // Per term: this CTA's sum in a fixed order (lanes, then warps).
+    // Per term: this CTA's sum in a fixed order (lanes, then warps), written
+    // as (re, im) of the pair sum before the i^popcount(x & z) factor.
 #pragma unroll
     for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
         if (t < nterms) {
-            double r = re[t], i = im[t];
-            for (int o = 16; o > 0; o >>= 1) {
-                r += __shfl_down_sync(0xffffffffu, r, o);
-                i += __shfl_down_sync(0xffffffffu, i, o);
-            }
+            double r = acc[t];
+            for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
             __syncthreads();
-            if ((threadIdx.x & 31) == 0) {
-                red[2 * (threadIdx.x >> 5)] = r;
-                red[2 * (threadIdx.x >> 5) + 1] = i;
-            }
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r;
             __syncthreads();
             if (threadIdx.x == 0) {
-                double sr = 0.0, si = 0.0;
-                for (int w = 0; w < kThreads / 32; ++w) {
-                    sr += red[2 * w];
-                    si += red[2 * w + 1];
-                }
-                double* p = partials + 2 * (static_cast<uint64_t>(sterm[t].out) * gridDim.x + blockIdx.x);
-                p[0] = sr;
-                p[1] = si;
+                double sum = 0.0;
+                for (int w = 0; w < kThreads / 32; ++w) sum += red[w];
+                double* p = partials + 2 * (static_cast<uint64_t>(terms[t].out) * gridDim.x + blockIdx.x);
+                const uint32_t mode = tmode[t];
+                p[0] = mode == 0 ? sum : mode == 1 ? 2.0 * sum : 0.0;
+                p[1] = mode == 2 ? -2.0 * sum : 0.0;
             }
         }
     }

@@ -151,7 +151,7 @@ struct BatchLayout {
 };
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
                      const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
-                     const BatchLayout* batch = nullptr, uint32_t ctas_per_sm = 0);
+                     const BatchLayout* batch = nullptr, uint32_t ctas_per_sm = 0, uint32_t buffers = 0);
 // Expectation of num_terms Pauli terms: partials (num_terms * kExpBlocks * 2
 // doubles) then the fixed-order finish into out (num_terms * 2 doubles), all
 // device pointers.
