@@ -118,8 +118,6 @@ typedef struct mb2_sweep_options {
     int32_t low_qubits;      /* qubits 0..low-1 held in every tile (contiguous runs); -1 = none, 0 = default 3 */
     int32_t tile_qubits;     /* qubits per multi-gate tile pass; 0 = autotuned */
     int32_t per_gate;        /* 1: one launch per block, no tiling (the reference's sweep shape) */
-    int32_t ctas_per_sm;     /* complex128 tiles below 12 qubits: resident CTAs per SM (2 or 3); 0 = 2 */
-    int32_t tile_buffers;    /* complex128 tiles: shared-memory tile buffers per CTA (2 or 3); 0 = 3 where they fit */
 } mb2_sweep_options;
 
 /* Applies a whole operation list (MeasureOps skipped) as a sequence of

@@ -21,8 +21,7 @@ C128, C64 = 0, 1
 
 class SweepOptions(C.Structure):
     _fields_ = [("fuse_gates", C.c_int32), ("low_qubits", C.c_int32), ("tile_qubits", C.c_int32),
-                ("per_gate", C.c_int32), ("ctas_per_sm", C.c_int32),
-                ("tile_buffers", C.c_int32)]
+                ("per_gate", C.c_int32)]
 
 
 class SweepEstimate(C.Structure):

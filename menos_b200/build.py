@@ -63,7 +63,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIB_DIR, exist_ok=True)
     cpp, cu = _sources()
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(ROOT, "include", "mb2.h"))
     jobs, objs = [], []
     for f in cpp:

@@ -318,7 +318,7 @@ int mb2_apply_matrix_generic(mb2_state* s, const double* matrix, const uint32_t*
 int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
                                 mb2_boundary_fn boundary, void* user) {
     if (s == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     for (uint32_t i = 0; i < num_ops; ++i) {
         if (ops[i].opcode == MB2_MEASURE) continue;
@@ -385,9 +385,7 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
         const int rc = c64 ? mb2::launch_tile_pass_c64(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata,
                                                        s->ctx->sm_count, s->stream)
                            : mb2::launch_tile_pass(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata,
-                                                   s->ctx->sm_count, s->stream, nullptr,
-                                                   o.ctas_per_sm > 0 ? static_cast<uint32_t>(o.ctas_per_sm) : 0u,
-                                                   o.tile_buffers > 0 ? static_cast<uint32_t>(o.tile_buffers) : 0u);
+                                                   s->ctx->sm_count, s->stream);
         if (rc != MB2_OK) return fail(s->ctx, rc, std::string("tile pass launch: ") + mb2::last_cuda_error_string());
         s->stats.passes += 1;
         s->stats.launches += 1;
@@ -407,7 +405,7 @@ int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const m
 int mb2_estimate_sweep(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
                        mb2_sweep_estimate* out) {
     if (out == nullptr || (ops == nullptr && num_ops != 0) || num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     *out = mb2_sweep_estimate{};
     try {
@@ -595,7 +593,7 @@ int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
                        uint64_t* matrix_len) {
     if (num_blocks == nullptr || matrix_len == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
     if (num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     std::vector<mb2::Block> blocks;
     std::vector<uint32_t> order, order_pass;

@@ -151,7 +151,32 @@ struct BatchLayout {
 };
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
                      const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
-                     const BatchLayout* batch = nullptr, uint32_t ctas_per_sm = 0, uint32_t buffers = 0);
+                     const BatchLayout* batch = nullptr);
+// One tile-pass launch, as the instances (kernels_tile_*.cu) take it.
+struct TileLaunch {
+    void* amps = nullptr;
+    uint32_t n_all = 0;  // index bits, bindings included
+    uint32_t m = 0;
+    uint64_t smask = 0;
+    const TileInstr* prog = nullptr;
+    uint32_t nprog = 0;
+    const double* sdata = nullptr;
+    uint32_t nsdata = 0;
+    const double* gdata = nullptr;
+    uint64_t ntiles = 0;
+    const double* pdata = nullptr;
+    uint32_t pstride = 0;
+    uint32_t bshift = 0;
+    uint32_t stages = 2;
+    int grid = 0;
+    uint32_t threads = 0;
+    size_t smem = 0;
+    void* stream = nullptr;
+};
+constexpr size_t kTileSmemMax = 227 * 1024;
+int launch_tile_generic(const TileLaunch& L);  // any tile width, 64-bit indices
+int launch_tile_m11(const TileLaunch& L);      // 11-qubit tiles
+int launch_tile_m12(const TileLaunch& L);      // 12-qubit tiles
 // Expectation of num_terms Pauli terms: partials (num_terms * kExpBlocks * 2
 // doubles) then the fixed-order finish into out (num_terms * 2 doubles), all
 // device pointers.

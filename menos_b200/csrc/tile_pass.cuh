@@ -1,0 +1,571 @@
+// The multi-gate tile pass of the plain complex128 path: the kernel template
+// and its launcher, instantiated in kernels_tile_*.cu (one file per tile
+// width, so the instances compile in parallel).
+//
+// Bitwise contract: as the per-gate kernels (kernels_apply.cu); every
+// amplitude sees the blocks of the pass in plan order, each applied with the
+// reference kernel's operation order.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device_math.cuh"
+#include "mb2_internal.h"
+
+namespace mb2 {
+namespace tile {
+using namespace dev;
+
+// ---------------------------------------------------------------- tile pass
+// Shared-memory slot of tile-local index l: the low three bits XOR-folded
+// with every higher 3-bit group, so quarter-warps whose eight threads vary
+// three tile bits of distinct residue mod 3 hit eight distinct 16-byte bank
+// groups.
+__host__ __device__ __forceinline__ constexpr uint32_t swz(uint32_t l) {
+    const uint32_t h = l >> 3;
+    return l ^ ((h ^ (h >> 3) ^ (h >> 6) ^ (h >> 9)) & 7u);
+}
+
+// A TileInstr read as four 64-bit words (fields extracted by shifts, so no
+// field is ever indexed dynamically in local memory).  Layout: bytes 0-3 op,
+// k, kind, nthread; 4-11 pos[8]; 12-15 data; 16-27 tperm[12]; 28-31 aux.
+struct DI {
+    uint64_t w0, w1, w2, w3;
+    __device__ __forceinline__ uint32_t op() const { return static_cast<uint32_t>(w0 & 0xffu); }
+    __device__ __forceinline__ uint32_t k() const { return static_cast<uint32_t>((w0 >> 8) & 0xffu); }
+    __device__ __forceinline__ uint32_t kind() const { return static_cast<uint32_t>((w0 >> 16) & 0xffu); }
+    __device__ __forceinline__ uint32_t nthread() const { return static_cast<uint32_t>((w0 >> 24) & 0xffu); }
+    __device__ __forceinline__ uint32_t pos(uint32_t b) const {
+        return static_cast<uint32_t>((b < 4 ? (w0 >> (32 + 8 * b)) : (w1 >> (8 * (b - 4)))) & 0xffu);
+    }
+    __device__ __forceinline__ uint32_t data() const { return static_cast<uint32_t>(w1 >> 32); }
+    __device__ __forceinline__ uint32_t tperm(uint32_t i) const {
+        return static_cast<uint32_t>((i < 8 ? (w2 >> (8 * i)) : (w3 >> (8 * (i - 8)))) & 0xffu);
+    }
+    __device__ __forceinline__ uint32_t aux() const { return static_cast<uint32_t>(w3 >> 32); }
+};
+
+// Reads one instruction from the pass program staged in shared memory
+// (a plain load: the program is not in the global address space).
+__device__ __forceinline__ DI load_instr(const TileInstr* p) {
+    const ulonglong2* s = reinterpret_cast<const ulonglong2*>(p);
+    const ulonglong2 a = s[0], b = s[1];
+    return DI{a.x, a.y, b.x, b.y};
+}
+
+constexpr int kR = static_cast<int>(kRegQubits);  // register qubits per thread
+constexpr int kNA = 1 << kR;                         // amplitudes per thread
+static_assert(kR == 4, "the register-slot dispatch below is written for 4 register qubits");
+
+// Index of the lowest set bit of a (compile-time) register index j > 0.
+__host__ __device__ constexpr int lowbit_index(int j) { return (j & 1) ? 0 : (j & 2) ? 1 : (j & 4) ? 2 : 3; }
+
+template <int P, int KIND>
+__device__ __forceinline__ void g1(double2 (&a)[kNA], const double* md, uint32_t aux) {
+    const double2 e0 = reinterpret_cast<const double2*>(md)[0], e1 = reinterpret_cast<const double2*>(md)[1];
+    const double2 e2 = reinterpret_cast<const double2*>(md)[2], e3 = reinterpret_cast<const double2*>(md)[3];
+    const double m00r = e0.x, m00i = e0.y, m01r = e1.x, m01i = e1.y;
+    const double m10r = e2.x, m10i = e2.y, m11r = e3.x, m11i = e3.y;
+#pragma unroll
+    for (int j = 0; j < kNA; ++j) {
+        if (j & (1 << P)) continue;
+        const double2 x = a[j];
+        const double2 y = a[j | (1 << P)];
+        double2 o0, o1;
+        if (KIND == TK_GEN) {
+            o0 = cadd(cmul(m00r, m00i, x), cmul(m01r, m01i, y));
+            o1 = cadd(cmul(m10r, m10i, x), cmul(m11r, m11i, y));
+        } else if (KIND == TK_U3) {
+            o0 = cadd(cmul_re(m00r, x), cmul(m01r, m01i, y));
+            o1 = cadd(cmul(m10r, m10i, x), cmul(m11r, m11i, y));
+        } else if (KIND == TK_REAL) {
+            o0 = cadd(cmul_re(m00r, x), cmul_re(m01r, y));
+            o1 = cadd(cmul_re(m10r, x), cmul_re(m11r, y));
+        } else {  // TK_MONO: row r takes entry (r, src_r) of column src_r, or is zero
+            const uint32_t s0 = aux & 7u, s1 = (aux >> 3) & 7u;
+            o0 = s0 == 7u ? make_double2(0.0, 0.0)
+                          : scale_entry(s0 ? m01r : m00r, s0 ? m01i : m00i, s0 ? y : x);
+            o1 = s1 == 7u ? make_double2(0.0, 0.0)
+                          : scale_entry(s1 ? m11r : m10r, s1 ? m11i : m10i, s1 ? y : x);
+        }
+        a[j] = o0;
+        a[j | (1 << P)] = o1;
+    }
+}
+
+template <int P0, int P1, int KIND>
+__device__ __forceinline__ void g2(double2 (&a)[kNA], const double* md, uint32_t aux) {
+    if constexpr (P0 == P1) {
+        return;
+    } else {
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) {
+            if (j & ((1 << P0) | (1 << P1))) continue;
+            const int idx[4] = {j, j | (1 << P0), j | (1 << P1), j | (1 << P0) | (1 << P1)};
+            const double2 in[4] = {a[idx[0]], a[idx[1]], a[idx[2]], a[idx[3]]};
+            double2 out[4];
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+                if (KIND == TK_MONO) {
+                    const uint32_t s = (aux >> (3 * o)) & 7u;
+                    if (s == 7u) {
+                        out[o] = make_double2(0.0, 0.0);
+                    } else {
+                        const double2 src = s == 0 ? in[0] : s == 1 ? in[1] : s == 2 ? in[2] : in[3];
+                        out[o] = scale_entry(md[8 * o + 2 * s], md[8 * o + 2 * s + 1], src);
+                    }
+                } else {
+                    double2 acc = cmul(md[8 * o], md[8 * o + 1], in[0]);
+#pragma unroll
+                    for (int i = 1; i < 4; ++i) acc = cadd(acc, cmul(md[8 * o + 2 * i], md[8 * o + 2 * i + 1], in[i]));
+                    out[o] = acc;
+                }
+            }
+#pragma unroll
+            for (int o = 0; o < 4; ++o) a[idx[o]] = out[o];
+        }
+    }
+}
+
+template <int KIND>
+__device__ __forceinline__ void dispatch_g1(int p, double2 (&a)[kNA], const double* md, uint32_t aux) {
+    switch (p) {
+        case 0: g1<0, KIND>(a, md, aux); break;
+        case 1: g1<1, KIND>(a, md, aux); break;
+        case 2: g1<2, KIND>(a, md, aux); break;
+        default: g1<3, KIND>(a, md, aux); break;
+    }
+}
+
+template <int P0, int KIND>
+__device__ __forceinline__ void dispatch_g2b(int p1, double2 (&a)[kNA], const double* md, uint32_t aux) {
+    switch (p1) {
+        case 0: g2<P0, 0, KIND>(a, md, aux); break;
+        case 1: g2<P0, 1, KIND>(a, md, aux); break;
+        case 2: g2<P0, 2, KIND>(a, md, aux); break;
+        default: g2<P0, 3, KIND>(a, md, aux); break;
+    }
+}
+
+template <int KIND>
+__device__ __forceinline__ void dispatch_g2(int p0, int p1, double2 (&a)[kNA], const double* md, uint32_t aux) {
+    switch (p0) {
+        case 0: dispatch_g2b<0, KIND>(p1, a, md, aux); break;
+        case 1: dispatch_g2b<1, KIND>(p1, a, md, aux); break;
+        case 2: dispatch_g2b<2, KIND>(p1, a, md, aux); break;
+        default: dispatch_g2b<3, KIND>(p1, a, md, aux); break;
+    }
+}
+
+// A diagonal block of k <= 2 qubits in registers.  Each operand is either
+// a register slot (its bit over j is known at compile time in the templates
+// below) or a thread bit (one value for all 16 amplitudes).  The entry of
+// amplitude j is e = bit0 | bit1 << 1; its class (aux, 2 bits per entry:
+// 0 copy, 1 negate, 2 multiply) is resolved once per gate or per thread, and
+// each class runs its own loop, so an amplitude costs nothing (copy), two
+// integer ops (negate) or one complex product (multiply).
+struct Diag4 {
+    double2 d[4];
+    uint32_t aux;
+};
+
+__device__ __forceinline__ double2 diag_entry(const Diag4& D, uint32_t e) {
+    return (e & 2u) ? ((e & 1u) ? D.d[3] : D.d[2]) : ((e & 1u) ? D.d[1] : D.d[0]);
+}
+
+// Applies entry class `cls` with entry d to the amplitudes j whose selector
+// bits (j >> P0 & 1, j >> P1 & 1) equal (b0, b1); P < 0 means "no condition".
+template <int P0, int P1>
+__device__ __forceinline__ void diag_set(double2 (&a)[kNA], uint32_t cls, double2 d, int b0, int b1) {
+    if (cls == 1u) {
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) {
+            if (P0 >= 0 && ((j >> (P0 < 0 ? 0 : P0)) & 1) != b0) continue;
+            if (P1 >= 0 && ((j >> (P1 < 0 ? 0 : P1)) & 1) != b1) continue;
+            a[j] = cneg(a[j]);
+        }
+    } else if (cls == 2u) {
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) {
+            if (P0 >= 0 && ((j >> (P0 < 0 ? 0 : P0)) & 1) != b0) continue;
+            if (P1 >= 0 && ((j >> (P1 < 0 ? 0 : P1)) & 1) != b1) continue;
+            a[j] = cmul(d.x, d.y, a[j]);
+        }
+    }
+}
+
+// Both operands in register slots (P1 < 0: one operand).
+template <int P0, int P1>
+__device__ __forceinline__ void diag_rr(double2 (&a)[kNA], const Diag4& D) {
+#pragma unroll
+    for (int e = 0; e < (P1 >= 0 ? 4 : 2); ++e)
+        diag_set<P0, P1>(a, (D.aux >> (2 * e)) & 3u, D.d[e], e & 1, (e >> 1) & 1);
+}
+
+// One operand in register slot P (bit `shift` of e), the other a thread bit tv.
+template <int P>
+__device__ __forceinline__ void diag_rt(double2 (&a)[kNA], const Diag4& D, uint32_t shift, uint32_t tv) {
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+        const uint32_t e = (static_cast<uint32_t>(b) << shift) | (tv << (1u - shift));
+        diag_set<P, -1>(a, (D.aux >> (2 * e)) & 3u, diag_entry(D, e), b, 0);
+    }
+}
+
+__device__ __forceinline__ void diag_small(double2 (&a)[kNA], const double* md, uint32_t k, uint32_t aux, int s0,
+                                           int s1, uint32_t t0, uint32_t t1) {
+    // s0/s1: register slot of operand 0/1, or -1 for a thread bit of value t0/t1.
+    Diag4 D;
+    D.aux = aux;
+    D.d[0] = reinterpret_cast<const double2*>(md)[0];
+    D.d[1] = reinterpret_cast<const double2*>(md)[1];
+    D.d[2] = k > 1 ? reinterpret_cast<const double2*>(md)[2] : D.d[0];
+    D.d[3] = k > 1 ? reinterpret_cast<const double2*>(md)[3] : D.d[1];
+    if (k == 1) {
+        if (s0 < 0) {
+            diag_set<-1, -1>(a, (aux >> (2 * t0)) & 3u, diag_entry(D, t0), 0, 0);
+            return;
+        }
+        switch (s0) {
+            case 0: diag_rr<0, -1>(a, D); break;
+            case 1: diag_rr<1, -1>(a, D); break;
+            case 2: diag_rr<2, -1>(a, D); break;
+            default: diag_rr<3, -1>(a, D); break;
+        }
+        return;
+    }
+    if (s0 >= 0 && s1 >= 0) {
+        switch (s0 * 4 + s1) {
+            case 1: diag_rr<0, 1>(a, D); break;
+            case 2: diag_rr<0, 2>(a, D); break;
+            case 3: diag_rr<0, 3>(a, D); break;
+            case 4: diag_rr<1, 0>(a, D); break;
+            case 6: diag_rr<1, 2>(a, D); break;
+            case 7: diag_rr<1, 3>(a, D); break;
+            case 8: diag_rr<2, 0>(a, D); break;
+            case 9: diag_rr<2, 1>(a, D); break;
+            case 11: diag_rr<2, 3>(a, D); break;
+            case 12: diag_rr<3, 0>(a, D); break;
+            case 13: diag_rr<3, 1>(a, D); break;
+            case 14: diag_rr<3, 2>(a, D); break;
+            default: break;
+        }
+        return;
+    }
+    if (s0 < 0 && s1 < 0) {
+        const uint32_t e = t0 | (t1 << 1);
+        diag_set<-1, -1>(a, (aux >> (2 * e)) & 3u, diag_entry(D, e), 0, 0);
+        return;
+    }
+    const int s = s0 >= 0 ? s0 : s1;
+    const uint32_t shift = s0 >= 0 ? 0u : 1u;
+    const uint32_t tv = s0 >= 0 ? t1 : t0;
+    switch (s) {
+        case 0: diag_rt<0>(a, D, shift, tv); break;
+        case 1: diag_rt<1>(a, D, shift, tv); break;
+        case 2: diag_rt<2>(a, D, shift, tv); break;
+        default: diag_rt<3>(a, D, shift, tv); break;
+    }
+}
+
+// Exact permutations (every nonzero entry (1,0)): register moves only.
+// TK_X: 1q swap; TK_SW12 / TK_SW13 / TK_SW23: 2q, exchange local indices
+// (1,2) (SWAP), (1,3) (CX, control = operand 0), (2,3) (CX, control = operand 1).
+template <int P>
+__device__ __forceinline__ void perm1(double2 (&a)[kNA]) {
+#pragma unroll
+    for (int j = 0; j < kNA; ++j) {
+        if (j & (1 << P)) continue;
+        const double2 t = a[j];
+        a[j] = a[j | (1 << P)];
+        a[j | (1 << P)] = t;
+    }
+}
+
+template <int P0, int P1, int KIND>
+__device__ __forceinline__ void perm2(double2 (&a)[kNA]) {
+    if constexpr (P0 == P1) {
+        return;
+    } else {
+        constexpr int lo = KIND == TK_SW23 ? 2 : 1;
+        constexpr int hi = KIND == TK_SW12 ? 2 : 3;
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) {
+            if (j & ((1 << P0) | (1 << P1))) continue;
+            const int il = j | ((lo & 1) ? (1 << P0) : 0) | ((lo & 2) ? (1 << P1) : 0);
+            const int ih = j | ((hi & 1) ? (1 << P0) : 0) | ((hi & 2) ? (1 << P1) : 0);
+            const double2 t = a[il];
+            a[il] = a[ih];
+            a[ih] = t;
+        }
+    }
+}
+
+template <int KIND>
+__device__ __forceinline__ void dispatch_perm2(int p0, int p1, double2 (&a)[kNA]) {
+    switch (p0 * 4 + p1) {
+        case 1: perm2<0, 1, KIND>(a); break;
+        case 2: perm2<0, 2, KIND>(a); break;
+        case 3: perm2<0, 3, KIND>(a); break;
+        case 4: perm2<1, 0, KIND>(a); break;
+        case 6: perm2<1, 2, KIND>(a); break;
+        case 7: perm2<1, 3, KIND>(a); break;
+        case 8: perm2<2, 0, KIND>(a); break;
+        case 9: perm2<2, 1, KIND>(a); break;
+        case 11: perm2<2, 3, KIND>(a); break;
+        case 12: perm2<3, 0, KIND>(a); break;
+        case 13: perm2<3, 1, KIND>(a); break;
+        case 14: perm2<3, 2, KIND>(a); break;
+        default: break;
+    }
+}
+
+// cp.async of one 16-byte amplitude, global -> shared (L2 only, no L1).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// One pass of the tiled sweep.  blockDim.x == 2^(m-4) <= 256; each thread
+// owns 16 amplitudes.  Persistent CTAs take tiles round-robin; the tiles
+// `stages - 1` ahead are gathered into shared-memory buffers with cp.async
+// while the current one is computed, so HBM traffic overlaps the FP64 work.
+// The pass's instructions and small-matrix data are staged in shared memory
+// once per CTA.
+//
+// MT > 0 fixes the tile width at compile time (shared-memory slots of the
+// canonical mapping become constants); IDX is the amplitude-index type,
+// 32-bit when the state (all bindings included) has at most 2^32
+// amplitudes.  A tile's base index is its number deposited on the bits
+// outside the tile (nmask); moving gridDim.x tiles on is the masked add
+// ((base | ~nmask) + step) & nmask, step = deposit(gridDim.x).
+template <int MAXT, int MINB, int MT, typename IDX>
+__global__ void __launch_bounds__(MAXT, MINB)
+    k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask,
+                const TileInstr* __restrict__ prog, uint32_t nprog, const double* __restrict__ sdata,
+                uint32_t nsdata, const double* __restrict__ gdata, uint64_t ntiles, const double* __restrict__ pdata,
+                uint32_t pstride, uint32_t bshift, uint32_t stages) {
+    extern __shared__ double2 smem_tiles[];
+    const uint32_t m = MT > 0 ? static_cast<uint32_t>(MT) : m_rt;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t tbits = m - kRegQubits;
+    const uint32_t tile_amps = 1u << m;
+    TileInstr* sprog = reinterpret_cast<TileInstr*>(smem_tiles + stages * tile_amps);
+    double* sd = reinterpret_cast<double*>(sprog + nprog);
+    for (uint32_t i = tid; i < nprog * 2; i += blockDim.x)
+        reinterpret_cast<ulonglong2*>(sprog)[i] = __ldg(reinterpret_cast<const ulonglong2*>(prog) + i);
+    for (uint32_t i = tid; i < nsdata; i += blockDim.x) sd[i] = __ldg(sdata + i);
+    // Canonical (load/store) mapping: thread bits = tile bits 0..tbits-1,
+    // register bits = tile bits tbits..m-1.
+    IDX off_lo = 0, hib0 = 0, hib1 = 0, hib2 = 0, hib3 = 0;
+    {
+        uint32_t b = 0;
+        for (uint32_t p = 0; p < n; ++p) {
+            if (!((smask >> p) & 1u)) continue;
+            if (b < tbits) {
+                off_lo |= static_cast<IDX>((tid >> b) & 1u) << p;
+            } else {
+                const IDX v = IDX{1} << p;
+                const uint32_t r = b - tbits;
+                if (r == 0) hib0 = v;
+                else if (r == 1) hib1 = v;
+                else if (r == 2) hib2 = v;
+                else hib3 = v;
+            }
+            ++b;
+        }
+    }
+    const uint64_t nmask64 = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~smask;
+    const IDX nmask = static_cast<IDX>(nmask64);
+    const IDX step = static_cast<IDX>(pdep64(gridDim.x, nmask64));
+    auto advance = [&](IDX b) -> IDX { return ((b | ~nmask) + step) & nmask; };
+    // Amplitude (tid, j) of the canonical mapping: global index base +
+    // off_lo + the register bits of j (disjoint bit sets, so + is |);
+    // shared-memory slot swz(tid) ^ swz(j << tbits) (swz is XOR-linear).
+    const uint32_t s_tid = swz(tid);
+    auto reg_off = [&](int j) -> IDX {
+        return ((j & 1) ? hib0 : IDX{0}) + ((j & 2) ? hib1 : IDX{0}) + ((j & 4) ? hib2 : IDX{0}) +
+               ((j & 8) ? hib3 : IDX{0});
+    };
+    auto slot = [&](int j) -> uint32_t { return s_tid ^ swz(static_cast<uint32_t>(j) << tbits); };
+    auto prefetch = [&](IDX base, double2* buf) {
+        const IDX b0 = base + off_lo;
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) cp_async16(buf + slot(j), st + (b0 + reg_off(j)));
+        cp_async_commit();
+    };
+
+    // `stages` tile buffers: the tiles `stages - 1` ahead are in flight
+    // while this one is computed (one commit group per tile, empty groups
+    // past the end keep the count uniform).
+    uint64_t tp = blockIdx.x;  // next tile to prefetch
+    IDX pbase = static_cast<IDX>(pdep64(blockIdx.x, nmask64));
+    IDX cbase = pbase;  // base of the tile being computed
+    for (uint32_t sg = 0; sg + 1 < stages; ++sg) {
+        if (tp < ntiles) prefetch(pbase, smem_tiles + sg * tile_amps);
+        else cp_async_commit();
+        tp += gridDim.x;
+        pbase = advance(pbase);
+    }
+    uint32_t cur = 0, nxt = stages - 1;  // buffer of this tile, of the next prefetch
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        double2* tile = smem_tiles + cur * tile_amps;
+        if (tp < ntiles) prefetch(pbase, smem_tiles + nxt * tile_amps);
+        else cp_async_commit();
+        tp += gridDim.x;
+        pbase = advance(pbase);
+        cur = cur + 1 == stages ? 0u : cur + 1;
+        nxt = nxt + 1 == stages ? 0u : nxt + 1;
+        if (stages == 3) cp_async_wait<2>();
+        else cp_async_wait<1>();
+        __syncthreads();
+
+        double2 a[kNA];
+        uint32_t pc = 0;
+        while (pc < nprog) {
+            const DI I = load_instr(sprog + pc);
+            ++pc;
+            if (I.op() == TOP_PHASE) {
+                uint32_t tb = 0;
+                if (MT > 0) {
+#pragma unroll
+                    for (uint32_t i = 0; i < (MT > 0 ? MT - kRegQubits : 1u); ++i)
+                        if (i < I.nthread()) tb |= ((tid >> i) & 1u) << I.tperm(i);
+                } else {
+                    for (uint32_t i = 0; i < I.nthread(); ++i) tb |= ((tid >> i) & 1u) << I.tperm(i);
+                }
+                uint32_t rb[kR];
+#pragma unroll
+                for (int b = 0; b < kR; ++b) rb[b] = 1u << I.pos(b);
+                // swz is linear over XOR, so slot j's address is swz(tb) XOR the
+                // swizzled register bits of j.
+                uint32_t adr[kNA];
+                adr[0] = swz(tb);
+#pragma unroll
+                for (int j = 1; j < kNA; ++j) adr[j] = adr[j & (j - 1)] ^ swz(rb[lowbit_index(j)]);
+#pragma unroll
+                for (int j = 0; j < kNA; ++j) a[j] = tile[adr[j]];
+                // The next instruction is read while this one executes (every
+                // group ends with TOP_END, so the read stays in the program).
+                DI G = load_instr(sprog + pc);
+                ++pc;
+                for (; G.op() != TOP_END; ++pc) {
+                    const DI Gn = load_instr(sprog + pc);
+                    // Parametric blocks (a batched sweep) read the matrix of
+                    // this tile's binding: binding = tile >> bshift.
+                    const double* md = G.nthread() ? pdata + (t >> bshift) * pstride + G.data() : sd + G.data();
+                    if (G.op() == TOP_G1) {
+                        switch (G.kind()) {
+                            case TK_GEN: dispatch_g1<TK_GEN>(G.pos(0), a, md, G.aux()); break;
+                            case TK_U3: dispatch_g1<TK_U3>(G.pos(0), a, md, G.aux()); break;
+                            case TK_REAL: dispatch_g1<TK_REAL>(G.pos(0), a, md, G.aux()); break;
+                            case TK_X:
+                                switch (G.pos(0)) {
+                                    case 0: perm1<0>(a); break;
+                                    case 1: perm1<1>(a); break;
+                                    case 2: perm1<2>(a); break;
+                                    default: perm1<3>(a); break;
+                                }
+                                break;
+                            default: dispatch_g1<TK_MONO>(G.pos(0), a, md, G.aux()); break;
+                        }
+                    } else if (G.op() == TOP_G2) {
+                        switch (G.kind()) {
+                            case TK_SW12: dispatch_perm2<TK_SW12>(G.pos(0), G.pos(1), a); break;
+                            case TK_SW13: dispatch_perm2<TK_SW13>(G.pos(0), G.pos(1), a); break;
+                            case TK_SW23: dispatch_perm2<TK_SW23>(G.pos(0), G.pos(1), a); break;
+                            case TK_MONO: dispatch_g2<TK_MONO>(G.pos(0), G.pos(1), a, md, G.aux()); break;
+                            default: dispatch_g2<TK_GEN>(G.pos(0), G.pos(1), a, md, G.aux()); break;
+                        }
+                    } else if (G.kind() == TK_DSMALL) {
+                        // Operand sources decided on the host: 0x80 | slot, or a thread bit.
+                        const uint32_t c0 = G.pos(4), c1 = G.pos(5);
+                        const int s0 = (c0 & 0x80u) ? static_cast<int>(c0 & 3u) : -1;
+                        const int s1 = (c1 & 0x80u) ? static_cast<int>(c1 & 3u) : -1;
+                        const uint32_t t0 = (c0 & 0x80u) ? 0u : (tb >> c0) & 1u;
+                        const uint32_t t1 = (c1 & 0x80u) ? 0u : (tb >> c1) & 1u;
+                        diag_small(a, md, G.k(), G.aux(), s0, s1, t0, t1);
+                    } else {  // TOP_DIAG, any k: entry index per amplitude
+                        const uint32_t k = G.k();
+                        uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+                        for (uint32_t b = 0; b < k; ++b) {
+                            const uint32_t bit = 1u << G.pos(b);
+                            et |= ((tb & bit) ? 1u : 0u) << b;
+                            if (bit == rb[0]) e0 = 1u << b;
+                            if (bit == rb[1]) e1 = 1u << b;
+                            if (bit == rb[2]) e2 = 1u << b;
+                            if (bit == rb[3]) e3 = 1u << b;
+                        }
+#pragma unroll
+                        for (int j = 0; j < kNA; ++j) {
+                            const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) | ((j & 4) ? e2 : 0u) |
+                                               ((j & 8) ? e3 : 0u);
+                            a[j] = scale_entry(md[2 * e], md[2 * e + 1], a[j]);
+                        }
+                    }
+                    G = Gn;
+                }
+#pragma unroll
+                for (int j = 0; j < kNA; ++j) tile[adr[j]] = a[j];
+                __syncthreads();
+            } else if (I.op() == TOP_SMEM) {
+                // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
+                const uint32_t k = I.k(), dim = 1u << k;
+                uint32_t opm = 0;
+                for (uint32_t b = 0; b < k; ++b) opm |= 1u << I.pos(b);
+                const double* md = gdata + I.data();
+#pragma unroll
+                for (int j = 0; j < kNA; ++j) {
+                    const uint32_t l = tid | (static_cast<uint32_t>(j) << tbits);
+                    uint32_t out = 0;
+                    for (uint32_t b = 0; b < k; ++b) out |= ((l >> I.pos(b)) & 1u) << b;
+                    const uint32_t gbase = l & ~opm;
+                    double2 acc = make_double2(0.0, 0.0);
+                    for (uint32_t in = 0; in < dim; ++in) {
+                        uint32_t li = gbase;
+                        for (uint32_t b = 0; b < k; ++b)
+                            if ((in >> b) & 1u) li |= 1u << I.pos(b);
+                        const double2 p = cmul(__ldg(md + 2 * (out * dim + in)), __ldg(md + 2 * (out * dim + in) + 1),
+                                               tile[swz(li)]);
+                        acc = (in == 0) ? p : cadd(acc, p);
+                    }
+                    a[j] = acc;
+                }
+                __syncthreads();
+#pragma unroll
+                for (int j = 0; j < kNA; ++j) tile[slot(j)] = a[j];
+                __syncthreads();
+            }
+        }
+
+        // Store: canonical mapping, -0.0 normalised.
+        const IDX b0 = cbase + off_lo;
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) st[b0 + reg_off(j)] = canon(tile[slot(j)]);
+        cbase = advance(cbase);
+        __syncthreads();  // the buffer is the target of a later prefetch
+    }
+}
+
+// Launches one instance; the shared-memory limit is raised once per instance.
+template <int MAXT, int MINB, int MT, typename IDX>
+int launch_instance(const TileLaunch& L) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_tile_pass<MAXT, MINB, MT, IDX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kTileSmemMax));
+        attr_set = true;
+    }
+    k_tile_pass<MAXT, MINB, MT, IDX><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
+        static_cast<double2*>(L.amps), L.n_all, L.m, L.smask, L.prog, L.nprog, L.sdata, L.nsdata, L.gdata, L.ntiles,
+        L.pdata, L.pstride, L.bshift, L.stages);
+    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+}
+
+}  // namespace tile
+}  // namespace mb2

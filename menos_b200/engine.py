@@ -96,11 +96,9 @@ class DeviceState:
         self._chk(f(self.h, m.ctypes.data, q.ctypes.data, len(q)), "mb2_apply_matrix")
 
     def apply_program(self, circ: Circuit, fuse_gates: bool = True, tile_qubits: int = 0,
-                      per_gate: bool = False, low_qubits: int = 0, ctas_per_sm: int = 0,
-                      tile_buffers: int = 0) -> SweepStats:
+                      per_gate: bool = False, low_qubits: int = 0) -> SweepStats:
         arr, keep = to_mb2_ops(circ)
-        opts = SweepOptions(1 if fuse_gates else 0, low_qubits, tile_qubits, 1 if per_gate else 0, ctas_per_sm,
-                            tile_buffers)
+        opts = SweepOptions(1 if fuse_gates else 0, low_qubits, tile_qubits, 1 if per_gate else 0)
         self._chk(lib().mb2_apply_program(self.h, arr, len(circ.ops), C.byref(opts)), "mb2_apply_program")
         del keep
         return self.stats()

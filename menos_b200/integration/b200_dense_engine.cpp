@@ -136,7 +136,7 @@ public:
             return CostEstimate{false, 0, 0, *reason, {}};
         if (request.num_qubits > 34) return CostEstimate{false, 0, 0, "more than 34 qubits on one B200", {}};
         Ops ops = to_mb2(*request.operations);
-        mb2_sweep_options o{request.fuse_gates ? 1 : 0, 0, 0, 0, 0, 0};
+        mb2_sweep_options o{request.fuse_gates ? 1 : 0, 0, 0, 0};
         mb2_sweep_estimate e{};
         if (mb2_estimate_sweep(ops.ops.data(), static_cast<uint32_t>(ops.ops.size()), &o, request.num_qubits, &e) !=
             MB2_OK)
@@ -169,7 +169,7 @@ public:
         StateGuard st;
         check(mb2_state_alloc(context(), request.num_qubits, MB2_C128, free_bytes, &st.s), "state");
         check(mb2_init(st.s, request.global_phase), "init");
-        mb2_sweep_options o{request.fuse_gates ? 1 : 0, 0, 0, 0, 0, 0};
+        mb2_sweep_options o{request.fuse_gates ? 1 : 0, 0, 0, 0};
         if (request.monitor != nullptr) {
             MonitorBridge bridge{request.monitor, nullptr};
             const int rc = mb2_apply_program_monitored(st.s, ops.ops.data(), static_cast<uint32_t>(ops.ops.size()),
