@@ -117,6 +117,11 @@ __device__ __forceinline__ void g2(double2 (&a)[kNA], const double* md, uint32_t
                         out[o] = scale_entry(md[8 * o + 2 * s], md[8 * o + 2 * s + 1], src);
                     }
                 } else {
+                    // Row o is read from shared memory where it is used: the
+                    // empty asm with a memory clobber keeps the compiler from
+                    // holding all 32 entries in registers across the groups,
+                    // which would set the register count of the whole kernel.
+                    asm volatile("" ::: "memory");
                     double2 acc = cmul(md[8 * o], md[8 * o + 1], in[0]);
 #pragma unroll
                     for (int i = 1; i < 4; ++i) acc = cadd(acc, cmul(md[8 * o + 2 * i], md[8 * o + 2 * i + 1], in[i]));
@@ -443,13 +448,14 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
                 for (int b = 0; b < kR; ++b) rb[b] = 1u << I.pos(b);
                 // swz is linear over XOR, so slot j's address is swz(tb) XOR the
-                // swizzled register bits of j.
-                uint32_t adr[kNA];
-                adr[0] = swz(tb);
+                // swizzled register bits of j (recomputed for the write-back
+                // rather than held in 16 registers through the gates).
+                const uint32_t z0 = swz(tb), z1 = swz(rb[0]), z2 = swz(rb[1]), z3 = swz(rb[2]), z4 = swz(rb[3]);
+                auto adr = [&](int j) -> uint32_t {
+                    return z0 ^ ((j & 1) ? z1 : 0u) ^ ((j & 2) ? z2 : 0u) ^ ((j & 4) ? z3 : 0u) ^ ((j & 8) ? z4 : 0u);
+                };
 #pragma unroll
-                for (int j = 1; j < kNA; ++j) adr[j] = adr[j & (j - 1)] ^ swz(rb[lowbit_index(j)]);
-#pragma unroll
-                for (int j = 0; j < kNA; ++j) a[j] = tile[adr[j]];
+                for (int j = 0; j < kNA; ++j) a[j] = tile[adr(j)];
                 // The next instruction is read while this one executes (every
                 // group ends with TOP_END, so the read stays in the program).
                 DI G = load_instr(sprog + pc);
@@ -511,7 +517,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
                     G = Gn;
                 }
 #pragma unroll
-                for (int j = 0; j < kNA; ++j) tile[adr[j]] = a[j];
+                for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
                 __syncthreads();
             } else if (I.op() == TOP_SMEM) {
                 // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
