@@ -155,7 +155,6 @@ int grid_for(uint64_t work, int threads) {
     return static_cast<int>(blocks < 148ull * 16 ? (blocks == 0 ? 1 : blocks) : 148ull * 16);
 }
 
-int status_of(cudaError_t e) { return e == cudaSuccess ? MB2_OK : MB2_ERR_CUDA; }
 
 }  // namespace
 
@@ -167,7 +166,7 @@ int launch_init(void* amps, uint64_t n_amps, int precision, double re, double im
     else
         k_init_c128<<<grid_for(n_amps, 256), 256, 0, s>>>(static_cast<double2*>(amps), n_amps, re, im);
     note_launches(1);
-    return status_of(cudaGetLastError());
+    return launch_status();
 }
 
 int launch_apply_1q(void* amps, uint32_t n, uint32_t q, const double* m8, void* stream) {
@@ -177,7 +176,7 @@ int launch_apply_1q(void* amps, uint32_t n, uint32_t q, const double* m8, void* 
     k_apply_1q<<<grid_for(npairs, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<double2*>(amps),
                                                                                     npairs, q, m);
     note_launches(1);
-    return status_of(cudaGetLastError());
+    return launch_status();
 }
 
 int launch_apply_2q(void* amps, uint32_t n, uint32_t q0, uint32_t q1, const double* m32, void* stream) {
@@ -187,7 +186,7 @@ int launch_apply_2q(void* amps, uint32_t n, uint32_t q0, uint32_t q1, const doub
     k_apply_2q<<<grid_for(ng, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<double2*>(amps), ng, q0,
                                                                                 q1, m);
     note_launches(1);
-    return status_of(cudaGetLastError());
+    return launch_status();
 }
 
 int launch_apply_diag(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* diag, void* stream) {
@@ -200,7 +199,7 @@ int launch_apply_diag(void* amps, uint32_t n, const uint32_t* q, uint32_t k, con
     k_apply_diag<<<grid_for(na, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<double2*>(amps), na, k, qq[0], qq[1], qq[2], qq[3], qq[4], qq[5], d);
     note_launches(1);
-    return status_of(cudaGetLastError());
+    return launch_status();
 }
 
 int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* dev_matrix,
@@ -221,7 +220,7 @@ int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, 
         static_cast<double2*>(amps), n, k, qq[0], qq[1], qq[2], qq[3], qq[4], qq[5],
         reinterpret_cast<const double2*>(dev_matrix));
     note_launches(1);
-    return status_of(cudaGetLastError());
+    return launch_status();
 }
 
 int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
@@ -263,6 +262,25 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileIns
     return rc;
 }
 
-const char* last_cuda_error_string() { return cudaGetErrorString(cudaGetLastError()); }
+namespace {
+// The error of the last failed launch on this thread: cudaGetLastError
+// clears the error it reports, so the launch wrappers keep it for the
+// message the caller builds.
+thread_local cudaError_t t_launch_error = cudaSuccess;
+}  // namespace
+
+int launch_status() {
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return MB2_OK;
+    t_launch_error = e;
+    return MB2_ERR_CUDA;
+}
+
+const char* last_cuda_error_string() {
+    cudaError_t e = t_launch_error;
+    t_launch_error = cudaSuccess;
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return cudaGetErrorString(e);
+}
 
 }  // namespace mb2

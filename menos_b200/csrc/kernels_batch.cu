@@ -132,7 +132,7 @@ int launch_batch_init(void* amps, uint32_t n, uint64_t bindings, double re, doub
     k_batch_init<<<static_cast<unsigned>(blocks < 148ull * 16 ? blocks : 148ull * 16), 256, 0,
                    static_cast<cudaStream_t>(stream)>>>(static_cast<double2*>(amps), total, n, re, im);
     note_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    return launch_status();
 }
 
 int launch_batch_expect(const void* amps, uint32_t n, uint64_t bindings, const uint64_t* dev_x,
@@ -149,7 +149,7 @@ int launch_batch_expect(const void* amps, uint32_t n, uint64_t bindings, const u
     k_batch_expect<<<static_cast<unsigned>(bindings * kCluster), kThreads, smem, static_cast<cudaStream_t>(stream)>>>(
         static_cast<const double2*>(amps), n, dev_x, dev_z, dev_coefs, num_terms, dev_out);
     note_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    return launch_status();
 }
 
 }  // namespace mb2

@@ -368,7 +368,7 @@ int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const Til
         static_cast<float2*>(amps), n, pass.m, pass.smask, dev_instrs + pass.prog_begin, pass.prog_count,
         dev_sdata + pass.sdata_begin, pass.sdata_count, dev_gdata, ntiles, stages);
     note_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    return launch_status();
 }
 
 int launch_scale_c64(void* amps, uint64_t n_amps, float s, void* stream) {
@@ -376,7 +376,7 @@ int launch_scale_c64(void* amps, uint64_t n_amps, float s, void* stream) {
     k_scale_c64<<<static_cast<unsigned>(blocks < 148ull * 16 ? blocks : 148ull * 16), 256, 0,
                   static_cast<cudaStream_t>(stream)>>>(static_cast<float2*>(amps), n_amps, s);
     note_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    return launch_status();
 }
 
 }  // namespace mb2

@@ -273,7 +273,7 @@ int launch_pauli_group(const void* amps, uint32_t n, uint32_t c, uint32_t d, con
         k_pauli_group<double2><<<grid, kThreads, smem, s>>>(static_cast<const double2*>(amps), c, d, dev_span,
                                                             free_mask, terms, nterms, ncosets, dev_partials);
     note_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    return launch_status();
 }
 
 int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const uint64_t* dev_x,
@@ -281,7 +281,7 @@ int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const
     k_expectation_finish<<<(num_terms + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
         dev_partials, blocks, dev_x, dev_z, num_terms, dev_out);
     note_launches(1);
-    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    return launch_status();
 }
 
 int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
@@ -297,7 +297,7 @@ int launch_expectation(const void* amps, uint32_t n, const uint64_t* dev_x, cons
     k_expectation_finish<<<(num_terms + 127) / 128, 128, 0, s>>>(dev_partials, kExpBlocks, dev_x, dev_z, num_terms,
                                                                   dev_out);
     note_launches(2);
-    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    return launch_status();
 }
 
 }  // namespace mb2

@@ -517,7 +517,7 @@ int launch_sample_t(const void* amps, uint32_t n, const double* dev_uniforms_sor
     k_assign<<<static_cast<unsigned>(nchunks), kThreads, 0, s>>>(st, na, chunk, maps, cst, seq,
                                                                  dev_uniforms_sorted, shots, dev_basis);
     k_leftover<<<1, 256, 0, s>>>(cst, nchunks, dev_uniforms_sorted, shots, na - 1, dev_basis);
-    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    return launch_status();
 }
 
 int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,

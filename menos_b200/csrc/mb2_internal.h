@@ -237,6 +237,9 @@ int launch_pauli_group(const void* amps, uint32_t n, uint32_t c, uint32_t d, con
                        uint32_t grid, void* stream, int precision);
 int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const uint64_t* dev_x,
                               const uint64_t* dev_z, uint32_t num_terms, double* dev_out, void* stream);
+// MB2_OK after a clean launch, else MB2_ERR_CUDA with the error kept for
+// last_cuda_error_string() (which reports and clears it).
+int launch_status();
 const char* last_cuda_error_string();
 // Counts kernels this library launched (process-wide; mb2_kernel_launches).
 void note_launches(uint32_t k);

@@ -561,16 +561,22 @@ __global__ void __launch_bounds__(MAXT, MINB)
 // Launches one instance; the shared-memory limit is raised once per instance.
 template <int MAXT, int MINB, int MT, typename IDX>
 int launch_instance(const TileLaunch& L) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_tile_pass<MAXT, MINB, MT, IDX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(kTileSmemMax));
-        attr_set = true;
+    // The dynamic limit is what the static shared memory leaves of the
+    // per-block maximum (a larger request is refused by the driver).
+    static size_t dyn_max = 0;
+    if (dyn_max == 0) {
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, k_tile_pass<MAXT, MINB, MT, IDX>) != cudaSuccess) return launch_status();
+        dyn_max = kTileSmemMax - fa.sharedSizeBytes;
+        if (cudaFuncSetAttribute(k_tile_pass<MAXT, MINB, MT, IDX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(dyn_max)) != cudaSuccess)
+            return launch_status();
     }
+    if (L.smem > dyn_max) return MB2_ERR_INVALID;
     k_tile_pass<MAXT, MINB, MT, IDX><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
         static_cast<double2*>(L.amps), L.n_all, L.m, L.smask, L.prog, L.nprog, L.sdata, L.nsdata, L.gdata, L.ntiles,
         L.pdata, L.pstride, L.bshift, L.stages);
-    return cudaGetLastError() == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    return launch_status();
 }
 
 }  // namespace tile
