@@ -172,7 +172,7 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     if (cudaStreamCreateWithFlags(&r.stream, cudaStreamNonBlocking) != cudaSuccess) return MB2_ERR_CUDA;
     const size_t state_bytes = (size_t{num_bindings} << num_qubits) * sizeof(mb2::Cd);
     auto al = [](size_t v) { return (v + 255) & ~size_t{255}; };
-    const size_t ib = prog.instrs.size() * sizeof(mb2::TileInstr), sb = prog.data.size() * 8,
+    const size_t ib = prog.words.size() * sizeof(uint32_t), sb = prog.data.size() * 8,
                  gb = prog.gdata.size() * 8, pb = pdata.size() * 8, tb = size_t{num_terms} * 8;
     const size_t o_s = al(ib), o_g = o_s + al(sb), o_p = o_g + al(gb), o_x = o_p + al(pb), o_z = o_x + al(tb),
                  o_c = o_z + al(tb), o_o = o_c + al(tb), total = o_o + al(size_t{num_bindings} * 8);
@@ -182,7 +182,7 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     }
     auto* w = static_cast<unsigned char*>(r.work);
     std::vector<unsigned char> host(o_o, 0);
-    std::memcpy(host.data(), prog.instrs.data(), ib);
+    std::memcpy(host.data(), prog.words.data(), ib);
     if (sb) std::memcpy(host.data() + o_s, prog.data.data(), sb);
     if (gb) std::memcpy(host.data() + o_g, prog.gdata.data(), gb);
     std::memcpy(host.data() + o_p, pdata.data(), pb);
@@ -203,7 +203,7 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     layout.pdata = reinterpret_cast<const double*>(w + o_p);
     layout.pstride = static_cast<uint32_t>(stride);
     for (const mb2::TilePass& pass : prog.passes) {
-        if (mb2::launch_tile_pass(r.state, num_qubits, pass, reinterpret_cast<const mb2::TileInstr*>(w),
+        if (mb2::launch_tile_pass(r.state, num_qubits, pass, reinterpret_cast<const uint32_t*>(w),
                                   reinterpret_cast<const double*>(w + o_s), reinterpret_cast<const double*>(w + o_g),
                                   sm, r.stream, &layout) != MB2_OK)
             return MB2_ERR_CUDA;

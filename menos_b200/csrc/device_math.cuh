@@ -28,10 +28,16 @@ __device__ __forceinline__ double canon1(double v) {
     return __hiloint2double((lo == 0 && hi == static_cast<int>(0x80000000u)) ? 0 : hi, lo);
 }
 __device__ __forceinline__ double2 canon(double2 v) { return make_double2(canon1(v.x), canon1(v.y)); }
-__device__ __forceinline__ double2 cneg(double2 v) {
-    return make_double2(__longlong_as_double(__double_as_longlong(v.x) ^ static_cast<long long>(0x8000000000000000ULL)),
-                        __longlong_as_double(__double_as_longlong(v.y) ^ static_cast<long long>(0x8000000000000000ULL)));
+// v negated when flip is 1: the sign bits flipped with an integer XOR (no
+// FP64 issue, and exact for every value).
+__device__ __forceinline__ double2 cneg_if(double2 v, uint32_t flip) {
+    const uint32_t msk = flip << 31;
+    int hx = __double2hiint(v.x), hy = __double2hiint(v.y);
+    asm("xor.b32 %0, %0, %1;" : "+r"(hx) : "r"(msk));
+    asm("xor.b32 %0, %0, %1;" : "+r"(hy) : "r"(msk));
+    return make_double2(__hiloint2double(hx, __double2loint(v.x)), __hiloint2double(hy, __double2loint(v.y)));
 }
+__device__ __forceinline__ double2 cneg(double2 v) { return cneg_if(v, 1u); }
 // d * a for one diagonal / monomial entry, exact up to a zero's sign:
 // (1, 0) -> a, (-1, 0) -> -a, else the full product.
 __device__ __forceinline__ double2 scale_entry(double dr, double di, double2 a) {

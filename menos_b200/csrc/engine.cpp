@@ -364,19 +364,22 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     } catch (const std::exception& e) {
         return fail(s->ctx, MB2_ERR_INVALID, e.what());
     }
-    const size_t ibytes = prog.instrs.size() * sizeof(mb2::TileInstr);
+    // One upload: the program (complex64: TileInstr records; complex128: the
+    // compact word stream), staged data, global-only data (256-byte aligned parts).
+    const size_t ibytes = c64 ? prog.instrs.size() * sizeof(mb2::TileInstr) : prog.words.size() * sizeof(uint32_t);
     const size_t dbytes = prog.data.size() * sizeof(double);
     const size_t gbytes = prog.gdata.size() * sizeof(double);
-    // One upload: instructions, staged data, global-only data (256-byte aligned parts).
     const size_t doff = (ibytes + 255) & ~size_t{255};
     const size_t goff = (doff + dbytes + 255) & ~size_t{255};
     if (int e = ensure_scratch(s, goff + gbytes + 256); e != MB2_OK) return e;
     std::vector<unsigned char> host(goff + gbytes);
-    std::memcpy(host.data(), prog.instrs.data(), ibytes);
+    if (c64) std::memcpy(host.data(), prog.instrs.data(), ibytes);
+    else std::memcpy(host.data(), prog.words.data(), ibytes);
     if (dbytes) std::memcpy(host.data() + doff, prog.data.data(), dbytes);
     if (gbytes) std::memcpy(host.data() + goff, prog.gdata.data(), gbytes);
     MB2_CUDA(s->ctx, cudaMemcpyAsync(s->scratch, host.data(), host.size(), cudaMemcpyHostToDevice, s->stream));
     const auto* dev_instrs = static_cast<const mb2::TileInstr*>(s->scratch);
+    const auto* dev_words = static_cast<const uint32_t*>(s->scratch);
     const auto* dev_sdata = reinterpret_cast<const double*>(static_cast<unsigned char*>(s->scratch) + doff);
     const auto* dev_gdata = reinterpret_cast<const double*>(static_cast<unsigned char*>(s->scratch) + goff);
     s->stats.fp64_ops_per_amp = prog.fp64_per_amp;
@@ -384,7 +387,7 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     for (const mb2::TilePass& pass : prog.passes) {
         const int rc = c64 ? mb2::launch_tile_pass_c64(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata,
                                                        s->ctx->sm_count, s->stream)
-                           : mb2::launch_tile_pass(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata,
+                           : mb2::launch_tile_pass(s->amps, s->n, pass, dev_words, dev_sdata, dev_gdata,
                                                    s->ctx->sm_count, s->stream);
         if (rc != MB2_OK) return fail(s->ctx, rc, std::string("tile pass launch: ") + mb2::last_cuda_error_string());
         s->stats.passes += 1;
@@ -424,7 +427,7 @@ int mb2_estimate_sweep(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
             const mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m);
             out->passes = prog.passes.size();
             out->launches = prog.passes.size() + 1;
-            out->h2d_bytes = prog.instrs.size() * sizeof(mb2::TileInstr) + (prog.data.size() + prog.gdata.size()) * sizeof(double);
+            out->h2d_bytes = prog.words.size() * sizeof(uint32_t) + (prog.data.size() + prog.gdata.size()) * sizeof(double);
             out->fp64_ops_per_amp = prog.fp64_per_amp;
         }
         out->device_bytes += out->h2d_bytes;

@@ -223,23 +223,25 @@ int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, 
     return launch_status();
 }
 
-int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
+int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
                      const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
                      const BatchLayout* batch) {
     if (pass.m > kMaxTileQubits || pass.m < kMinTileQubits) return MB2_ERR_INVALID;
-    const size_t staged = size_t{pass.prog_count} * sizeof(TileInstr) + size_t{pass.sdata_count} * sizeof(double);
-    if (staged > kMaxStagedBytes) return MB2_ERR_INVALID;
+    if ((pass.word_count & 3u) != 0 || (pass.param_len != 0 && batch == nullptr)) return MB2_ERR_INVALID;
+    const size_t staged = size_t{pass.word_count} * 4 + (size_t{pass.sdata_count} + pass.param_len) * sizeof(double);
     TileLaunch L;
     L.amps = amps;
     L.m = pass.m;
     L.smask = pass.smask;
-    L.prog = dev_instrs + pass.prog_begin;
-    L.nprog = pass.prog_count;
+    L.words = dev_words + pass.word_begin;
+    L.nwords = pass.word_count;
     L.sdata = dev_sdata + pass.sdata_begin;
     L.nsdata = pass.sdata_count;
     L.gdata = dev_gdata;
     L.pdata = batch ? batch->pdata : nullptr;
     L.pstride = batch ? batch->pstride : 0u;
+    L.param_lo = pass.param_lo;
+    L.param_len = pass.param_len;
     L.bshift = n - pass.m;
     L.stream = stream;
     L.threads = 1u << (pass.m - kRegQubits);

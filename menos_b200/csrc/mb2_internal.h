@@ -93,7 +93,49 @@ struct TilePass {
     uint32_t sdata_begin = 0;  // this pass's staged data (doubles), copied to shared memory
     uint32_t sdata_count = 0;
     uint32_t gates = 0;      // blocks applied in this pass
+    // The complex128 kernel's compact stream (tile_encode.cpp).
+    uint32_t word_begin = 0;
+    uint32_t word_count = 0;
+    // Parametric data this pass reads from a binding's record: doubles
+    // [param_lo, param_lo + param_len), staged after the pass's data.
+    uint32_t param_lo = 0;
+    uint32_t param_len = 0;
 };
+
+// Compact instruction stream of the complex128 tile kernel, written from the
+// TileInstr list by encode_compact (tile_encode.cpp).  A header word holds
+//   bits 0-7 the opcode, 8-15 aux, 16-19 a thread tile bit, 20-31 the data
+//   offset in 16-byte units from the start of the pass's staged data;
+// some opcodes take extra words.  Register-slot operands are part of the
+// opcode, so a gate is one jump.  Ordered slot pairs (p0, p1), p0 != p1, are
+// numbered p0 * 3 + (p1 < p0 ? p1 : p1 - 1).
+namespace cop {
+constexpr uint32_t kEnd = 0;     // end of a phase
+constexpr uint32_t kU3 = 1;      // + slot
+constexpr uint32_t kGen1 = 5;    // + slot
+constexpr uint32_t kReal1 = 9;   // + slot
+constexpr uint32_t kMono1 = 13;  // + slot; aux = source rows (3 bits each)
+constexpr uint32_t kX1 = 17;     // + slot
+constexpr uint32_t kGen2 = 21;   // + pair
+constexpr uint32_t kMono2 = 33;  // + pair; extra word = source rows (3 bits each)
+constexpr uint32_t kSw12 = 45;   // + pair
+constexpr uint32_t kSw13 = 57;   // + pair
+constexpr uint32_t kSw23 = 69;   // + pair
+constexpr uint32_t kDs1R = 81;   // + slot; aux = entry classes
+constexpr uint32_t kDs1T = 85;   // aux = classes; the operand's tile bit in bits 16-19
+constexpr uint32_t kDs2RR = 86;  // + pair; aux = classes
+constexpr uint32_t kDs2RT = 98;  // + 2 * slot + (index of the thread-bit operand); tile bit in bits 16-19
+constexpr uint32_t kDs2TT = 106; // aux = classes; extra word = the two tile bits (4 bits each)
+constexpr uint32_t kDiagK = 107; // aux = k; extra word = tile positions (4 bits each)
+constexpr uint32_t kSigns = 108; // aux = monomial count; one word per monomial
+constexpr uint32_t kPhase = 200; // aux = thread bits; bits 16-31 register positions; 2 words of tperm
+constexpr uint32_t kSmem = 201;  // aux = k; extra words: tile positions, gdata offset (doubles)
+// A sign monomial: six 5-bit sources, 31 = none, 16 + s = register slot s,
+// else a tile bit (a thread bit in that phase).  The amplitudes whose
+// sources are all 1 change sign.
+constexpr uint32_t kSrcNone = 31;
+constexpr uint32_t kSrcReg = 16;
+}  // namespace cop
 
 // Shared-memory budget of one pass's staged instructions + data.
 constexpr size_t kMaxStagedBytes = 32 * 1024;
@@ -110,8 +152,11 @@ struct TileProgram {
     uint32_t param_stride = 0;            // doubles per binding record
     std::vector<TileInstr> instrs;
     std::vector<double> data;
-    uint64_t fp64_per_amp = 0;  // modelled FP64 instructions per amplitude
+    std::vector<uint32_t> words;  // compact stream of every pass (complex128 kernel)
+    uint64_t fp64_per_amp = 0;    // modelled FP64 instructions per amplitude
 };
+// Writes prog.words and each pass's word range and parametric slice.
+void encode_compact(TileProgram& prog);
 
 // Register qubits per thread in the tile kernel (16 amplitudes per thread).
 constexpr uint32_t kRegQubits = 4;
@@ -149,7 +194,7 @@ struct BatchLayout {
     const double* pdata = nullptr;
     uint32_t pstride = 0;
 };
-int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
+int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
                      const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
                      const BatchLayout* batch = nullptr);
 // One tile-pass launch, as the instances (kernels_tile_*.cu) take it.
@@ -158,14 +203,16 @@ struct TileLaunch {
     uint32_t n_all = 0;  // index bits, bindings included
     uint32_t m = 0;
     uint64_t smask = 0;
-    const TileInstr* prog = nullptr;
-    uint32_t nprog = 0;
+    const uint32_t* words = nullptr;
+    uint32_t nwords = 0;
     const double* sdata = nullptr;
     uint32_t nsdata = 0;
     const double* gdata = nullptr;
     uint64_t ntiles = 0;
     const double* pdata = nullptr;
     uint32_t pstride = 0;
+    uint32_t param_lo = 0;
+    uint32_t param_len = 0;
     uint32_t bshift = 0;
     uint32_t stages = 2;
     int grid = 0;

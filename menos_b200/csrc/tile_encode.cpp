@@ -1,0 +1,210 @@
+// Encoder of the complex128 tile kernel's compact instruction stream (the
+// format is described with the opcodes in mb2_internal.h).
+//
+// Besides the one-to-one translation of the planned instructions, one rewrite
+// is made: a run of consecutive diagonal blocks whose entries are all +1 or
+// -1 becomes one sign instruction.  Such a block only flips the sign of the
+// amplitudes where a boolean function of its operand bits is 1; written in
+// algebraic normal form that function is an XOR of AND-monomials, and the
+// blocks of a run compose by XOR-ing their monomials (pairs cancel).
+// Negation is exact and sign flips commute, so the state is the one the
+// blocks give one by one (up to the sign of zero results, which the store
+// normalises, as for every specialisation of the per-gate arithmetic).
+#include <algorithm>
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <vector>
+
+#include "mb2_internal.h"
+
+namespace mb2 {
+namespace {
+
+uint32_t pair_index(uint32_t p0, uint32_t p1) { return p0 * 3 + (p1 < p0 ? p1 : p1 - 1); }
+
+uint32_t header(uint32_t op, uint32_t aux, uint32_t tbit, uint32_t off_doubles) {
+    if (off_doubles & 1u) throw std::logic_error("staged data offset is not 16-byte aligned");
+    const uint32_t off = off_doubles / 2;
+    if (off >= 4096u || aux > 255u || tbit > 15u)
+        throw std::invalid_argument("pass data beyond the compact stream's reach");
+    return op | (aux << 8) | (tbit << 16) | (off << 20);
+}
+
+bool is_param(const TileInstr& g) { return g.op != TOP_PHASE && g.op != TOP_END && g.nthread != 0; }
+
+// Doubles of a parametric instruction's per-binding record.
+uint32_t param_doubles(const TileInstr& g) {
+    const uint32_t dim = 1u << g.k;
+    return g.op == TOP_DIAG ? 2 * dim : 2 * dim * dim;
+}
+
+}  // namespace
+
+void encode_compact(TileProgram& prog) {
+    prog.words.clear();
+    for (TilePass& pass : prog.passes) {
+        pass.word_begin = static_cast<uint32_t>(prog.words.size());
+        const TileInstr* ins = prog.instrs.data() + pass.prog_begin;
+        const double* sdata = prog.data.data() + pass.sdata_begin;
+        // The parametric slice this pass reads.
+        uint32_t lo = UINT32_MAX, hi = 0;
+        for (uint32_t i = 0; i < pass.prog_count; ++i)
+            if (is_param(ins[i])) {
+                lo = std::min(lo, ins[i].data);
+                hi = std::max(hi, ins[i].data + param_doubles(ins[i]));
+            }
+        pass.param_lo = lo == UINT32_MAX ? 0u : lo;
+        pass.param_len = lo == UINT32_MAX ? 0u : hi - lo;
+        auto data_off = [&](const TileInstr& g) {
+            return is_param(g) ? pass.sdata_count + (g.data - pass.param_lo) : g.data;
+        };
+        auto& w = prog.words;
+        uint32_t reg[kRegQubits] = {0, 1, 2, 3};
+        // Pending sign monomials (canonical words), toggled so pairs cancel.
+        std::map<uint32_t, bool> signs;
+        auto flush_signs = [&]() {
+            std::vector<uint32_t> live;
+            for (const auto& [mono, on] : signs)
+                if (on) live.push_back(mono);
+            signs.clear();
+            for (size_t i = 0; i < live.size(); i += 255) {
+                const uint32_t cnt = static_cast<uint32_t>(std::min<size_t>(255, live.size() - i));
+                w.push_back(header(cop::kSigns, cnt, 0, 0));
+                w.insert(w.end(), live.begin() + static_cast<long>(i), live.begin() + static_cast<long>(i + cnt));
+            }
+        };
+        // Source code of tile position p in the current phase.
+        auto source_of = [&](uint32_t p) -> uint32_t {
+            for (uint32_t s = 0; s < kRegQubits; ++s)
+                if (reg[s] == p) return cop::kSrcReg + s;
+            return p;
+        };
+        // Adds the sign function of a +-1 diagonal (neg[e]: entry e is -1)
+        // on tile positions pos[0..k-1].
+        auto add_signs = [&](uint32_t k, const uint32_t* pos, const std::vector<uint8_t>& neg) {
+            const uint32_t dim = 1u << k;
+            std::vector<uint8_t> c(neg);
+            for (uint32_t i = 0; i < k; ++i)
+                for (uint32_t s = 0; s < dim; ++s)
+                    if (s & (1u << i)) c[s] ^= c[s ^ (1u << i)];
+            for (uint32_t s = 0; s < dim; ++s) {
+                if (!c[s]) continue;
+                std::vector<uint32_t> src;
+                for (uint32_t t = 0; t < k; ++t)
+                    if (s & (1u << t)) src.push_back(source_of(pos[t]));
+                std::sort(src.begin(), src.end());
+                uint32_t mono = 0;
+                for (uint32_t f = 0; f < 6; ++f)
+                    mono |= (f < src.size() ? src[f] : cop::kSrcNone) << (5 * f);
+                signs[mono] = !signs[mono];
+            }
+        };
+        for (uint32_t i = 0; i < pass.prog_count; ++i) {
+            const TileInstr& g = ins[i];
+            if (g.op == TOP_DIAG && !is_param(g)) {
+                const uint32_t dim = 1u << g.k;
+                std::vector<uint8_t> neg(dim, 0);
+                bool pm1 = true;
+                for (uint32_t e = 0; e < dim && pm1; ++e) {
+                    const double re = sdata[g.data + 2 * e], im = sdata[g.data + 2 * e + 1];
+                    if (im != 0.0 || (re != 1.0 && re != -1.0)) pm1 = false;
+                    neg[e] = re == -1.0;
+                }
+                if (pm1) {
+                    uint32_t pos[8];
+                    for (uint32_t t = 0; t < g.k; ++t) pos[t] = g.pos[t];
+                    add_signs(g.k, pos, neg);
+                    continue;
+                }
+            }
+            flush_signs();
+            const uint32_t off = (g.op == TOP_PHASE || g.op == TOP_END || g.op == TOP_SMEM) ? 0u : data_off(g);
+            switch (g.op) {
+                case TOP_PHASE: {
+                    uint32_t packed = 0;
+                    for (uint32_t s = 0; s < kRegQubits; ++s) {
+                        reg[s] = g.pos[s];
+                        packed |= static_cast<uint32_t>(g.pos[s]) << (4 * s);
+                    }
+                    w.push_back(cop::kPhase | (static_cast<uint32_t>(g.nthread) << 8) | (packed << 16));
+                    uint32_t t0 = 0, t1 = 0;
+                    for (uint32_t t = 0; t < 8; ++t) t0 |= static_cast<uint32_t>(g.tperm[t] & 15u) << (4 * t);
+                    for (uint32_t t = 8; t < 12; ++t) t1 |= static_cast<uint32_t>(g.tperm[t] & 15u) << (4 * (t - 8));
+                    w.push_back(t0);
+                    w.push_back(t1);
+                    break;
+                }
+                case TOP_END:
+                    w.push_back(cop::kEnd);
+                    break;
+                case TOP_SMEM: {
+                    uint32_t packed = 0;
+                    for (uint32_t t = 0; t < g.k; ++t) packed |= static_cast<uint32_t>(g.pos[t]) << (4 * t);
+                    w.push_back(cop::kSmem | (static_cast<uint32_t>(g.k) << 8));
+                    w.push_back(packed);
+                    w.push_back(g.data);
+                    break;
+                }
+                case TOP_G1: {
+                    const uint32_t p = g.pos[0];
+                    switch (g.kind) {
+                        case TK_U3: w.push_back(header(cop::kU3 + p, 0, 0, off)); break;
+                        case TK_REAL: w.push_back(header(cop::kReal1 + p, 0, 0, off)); break;
+                        case TK_X: w.push_back(header(cop::kX1 + p, 0, 0, 0)); break;
+                        case TK_MONO: w.push_back(header(cop::kMono1 + p, g.aux & 63u, 0, off)); break;
+                        default: w.push_back(header(cop::kGen1 + p, 0, 0, off)); break;
+                    }
+                    break;
+                }
+                case TOP_G2: {
+                    const uint32_t pr = pair_index(g.pos[0], g.pos[1]);
+                    switch (g.kind) {
+                        case TK_SW12: w.push_back(header(cop::kSw12 + pr, 0, 0, 0)); break;
+                        case TK_SW13: w.push_back(header(cop::kSw13 + pr, 0, 0, 0)); break;
+                        case TK_SW23: w.push_back(header(cop::kSw23 + pr, 0, 0, 0)); break;
+                        case TK_MONO:
+                            w.push_back(header(cop::kMono2 + pr, 0, 0, off));
+                            w.push_back(g.aux);
+                            break;
+                        default: w.push_back(header(cop::kGen2 + pr, 0, 0, off)); break;
+                    }
+                    break;
+                }
+                case TOP_DIAG: {
+                    if (g.kind == TK_DSMALL) {
+                        const uint32_t c0 = g.pos[4], c1 = g.pos[5];
+                        const bool r0 = (c0 & 0x80u) != 0, r1 = (c1 & 0x80u) != 0;
+                        const uint32_t cls = g.aux & 255u;
+                        if (g.k == 1) {
+                            if (r0) w.push_back(header(cop::kDs1R + (c0 & 3u), cls, 0, off));
+                            else w.push_back(header(cop::kDs1T, cls, c0, off));
+                        } else if (r0 && r1) {
+                            w.push_back(header(cop::kDs2RR + pair_index(c0 & 3u, c1 & 3u), cls, 0, off));
+                        } else if (r0) {
+                            w.push_back(header(cop::kDs2RT + 2 * (c0 & 3u) + 1, cls, c1, off));
+                        } else if (r1) {
+                            w.push_back(header(cop::kDs2RT + 2 * (c1 & 3u), cls, c0, off));
+                        } else {
+                            w.push_back(header(cop::kDs2TT, cls, 0, off));
+                            w.push_back(c0 | (c1 << 4));
+                        }
+                    } else {
+                        uint32_t packed = 0;
+                        for (uint32_t t = 0; t < g.k; ++t) packed |= static_cast<uint32_t>(g.pos[t]) << (4 * t);
+                        w.push_back(header(cop::kDiagK, g.k, 0, off));
+                        w.push_back(packed);
+                    }
+                    break;
+                }
+                default:
+                    throw std::logic_error("unknown tile instruction");
+            }
+        }
+        flush_signs();
+        while (w.size() & 3u) w.push_back(cop::kEnd);  // 16-byte multiple: the staged data follows
+        pass.word_count = static_cast<uint32_t>(w.size()) - pass.word_begin;
+    }
+}
+
+}  // namespace mb2

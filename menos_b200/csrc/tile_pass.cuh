@@ -28,33 +28,6 @@ __host__ __device__ __forceinline__ constexpr uint32_t swz(uint32_t l) {
     return l ^ ((h ^ (h >> 3) ^ (h >> 6) ^ (h >> 9)) & 7u);
 }
 
-// A TileInstr read as four 64-bit words (fields extracted by shifts, so no
-// field is ever indexed dynamically in local memory).  Layout: bytes 0-3 op,
-// k, kind, nthread; 4-11 pos[8]; 12-15 data; 16-27 tperm[12]; 28-31 aux.
-struct DI {
-    uint64_t w0, w1, w2, w3;
-    __device__ __forceinline__ uint32_t op() const { return static_cast<uint32_t>(w0 & 0xffu); }
-    __device__ __forceinline__ uint32_t k() const { return static_cast<uint32_t>((w0 >> 8) & 0xffu); }
-    __device__ __forceinline__ uint32_t kind() const { return static_cast<uint32_t>((w0 >> 16) & 0xffu); }
-    __device__ __forceinline__ uint32_t nthread() const { return static_cast<uint32_t>((w0 >> 24) & 0xffu); }
-    __device__ __forceinline__ uint32_t pos(uint32_t b) const {
-        return static_cast<uint32_t>((b < 4 ? (w0 >> (32 + 8 * b)) : (w1 >> (8 * (b - 4)))) & 0xffu);
-    }
-    __device__ __forceinline__ uint32_t data() const { return static_cast<uint32_t>(w1 >> 32); }
-    __device__ __forceinline__ uint32_t tperm(uint32_t i) const {
-        return static_cast<uint32_t>((i < 8 ? (w2 >> (8 * i)) : (w3 >> (8 * (i - 8)))) & 0xffu);
-    }
-    __device__ __forceinline__ uint32_t aux() const { return static_cast<uint32_t>(w3 >> 32); }
-};
-
-// Reads one instruction from the pass program staged in shared memory
-// (a plain load: the program is not in the global address space).
-__device__ __forceinline__ DI load_instr(const TileInstr* p) {
-    const ulonglong2* s = reinterpret_cast<const ulonglong2*>(p);
-    const ulonglong2 a = s[0], b = s[1];
-    return DI{a.x, a.y, b.x, b.y};
-}
-
 constexpr int kR = static_cast<int>(kRegQubits);  // register qubits per thread
 constexpr int kNA = 1 << kR;                         // amplitudes per thread
 static_assert(kR == 4, "the register-slot dispatch below is written for 4 register qubits");
@@ -134,36 +107,6 @@ __device__ __forceinline__ void g2(double2 (&a)[kNA], const double* md, uint32_t
     }
 }
 
-template <int KIND>
-__device__ __forceinline__ void dispatch_g1(int p, double2 (&a)[kNA], const double* md, uint32_t aux) {
-    switch (p) {
-        case 0: g1<0, KIND>(a, md, aux); break;
-        case 1: g1<1, KIND>(a, md, aux); break;
-        case 2: g1<2, KIND>(a, md, aux); break;
-        default: g1<3, KIND>(a, md, aux); break;
-    }
-}
-
-template <int P0, int KIND>
-__device__ __forceinline__ void dispatch_g2b(int p1, double2 (&a)[kNA], const double* md, uint32_t aux) {
-    switch (p1) {
-        case 0: g2<P0, 0, KIND>(a, md, aux); break;
-        case 1: g2<P0, 1, KIND>(a, md, aux); break;
-        case 2: g2<P0, 2, KIND>(a, md, aux); break;
-        default: g2<P0, 3, KIND>(a, md, aux); break;
-    }
-}
-
-template <int KIND>
-__device__ __forceinline__ void dispatch_g2(int p0, int p1, double2 (&a)[kNA], const double* md, uint32_t aux) {
-    switch (p0) {
-        case 0: dispatch_g2b<0, KIND>(p1, a, md, aux); break;
-        case 1: dispatch_g2b<1, KIND>(p1, a, md, aux); break;
-        case 2: dispatch_g2b<2, KIND>(p1, a, md, aux); break;
-        default: dispatch_g2b<3, KIND>(p1, a, md, aux); break;
-    }
-}
-
 // A diagonal block of k <= 2 qubits in registers.  Each operand is either
 // a register slot (its bit over j is known at compile time in the templates
 // below) or a thread bit (one value for all 16 amplitudes).  The entry of
@@ -175,6 +118,18 @@ struct Diag4 {
     double2 d[4];
     uint32_t aux;
 };
+
+// The entries of a k <= 2 diagonal (k = 1: entries 2 and 3 repeat 0 and 1,
+// which only the k = 1 paths' selectors never reach) with its classes.
+__device__ __forceinline__ Diag4 load_diag(const double* md, uint32_t k, uint32_t aux) {
+    Diag4 D;
+    D.aux = aux;
+    D.d[0] = reinterpret_cast<const double2*>(md)[0];
+    D.d[1] = reinterpret_cast<const double2*>(md)[1];
+    D.d[2] = k > 1 ? reinterpret_cast<const double2*>(md)[2] : D.d[0];
+    D.d[3] = k > 1 ? reinterpret_cast<const double2*>(md)[3] : D.d[1];
+    return D;
+}
 
 __device__ __forceinline__ double2 diag_entry(const Diag4& D, uint32_t e) {
     return (e & 2u) ? ((e & 1u) ? D.d[3] : D.d[2]) : ((e & 1u) ? D.d[1] : D.d[0]);
@@ -219,62 +174,6 @@ __device__ __forceinline__ void diag_rt(double2 (&a)[kNA], const Diag4& D, uint3
     }
 }
 
-__device__ __forceinline__ void diag_small(double2 (&a)[kNA], const double* md, uint32_t k, uint32_t aux, int s0,
-                                           int s1, uint32_t t0, uint32_t t1) {
-    // s0/s1: register slot of operand 0/1, or -1 for a thread bit of value t0/t1.
-    Diag4 D;
-    D.aux = aux;
-    D.d[0] = reinterpret_cast<const double2*>(md)[0];
-    D.d[1] = reinterpret_cast<const double2*>(md)[1];
-    D.d[2] = k > 1 ? reinterpret_cast<const double2*>(md)[2] : D.d[0];
-    D.d[3] = k > 1 ? reinterpret_cast<const double2*>(md)[3] : D.d[1];
-    if (k == 1) {
-        if (s0 < 0) {
-            diag_set<-1, -1>(a, (aux >> (2 * t0)) & 3u, diag_entry(D, t0), 0, 0);
-            return;
-        }
-        switch (s0) {
-            case 0: diag_rr<0, -1>(a, D); break;
-            case 1: diag_rr<1, -1>(a, D); break;
-            case 2: diag_rr<2, -1>(a, D); break;
-            default: diag_rr<3, -1>(a, D); break;
-        }
-        return;
-    }
-    if (s0 >= 0 && s1 >= 0) {
-        switch (s0 * 4 + s1) {
-            case 1: diag_rr<0, 1>(a, D); break;
-            case 2: diag_rr<0, 2>(a, D); break;
-            case 3: diag_rr<0, 3>(a, D); break;
-            case 4: diag_rr<1, 0>(a, D); break;
-            case 6: diag_rr<1, 2>(a, D); break;
-            case 7: diag_rr<1, 3>(a, D); break;
-            case 8: diag_rr<2, 0>(a, D); break;
-            case 9: diag_rr<2, 1>(a, D); break;
-            case 11: diag_rr<2, 3>(a, D); break;
-            case 12: diag_rr<3, 0>(a, D); break;
-            case 13: diag_rr<3, 1>(a, D); break;
-            case 14: diag_rr<3, 2>(a, D); break;
-            default: break;
-        }
-        return;
-    }
-    if (s0 < 0 && s1 < 0) {
-        const uint32_t e = t0 | (t1 << 1);
-        diag_set<-1, -1>(a, (aux >> (2 * e)) & 3u, diag_entry(D, e), 0, 0);
-        return;
-    }
-    const int s = s0 >= 0 ? s0 : s1;
-    const uint32_t shift = s0 >= 0 ? 0u : 1u;
-    const uint32_t tv = s0 >= 0 ? t1 : t0;
-    switch (s) {
-        case 0: diag_rt<0>(a, D, shift, tv); break;
-        case 1: diag_rt<1>(a, D, shift, tv); break;
-        case 2: diag_rt<2>(a, D, shift, tv); break;
-        default: diag_rt<3>(a, D, shift, tv); break;
-    }
-}
-
 // Exact permutations (every nonzero entry (1,0)): register moves only.
 // TK_X: 1q swap; TK_SW12 / TK_SW13 / TK_SW23: 2q, exchange local indices
 // (1,2) (SWAP), (1,3) (CX, control = operand 0), (2,3) (CX, control = operand 1).
@@ -308,25 +207,6 @@ __device__ __forceinline__ void perm2(double2 (&a)[kNA]) {
     }
 }
 
-template <int KIND>
-__device__ __forceinline__ void dispatch_perm2(int p0, int p1, double2 (&a)[kNA]) {
-    switch (p0 * 4 + p1) {
-        case 1: perm2<0, 1, KIND>(a); break;
-        case 2: perm2<0, 2, KIND>(a); break;
-        case 3: perm2<0, 3, KIND>(a); break;
-        case 4: perm2<1, 0, KIND>(a); break;
-        case 6: perm2<1, 2, KIND>(a); break;
-        case 7: perm2<1, 3, KIND>(a); break;
-        case 8: perm2<2, 0, KIND>(a); break;
-        case 9: perm2<2, 1, KIND>(a); break;
-        case 11: perm2<2, 3, KIND>(a); break;
-        case 12: perm2<3, 0, KIND>(a); break;
-        case 13: perm2<3, 1, KIND>(a); break;
-        case 14: perm2<3, 2, KIND>(a); break;
-        default: break;
-    }
-}
-
 // cp.async of one 16-byte amplitude, global -> shared (L2 only, no L1).
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
@@ -352,18 +232,20 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <int MAXT, int MINB, int MT, typename IDX>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask,
-                const TileInstr* __restrict__ prog, uint32_t nprog, const double* __restrict__ sdata,
+                const uint32_t* __restrict__ words, uint32_t nwords, const double* __restrict__ sdata,
                 uint32_t nsdata, const double* __restrict__ gdata, uint64_t ntiles, const double* __restrict__ pdata,
-                uint32_t pstride, uint32_t bshift, uint32_t stages) {
+                uint32_t pstride, uint32_t param_lo, uint32_t param_len, uint32_t bshift, uint32_t stages) {
     extern __shared__ double2 smem_tiles[];
     const uint32_t m = MT > 0 ? static_cast<uint32_t>(MT) : m_rt;
     const uint32_t tid = threadIdx.x;
     const uint32_t tbits = m - kRegQubits;
     const uint32_t tile_amps = 1u << m;
-    TileInstr* sprog = reinterpret_cast<TileInstr*>(smem_tiles + stages * tile_amps);
-    double* sd = reinterpret_cast<double*>(sprog + nprog);
-    for (uint32_t i = tid; i < nprog * 2; i += blockDim.x)
-        reinterpret_cast<ulonglong2*>(sprog)[i] = __ldg(reinterpret_cast<const ulonglong2*>(prog) + i);
+    // Shared memory: tile buffers, the pass's words (a multiple of four),
+    // its staged data, then the parametric slice of the current tile's binding.
+    uint32_t* sw = reinterpret_cast<uint32_t*>(smem_tiles + stages * tile_amps);
+    double* sd = reinterpret_cast<double*>(sw + nwords);
+    for (uint32_t i = tid; i < nwords / 4; i += blockDim.x)
+        reinterpret_cast<uint4*>(sw)[i] = __ldg(reinterpret_cast<const uint4*>(words) + i);
     for (uint32_t i = tid; i < nsdata; i += blockDim.x) sd[i] = __ldg(sdata + i);
     // Canonical (load/store) mapping: thread bits = tile bits 0..tbits-1,
     // register bits = tile bits tbits..m-1.
@@ -426,27 +308,36 @@ __global__ void __launch_bounds__(MAXT, MINB)
         pbase = advance(pbase);
         cur = cur + 1 == stages ? 0u : cur + 1;
         nxt = nxt + 1 == stages ? 0u : nxt + 1;
+        if (param_len != 0) {  // a batched sweep: this tile's binding is t >> bshift
+            const double2* src = reinterpret_cast<const double2*>(pdata + (t >> bshift) * pstride + param_lo);
+            double2* dst = reinterpret_cast<double2*>(sd + nsdata);
+            for (uint32_t i = tid; i < param_len / 2; i += blockDim.x) dst[i] = __ldg(src + i);
+        }
         if (stages == 3) cp_async_wait<2>();
         else cp_async_wait<1>();
         __syncthreads();
 
         double2 a[kNA];
         uint32_t pc = 0;
-        while (pc < nprog) {
-            const DI I = load_instr(sprog + pc);
-            ++pc;
-            if (I.op() == TOP_PHASE) {
+        while (pc < nwords) {
+            const uint32_t w0 = sw[pc];
+            const uint32_t op0 = w0 & 0xffu;
+            if (op0 == cop::kPhase) {
+                const uint32_t tp0 = sw[pc + 1], tp1 = sw[pc + 2];
+                pc += 3;
+                const uint32_t nthread = (w0 >> 8) & 0xffu;
+                auto tperm = [&](uint32_t i) -> uint32_t { return (i < 8 ? (tp0 >> (4 * i)) : (tp1 >> (4 * (i - 8)))) & 15u; };
                 uint32_t tb = 0;
                 if (MT > 0) {
 #pragma unroll
                     for (uint32_t i = 0; i < (MT > 0 ? MT - kRegQubits : 1u); ++i)
-                        if (i < I.nthread()) tb |= ((tid >> i) & 1u) << I.tperm(i);
+                        if (i < nthread) tb |= ((tid >> i) & 1u) << tperm(i);
                 } else {
-                    for (uint32_t i = 0; i < I.nthread(); ++i) tb |= ((tid >> i) & 1u) << I.tperm(i);
+                    for (uint32_t i = 0; i < nthread; ++i) tb |= ((tid >> i) & 1u) << tperm(i);
                 }
                 uint32_t rb[kR];
 #pragma unroll
-                for (int b = 0; b < kR; ++b) rb[b] = 1u << I.pos(b);
+                for (int b = 0; b < kR; ++b) rb[b] = 1u << ((w0 >> (16 + 4 * b)) & 15u);
                 // swz is linear over XOR, so slot j's address is swz(tb) XOR the
                 // swizzled register bits of j (recomputed for the write-back
                 // rather than held in 16 registers through the gates).
@@ -456,86 +347,128 @@ __global__ void __launch_bounds__(MAXT, MINB)
                 };
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) a[j] = tile[adr(j)];
-                // The next instruction is read while this one executes (every
-                // group ends with TOP_END, so the read stays in the program).
-                DI G = load_instr(sprog + pc);
-                ++pc;
-                for (; G.op() != TOP_END; ++pc) {
-                    const DI Gn = load_instr(sprog + pc);
-                    // Parametric blocks (a batched sweep) read the matrix of
-                    // this tile's binding: binding = tile >> bshift.
-                    const double* md = G.nthread() ? pdata + (t >> bshift) * pstride + G.data() : sd + G.data();
-                    if (G.op() == TOP_G1) {
-                        switch (G.kind()) {
-                            case TK_GEN: dispatch_g1<TK_GEN>(G.pos(0), a, md, G.aux()); break;
-                            case TK_U3: dispatch_g1<TK_U3>(G.pos(0), a, md, G.aux()); break;
-                            case TK_REAL: dispatch_g1<TK_REAL>(G.pos(0), a, md, G.aux()); break;
-                            case TK_X:
-                                switch (G.pos(0)) {
-                                    case 0: perm1<0>(a); break;
-                                    case 1: perm1<1>(a); break;
-                                    case 2: perm1<2>(a); break;
-                                    default: perm1<3>(a); break;
+                for (;;) {
+                    const uint32_t w = sw[pc++];
+                    const uint32_t op = w & 0xffu;
+                    if (op == cop::kEnd) break;
+                    const uint32_t aux = (w >> 8) & 0xffu;
+                    const double* md = sd + ((w >> 20) << 1);
+                    const uint32_t tv = (tb >> ((w >> 16) & 15u)) & 1u;  // the thread-bit operand's value
+                    switch (op) {
+#define MB2_CASE4(BASE, STMT) \
+    case BASE + 0: { constexpr int P = 0; STMT; } break; \
+    case BASE + 1: { constexpr int P = 1; STMT; } break; \
+    case BASE + 2: { constexpr int P = 2; STMT; } break; \
+    case BASE + 3: { constexpr int P = 3; STMT; } break;
+#define MB2_CASE12(BASE, STMT) \
+    case BASE + 0: { constexpr int P0 = 0, P1 = 1; STMT; } break; \
+    case BASE + 1: { constexpr int P0 = 0, P1 = 2; STMT; } break; \
+    case BASE + 2: { constexpr int P0 = 0, P1 = 3; STMT; } break; \
+    case BASE + 3: { constexpr int P0 = 1, P1 = 0; STMT; } break; \
+    case BASE + 4: { constexpr int P0 = 1, P1 = 2; STMT; } break; \
+    case BASE + 5: { constexpr int P0 = 1, P1 = 3; STMT; } break; \
+    case BASE + 6: { constexpr int P0 = 2, P1 = 0; STMT; } break; \
+    case BASE + 7: { constexpr int P0 = 2, P1 = 1; STMT; } break; \
+    case BASE + 8: { constexpr int P0 = 2, P1 = 3; STMT; } break; \
+    case BASE + 9: { constexpr int P0 = 3, P1 = 0; STMT; } break; \
+    case BASE + 10: { constexpr int P0 = 3, P1 = 1; STMT; } break; \
+    case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
+                        MB2_CASE4(cop::kU3, (g1<P, TK_U3>(a, md, 0u)))
+                        MB2_CASE4(cop::kGen1, (g1<P, TK_GEN>(a, md, 0u)))
+                        MB2_CASE4(cop::kReal1, (g1<P, TK_REAL>(a, md, 0u)))
+                        MB2_CASE4(cop::kMono1, (g1<P, TK_MONO>(a, md, aux)))
+                        MB2_CASE4(cop::kX1, (perm1<P>(a)))
+                        MB2_CASE12(cop::kGen2, (g2<P0, P1, TK_GEN>(a, md, 0u)))
+                        MB2_CASE12(cop::kMono2, (g2<P0, P1, TK_MONO>(a, md, sw[pc++])))
+                        MB2_CASE12(cop::kSw12, (perm2<P0, P1, TK_SW12>(a)))
+                        MB2_CASE12(cop::kSw13, (perm2<P0, P1, TK_SW13>(a)))
+                        MB2_CASE12(cop::kSw23, (perm2<P0, P1, TK_SW23>(a)))
+                        MB2_CASE4(cop::kDs1R, (diag_rr<P, -1>(a, load_diag(md, 1, aux))))
+                        MB2_CASE12(cop::kDs2RR, (diag_rr<P0, P1>(a, load_diag(md, 2, aux))))
+#undef MB2_CASE4
+#undef MB2_CASE12
+                        case cop::kDs1T: {
+                            const Diag4 D = load_diag(md, 1, aux);
+                            diag_set<-1, -1>(a, (aux >> (2 * tv)) & 3u, diag_entry(D, tv), 0, 0);
+                        } break;
+                        // One register operand (slot s) and one thread bit (operand index wi).
+                        case cop::kDs2RT + 0: diag_rt<0>(a, load_diag(md, 2, aux), 1u, tv); break;
+                        case cop::kDs2RT + 1: diag_rt<0>(a, load_diag(md, 2, aux), 0u, tv); break;
+                        case cop::kDs2RT + 2: diag_rt<1>(a, load_diag(md, 2, aux), 1u, tv); break;
+                        case cop::kDs2RT + 3: diag_rt<1>(a, load_diag(md, 2, aux), 0u, tv); break;
+                        case cop::kDs2RT + 4: diag_rt<2>(a, load_diag(md, 2, aux), 1u, tv); break;
+                        case cop::kDs2RT + 5: diag_rt<2>(a, load_diag(md, 2, aux), 0u, tv); break;
+                        case cop::kDs2RT + 6: diag_rt<3>(a, load_diag(md, 2, aux), 1u, tv); break;
+                        case cop::kDs2RT + 7: diag_rt<3>(a, load_diag(md, 2, aux), 0u, tv); break;
+                        case cop::kDs2TT: {
+                            const uint32_t cc = sw[pc++];
+                            const uint32_t e = ((tb >> (cc & 15u)) & 1u) | (((tb >> ((cc >> 4) & 15u)) & 1u) << 1);
+                            const Diag4 D = load_diag(md, 2, aux);
+                            diag_set<-1, -1>(a, (aux >> (2 * e)) & 3u, diag_entry(D, e), 0, 0);
+                        } break;
+                        case cop::kSigns: {
+                            // XOR of the monomials' masks over the 16 register slots j.
+                            uint32_t M = 0;
+                            for (uint32_t i = 0; i < aux; ++i) {
+                                const uint32_t mono = sw[pc++];
+                                uint32_t mm = 0xffffu;
+                                for (uint32_t f = 0; f < 6; ++f) {
+                                    const uint32_t src = (mono >> (5 * f)) & 31u;
+                                    if (src == cop::kSrcNone) break;
+                                    const uint32_t v =
+                                        (src & cop::kSrcReg)
+                                            ? static_cast<uint32_t>(0xFF00F0F0CCCCAAAAull >> (16 * (src & 3u))) & 0xffffu
+                                            : (((tb >> src) & 1u) ? 0xffffu : 0u);
+                                    mm &= v;
                                 }
-                                break;
-                            default: dispatch_g1<TK_MONO>(G.pos(0), a, md, G.aux()); break;
-                        }
-                    } else if (G.op() == TOP_G2) {
-                        switch (G.kind()) {
-                            case TK_SW12: dispatch_perm2<TK_SW12>(G.pos(0), G.pos(1), a); break;
-                            case TK_SW13: dispatch_perm2<TK_SW13>(G.pos(0), G.pos(1), a); break;
-                            case TK_SW23: dispatch_perm2<TK_SW23>(G.pos(0), G.pos(1), a); break;
-                            case TK_MONO: dispatch_g2<TK_MONO>(G.pos(0), G.pos(1), a, md, G.aux()); break;
-                            default: dispatch_g2<TK_GEN>(G.pos(0), G.pos(1), a, md, G.aux()); break;
-                        }
-                    } else if (G.kind() == TK_DSMALL) {
-                        // Operand sources decided on the host: 0x80 | slot, or a thread bit.
-                        const uint32_t c0 = G.pos(4), c1 = G.pos(5);
-                        const int s0 = (c0 & 0x80u) ? static_cast<int>(c0 & 3u) : -1;
-                        const int s1 = (c1 & 0x80u) ? static_cast<int>(c1 & 3u) : -1;
-                        const uint32_t t0 = (c0 & 0x80u) ? 0u : (tb >> c0) & 1u;
-                        const uint32_t t1 = (c1 & 0x80u) ? 0u : (tb >> c1) & 1u;
-                        diag_small(a, md, G.k(), G.aux(), s0, s1, t0, t1);
-                    } else {  // TOP_DIAG, any k: entry index per amplitude
-                        const uint32_t k = G.k();
-                        uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
-                        for (uint32_t b = 0; b < k; ++b) {
-                            const uint32_t bit = 1u << G.pos(b);
-                            et |= ((tb & bit) ? 1u : 0u) << b;
-                            if (bit == rb[0]) e0 = 1u << b;
-                            if (bit == rb[1]) e1 = 1u << b;
-                            if (bit == rb[2]) e2 = 1u << b;
-                            if (bit == rb[3]) e3 = 1u << b;
-                        }
+                                M ^= mm;
+                            }
 #pragma unroll
-                        for (int j = 0; j < kNA; ++j) {
-                            const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) | ((j & 4) ? e2 : 0u) |
-                                               ((j & 8) ? e3 : 0u);
-                            a[j] = scale_entry(md[2 * e], md[2 * e + 1], a[j]);
-                        }
+                            for (int j = 0; j < kNA; ++j) a[j] = cneg_if(a[j], (M >> j) & 1u);
+                        } break;
+                        default: {  // cop::kDiagK: any k, entry index per amplitude
+                            const uint32_t pos = sw[pc++];
+                            uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+                            for (uint32_t b = 0; b < aux; ++b) {
+                                const uint32_t bit = 1u << ((pos >> (4 * b)) & 15u);
+                                et |= ((tb & bit) ? 1u : 0u) << b;
+                                if (bit == rb[0]) e0 = 1u << b;
+                                if (bit == rb[1]) e1 = 1u << b;
+                                if (bit == rb[2]) e2 = 1u << b;
+                                if (bit == rb[3]) e3 = 1u << b;
+                            }
+#pragma unroll
+                            for (int j = 0; j < kNA; ++j) {
+                                const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) |
+                                                   ((j & 4) ? e2 : 0u) | ((j & 8) ? e3 : 0u);
+                                a[j] = scale_entry(md[2 * e], md[2 * e + 1], a[j]);
+                            }
+                        } break;
                     }
-                    G = Gn;
                 }
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
                 __syncthreads();
-            } else if (I.op() == TOP_SMEM) {
+            } else if (op0 == cop::kSmem) {
                 // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
-                const uint32_t k = I.k(), dim = 1u << k;
+                const uint32_t k = (w0 >> 8) & 0xffu, dim = 1u << k;
+                const uint32_t pos = sw[pc + 1];
+                const double* md = gdata + sw[pc + 2];
+                pc += 3;
+                auto qpos = [&](uint32_t b) -> uint32_t { return (pos >> (4 * b)) & 15u; };
                 uint32_t opm = 0;
-                for (uint32_t b = 0; b < k; ++b) opm |= 1u << I.pos(b);
-                const double* md = gdata + I.data();
+                for (uint32_t b = 0; b < k; ++b) opm |= 1u << qpos(b);
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) {
                     const uint32_t l = tid | (static_cast<uint32_t>(j) << tbits);
                     uint32_t out = 0;
-                    for (uint32_t b = 0; b < k; ++b) out |= ((l >> I.pos(b)) & 1u) << b;
+                    for (uint32_t b = 0; b < k; ++b) out |= ((l >> qpos(b)) & 1u) << b;
                     const uint32_t gbase = l & ~opm;
                     double2 acc = make_double2(0.0, 0.0);
                     for (uint32_t in = 0; in < dim; ++in) {
                         uint32_t li = gbase;
                         for (uint32_t b = 0; b < k; ++b)
-                            if ((in >> b) & 1u) li |= 1u << I.pos(b);
+                            if ((in >> b) & 1u) li |= 1u << qpos(b);
                         const double2 p = cmul(__ldg(md + 2 * (out * dim + in)), __ldg(md + 2 * (out * dim + in) + 1),
                                                tile[swz(li)]);
                         acc = (in == 0) ? p : cadd(acc, p);
@@ -546,6 +479,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) tile[slot(j)] = a[j];
                 __syncthreads();
+            } else {
+                break;  // padding after the last instruction
             }
         }
 
@@ -574,8 +509,8 @@ int launch_instance(const TileLaunch& L) {
     }
     if (L.smem > dyn_max) return MB2_ERR_INVALID;
     k_tile_pass<MAXT, MINB, MT, IDX><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
-        static_cast<double2*>(L.amps), L.n_all, L.m, L.smask, L.prog, L.nprog, L.sdata, L.nsdata, L.gdata, L.ntiles,
-        L.pdata, L.pstride, L.bshift, L.stages);
+        static_cast<double2*>(L.amps), L.n_all, L.m, L.smask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata,
+        L.ntiles, L.pdata, L.pstride, L.param_lo, L.param_len, L.bshift, L.stages);
     return launch_status();
 }
 

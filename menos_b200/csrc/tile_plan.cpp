@@ -355,6 +355,7 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
         pass.sdata_count = static_cast<uint32_t>(prog.data.size()) - pass.sdata_begin;
         prog.passes.push_back(pass);
     }
+    encode_compact(prog);
     return prog;
 }
 
