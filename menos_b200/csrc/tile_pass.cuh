@@ -216,6 +216,187 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// The instructions of one pass applied to one tile held in shared memory
+// (canonical layout on entry and exit).  `sync` is the barrier of the
+// threads that share the tile; parametric data sits pshift doubles past the
+// staged data's end.
+template <int MT, typename SYNC>
+__device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const uint32_t* __restrict__ sw,
+                                             uint32_t nwords, const double* __restrict__ sd, uint32_t nsdata,
+                                             uint32_t pshift, const double* __restrict__ gdata, uint32_t tid,
+                                             uint32_t m, SYNC sync) {
+    const uint32_t tbits = m - kRegQubits;
+    const uint32_t s_tid = swz(tid);
+    auto slot = [&](int j) -> uint32_t { return s_tid ^ swz(static_cast<uint32_t>(j) << tbits); };
+    double2 a[kNA];
+    uint32_t pc = 0;
+    while (pc < nwords) {
+        const uint32_t w0 = sw[pc];
+        const uint32_t op0 = w0 & 0xffu;
+        if (op0 == cop::kPhase) {
+            const uint32_t tp0 = sw[pc + 1], tp1 = sw[pc + 2];
+            pc += 3;
+            const uint32_t nthread = (w0 >> 8) & 0xffu;
+            auto tperm = [&](uint32_t i) -> uint32_t { return (i < 8 ? (tp0 >> (4 * i)) : (tp1 >> (4 * (i - 8)))) & 15u; };
+            uint32_t tb = 0;
+            if (MT > 0) {
+#pragma unroll
+                for (uint32_t i = 0; i < (MT > 0 ? MT - kRegQubits : 1u); ++i)
+                    if (i < nthread) tb |= ((tid >> i) & 1u) << tperm(i);
+            } else {
+                for (uint32_t i = 0; i < nthread; ++i) tb |= ((tid >> i) & 1u) << tperm(i);
+            }
+            uint32_t rb[kR];
+#pragma unroll
+            for (int b = 0; b < kR; ++b) rb[b] = 1u << ((w0 >> (16 + 4 * b)) & 15u);
+            // swz is linear over XOR, so slot j's address is swz(tb) XOR the
+            // swizzled register bits of j (recomputed for the write-back
+            // rather than held in 16 registers through the gates).
+            const uint32_t z0 = swz(tb), z1 = swz(rb[0]), z2 = swz(rb[1]), z3 = swz(rb[2]), z4 = swz(rb[3]);
+            auto adr = [&](int j) -> uint32_t {
+                return z0 ^ ((j & 1) ? z1 : 0u) ^ ((j & 2) ? z2 : 0u) ^ ((j & 4) ? z3 : 0u) ^ ((j & 8) ? z4 : 0u);
+            };
+#pragma unroll
+            for (int j = 0; j < kNA; ++j) a[j] = tile[adr(j)];
+            for (;;) {
+                const uint32_t w = sw[pc++];
+                const uint32_t op = w & 0xffu;
+                if (op == cop::kEnd) break;
+                const uint32_t aux = (w >> 8) & 0xffu;
+                const uint32_t off = (w >> 20) << 1;
+                const double* md = sd + off + (off >= nsdata ? pshift : 0u);
+                const uint32_t tv = (tb >> ((w >> 16) & 15u)) & 1u;  // the thread-bit operand's value
+                switch (op) {
+#define MB2_CASE4(BASE, STMT) \
+case BASE + 0: { constexpr int P = 0; STMT; } break; \
+case BASE + 1: { constexpr int P = 1; STMT; } break; \
+case BASE + 2: { constexpr int P = 2; STMT; } break; \
+case BASE + 3: { constexpr int P = 3; STMT; } break;
+#define MB2_CASE12(BASE, STMT) \
+case BASE + 0: { constexpr int P0 = 0, P1 = 1; STMT; } break; \
+case BASE + 1: { constexpr int P0 = 0, P1 = 2; STMT; } break; \
+case BASE + 2: { constexpr int P0 = 0, P1 = 3; STMT; } break; \
+case BASE + 3: { constexpr int P0 = 1, P1 = 0; STMT; } break; \
+case BASE + 4: { constexpr int P0 = 1, P1 = 2; STMT; } break; \
+case BASE + 5: { constexpr int P0 = 1, P1 = 3; STMT; } break; \
+case BASE + 6: { constexpr int P0 = 2, P1 = 0; STMT; } break; \
+case BASE + 7: { constexpr int P0 = 2, P1 = 1; STMT; } break; \
+case BASE + 8: { constexpr int P0 = 2, P1 = 3; STMT; } break; \
+case BASE + 9: { constexpr int P0 = 3, P1 = 0; STMT; } break; \
+case BASE + 10: { constexpr int P0 = 3, P1 = 1; STMT; } break; \
+case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
+                    MB2_CASE4(cop::kU3, (g1<P, TK_U3>(a, md, 0u)))
+                    MB2_CASE4(cop::kGen1, (g1<P, TK_GEN>(a, md, 0u)))
+                    MB2_CASE4(cop::kReal1, (g1<P, TK_REAL>(a, md, 0u)))
+                    MB2_CASE4(cop::kMono1, (g1<P, TK_MONO>(a, md, aux)))
+                    MB2_CASE4(cop::kX1, (perm1<P>(a)))
+                    MB2_CASE12(cop::kGen2, (g2<P0, P1, TK_GEN>(a, md, 0u)))
+                    MB2_CASE12(cop::kMono2, (g2<P0, P1, TK_MONO>(a, md, sw[pc++])))
+                    MB2_CASE12(cop::kSw12, (perm2<P0, P1, TK_SW12>(a)))
+                    MB2_CASE12(cop::kSw13, (perm2<P0, P1, TK_SW13>(a)))
+                    MB2_CASE12(cop::kSw23, (perm2<P0, P1, TK_SW23>(a)))
+                    MB2_CASE4(cop::kDs1R, (diag_rr<P, -1>(a, load_diag(md, 1, aux))))
+                    MB2_CASE12(cop::kDs2RR, (diag_rr<P0, P1>(a, load_diag(md, 2, aux))))
+#undef MB2_CASE4
+#undef MB2_CASE12
+                    case cop::kDs1T: {
+                        const Diag4 D = load_diag(md, 1, aux);
+                        diag_set<-1, -1>(a, (aux >> (2 * tv)) & 3u, diag_entry(D, tv), 0, 0);
+                    } break;
+                    // One register operand (slot s) and one thread bit (operand index wi).
+                    case cop::kDs2RT + 0: diag_rt<0>(a, load_diag(md, 2, aux), 1u, tv); break;
+                    case cop::kDs2RT + 1: diag_rt<0>(a, load_diag(md, 2, aux), 0u, tv); break;
+                    case cop::kDs2RT + 2: diag_rt<1>(a, load_diag(md, 2, aux), 1u, tv); break;
+                    case cop::kDs2RT + 3: diag_rt<1>(a, load_diag(md, 2, aux), 0u, tv); break;
+                    case cop::kDs2RT + 4: diag_rt<2>(a, load_diag(md, 2, aux), 1u, tv); break;
+                    case cop::kDs2RT + 5: diag_rt<2>(a, load_diag(md, 2, aux), 0u, tv); break;
+                    case cop::kDs2RT + 6: diag_rt<3>(a, load_diag(md, 2, aux), 1u, tv); break;
+                    case cop::kDs2RT + 7: diag_rt<3>(a, load_diag(md, 2, aux), 0u, tv); break;
+                    case cop::kDs2TT: {
+                        const uint32_t cc = sw[pc++];
+                        const uint32_t e = ((tb >> (cc & 15u)) & 1u) | (((tb >> ((cc >> 4) & 15u)) & 1u) << 1);
+                        const Diag4 D = load_diag(md, 2, aux);
+                        diag_set<-1, -1>(a, (aux >> (2 * e)) & 3u, diag_entry(D, e), 0, 0);
+                    } break;
+                    case cop::kSigns: {
+                        // XOR of the monomials' masks over the 16 register slots j.
+                        uint32_t M = 0;
+                        for (uint32_t i = 0; i < aux; ++i) {
+                            const uint32_t mono = sw[pc++];
+                            uint32_t mm = 0xffffu;
+                            for (uint32_t f = 0; f < 6; ++f) {
+                                const uint32_t src = (mono >> (5 * f)) & 31u;
+                                if (src == cop::kSrcNone) break;
+                                const uint32_t v =
+                                    (src & cop::kSrcReg)
+                                        ? static_cast<uint32_t>(0xFF00F0F0CCCCAAAAull >> (16 * (src & 3u))) & 0xffffu
+                                        : (((tb >> src) & 1u) ? 0xffffu : 0u);
+                                mm &= v;
+                            }
+                            M ^= mm;
+                        }
+#pragma unroll
+                        for (int j = 0; j < kNA; ++j) a[j] = cneg_if(a[j], (M >> j) & 1u);
+                    } break;
+                    default: {  // cop::kDiagK: any k, entry index per amplitude
+                        const uint32_t pos = sw[pc++];
+                        uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+                        for (uint32_t b = 0; b < aux; ++b) {
+                            const uint32_t bit = 1u << ((pos >> (4 * b)) & 15u);
+                            et |= ((tb & bit) ? 1u : 0u) << b;
+                            if (bit == rb[0]) e0 = 1u << b;
+                            if (bit == rb[1]) e1 = 1u << b;
+                            if (bit == rb[2]) e2 = 1u << b;
+                            if (bit == rb[3]) e3 = 1u << b;
+                        }
+#pragma unroll
+                        for (int j = 0; j < kNA; ++j) {
+                            const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) |
+                                               ((j & 4) ? e2 : 0u) | ((j & 8) ? e3 : 0u);
+                            a[j] = scale_entry(md[2 * e], md[2 * e + 1], a[j]);
+                        }
+                    } break;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
+            sync();
+        } else if (op0 == cop::kSmem) {
+            // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
+            const uint32_t k = (w0 >> 8) & 0xffu, dim = 1u << k;
+            const uint32_t pos = sw[pc + 1];
+            const double* md = gdata + sw[pc + 2];
+            pc += 3;
+            auto qpos = [&](uint32_t b) -> uint32_t { return (pos >> (4 * b)) & 15u; };
+            uint32_t opm = 0;
+            for (uint32_t b = 0; b < k; ++b) opm |= 1u << qpos(b);
+#pragma unroll
+            for (int j = 0; j < kNA; ++j) {
+                const uint32_t l = tid | (static_cast<uint32_t>(j) << tbits);
+                uint32_t out = 0;
+                for (uint32_t b = 0; b < k; ++b) out |= ((l >> qpos(b)) & 1u) << b;
+                const uint32_t gbase = l & ~opm;
+                double2 acc = make_double2(0.0, 0.0);
+                for (uint32_t in = 0; in < dim; ++in) {
+                    uint32_t li = gbase;
+                    for (uint32_t b = 0; b < k; ++b)
+                        if ((in >> b) & 1u) li |= 1u << qpos(b);
+                    const double2 p = cmul(__ldg(md + 2 * (out * dim + in)), __ldg(md + 2 * (out * dim + in) + 1),
+                                           tile[swz(li)]);
+                    acc = (in == 0) ? p : cadd(acc, p);
+                }
+                a[j] = acc;
+            }
+            sync();
+#pragma unroll
+            for (int j = 0; j < kNA; ++j) tile[slot(j)] = a[j];
+            sync();
+        } else {
+            break;  // padding after the last instruction
+        }
+    }
+}
+
 // One pass of the tiled sweep.  blockDim.x == 2^(m-4) <= 256; each thread
 // owns 16 amplitudes.  Persistent CTAs take tiles round-robin; the tiles
 // `stages - 1` ahead are gathered into shared-memory buffers with cp.async
@@ -317,172 +498,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
         else cp_async_wait<1>();
         __syncthreads();
 
-        double2 a[kNA];
-        uint32_t pc = 0;
-        while (pc < nwords) {
-            const uint32_t w0 = sw[pc];
-            const uint32_t op0 = w0 & 0xffu;
-            if (op0 == cop::kPhase) {
-                const uint32_t tp0 = sw[pc + 1], tp1 = sw[pc + 2];
-                pc += 3;
-                const uint32_t nthread = (w0 >> 8) & 0xffu;
-                auto tperm = [&](uint32_t i) -> uint32_t { return (i < 8 ? (tp0 >> (4 * i)) : (tp1 >> (4 * (i - 8)))) & 15u; };
-                uint32_t tb = 0;
-                if (MT > 0) {
-#pragma unroll
-                    for (uint32_t i = 0; i < (MT > 0 ? MT - kRegQubits : 1u); ++i)
-                        if (i < nthread) tb |= ((tid >> i) & 1u) << tperm(i);
-                } else {
-                    for (uint32_t i = 0; i < nthread; ++i) tb |= ((tid >> i) & 1u) << tperm(i);
-                }
-                uint32_t rb[kR];
-#pragma unroll
-                for (int b = 0; b < kR; ++b) rb[b] = 1u << ((w0 >> (16 + 4 * b)) & 15u);
-                // swz is linear over XOR, so slot j's address is swz(tb) XOR the
-                // swizzled register bits of j (recomputed for the write-back
-                // rather than held in 16 registers through the gates).
-                const uint32_t z0 = swz(tb), z1 = swz(rb[0]), z2 = swz(rb[1]), z3 = swz(rb[2]), z4 = swz(rb[3]);
-                auto adr = [&](int j) -> uint32_t {
-                    return z0 ^ ((j & 1) ? z1 : 0u) ^ ((j & 2) ? z2 : 0u) ^ ((j & 4) ? z3 : 0u) ^ ((j & 8) ? z4 : 0u);
-                };
-#pragma unroll
-                for (int j = 0; j < kNA; ++j) a[j] = tile[adr(j)];
-                for (;;) {
-                    const uint32_t w = sw[pc++];
-                    const uint32_t op = w & 0xffu;
-                    if (op == cop::kEnd) break;
-                    const uint32_t aux = (w >> 8) & 0xffu;
-                    const double* md = sd + ((w >> 20) << 1);
-                    const uint32_t tv = (tb >> ((w >> 16) & 15u)) & 1u;  // the thread-bit operand's value
-                    switch (op) {
-#define MB2_CASE4(BASE, STMT) \
-    case BASE + 0: { constexpr int P = 0; STMT; } break; \
-    case BASE + 1: { constexpr int P = 1; STMT; } break; \
-    case BASE + 2: { constexpr int P = 2; STMT; } break; \
-    case BASE + 3: { constexpr int P = 3; STMT; } break;
-#define MB2_CASE12(BASE, STMT) \
-    case BASE + 0: { constexpr int P0 = 0, P1 = 1; STMT; } break; \
-    case BASE + 1: { constexpr int P0 = 0, P1 = 2; STMT; } break; \
-    case BASE + 2: { constexpr int P0 = 0, P1 = 3; STMT; } break; \
-    case BASE + 3: { constexpr int P0 = 1, P1 = 0; STMT; } break; \
-    case BASE + 4: { constexpr int P0 = 1, P1 = 2; STMT; } break; \
-    case BASE + 5: { constexpr int P0 = 1, P1 = 3; STMT; } break; \
-    case BASE + 6: { constexpr int P0 = 2, P1 = 0; STMT; } break; \
-    case BASE + 7: { constexpr int P0 = 2, P1 = 1; STMT; } break; \
-    case BASE + 8: { constexpr int P0 = 2, P1 = 3; STMT; } break; \
-    case BASE + 9: { constexpr int P0 = 3, P1 = 0; STMT; } break; \
-    case BASE + 10: { constexpr int P0 = 3, P1 = 1; STMT; } break; \
-    case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
-                        MB2_CASE4(cop::kU3, (g1<P, TK_U3>(a, md, 0u)))
-                        MB2_CASE4(cop::kGen1, (g1<P, TK_GEN>(a, md, 0u)))
-                        MB2_CASE4(cop::kReal1, (g1<P, TK_REAL>(a, md, 0u)))
-                        MB2_CASE4(cop::kMono1, (g1<P, TK_MONO>(a, md, aux)))
-                        MB2_CASE4(cop::kX1, (perm1<P>(a)))
-                        MB2_CASE12(cop::kGen2, (g2<P0, P1, TK_GEN>(a, md, 0u)))
-                        MB2_CASE12(cop::kMono2, (g2<P0, P1, TK_MONO>(a, md, sw[pc++])))
-                        MB2_CASE12(cop::kSw12, (perm2<P0, P1, TK_SW12>(a)))
-                        MB2_CASE12(cop::kSw13, (perm2<P0, P1, TK_SW13>(a)))
-                        MB2_CASE12(cop::kSw23, (perm2<P0, P1, TK_SW23>(a)))
-                        MB2_CASE4(cop::kDs1R, (diag_rr<P, -1>(a, load_diag(md, 1, aux))))
-                        MB2_CASE12(cop::kDs2RR, (diag_rr<P0, P1>(a, load_diag(md, 2, aux))))
-#undef MB2_CASE4
-#undef MB2_CASE12
-                        case cop::kDs1T: {
-                            const Diag4 D = load_diag(md, 1, aux);
-                            diag_set<-1, -1>(a, (aux >> (2 * tv)) & 3u, diag_entry(D, tv), 0, 0);
-                        } break;
-                        // One register operand (slot s) and one thread bit (operand index wi).
-                        case cop::kDs2RT + 0: diag_rt<0>(a, load_diag(md, 2, aux), 1u, tv); break;
-                        case cop::kDs2RT + 1: diag_rt<0>(a, load_diag(md, 2, aux), 0u, tv); break;
-                        case cop::kDs2RT + 2: diag_rt<1>(a, load_diag(md, 2, aux), 1u, tv); break;
-                        case cop::kDs2RT + 3: diag_rt<1>(a, load_diag(md, 2, aux), 0u, tv); break;
-                        case cop::kDs2RT + 4: diag_rt<2>(a, load_diag(md, 2, aux), 1u, tv); break;
-                        case cop::kDs2RT + 5: diag_rt<2>(a, load_diag(md, 2, aux), 0u, tv); break;
-                        case cop::kDs2RT + 6: diag_rt<3>(a, load_diag(md, 2, aux), 1u, tv); break;
-                        case cop::kDs2RT + 7: diag_rt<3>(a, load_diag(md, 2, aux), 0u, tv); break;
-                        case cop::kDs2TT: {
-                            const uint32_t cc = sw[pc++];
-                            const uint32_t e = ((tb >> (cc & 15u)) & 1u) | (((tb >> ((cc >> 4) & 15u)) & 1u) << 1);
-                            const Diag4 D = load_diag(md, 2, aux);
-                            diag_set<-1, -1>(a, (aux >> (2 * e)) & 3u, diag_entry(D, e), 0, 0);
-                        } break;
-                        case cop::kSigns: {
-                            // XOR of the monomials' masks over the 16 register slots j.
-                            uint32_t M = 0;
-                            for (uint32_t i = 0; i < aux; ++i) {
-                                const uint32_t mono = sw[pc++];
-                                uint32_t mm = 0xffffu;
-                                for (uint32_t f = 0; f < 6; ++f) {
-                                    const uint32_t src = (mono >> (5 * f)) & 31u;
-                                    if (src == cop::kSrcNone) break;
-                                    const uint32_t v =
-                                        (src & cop::kSrcReg)
-                                            ? static_cast<uint32_t>(0xFF00F0F0CCCCAAAAull >> (16 * (src & 3u))) & 0xffffu
-                                            : (((tb >> src) & 1u) ? 0xffffu : 0u);
-                                    mm &= v;
-                                }
-                                M ^= mm;
-                            }
-#pragma unroll
-                            for (int j = 0; j < kNA; ++j) a[j] = cneg_if(a[j], (M >> j) & 1u);
-                        } break;
-                        default: {  // cop::kDiagK: any k, entry index per amplitude
-                            const uint32_t pos = sw[pc++];
-                            uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
-                            for (uint32_t b = 0; b < aux; ++b) {
-                                const uint32_t bit = 1u << ((pos >> (4 * b)) & 15u);
-                                et |= ((tb & bit) ? 1u : 0u) << b;
-                                if (bit == rb[0]) e0 = 1u << b;
-                                if (bit == rb[1]) e1 = 1u << b;
-                                if (bit == rb[2]) e2 = 1u << b;
-                                if (bit == rb[3]) e3 = 1u << b;
-                            }
-#pragma unroll
-                            for (int j = 0; j < kNA; ++j) {
-                                const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) |
-                                                   ((j & 4) ? e2 : 0u) | ((j & 8) ? e3 : 0u);
-                                a[j] = scale_entry(md[2 * e], md[2 * e + 1], a[j]);
-                            }
-                        } break;
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
-                __syncthreads();
-            } else if (op0 == cop::kSmem) {
-                // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
-                const uint32_t k = (w0 >> 8) & 0xffu, dim = 1u << k;
-                const uint32_t pos = sw[pc + 1];
-                const double* md = gdata + sw[pc + 2];
-                pc += 3;
-                auto qpos = [&](uint32_t b) -> uint32_t { return (pos >> (4 * b)) & 15u; };
-                uint32_t opm = 0;
-                for (uint32_t b = 0; b < k; ++b) opm |= 1u << qpos(b);
-#pragma unroll
-                for (int j = 0; j < kNA; ++j) {
-                    const uint32_t l = tid | (static_cast<uint32_t>(j) << tbits);
-                    uint32_t out = 0;
-                    for (uint32_t b = 0; b < k; ++b) out |= ((l >> qpos(b)) & 1u) << b;
-                    const uint32_t gbase = l & ~opm;
-                    double2 acc = make_double2(0.0, 0.0);
-                    for (uint32_t in = 0; in < dim; ++in) {
-                        uint32_t li = gbase;
-                        for (uint32_t b = 0; b < k; ++b)
-                            if ((in >> b) & 1u) li |= 1u << qpos(b);
-                        const double2 p = cmul(__ldg(md + 2 * (out * dim + in)), __ldg(md + 2 * (out * dim + in) + 1),
-                                               tile[swz(li)]);
-                        acc = (in == 0) ? p : cadd(acc, p);
-                    }
-                    a[j] = acc;
-                }
-                __syncthreads();
-#pragma unroll
-                for (int j = 0; j < kNA; ++j) tile[slot(j)] = a[j];
-                __syncthreads();
-            } else {
-                break;  // padding after the last instruction
-            }
-        }
+        compute_tile<MT>(tile, sw, nwords, sd, nsdata, 0u, gdata, tid, m, [] { __syncthreads(); });
 
         // Store: canonical mapping, -0.0 normalised.
         const IDX b0 = cbase + off_lo;
@@ -491,6 +507,148 @@ __global__ void __launch_bounds__(MAXT, MINB)
         cbase = advance(cbase);
         __syncthreads();  // the buffer is the target of a later prefetch
     }
+}
+
+// The 11-qubit pass as two groups of four warps per CTA ("ping-pong"): each
+// group streams its own tiles through its own buffers, and the two groups
+// take turns at the gates, so that one group's loads, stores and waits run
+// while the other group's FP64 work has the SMs' FP64 pipes to itself.  (Two
+// independent CTAs per SM drift into lockstep -- both computing, then both
+// moving data -- which leaves each resource idle half the time.)
+//
+// Turns are passed with two named barriers of 256 threads, X and Y:
+//   group A (tiles 2b, 2b + 2G, ...):  [k >= 1: sync X] gates k [k < KB: arrive Y]
+//   group B (tiles 2b + 1, ...):       sync Y, gates k [k < KA - 1: arrive X]
+// so gates run A0 B0 A1 B1 ...; KA is KB or KB + 1, and every sync meets
+// exactly one arrive (a host-side simulation of the protocol checks this for
+// every KA, KB).  Barriers 1 and 2 are each group's own.
+template <int MT, typename IDX>
+__global__ void __launch_bounds__(256, 1)
+    k_tile_pingpong(double2* __restrict__ st, uint32_t n, uint64_t smask, const uint32_t* __restrict__ words,
+                    uint32_t nwords, const double* __restrict__ sdata, uint32_t nsdata,
+                    const double* __restrict__ gdata, uint64_t ntiles, const double* __restrict__ pdata,
+                    uint32_t pstride, uint32_t param_lo, uint32_t param_len, uint32_t bshift, uint32_t stages) {
+    extern __shared__ double2 smem_tiles[];
+    constexpr uint32_t m = MT;
+    constexpr uint32_t tbits = m - kRegQubits;
+    constexpr uint32_t tile_amps = 1u << m;
+    constexpr uint32_t kGroupThreads = 1u << tbits;
+    const uint32_t grp = threadIdx.x >> tbits;  // 0: A, 1: B
+    const uint32_t tid = threadIdx.x & (kGroupThreads - 1);
+    // Shared memory: group A's tile buffers, group B's, the words, the staged
+    // data, then A's and B's parametric slices.
+    uint32_t* sw = reinterpret_cast<uint32_t*>(smem_tiles + 2 * stages * tile_amps);
+    double* sd = reinterpret_cast<double*>(sw + nwords);
+    for (uint32_t i = threadIdx.x; i < nwords / 4; i += blockDim.x)
+        reinterpret_cast<uint4*>(sw)[i] = __ldg(reinterpret_cast<const uint4*>(words) + i);
+    for (uint32_t i = threadIdx.x; i < nsdata; i += blockDim.x) sd[i] = __ldg(sdata + i);
+    __syncthreads();
+    double2* tiles = smem_tiles + grp * stages * tile_amps;
+    const uint32_t pshift = grp * param_len;
+    const uint32_t bar_group = 1u + grp;
+    auto group_sync = [bar_group] { asm volatile("bar.sync %0, %1;" ::"r"(bar_group), "r"(kGroupThreads) : "memory"); };
+
+    IDX off_lo = 0, hib0 = 0, hib1 = 0, hib2 = 0, hib3 = 0;
+    {
+        uint32_t b = 0;
+        for (uint32_t p = 0; p < n; ++p) {
+            if (!((smask >> p) & 1u)) continue;
+            if (b < tbits) {
+                off_lo |= static_cast<IDX>((tid >> b) & 1u) << p;
+            } else {
+                const IDX v = IDX{1} << p;
+                const uint32_t r = b - tbits;
+                if (r == 0) hib0 = v;
+                else if (r == 1) hib1 = v;
+                else if (r == 2) hib2 = v;
+                else hib3 = v;
+            }
+            ++b;
+        }
+    }
+    // Group g of CTA b takes the tiles 2b + g + k * 2G (G = gridDim.x).
+    const uint64_t first = 2ull * blockIdx.x + grp, vgrid = 2ull * gridDim.x;
+    auto count_of = [&](uint64_t v) -> uint64_t { return v < ntiles ? (ntiles - v + vgrid - 1) / vgrid : 0; };
+    const uint64_t KA = count_of(2ull * blockIdx.x), KB = count_of(2ull * blockIdx.x + 1);
+    const uint64_t nmask64 = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~smask;
+    const IDX nmask = static_cast<IDX>(nmask64);
+    const IDX step = static_cast<IDX>(pdep64(vgrid, nmask64));
+    auto advance = [&](IDX b) -> IDX { return ((b | ~nmask) + step) & nmask; };
+    const uint32_t s_tid = swz(tid);
+    auto reg_off = [&](int j) -> IDX {
+        return ((j & 1) ? hib0 : IDX{0}) + ((j & 2) ? hib1 : IDX{0}) + ((j & 4) ? hib2 : IDX{0}) +
+               ((j & 8) ? hib3 : IDX{0});
+    };
+    auto slot = [&](int j) -> uint32_t { return s_tid ^ swz(static_cast<uint32_t>(j) << tbits); };
+    auto prefetch = [&](IDX base, double2* buf) {
+        const IDX b0 = base + off_lo;
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) cp_async16(buf + slot(j), st + (b0 + reg_off(j)));
+        cp_async_commit();
+    };
+    uint64_t tp = first;
+    IDX pbase = static_cast<IDX>(pdep64(first, nmask64));
+    IDX cbase = pbase;
+    for (uint32_t sg = 0; sg + 1 < stages; ++sg) {
+        if (tp < ntiles) prefetch(pbase, tiles + sg * tile_amps);
+        else cp_async_commit();
+        tp += vgrid;
+        pbase = advance(pbase);
+    }
+    uint32_t cur = 0, nxt = stages - 1;
+    uint64_t k = 0;
+    for (uint64_t t = first; t < ntiles; t += vgrid, ++k) {
+        double2* tile = tiles + cur * tile_amps;
+        if (tp < ntiles) prefetch(pbase, tiles + nxt * tile_amps);
+        else cp_async_commit();
+        tp += vgrid;
+        pbase = advance(pbase);
+        cur = cur + 1 == stages ? 0u : cur + 1;
+        nxt = nxt + 1 == stages ? 0u : nxt + 1;
+        if (param_len != 0) {
+            const double2* src = reinterpret_cast<const double2*>(pdata + (t >> bshift) * pstride + param_lo);
+            double2* dst = reinterpret_cast<double2*>(sd + nsdata + pshift);
+            for (uint32_t i = tid; i < param_len / 2; i += kGroupThreads) dst[i] = __ldg(src + i);
+        }
+        if (stages == 3) cp_async_wait<2>();
+        else cp_async_wait<1>();
+        group_sync();
+        // Wait for the turn: A's gates k follow B's gates k - 1, B's follow A's k.
+        if (grp == 0) {
+            if (k >= 1) asm volatile("bar.sync 3, 256;" ::: "memory");
+        } else {
+            asm volatile("bar.sync 4, 256;" ::: "memory");
+        }
+        compute_tile<MT>(tile, sw, nwords, sd, nsdata, pshift, gdata, tid, m, group_sync);
+        if (grp == 0) {
+            if (k < KB) asm volatile("bar.arrive 4, 256;" ::: "memory");
+        } else {
+            if (k + 1 < KA) asm volatile("bar.arrive 3, 256;" ::: "memory");
+        }
+        const IDX b0 = cbase + off_lo;
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) st[b0 + reg_off(j)] = canon(tile[slot(j)]);
+        cbase = advance(cbase);
+        group_sync();  // the buffer is the target of a later prefetch
+    }
+}
+
+template <int MT, typename IDX>
+int launch_pingpong(const TileLaunch& L) {
+    static size_t dyn_max = 0;
+    if (dyn_max == 0) {
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, k_tile_pingpong<MT, IDX>) != cudaSuccess) return launch_status();
+        dyn_max = kTileSmemMax - fa.sharedSizeBytes;
+        if (cudaFuncSetAttribute(k_tile_pingpong<MT, IDX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(dyn_max)) != cudaSuccess)
+            return launch_status();
+    }
+    if (L.smem > dyn_max) return MB2_ERR_INVALID;
+    k_tile_pingpong<MT, IDX><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
+        static_cast<double2*>(L.amps), L.n_all, L.smask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata, L.ntiles,
+        L.pdata, L.pstride, L.param_lo, L.param_len, L.bshift, L.stages);
+    return launch_status();
 }
 
 // Launches one instance; the shared-memory limit is raised once per instance.
