@@ -245,15 +245,12 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const uint32_
     L.bshift = n - pass.m;
     L.stream = stream;
     L.threads = 1u << (pass.m - kRegQubits);
-    // 12-qubit tiles: one CTA per SM with three tile buffers (two tiles in
-    // flight); 11-qubit tiles: one ping-pong CTA per SM, two groups with two
-    // buffers each; smaller tiles: two CTAs per SM with two buffers each.
-    const bool pingpong = pass.m == 11;
-    const uint32_t groups = pingpong ? 2u : 1u;
+    // 12-qubit tiles keep three tile buffers (two tiles in flight), smaller
+    // ones two; the instance launchers size the grid (CTAs per SM).
     L.stages = pass.m == kMaxTileQubits ? 3u : 2u;
-    L.threads *= groups;
-    L.smem = groups * L.stages * (size_t{1} << pass.m) * sizeof(double2) + staged +
-             (groups - 1) * size_t{pass.param_len} * sizeof(double);
+    L.smem = L.stages * (size_t{1} << pass.m) * sizeof(double2) + staged;
+    L.sm_count = sm_count;
+    L.heavy = pass.heavy;
     // A batch adds the bindings above the n qubits: ntiles counts every
     // binding's tiles, and n grows to the bits the binding index occupies.
     L.ntiles = (uint64_t{1} << n) >> pass.m;
@@ -262,9 +259,6 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const uint32_
         L.ntiles *= batch->bindings;
         while ((uint64_t{1} << (L.n_all - n)) < batch->bindings) ++L.n_all;
     }
-    const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m >= 11 ? 1u : 2u);
-    const uint64_t ctas = (L.ntiles + groups - 1) / groups;
-    L.grid = static_cast<int>(ctas < cap ? ctas : cap);
     const int rc = pass.m == 11 ? launch_tile_m11(L) : pass.m == 12 ? launch_tile_m12(L) : launch_tile_generic(L);
     note_launches(1);
     return rc;

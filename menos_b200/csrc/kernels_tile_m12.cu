@@ -3,9 +3,11 @@
 
 namespace mb2 {
 
-int launch_tile_m12(const TileLaunch& L) {
-    return L.n_all <= 32 ? tile::launch_instance<256, 1, 12, uint32_t>(L)
-                         : tile::launch_instance<256, 1, 12, uint64_t>(L);
+int launch_tile_m12(TileLaunch& L) {
+    const uint64_t cap = static_cast<uint64_t>(L.sm_count);
+    L.grid = static_cast<int>(L.ntiles < cap ? L.ntiles : cap);
+    return L.n_all <= 32 ? tile::launch_instance<256, 1, 12, uint32_t, true>(L)
+                         : tile::launch_instance<256, 1, 12, uint64_t, true>(L);
 }
 
 }  // namespace mb2

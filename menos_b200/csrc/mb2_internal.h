@@ -100,6 +100,7 @@ struct TilePass {
     // [param_lo, param_lo + param_len), staged after the pass's data.
     uint32_t param_lo = 0;
     uint32_t param_len = 0;
+    bool heavy = false;  // has kGen2, kDiagK or kSmem words
 };
 
 // Compact instruction stream of the complex128 tile kernel, written from the
@@ -215,15 +216,18 @@ struct TileLaunch {
     uint32_t param_len = 0;
     uint32_t bshift = 0;
     uint32_t stages = 2;
-    int grid = 0;
+    int grid = 0;       // set by the instance launcher
+    int sm_count = 0;
+    bool heavy = false;  // the pass has dense 2q, wide diagonal or shared-memory blocks
     uint32_t threads = 0;
     size_t smem = 0;
     void* stream = nullptr;
 };
-constexpr size_t kTileSmemMax = 227 * 1024;
-int launch_tile_generic(const TileLaunch& L);  // any tile width, 64-bit indices
-int launch_tile_m11(const TileLaunch& L);      // 11-qubit tiles
-int launch_tile_m12(const TileLaunch& L);      // 12-qubit tiles
+constexpr size_t kTileSmemMax = 227 * 1024;  // per block
+constexpr size_t kSmemPerSm = 228 * 1024;    // per SM (1 KiB of it reserved per resident block)
+int launch_tile_generic(TileLaunch& L);  // any tile width, 64-bit indices
+int launch_tile_m11(TileLaunch& L);      // 11-qubit tiles
+int launch_tile_m12(TileLaunch& L);      // 12-qubit tiles
 // Expectation of num_terms Pauli terms: partials (num_terms * kExpBlocks * 2
 // doubles) then the fixed-order finish into out (num_terms * 2 doubles), all
 // device pointers.

@@ -60,6 +60,7 @@ void encode_compact(TileProgram& prog) {
             return is_param(g) ? pass.sdata_count + (g.data - pass.param_lo) : g.data;
         };
         auto& w = prog.words;
+        bool heavy = false;
         uint32_t reg[kRegQubits] = {0, 1, 2, 3};
         // Pending sign monomials (canonical words), toggled so pairs cancel.
         std::map<uint32_t, bool> signs;
@@ -139,6 +140,7 @@ void encode_compact(TileProgram& prog) {
                     w.push_back(cop::kEnd);
                     break;
                 case TOP_SMEM: {
+                    heavy = true;
                     uint32_t packed = 0;
                     for (uint32_t t = 0; t < g.k; ++t) packed |= static_cast<uint32_t>(g.pos[t]) << (4 * t);
                     w.push_back(cop::kSmem | (static_cast<uint32_t>(g.k) << 8));
@@ -167,7 +169,10 @@ void encode_compact(TileProgram& prog) {
                             w.push_back(header(cop::kMono2 + pr, 0, 0, off));
                             w.push_back(g.aux);
                             break;
-                        default: w.push_back(header(cop::kGen2 + pr, 0, 0, off)); break;
+                        default:
+                            heavy = true;
+                            w.push_back(header(cop::kGen2 + pr, 0, 0, off));
+                            break;
                     }
                     break;
                 }
@@ -190,6 +195,7 @@ void encode_compact(TileProgram& prog) {
                             w.push_back(c0 | (c1 << 4));
                         }
                     } else {
+                        heavy = true;
                         uint32_t packed = 0;
                         for (uint32_t t = 0; t < g.k; ++t) packed |= static_cast<uint32_t>(g.pos[t]) << (4 * t);
                         w.push_back(header(cop::kDiagK, g.k, 0, off));
@@ -202,6 +208,7 @@ void encode_compact(TileProgram& prog) {
             }
         }
         flush_signs();
+        pass.heavy = heavy;
         while (w.size() & 3u) w.push_back(cop::kEnd);  // 16-byte multiple: the staged data follows
         pass.word_count = static_cast<uint32_t>(w.size()) - pass.word_begin;
     }

@@ -174,6 +174,12 @@ __device__ __forceinline__ void diag_rt(double2 (&a)[kNA], const Diag4& D, uint3
     }
 }
 
+// A dense two-qubit block in registers, compiled only into the FULL variant.
+template <int P0, int P1, bool FULL>
+__device__ __forceinline__ void gen2_if(double2 (&a)[kNA], const double* md) {
+    if constexpr (FULL) g2<P0, P1, TK_GEN>(a, md, 0u);
+}
+
 // Exact permutations (every nonzero entry (1,0)): register moves only.
 // TK_X: 1q swap; TK_SW12 / TK_SW13 / TK_SW23: 2q, exchange local indices
 // (1,2) (SWAP), (1,3) (CX, control = operand 0), (2,3) (CX, control = operand 1).
@@ -219,8 +225,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // The instructions of one pass applied to one tile held in shared memory
 // (canonical layout on entry and exit).  `sync` is the barrier of the
 // threads that share the tile; parametric data sits pshift doubles past the
-// staged data's end.
-template <int MT, typename SYNC>
+// staged data's end.  FULL = false compiles out the rare heavy instructions
+// (dense two-qubit blocks, wide diagonals, shared-memory blocks), whose
+// register needs would otherwise set the count for the whole kernel; the
+// launcher picks that variant only for passes without them.
+template <int MT, bool FULL, typename SYNC>
 __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const uint32_t* __restrict__ sw,
                                              uint32_t nwords, const double* __restrict__ sd, uint32_t nsdata,
                                              uint32_t pshift, const double* __restrict__ gdata, uint32_t tid,
@@ -290,7 +299,7 @@ case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
                     MB2_CASE4(cop::kReal1, (g1<P, TK_REAL>(a, md, 0u)))
                     MB2_CASE4(cop::kMono1, (g1<P, TK_MONO>(a, md, aux)))
                     MB2_CASE4(cop::kX1, (perm1<P>(a)))
-                    MB2_CASE12(cop::kGen2, (g2<P0, P1, TK_GEN>(a, md, 0u)))
+                    MB2_CASE12(cop::kGen2, (gen2_if<P0, P1, FULL>(a, md)))
                     MB2_CASE12(cop::kMono2, (g2<P0, P1, TK_MONO>(a, md, sw[pc++])))
                     MB2_CASE12(cop::kSw12, (perm2<P0, P1, TK_SW12>(a)))
                     MB2_CASE12(cop::kSw13, (perm2<P0, P1, TK_SW13>(a)))
@@ -339,6 +348,7 @@ case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
                         for (int j = 0; j < kNA; ++j) a[j] = cneg_if(a[j], (M >> j) & 1u);
                     } break;
                     default: {  // cop::kDiagK: any k, entry index per amplitude
+                        if constexpr (!FULL) break;
                         const uint32_t pos = sw[pc++];
                         uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
                         for (uint32_t b = 0; b < aux; ++b) {
@@ -361,7 +371,7 @@ case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
 #pragma unroll
             for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
             sync();
-        } else if (op0 == cop::kSmem) {
+        } else if (FULL && op0 == cop::kSmem) {
             // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
             const uint32_t k = (w0 >> 8) & 0xffu, dim = 1u << k;
             const uint32_t pos = sw[pc + 1];
@@ -410,7 +420,7 @@ case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
 // amplitudes.  A tile's base index is its number deposited on the bits
 // outside the tile (nmask); moving gridDim.x tiles on is the masked add
 // ((base | ~nmask) + step) & nmask, step = deposit(gridDim.x).
-template <int MAXT, int MINB, int MT, typename IDX>
+template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask,
                 const uint32_t* __restrict__ words, uint32_t nwords, const double* __restrict__ sdata,
@@ -498,7 +508,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
         else cp_async_wait<1>();
         __syncthreads();
 
-        compute_tile<MT>(tile, sw, nwords, sd, nsdata, 0u, gdata, tid, m, [] { __syncthreads(); });
+        compute_tile<MT, FULL>(tile, sw, nwords, sd, nsdata, 0u, gdata, tid, m, [] { __syncthreads(); });
 
         // Store: canonical mapping, -0.0 normalised.
         const IDX b0 = cbase + off_lo;
@@ -509,164 +519,22 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
 }
 
-// The 11-qubit pass as two groups of four warps per CTA ("ping-pong"): each
-// group streams its own tiles through its own buffers, and the two groups
-// take turns at the gates, so that one group's loads, stores and waits run
-// while the other group's FP64 work has the SMs' FP64 pipes to itself.  (Two
-// independent CTAs per SM drift into lockstep -- both computing, then both
-// moving data -- which leaves each resource idle half the time.)
-//
-// Turns are passed with two named barriers of 256 threads, X and Y:
-//   group A (tiles 2b, 2b + 2G, ...):  [k >= 1: sync X] gates k [k < KB: arrive Y]
-//   group B (tiles 2b + 1, ...):       sync Y, gates k [k < KA - 1: arrive X]
-// so gates run A0 B0 A1 B1 ...; KA is KB or KB + 1, and every sync meets
-// exactly one arrive (a host-side simulation of the protocol checks this for
-// every KA, KB).  Barriers 1 and 2 are each group's own.
-template <int MT, typename IDX>
-__global__ void __launch_bounds__(256, 1)
-    k_tile_pingpong(double2* __restrict__ st, uint32_t n, uint64_t smask, const uint32_t* __restrict__ words,
-                    uint32_t nwords, const double* __restrict__ sdata, uint32_t nsdata,
-                    const double* __restrict__ gdata, uint64_t ntiles, const double* __restrict__ pdata,
-                    uint32_t pstride, uint32_t param_lo, uint32_t param_len, uint32_t bshift, uint32_t stages) {
-    extern __shared__ double2 smem_tiles[];
-    constexpr uint32_t m = MT;
-    constexpr uint32_t tbits = m - kRegQubits;
-    constexpr uint32_t tile_amps = 1u << m;
-    constexpr uint32_t kGroupThreads = 1u << tbits;
-    const uint32_t grp = threadIdx.x >> tbits;  // 0: A, 1: B
-    const uint32_t tid = threadIdx.x & (kGroupThreads - 1);
-    // Shared memory: group A's tile buffers, group B's, the words, the staged
-    // data, then A's and B's parametric slices.
-    uint32_t* sw = reinterpret_cast<uint32_t*>(smem_tiles + 2 * stages * tile_amps);
-    double* sd = reinterpret_cast<double*>(sw + nwords);
-    for (uint32_t i = threadIdx.x; i < nwords / 4; i += blockDim.x)
-        reinterpret_cast<uint4*>(sw)[i] = __ldg(reinterpret_cast<const uint4*>(words) + i);
-    for (uint32_t i = threadIdx.x; i < nsdata; i += blockDim.x) sd[i] = __ldg(sdata + i);
-    __syncthreads();
-    double2* tiles = smem_tiles + grp * stages * tile_amps;
-    const uint32_t pshift = grp * param_len;
-    const uint32_t bar_group = 1u + grp;
-    auto group_sync = [bar_group] { asm volatile("bar.sync %0, %1;" ::"r"(bar_group), "r"(kGroupThreads) : "memory"); };
-
-    IDX off_lo = 0, hib0 = 0, hib1 = 0, hib2 = 0, hib3 = 0;
-    {
-        uint32_t b = 0;
-        for (uint32_t p = 0; p < n; ++p) {
-            if (!((smask >> p) & 1u)) continue;
-            if (b < tbits) {
-                off_lo |= static_cast<IDX>((tid >> b) & 1u) << p;
-            } else {
-                const IDX v = IDX{1} << p;
-                const uint32_t r = b - tbits;
-                if (r == 0) hib0 = v;
-                else if (r == 1) hib1 = v;
-                else if (r == 2) hib2 = v;
-                else hib3 = v;
-            }
-            ++b;
-        }
-    }
-    // Group g of CTA b takes the tiles 2b + g + k * 2G (G = gridDim.x).
-    const uint64_t first = 2ull * blockIdx.x + grp, vgrid = 2ull * gridDim.x;
-    auto count_of = [&](uint64_t v) -> uint64_t { return v < ntiles ? (ntiles - v + vgrid - 1) / vgrid : 0; };
-    const uint64_t KA = count_of(2ull * blockIdx.x), KB = count_of(2ull * blockIdx.x + 1);
-    const uint64_t nmask64 = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~smask;
-    const IDX nmask = static_cast<IDX>(nmask64);
-    const IDX step = static_cast<IDX>(pdep64(vgrid, nmask64));
-    auto advance = [&](IDX b) -> IDX { return ((b | ~nmask) + step) & nmask; };
-    const uint32_t s_tid = swz(tid);
-    auto reg_off = [&](int j) -> IDX {
-        return ((j & 1) ? hib0 : IDX{0}) + ((j & 2) ? hib1 : IDX{0}) + ((j & 4) ? hib2 : IDX{0}) +
-               ((j & 8) ? hib3 : IDX{0});
-    };
-    auto slot = [&](int j) -> uint32_t { return s_tid ^ swz(static_cast<uint32_t>(j) << tbits); };
-    auto prefetch = [&](IDX base, double2* buf) {
-        const IDX b0 = base + off_lo;
-#pragma unroll
-        for (int j = 0; j < kNA; ++j) cp_async16(buf + slot(j), st + (b0 + reg_off(j)));
-        cp_async_commit();
-    };
-    uint64_t tp = first;
-    IDX pbase = static_cast<IDX>(pdep64(first, nmask64));
-    IDX cbase = pbase;
-    for (uint32_t sg = 0; sg + 1 < stages; ++sg) {
-        if (tp < ntiles) prefetch(pbase, tiles + sg * tile_amps);
-        else cp_async_commit();
-        tp += vgrid;
-        pbase = advance(pbase);
-    }
-    uint32_t cur = 0, nxt = stages - 1;
-    uint64_t k = 0;
-    for (uint64_t t = first; t < ntiles; t += vgrid, ++k) {
-        double2* tile = tiles + cur * tile_amps;
-        if (tp < ntiles) prefetch(pbase, tiles + nxt * tile_amps);
-        else cp_async_commit();
-        tp += vgrid;
-        pbase = advance(pbase);
-        cur = cur + 1 == stages ? 0u : cur + 1;
-        nxt = nxt + 1 == stages ? 0u : nxt + 1;
-        if (param_len != 0) {
-            const double2* src = reinterpret_cast<const double2*>(pdata + (t >> bshift) * pstride + param_lo);
-            double2* dst = reinterpret_cast<double2*>(sd + nsdata + pshift);
-            for (uint32_t i = tid; i < param_len / 2; i += kGroupThreads) dst[i] = __ldg(src + i);
-        }
-        if (stages == 3) cp_async_wait<2>();
-        else cp_async_wait<1>();
-        group_sync();
-        // Wait for the turn: A's gates k follow B's gates k - 1, B's follow A's k.
-        if (grp == 0) {
-            if (k >= 1) asm volatile("bar.sync 3, 256;" ::: "memory");
-        } else {
-            asm volatile("bar.sync 4, 256;" ::: "memory");
-        }
-        compute_tile<MT>(tile, sw, nwords, sd, nsdata, pshift, gdata, tid, m, group_sync);
-        if (grp == 0) {
-            if (k < KB) asm volatile("bar.arrive 4, 256;" ::: "memory");
-        } else {
-            if (k + 1 < KA) asm volatile("bar.arrive 3, 256;" ::: "memory");
-        }
-        const IDX b0 = cbase + off_lo;
-#pragma unroll
-        for (int j = 0; j < kNA; ++j) st[b0 + reg_off(j)] = canon(tile[slot(j)]);
-        cbase = advance(cbase);
-        group_sync();  // the buffer is the target of a later prefetch
-    }
-}
-
-template <int MT, typename IDX>
-int launch_pingpong(const TileLaunch& L) {
-    static size_t dyn_max = 0;
-    if (dyn_max == 0) {
-        cudaFuncAttributes fa{};
-        if (cudaFuncGetAttributes(&fa, k_tile_pingpong<MT, IDX>) != cudaSuccess) return launch_status();
-        dyn_max = kTileSmemMax - fa.sharedSizeBytes;
-        if (cudaFuncSetAttribute(k_tile_pingpong<MT, IDX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(dyn_max)) != cudaSuccess)
-            return launch_status();
-    }
-    if (L.smem > dyn_max) return MB2_ERR_INVALID;
-    k_tile_pingpong<MT, IDX><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
-        static_cast<double2*>(L.amps), L.n_all, L.smask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata, L.ntiles,
-        L.pdata, L.pstride, L.param_lo, L.param_len, L.bshift, L.stages);
-    return launch_status();
-}
-
 // Launches one instance; the shared-memory limit is raised once per instance.
-template <int MAXT, int MINB, int MT, typename IDX>
+template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
 int launch_instance(const TileLaunch& L) {
     // The dynamic limit is what the static shared memory leaves of the
     // per-block maximum (a larger request is refused by the driver).
     static size_t dyn_max = 0;
     if (dyn_max == 0) {
         cudaFuncAttributes fa{};
-        if (cudaFuncGetAttributes(&fa, k_tile_pass<MAXT, MINB, MT, IDX>) != cudaSuccess) return launch_status();
+        if (cudaFuncGetAttributes(&fa, k_tile_pass<MAXT, MINB, MT, IDX, FULL>) != cudaSuccess) return launch_status();
         dyn_max = kTileSmemMax - fa.sharedSizeBytes;
-        if (cudaFuncSetAttribute(k_tile_pass<MAXT, MINB, MT, IDX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_tile_pass<MAXT, MINB, MT, IDX, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(dyn_max)) != cudaSuccess)
             return launch_status();
     }
     if (L.smem > dyn_max) return MB2_ERR_INVALID;
-    k_tile_pass<MAXT, MINB, MT, IDX><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
+    k_tile_pass<MAXT, MINB, MT, IDX, FULL><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
         static_cast<double2*>(L.amps), L.n_all, L.m, L.smask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata,
         L.ntiles, L.pdata, L.pstride, L.param_lo, L.param_len, L.bshift, L.stages);
     return launch_status();
