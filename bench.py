@@ -31,6 +31,15 @@ METRIC = "circuits/s, 30q complex128 job (brick d40 + QFT, norm, 64 Paulis, 1e6 
 UNIT = "circuits/s"
 
 
+def kernel_launches() -> int:
+    """Kernels the library has launched so far (its own counter, mb2_kernel_launches)."""
+    import ctypes as C
+    from menos_b200 import _lib
+    v = C.c_uint64()
+    _lib.check(_lib.lib().mb2_kernel_launches(C.byref(v)), None, "mb2_kernel_launches")
+    return int(v.value)
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -211,6 +220,7 @@ def main():
     clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = kernel_launches()
     with torch.cuda.stream(stream):
         ev0.record(stream)
     for _ in range(args.steps):
@@ -218,6 +228,7 @@ def main():
     ev1.record(stream)
     ev1.synchronize()
     job_ms = ev0.elapsed_time(ev1)
+    launches = kernel_launches() - launches0
     # ---- the sweep alone: average tile-pass launch duration
     sweep_ms = []
     for _ in range(max(2, args.steps)):
@@ -283,7 +294,7 @@ def main():
                  "model_ops_per_amp": int(stats.fp64_ops_per_amp), "copy_gbs_probe": round(copy_peak, 1)},
         "e2e": {"value": round(world * args.steps / e2e_s, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": args.steps * (passes + 1 + 2 + 2),
+        "gpu_launches": launches,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -522,13 +522,23 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
         return MB2_OK;
     }
     // Uniforms exactly as common::Rng (src/common/rng.cpp:176-186), sorted
-    // (src/engines/dense/sample.cpp:37-42).
+    // (src/engines/dense/sample.cpp:37-42).  u = k * 2^-53 with k the top 53
+    // bits of a word, so sorting the integers k sorts the uniforms; an LSD
+    // radix sort (five 11-bit digits) does it in linear time.
     std::vector<double> u(shots);
     {
+        std::vector<uint64_t> key(shots), tmp(shots);
         std::mt19937_64 eng(seed);
-        for (uint64_t i = 0; i < shots; ++i) u[i] = static_cast<double>(eng() >> 11) * (1.0 / 9007199254740992.0);
+        for (uint64_t i = 0; i < shots; ++i) key[i] = eng() >> 11;
+        for (uint32_t shift = 0; shift < 55; shift += 11) {
+            std::vector<uint64_t> bucket(2049, 0);
+            for (uint64_t i = 0; i < shots; ++i) ++bucket[((key[i] >> shift) & 2047u) + 1];
+            for (uint32_t b = 0; b < 2048; ++b) bucket[b + 1] += bucket[b];
+            for (uint64_t i = 0; i < shots; ++i) tmp[bucket[(key[i] >> shift) & 2047u]++] = key[i];
+            key.swap(tmp);
+        }
+        for (uint64_t i = 0; i < shots; ++i) u[i] = static_cast<double>(key[i]) * (1.0 / 9007199254740992.0);
     }
-    std::sort(u.begin(), u.end());
     // The walk (sample.cpp:55-69), reproduced exactly on the device.
     const size_t al_u = (shots * 8 + 255) & ~size_t{255};
     const size_t need = 2 * al_u + mb2::sample_scratch_bytes(s->n, shots);
@@ -543,24 +553,32 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
     std::vector<uint64_t> basis(shots);
     MB2_CUDA(s->ctx, cudaMemcpyAsync(basis.data(), dev_basis, shots * 8, cudaMemcpyDeviceToHost, s->stream));
     MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
-    // Outcomes through the measure targets, ascending, with counts.
-    std::vector<uint64_t> oc(shots);
-    for (uint64_t i = 0; i < shots; ++i) {
+    // Outcomes through the measure targets, ascending, with counts.  The walk
+    // gives non-decreasing basis indices (sorted uniforms against the
+    // cumulative sum), so runs are counted first; the distinct outcomes are
+    // sorted only when the target map does not keep their order.
+    std::vector<std::pair<uint64_t, uint64_t>> oc;
+    for (uint64_t i = 0; i < shots;) {
+        uint64_t j = i + 1;
+        while (j < shots && basis[j] == basis[i]) ++j;
         uint64_t o = 0;
         for (uint32_t t = 0; t < num_targets; ++t)
             if ((basis[i] >> targets[2 * t]) & 1u) o |= uint64_t{1} << targets[2 * t + 1];
-        oc[i] = o;
+        oc.emplace_back(o, j - i);
+        i = j;
     }
-    std::sort(oc.begin(), oc.end());
+    bool ordered = true;
+    for (size_t i = 1; i < oc.size() && ordered; ++i) ordered = oc[i - 1].first < oc[i].first;
+    if (!ordered) std::sort(oc.begin(), oc.end());
     uint64_t d = 0;
-    for (uint64_t i = 0; i < shots; ++i) {
-        if (d > 0 && outcomes[d - 1] == oc[i]) {
-            counts[d - 1] += 1;
+    for (const auto& [o, c] : oc) {
+        if (d > 0 && outcomes[d - 1] == o) {
+            counts[d - 1] += c;
             continue;
         }
         if (d >= *num_outcomes) return fail(s->ctx, MB2_ERR_INVALID, "outcome capacity too small");
-        outcomes[d] = oc[i];
-        counts[d] = 1;
+        outcomes[d] = o;
+        counts[d] = c;
         ++d;
     }
     *num_outcomes = d;

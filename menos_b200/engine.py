@@ -139,7 +139,7 @@ class DeviceState:
         self._chk(lib().mb2_sample(self.h, shots, seed, t.ctypes.data if len(t) else None, len(t) // 2,
                                    outc.ctypes.data, cnt.ctypes.data, C.byref(nout)), "mb2_sample")
         d = nout.value
-        return {int(o): int(c) for o, c in zip(outc[:d], cnt[:d])}
+        return dict(zip(outc[:d].tolist(), cnt[:d].tolist()))
 
     def copy_out(self) -> np.ndarray:
         dt = np.complex128 if self.precision == C128 else np.complex64
