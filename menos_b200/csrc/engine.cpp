@@ -474,6 +474,20 @@ int mb2_expectation(mb2_state* s, const uint64_t* x_masks, const uint64_t* z_mas
     MB2_CUDA(s->ctx, cudaMemcpyAsync(base + off_s, host.data(), host.size(), cudaMemcpyHostToDevice, s->stream));
     auto* partials = reinterpret_cast<double*>(base + off_p);
     for (const mb2::PauliGroupPlan& g : plan.groups) {
+        if (g.nterms == 1 || g.c + g.d < mb2::kPauliMinTileQubits) {
+            // Nothing to share (or a state too small for the grouped tiles):
+            // one streaming read per term, its partials in place.
+            for (uint32_t i = 0; i < g.nterms; ++i) {
+                const uint32_t t = plan.terms[g.term_off + i].out;
+                const int rc = mb2::launch_expectation_partials(
+                    s->amps, s->n, reinterpret_cast<const uint64_t*>(base) + t,
+                    reinterpret_cast<const uint64_t*>(base + off_z) + t, 1,
+                    partials + 2 * static_cast<size_t>(t) * mb2::kExpBlocks, s->stream, s->precision);
+                if (rc != MB2_OK)
+                    return fail(s->ctx, rc, std::string("expectation launch: ") + mb2::last_cuda_error_string());
+            }
+            continue;
+        }
         const int rc = mb2::launch_pauli_group(
             s->amps, s->n, g.c, g.d, reinterpret_cast<const uint64_t*>(base + off_s) + g.span_off, g.free_mask,
             base + off_t + size_t{g.term_off} * sizeof(mb2::PauliGroupTerm), g.nterms, partials, mb2::kExpBlocks,

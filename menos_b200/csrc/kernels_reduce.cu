@@ -142,20 +142,35 @@ __global__ void k_expectation_finish(const double* __restrict__ partials, uint32
 using GroupTerm = PauliGroupTerm;
 constexpr uint32_t kChunkWords = (1u << kPauliMaxSpan) / 32;
 
+// cp.async of one amplitude (16 or 8 bytes), global -> shared.
+__device__ __forceinline__ void cp_async_amp(double2* smem, const double2* gmem) {
+    const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_amp(float2* smem, const float2* gmem) {
+    const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// Cosets are processed with two shared-memory buffers: the next coset's
+// amplitudes are gathered with cp.async while this one is reduced.  Each
+// thread keeps two accumulators per term (alternate pairs) so consecutive
+// adds do not wait on each other.
 template <typename A>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     k_pauli_group(const A* __restrict__ st, uint32_t c, uint32_t d, const uint64_t* __restrict__ span,
                   uint64_t free_mask, const GroupTerm* __restrict__ terms, uint32_t nterms, uint64_t ncosets,
                   double* __restrict__ partials) {
-    extern __shared__ double2 gtile[];
+    extern __shared__ __align__(16) unsigned char gsm[];
     __shared__ uint64_t sspan[1u << kPauliMaxSpan];
     __shared__ uint32_t cpar[kMaxGroupTerms][kChunkWords];  // parity of z_hi & span[k], bit k
-    __shared__ uint32_t rpar[kMaxGroupTerms];               // parity of z_hi & rep, this coset
     __shared__ uint32_t tdl[kMaxGroupTerms], tzl[kMaxGroupTerms], tmode[kMaxGroupTerms];
     __shared__ uint64_t tzh[kMaxGroupTerms];
     __shared__ double red[kThreads / 32];
     const uint32_t tile_amps = 1u << (c + d);
     const uint32_t nchunks = 1u << d;
+    A* buf0 = reinterpret_cast<A*>(gsm);
+    A* buf1 = buf0 + tile_amps;
     for (uint32_t i = threadIdx.x; i < nchunks; i += kThreads) sspan[i] = span[i];
     for (uint32_t t = threadIdx.x; t < nterms; t += kThreads) {
         const GroupTerm T = terms[t];
@@ -174,65 +189,99 @@ __global__ void __launch_bounds__(kThreads)
                 bits |= static_cast<uint32_t>(__popcll(tzh[t] & sspan[w * 32 + b]) & 1) << b;
         cpar[t][w] = bits;
     }
-    double acc[kMaxGroupTerms];
-#pragma unroll
-    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) acc[t] = 0.0;
     const uint32_t lowmask = (1u << c) - 1;
-    for (uint64_t cs = blockIdx.x; cs < ncosets; cs += gridDim.x) {
-        // Coset representative: the bits of cs deposited on the free
-        // (non-pivot) high bits; the pivots stay zero.
-        uint64_t rep = 0;
-        {
-            uint64_t v = cs, mask = free_mask;
-            while (mask != 0) {
-                const uint64_t low = mask & (~mask + 1);
-                if (v & 1) rep |= low;
-                v >>= 1;
-                mask ^= low;
-            }
+    // Coset representatives: the coset number deposited on the free (non-
+    // pivot) high bits; moving gridDim.x cosets on is a masked add.
+    auto deposit = [&](uint64_t v) {
+        uint64_t r = 0, mask = free_mask;
+        while (mask != 0) {
+            const uint64_t low = mask & (~mask + 1);
+            if (v & 1) r |= low;
+            v >>= 1;
+            mask ^= low;
         }
-        __syncthreads();  // the previous coset's reads are done
+        return r;
+    };
+    const uint64_t rstep = deposit(gridDim.x);
+    auto advance = [&](uint64_t r) { return ((r | ~free_mask) + rstep) & free_mask; };
+    auto gather = [&](uint64_t rep, A* buf) {
         for (uint32_t L = threadIdx.x; L < tile_amps; L += kThreads) {
             const uint64_t m = ((rep ^ sspan[L >> c]) << c) | (L & lowmask);
-            gtile[L] = as_d2(st[m]);
+            cp_async_amp(buf + L, st + m);
         }
-        if (threadIdx.x < nterms) rpar[threadIdx.x] = __popcll(tzh[threadIdx.x] & rep) & 1;
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    __syncthreads();  // sspan, cpar ready
+    double acc0[kMaxGroupTerms], acc1[kMaxGroupTerms];
+#pragma unroll
+    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
+        acc0[t] = 0.0;
+        acc1[t] = 0.0;
+    }
+    uint64_t rep = deposit(blockIdx.x);
+    if (blockIdx.x < ncosets) gather(rep, buf0);
+    A* cur = buf0;
+    A* nxt = buf1;
+    for (uint64_t cs = blockIdx.x; cs < ncosets; cs += gridDim.x) {
+        const uint64_t rep_next = advance(rep);
+        if (cs + gridDim.x < ncosets) gather(rep_next, nxt);
+        else asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         __syncthreads();
 #pragma unroll
         for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
             if (t < nterms) {
-                const uint32_t dl = tdl[t], zl = tzl[t], mode = tmode[t], rp = rpar[t];
+                const uint32_t dl = tdl[t], zl = tzl[t], mode = tmode[t];
+                const uint32_t rp = static_cast<uint32_t>(__popcll(tzh[t] & rep)) & 1u;
                 const uint32_t* cp = cpar[t];
                 if (mode == 0) {
-                    for (uint32_t L = threadIdx.x; L < tile_amps; L += kThreads) {
-                        const uint32_t k = L >> c;
-                        const uint32_t neg = rp ^ (cp[k >> 5] >> (k & 31)) ^ __popc(zl & L);
-                        const double2 a = gtile[L];
-                        const double p = __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
-                        acc[t] = (neg & 1) ? __dsub_rn(acc[t], p) : __dadd_rn(acc[t], p);
+                    for (uint32_t L = threadIdx.x; L < tile_amps; L += 2 * kThreads) {
+                        const uint32_t L1 = L + kThreads;
+                        const uint32_t k0 = L >> c, k1 = L1 >> c;
+                        const uint32_t n0 = rp ^ (cp[k0 >> 5] >> (k0 & 31)) ^ __popc(zl & L);
+                        const uint32_t n1 = rp ^ (cp[k1 >> 5] >> (k1 & 31)) ^ __popc(zl & L1);
+                        const double2 a0 = as_d2(cur[L]), a1 = as_d2(cur[L1]);
+                        const double p0 = __dadd_rn(__dmul_rn(a0.x, a0.x), __dmul_rn(a0.y, a0.y));
+                        const double p1 = __dadd_rn(__dmul_rn(a1.x, a1.x), __dmul_rn(a1.y, a1.y));
+                        acc0[t] = (n0 & 1) ? __dsub_rn(acc0[t], p0) : __dadd_rn(acc0[t], p0);
+                        acc1[t] = (n1 & 1) ? __dsub_rn(acc1[t], p1) : __dadd_rn(acc1[t], p1);
                     }
                 } else {
                     const uint32_t hb = 31 - __clz(dl);
                     const uint32_t below = (1u << hb) - 1;
-                    for (uint32_t q = threadIdx.x; q < tile_amps / 2; q += kThreads) {
-                        const uint32_t L = ((q & ~below) << 1) | (q & below);
-                        const uint32_t k = L >> c;
-                        const uint32_t neg = rp ^ (cp[k >> 5] >> (k & 31)) ^ __popc(zl & L);
-                        const double2 a = gtile[L], b = gtile[L ^ dl];
-                        const double v = mode == 1 ? __dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y))
-                                                   : __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x));
-                        acc[t] = (neg & 1) ? __dsub_rn(acc[t], v) : __dadd_rn(acc[t], v);
+                    for (uint32_t q = threadIdx.x; q < tile_amps / 2; q += 2 * kThreads) {
+                        const uint32_t q1 = q + kThreads;
+                        const uint32_t L0 = ((q & ~below) << 1) | (q & below);
+                        const uint32_t L1 = ((q1 & ~below) << 1) | (q1 & below);
+                        const uint32_t k0 = L0 >> c, k1 = L1 >> c;
+                        const uint32_t n0 = rp ^ (cp[k0 >> 5] >> (k0 & 31)) ^ __popc(zl & L0);
+                        const uint32_t n1 = rp ^ (cp[k1 >> 5] >> (k1 & 31)) ^ __popc(zl & L1);
+                        const double2 a0 = as_d2(cur[L0]), b0 = as_d2(cur[L0 ^ dl]);
+                        const double2 a1 = as_d2(cur[L1]), b1 = as_d2(cur[L1 ^ dl]);
+                        const double v0 = mode == 1 ? __dadd_rn(__dmul_rn(a0.x, b0.x), __dmul_rn(a0.y, b0.y))
+                                                    : __dsub_rn(__dmul_rn(a0.x, b0.y), __dmul_rn(a0.y, b0.x));
+                        const double v1 = mode == 1 ? __dadd_rn(__dmul_rn(a1.x, b1.x), __dmul_rn(a1.y, b1.y))
+                                                    : __dsub_rn(__dmul_rn(a1.x, b1.y), __dmul_rn(a1.y, b1.x));
+                        acc0[t] = (n0 & 1) ? __dsub_rn(acc0[t], v0) : __dadd_rn(acc0[t], v0);
+                        acc1[t] = (n1 & 1) ? __dsub_rn(acc1[t], v1) : __dadd_rn(acc1[t], v1);
                     }
                 }
             }
         }
+        __syncthreads();  // this buffer is the target of the gather after next
+        rep = rep_next;
+        A* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
     }
-    // Per term: this CTA's sum in a fixed order (lanes, then warps), written
-    // as (re, im) of the pair sum before the i^popcount(x & z) factor.
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    // Per term: this CTA's sum in a fixed order (the two accumulators, lanes,
+    // then warps), written as (re, im) of the pair sum before the
+    // i^popcount(x & z) factor.
 #pragma unroll
     for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
         if (t < nterms) {
-            double r = acc[t];
+            double r = __dadd_rn(acc0[t], acc1[t]);
             for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
             __syncthreads();
             if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r;
@@ -258,11 +307,14 @@ int launch_pauli_group(const void* amps, uint32_t n, uint32_t c, uint32_t d, con
     if (nterms > kMaxGroupTerms || c + d > kPauliTileQubits || d > kPauliMaxSpan) return MB2_ERR_INVALID;
     const auto s = static_cast<cudaStream_t>(stream);
     const uint64_t ncosets = uint64_t{1} << (n - c - d);
-    const size_t smem = (size_t{1} << (c + d)) * sizeof(double2);
+    // Two buffers of 2^(c+d) amplitudes; each thread takes two amplitudes (or
+    // two pairs) per step, so a tile holds at least 4 * kThreads of them.
+    if (c + d < kPauliMinTileQubits) return MB2_ERR_INVALID;
+    const size_t smem = 2 * (size_t{1} << (c + d)) * (precision == MB2_C64 ? sizeof(float2) : sizeof(double2));
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_pauli_group<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-        cudaFuncSetAttribute(k_pauli_group<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        cudaFuncSetAttribute(k_pauli_group<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
+        cudaFuncSetAttribute(k_pauli_group<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
         attr = true;
     }
     const auto* terms = static_cast<const GroupTerm*>(dev_terms);
@@ -280,6 +332,20 @@ int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const
                               const uint64_t* dev_z, uint32_t num_terms, double* dev_out, void* stream) {
     k_expectation_finish<<<(num_terms + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
         dev_partials, blocks, dev_x, dev_z, num_terms, dev_out);
+    note_launches(1);
+    return launch_status();
+}
+
+int launch_expectation_partials(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
+                                uint32_t num_terms, double* dev_partials, void* stream, int precision) {
+    if (num_terms == 0) return MB2_OK;
+    const auto s = static_cast<cudaStream_t>(stream);
+    const dim3 grid(kExpBlocks, num_terms);
+    if (precision == MB2_C64)
+        k_expectation<float2><<<grid, kThreads, 0, s>>>(static_cast<const float2*>(amps), n, dev_x, dev_z, dev_partials);
+    else
+        k_expectation<double2><<<grid, kThreads, 0, s>>>(static_cast<const double2*>(amps), n, dev_x, dev_z,
+                                                         dev_partials);
     note_launches(1);
     return launch_status();
 }

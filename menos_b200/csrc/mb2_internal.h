@@ -263,8 +263,9 @@ int probe_rates(int sm_count, double* fp64_per_s, double* copy_gbs);
 // share one read of the state, in tiles of 2^(c+d) <= 2^12 amplitudes.
 // Partials are written at (term.out * grid + CTA).
 constexpr uint32_t kMaxGroupTerms = 16;
-constexpr uint32_t kPauliTileQubits = 12;
-constexpr uint32_t kPauliMaxSpan = 9;
+constexpr uint32_t kPauliTileQubits = 11;
+constexpr uint32_t kPauliMinTileQubits = 10;  // smaller states: one streaming pass per term
+constexpr uint32_t kPauliMaxSpan = 8;
 struct PauliGroupTerm {
     uint64_t x, z;
     uint32_t kx;   // coordinates of x >> c in the group's basis
@@ -286,6 +287,9 @@ PauliPlan plan_pauli_groups(const uint64_t* x, const uint64_t* z, uint32_t num_t
 int launch_pauli_group(const void* amps, uint32_t n, uint32_t c, uint32_t d, const uint64_t* dev_span,
                        uint64_t free_mask, const void* dev_terms, uint32_t nterms, double* dev_partials,
                        uint32_t grid, void* stream, int precision);
+// One streaming pass per term (partials only), for terms that share no read.
+int launch_expectation_partials(const void* amps, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z,
+                                uint32_t num_terms, double* dev_partials, void* stream, int precision);
 int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const uint64_t* dev_x,
                               const uint64_t* dev_z, uint32_t num_terms, double* dev_out, void* stream);
 // MB2_OK after a clean launch, else MB2_ERR_CUDA with the error kept for

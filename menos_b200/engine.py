@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+from collections.abc import Mapping
 from typing import Optional, Sequence
 
 import numpy as np
@@ -16,6 +17,45 @@ import numpy as np
 from . import _lib
 from ._lib import C128, C64, SweepOptions, SweepStats, check, lib
 from .circuit import Circuit, to_mb2_ops
+
+
+class Counts(Mapping):
+    """Measurement counts as the engine returns them: outcome -> shots, in
+    ascending outcome order, held as two numpy arrays (a million distinct
+    outcomes cost no Python objects until they are read).  Compares equal
+    to a dict with the same items."""
+
+    def __init__(self, outcomes: np.ndarray, counts: np.ndarray):
+        self.outcomes = outcomes
+        self.counts = counts
+
+    def __len__(self) -> int:
+        return int(self.outcomes.size)
+
+    def __iter__(self):
+        return iter(self.outcomes.tolist())
+
+    def __getitem__(self, key) -> int:
+        i = int(np.searchsorted(self.outcomes, np.uint64(key)))
+        if i < self.outcomes.size and int(self.outcomes[i]) == int(key):
+            return int(self.counts[i])
+        raise KeyError(key)
+
+    def items(self):
+        return zip(self.outcomes.tolist(), self.counts.tolist())
+
+    def to_dict(self) -> dict:
+        return dict(self.items())
+
+    def __eq__(self, other):
+        if isinstance(other, Counts):
+            return np.array_equal(self.outcomes, other.outcomes) and np.array_equal(self.counts, other.counts)
+        if isinstance(other, Mapping):
+            return self.to_dict() == dict(other.items())
+        return NotImplemented
+
+    def __repr__(self) -> str:
+        return f"Counts({len(self)} outcomes, {int(self.counts.sum())} shots)"
 
 
 class Context:
@@ -130,7 +170,7 @@ class DeviceState:
         self._chk(lib().mb2_norm(self.h, C.byref(v)), "mb2_norm")
         return v.value
 
-    def sample(self, shots: int, seed: int, targets) -> dict:
+    def sample(self, shots: int, seed: int, targets) -> "Counts":
         t = np.ascontiguousarray(np.asarray(targets, np.uint32).ravel())
         cap = max(int(shots), 1)
         outc = np.zeros(cap, np.uint64)
@@ -139,7 +179,7 @@ class DeviceState:
         self._chk(lib().mb2_sample(self.h, shots, seed, t.ctypes.data if len(t) else None, len(t) // 2,
                                    outc.ctypes.data, cnt.ctypes.data, C.byref(nout)), "mb2_sample")
         d = nout.value
-        return dict(zip(outc[:d].tolist(), cnt[:d].tolist()))
+        return Counts(outc[:d].copy(), cnt[:d].copy())
 
     def copy_out(self) -> np.ndarray:
         dt = np.complex128 if self.precision == C128 else np.complex64
