@@ -18,6 +18,7 @@
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "mb2_internal.h"
@@ -537,21 +538,34 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
     }
     // Uniforms exactly as common::Rng (src/common/rng.cpp:176-186), sorted
     // (src/engines/dense/sample.cpp:37-42).  u = k * 2^-53 with k the top 53
-    // bits of a word, so sorting the integers k sorts the uniforms; an LSD
-    // radix sort (five 11-bit digits) does it in linear time.
+    // bits of a word, so sorting the integers k sorts the uniforms: one
+    // counting pass on the top 12 bits, then the buckets (about shots / 4096
+    // keys each, uniform) sorted independently on a few host threads.
     std::vector<double> u(shots);
     {
-        std::vector<uint64_t> key(shots), tmp(shots);
+        std::vector<uint64_t> key(shots), sorted(shots);
         std::mt19937_64 eng(seed);
         for (uint64_t i = 0; i < shots; ++i) key[i] = eng() >> 11;
-        for (uint32_t shift = 0; shift < 55; shift += 11) {
-            std::vector<uint64_t> bucket(2049, 0);
-            for (uint64_t i = 0; i < shots; ++i) ++bucket[((key[i] >> shift) & 2047u) + 1];
-            for (uint32_t b = 0; b < 2048; ++b) bucket[b + 1] += bucket[b];
-            for (uint64_t i = 0; i < shots; ++i) tmp[bucket[(key[i] >> shift) & 2047u]++] = key[i];
-            key.swap(tmp);
+        constexpr uint32_t kBits = 12, kBuckets = 1u << kBits;
+        std::vector<uint64_t> start(kBuckets + 1, 0);
+        for (uint64_t i = 0; i < shots; ++i) ++start[(key[i] >> (53 - kBits)) + 1];
+        for (uint32_t b = 0; b < kBuckets; ++b) start[b + 1] += start[b];
+        {
+            std::vector<uint64_t> pos(start.begin(), start.end() - 1);
+            for (uint64_t i = 0; i < shots; ++i) sorted[pos[key[i] >> (53 - kBits)]++] = key[i];
         }
-        for (uint64_t i = 0; i < shots; ++i) u[i] = static_cast<double>(key[i]) * (1.0 / 9007199254740992.0);
+        const uint32_t nthreads = shots < (1u << 16) ? 1u : std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+        auto sort_range = [&](uint32_t w) {
+            for (uint32_t b = w; b < kBuckets; b += nthreads) {
+                std::sort(sorted.begin() + static_cast<long>(start[b]), sorted.begin() + static_cast<long>(start[b + 1]));
+                for (uint64_t i = start[b]; i < start[b + 1]; ++i)
+                    u[i] = static_cast<double>(sorted[i]) * (1.0 / 9007199254740992.0);
+            }
+        };
+        std::vector<std::thread> pool;
+        for (uint32_t w = 1; w < nthreads; ++w) pool.emplace_back(sort_range, w);
+        sort_range(0);
+        for (auto& th : pool) th.join();
     }
     // The walk (sample.cpp:55-69), reproduced exactly on the device.
     const size_t al_u = (shots * 8 + 255) & ~size_t{255};
@@ -571,14 +585,35 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
     // gives non-decreasing basis indices (sorted uniforms against the
     // cumulative sum), so runs are counted first; the distinct outcomes are
     // sorted only when the target map does not keep their order.
+    // Outcome of a basis index: one table per byte of the index (the OR of
+    // the target bits that byte carries), or the index itself when every
+    // qubit is read into the clbit of its own number.
+    bool identity = num_targets == s->n;
+    std::vector<uint64_t> table(8 * 256, 0);
+    for (uint32_t t = 0; t < num_targets; ++t) {
+        const uint32_t q = targets[2 * t], c = targets[2 * t + 1];
+        if (q != c) identity = false;
+        for (uint32_t v = 0; v < 256; ++v)
+            if ((v >> (q & 7u)) & 1u) table[(q >> 3) * 256 + v] |= uint64_t{1} << c;
+    }
+    if (identity) {
+        uint64_t seen = 0;
+        for (uint32_t t = 0; t < num_targets; ++t) seen |= uint64_t{1} << targets[2 * t];
+        identity = seen == ((s->n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << s->n) - 1));
+    }
+    const uint32_t nbytes = (s->n + 7) / 8;
+    auto outcome_of = [&](uint64_t b) {
+        if (identity) return b;
+        uint64_t o = 0;
+        for (uint32_t k = 0; k < nbytes; ++k) o |= table[k * 256 + ((b >> (8 * k)) & 255u)];
+        return o;
+    };
     std::vector<std::pair<uint64_t, uint64_t>> oc;
+    oc.reserve(std::min<uint64_t>(shots, uint64_t{1} << std::min<uint32_t>(s->n, 30)));
     for (uint64_t i = 0; i < shots;) {
         uint64_t j = i + 1;
         while (j < shots && basis[j] == basis[i]) ++j;
-        uint64_t o = 0;
-        for (uint32_t t = 0; t < num_targets; ++t)
-            if ((basis[i] >> targets[2 * t]) & 1u) o |= uint64_t{1} << targets[2 * t + 1];
-        oc.emplace_back(o, j - i);
+        oc.emplace_back(outcome_of(basis[i]), j - i);
         i = j;
     }
     bool ordered = true;
