@@ -9,6 +9,15 @@ L2 flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+Other workloads (one JSON line each, not the headline):
+    --mode serve   the serving stream: Poisson arrivals of mixed requests (12-28
+                   qubits, depth 4-40, shots or <H>), the continuous-batching
+                   server against the sequential plain loop
+    --mode batch   the batched parameter sweep: 16-qubit RY/RZ + CX ansatz, 8
+                   layers, 4096 bindings, <H> over 32 weighted Pauli strings
+    --mode c64     the complex64 path: 32-qubit brick depth 32, error against the
+                   complex128 path at 28 qubits
+
 Multi-GPU: replicas only (the statevector is not sharded); each rank runs
 its own job and `value` counts the jobs of all ranks over the slowest rank's
 time.  Prints one JSON line on rank 0.
@@ -52,6 +61,10 @@ def parse():
     p.add_argument("--terms", type=int, default=64)
     p.add_argument("--tile", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--mode", default="job", choices=["job", "serve", "batch", "c64"])
+    p.add_argument("--requests", type=int, default=600)
+    p.add_argument("--load", type=float, default=4.0, help="serve: arrival rate / plain-loop capacity")
+    p.add_argument("--bindings", type=int, default=4096)
     return p.parse_args()
 
 
@@ -184,6 +197,10 @@ def main():
     rank, world, local = rank_info()
     if args.impl == "reference":
         return main_reference(args, rank, world)
+    if args.mode != "job":
+        if rank == 0:
+            {"serve": main_serve, "batch": main_batch, "c64": main_c64}[args.mode](args, local)
+        return
     dist = dist_setup(world)
     import numpy as np
     import torch
@@ -307,6 +324,225 @@ def main():
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def percentile(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+def main_serve(args, local):
+    """The serving stream against the sequential plain loop, same requests."""
+    import numpy as np
+    from menos_b200 import Context, DeviceState, workloads
+    from menos_b200.serve import Server
+    ctx = Context(local)
+    reqs = workloads.serving_stream(args.requests, 1.0, 20261201)
+
+    def run_plain(r):
+        st = DeviceState(ctx, r["circuit"].num_qubits)
+        st.init(r["circuit"].global_phase)
+        st.apply_program(r["circuit"])
+        if r["output"] == "counts":
+            out = st.sample(r["shots"], r["seed"], [(q, q) for q in range(r["circuit"].num_qubits)])
+        else:
+            vals = st.expectation(r["paulis"])
+            out = float(sum(c * v.real for c, v in zip(r["coefs"], vals)))
+        st.free()
+        return out
+
+    for r in reqs[:8]:  # warm-up (planner, allocator, module load)
+        run_plain(r)
+    # Sequential plain loop: service times, then FIFO latencies for any arrival process.
+    service, plain_out = [], []
+    t_all = time.perf_counter()
+    for r in reqs:
+        t0 = time.perf_counter()
+        plain_out.append(run_plain(r))
+        service.append(time.perf_counter() - t0)
+    plain_total = time.perf_counter() - t_all
+    plain_rate = len(reqs) / plain_total
+    rate = args.load * plain_rate
+    arrivals = [r["arrival_s"] / rate for r in reqs]  # the stream was drawn at rate 1
+
+    def fifo_latencies():
+        lat, free_at = [], 0.0
+        for a, s in zip(arrivals, service):
+            start = max(a, free_at)
+            free_at = start + s
+            lat.append(free_at - a)
+        return lat, free_at
+    plain_lat, plain_end = fifo_latencies()
+
+    def serve(arrive):
+        srv = Server(ctx, budget_bytes=160 * 10**9)
+        done, results = {}, {}
+        tickets = {}
+        t0 = time.perf_counter()
+        i = 0
+        while len(done) < len(reqs):
+            now = time.perf_counter() - t0
+            while i < len(reqs) and (not arrive or arrive[i] <= now):
+                r = reqs[i]
+                nq = r["circuit"].num_qubits
+                if r["output"] == "counts":
+                    tk = srv.submit(r["circuit"], "counts", shots=r["shots"], seed=r["seed"],
+                                    targets=[(q, q) for q in range(nq)])
+                else:
+                    tk = srv.submit(r["circuit"], "expectation", paulis=r["paulis"], coefs=r["coefs"])
+                tickets[tk] = i
+                i += 1
+            for c in srv.poll(timeout_ms=1):
+                k = tickets[c["ticket"]]
+                done[k] = c["latency_s"]
+                results[k] = c["counts"] if reqs[k]["output"] == "counts" else c["value"]
+        total = time.perf_counter() - t0
+        srv.close()
+        return done, results, total
+
+    burst_done, burst_res, burst_total = serve(None)
+    live_done, live_res, live_total = serve(arrivals)
+    # Each result the same alone (plain loop) and in the mix.
+    worst_exp, counts_same = 0.0, True
+    for k, r in enumerate(reqs):
+        for res in (burst_res, live_res):
+            if r["output"] == "counts":
+                counts_same = counts_same and (res[k] == plain_out[k])
+            else:
+                worst_exp = max(worst_exp, abs(res[k] - plain_out[k]))
+    live_lat = [live_done[k] for k in range(len(reqs))]
+    line = {
+        "metric": "served circuits/s (continuous batching) vs sequential plain loop", "unit": "circuits/s",
+        "mode": "serve", "requests": len(reqs), "higher_is_better": True,
+        "value": round(len(reqs) / burst_total, 2),
+        "plain_loop": {"circuits_per_s": round(plain_rate, 2), "total_s": round(plain_total, 3)},
+        "speedup_vs_plain": round(plain_total / burst_total, 2),
+        "live": {"arrival_rate_per_s": round(rate, 2), "load_vs_plain_capacity": args.load,
+                 "circuits_per_s": round(len(reqs) / live_total, 2),
+                 "p50_ms": round(1e3 * percentile(live_lat, 50), 2), "p99_ms": round(1e3 * percentile(live_lat, 99), 2),
+                 "plain_fifo_p50_ms": round(1e3 * percentile(plain_lat, 50), 2),
+                 "plain_fifo_p99_ms": round(1e3 * percentile(plain_lat, 99), 2)},
+        "same_alone_and_in_mix": {"counts_identical": counts_same, "max_abs_dH": worst_exp},
+        "config": {"workload": "serving stream: qubits 12-28, depth 4-40 (U3/CZ brick or RY/RZ+CX), "
+                               "4096 shots or <H> over 32 weighted Paulis, complex128, budget 160 GB",
+                   "seed": 20261201},
+        "data": "synthetic (seeded requests)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main_batch(args, local):
+    """The batched parameter sweep against one plain run per binding."""
+    import numpy as np
+    import torch
+    from menos_b200 import Context, DeviceState, workloads
+    from menos_b200.engine import sweep_batch
+    ctx = Context(local)
+    n, layers, B = 16, 8, args.bindings
+    circ = workloads.hea(n, layers, 11)
+    params = np.asarray(workloads.hea_bindings(n, layers, B, 12))
+    paulis = workloads.pauli_strings(n, 32, 13)
+    coefs = workloads.weights(32, 14)
+    sweep_batch(ctx, circ, params[:64], paulis, coefs)  # warm-up
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        vals, _, stats = sweep_batch(ctx, circ, params, paulis, coefs)
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+
+    def bound(row):
+        c = workloads.hea(n, layers, 11)
+        k, ops = 0, []
+        for oc, qs, ps, m, cl in c.ops:
+            if ps:
+                ps = tuple(float(v) for v in row[k:k + len(ps)])
+                k += len(ps)
+            ops.append((oc, qs, ps, m, cl))
+        c.ops = ops
+        return c
+    sample = min(64, B)
+    st = DeviceState(ctx, n)
+    t0 = time.perf_counter()
+    worst = 0.0
+    for b in range(sample):
+        st.init(0.0)
+        st.apply_program(bound(params[b]), fuse_gates=False)
+        v = st.expectation(paulis)
+        h = float(sum(c * x.real for c, x in zip(coefs, v)))
+        worst = max(worst, abs(h - vals[b]))
+    plain_per = (time.perf_counter() - t0) / sample
+    line = {
+        "metric": "bindings/s, batched parameter sweep (16q RY/RZ+CX x8, <H> over 32 Paulis)", "unit": "bindings/s",
+        "mode": "batch", "value": round(B / t, 1), "higher_is_better": True, "bindings": B, "s_per_sweep": round(t, 4),
+        "plain_loop": {"bindings_per_s": round(1.0 / plain_per, 1), "sampled_bindings": sample},
+        "speedup_vs_plain": round((B / t) * plain_per, 2),
+        "max_abs_dH_vs_plain": worst, "passes": int(stats.passes), "dtype": "c128 (f64)",
+        "config": {"workload": f"hea({n}, {layers}) x {B} bindings, 32 weighted Paulis", "seed": 11},
+        "data": "synthetic (seeded angles)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main_c64(args, local):
+    """The complex64 path: 32-qubit throughput, error against complex128 at 28 qubits."""
+    import numpy as np
+    import torch
+    from menos_b200 import Context, DeviceState, workloads
+    from menos_b200._lib import C64
+    ctx = Context(local)
+    paulis = workloads.pauli_strings(28, 64, 21)
+    circ28 = workloads.brick(28, 32, 20260929)
+    ref = DeviceState(ctx, 28)
+    ref.init(0.0)
+    ref.apply_program(circ28)
+    ref_amps = ref.copy_out()
+    ref_exp = ref.expectation(paulis)
+    ref.free()
+    lo = DeviceState(ctx, 28, precision=C64)
+    lo.init(0.0)
+    lo.apply_program(circ28)
+    lo.normalize()
+    lo_amps = lo.copy_out()
+    lo_exp = lo.expectation(paulis)
+    lo.free()
+    d_amp = float(np.max(np.abs(lo_amps.astype(np.complex128) - ref_amps)))
+    d_exp = float(np.max(np.abs(lo_exp - ref_exp)))
+    del ref_amps, lo_amps
+    n = args.qubits if args.qubits != 30 else 32
+    circ = workloads.brick(n, 32, 20260929)
+    st = DeviceState(ctx, n, precision=C64)
+    stream = torch.cuda.ExternalStream(st.stream_handle())
+    st.init(0.0)
+    st.apply_program(circ)
+    st.synchronize()
+    ts = []
+    for _ in range(max(1, args.steps)):
+        st.init(0.0)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        stats = st.apply_program(circ)
+        st.normalize()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    ms = statistics.median(ts)
+    per_pass = ms / max(1, int(stats.passes))
+    line = {
+        "metric": f"circuits/s, {n}q complex64 brick depth 32 (sweep + renormalisation)", "unit": "circuits/s",
+        "mode": "c64", "value": round(1000.0 / ms, 4), "ms_per_circuit": round(ms, 2), "higher_is_better": True,
+        "passes": int(stats.passes), "hbm_gbs_per_pass": round(2 * (8 << n) / (per_pass * 1e-3) / 1e9, 1),
+        "error_28q_vs_complex128": {"max_abs_amp": d_amp, "max_abs_pauli": d_exp, "paulis": 64},
+        "dtype": "c64 (f32 amplitudes, f64 reductions)",
+        "config": {"workload": f"brick({n}, 32), state {8 << n >> 30} GiB", "seed": 20260929},
+        "data": "synthetic (seeded circuit)",
+    }
+    print(json.dumps(line), flush=True)
 
 
 def main_reference(args, rank, world):
