@@ -224,7 +224,7 @@ int mb2_synchronize(mb2_state* state);
  * (src/api/batch.cpp:10-27) for a parameter sweep; no direct counterpart. */
 #define MB2_BATCH_MAX_TERMS 64
 typedef struct mb2_batch_options {
-    int32_t precision;   /* MB2_C128 */
+    int32_t precision;   /* MB2_C128, or MB2_C64: complex64 states (FP32 gates, FP64 reductions; states_out promoted) */
     int32_t fuse_gates;  /* 1: the reference's containment fusion per binding; 0: gate by gate */
     int32_t tile_qubits; /* 0: default */
     int32_t reserved;
@@ -270,6 +270,8 @@ typedef struct mb2_request {
     const uint64_t* x_masks;
     const uint64_t* z_masks;
     const double* coefs;
+    int32_t precision;             /* MB2_C128 (0, bitwise the reference) or MB2_C64 (complex64 state) */
+    uint32_t reserved;
 } mb2_request;
 typedef struct mb2_completion {
     uint64_t ticket;

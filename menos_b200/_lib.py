@@ -52,7 +52,7 @@ class Request(C.Structure):
                 ("global_phase", C.c_double), ("fuse_gates", C.c_int32), ("output", C.c_int32),
                 ("shots", C.c_uint64), ("seed", C.c_uint64), ("targets", C.c_void_p), ("num_targets", C.c_uint32),
                 ("num_terms", C.c_uint32), ("x_masks", C.c_void_p), ("z_masks", C.c_void_p),
-                ("coefs", C.c_void_p)]
+                ("coefs", C.c_void_p), ("precision", C.c_int32), ("reserved", C.c_uint32)]
 
 
 class Completion(C.Structure):

@@ -20,10 +20,11 @@
 #include "mb2_internal.h"
 
 namespace mb2 {
-int launch_batch_init(void* amps, uint32_t n, uint64_t bindings, double re, double im, void* stream);
+int launch_batch_init(void* amps, uint32_t n, uint64_t bindings, double re, double im, void* stream,
+                      int precision);
 int launch_batch_expect(const void* amps, uint32_t n, uint64_t bindings, const uint64_t* dev_x,
                         const uint64_t* dev_z, const double* dev_coefs, uint32_t num_terms, double* dev_out,
-                        void* stream);
+                        void* stream, int precision);
 }  // namespace mb2
 
 namespace {
@@ -85,7 +86,8 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
         if ((x_masks[t] | z_masks[t]) & ~lim) return MB2_ERR_INVALID;
     mb2_batch_options o{MB2_C128, 0, 0, 0};
     if (opts != nullptr) o = *opts;
-    if (o.precision != MB2_C128) return MB2_ERR_UNSUPPORTED;
+    if (o.precision != MB2_C128 && o.precision != MB2_C64) return MB2_ERR_INVALID;
+    const bool c64 = o.precision == MB2_C64;
     const bool fuse = o.fuse_gates != 0;
 
     // ---- host: every binding's blocks (threads), the shared structure, flags.
@@ -136,9 +138,10 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
         }
         (void)dim;
     }
-    uint32_t m = o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 12;
+    const uint32_t mmax = c64 ? mb2::kMaxTileQubitsC64 : mb2::kMaxTileQubits;
+    uint32_t m = o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : (c64 ? mb2::kMaxTileQubitsC64 : 11u);
     for (const auto& b : shape) m = std::max(m, b.k);
-    m = std::min(std::max(m, mb2::kMinTileQubits), std::min(mb2::kMaxTileQubits, num_qubits));
+    m = std::min(std::max(m, mb2::kMinTileQubits), std::min(mmax, num_qubits));
     mb2::TileProgram prog;
     try {
         prog = mb2::plan_tile_program(shape, num_qubits, m, mb2::kDefaultFixedLow, &flags);
@@ -170,7 +173,7 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     int dev = 0;
     cudaGetDevice(&dev);
     if (cudaStreamCreateWithFlags(&r.stream, cudaStreamNonBlocking) != cudaSuccess) return MB2_ERR_CUDA;
-    const size_t state_bytes = (size_t{num_bindings} << num_qubits) * sizeof(mb2::Cd);
+    const size_t state_bytes = (size_t{num_bindings} << num_qubits) * (c64 ? 8 : sizeof(mb2::Cd));
     auto al = [](size_t v) { return (v + 255) & ~size_t{255}; };
     const size_t ib = prog.words.size() * sizeof(uint32_t), sb = prog.data.size() * 8,
                  gb = prog.gdata.size() * 8, pb = pdata.size() * 8, tb = size_t{num_terms} * 8;
@@ -194,7 +197,8 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     if (cudaMemcpyAsync(w, host.data(), host.size(), cudaMemcpyHostToDevice, r.stream) != cudaSuccess)
         return MB2_ERR_CUDA;
     const mb2::Cd ph = mb2::initial_phase(0.0);
-    if (mb2::launch_batch_init(r.state, num_qubits, num_bindings, ph.real(), ph.imag(), r.stream) != MB2_OK)
+    if (mb2::launch_batch_init(r.state, num_qubits, num_bindings, ph.real(), ph.imag(), r.stream, o.precision) !=
+        MB2_OK)
         return MB2_ERR_CUDA;
     int sm = 148;
     cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
@@ -203,25 +207,37 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     layout.pdata = reinterpret_cast<const double*>(w + o_p);
     layout.pstride = static_cast<uint32_t>(stride);
     for (const mb2::TilePass& pass : prog.passes) {
-        if (mb2::launch_tile_pass(r.state, num_qubits, pass, reinterpret_cast<const uint32_t*>(w),
-                                  reinterpret_cast<const double*>(w + o_s), reinterpret_cast<const double*>(w + o_g),
-                                  sm, r.stream, &layout) != MB2_OK)
-            return MB2_ERR_CUDA;
+        const auto* dw = reinterpret_cast<const uint32_t*>(w);
+        const auto* ds = reinterpret_cast<const double*>(w + o_s);
+        const auto* dg = reinterpret_cast<const double*>(w + o_g);
+        const int rc = c64 ? mb2::launch_tile_pass_c64(r.state, num_qubits, pass, dw, ds, dg, sm, r.stream, &layout)
+                           : mb2::launch_tile_pass(r.state, num_qubits, pass, dw, ds, dg, sm, r.stream, &layout);
+        if (rc != MB2_OK) return MB2_ERR_CUDA;
     }
     if (num_terms > 0) {
         if (mb2::launch_batch_expect(r.state, num_qubits, num_bindings, reinterpret_cast<const uint64_t*>(w + o_x),
                                      reinterpret_cast<const uint64_t*>(w + o_z), reinterpret_cast<const double*>(w + o_c),
-                                     num_terms, reinterpret_cast<double*>(w + o_o), r.stream) != MB2_OK)
+                                     num_terms, reinterpret_cast<double*>(w + o_o), r.stream, o.precision) != MB2_OK)
             return MB2_ERR_CUDA;
         if (cudaMemcpyAsync(out, w + o_o, size_t{num_bindings} * 8, cudaMemcpyDeviceToHost, r.stream) != cudaSuccess)
             return MB2_ERR_CUDA;
     } else {
         std::fill(out, out + num_bindings, 0.0);
     }
-    if (states_out != nullptr &&
-        cudaMemcpyAsync(states_out, r.state, state_bytes, cudaMemcpyDeviceToHost, r.stream) != cudaSuccess)
-        return MB2_ERR_CUDA;
+    // States out as complex128 (a complex64 batch's amplitudes promoted).
+    std::vector<float> lo;
+    if (states_out != nullptr) {
+        void* dst = states_out;
+        if (c64) {
+            lo.resize(state_bytes / sizeof(float));
+            dst = lo.data();
+        }
+        if (cudaMemcpyAsync(dst, r.state, state_bytes, cudaMemcpyDeviceToHost, r.stream) != cudaSuccess)
+            return MB2_ERR_CUDA;
+    }
     if (cudaStreamSynchronize(r.stream) != cudaSuccess) return MB2_ERR_CUDA;
+    if (states_out != nullptr && c64)
+        for (size_t i = 0; i < lo.size(); ++i) states_out[i] = static_cast<double>(lo[i]);
     if (stats != nullptr) {
         stats->passes = prog.passes.size();
         stats->blocks = nb;

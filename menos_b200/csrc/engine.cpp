@@ -148,15 +148,19 @@ int context_device(const mb2_context* ctx) { return ctx == nullptr ? 0 : ctx->de
 // A state whose work is queued on a stream the caller owns (the serving
 // loop's worker streams); freed with mb2_state_free, which leaves the
 // stream alone.
-int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, void* stream, mb2_state** out) {
+int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, void* stream, mb2_state** out,
+                    int precision) {
     if (ctx == nullptr || out == nullptr || stream == nullptr) return MB2_ERR_INVALID;
     *out = nullptr;
     if (num_qubits < 1 || num_qubits > 40) return fail(ctx, MB2_ERR_INVALID, "num_qubits must be 1..40");
-    const uint64_t bytes = (uint64_t{1} << num_qubits) * 16;
+    if (precision == MB2_C64 && num_qubits < mb2::kMinTileQubits)
+        return fail(ctx, MB2_ERR_UNSUPPORTED, "complex64 states need >= 4 qubits");
+    const uint64_t bytes = (uint64_t{1} << num_qubits) * amp_bytes(precision);
     if (bytes > budget_bytes) return fail(ctx, MB2_ERR_RESOURCE, "state over budget");
     auto* s = new mb2_state;
     s->ctx = ctx;
     s->n = num_qubits;
+    s->precision = precision;
     s->stream = static_cast<cudaStream_t>(stream);
     s->owns_stream = false;
     const cudaError_t e = cudaMallocAsync(&s->amps, bytes, s->stream);
@@ -365,28 +369,26 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     } catch (const std::exception& e) {
         return fail(s->ctx, MB2_ERR_INVALID, e.what());
     }
-    // One upload: the program (complex64: TileInstr records; complex128: the
-    // compact word stream), staged data, global-only data (256-byte aligned parts).
-    const size_t ibytes = c64 ? prog.instrs.size() * sizeof(mb2::TileInstr) : prog.words.size() * sizeof(uint32_t);
+    // One upload: the compact word stream, staged data, global-only data
+    // (256-byte aligned parts).
+    const size_t ibytes = prog.words.size() * sizeof(uint32_t);
     const size_t dbytes = prog.data.size() * sizeof(double);
     const size_t gbytes = prog.gdata.size() * sizeof(double);
     const size_t doff = (ibytes + 255) & ~size_t{255};
     const size_t goff = (doff + dbytes + 255) & ~size_t{255};
     if (int e = ensure_scratch(s, goff + gbytes + 256); e != MB2_OK) return e;
     std::vector<unsigned char> host(goff + gbytes);
-    if (c64) std::memcpy(host.data(), prog.instrs.data(), ibytes);
-    else std::memcpy(host.data(), prog.words.data(), ibytes);
+    std::memcpy(host.data(), prog.words.data(), ibytes);
     if (dbytes) std::memcpy(host.data() + doff, prog.data.data(), dbytes);
     if (gbytes) std::memcpy(host.data() + goff, prog.gdata.data(), gbytes);
     MB2_CUDA(s->ctx, cudaMemcpyAsync(s->scratch, host.data(), host.size(), cudaMemcpyHostToDevice, s->stream));
-    const auto* dev_instrs = static_cast<const mb2::TileInstr*>(s->scratch);
     const auto* dev_words = static_cast<const uint32_t*>(s->scratch);
     const auto* dev_sdata = reinterpret_cast<const double*>(static_cast<unsigned char*>(s->scratch) + doff);
     const auto* dev_gdata = reinterpret_cast<const double*>(static_cast<unsigned char*>(s->scratch) + goff);
     s->stats.fp64_ops_per_amp = prog.fp64_per_amp;
     uint64_t done = 0;
     for (const mb2::TilePass& pass : prog.passes) {
-        const int rc = c64 ? mb2::launch_tile_pass_c64(s->amps, s->n, pass, dev_instrs, dev_sdata, dev_gdata,
+        const int rc = c64 ? mb2::launch_tile_pass_c64(s->amps, s->n, pass, dev_words, dev_sdata, dev_gdata,
                                                        s->ctx->sm_count, s->stream)
                            : mb2::launch_tile_pass(s->amps, s->n, pass, dev_words, dev_sdata, dev_gdata,
                                                    s->ctx->sm_count, s->stream);

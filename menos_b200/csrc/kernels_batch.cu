@@ -24,11 +24,23 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kCluster = 8;
 
-__global__ void k_batch_init(double2* st, uint64_t total, uint32_t n, double re, double im) {
+template <typename A>
+__device__ __forceinline__ A make_amp(double re, double im);
+template <>
+__device__ __forceinline__ double2 make_amp<double2>(double re, double im) { return make_double2(re, im); }
+template <>
+__device__ __forceinline__ float2 make_amp<float2>(double re, double im) {
+    return make_float2(static_cast<float>(re), static_cast<float>(im));
+}
+__device__ __forceinline__ double2 as_d2(double2 a) { return a; }
+__device__ __forceinline__ double2 as_d2(float2 a) { return make_double2(a.x, a.y); }
+
+template <typename A>
+__global__ void k_batch_init(A* st, uint64_t total, uint32_t n, double re, double im) {
     const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
     const uint64_t mask = (uint64_t{1} << n) - 1;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += stride)
-        st[i] = (i & mask) == 0 ? make_double2(re, im) : make_double2(0.0, 0.0);
+        st[i] = (i & mask) == 0 ? make_amp<A>(re, im) : make_amp<A>(0.0, 0.0);
 }
 
 __device__ __forceinline__ void block_sum2(double& re, double& im, double* sh) {
@@ -53,8 +65,9 @@ __device__ __forceinline__ void block_sum2(double& re, double& im, double* sh) {
     }
 }
 
+template <typename A>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
-    k_batch_expect(const double2* __restrict__ st, uint32_t n, const uint64_t* __restrict__ xs,
+    k_batch_expect(const A* __restrict__ st, uint32_t n, const uint64_t* __restrict__ xs,
                    const uint64_t* __restrict__ zs, const double* __restrict__ coefs, uint32_t num_terms,
                    double* __restrict__ out) {
     extern __shared__ double2 slice[];
@@ -65,8 +78,8 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
     const uint64_t b = blockIdx.x / kCluster;
     const uint32_t sl = n - 3;
     const uint32_t S = 1u << sl;
-    const double2* src = st + (b << n) + (static_cast<uint64_t>(rank) << sl);
-    for (uint32_t i = threadIdx.x; i < S; i += kThreads) slice[i] = src[i];
+    const A* src = st + (b << n) + (static_cast<uint64_t>(rank) << sl);
+    for (uint32_t i = threadIdx.x; i < S; i += kThreads) slice[i] = as_d2(src[i]);
     cluster.sync();
     for (uint32_t t = 0; t < num_terms; ++t) {
         const uint64_t x = xs[t], z = zs[t];
@@ -126,28 +139,41 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kThreads)
 
 }  // namespace
 
-int launch_batch_init(void* amps, uint32_t n, uint64_t bindings, double re, double im, void* stream) {
+int launch_batch_init(void* amps, uint32_t n, uint64_t bindings, double re, double im, void* stream,
+                      int precision) {
     const uint64_t total = bindings << n;
     const uint64_t blocks = (total + 255) / 256;
-    k_batch_init<<<static_cast<unsigned>(blocks < 148ull * 16 ? blocks : 148ull * 16), 256, 0,
-                   static_cast<cudaStream_t>(stream)>>>(static_cast<double2*>(amps), total, n, re, im);
+    const unsigned grid = static_cast<unsigned>(blocks < 148ull * 16 ? blocks : 148ull * 16);
+    if (precision == MB2_C64)
+        k_batch_init<float2><<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<float2*>(amps), total, n,
+                                                                                 re, im);
+    else
+        k_batch_init<double2><<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<double2*>(amps), total,
+                                                                                  n, re, im);
     note_launches(1);
     return launch_status();
 }
 
 int launch_batch_expect(const void* amps, uint32_t n, uint64_t bindings, const uint64_t* dev_x,
                         const uint64_t* dev_z, const double* dev_coefs, uint32_t num_terms, double* dev_out,
-                        void* stream) {
+                        void* stream, int precision) {
     if (n < 3 || n > 16 || num_terms > kMaxBatchTerms) return MB2_ERR_INVALID;
     const size_t smem = (size_t{1} << (n - 3)) * sizeof(double2);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_batch_expect, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>((size_t{1} << 13) * sizeof(double2)));
+        const int most = static_cast<int>((size_t{1} << 13) * sizeof(double2));
+        cudaFuncSetAttribute(k_batch_expect<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        cudaFuncSetAttribute(k_batch_expect<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         attr = true;
     }
-    k_batch_expect<<<static_cast<unsigned>(bindings * kCluster), kThreads, smem, static_cast<cudaStream_t>(stream)>>>(
-        static_cast<const double2*>(amps), n, dev_x, dev_z, dev_coefs, num_terms, dev_out);
+    const unsigned grid = static_cast<unsigned>(bindings * kCluster);
+    const auto s = static_cast<cudaStream_t>(stream);
+    if (precision == MB2_C64)
+        k_batch_expect<float2><<<grid, kThreads, smem, s>>>(static_cast<const float2*>(amps), n, dev_x, dev_z,
+                                                            dev_coefs, num_terms, dev_out);
+    else
+        k_batch_expect<double2><<<grid, kThreads, smem, s>>>(static_cast<const double2*>(amps), n, dev_x, dev_z,
+                                                             dev_coefs, num_terms, dev_out);
     note_launches(1);
     return launch_status();
 }

@@ -1,6 +1,6 @@
 // The complex64 precision path's tile pass: the same tiled multi-gate sweep
-// as the complex128 kernel (same planner, same instruction stream) on a
-// state of (float, float) amplitudes, with FP32 fused multiply-adds.
+// as the complex128 kernel (same planner, same compact instruction stream)
+// on a state of (float, float) amplitudes, with FP32 fused multiply-adds.
 //
 // Gate matrices are composed in FP64 on the host and rounded to FP32 once
 // per gate; every amplitude update is an FMA chain (one rounding per term
@@ -12,55 +12,21 @@
 
 #include <cstdint>
 
+#include "device_math.cuh"
 #include "mb2_internal.h"
 
 namespace mb2 {
 namespace {
+using dev::pdep64;
 
 constexpr int kR = static_cast<int>(kRegQubits);
 constexpr int kNA = 1 << kR;
 static_assert(kR == 4, "written for 4 register qubits");
 
-__host__ __device__ constexpr int lowbit_index(int j) { return (j & 1) ? 0 : (j & 2) ? 1 : (j & 4) ? 2 : 3; }
-
 // 8-byte slots: the low four bits XOR-folded with every higher 4-bit group
 // (XOR-linear, so slot addresses compose by XOR).
-__device__ __forceinline__ uint32_t swz8(uint32_t l) {
-    const uint32_t h = l >> 4;
-    return l ^ ((h ^ (h >> 4) ^ (h >> 8)) & 15u);
-}
-
-struct DI {
-    uint64_t w0, w1, w2, w3;
-    __device__ __forceinline__ uint32_t op() const { return static_cast<uint32_t>(w0 & 0xffu); }
-    __device__ __forceinline__ uint32_t k() const { return static_cast<uint32_t>((w0 >> 8) & 0xffu); }
-    __device__ __forceinline__ uint32_t kind() const { return static_cast<uint32_t>((w0 >> 16) & 0xffu); }
-    __device__ __forceinline__ uint32_t nthread() const { return static_cast<uint32_t>((w0 >> 24) & 0xffu); }
-    __device__ __forceinline__ uint32_t pos(uint32_t b) const {
-        return static_cast<uint32_t>((b < 4 ? (w0 >> (32 + 8 * b)) : (w1 >> (8 * (b - 4)))) & 0xffu);
-    }
-    __device__ __forceinline__ uint32_t data() const { return static_cast<uint32_t>(w1 >> 32); }
-    __device__ __forceinline__ uint32_t tperm(uint32_t i) const {
-        return static_cast<uint32_t>((i < 8 ? (w2 >> (8 * i)) : (w3 >> (8 * (i - 8)))) & 0xffu);
-    }
-    __device__ __forceinline__ uint32_t aux() const { return static_cast<uint32_t>(w3 >> 32); }
-};
-
-__device__ __forceinline__ DI load_instr(const TileInstr* p) {
-    const ulonglong2* s = reinterpret_cast<const ulonglong2*>(p);
-    const ulonglong2 a = s[0], b = s[1];
-    return DI{a.x, a.y, b.x, b.y};
-}
-
-__device__ __forceinline__ uint64_t pdep64(uint64_t v, uint64_t mask) {
-    uint64_t r = 0;
-    while (mask != 0) {
-        const uint64_t low = mask & (~mask + 1);
-        if (v & 1) r |= low;
-        v >>= 1;
-        mask ^= low;
-    }
-    return r;
+__host__ __device__ __forceinline__ constexpr uint32_t swz8(uint32_t l) {
+    return l ^ (((l >> 4) ^ (l >> 8) ^ (l >> 12)) & 15u);
 }
 
 struct Cf {
@@ -75,6 +41,10 @@ __device__ __forceinline__ float2 cfma(Cf m, float2 x, float2 acc) {
     return make_float2(fmaf(m.r, x.x, fmaf(-m.i, x.y, acc.x)), fmaf(m.r, x.y, fmaf(m.i, x.x, acc.y)));
 }
 __device__ __forceinline__ float2 cmulf(Cf m, float2 x) { return cfma(m, x, make_float2(0.f, 0.f)); }
+__device__ __forceinline__ float2 fneg_if(float2 v, uint32_t flip) {
+    const uint32_t msk = flip << 31;
+    return make_float2(__uint_as_float(__float_as_uint(v.x) ^ msk), __uint_as_float(__float_as_uint(v.y) ^ msk));
+}
 
 template <int P>
 __device__ __forceinline__ void g1(float2 (&a)[kNA], const double* md) {
@@ -142,22 +112,28 @@ __device__ __forceinline__ void perm2(float2 (&a)[kNA]) {
     }
 }
 
-#define MB2_PAIR_SWITCH(p0, p1, CALL)                 \
-    switch ((p0) * 4 + (p1)) {                        \
-        case 1: CALL(0, 1); break;                    \
-        case 2: CALL(0, 2); break;                    \
-        case 3: CALL(0, 3); break;                    \
-        case 4: CALL(1, 0); break;                    \
-        case 6: CALL(1, 2); break;                    \
-        case 7: CALL(1, 3); break;                    \
-        case 8: CALL(2, 0); break;                    \
-        case 9: CALL(2, 1); break;                    \
-        case 11: CALL(2, 3); break;                   \
-        case 12: CALL(3, 0); break;                   \
-        case 13: CALL(3, 1); break;                   \
-        case 14: CALL(3, 2); break;                   \
-        default: break;                               \
+// A diagonal of k <= 2 operands: operand b is register slot P_b (P < 0: a
+// thread bit of value v_b).  Entry e multiplies the amplitudes whose operand
+// bits spell e; class 0 entries (exactly 1) are skipped.
+template <int P0, int P1>
+__device__ __forceinline__ void diag_regs(float2 (&a)[kNA], const double* md, uint32_t k, uint32_t cls, uint32_t v0,
+                                          uint32_t v1) {
+#pragma unroll
+    for (uint32_t e = 0; e < 4; ++e) {
+        if (e >= (1u << k)) break;
+        if (P0 < 0 && (e & 1u) != v0) continue;
+        if (P1 < 0 && k > 1 && ((e >> 1) & 1u) != v1) continue;
+        const uint32_t c = (cls >> (2 * e)) & 3u;
+        if (c == 0u) continue;
+        const Cf d = entry(md, e);
+#pragma unroll
+        for (int j = 0; j < kNA; ++j) {
+            if (P0 >= 0 && ((j >> (P0 < 0 ? 0 : P0)) & 1) != static_cast<int>(e & 1u)) continue;
+            if (P1 >= 0 && ((j >> (P1 < 0 ? 0 : P1)) & 1) != static_cast<int>((e >> 1) & 1u)) continue;
+            a[j] = c == 1u ? fneg_if(a[j], 1u) : cmulf(d, a[j]);
+        }
     }
+}
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
@@ -167,173 +143,270 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-__global__ void __launch_bounds__(512, 1)
-    k_tile_pass_c64(float2* __restrict__ st, uint32_t n, uint32_t m, uint64_t smask, const TileInstr* __restrict__ prog,
-                    uint32_t nprog, const double* __restrict__ sdata, uint32_t nsdata, const double* __restrict__ gdata,
-                    uint64_t ntiles, uint32_t stages) {
-    extern __shared__ float2 smem_tiles_f[];
+// One pass: the complex128 kernel's structure (persistent CTAs, tiles
+// `stages - 1` ahead in flight, masked-add tile bases, the pass's words and
+// data staged in shared memory, a batch's parametric slice per tile) with
+// FP32 gates.  MT > 0 fixes the tile width; IDX is the index type.
+template <int MAXT, int MINB, int MT, typename IDX>
+__global__ void __launch_bounds__(MAXT, MINB)
+    k_tile_pass_c64(float2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask,
+                    const uint32_t* __restrict__ words, uint32_t nwords, const double* __restrict__ sdata,
+                    uint32_t nsdata, const double* __restrict__ gdata, uint64_t ntiles,
+                    const double* __restrict__ pdata, uint32_t pstride, uint32_t param_lo, uint32_t param_len,
+                    uint32_t bshift, uint32_t stages) {
+    extern __shared__ float2 smem_f[];
+    const uint32_t m = MT > 0 ? static_cast<uint32_t>(MT) : m_rt;
     const uint32_t tid = threadIdx.x;
     const uint32_t tbits = m - kRegQubits;
     const uint32_t tile_amps = 1u << m;
-    TileInstr* sprog = reinterpret_cast<TileInstr*>(smem_tiles_f + stages * tile_amps);
-    double* sd = reinterpret_cast<double*>(sprog + nprog);
-    for (uint32_t i = tid; i < nprog * 2; i += blockDim.x)
-        reinterpret_cast<ulonglong2*>(sprog)[i] = __ldg(reinterpret_cast<const ulonglong2*>(prog) + i);
+    uint32_t* sw = reinterpret_cast<uint32_t*>(smem_f + stages * tile_amps);
+    double* sd = reinterpret_cast<double*>(sw + nwords);
+    for (uint32_t i = tid; i < nwords / 4; i += blockDim.x)
+        reinterpret_cast<uint4*>(sw)[i] = __ldg(reinterpret_cast<const uint4*>(words) + i);
     for (uint32_t i = tid; i < nsdata; i += blockDim.x) sd[i] = __ldg(sdata + i);
-    uint64_t off_lo = 0, hib[kR] = {0, 0, 0, 0};
+    IDX off_lo = 0, hib0 = 0, hib1 = 0, hib2 = 0, hib3 = 0;
     {
         uint32_t b = 0;
         for (uint32_t p = 0; p < n; ++p) {
             if (!((smask >> p) & 1u)) continue;
             if (b < tbits) {
-                off_lo |= static_cast<uint64_t>((tid >> b) & 1u) << p;
+                off_lo |= static_cast<IDX>((tid >> b) & 1u) << p;
             } else {
-#pragma unroll
-                for (int r = 0; r < kR; ++r)
-                    if (static_cast<uint32_t>(r) == b - tbits) hib[r] = uint64_t{1} << p;
+                const IDX v = IDX{1} << p;
+                const uint32_t r = b - tbits;
+                if (r == 0) hib0 = v;
+                else if (r == 1) hib1 = v;
+                else if (r == 2) hib2 = v;
+                else hib3 = v;
             }
             ++b;
         }
     }
-    const uint64_t nmask = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~smask;
-    // Canonical slots: tid | j << tbits, by XOR-linearity from four constants.
-    uint32_t cadr[kNA];
-    cadr[0] = swz8(tid);
-#pragma unroll
-    for (int j = 1; j < kNA; ++j) cadr[j] = cadr[j & (j - 1)] ^ swz8(1u << (tbits + lowbit_index(j)));
-    auto reg_off = [&](int j) -> uint64_t {
-        return ((j & 1) ? hib[0] : 0) | ((j & 2) ? hib[1] : 0) | ((j & 4) ? hib[2] : 0) | ((j & 8) ? hib[3] : 0);
+    const uint64_t nmask64 = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~smask;
+    const IDX nmask = static_cast<IDX>(nmask64);
+    const IDX step = static_cast<IDX>(pdep64(gridDim.x, nmask64));
+    auto advance = [&](IDX b) -> IDX { return ((b | ~nmask) + step) & nmask; };
+    const uint32_t s_tid = swz8(tid);
+    auto reg_off = [&](int j) -> IDX {
+        return ((j & 1) ? hib0 : IDX{0}) + ((j & 2) ? hib1 : IDX{0}) + ((j & 4) ? hib2 : IDX{0}) +
+               ((j & 8) ? hib3 : IDX{0});
     };
-    auto prefetch = [&](uint64_t t, float2* buf) {
-        const uint64_t base = pdep64(t, nmask) | off_lo;
+    auto slot = [&](int j) -> uint32_t { return s_tid ^ swz8(static_cast<uint32_t>(j) << tbits); };
+    auto prefetch = [&](IDX base, float2* buf) {
+        const IDX b0 = base + off_lo;
 #pragma unroll
-        for (int j = 0; j < kNA; ++j) cp_async8(buf + cadr[j], st + (base | reg_off(j)));
+        for (int j = 0; j < kNA; ++j) cp_async8(buf + slot(j), st + (b0 + reg_off(j)));
         cp_async_commit();
     };
-
-    const uint64_t t0 = blockIdx.x;
+    uint64_t tp = blockIdx.x;
+    IDX pbase = static_cast<IDX>(pdep64(blockIdx.x, nmask64));
+    IDX cbase = pbase;
     for (uint32_t sg = 0; sg + 1 < stages; ++sg) {
-        const uint64_t tp = t0 + static_cast<uint64_t>(sg) * gridDim.x;
-        if (tp < ntiles) prefetch(tp, smem_tiles_f + sg * tile_amps);
+        if (tp < ntiles) prefetch(pbase, smem_f + sg * tile_amps);
         else cp_async_commit();
+        tp += gridDim.x;
+        pbase = advance(pbase);
     }
-    uint64_t t = t0;
-    for (uint32_t it = 0; t < ntiles; t += gridDim.x, ++it) {
-        float2* tile = smem_tiles_f + (it % stages) * tile_amps;
-        const uint64_t tn = t + static_cast<uint64_t>(stages - 1) * gridDim.x;
-        if (tn < ntiles) prefetch(tn, smem_tiles_f + ((it + stages - 1) % stages) * tile_amps);
+    uint32_t cur = 0, nxt = stages - 1;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        float2* tile = smem_f + cur * tile_amps;
+        if (tp < ntiles) prefetch(pbase, smem_f + nxt * tile_amps);
         else cp_async_commit();
+        tp += gridDim.x;
+        pbase = advance(pbase);
+        cur = cur + 1 == stages ? 0u : cur + 1;
+        nxt = nxt + 1 == stages ? 0u : nxt + 1;
+        if (param_len != 0) {  // a batched sweep: this tile's binding is t >> bshift
+            const double2* src = reinterpret_cast<const double2*>(pdata + (t >> bshift) * pstride + param_lo);
+            double2* dst = reinterpret_cast<double2*>(sd + nsdata);
+            for (uint32_t i = tid; i < param_len / 2; i += blockDim.x) dst[i] = __ldg(src + i);
+        }
         if (stages == 3) cp_async_wait<2>();
         else cp_async_wait<1>();
         __syncthreads();
 
         float2 a[kNA];
         uint32_t pc = 0;
-        while (pc < nprog) {
-            const DI I = load_instr(sprog + pc);
-            ++pc;
-            if (I.op() == TOP_PHASE) {
+        while (pc < nwords) {
+            const uint32_t w0 = sw[pc];
+            const uint32_t op0 = w0 & 0xffu;
+            if (op0 == cop::kPhase) {
+                const uint32_t tp0 = sw[pc + 1], tp1 = sw[pc + 2];
+                pc += 3;
+                const uint32_t nthread = (w0 >> 8) & 0xffu;
+                auto tperm = [&](uint32_t i) -> uint32_t {
+                    return (i < 8 ? (tp0 >> (4 * i)) : (tp1 >> (4 * (i - 8)))) & 15u;
+                };
                 uint32_t tb = 0;
-                for (uint32_t i = 0; i < I.nthread(); ++i) tb |= ((tid >> i) & 1u) << I.tperm(i);
+                if (MT > 0) {
+#pragma unroll
+                    for (uint32_t i = 0; i < (MT > 0 ? MT - kRegQubits : 1u); ++i)
+                        if (i < nthread) tb |= ((tid >> i) & 1u) << tperm(i);
+                } else {
+                    for (uint32_t i = 0; i < nthread; ++i) tb |= ((tid >> i) & 1u) << tperm(i);
+                }
                 uint32_t rb[kR];
 #pragma unroll
-                for (int b = 0; b < kR; ++b) rb[b] = 1u << I.pos(b);
-                uint32_t adr[kNA];
-                adr[0] = swz8(tb);
+                for (int b = 0; b < kR; ++b) rb[b] = 1u << ((w0 >> (16 + 4 * b)) & 15u);
+                const uint32_t z0 = swz8(tb), z1 = swz8(rb[0]), z2 = swz8(rb[1]), z3 = swz8(rb[2]), z4 = swz8(rb[3]);
+                auto adr = [&](int j) -> uint32_t {
+                    return z0 ^ ((j & 1) ? z1 : 0u) ^ ((j & 2) ? z2 : 0u) ^ ((j & 4) ? z3 : 0u) ^ ((j & 8) ? z4 : 0u);
+                };
 #pragma unroll
-                for (int j = 1; j < kNA; ++j) adr[j] = adr[j & (j - 1)] ^ swz8(rb[lowbit_index(j)]);
-#pragma unroll
-                for (int j = 0; j < kNA; ++j) a[j] = tile[adr[j]];
+                for (int j = 0; j < kNA; ++j) a[j] = tile[adr(j)];
                 for (;;) {
-                    const DI G = load_instr(sprog + pc);
-                    ++pc;
-                    if (G.op() == TOP_END) break;
-                    const double* md = sd + G.data();
-                    if (G.op() == TOP_G1) {
-                        if (G.kind() == TK_X) {
-                            switch (G.pos(0)) {
-                                case 0: perm1<0>(a); break;
-                                case 1: perm1<1>(a); break;
-                                case 2: perm1<2>(a); break;
-                                default: perm1<3>(a); break;
+                    const uint32_t w = sw[pc++];
+                    const uint32_t op = w & 0xffu;
+                    if (op == cop::kEnd) break;
+                    const uint32_t aux = (w >> 8) & 0xffu;
+                    const double* md = sd + ((w >> 20) << 1);
+                    const uint32_t tv = (tb >> ((w >> 16) & 15u)) & 1u;
+                    switch (op) {
+#define MB2_CASE4(BASE, STMT) \
+    case BASE + 0: { constexpr int P = 0; STMT; } break; \
+    case BASE + 1: { constexpr int P = 1; STMT; } break; \
+    case BASE + 2: { constexpr int P = 2; STMT; } break; \
+    case BASE + 3: { constexpr int P = 3; STMT; } break;
+#define MB2_CASE12(BASE, STMT) \
+    case BASE + 0: { constexpr int P0 = 0, P1 = 1; STMT; } break; \
+    case BASE + 1: { constexpr int P0 = 0, P1 = 2; STMT; } break; \
+    case BASE + 2: { constexpr int P0 = 0, P1 = 3; STMT; } break; \
+    case BASE + 3: { constexpr int P0 = 1, P1 = 0; STMT; } break; \
+    case BASE + 4: { constexpr int P0 = 1, P1 = 2; STMT; } break; \
+    case BASE + 5: { constexpr int P0 = 1, P1 = 3; STMT; } break; \
+    case BASE + 6: { constexpr int P0 = 2, P1 = 0; STMT; } break; \
+    case BASE + 7: { constexpr int P0 = 2, P1 = 1; STMT; } break; \
+    case BASE + 8: { constexpr int P0 = 2, P1 = 3; STMT; } break; \
+    case BASE + 9: { constexpr int P0 = 3, P1 = 0; STMT; } break; \
+    case BASE + 10: { constexpr int P0 = 3, P1 = 1; STMT; } break; \
+    case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
+                        // Every dense 1q kind is the general 2x2 in FP32.
+                        MB2_CASE4(cop::kU3, (g1<P>(a, md)))
+                        MB2_CASE4(cop::kGen1, (g1<P>(a, md)))
+                        MB2_CASE4(cop::kReal1, (g1<P>(a, md)))
+                        MB2_CASE4(cop::kMono1, (g1<P>(a, md)))
+                        MB2_CASE4(cop::kX1, (perm1<P>(a)))
+                        MB2_CASE12(cop::kGen2, (g2<P0, P1>(a, md)))
+                        MB2_CASE12(cop::kMono2, (++pc, g2<P0, P1>(a, md)))
+                        MB2_CASE12(cop::kSw12, (perm2<P0, P1, TK_SW12>(a)))
+                        MB2_CASE12(cop::kSw13, (perm2<P0, P1, TK_SW13>(a)))
+                        MB2_CASE12(cop::kSw23, (perm2<P0, P1, TK_SW23>(a)))
+                        MB2_CASE4(cop::kDs1R, (diag_regs<P, -1>(a, md, 1, aux, 0u, 0u)))
+                        MB2_CASE12(cop::kDs2RR, (diag_regs<P0, P1>(a, md, 2, aux, 0u, 0u)))
+#undef MB2_CASE4
+#undef MB2_CASE12
+                        case cop::kDs1T: diag_regs<-1, -1>(a, md, 1, aux, tv, 0u); break;
+                        // kDs2RT + 2s + w: register slot s and a thread bit as operand w
+                        // (w = 0: operand 0 is the thread bit, operand 1 the register).
+                        case cop::kDs2RT + 0: diag_regs<-1, 0>(a, md, 2, aux, tv, 0u); break;
+                        case cop::kDs2RT + 1: diag_regs<0, -1>(a, md, 2, aux, 0u, tv); break;
+                        case cop::kDs2RT + 2: diag_regs<-1, 1>(a, md, 2, aux, tv, 0u); break;
+                        case cop::kDs2RT + 3: diag_regs<1, -1>(a, md, 2, aux, 0u, tv); break;
+                        case cop::kDs2RT + 4: diag_regs<-1, 2>(a, md, 2, aux, tv, 0u); break;
+                        case cop::kDs2RT + 5: diag_regs<2, -1>(a, md, 2, aux, 0u, tv); break;
+                        case cop::kDs2RT + 6: diag_regs<-1, 3>(a, md, 2, aux, tv, 0u); break;
+                        case cop::kDs2RT + 7: diag_regs<3, -1>(a, md, 2, aux, 0u, tv); break;
+                        case cop::kDs2TT: {
+                            const uint32_t cc = sw[pc++];
+                            diag_regs<-1, -1>(a, md, 2, aux, (tb >> (cc & 15u)) & 1u, (tb >> ((cc >> 4) & 15u)) & 1u);
+                        } break;
+                        case cop::kSigns: {
+                            uint32_t M = 0;
+                            for (uint32_t i = 0; i < aux; ++i) {
+                                const uint32_t mono = sw[pc++];
+                                uint32_t mm = 0xffffu;
+                                for (uint32_t f = 0; f < 6; ++f) {
+                                    const uint32_t src = (mono >> (5 * f)) & 31u;
+                                    if (src == cop::kSrcNone) break;
+                                    const uint32_t v =
+                                        (src & cop::kSrcReg)
+                                            ? static_cast<uint32_t>(0xFF00F0F0CCCCAAAAull >> (16 * (src & 3u))) & 0xffffu
+                                            : (((tb >> src) & 1u) ? 0xffffu : 0u);
+                                    mm &= v;
+                                }
+                                M ^= mm;
                             }
-                        } else {
-                            switch (G.pos(0)) {
-                                case 0: g1<0>(a, md); break;
-                                case 1: g1<1>(a, md); break;
-                                case 2: g1<2>(a, md); break;
-                                default: g1<3>(a, md); break;
-                            }
-                        }
-                    } else if (G.op() == TOP_G2) {
-                        const int p0 = static_cast<int>(G.pos(0)), p1 = static_cast<int>(G.pos(1));
-                        switch (G.kind()) {
-#define MB2_P12(x, y) perm2<x, y, TK_SW12>(a)
-#define MB2_P13(x, y) perm2<x, y, TK_SW13>(a)
-#define MB2_P23(x, y) perm2<x, y, TK_SW23>(a)
-#define MB2_G2(x, y) g2<x, y>(a, md)
-                            case TK_SW12: MB2_PAIR_SWITCH(p0, p1, MB2_P12); break;
-                            case TK_SW13: MB2_PAIR_SWITCH(p0, p1, MB2_P13); break;
-                            case TK_SW23: MB2_PAIR_SWITCH(p0, p1, MB2_P23); break;
-                            default: MB2_PAIR_SWITCH(p0, p1, MB2_G2); break;
-#undef MB2_P12
-#undef MB2_P13
-#undef MB2_P23
-#undef MB2_G2
-                        }
-                    } else {  // TOP_DIAG: entry per amplitude (k <= 6)
-                        const uint32_t k = G.k();
-                        uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
-                        for (uint32_t b = 0; b < k; ++b) {
-                            const uint32_t bit = 1u << G.pos(b);
-                            et |= ((tb & bit) ? 1u : 0u) << b;
-                            if (bit == rb[0]) e0 = 1u << b;
-                            if (bit == rb[1]) e1 = 1u << b;
-                            if (bit == rb[2]) e2 = 1u << b;
-                            if (bit == rb[3]) e3 = 1u << b;
-                        }
 #pragma unroll
-                        for (int j = 0; j < kNA; ++j) {
-                            const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) | ((j & 4) ? e2 : 0u) |
-                                               ((j & 8) ? e3 : 0u);
-                            a[j] = cmulf(entry(md, e), a[j]);
-                        }
+                            for (int j = 0; j < kNA; ++j) a[j] = fneg_if(a[j], (M >> j) & 1u);
+                        } break;
+                        default: {  // cop::kDiagK: entry per amplitude
+                            const uint32_t pos = sw[pc++];
+                            uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+                            for (uint32_t b = 0; b < aux; ++b) {
+                                const uint32_t bit = 1u << ((pos >> (4 * b)) & 15u);
+                                et |= ((tb & bit) ? 1u : 0u) << b;
+                                if (bit == rb[0]) e0 = 1u << b;
+                                if (bit == rb[1]) e1 = 1u << b;
+                                if (bit == rb[2]) e2 = 1u << b;
+                                if (bit == rb[3]) e3 = 1u << b;
+                            }
+#pragma unroll
+                            for (int j = 0; j < kNA; ++j) {
+                                const uint32_t e = et | ((j & 1) ? e0 : 0u) | ((j & 2) ? e1 : 0u) |
+                                                   ((j & 4) ? e2 : 0u) | ((j & 8) ? e3 : 0u);
+                                a[j] = cmulf(entry(md, e), a[j]);
+                            }
+                        } break;
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < kNA; ++j) tile[adr[j]] = a[j];
+                for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
                 __syncthreads();
-            } else if (I.op() == TOP_SMEM) {
-                const uint32_t k = I.k(), dim = 1u << k;
+            } else if (op0 == cop::kSmem) {
+                const uint32_t k = (w0 >> 8) & 0xffu, dim = 1u << k;
+                const uint32_t pos = sw[pc + 1];
+                const double* md = gdata + sw[pc + 2];
+                pc += 3;
+                auto qpos = [&](uint32_t b) -> uint32_t { return (pos >> (4 * b)) & 15u; };
                 uint32_t opm = 0;
-                for (uint32_t b = 0; b < k; ++b) opm |= 1u << I.pos(b);
-                const double* md = gdata + I.data();
+                for (uint32_t b = 0; b < k; ++b) opm |= 1u << qpos(b);
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) {
                     const uint32_t l = tid | (static_cast<uint32_t>(j) << tbits);
                     uint32_t out = 0;
-                    for (uint32_t b = 0; b < k; ++b) out |= ((l >> I.pos(b)) & 1u) << b;
+                    for (uint32_t b = 0; b < k; ++b) out |= ((l >> qpos(b)) & 1u) << b;
                     const uint32_t gbase = l & ~opm;
                     float2 acc = make_float2(0.f, 0.f);
                     for (uint32_t in = 0; in < dim; ++in) {
                         uint32_t li = gbase;
                         for (uint32_t b = 0; b < k; ++b)
-                            if ((in >> b) & 1u) li |= 1u << I.pos(b);
+                            if ((in >> b) & 1u) li |= 1u << qpos(b);
                         acc = cfma(entry(md, out * dim + in), tile[swz8(li)], acc);
                     }
                     a[j] = acc;
                 }
                 __syncthreads();
 #pragma unroll
-                for (int j = 0; j < kNA; ++j) tile[cadr[j]] = a[j];
+                for (int j = 0; j < kNA; ++j) tile[slot(j)] = a[j];
                 __syncthreads();
+            } else {
+                break;  // padding after the last instruction
             }
         }
-        const uint64_t base = pdep64(t, nmask) | off_lo;
+        const IDX b0 = cbase + off_lo;
 #pragma unroll
-        for (int j = 0; j < kNA; ++j) st[base | reg_off(j)] = tile[cadr[j]];
+        for (int j = 0; j < kNA; ++j) st[b0 + reg_off(j)] = tile[slot(j)];
+        cbase = advance(cbase);
         __syncthreads();
     }
+}
+
+template <int MAXT, int MINB, int MT, typename IDX>
+int launch_c64_instance(const TileLaunch& L) {
+    static size_t dyn_max = 0;
+    if (dyn_max == 0) {
+        cudaFuncAttributes fa{};
+        if (cudaFuncGetAttributes(&fa, k_tile_pass_c64<MAXT, MINB, MT, IDX>) != cudaSuccess) return launch_status();
+        dyn_max = kTileSmemMax - fa.sharedSizeBytes;
+        if (cudaFuncSetAttribute(k_tile_pass_c64<MAXT, MINB, MT, IDX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(dyn_max)) != cudaSuccess)
+            return launch_status();
+    }
+    if (L.smem > dyn_max) return MB2_ERR_INVALID;
+    k_tile_pass_c64<MAXT, MINB, MT, IDX><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
+        static_cast<float2*>(L.amps), L.n_all, L.m, L.smask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata, L.ntiles,
+        L.pdata, L.pstride, L.param_lo, L.param_len, L.bshift, L.stages);
+    return launch_status();
 }
 
 // Scales every amplitude by s (FP32 product of an FP64-computed factor).
@@ -347,28 +420,47 @@ __global__ void k_scale_c64(float2* st, uint64_t n_amps, float s) {
 
 }  // namespace
 
-int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
-                         const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_tile_pass_c64, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(3 * (size_t{1} << kMaxTileQubitsC64) * sizeof(float2) + kMaxStagedBytes));
-        attr_set = true;
-    }
+int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
+                         const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
+                         const BatchLayout* batch) {
     if (pass.m > kMaxTileQubitsC64 || pass.m < kMinTileQubits) return MB2_ERR_INVALID;
-    const size_t staged = size_t{pass.prog_count} * sizeof(TileInstr) + size_t{pass.sdata_count} * sizeof(double);
-    if (staged > kMaxStagedBytes) return MB2_ERR_INVALID;
-    const uint32_t threads = 1u << (pass.m - kRegQubits);
-    const uint32_t stages = pass.m == kMaxTileQubitsC64 ? 3u : 2u;
-    const size_t smem = stages * (size_t{1} << pass.m) * sizeof(float2) + staged;
-    const uint64_t ntiles = (uint64_t{1} << n) >> pass.m;
-    const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m <= 12 ? 2u : 1u);
-    const int grid = static_cast<int>(ntiles < cap ? ntiles : cap);
-    k_tile_pass_c64<<<grid, threads, smem, static_cast<cudaStream_t>(stream)>>>(
-        static_cast<float2*>(amps), n, pass.m, pass.smask, dev_instrs + pass.prog_begin, pass.prog_count,
-        dev_sdata + pass.sdata_begin, pass.sdata_count, dev_gdata, ntiles, stages);
+    if ((pass.word_count & 3u) != 0 || (pass.param_len != 0 && batch == nullptr)) return MB2_ERR_INVALID;
+    TileLaunch L;
+    L.amps = amps;
+    L.m = pass.m;
+    L.smask = pass.smask;
+    L.words = dev_words + pass.word_begin;
+    L.nwords = pass.word_count;
+    L.sdata = dev_sdata + pass.sdata_begin;
+    L.nsdata = pass.sdata_count;
+    L.gdata = dev_gdata;
+    L.pdata = batch ? batch->pdata : nullptr;
+    L.pstride = batch ? batch->pstride : 0u;
+    L.param_lo = pass.param_lo;
+    L.param_len = pass.param_len;
+    L.bshift = n - pass.m;
+    L.stream = stream;
+    L.threads = 1u << (pass.m - kRegQubits);
+    // 13-qubit tiles (64 KiB): one CTA per SM with three buffers; smaller
+    // tiles: two CTAs per SM with two buffers each.
+    L.stages = pass.m == kMaxTileQubitsC64 ? 3u : 2u;
+    L.smem = L.stages * (size_t{1} << pass.m) * sizeof(float2) + size_t{pass.word_count} * 4 +
+             (size_t{pass.sdata_count} + pass.param_len) * sizeof(double);
+    L.ntiles = (uint64_t{1} << n) >> pass.m;
+    L.n_all = n;
+    if (batch != nullptr) {
+        L.ntiles *= batch->bindings;
+        while ((uint64_t{1} << (L.n_all - n)) < batch->bindings) ++L.n_all;
+    }
+    const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m == kMaxTileQubitsC64 ? 1u : 2u);
+    L.grid = static_cast<int>(L.ntiles < cap ? L.ntiles : cap);
+    int rc;
+    if (pass.m == kMaxTileQubitsC64)
+        rc = L.n_all <= 32 ? launch_c64_instance<512, 1, 13, uint32_t>(L) : launch_c64_instance<512, 1, 13, uint64_t>(L);
+    else
+        rc = launch_c64_instance<512, 1, 0, uint64_t>(L);
     note_launches(1);
-    return launch_status();
+    return rc;
 }
 
 int launch_scale_c64(void* amps, uint64_t n_amps, float s, void* stream) {

@@ -248,12 +248,14 @@ int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorte
                   uint64_t* dev_basis, void* stream, int precision = MB2_C128);
 // complex64 precision path (kernels_c64.cu).
 constexpr uint32_t kMaxTileQubitsC64 = 13;
-int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const TileInstr* dev_instrs,
-                         const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream);
+int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
+                         const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
+                         const BatchLayout* batch = nullptr);
 int launch_scale_c64(void* amps, uint64_t n_amps, float s, void* stream);
 int context_device(const mb2_context* ctx);
 // A complex128 state on a caller-owned stream (engine.cpp).
-int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, void* stream, mb2_state** out);
+int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, void* stream, mb2_state** out,
+                    int precision = MB2_C128);
 
 // Calibration probes (kernels_probe.cu): FP64 instructions per second and
 // device-to-device copy GB/s (read + write bytes), on the current device.

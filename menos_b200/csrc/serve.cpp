@@ -43,6 +43,7 @@ struct Request {
     double global_phase = 0.0;
     int32_t fuse = 1;
     int32_t output = MB2_OUT_EXPECTATION;
+    int32_t precision = MB2_C128;
     uint64_t shots = 0, seed = 0;
     std::vector<uint32_t> targets;
     std::vector<uint64_t> xs, zs;
@@ -57,7 +58,7 @@ struct Done {
 };
 
 uint64_t admission_bytes(const Request& r) {
-    const uint64_t state = (uint64_t{1} << r.n) * 16;
+    const uint64_t state = (uint64_t{1} << r.n) * (r.precision == MB2_C64 ? 8 : 16);
     const uint64_t nchunks = std::max<uint64_t>(1, (uint64_t{1} << r.n) / mb2::kSampleChunk);
     const uint64_t sampler = r.output == MB2_OUT_COUNTS ? 16 * r.shots + 128 * nchunks : 0;
     const uint64_t expect = 16ull * mb2::kExpBlocks * std::max<size_t>(1, r.xs.size());
@@ -108,7 +109,7 @@ bool pick(mb2_server* s, Request& out) {
 
 void run_request(mb2_server* s, cudaStream_t stream, Request& r, Done& d) {
     mb2_state* st = nullptr;
-    int rc = mb2::state_on_stream(s->ctx, r.n, ~uint64_t{0}, stream, &st);
+    int rc = mb2::state_on_stream(s->ctx, r.n, ~uint64_t{0}, stream, &st, r.precision);
     if (rc == MB2_OK) rc = mb2_init(st, r.global_phase);
     if (rc == MB2_OK) {
         mb2_sweep_options o{r.fuse, 0, 0, 0};
@@ -203,6 +204,8 @@ int mb2_server_submit(mb2_server* s, const mb2_request* q, uint64_t* ticket) {
     r.global_phase = q->global_phase;
     r.fuse = q->fuse_gates;
     r.output = q->output;
+    if (q->precision != MB2_C128 && q->precision != MB2_C64) return MB2_ERR_INVALID;
+    r.precision = q->precision;
     r.shots = q->shots;
     r.seed = q->seed;
     r.ops.assign(q->ops, q->ops + q->num_ops);

@@ -197,10 +197,11 @@ class DeviceState:
 
 
 def sweep_batch(ctx: Context, circ: Circuit, params, paulis, coefs, fuse_gates: bool = False, tile_qubits: int = 0,
-                want_states: bool = False):
+                want_states: bool = False, precision: int = C128):
     """mb2_sweep_batch: <H> per binding for params[b] (one row per binding,
     the circuit's parameter slots in op order).  Returns (values, states or
-    None, stats)."""
+    None, stats).  precision C64: complex64 states (FP32 gates, FP64
+    reductions); states are returned promoted to complex128."""
     params = np.ascontiguousarray(np.asarray(params, np.float64))
     if params.ndim == 1:
         params = params.reshape(1, -1)
@@ -211,7 +212,7 @@ def sweep_batch(ctx: Context, circ: Circuit, params, paulis, coefs, fuse_gates: 
     cs = np.ascontiguousarray(list(coefs) or [0.0], dtype=np.float64)
     out = np.zeros(B, np.float64)
     states = np.zeros((B, 1 << circ.num_qubits), np.complex128) if want_states else None
-    opts = _lib.BatchOptions(C128, 1 if fuse_gates else 0, tile_qubits, 0)
+    opts = _lib.BatchOptions(precision, 1 if fuse_gates else 0, tile_qubits, 0)
     stats = _lib.BatchStats()
     check(lib().mb2_sweep_batch(ctx.h, arr, len(circ.ops), circ.num_qubits, params.ctypes.data, ppb, B,
                                 xs.ctypes.data, zs.ctypes.data, cs.ctypes.data, len(paulis), C.byref(opts),

@@ -22,7 +22,7 @@ class Server:
         self.h = h
 
     def submit(self, circ: Circuit, output: str = "expectation", shots: int = 0, seed: int = 0, targets=(),
-               paulis=(), coefs=(), fuse_gates: bool = True) -> int:
+               paulis=(), coefs=(), fuse_gates: bool = True, precision: int = _lib.C128) -> int:
         arr, keep = to_mb2_ops(circ)
         t = np.ascontiguousarray(np.asarray(targets, np.uint32).ravel())
         xs = np.ascontiguousarray([int(p[0]) for p in paulis] or [0], dtype=np.uint64)
@@ -43,6 +43,7 @@ class Server:
         req.x_masks = xs.ctypes.data
         req.z_masks = zs.ctypes.data
         req.coefs = cs.ctypes.data
+        req.precision = precision
         ticket = C.c_uint64()
         check(lib().mb2_server_submit(self.h, C.byref(req), C.byref(ticket)), self.ctx.h, "mb2_server_submit")
         del keep

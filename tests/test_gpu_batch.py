@@ -55,3 +55,19 @@ def test_batch_hea16_subset(ctx, ref):
         assert bits_equal(states[b], r["statevector"])
         h = sum(w * t for w, t in zip(coefs, r["terms"]))
         assert abs(vals[b] - h.real) <= 1e-11
+
+
+def test_batch_complex64_within_tolerance(ctx):
+    # The complex64 batch against the complex128 one (itself bitwise the
+    # reference): <H> within the precision path's 1e-6, states within 1e-5.
+    from menos_b200._lib import C64
+    n, layers, B = 16, 8, 24
+    rows = workloads.hea_bindings(n, layers, B, 31)
+    paulis = workloads.pauli_strings(n, 32, 32)
+    coefs = workloads.weights(32, 33)
+    circ = workloads.hea(n, layers, 0)
+    hi, s_hi, _ = sweep_batch(ctx, circ, rows, paulis, coefs, want_states=True)
+    lo, s_lo, stats = sweep_batch(ctx, circ, rows, paulis, coefs, want_states=True, precision=C64)
+    assert stats.parametric_blocks > 0
+    assert np.max(np.abs(lo - hi)) <= 1e-6
+    assert np.max(np.abs(s_lo - s_hi)) <= 1e-5

@@ -72,3 +72,33 @@ def test_poll_times_out_when_idle(ctx):
     srv = Server(ctx, slots=2)
     assert srv.poll(timeout_ms=50) == []
     srv.close()
+
+
+def test_complex64_requests_same_alone_and_in_the_mix(ctx):
+    # The precision path through the server: each result equals the same
+    # request run alone in complex64, and <H> is within 1e-6 of complex128.
+    from menos_b200._lib import C64
+    reqs = workloads.serving_stream(24, 1000.0, 11, nmin=8, nmax=18, dmin=2, dmax=10, shots=2048, terms=16)
+    srv = Server(ctx, slots=8)
+    tickets = {}
+    for r in reqs:
+        n = r["circuit"].num_qubits
+        t = srv.submit(r["circuit"], r["output"], shots=r["shots"], seed=r["seed"],
+                       targets=[(q, q) for q in range(n)], paulis=r["paulis"], coefs=r["coefs"], precision=C64)
+        tickets[t] = r
+    got = collect(srv, len(reqs))
+    srv.close()
+    assert len(got) == len(reqs)
+    for t, r in tickets.items():
+        c = got[t]
+        assert c["status"] == 0
+        circ = r["circuit"]
+        st = DeviceState(ctx, circ.num_qubits, precision=C64)
+        st.init(circ.global_phase)
+        st.apply_program(circ)
+        if r["output"] == "counts":
+            assert c["counts"] == st.sample(r["shots"], r["seed"], [(q, q) for q in range(circ.num_qubits)])
+        else:
+            terms = st.expectation(r["paulis"])
+            assert c["value"] == sum(w * v.real for w, v in zip(r["coefs"], terms))
+            assert abs(c["value"] - alone(ctx, r)) <= 1e-6
