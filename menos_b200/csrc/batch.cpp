@@ -90,53 +90,113 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     const bool c64 = o.precision == MB2_C64;
     const bool fuse = o.fuse_gates != 0;
 
-    // ---- host: every binding's blocks (threads), the shared structure, flags.
-    std::vector<std::vector<mb2::Block>> per(num_bindings);
-    try {
-        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        const unsigned nt = std::min<unsigned>(hw, num_bindings);
+    // ---- host: the shared block structure and, per block, whether it is
+    // parametric and what holds for every binding (threads over bindings).
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = std::min<unsigned>(hw, num_bindings);
+    auto parallel = [&](auto&& body) {  // body(worker) for workers 0..nt-1; false on any exception
         std::vector<std::thread> pool;
         std::vector<std::string> errors(nt);
-        for (unsigned w = 0; w < nt; ++w) {
+        for (unsigned w = 0; w < nt; ++w)
             pool.emplace_back([&, w]() {
                 try {
-                    for (uint32_t b = w; b < num_bindings; b += nt)
-                        per[b] = binding_blocks(ops, num_ops, params + size_t{b} * params_per_binding, fuse);
+                    body(w);
                 } catch (const std::exception& e) {
                     errors[w] = e.what();
                 }
             });
-        }
         for (auto& th : pool) th.join();
         for (const auto& e : errors)
-            if (!e.empty()) throw std::invalid_argument(e);
+            if (!e.empty()) return false;
+        return true;
+    };
+    std::vector<mb2::Block> shape;
+    std::vector<std::vector<mb2::Block>> per;  // every binding's blocks (fused batches only)
+    // Unfused: block i is gate op i; only gates with parameters can differ,
+    // and their matrices are built per binding from the gate table.
+    std::vector<uint32_t> gate_op, gate_pofs;
+    try {
+        shape = binding_blocks(ops, num_ops, params, fuse);
     } catch (const std::exception&) {
         return MB2_ERR_INVALID;
     }
-    std::vector<mb2::Block> shape = per[0];
     const size_t nb = shape.size();
-    for (uint32_t b = 1; b < num_bindings; ++b) {  // one structure for every binding
-        if (per[b].size() != nb) return MB2_ERR_INVALID;
-        for (size_t i = 0; i < nb; ++i)
-            if (per[b][i].k != shape[i].k || per[b][i].mask() != shape[i].mask()) return MB2_ERR_INVALID;
-    }
     std::vector<uint8_t> flags(nb, 0);
-    for (size_t i = 0; i < nb; ++i) {
-        const uint32_t dim = 1u << shape[i].k;
-        bool differs = false, all_real = true, m00_real = true, all_diag = true;
-        for (uint32_t b = 0; b < num_bindings; ++b) {
-            const auto& m = per[b][i].m;
-            if (std::memcmp(m.data(), shape[i].m.data(), m.size() * sizeof(mb2::Cd)) != 0) differs = true;
-            for (const mb2::Cd& c : m) all_real = all_real && c.imag() == 0.0;
-            m00_real = m00_real && m[0].imag() == 0.0;
-            all_diag = all_diag && per[b][i].diagonal;
+    if (!fuse) {
+        uint32_t k = 0;
+        for (uint32_t i = 0; i < num_ops; ++i) {
+            if (ops[i].opcode == MB2_MEASURE) continue;
+            gate_op.push_back(i);
+            gate_pofs.push_back(k);
+            if (ops[i].opcode != MB2_UNITARY) k += static_cast<uint32_t>(mb2::gate_num_params(ops[i].opcode));
         }
-        shape[i].diagonal = all_diag;
-        if (differs) {
-            flags[i] = mb2::kParamBlock | (all_real ? mb2::kParamAllReal : 0) | (m00_real ? mb2::kParamM00Real : 0);
-            if (!all_diag && shape[i].k > 2) return MB2_ERR_UNSUPPORTED;  // parametric wide dense blocks
+        if (gate_op.size() != nb) return MB2_ERR_INVALID;
+        // Per worker: differs / all_real / m00_real / all_diag per block.
+        std::vector<std::vector<uint8_t>> acc(nt, std::vector<uint8_t>(4 * nb, 0));
+        const bool ok = parallel([&](unsigned w) {
+            std::vector<mb2::Cd> m;
+            auto& f = acc[w];
+            for (size_t i = 0; i < nb; ++i) f[4 * i + 1] = f[4 * i + 2] = f[4 * i + 3] = 1;
+            for (uint32_t b = w; b < num_bindings; b += nt) {
+                const double* pb = params + size_t{b} * params_per_binding;
+                for (size_t i = 0; i < nb; ++i) {
+                    const mb2_op& o = ops[gate_op[i]];
+                    const int np = o.opcode == MB2_UNITARY ? 0 : mb2::gate_num_params(o.opcode);
+                    if (np == 0) continue;
+                    if (mb2::gate_matrix(o.opcode, pb + gate_pofs[i], m) == 0)
+                        throw std::invalid_argument("gate matrix");
+                    const uint32_t dim = 1u << shape[i].k;
+                    if (std::memcmp(m.data(), shape[i].m.data(), m.size() * sizeof(mb2::Cd)) != 0) f[4 * i] = 1;
+                    for (const mb2::Cd& c : m) f[4 * i + 1] &= c.imag() == 0.0 ? 1 : 0;
+                    f[4 * i + 2] &= m[0].imag() == 0.0 ? 1 : 0;
+                    for (uint32_t r = 0; r < dim; ++r)
+                        for (uint32_t c = 0; c < dim; ++c)
+                            if (r != c && (m[r * dim + c].real() != 0.0 || m[r * dim + c].imag() != 0.0)) f[4 * i + 3] = 0;
+                }
+            }
+        });
+        if (!ok) return MB2_ERR_INVALID;
+        for (size_t i = 0; i < nb; ++i) {
+            bool differs = false, all_real = true, m00_real = true, all_diag = true;
+            for (unsigned w = 0; w < nt; ++w) {
+                differs = differs || acc[w][4 * i];
+                all_real = all_real && acc[w][4 * i + 1];
+                m00_real = m00_real && acc[w][4 * i + 2];
+                all_diag = all_diag && acc[w][4 * i + 3];
+            }
+            shape[i].diagonal = shape[i].diagonal && all_diag;
+            if (differs) {
+                flags[i] = mb2::kParamBlock | (all_real ? mb2::kParamAllReal : 0) | (m00_real ? mb2::kParamM00Real : 0);
+                if (!shape[i].diagonal && shape[i].k > 2) return MB2_ERR_UNSUPPORTED;
+            }
         }
-        (void)dim;
+    } else {
+        per.resize(num_bindings);
+        const bool ok = parallel([&](unsigned w) {
+            for (uint32_t b = w; b < num_bindings; b += nt)
+                per[b] = binding_blocks(ops, num_ops, params + size_t{b} * params_per_binding, fuse);
+        });
+        if (!ok) return MB2_ERR_INVALID;
+        for (uint32_t b = 1; b < num_bindings; ++b) {  // one structure for every binding
+            if (per[b].size() != nb) return MB2_ERR_INVALID;
+            for (size_t i = 0; i < nb; ++i)
+                if (per[b][i].k != shape[i].k || per[b][i].mask() != shape[i].mask()) return MB2_ERR_INVALID;
+        }
+        for (size_t i = 0; i < nb; ++i) {
+            bool differs = false, all_real = true, m00_real = true, all_diag = true;
+            for (uint32_t b = 0; b < num_bindings; ++b) {
+                const auto& m = per[b][i].m;
+                if (std::memcmp(m.data(), shape[i].m.data(), m.size() * sizeof(mb2::Cd)) != 0) differs = true;
+                for (const mb2::Cd& c : m) all_real = all_real && c.imag() == 0.0;
+                m00_real = m00_real && m[0].imag() == 0.0;
+                all_diag = all_diag && per[b][i].diagonal;
+            }
+            shape[i].diagonal = all_diag;
+            if (differs) {
+                flags[i] = mb2::kParamBlock | (all_real ? mb2::kParamAllReal : 0) | (m00_real ? mb2::kParamM00Real : 0);
+                if (!all_diag && shape[i].k > 2) return MB2_ERR_UNSUPPORTED;  // parametric wide dense blocks
+            }
+        }
     }
     const uint32_t mmax = c64 ? mb2::kMaxTileQubitsC64 : mb2::kMaxTileQubits;
     uint32_t m = o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : (c64 ? mb2::kMaxTileQubitsC64 : 11u);
@@ -151,22 +211,34 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     // Per-binding records of the parametric blocks, in the kernel's layout.
     const size_t stride = prog.param_stride;
     std::vector<double> pdata(std::max<size_t>(1, stride * num_bindings), 0.0);
-    for (uint32_t b = 0; b < num_bindings; ++b) {
-        for (size_t i = 0; i < nb; ++i) {
-            if (!(flags[i] & mb2::kParamBlock)) continue;
-            const mb2::Block& blk = per[b][i];
-            const uint32_t dim = 1u << blk.k;
-            double* dst = pdata.data() + size_t{b} * stride + prog.param_offsets[i];
-            if (shape[i].diagonal) {
-                for (uint32_t e = 0; e < dim; ++e) {
-                    dst[2 * e] = blk.m[size_t{e} * dim + e].real();
-                    dst[2 * e + 1] = blk.m[size_t{e} * dim + e].imag();
-                }
-            } else {
-                std::memcpy(dst, blk.m.data(), size_t{dim} * dim * sizeof(mb2::Cd));
+    auto write_record = [&](uint32_t b, size_t i, const std::vector<mb2::Cd>& m, uint32_t k) {
+        const uint32_t dim = 1u << k;
+        double* dst = pdata.data() + size_t{b} * stride + prog.param_offsets[i];
+        if (shape[i].diagonal) {
+            for (uint32_t e = 0; e < dim; ++e) {
+                dst[2 * e] = m[size_t{e} * dim + e].real();
+                dst[2 * e + 1] = m[size_t{e} * dim + e].imag();
             }
+        } else {
+            std::memcpy(dst, m.data(), size_t{dim} * dim * sizeof(mb2::Cd));
         }
-    }
+    };
+    const bool filled = parallel([&](unsigned w) {
+        std::vector<mb2::Cd> m;
+        for (uint32_t b = w; b < num_bindings; b += nt)
+            for (size_t i = 0; i < nb; ++i) {
+                if (!(flags[i] & mb2::kParamBlock)) continue;
+                if (fuse) {
+                    write_record(b, i, per[b][i].m, per[b][i].k);
+                } else {
+                    const mb2_op& o = ops[gate_op[i]];
+                    if (mb2::gate_matrix(o.opcode, params + size_t{b} * params_per_binding + gate_pofs[i], m) == 0)
+                        throw std::invalid_argument("gate matrix");
+                    write_record(b, i, m, shape[i].k);
+                }
+            }
+    });
+    if (!filled) return MB2_ERR_INVALID;
 
     // ---- device
     Runner r{0};
