@@ -49,6 +49,20 @@ def kernel_launches() -> int:
     return int(v.value)
 
 
+def profiled_traffic(n: int):
+    """DRAM bytes of one tile-pass launch, from the committed ncu summary
+    (measured at 26 qubits, scaled to 2^n: every tile is read and written
+    once), or None when the summary is absent."""
+    import re
+    path = os.path.join(ROOT, "profiles", "k_tile_pass_c2_26q_ncu_full.md")
+    try:
+        with open(path) as f:
+            m = re.search(r"traffic_bytes_per_launch_30q:\s*([0-9.eE+]+)", f.read())
+    except OSError:
+        return None
+    return round(float(m.group(1)) * 2.0 ** (n - 30)) if m else None
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -302,7 +316,9 @@ def main():
                    "passes": passes, "blocks": int(stats.blocks), "sweep_ms": round(sweep_avg, 2),
                    "tile_qubits": args.tile or 11},
         "roofline": {"bound": "hbm", "kernel": "k_tile_pass", "achieved": round(achieved, 1), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": profiled_traffic(n),
+                     "traffic_source": "ncu dram__bytes_read+write of one pass at 26 qubits, scaled by the "
+                                       "state size (profiles/k_tile_pass_c2_26q_ncu_full.md)",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": 2 * state_bytes},
         "fp64": {"kernel": "k_tile_pass", "achieved_ops_per_s": round(stats.fp64_ops_per_amp * (1 << n) /
