@@ -100,7 +100,7 @@ struct TilePass {
     // [param_lo, param_lo + param_len), staged after the pass's data.
     uint32_t param_lo = 0;
     uint32_t param_len = 0;
-    bool heavy = false;  // has kGen2, kDiagK or kSmem words
+    bool heavy = false;  // has two-qubit dense/monomial/permutation, kDiagK or kSmem words
 };
 
 // Compact instruction stream of the complex128 tile kernel, written from the
@@ -218,7 +218,7 @@ struct TileLaunch {
     uint32_t stages = 2;
     int grid = 0;       // set by the instance launcher
     int sm_count = 0;
-    bool heavy = false;  // the pass has dense 2q, wide diagonal or shared-memory blocks
+    bool heavy = false;  // the pass needs the full kernel variant (see TilePass::heavy)
     uint32_t threads = 0;
     size_t smem = 0;
     void* stream = nullptr;

@@ -149,17 +149,28 @@ void encode_compact(TileProgram& prog) {
                     break;
                 }
                 case TOP_G1: {
+                    // X and monomial rows as general 2x2 products: the zero
+                    // entry's product only moves a zero's sign, so the result
+                    // is the same, and the kernel's lean variant keeps no
+                    // register-moving instructions.
                     const uint32_t p = g.pos[0];
                     switch (g.kind) {
                         case TK_U3: w.push_back(header(cop::kU3 + p, 0, 0, off)); break;
                         case TK_REAL: w.push_back(header(cop::kReal1 + p, 0, 0, off)); break;
-                        case TK_X: w.push_back(header(cop::kX1 + p, 0, 0, 0)); break;
-                        case TK_MONO: w.push_back(header(cop::kMono1 + p, g.aux & 63u, 0, off)); break;
+                        case TK_X:
+                            w.push_back(header(cop::kReal1 + p, 0, 0, off));
+                            prog.fp64_per_amp += 6;
+                            break;
+                        case TK_MONO:
+                            w.push_back(header(cop::kGen1 + p, 0, 0, off));
+                            prog.fp64_per_amp += 8;
+                            break;
                         default: w.push_back(header(cop::kGen1 + p, 0, 0, off)); break;
                     }
                     break;
                 }
                 case TOP_G2: {
+                    heavy = true;  // permutations and monomials move registers: full variant
                     const uint32_t pr = pair_index(g.pos[0], g.pos[1]);
                     switch (g.kind) {
                         case TK_SW12: w.push_back(header(cop::kSw12 + pr, 0, 0, 0)); break;
@@ -169,10 +180,7 @@ void encode_compact(TileProgram& prog) {
                             w.push_back(header(cop::kMono2 + pr, 0, 0, off));
                             w.push_back(g.aux);
                             break;
-                        default:
-                            heavy = true;
-                            w.push_back(header(cop::kGen2 + pr, 0, 0, off));
-                            break;
+                        default: w.push_back(header(cop::kGen2 + pr, 0, 0, off)); break;
                     }
                     break;
                 }

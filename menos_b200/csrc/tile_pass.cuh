@@ -225,10 +225,14 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // The instructions of one pass applied to one tile held in shared memory
 // (canonical layout on entry and exit).  `sync` is the barrier of the
 // threads that share the tile; parametric data sits pshift doubles past the
-// staged data's end.  FULL = false compiles out the rare heavy instructions
-// (dense two-qubit blocks, wide diagonals, shared-memory blocks), whose
-// register needs would otherwise set the count for the whole kernel; the
-// launcher picks that variant only for passes without them.
+// staged data's end.  FULL = false compiles out every instruction that moves
+// amplitudes between registers or selects them at run time (permutations,
+// monomial rows) and the rare heavy ones (dense two-qubit blocks, wide
+// diagonals, shared-memory blocks): measured per U3, their presence in the
+// same switch costs ~60-85 extra register moves on every gate path (the
+// allocator's layout at the merge).  The launcher picks the lean variant for
+// passes without them (the encoder writes single-qubit X and monomial gates
+// as general 2x2 products, exact up to zero signs).
 template <int MT, bool FULL, typename SYNC>
 __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const uint32_t* __restrict__ sw,
                                              uint32_t nwords, const double* __restrict__ sd, uint32_t nsdata,
@@ -276,34 +280,34 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
                 const double* md = sd + off + (off >= nsdata ? pshift : 0u);
                 const uint32_t tv = (tb >> ((w >> 16) & 15u)) & 1u;  // the thread-bit operand's value
                 switch (op) {
-#define MB2_CASE4(BASE, STMT) \
-case BASE + 0: { constexpr int P = 0; STMT; } break; \
-case BASE + 1: { constexpr int P = 1; STMT; } break; \
-case BASE + 2: { constexpr int P = 2; STMT; } break; \
-case BASE + 3: { constexpr int P = 3; STMT; } break;
-#define MB2_CASE12(BASE, STMT) \
-case BASE + 0: { constexpr int P0 = 0, P1 = 1; STMT; } break; \
-case BASE + 1: { constexpr int P0 = 0, P1 = 2; STMT; } break; \
-case BASE + 2: { constexpr int P0 = 0, P1 = 3; STMT; } break; \
-case BASE + 3: { constexpr int P0 = 1, P1 = 0; STMT; } break; \
-case BASE + 4: { constexpr int P0 = 1, P1 = 2; STMT; } break; \
-case BASE + 5: { constexpr int P0 = 1, P1 = 3; STMT; } break; \
-case BASE + 6: { constexpr int P0 = 2, P1 = 0; STMT; } break; \
-case BASE + 7: { constexpr int P0 = 2, P1 = 1; STMT; } break; \
-case BASE + 8: { constexpr int P0 = 2, P1 = 3; STMT; } break; \
-case BASE + 9: { constexpr int P0 = 3, P1 = 0; STMT; } break; \
-case BASE + 10: { constexpr int P0 = 3, P1 = 1; STMT; } break; \
-case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
+#define MB2_CASE4(BASE, ...) \
+    case BASE + 0: { constexpr int P = 0; __VA_ARGS__; } break; \
+    case BASE + 1: { constexpr int P = 1; __VA_ARGS__; } break; \
+    case BASE + 2: { constexpr int P = 2; __VA_ARGS__; } break; \
+    case BASE + 3: { constexpr int P = 3; __VA_ARGS__; } break;
+#define MB2_CASE12(BASE, ...) \
+    case BASE + 0: { constexpr int P0 = 0, P1 = 1; __VA_ARGS__; } break; \
+    case BASE + 1: { constexpr int P0 = 0, P1 = 2; __VA_ARGS__; } break; \
+    case BASE + 2: { constexpr int P0 = 0, P1 = 3; __VA_ARGS__; } break; \
+    case BASE + 3: { constexpr int P0 = 1, P1 = 0; __VA_ARGS__; } break; \
+    case BASE + 4: { constexpr int P0 = 1, P1 = 2; __VA_ARGS__; } break; \
+    case BASE + 5: { constexpr int P0 = 1, P1 = 3; __VA_ARGS__; } break; \
+    case BASE + 6: { constexpr int P0 = 2, P1 = 0; __VA_ARGS__; } break; \
+    case BASE + 7: { constexpr int P0 = 2, P1 = 1; __VA_ARGS__; } break; \
+    case BASE + 8: { constexpr int P0 = 2, P1 = 3; __VA_ARGS__; } break; \
+    case BASE + 9: { constexpr int P0 = 3, P1 = 0; __VA_ARGS__; } break; \
+    case BASE + 10: { constexpr int P0 = 3, P1 = 1; __VA_ARGS__; } break; \
+    case BASE + 11: { constexpr int P0 = 3, P1 = 2; __VA_ARGS__; } break;
                     MB2_CASE4(cop::kU3, (g1<P, TK_U3>(a, md, 0u)))
                     MB2_CASE4(cop::kGen1, (g1<P, TK_GEN>(a, md, 0u)))
                     MB2_CASE4(cop::kReal1, (g1<P, TK_REAL>(a, md, 0u)))
-                    MB2_CASE4(cop::kMono1, (g1<P, TK_MONO>(a, md, aux)))
-                    MB2_CASE4(cop::kX1, (perm1<P>(a)))
+                    MB2_CASE4(cop::kMono1, if constexpr (FULL) g1<P, TK_MONO>(a, md, aux))
+                    MB2_CASE4(cop::kX1, if constexpr (FULL) perm1<P>(a))
                     MB2_CASE12(cop::kGen2, (gen2_if<P0, P1, FULL>(a, md)))
-                    MB2_CASE12(cop::kMono2, (g2<P0, P1, TK_MONO>(a, md, sw[pc++])))
-                    MB2_CASE12(cop::kSw12, (perm2<P0, P1, TK_SW12>(a)))
-                    MB2_CASE12(cop::kSw13, (perm2<P0, P1, TK_SW13>(a)))
-                    MB2_CASE12(cop::kSw23, (perm2<P0, P1, TK_SW23>(a)))
+                    MB2_CASE12(cop::kMono2, if constexpr (FULL) g2<P0, P1, TK_MONO>(a, md, sw[pc++]))
+                    MB2_CASE12(cop::kSw12, if constexpr (FULL) perm2<P0, P1, TK_SW12>(a))
+                    MB2_CASE12(cop::kSw13, if constexpr (FULL) perm2<P0, P1, TK_SW13>(a))
+                    MB2_CASE12(cop::kSw23, if constexpr (FULL) perm2<P0, P1, TK_SW23>(a))
                     MB2_CASE4(cop::kDs1R, (diag_rr<P, -1>(a, load_diag(md, 1, aux))))
                     MB2_CASE12(cop::kDs2RR, (diag_rr<P0, P1>(a, load_diag(md, 2, aux))))
 #undef MB2_CASE4
