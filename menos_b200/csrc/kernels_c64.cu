@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
             if (op0 == cop::kPhase) {
                 const uint32_t tp0 = sw[pc + 1], tp1 = sw[pc + 2];
                 pc += 3;
-                const uint32_t nthread = (w0 >> 8) & 0x7fu;  // bit 7: direct store (complex128 only)
+                const uint32_t nthread = (w0 >> 8) & 0xffu;
                 auto tperm = [&](uint32_t i) -> uint32_t {
                     return (i < 8 ? (tp0 >> (4 * i)) : (tp1 >> (4 * (i - 8)))) & 15u;
                 };

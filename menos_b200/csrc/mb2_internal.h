@@ -129,7 +129,7 @@ constexpr uint32_t kDs2RT = 98;  // + 2 * slot + (index of the thread-bit operan
 constexpr uint32_t kDs2TT = 106; // aux = classes; extra word = the two tile bits (4 bits each)
 constexpr uint32_t kDiagK = 107; // aux = k; extra word = tile positions (4 bits each)
 constexpr uint32_t kSigns = 108; // aux = monomial count; one word per monomial
-constexpr uint32_t kPhase = 200; // aux = thread bits (bit 7: direct store); bits 16-31 register positions; 2 words of tperm
+constexpr uint32_t kPhase = 200; // aux = thread bits; bits 16-31 register positions; 2 words of tperm
 constexpr uint32_t kSmem = 201;  // aux = k; extra words: tile positions, gdata offset (doubles)
 // A sign monomial: six 5-bit sources, 31 = none, 16 + s = register slot s,
 // else a tile bit (a thread bit in that phase).  The amplitudes whose

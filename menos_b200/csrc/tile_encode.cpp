@@ -61,7 +61,6 @@ void encode_compact(TileProgram& prog) {
         };
         auto& w = prog.words;
         bool heavy = false;
-        uint32_t last_phase = UINT32_MAX;  // word index of the last phase, while it is the last group
         uint32_t reg[kRegQubits] = {0, 1, 2, 3};
         // Pending sign monomials (canonical words), toggled so pairs cancel.
         std::map<uint32_t, bool> signs;
@@ -124,7 +123,6 @@ void encode_compact(TileProgram& prog) {
             const uint32_t off = (g.op == TOP_PHASE || g.op == TOP_END || g.op == TOP_SMEM) ? 0u : data_off(g);
             switch (g.op) {
                 case TOP_PHASE: {
-                    last_phase = static_cast<uint32_t>(w.size());
                     uint32_t packed = 0;
                     for (uint32_t s = 0; s < kRegQubits; ++s) {
                         reg[s] = g.pos[s];
@@ -143,7 +141,6 @@ void encode_compact(TileProgram& prog) {
                     break;
                 case TOP_SMEM: {
                     heavy = true;
-                    last_phase = UINT32_MAX;
                     uint32_t packed = 0;
                     for (uint32_t t = 0; t < g.k; ++t) packed |= static_cast<uint32_t>(g.pos[t]) << (4 * t);
                     w.push_back(cop::kSmem | (static_cast<uint32_t>(g.k) << 8));
@@ -219,16 +216,6 @@ void encode_compact(TileProgram& prog) {
             }
         }
         flush_signs();
-        // The pass's last phase may store straight from registers when it is
-        // the last instruction group and its thread bits 0-2 are tile bits
-        // 0-2, which hold qubits 0-2 (eight lanes then cover 128 contiguous
-        // bytes).
-        if (last_phase != UINT32_MAX && (pass.smask & 7u) == 7u) {
-            const uint32_t t0 = w[last_phase + 1];
-            const uint32_t lanes = (1u << (t0 & 15u)) | (1u << ((t0 >> 4) & 15u)) | (1u << ((t0 >> 8) & 15u));
-            const uint32_t nthread = (w[last_phase] >> 8) & 0x7fu;
-            if (lanes == 7u && nthread >= 3) w[last_phase] |= 1u << 15;
-        }
         pass.heavy = heavy;
         while (w.size() & 3u) w.push_back(cop::kEnd);  // 16-byte multiple: the staged data follows
         pass.word_count = static_cast<uint32_t>(w.size()) - pass.word_begin;

@@ -233,20 +233,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // allocator's layout at the merge).  The launcher picks the lean variant for
 // passes without them (the encoder writes single-qubit X and monomial gates
 // as general 2x2 products, exact up to zero signs).
-//
-// A PHASE word with the direct-store flag is the tile's last phase, and its
-// thread bits 0-2 are tile bits 0-2 (qubits 0-2): its amplitudes go from
-// registers straight to HBM (eight lanes write 128 contiguous bytes), which
-// saves a shared-memory write and read of the whole tile; the function then
-// returns true and the caller skips its canonical store.  sbit[i] is the
-// global index bit of tile bit i; tile_base is the tile's deposited index.
-template <int MT, bool FULL, typename IDX, typename SYNC>
-__device__ __forceinline__ bool compute_tile(double2* __restrict__ tile, const uint32_t* __restrict__ sw,
+template <int MT, bool FULL, typename SYNC>
+__device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const uint32_t* __restrict__ sw,
                                              uint32_t nwords, const double* __restrict__ sd, uint32_t nsdata,
                                              uint32_t pshift, const double* __restrict__ gdata, uint32_t tid,
-                                             uint32_t m, SYNC sync, double2* __restrict__ st, IDX tile_base,
-                                             const IDX* __restrict__ sbit) {
-    bool stored = false;
+                                             uint32_t m, SYNC sync) {
     const uint32_t tbits = m - kRegQubits;
     const uint32_t s_tid = swz(tid);
     auto slot = [&](int j) -> uint32_t { return s_tid ^ swz(static_cast<uint32_t>(j) << tbits); };
@@ -258,8 +249,7 @@ __device__ __forceinline__ bool compute_tile(double2* __restrict__ tile, const u
         if (op0 == cop::kPhase) {
             const uint32_t tp0 = sw[pc + 1], tp1 = sw[pc + 2];
             pc += 3;
-            const uint32_t nthread = (w0 >> 8) & 0x7fu;
-            const bool direct = ((w0 >> 15) & 1u) != 0;
+            const uint32_t nthread = (w0 >> 8) & 0xffu;
             auto tperm = [&](uint32_t i) -> uint32_t { return (i < 8 ? (tp0 >> (4 * i)) : (tp1 >> (4 * (i - 8)))) & 15u; };
             uint32_t tb = 0;
             if (MT > 0) {
@@ -382,22 +372,9 @@ __device__ __forceinline__ bool compute_tile(double2* __restrict__ tile, const u
                     } break;
                 }
             }
-            if (direct) {
-                IDX gt = tile_base;
-                for (uint32_t i = 0; i < nthread; ++i)
-                    if ((tid >> i) & 1u) gt += sbit[tperm(i)];
-                const IDX g0 = sbit[(w0 >> 16) & 15u], g1v = sbit[(w0 >> 20) & 15u], g2v = sbit[(w0 >> 24) & 15u],
-                          g3 = sbit[(w0 >> 28) & 15u];
 #pragma unroll
-                for (int j = 0; j < kNA; ++j)
-                    st[gt + ((j & 1) ? g0 : IDX{0}) + ((j & 2) ? g1v : IDX{0}) + ((j & 4) ? g2v : IDX{0}) +
-                       ((j & 8) ? g3 : IDX{0})] = canon(a[j]);
-                stored = true;
-            } else {
-#pragma unroll
-                for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
-                sync();
-            }
+            for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
+            sync();
         } else if (FULL && op0 == cop::kSmem) {
             // A dense k-qubit block (k >= 3) on the whole tile in shared memory.
             const uint32_t k = (w0 >> 8) & 0xffu, dim = 1u << k;
@@ -432,7 +409,6 @@ __device__ __forceinline__ bool compute_tile(double2* __restrict__ tile, const u
             break;  // padding after the last instruction
         }
     }
-    return stored;
 }
 
 // One pass of the tiled sweep.  blockDim.x == 2^(m-4) <= 256; each thread
@@ -466,12 +442,6 @@ __global__ void __launch_bounds__(MAXT, MINB)
     for (uint32_t i = tid; i < nwords / 4; i += blockDim.x)
         reinterpret_cast<uint4*>(sw)[i] = __ldg(reinterpret_cast<const uint4*>(words) + i);
     for (uint32_t i = tid; i < nsdata; i += blockDim.x) sd[i] = __ldg(sdata + i);
-    __shared__ IDX sbit[kMaxTileQubits];  // global index bit of each tile bit
-    if (tid == 0) {
-        uint32_t b = 0;
-        for (uint32_t p = 0; p < n && b < m; ++p)
-            if ((smask >> p) & 1u) sbit[b++] = IDX{1} << p;
-    }
     // Canonical (load/store) mapping: thread bits = tile bits 0..tbits-1,
     // register bits = tile bits tbits..m-1.
     IDX off_lo = 0, hib0 = 0, hib1 = 0, hib2 = 0, hib3 = 0;
@@ -542,13 +512,12 @@ __global__ void __launch_bounds__(MAXT, MINB)
         else cp_async_wait<1>();
         __syncthreads();
 
-        const bool stored = compute_tile<MT, FULL, IDX>(tile, sw, nwords, sd, nsdata, 0u, gdata, tid, m,
-                                                         [] { __syncthreads(); }, st, cbase, sbit);
-        if (!stored) {  // canonical mapping, -0.0 normalised
-            const IDX b0 = cbase + off_lo;
+        compute_tile<MT, FULL>(tile, sw, nwords, sd, nsdata, 0u, gdata, tid, m, [] { __syncthreads(); });
+
+        // Store: canonical mapping, -0.0 normalised.
+        const IDX b0 = cbase + off_lo;
 #pragma unroll
-            for (int j = 0; j < kNA; ++j) st[b0 + reg_off(j)] = canon(tile[slot(j)]);
-        }
+        for (int j = 0; j < kNA; ++j) st[b0 + reg_off(j)] = canon(tile[slot(j)]);
         cbase = advance(cbase);
         __syncthreads();  // the buffer is the target of a later prefetch
     }
