@@ -286,6 +286,26 @@ __global__ void __launch_bounds__(MAXT, MINB)
                         MB2_CASE4(cop::kReal1, (g1<P>(a, md)))
                         MB2_CASE4(cop::kMono1, (g1<P>(a, md)))
                         MB2_CASE4(cop::kX1, (perm1<P>(a)))
+                        case cop::kU3Run0123:
+                            g1<0>(a, md);
+                            g1<1>(a, md + 8);
+                            g1<2>(a, md + 16);
+                            g1<3>(a, md + 24);
+                            break;
+                        case cop::kU3Run01:
+                            g1<0>(a, md);
+                            g1<1>(a, md + 8);
+                            break;
+                        case cop::kU3Run123:
+                            g1<1>(a, md);
+                            g1<2>(a, md + 8);
+                            g1<3>(a, md + 16);
+                            break;
+                        case cop::kU3Run012:
+                            g1<0>(a, md);
+                            g1<1>(a, md + 8);
+                            g1<2>(a, md + 16);
+                            break;
                         MB2_CASE12(cop::kGen2, (g2<P0, P1>(a, md)))
                         MB2_CASE12(cop::kMono2, (++pc, g2<P0, P1>(a, md)))
                         MB2_CASE12(cop::kSw12, (perm2<P0, P1, TK_SW12>(a)))

@@ -129,6 +129,12 @@ constexpr uint32_t kDs2RT = 98;  // + 2 * slot + (index of the thread-bit operan
 constexpr uint32_t kDs2TT = 106; // aux = classes; extra word = the two tile bits (4 bits each)
 constexpr uint32_t kDiagK = 107; // aux = k; extra word = tile positions (4 bits each)
 constexpr uint32_t kSigns = 108; // aux = monomial count; one word per monomial
+// Runs of U3 blocks on consecutive register slots, their matrices
+// consecutive in the staged data (one jump for the run).
+constexpr uint32_t kU3Run0123 = 109;
+constexpr uint32_t kU3Run01 = 110;
+constexpr uint32_t kU3Run123 = 111;
+constexpr uint32_t kU3Run012 = 112;
 constexpr uint32_t kPhase = 200; // aux = thread bits; bits 16-31 register positions; 2 words of tperm
 constexpr uint32_t kSmem = 201;  // aux = k; extra words: tile positions, gdata offset (doubles)
 // A sign monomial: six 5-bit sources, 31 = none, 16 + s = register slot s,

@@ -39,6 +39,48 @@ uint32_t param_doubles(const TileInstr& g) {
     return g.op == TOP_DIAG ? 2 * dim : 2 * dim * dim;
 }
 
+// Rewrites runs of U3 words on slots 0-1-2-3, 0-1, 1-2-3 or 0-1-2 whose
+// matrices are consecutive (8 doubles apart) into one run word, in the
+// words from `begin` on.
+void fuse_u3_runs(std::vector<uint32_t>& w, size_t begin) {
+    std::vector<uint32_t> out(w.begin(), w.begin() + static_cast<long>(begin));
+    size_t i = begin;
+    auto is_u3 = [&](size_t k, uint32_t slot) { return k < w.size() && (w[k] & 0xffu) == cop::kU3 + slot; };
+    auto off = [&](size_t k) { return w[k] >> 20; };
+    auto chain = [&](size_t k, uint32_t first, uint32_t len) {
+        for (uint32_t t = 0; t < len; ++t) {
+            if (!is_u3(k + t, first + t)) return false;
+            if (t > 0 && off(k + t) != off(k) + 4 * t) return false;
+        }
+        return true;
+    };
+    while (i < w.size()) {
+        const uint32_t op = w[i] & 0xffu;
+        // Skip over multi-word instructions unchanged.
+        uint32_t len = 1;
+        if (op == cop::kPhase || op == cop::kSmem) len = 3;
+        else if ((op >= cop::kMono2 && op < cop::kSw12) || op == cop::kDs2TT || op == cop::kDiagK) len = 2;
+        else if (op == cop::kSigns) len = 1 + ((w[i] >> 8) & 0xffu);
+        if (op == cop::kU3 && chain(i, 0, 4)) {
+            out.push_back((w[i] & ~0xffu) | cop::kU3Run0123);
+            i += 4;
+        } else if (op == cop::kU3 && chain(i, 0, 3)) {
+            out.push_back((w[i] & ~0xffu) | cop::kU3Run012);
+            i += 3;
+        } else if (op == cop::kU3 && chain(i, 0, 2)) {
+            out.push_back((w[i] & ~0xffu) | cop::kU3Run01);
+            i += 2;
+        } else if (op == cop::kU3 + 1 && chain(i, 1, 3)) {
+            out.push_back((w[i] & ~0xffu) | cop::kU3Run123);
+            i += 3;
+        } else {
+            out.insert(out.end(), w.begin() + static_cast<long>(i), w.begin() + static_cast<long>(i + len));
+            i += len;
+        }
+    }
+    w.swap(out);
+}
+
 }  // namespace
 
 void encode_compact(TileProgram& prog) {
@@ -216,6 +258,7 @@ void encode_compact(TileProgram& prog) {
             }
         }
         flush_signs();
+        fuse_u3_runs(w, pass.word_begin);
         pass.heavy = heavy;
         while (w.size() & 3u) w.push_back(cop::kEnd);  // 16-byte multiple: the staged data follows
         pass.word_count = static_cast<uint32_t>(w.size()) - pass.word_begin;

@@ -308,6 +308,26 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
                     MB2_CASE12(cop::kSw12, if constexpr (FULL) perm2<P0, P1, TK_SW12>(a))
                     MB2_CASE12(cop::kSw13, if constexpr (FULL) perm2<P0, P1, TK_SW13>(a))
                     MB2_CASE12(cop::kSw23, if constexpr (FULL) perm2<P0, P1, TK_SW23>(a))
+                    case cop::kU3Run0123:
+                        g1<0, TK_U3>(a, md, 0u);
+                        g1<1, TK_U3>(a, md + 8, 0u);
+                        g1<2, TK_U3>(a, md + 16, 0u);
+                        g1<3, TK_U3>(a, md + 24, 0u);
+                        break;
+                    case cop::kU3Run01:
+                        g1<0, TK_U3>(a, md, 0u);
+                        g1<1, TK_U3>(a, md + 8, 0u);
+                        break;
+                    case cop::kU3Run123:
+                        g1<1, TK_U3>(a, md, 0u);
+                        g1<2, TK_U3>(a, md + 8, 0u);
+                        g1<3, TK_U3>(a, md + 16, 0u);
+                        break;
+                    case cop::kU3Run012:
+                        g1<0, TK_U3>(a, md, 0u);
+                        g1<1, TK_U3>(a, md + 8, 0u);
+                        g1<2, TK_U3>(a, md + 16, 0u);
+                        break;
                     MB2_CASE4(cop::kDs1R, (diag_rr<P, -1>(a, load_diag(md, 1, aux))))
                     MB2_CASE12(cop::kDs2RR, (diag_rr<P0, P1>(a, load_diag(md, 2, aux))))
 #undef MB2_CASE4
