@@ -399,7 +399,7 @@ def main_serve(args, local):
 
     def serve(arrive):
         srv = Server(ctx, budget_bytes=160 * 10**9)
-        done, results = {}, {}
+        done, results, failed = {}, {}, {}
         tickets = {}
         t0 = time.perf_counter()
         i = 0
@@ -419,19 +419,23 @@ def main_serve(args, local):
             for c in srv.poll(timeout_ms=1):
                 k = tickets[c["ticket"]]
                 done[k] = c["latency_s"]
+                if c["status"] != 0:
+                    failed[k] = c["status"]
                 results[k] = c["counts"] if reqs[k]["output"] == "counts" else c["value"]
         total = time.perf_counter() - t0
         srv.close()
-        return done, results, total
+        return done, results, total, failed
 
-    burst_done, burst_res, burst_total = serve(None)
-    live_done, live_res, live_total = serve(arrivals)
+    burst_done, burst_res, burst_total, burst_failed = serve(None)
+    live_done, live_res, live_total, live_failed = serve(arrivals)
     # Each result the same in the burst and in the live mix; against the
     # complex128 plain loop: identical counts and <H> (complex128), or <H>
     # within the precision path's error (complex64; counts then follow the
     # complex64 probabilities).
     worst_exp, counts_same, mix_same = 0.0, True, True
     for k, r in enumerate(reqs):
+        if k in burst_failed or k in live_failed:
+            continue
         mix_same = mix_same and (burst_res[k] == live_res[k])
         if r["output"] == "counts":
             counts_same = counts_same and (burst_res[k] == plain_out[k])
@@ -449,6 +453,8 @@ def main_serve(args, local):
                  "p50_ms": round(1e3 * percentile(live_lat, 50), 2), "p99_ms": round(1e3 * percentile(live_lat, 99), 2),
                  "plain_fifo_p50_ms": round(1e3 * percentile(plain_lat, 50), 2),
                  "plain_fifo_p99_ms": round(1e3 * percentile(plain_lat, 99), 2)},
+        "failed_requests": {"burst": len(burst_failed), "live": len(live_failed),
+                            "statuses": sorted(set(burst_failed.values()) | set(live_failed.values()))},
         "results": {"burst_equals_live": mix_same, "counts_identical_to_plain_c128": counts_same,
                     "max_abs_dH_vs_plain_c128": worst_exp},
         "precision": args.precision,

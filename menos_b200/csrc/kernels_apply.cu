@@ -208,11 +208,11 @@ int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, 
     for (uint32_t j = 0; j < k; ++j) qq[j] = q[j];
     const uint32_t dim = 1u << k;
     const size_t smem = (size_t{dim} * dim + kGenBatch) * sizeof(double2);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_apply_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        attr_set = true;
-    }
+    static const bool attr_set = [] {  // once, thread-safe
+        return cudaFuncSetAttribute(k_apply_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024) ==
+               cudaSuccess;
+    }();
+    if (!attr_set) return launch_status();
     const uint64_t ngroups = (uint64_t{1} << n) >> k;
     const uint64_t nb = (ngroups + (kGenBatch >> k) - 1) / (kGenBatch >> k);
     const int grid = static_cast<int>(nb < 148ull * 4 ? nb : 148ull * 4);

@@ -159,13 +159,14 @@ int launch_batch_expect(const void* amps, uint32_t n, uint64_t bindings, const u
                         void* stream, int precision) {
     if (n < 3 || n > 16 || num_terms > kMaxBatchTerms) return MB2_ERR_INVALID;
     const size_t smem = (size_t{1} << (n - 3)) * sizeof(double2);
-    static bool attr = false;
-    if (!attr) {
+    static const bool attr = [] {  // once, thread-safe
         const int most = static_cast<int>((size_t{1} << 13) * sizeof(double2));
-        cudaFuncSetAttribute(k_batch_expect<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
-        cudaFuncSetAttribute(k_batch_expect<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
-        attr = true;
-    }
+        return cudaFuncSetAttribute(k_batch_expect<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, most) ==
+                   cudaSuccess &&
+               cudaFuncSetAttribute(k_batch_expect<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, most) ==
+                   cudaSuccess;
+    }();
+    if (!attr) return launch_status();
     const unsigned grid = static_cast<unsigned>(bindings * kCluster);
     const auto s = static_cast<cudaStream_t>(stream);
     if (precision == MB2_C64)

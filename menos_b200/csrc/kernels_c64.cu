@@ -147,7 +147,9 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // `stages - 1` ahead in flight, masked-add tile bases, the pass's words and
 // data staged in shared memory, a batch's parametric slice per tile) with
 // FP32 gates.  MT > 0 fixes the tile width; IDX is the index type.
-template <int MAXT, int MINB, int MT, typename IDX>
+// FULL = false: the lean variant without register-moving and rare heavy
+// instructions (as the complex128 kernel's), for passes without them.
+template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_tile_pass_c64(float2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask,
                     const uint32_t* __restrict__ words, uint32_t nwords, const double* __restrict__ sdata,
@@ -262,30 +264,30 @@ __global__ void __launch_bounds__(MAXT, MINB)
                     const double* md = sd + ((w >> 20) << 1);
                     const uint32_t tv = (tb >> ((w >> 16) & 15u)) & 1u;
                     switch (op) {
-#define MB2_CASE4(BASE, STMT) \
-    case BASE + 0: { constexpr int P = 0; STMT; } break; \
-    case BASE + 1: { constexpr int P = 1; STMT; } break; \
-    case BASE + 2: { constexpr int P = 2; STMT; } break; \
-    case BASE + 3: { constexpr int P = 3; STMT; } break;
-#define MB2_CASE12(BASE, STMT) \
-    case BASE + 0: { constexpr int P0 = 0, P1 = 1; STMT; } break; \
-    case BASE + 1: { constexpr int P0 = 0, P1 = 2; STMT; } break; \
-    case BASE + 2: { constexpr int P0 = 0, P1 = 3; STMT; } break; \
-    case BASE + 3: { constexpr int P0 = 1, P1 = 0; STMT; } break; \
-    case BASE + 4: { constexpr int P0 = 1, P1 = 2; STMT; } break; \
-    case BASE + 5: { constexpr int P0 = 1, P1 = 3; STMT; } break; \
-    case BASE + 6: { constexpr int P0 = 2, P1 = 0; STMT; } break; \
-    case BASE + 7: { constexpr int P0 = 2, P1 = 1; STMT; } break; \
-    case BASE + 8: { constexpr int P0 = 2, P1 = 3; STMT; } break; \
-    case BASE + 9: { constexpr int P0 = 3, P1 = 0; STMT; } break; \
-    case BASE + 10: { constexpr int P0 = 3, P1 = 1; STMT; } break; \
-    case BASE + 11: { constexpr int P0 = 3, P1 = 2; STMT; } break;
+#define MB2_CASE4(BASE, ...) \
+    case BASE + 0: { constexpr int P = 0; __VA_ARGS__; } break; \
+    case BASE + 1: { constexpr int P = 1; __VA_ARGS__; } break; \
+    case BASE + 2: { constexpr int P = 2; __VA_ARGS__; } break; \
+    case BASE + 3: { constexpr int P = 3; __VA_ARGS__; } break;
+#define MB2_CASE12(BASE, ...) \
+    case BASE + 0: { constexpr int P0 = 0, P1 = 1; __VA_ARGS__; } break; \
+    case BASE + 1: { constexpr int P0 = 0, P1 = 2; __VA_ARGS__; } break; \
+    case BASE + 2: { constexpr int P0 = 0, P1 = 3; __VA_ARGS__; } break; \
+    case BASE + 3: { constexpr int P0 = 1, P1 = 0; __VA_ARGS__; } break; \
+    case BASE + 4: { constexpr int P0 = 1, P1 = 2; __VA_ARGS__; } break; \
+    case BASE + 5: { constexpr int P0 = 1, P1 = 3; __VA_ARGS__; } break; \
+    case BASE + 6: { constexpr int P0 = 2, P1 = 0; __VA_ARGS__; } break; \
+    case BASE + 7: { constexpr int P0 = 2, P1 = 1; __VA_ARGS__; } break; \
+    case BASE + 8: { constexpr int P0 = 2, P1 = 3; __VA_ARGS__; } break; \
+    case BASE + 9: { constexpr int P0 = 3, P1 = 0; __VA_ARGS__; } break; \
+    case BASE + 10: { constexpr int P0 = 3, P1 = 1; __VA_ARGS__; } break; \
+    case BASE + 11: { constexpr int P0 = 3, P1 = 2; __VA_ARGS__; } break;
                         // Every dense 1q kind is the general 2x2 in FP32.
                         MB2_CASE4(cop::kU3, (g1<P>(a, md)))
                         MB2_CASE4(cop::kGen1, (g1<P>(a, md)))
                         MB2_CASE4(cop::kReal1, (g1<P>(a, md)))
                         MB2_CASE4(cop::kMono1, (g1<P>(a, md)))
-                        MB2_CASE4(cop::kX1, (perm1<P>(a)))
+                        MB2_CASE4(cop::kX1, if constexpr (FULL) perm1<P>(a))
                         case cop::kU3Run0123:
                             g1<0>(a, md);
                             g1<1>(a, md + 8);
@@ -306,11 +308,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
                             g1<1>(a, md + 8);
                             g1<2>(a, md + 16);
                             break;
-                        MB2_CASE12(cop::kGen2, (g2<P0, P1>(a, md)))
-                        MB2_CASE12(cop::kMono2, (++pc, g2<P0, P1>(a, md)))
-                        MB2_CASE12(cop::kSw12, (perm2<P0, P1, TK_SW12>(a)))
-                        MB2_CASE12(cop::kSw13, (perm2<P0, P1, TK_SW13>(a)))
-                        MB2_CASE12(cop::kSw23, (perm2<P0, P1, TK_SW23>(a)))
+                        MB2_CASE12(cop::kGen2, if constexpr (FULL) g2<P0, P1>(a, md))
+                        MB2_CASE12(cop::kMono2, if constexpr (FULL) { ++pc; g2<P0, P1>(a, md); })
+                        MB2_CASE12(cop::kSw12, if constexpr (FULL) perm2<P0, P1, TK_SW12>(a))
+                        MB2_CASE12(cop::kSw13, if constexpr (FULL) perm2<P0, P1, TK_SW13>(a))
+                        MB2_CASE12(cop::kSw23, if constexpr (FULL) perm2<P0, P1, TK_SW23>(a))
                         MB2_CASE4(cop::kDs1R, (diag_regs<P, -1>(a, md, 1, aux, 0u, 0u)))
                         MB2_CASE12(cop::kDs2RR, (diag_regs<P0, P1>(a, md, 2, aux, 0u, 0u)))
 #undef MB2_CASE4
@@ -350,6 +352,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
                             for (int j = 0; j < kNA; ++j) a[j] = fneg_if(a[j], (M >> j) & 1u);
                         } break;
                         default: {  // cop::kDiagK: entry per amplitude
+                            if constexpr (!FULL) break;
                             const uint32_t pos = sw[pc++];
                             uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
                             for (uint32_t b = 0; b < aux; ++b) {
@@ -372,7 +375,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
                 __syncthreads();
-            } else if (op0 == cop::kSmem) {
+            } else if (FULL && op0 == cop::kSmem) {
                 const uint32_t k = (w0 >> 8) & 0xffu, dim = 1u << k;
                 const uint32_t pos = sw[pc + 1];
                 const double* md = gdata + sw[pc + 2];
@@ -411,19 +414,24 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
 }
 
-template <int MAXT, int MINB, int MT, typename IDX>
+template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
 int launch_c64_instance(const TileLaunch& L) {
-    static size_t dyn_max = 0;
-    if (dyn_max == 0) {
+    // The dynamic limit is what the static shared memory leaves of the
+    // per-block maximum; it is raised once, by whichever thread launches
+    // first (the serving loop's workers launch concurrently: the static's
+    // initialisation is thread-safe and every thread sees it complete).
+    static const size_t dyn_max = [] {
         cudaFuncAttributes fa{};
-        if (cudaFuncGetAttributes(&fa, k_tile_pass_c64<MAXT, MINB, MT, IDX>) != cudaSuccess) return launch_status();
-        dyn_max = kTileSmemMax - fa.sharedSizeBytes;
-        if (cudaFuncSetAttribute(k_tile_pass_c64<MAXT, MINB, MT, IDX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(dyn_max)) != cudaSuccess)
-            return launch_status();
-    }
+        if (cudaFuncGetAttributes(&fa, k_tile_pass_c64<MAXT, MINB, MT, IDX, FULL>) != cudaSuccess) return size_t{0};
+        const size_t v = kTileSmemMax - fa.sharedSizeBytes;
+        if (cudaFuncSetAttribute(k_tile_pass_c64<MAXT, MINB, MT, IDX, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(v)) != cudaSuccess)
+            return size_t{0};
+        return v;
+    }();
+    if (dyn_max == 0) return launch_status();
     if (L.smem > dyn_max) return MB2_ERR_INVALID;
-    k_tile_pass_c64<MAXT, MINB, MT, IDX><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
+    k_tile_pass_c64<MAXT, MINB, MT, IDX, FULL><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
         static_cast<float2*>(L.amps), L.n_all, L.m, L.smask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata, L.ntiles,
         L.pdata, L.pstride, L.param_lo, L.param_len, L.bshift, L.stages);
     return launch_status();
@@ -475,10 +483,14 @@ int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uin
     const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m == kMaxTileQubitsC64 ? 1u : 2u);
     L.grid = static_cast<int>(L.ntiles < cap ? L.ntiles : cap);
     int rc;
-    if (pass.m == kMaxTileQubitsC64)
-        rc = L.n_all <= 32 ? launch_c64_instance<512, 1, 13, uint32_t>(L) : launch_c64_instance<512, 1, 13, uint64_t>(L);
+    if (pass.m == kMaxTileQubitsC64 && !pass.heavy)
+        rc = L.n_all <= 32 ? launch_c64_instance<512, 1, 13, uint32_t, false>(L)
+                           : launch_c64_instance<512, 1, 13, uint64_t, false>(L);
+    else if (pass.m == kMaxTileQubitsC64)
+        rc = L.n_all <= 32 ? launch_c64_instance<512, 1, 13, uint32_t, true>(L)
+                           : launch_c64_instance<512, 1, 13, uint64_t, true>(L);
     else
-        rc = launch_c64_instance<512, 1, 0, uint64_t>(L);
+        rc = launch_c64_instance<512, 1, 0, uint64_t, true>(L);
     note_launches(1);
     return rc;
 }

@@ -311,12 +311,13 @@ int launch_pauli_group(const void* amps, uint32_t n, uint32_t c, uint32_t d, con
     // two pairs) per step, so a tile holds at least 4 * kThreads of them.
     if (c + d < kPauliMinTileQubits) return MB2_ERR_INVALID;
     const size_t smem = 2 * (size_t{1} << (c + d)) * (precision == MB2_C64 ? sizeof(float2) : sizeof(double2));
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_pauli_group<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
-        cudaFuncSetAttribute(k_pauli_group<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
-        attr = true;
-    }
+    static const bool attr = [] {  // once, thread-safe (concurrent callers wait for it)
+        return cudaFuncSetAttribute(k_pauli_group<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    128 * 1024) == cudaSuccess &&
+               cudaFuncSetAttribute(k_pauli_group<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    128 * 1024) == cudaSuccess;
+    }();
+    if (!attr) return launch_status();
     const auto* terms = static_cast<const GroupTerm*>(dev_terms);
     if (precision == MB2_C64)
         k_pauli_group<float2><<<grid, kThreads, smem, s>>>(static_cast<const float2*>(amps), c, d, dev_span,

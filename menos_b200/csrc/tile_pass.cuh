@@ -547,16 +547,19 @@ __global__ void __launch_bounds__(MAXT, MINB)
 template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
 int launch_instance(const TileLaunch& L) {
     // The dynamic limit is what the static shared memory leaves of the
-    // per-block maximum (a larger request is refused by the driver).
-    static size_t dyn_max = 0;
-    if (dyn_max == 0) {
+    // per-block maximum; it is raised once, by whichever thread launches
+    // first (the serving loop's workers launch concurrently: the static's
+    // initialisation is thread-safe and every thread sees it complete).
+    static const size_t dyn_max = [] {
         cudaFuncAttributes fa{};
-        if (cudaFuncGetAttributes(&fa, k_tile_pass<MAXT, MINB, MT, IDX, FULL>) != cudaSuccess) return launch_status();
-        dyn_max = kTileSmemMax - fa.sharedSizeBytes;
+        if (cudaFuncGetAttributes(&fa, k_tile_pass<MAXT, MINB, MT, IDX, FULL>) != cudaSuccess) return size_t{0};
+        const size_t v = kTileSmemMax - fa.sharedSizeBytes;
         if (cudaFuncSetAttribute(k_tile_pass<MAXT, MINB, MT, IDX, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(dyn_max)) != cudaSuccess)
-            return launch_status();
-    }
+                                 static_cast<int>(v)) != cudaSuccess)
+            return size_t{0};
+        return v;
+    }();
+    if (dyn_max == 0) return launch_status();
     if (L.smem > dyn_max) return MB2_ERR_INVALID;
     k_tile_pass<MAXT, MINB, MT, IDX, FULL><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
         static_cast<double2*>(L.amps), L.n_all, L.m, L.smask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata,

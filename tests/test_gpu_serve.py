@@ -102,3 +102,37 @@ def test_complex64_requests_same_alone_and_in_the_mix(ctx):
             terms = st.expectation(r["paulis"])
             assert c["value"] == sum(w * v.real for w, v in zip(r["coefs"], terms))
             assert abs(c["value"] - alone(ctx, r)) <= 1e-6
+
+
+def test_first_launches_concurrent_in_a_fresh_process():
+    # The kernels' one-time set-up (raising their shared-memory limits) must
+    # hold when the first launches of a process come from several serving
+    # workers at once: run a burst as the first GPU work of a new process.
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = r'''
+import sys
+sys.path.insert(0, sys.argv[1])
+from menos_b200 import Context, workloads
+from menos_b200._lib import C64, C128
+from menos_b200.serve import Server
+ctx = Context(0)
+bad = 0
+for prec in (C64, C128):
+    srv = Server(ctx, slots=16)
+    reqs = workloads.serving_stream(32, 1000.0, 5, nmin=14, nmax=20, dmin=2, dmax=6, shots=512, terms=8)
+    for r in reqs:
+        srv.submit(r["circuit"], "expectation", paulis=r["paulis"], coefs=r["coefs"], precision=prec)
+    got = 0
+    while got < len(reqs):
+        for c in srv.poll(timeout_ms=200):
+            got += 1
+            bad += c["status"] != 0
+    srv.close()
+print("BAD", bad)
+'''
+    out = subprocess.run([sys.executable, "-c", code, root], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert "BAD 0" in out.stdout, out.stdout + out.stderr[-2000:]
