@@ -343,9 +343,10 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     const bool c64 = s->precision == MB2_C64;
     uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, s->n, blocks);
     if (c64) {
-        // 8-byte amplitudes: 13-qubit tiles fit the same shared memory.
+        // 8-byte amplitudes: up to 13-qubit tiles fit the same shared memory;
+        // 12 by default (two CTAs per SM).
         m = o.tile_qubits > 0 ? std::min<uint32_t>(static_cast<uint32_t>(o.tile_qubits), mb2::kMaxTileQubitsC64)
-                              : std::min<uint32_t>(mb2::kMaxTileQubitsC64, s->n);
+                              : std::min<uint32_t>(mb2::kDefaultTileQubitsC64, s->n);
         for (const mb2::Block& b : blocks) m = std::max(m, b.k);
         m = std::max(m, mb2::kMinTileQubits);
         if (s->n < mb2::kMinTileQubits) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "complex64 states need >= 4 qubits");

@@ -470,7 +470,8 @@ int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uin
     L.stream = stream;
     L.threads = 1u << (pass.m - kRegQubits);
     // 13-qubit tiles (64 KiB): one CTA per SM with three buffers; smaller
-    // tiles: two CTAs per SM with two buffers each.
+    // tiles (12 by default, its own instances): two CTAs per SM with two
+    // buffers each.
     L.stages = pass.m == kMaxTileQubitsC64 ? 3u : 2u;
     L.smem = L.stages * (size_t{1} << pass.m) * sizeof(float2) + size_t{pass.word_count} * 4 +
              (size_t{pass.sdata_count} + pass.param_len) * sizeof(double);
@@ -489,6 +490,12 @@ int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uin
     else if (pass.m == kMaxTileQubitsC64)
         rc = L.n_all <= 32 ? launch_c64_instance<512, 1, 13, uint32_t, true>(L)
                            : launch_c64_instance<512, 1, 13, uint64_t, true>(L);
+    else if (pass.m == 12 && !pass.heavy)
+        rc = L.n_all <= 32 ? launch_c64_instance<256, 2, 12, uint32_t, false>(L)
+                           : launch_c64_instance<256, 2, 12, uint64_t, false>(L);
+    else if (pass.m == 12)
+        rc = L.n_all <= 32 ? launch_c64_instance<256, 2, 12, uint32_t, true>(L)
+                           : launch_c64_instance<256, 2, 12, uint64_t, true>(L);
     else
         rc = launch_c64_instance<512, 1, 0, uint64_t, true>(L);
     note_launches(1);

@@ -254,6 +254,9 @@ int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorte
                   uint64_t* dev_basis, void* stream, int precision = MB2_C128);
 // complex64 precision path (kernels_c64.cu).
 constexpr uint32_t kMaxTileQubitsC64 = 13;
+// Default complex64 tile: 12 qubits, two CTAs per SM (measured faster per
+// circuit than 13-qubit tiles at one CTA per SM, despite more passes).
+constexpr uint32_t kDefaultTileQubitsC64 = 12;
 int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
                          const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
                          const BatchLayout* batch = nullptr);
