@@ -199,7 +199,7 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
         }
     }
     const uint32_t mmax = c64 ? mb2::kMaxTileQubitsC64 : mb2::kMaxTileQubits;
-    uint32_t m = o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : (c64 ? mb2::kDefaultTileQubitsC64 : 11u);
+    uint32_t m = o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : (c64 ? mb2::kMaxTileQubitsC64 : 11u);
     for (const auto& b : shape) m = std::max(m, b.k);
     m = std::min(std::max(m, mb2::kMinTileQubits), std::min(mmax, num_qubits));
     mb2::TileProgram prog;
