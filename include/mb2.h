@@ -305,6 +305,41 @@ int mb2_server_destroy(mb2_server* server);
  * CudaCalibration (src/plan/cuda_calibration.h:9-48). */
 int mb2_probe_rates(mb2_context* ctx, double* fp64_ops_per_s, double* copy_gbs);
 
+/* ---- autotuning and the calibrated time model --------------------------
+ * Measures, on the context's device, which tile width runs a synthetic
+ * brick sweep fastest (complex128: 10, 11, 12 qubits; complex64: 12, 13) at
+ * probe_qubits (0: 24; 16..30) and the costs of the time model, in which a
+ * pass takes  fixed + amplitudes * max(memory, sum of its blocks' compute):
+ * the fixed launch cost and the memory cost of an empty pass (the state read
+ * and written once, at probe_qubits and probe_qubits - 2), the compute of a
+ * dense single-qubit block (a dense k-qubit block counts 2^(k-1) of them) and
+ * of a diagonal block.  The widths become the context's defaults for
+ * sweeps with tile_qubits = 0; the costs feed mb2_estimate_sweep_time.
+ * Replaces the reference's device microbenchmarks feeding CudaCalibration
+ * (src/kernels/cuda/device_benchmarks.h:30-67, src/plan/cuda_calibration.h:9-48),
+ * extended to the tile width. */
+typedef struct mb2_tuning {
+    uint32_t tile_qubits;          /* complex128 */
+    uint32_t tile_qubits_c64;      /* complex64 */
+    double pass_s_fixed;           /* complex128: seconds per pass (launch) */
+    double pass_s_per_amp;         /* complex128 costs, seconds per amplitude */
+    double dense1_s_per_amp;
+    double diag_s_per_amp;
+    double pass_s_fixed_c64;       /* complex64 costs */
+    double pass_s_per_amp_c64;
+    double dense1_s_per_amp_c64;
+    double diag_s_per_amp_c64;
+    uint32_t probe_qubits;         /* 0: not measured (the built-in defaults) */
+    uint32_t reserved;
+} mb2_tuning;
+int mb2_autotune(mb2_context* ctx, uint32_t probe_qubits, mb2_tuning* out);
+int mb2_context_tuning(mb2_context* ctx, mb2_tuning* out);
+/* Seconds a sweep of these ops would take on this context's device: the
+ * tile program's passes and blocks weighted by the tuned costs (the planner's
+ * calibrated CUDA time model).  Plans only; runs nothing. */
+int mb2_estimate_sweep_time(mb2_context* ctx, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
+                            uint32_t num_qubits, int32_t precision, double* seconds);
+
 /* Kernels this library has launched since it was loaded, over all contexts
  * and states (probes excluded).  Read before and after a region to count its
  * device launches.  Has no counterpart in the reference. */

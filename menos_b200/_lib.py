@@ -65,6 +65,13 @@ class Completion(C.Structure):
 OUT_COUNTS, OUT_EXPECTATION = 1, 2
 
 
+class Tuning(C.Structure):
+    _fields_ = [("tile_qubits", C.c_uint32), ("tile_qubits_c64", C.c_uint32), ("pass_s_fixed", C.c_double),
+                ("pass_s_per_amp", C.c_double), ("dense1_s_per_amp", C.c_double), ("diag_s_per_amp", C.c_double),
+                ("pass_s_fixed_c64", C.c_double), ("pass_s_per_amp_c64", C.c_double), ("dense1_s_per_amp_c64", C.c_double),
+                ("diag_s_per_amp_c64", C.c_double), ("probe_qubits", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class SweepStats(C.Structure):
     _fields_ = [("blocks", C.c_uint64), ("passes", C.c_uint64), ("launches", C.c_uint64),
                 ("fp64_ops_per_amp", C.c_uint64)]
@@ -90,6 +97,10 @@ SIGNATURES = {
     "mb2_server_destroy": (C.c_int, [_VP]),
     "mb2_probe_rates": (C.c_int, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mb2_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),
+    "mb2_autotune": (C.c_int, [_VP, C.c_uint32, _VP]),
+    "mb2_context_tuning": (C.c_int, [_VP, _VP]),
+    "mb2_estimate_sweep_time": (C.c_int, [_VP, C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions), C.c_uint32,
+                                          C.c_int32, C.POINTER(C.c_double)]),
     "mb2_debug_pauli_groups": (C.c_int, [_VP, _VP, C.c_uint32, C.c_uint32, _VP, C.POINTER(C.c_uint64)]),
     "mb2_state_alloc": (C.c_int, [_VP, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(_VP)]),
     "mb2_state_free": (C.c_int, [_VP]),

@@ -28,6 +28,10 @@ struct mb2_context {
     int sm_count = 0;
     std::mutex mu;
     std::string last_error;
+    // Tile widths and time-model costs (mb2_autotune; built-in defaults
+    // measured on B200 until then).
+    std::atomic<uint32_t> tile_c128{0}, tile_c64{0};
+    mb2_tuning tuning{11, 12, 4e-6, 5.3e-12, 6.0e-13, 3.0e-13, 4e-6, 3.0e-12, 3.5e-13, 2.0e-13, 0, 0};
 };
 
 struct mb2_state {
@@ -341,12 +345,15 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     s->stats.blocks = blocks.size();
     if (blocks.empty()) return MB2_OK;
     const bool c64 = s->precision == MB2_C64;
-    uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, s->n, blocks);
+    uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : s->ctx->tile_c128.load(), s->n,
+                            blocks);
     if (c64) {
         // 8-byte amplitudes: up to 13-qubit tiles fit the same shared memory;
         // 12 by default (two CTAs per SM).
         m = o.tile_qubits > 0 ? std::min<uint32_t>(static_cast<uint32_t>(o.tile_qubits), mb2::kMaxTileQubitsC64)
-                              : std::min<uint32_t>(mb2::kDefaultTileQubitsC64, s->n);
+                              : std::min<uint32_t>(s->ctx->tile_c64.load() ? s->ctx->tile_c64.load()
+                                                                            : mb2::kDefaultTileQubitsC64,
+                                                   s->n);
         for (const mb2::Block& b : blocks) m = std::max(m, b.k);
         m = std::max(m, mb2::kMinTileQubits);
         if (s->n < mb2::kMinTileQubits) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "complex64 states need >= 4 qubits");
@@ -702,6 +709,207 @@ int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
     }
     *num_blocks = order.size();
     *matrix_len = mlen;
+    return MB2_OK;
+}
+
+// ---- autotuning -----------------------------------------------------------
+namespace {
+
+// Synthetic probe circuits (angles from a fixed LCG; their values do not
+// change the work).
+struct ProbeOps {
+    std::vector<mb2_op> ops;
+    uint64_t seed = 0x9E3779B97F4A7C15ull;
+    double angle() {
+        seed = seed * 6364136223846793005ull + 1442695040888963407ull;
+        return static_cast<double>(seed >> 11) * (6.283185307179586 / 9007199254740992.0);
+    }
+    void gate(int32_t opcode, std::initializer_list<uint32_t> qs, int np) {
+        mb2_op o{};
+        o.opcode = opcode;
+        o.num_qubits = static_cast<uint32_t>(qs.size());
+        uint32_t i = 0;
+        for (uint32_t q : qs) o.qubits[i++] = q;
+        for (int p = 0; p < np; ++p) o.params[p] = angle();
+        ops.push_back(o);
+    }
+};
+
+std::vector<mb2_op> probe_brick(uint32_t n, uint32_t layers) {
+    ProbeOps p;
+    for (uint32_t l = 0; l < layers; ++l) {
+        for (uint32_t q = 0; q < n; ++q) p.gate(MB2_U, {q}, 3);
+        for (uint32_t q = l % 2; q + 1 < n; q += 2) p.gate(MB2_CZ, {q, q + 1}, 0);
+    }
+    return p.ops;
+}
+
+int time_sweep(mb2_state* st, const std::vector<mb2_op>& ops, uint32_t tile, double* ms, int32_t fuse = 1) {
+    mb2_sweep_options o{fuse, 0, static_cast<int32_t>(tile), 0};
+    if (int e = mb2_init(st, 0.0); e != MB2_OK) return e;
+    if (int e = mb2_apply_program(st, ops.data(), static_cast<uint32_t>(ops.size()), &o); e != MB2_OK) return e;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return MB2_ERR_CUDA;
+    double best = 1e30;
+    int rc = MB2_OK;
+    for (int rep = 0; rep < 3 && rc == MB2_OK; ++rep) {
+        rc = mb2_init(st, 0.0);
+        if (rc != MB2_OK) break;
+        cudaEventRecord(a, st->stream);
+        rc = mb2_apply_program(st, ops.data(), static_cast<uint32_t>(ops.size()), &o);
+        cudaEventRecord(b, st->stream);
+        if (cudaEventSynchronize(b) != cudaSuccess) rc = MB2_ERR_CUDA;
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        best = std::min(best, static_cast<double>(t));
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = best;
+    return rc;
+}
+
+// The time model's costs at one precision and tile width.  A pass takes
+//   fixed + amps * max(memory, sum over its blocks of compute),
+// memory and the fixed launch cost from an empty pass at n and n - 2 qubits,
+// compute from passes of many unfused blocks (compute-bound by construction):
+// a dense one-qubit block and a two-qubit diagonal block.
+int measure_costs(mb2_state* st, mb2_state* small, uint32_t m, double* fixed, double* pass, double* dense1,
+                  double* diag) {
+    const uint32_t n = st->n;
+    ProbeOps e, es, u, d;
+    e.gate(MB2_Z, {n - 1}, 0);
+    es.gate(MB2_Z, {small->n - 1}, 0);
+    for (int rep = 0; rep < 3; ++rep)
+        for (uint32_t q = 0; q < m; ++q) u.gate(MB2_U, {q}, 3);
+    for (int rep = 0; rep < 6; ++rep)
+        for (uint32_t q = 0; q + 1 < m; ++q) d.gate(MB2_CP, {q, q + 1}, 1);
+    double te = 0, tes = 0, tu = 0, td = 0;
+    if (int rc = time_sweep(st, e.ops, m, &te); rc != MB2_OK) return rc;
+    if (int rc = time_sweep(small, es.ops, m, &tes); rc != MB2_OK) return rc;
+    if (int rc = time_sweep(st, u.ops, m, &tu, 0); rc != MB2_OK) return rc;
+    if (int rc = time_sweep(st, d.ops, m, &td, 0); rc != MB2_OK) return rc;
+    const double amps = static_cast<double>(uint64_t{1} << n);
+    const double f = std::max(0.0, (4.0 * tes - te) / 3.0) * 1e-3;  // te = f + A p, tes = f + A p / 4
+    *fixed = f;
+    *pass = std::max(0.0, te * 1e-3 - f) / amps;
+    *dense1 = std::max(0.0, tu * 1e-3 - f) / (amps * static_cast<double>(u.ops.size()));
+    *diag = std::max(0.0, td * 1e-3 - f) / (amps * static_cast<double>(d.ops.size()));
+    return MB2_OK;
+}
+
+// Seconds for one pass of blocks [b0, b1) over 2^n amplitudes.
+double pass_seconds(const mb2_tuning& t, bool c64, const std::vector<mb2::Block>& blocks, size_t b0, size_t b1,
+                    uint32_t n) {
+    const double mem = c64 ? t.pass_s_per_amp_c64 : t.pass_s_per_amp;
+    const double dense1 = c64 ? t.dense1_s_per_amp_c64 : t.dense1_s_per_amp;
+    const double diag = c64 ? t.diag_s_per_amp_c64 : t.diag_s_per_amp;
+    double compute = 0.0;
+    for (size_t i = b0; i < b1; ++i)  // a dense k-qubit block sums 2^k terms per amplitude
+        compute += blocks[i].diagonal ? diag : dense1 * static_cast<double>(uint64_t{1} << (blocks[i].k - 1));
+    return (c64 ? t.pass_s_fixed_c64 : t.pass_s_fixed) + std::max(mem, compute) * static_cast<double>(uint64_t{1} << n);
+}
+
+}  // namespace
+
+int mb2_autotune(mb2_context* ctx, uint32_t probe_qubits, mb2_tuning* out) {
+    if (ctx == nullptr) return MB2_ERR_INVALID;
+    const uint32_t n = probe_qubits == 0 ? 24u : probe_qubits;
+    if (n < 16 || n > 30) return fail(ctx, MB2_ERR_INVALID, "probe_qubits must be 16..30");
+    mb2_tuning t = ctx->tuning;
+    const std::vector<mb2_op> brick = probe_brick(n, 8);
+    for (int prec : {MB2_C128, MB2_C64}) {
+        mb2_state* st = nullptr;
+        mb2_state* small = nullptr;
+        if (int rc = mb2_state_alloc(ctx, n, prec, ~uint64_t{0}, &st); rc != MB2_OK) return rc;
+        if (int rc = mb2_state_alloc(ctx, n - 2, prec, ~uint64_t{0}, &small); rc != MB2_OK) {
+            mb2_state_free(st);
+            return rc;
+        }
+        const std::vector<uint32_t> widths = prec == MB2_C128 ? std::vector<uint32_t>{10, 11, 12}
+                                                              : std::vector<uint32_t>{12, 13};
+        uint32_t best_m = widths[0];
+        double best_ms = 1e30;
+        int rc = MB2_OK;
+        for (uint32_t m : widths) {
+            double ms = 0;
+            rc = time_sweep(st, brick, m, &ms);
+            if (rc != MB2_OK) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_m = m;
+            }
+        }
+        if (rc == MB2_OK) {
+            if (prec == MB2_C128) {
+                t.tile_qubits = best_m;
+                rc = measure_costs(st, small, best_m, &t.pass_s_fixed, &t.pass_s_per_amp, &t.dense1_s_per_amp,
+                                   &t.diag_s_per_amp);
+            } else {
+                t.tile_qubits_c64 = best_m;
+                rc = measure_costs(st, small, best_m, &t.pass_s_fixed_c64, &t.pass_s_per_amp_c64,
+                                   &t.dense1_s_per_amp_c64, &t.diag_s_per_amp_c64);
+            }
+        }
+        mb2_state_free(small);
+        mb2_state_free(st);
+        if (rc != MB2_OK) return rc;
+    }
+    t.probe_qubits = n;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        ctx->tuning = t;
+    }
+    ctx->tile_c128.store(t.tile_qubits);
+    ctx->tile_c64.store(t.tile_qubits_c64);
+    if (out != nullptr) *out = t;
+    return MB2_OK;
+}
+
+int mb2_context_tuning(mb2_context* ctx, mb2_tuning* out) {
+    if (ctx == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    *out = ctx->tuning;
+    return MB2_OK;
+}
+
+int mb2_estimate_sweep_time(mb2_context* ctx, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
+                            uint32_t num_qubits, int32_t precision, double* seconds) {
+    if (ctx == nullptr || seconds == nullptr || (ops == nullptr && num_ops != 0) || num_qubits < 1 ||
+        num_qubits > 40 || (precision != MB2_C128 && precision != MB2_C64))
+        return MB2_ERR_INVALID;
+    mb2_sweep_options o{1, 0, 0, 0};
+    if (opts != nullptr) o = *opts;
+    mb2_tuning t;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        t = ctx->tuning;
+    }
+    const bool c64 = precision == MB2_C64;
+    try {
+        const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+        double total = 0.0;
+        if (o.per_gate != 0 || num_qubits < mb2::kMinTileQubits || blocks.empty()) {
+            for (size_t i = 0; i < blocks.size(); ++i) total += pass_seconds(t, c64, blocks, i, i + 1, num_qubits);
+        } else {
+            const uint32_t req = o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits)
+                                                   : (c64 ? t.tile_qubits_c64 : t.tile_qubits);
+            uint32_t m = c64 ? std::min<uint32_t>(std::max<uint32_t>(req, mb2::kMinTileQubits), mb2::kMaxTileQubitsC64)
+                             : tile_width(req, num_qubits, blocks);
+            for (const mb2::Block& b : blocks) m = std::max(m, b.k);
+            m = std::min(m, num_qubits);
+            // A pass applies the next `gates` blocks in order (blocks are never reordered).
+            size_t b0 = 0;
+            for (const mb2::TilePass& p : mb2::plan_tile_program(blocks, num_qubits, m).passes) {
+                const size_t b1 = std::min(blocks.size(), b0 + p.gates);
+                total += pass_seconds(t, c64, blocks, b0, b1, num_qubits);
+                b0 = b1;
+            }
+        }
+        *seconds = total;
+    } catch (const std::exception& e) {
+        return fail(ctx, MB2_ERR_INVALID, e.what());
+    }
     return MB2_OK;
 }
 

@@ -87,6 +87,29 @@ class Context:
         check(lib().mb2_probe_rates(self.h, C.byref(f), C.byref(c)), self.h, "probe_rates")
         return f.value, c.value
 
+    def autotune(self, probe_qubits: int = 0) -> dict:
+        """Measures the best tile widths and the time model's costs on this
+        device (mb2_autotune); they become this context's defaults."""
+        t = _lib.Tuning()
+        check(lib().mb2_autotune(self.h, probe_qubits, C.byref(t)), self.h, "mb2_autotune")
+        return {f: getattr(t, f) for f, _ in t._fields_ if f != "reserved"}
+
+    def tuning(self) -> dict:
+        t = _lib.Tuning()
+        check(lib().mb2_context_tuning(self.h, C.byref(t)), self.h, "mb2_context_tuning")
+        return {f: getattr(t, f) for f, _ in t._fields_ if f != "reserved"}
+
+    def estimate_time(self, circ: Circuit, precision: int = C128, fuse_gates: bool = True,
+                      tile_qubits: int = 0) -> float:
+        """Seconds the sweep of circ would take here, from the tuned time model."""
+        arr, keep = to_mb2_ops(circ)
+        opts = SweepOptions(1 if fuse_gates else 0, 0, tile_qubits, 0)
+        sec = C.c_double()
+        check(lib().mb2_estimate_sweep_time(self.h, arr, len(circ.ops), C.byref(opts), circ.num_qubits, precision,
+                                            C.byref(sec)), self.h, "mb2_estimate_sweep_time")
+        del keep
+        return sec.value
+
     def info(self):
         sm, tot, fr = C.c_int(), C.c_uint64(), C.c_uint64()
         check(lib().mb2_device_info(self.h, C.byref(sm), C.byref(tot), C.byref(fr)), self.h, "device_info")

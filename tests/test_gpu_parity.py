@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from menos_b200 import B200DenseEngine, DeviceState, EngineExecutionRequest, PauliTerm, workloads
+from menos_b200.engine import C64 as MB2_C64, C128 as MB2_C128
 from menos_b200._lib import MB2Error, ResourceExceeded
 from menos_b200.circuit import OP, Circuit
 from test_host import as_oracle_circuit
@@ -253,3 +254,35 @@ def test_large_state_tiled_equals_per_gate(ctx):
     xa, xb = a.copy_out(), b.copy_out()
     assert bits_equal(xa, xb)
     assert abs(a.norm() - 1.0) < 1e-10
+
+
+def test_autotune_and_time_model(ctx):
+    # The autotuner picks widths it measured and feeds a time model that
+    # predicts a brick sweep within a factor of two; the tuned widths stay
+    # bitwise (the plain path does not depend on the tile width).
+    t = ctx.autotune()
+    assert t["tile_qubits"] in (10, 11, 12) and t["tile_qubits_c64"] in (12, 13)
+    assert t["probe_qubits"] == 24 and t["pass_s_per_amp"] > 0 and t["dense1_s_per_amp"] > 0
+    assert ctx.tuning()["tile_qubits"] == t["tile_qubits"]
+    import time
+    n = 26
+    for c, precision in ((workloads.brick(n, 20, 3), MB2_C128), (workloads.qft(n), MB2_C128),
+                         (workloads.brick(n, 20, 3), MB2_C64)):
+        st = DeviceState(ctx, n, precision=precision)
+        st.init(0.0)
+        st.apply_program(c)
+        st.synchronize()
+        t0 = time.perf_counter()
+        st.apply_program(c)
+        st.synchronize()
+        measured = time.perf_counter() - t0
+        est = ctx.estimate_time(c, precision=precision)
+        assert 0.5 * measured <= est <= 2.0 * measured, (est, measured, precision)
+    small = workloads.brick(14, 6, 4)
+    a = DeviceState(ctx, 14)
+    a.init(0.0)
+    a.apply_program(small)
+    b = DeviceState(ctx, 14)
+    b.init(0.0)
+    b.apply_program(small, tile_qubits=11)
+    assert bits_equal(a.copy_out(), b.copy_out())
