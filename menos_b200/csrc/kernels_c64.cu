@@ -23,11 +23,7 @@ constexpr int kR = static_cast<int>(kRegQubits);
 constexpr int kNA = 1 << kR;
 static_assert(kR == 4, "written for 4 register qubits");
 
-// 8-byte slots: the low four bits XOR-folded with every higher 4-bit group
-// (XOR-linear, so slot addresses compose by XOR).
-__host__ __device__ __forceinline__ constexpr uint32_t swz8(uint32_t l) {
-    return l ^ (((l >> 4) ^ (l >> 8) ^ (l >> 12)) & 15u);
-}
+// Tile slots are swizzled by swz8 (mb2_internal.h).
 
 struct Cf {
     float r, i;
@@ -233,29 +229,24 @@ __global__ void __launch_bounds__(MAXT, MINB)
             const uint32_t w0 = sw[pc];
             const uint32_t op0 = w0 & 0xffu;
             if (op0 == cop::kPhase) {
-                const uint32_t tp0 = sw[pc + 1], tp1 = sw[pc + 2];
-                pc += 3;
-                const uint32_t nthread = (w0 >> 8) & 0xffu;
-                auto tperm = [&](uint32_t i) -> uint32_t {
-                    return (i < 8 ? (tp0 >> (4 * i)) : (tp1 >> (4 * (i - 8)))) & 15u;
-                };
-                uint32_t tb = 0;
-                if (MT > 0) {
-#pragma unroll
-                    for (uint32_t i = 0; i < (MT > 0 ? MT - kRegQubits : 1u); ++i)
-                        if (i < nthread) tb |= ((tid >> i) & 1u) << tperm(i);
-                } else {
-                    for (uint32_t i = 0; i < nthread; ++i) tb |= ((tid >> i) & 1u) << tperm(i);
-                }
+                // The phase record (cop::kPhase), 8-byte slot offsets.
+                const uint32_t* rec = sw + pc;
+                pc += cop::kPhaseWords;
+                const uint16_t* et = reinterpret_cast<const uint16_t*>(rec + 5);
+                uint32_t tb = static_cast<uint32_t>(et[tid & 15u]) | static_cast<uint32_t>(et[16 + ((tid >> 4) & 15u)]);
+                if (MT == 0 || MT > 12) tb |= static_cast<uint32_t>(et[32 + ((tid >> 8) & 15u)]);
                 uint32_t rb[kR];
 #pragma unroll
                 for (int b = 0; b < kR; ++b) rb[b] = 1u << ((w0 >> (16 + 4 * b)) & 15u);
-                const uint32_t z0 = swz8(tb), z1 = swz8(rb[0]), z2 = swz8(rb[1]), z3 = swz8(rb[2]), z4 = swz8(rb[3]);
-                auto adr = [&](int j) -> uint32_t {
-                    return z0 ^ ((j & 1) ? z1 : 0u) ^ ((j & 2) ? z2 : 0u) ^ ((j & 4) ? z3 : 0u) ^ ((j & 8) ? z4 : 0u);
+                const uint32_t z0 = swz8(tb) << 3, z1 = rec[3] & 0xffffu, z2 = rec[3] >> 16, z3 = rec[4] & 0xffffu,
+                               z4 = rec[4] >> 16;
+                char* const tile_b = reinterpret_cast<char*>(tile);
+                auto at = [&](int j) -> float2& {
+                    return *reinterpret_cast<float2*>(tile_b + (z0 ^ ((j & 1) ? z1 : 0u) ^ ((j & 2) ? z2 : 0u) ^
+                                                                 ((j & 4) ? z3 : 0u) ^ ((j & 8) ? z4 : 0u)));
                 };
 #pragma unroll
-                for (int j = 0; j < kNA; ++j) a[j] = tile[adr(j)];
+                for (int j = 0; j < kNA; ++j) a[j] = at(j);
                 for (;;) {
                     const uint32_t w = sw[pc++];
                     const uint32_t op = w & 0xffu;
@@ -373,7 +364,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
+                for (int j = 0; j < kNA; ++j) at(j) = a[j];
                 __syncthreads();
             } else if (FULL && op0 == cop::kSmem) {
                 const uint32_t k = (w0 >> 8) & 0xffu, dim = 1u << k;

@@ -9,9 +9,27 @@
 
 #include "../../include/mb2.h"
 
+#if defined(__CUDACC__)
+#define MB2_HD __host__ __device__
+#else
+#define MB2_HD
+#endif
+
 namespace mb2 {
 
 using Cd = std::complex<double>;
+
+// Shared-memory slot of tile-local index l in the tile kernels.
+// complex128 (16-byte slots): the low three bits XOR-folded with every
+// higher 3-bit group, so quarter-warps whose eight threads vary three tile
+// bits of distinct residue mod 3 hit eight distinct 16-byte bank groups.
+MB2_HD inline constexpr uint32_t swz(uint32_t l) {
+    const uint32_t h = l >> 3;
+    return l ^ ((h ^ (h >> 3) ^ (h >> 6) ^ (h >> 9)) & 7u);
+}
+// complex64 (8-byte slots): the low four bits XOR-folded with every higher
+// 4-bit group.  Both are linear over XOR, so slot addresses compose by XOR.
+MB2_HD inline constexpr uint32_t swz8(uint32_t l) { return l ^ (((l >> 4) ^ (l >> 8) ^ (l >> 12)) & 15u); }
 
 // ---- gate table (gate_table.cpp) -------------------------------------------
 int gate_num_qubits(int opcode);
@@ -135,7 +153,13 @@ constexpr uint32_t kU3Run0123 = 109;
 constexpr uint32_t kU3Run01 = 110;
 constexpr uint32_t kU3Run123 = 111;
 constexpr uint32_t kU3Run012 = 112;
-constexpr uint32_t kPhase = 200; // aux = thread bits; bits 16-31 register positions; 2 words of tperm
+// aux = thread bits; bits 16-31 register positions; then the phase record:
+// words 1-2 the byte offsets (16 bits each) of the four register bits' slots
+// with 16-byte slots, words 3-4 the same with 8-byte slots, words 5-28 a
+// table of 48 16-bit entries: entry 16 g + v is the tile bits that thread
+// index bits 4g..4g+3 equal to v stand for in this phase.
+constexpr uint32_t kPhase = 200;
+constexpr uint32_t kPhaseWords = 29;
 constexpr uint32_t kSmem = 201;  // aux = k; extra words: tile positions, gdata offset (doubles)
 // A sign monomial: six 5-bit sources, 31 = none, 16 + s = register slot s,
 // else a tile bit (a thread bit in that phase).  The amplitudes whose

@@ -58,7 +58,8 @@ void fuse_u3_runs(std::vector<uint32_t>& w, size_t begin) {
         const uint32_t op = w[i] & 0xffu;
         // Skip over multi-word instructions unchanged.
         uint32_t len = 1;
-        if (op == cop::kPhase || op == cop::kSmem) len = 3;
+        if (op == cop::kPhase) len = cop::kPhaseWords;
+        else if (op == cop::kSmem) len = 3;
         else if ((op >= cop::kMono2 && op < cop::kSw12) || op == cop::kDs2TT || op == cop::kDiagK) len = 2;
         else if (op == cop::kSigns) len = 1 + ((w[i] >> 8) & 0xffu);
         if (op == cop::kU3 && chain(i, 0, 4)) {
@@ -171,11 +172,26 @@ void encode_compact(TileProgram& prog) {
                         packed |= static_cast<uint32_t>(g.pos[s]) << (4 * s);
                     }
                     w.push_back(cop::kPhase | (static_cast<uint32_t>(g.nthread) << 8) | (packed << 16));
-                    uint32_t t0 = 0, t1 = 0;
-                    for (uint32_t t = 0; t < 8; ++t) t0 |= static_cast<uint32_t>(g.tperm[t] & 15u) << (4 * t);
-                    for (uint32_t t = 8; t < 12; ++t) t1 |= static_cast<uint32_t>(g.tperm[t] & 15u) << (4 * (t - 8));
-                    w.push_back(t0);
-                    w.push_back(t1);
+                    // Slot byte offsets of the register bits (16-byte slots:
+                    // tiles of at most 12 qubits; 8-byte slots: at most 13).
+                    uint32_t z16[kRegQubits], z8[kRegQubits];
+                    for (uint32_t s = 0; s < kRegQubits; ++s) {
+                        z16[s] = (swz(1u << g.pos[s]) << 4) & 0xffffu;
+                        z8[s] = (swz8(1u << g.pos[s]) << 3) & 0xffffu;
+                    }
+                    w.push_back(z16[0] | (z16[1] << 16));
+                    w.push_back(z16[2] | (z16[3] << 16));
+                    w.push_back(z8[0] | (z8[1] << 16));
+                    w.push_back(z8[2] | (z8[3] << 16));
+                    // Tile bits of each nibble of the thread index.
+                    uint32_t et[48] = {};
+                    for (uint32_t gi = 0; gi < 3; ++gi)
+                        for (uint32_t v = 0; v < 16; ++v)
+                            for (uint32_t t = 0; t < 4; ++t) {
+                                const uint32_t i = 4 * gi + t;
+                                if (i < g.nthread && ((v >> t) & 1u)) et[16 * gi + v] |= 1u << g.tperm[i];
+                            }
+                    for (uint32_t k = 0; k < 24; ++k) w.push_back(et[2 * k] | (et[2 * k + 1] << 16));
                     break;
                 }
                 case TOP_END:

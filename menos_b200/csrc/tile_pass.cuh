@@ -19,14 +19,7 @@ namespace tile {
 using namespace dev;
 
 // ---------------------------------------------------------------- tile pass
-// Shared-memory slot of tile-local index l: the low three bits XOR-folded
-// with every higher 3-bit group, so quarter-warps whose eight threads vary
-// three tile bits of distinct residue mod 3 hit eight distinct 16-byte bank
-// groups.
-__host__ __device__ __forceinline__ constexpr uint32_t swz(uint32_t l) {
-    const uint32_t h = l >> 3;
-    return l ^ ((h ^ (h >> 3) ^ (h >> 6) ^ (h >> 9)) & 7u);
-}
+// Tile slots are swizzled by swz (mb2_internal.h).
 
 constexpr int kR = static_cast<int>(kRegQubits);  // register qubits per thread
 constexpr int kNA = 1 << kR;                         // amplitudes per thread
@@ -247,30 +240,28 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
         const uint32_t w0 = sw[pc];
         const uint32_t op0 = w0 & 0xffu;
         if (op0 == cop::kPhase) {
-            const uint32_t tp0 = sw[pc + 1], tp1 = sw[pc + 2];
-            pc += 3;
-            const uint32_t nthread = (w0 >> 8) & 0xffu;
-            auto tperm = [&](uint32_t i) -> uint32_t { return (i < 8 ? (tp0 >> (4 * i)) : (tp1 >> (4 * (i - 8)))) & 15u; };
-            uint32_t tb = 0;
-            if (MT > 0) {
-#pragma unroll
-                for (uint32_t i = 0; i < (MT > 0 ? MT - kRegQubits : 1u); ++i)
-                    if (i < nthread) tb |= ((tid >> i) & 1u) << tperm(i);
-            } else {
-                for (uint32_t i = 0; i < nthread; ++i) tb |= ((tid >> i) & 1u) << tperm(i);
-            }
+            // The phase record (cop::kPhase): this thread's tile bits from
+            // the nibble table, the register bits' slot byte offsets as words.
+            const uint32_t* rec = sw + pc;
+            pc += cop::kPhaseWords;
+            const uint16_t* et = reinterpret_cast<const uint16_t*>(rec + 5);
+            uint32_t tb = static_cast<uint32_t>(et[tid & 15u]) | static_cast<uint32_t>(et[16 + ((tid >> 4) & 15u)]);
+            if (MT == 0 || MT > 12) tb |= static_cast<uint32_t>(et[32 + ((tid >> 8) & 15u)]);
             uint32_t rb[kR];
 #pragma unroll
             for (int b = 0; b < kR; ++b) rb[b] = 1u << ((w0 >> (16 + 4 * b)) & 15u);
-            // swz is linear over XOR, so slot j's address is swz(tb) XOR the
-            // swizzled register bits of j (recomputed for the write-back
+            // swz is linear over XOR, so slot j's byte offset is swz(tb)'s
+            // XOR the register bits' of j (recomputed for the write-back
             // rather than held in 16 registers through the gates).
-            const uint32_t z0 = swz(tb), z1 = swz(rb[0]), z2 = swz(rb[1]), z3 = swz(rb[2]), z4 = swz(rb[3]);
-            auto adr = [&](int j) -> uint32_t {
-                return z0 ^ ((j & 1) ? z1 : 0u) ^ ((j & 2) ? z2 : 0u) ^ ((j & 4) ? z3 : 0u) ^ ((j & 8) ? z4 : 0u);
+            const uint32_t z0 = swz(tb) << 4, z1 = rec[1] & 0xffffu, z2 = rec[1] >> 16, z3 = rec[2] & 0xffffu,
+                           z4 = rec[2] >> 16;
+            char* const tile_b = reinterpret_cast<char*>(tile);
+            auto at = [&](int j) -> double2& {
+                return *reinterpret_cast<double2*>(
+                    tile_b + (z0 ^ ((j & 1) ? z1 : 0u) ^ ((j & 2) ? z2 : 0u) ^ ((j & 4) ? z3 : 0u) ^ ((j & 8) ? z4 : 0u)));
             };
 #pragma unroll
-            for (int j = 0; j < kNA; ++j) a[j] = tile[adr(j)];
+            for (int j = 0; j < kNA; ++j) a[j] = at(j);
             for (;;) {
                 const uint32_t w = sw[pc++];
                 const uint32_t op = w & 0xffu;
@@ -393,7 +384,7 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
                 }
             }
 #pragma unroll
-            for (int j = 0; j < kNA; ++j) tile[adr(j)] = a[j];
+            for (int j = 0; j < kNA; ++j) at(j) = a[j];
             sync();
         } else if (FULL && op0 == cop::kSmem) {
             // A dense k-qubit block (k >= 3) on the whole tile in shared memory.

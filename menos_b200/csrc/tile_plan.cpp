@@ -25,15 +25,15 @@
 namespace mb2 {
 namespace {
 
-// A pass's instructions and small-matrix data are staged in shared memory
-// (kMaxStagedBytes); a block costs at most three records (phase, gate, end)
-// plus its staged entries.
+// A pass's instruction words and small-matrix data are staged in shared
+// memory (kMaxStagedBytes); a block costs at most a phase record, three
+// more words (gate, extra word, end) and its staged entries.
 constexpr size_t kMaxBlocksPerPass = 300;
 
 size_t staged_bytes(const Block& b) {
     const size_t dim = size_t{1} << b.k;
     const size_t entries = b.diagonal ? dim : (b.k <= 2 ? dim * dim : 0);
-    return 3 * sizeof(TileInstr) + entries * 2 * sizeof(double);
+    return (cop::kPhaseWords + 3) * sizeof(uint32_t) + entries * 2 * sizeof(double);
 }
 
 
