@@ -356,11 +356,13 @@ int mb2_gate_matrix(int32_t opcode, const double* params, double* out, uint32_t 
  * index, operand count, operands (6 slots) and matrix (2*4^k doubles,
  * appended to `matrices`).  *num_blocks in: capacity of pass/k/qubits,
  * out: blocks written; *matrix_len in: capacity of matrices (doubles), out:
- * doubles written.  Lets tests check the tiled schedule's reordering on the
- * CPU oracle.  Has no counterpart in the reference (its sweep is in op order). */
+ * doubles written.  precision: the state's (MB2_C64 schedules reorder
+ * commuting blocks into fewer passes; MB2_C128 keeps the plan order).  Lets
+ * tests check the tiled schedule on the CPU oracle.  Has no counterpart in
+ * the reference (its sweep is in op order). */
 int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
                        uint32_t num_qubits, uint32_t* pass, uint32_t* k, uint32_t* qubits,
-                       double* matrices, uint64_t* num_blocks, uint64_t* matrix_len);
+                       double* matrices, uint64_t* num_blocks, uint64_t* matrix_len, int32_t precision);
 
 /* The grouping mb2_expectation uses for these terms on a num_qubits state,
  * as 64-bit words: the group count, then per group c, d, free_mask, nterms,

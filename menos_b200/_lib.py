@@ -125,7 +125,7 @@ SIGNATURES = {
     "mb2_synchronize": (C.c_int, [_VP]),
     "mb2_gate_matrix": (C.c_int, [C.c_int32, _VP, _VP, C.c_uint32]),
     "mb2_debug_schedule": (C.c_int, [C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions), C.c_uint32, _VP, _VP,
-                                     _VP, _VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+                                     _VP, _VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int32]),
 }
 
 _lib = None

@@ -204,7 +204,7 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     m = std::min(std::max(m, mb2::kMinTileQubits), std::min(mmax, num_qubits));
     mb2::TileProgram prog;
     try {
-        prog = mb2::plan_tile_program(shape, num_qubits, m, mb2::kDefaultFixedLow, &flags);
+        prog = mb2::plan_tile_program(shape, num_qubits, m, mb2::kDefaultFixedLow, &flags, c64);
     } catch (const std::exception&) {
         return MB2_ERR_INVALID;
     }

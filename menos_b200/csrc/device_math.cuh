@@ -38,6 +38,11 @@ __device__ __forceinline__ double2 cneg_if(double2 v, uint32_t flip) {
     return make_double2(__hiloint2double(hx, __double2loint(v.x)), __hiloint2double(hy, __double2loint(v.y)));
 }
 __device__ __forceinline__ double2 cneg(double2 v) { return cneg_if(v, 1u); }
+// Negates both parts when msk (0 or 0x80000000) is set.
+__device__ __forceinline__ double2 cneg_mask(double2 v, uint32_t msk) {
+    return make_double2(__hiloint2double(__double2hiint(v.x) ^ static_cast<int>(msk), __double2loint(v.x)),
+                        __hiloint2double(__double2hiint(v.y) ^ static_cast<int>(msk), __double2loint(v.y)));
+}
 // d * a for one diagonal / monomial entry, exact up to a zero's sign:
 // (1, 0) -> a, (-1, 0) -> -a, else the full product.
 __device__ __forceinline__ double2 scale_entry(double dr, double di, double2 a) {

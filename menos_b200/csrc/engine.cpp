@@ -373,7 +373,9 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     try {
         const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
                                                                          : static_cast<uint32_t>(o.low_qubits));
-        prog = mb2::plan_tile_program(blocks, s->n, m, low);
+        // complex64 results are not bitwise the reference's: commuting
+        // blocks may be reordered into fewer passes.
+        prog = mb2::plan_tile_program(blocks, s->n, m, low, nullptr, c64);
     } catch (const std::exception& e) {
         return fail(s->ctx, MB2_ERR_INVALID, e.what());
     }
@@ -670,8 +672,10 @@ int mb2_synchronize(mb2_state* s) {
 
 int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
                        uint32_t* pass, uint32_t* k, uint32_t* qubits, double* matrices, uint64_t* num_blocks,
-                       uint64_t* matrix_len) {
+                       uint64_t* matrix_len, int32_t precision) {
     if (num_blocks == nullptr || matrix_len == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
+    if (precision != MB2_C128 && precision != MB2_C64) return MB2_ERR_INVALID;
+    const bool c64 = precision == MB2_C64;
     if (num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
     mb2_sweep_options o{1, 0, 0, 0};
     if (opts != nullptr) o = *opts;
@@ -679,8 +683,14 @@ int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
     std::vector<uint32_t> order, order_pass;
     try {
         blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
-        const uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, num_qubits, blocks);
-        if (o.per_gate != 0 || num_qubits < mb2::kMinTileQubits || blocks.empty()) {
+        uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, num_qubits, blocks);
+        if (c64) {
+            m = o.tile_qubits > 0 ? std::min<uint32_t>(static_cast<uint32_t>(o.tile_qubits), mb2::kMaxTileQubitsC64)
+                                  : std::min<uint32_t>(mb2::kDefaultTileQubitsC64, num_qubits);
+            for (const mb2::Block& b : blocks) m = std::max(m, b.k);
+            m = std::max(m, mb2::kMinTileQubits);
+        }
+        if ((!c64 && o.per_gate != 0) || num_qubits < mb2::kMinTileQubits || blocks.empty()) {
             for (uint32_t i = 0; i < blocks.size(); ++i) {
                 order.push_back(i);
                 order_pass.push_back(i);
@@ -688,7 +698,7 @@ int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
         } else {
             const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
                                                                              : static_cast<uint32_t>(o.low_qubits));
-            const mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m, low);
+            const mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m, low, nullptr, c64);
             order = prog.order;
             order_pass = prog.order_pass;
         }
@@ -898,11 +908,16 @@ int mb2_estimate_sweep_time(mb2_context* ctx, const mb2_op* ops, uint32_t num_op
                              : tile_width(req, num_qubits, blocks);
             for (const mb2::Block& b : blocks) m = std::max(m, b.k);
             m = std::min(m, num_qubits);
-            // A pass applies the next `gates` blocks in order (blocks are never reordered).
+            // Pass i applies the next `gates` blocks of the program's order.
+            const mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m, mb2::kDefaultFixedLow,
+                                                                 nullptr, c64);
+            std::vector<mb2::Block> ordered;
+            ordered.reserve(prog.order.size());
+            for (uint32_t i : prog.order) ordered.push_back(blocks[i]);
             size_t b0 = 0;
-            for (const mb2::TilePass& p : mb2::plan_tile_program(blocks, num_qubits, m).passes) {
-                const size_t b1 = std::min(blocks.size(), b0 + p.gates);
-                total += pass_seconds(t, c64, blocks, b0, b1, num_qubits);
+            for (const mb2::TilePass& p : prog.passes) {
+                const size_t b1 = std::min(ordered.size(), b0 + p.gates);
+                total += pass_seconds(t, c64, ordered, b0, b1, num_qubits);
                 b0 = b1;
             }
         }

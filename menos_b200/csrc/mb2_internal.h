@@ -161,11 +161,10 @@ constexpr uint32_t kU3Run012 = 112;
 constexpr uint32_t kPhase = 200;
 constexpr uint32_t kPhaseWords = 29;
 constexpr uint32_t kSmem = 201;  // aux = k; extra words: tile positions, gdata offset (doubles)
-// A sign monomial: six 5-bit sources, 31 = none, 16 + s = register slot s,
-// else a tile bit (a thread bit in that phase).  The amplitudes whose
-// sources are all 1 change sign.
-constexpr uint32_t kSrcNone = 31;
-constexpr uint32_t kSrcReg = 16;
+// A sign monomial word: bits 0-15 the register slots j (of 16) whose
+// register-bit factors are all 1 (0xffff: no register factor), bits 16-31
+// the tile bits of its thread-bit factors.  The amplitudes of slots j in
+// threads whose tile bits cover bits 16-31 change sign.
 }  // namespace cop
 
 // Shared-memory budget of one pass's staged instructions + data.
@@ -204,9 +203,12 @@ constexpr uint8_t kParamM00Real = 4;   // ... entry (0,0) is real in every bindi
 // staged; each gets an offset in a per-binding record instead
 // (param_offsets[block], record length param_stride doubles), and a kind
 // that holds for every parameter value.
+// commuting: blocks on disjoint qubits may be applied in either order
+// (the complex64 path, whose result is not bitwise the reference's), and
+// the passes follow a dependency order chosen for few passes and phases.
 TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint32_t m,
                               uint32_t fixed_low = kDefaultFixedLow,
-                              const std::vector<uint8_t>* parametric = nullptr);
+                              const std::vector<uint8_t>* parametric = nullptr, bool commuting = false);
 
 // ---- device launches (kernels_*.cu) ----------------------------------------
 struct DevCtx;  // forward (engine.cpp)

@@ -118,11 +118,11 @@ void encode_compact(TileProgram& prog) {
                 w.insert(w.end(), live.begin() + static_cast<long>(i), live.begin() + static_cast<long>(i + cnt));
             }
         };
-        // Source code of tile position p in the current phase.
-        auto source_of = [&](uint32_t p) -> uint32_t {
+        // Register slot of tile position p in the current phase, -1 for a thread bit.
+        auto slot_of = [&](uint32_t p) -> int {
             for (uint32_t s = 0; s < kRegQubits; ++s)
-                if (reg[s] == p) return cop::kSrcReg + s;
-            return p;
+                if (reg[s] == p) return static_cast<int>(s);
+            return -1;
         };
         // Adds the sign function of a +-1 diagonal (neg[e]: entry e is -1)
         // on tile positions pos[0..k-1].
@@ -132,15 +132,18 @@ void encode_compact(TileProgram& prog) {
             for (uint32_t i = 0; i < k; ++i)
                 for (uint32_t s = 0; s < dim; ++s)
                     if (s & (1u << i)) c[s] ^= c[s ^ (1u << i)];
+            // Register slot s's bit over the 16 slots j: 0xAAAA, 0xCCCC, 0xF0F0, 0xFF00.
+            constexpr uint32_t kSlotBits[kRegQubits] = {0xAAAAu, 0xCCCCu, 0xF0F0u, 0xFF00u};
             for (uint32_t s = 0; s < dim; ++s) {
                 if (!c[s]) continue;
-                std::vector<uint32_t> src;
-                for (uint32_t t = 0; t < k; ++t)
-                    if (s & (1u << t)) src.push_back(source_of(pos[t]));
-                std::sort(src.begin(), src.end());
-                uint32_t mono = 0;
-                for (uint32_t f = 0; f < 6; ++f)
-                    mono |= (f < src.size() ? src[f] : cop::kSrcNone) << (5 * f);
+                uint32_t slots = 0xffffu, tbits = 0;
+                for (uint32_t t = 0; t < k; ++t) {
+                    if (!(s & (1u << t))) continue;
+                    const int r = slot_of(pos[t]);
+                    if (r >= 0) slots &= kSlotBits[r];
+                    else tbits |= 1u << pos[t];
+                }
+                const uint32_t mono = slots | (tbits << 16);
                 signs[mono] = !signs[mono];
             }
         };

@@ -347,20 +347,11 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
                         uint32_t M = 0;
                         for (uint32_t i = 0; i < aux; ++i) {
                             const uint32_t mono = sw[pc++];
-                            uint32_t mm = 0xffffu;
-                            for (uint32_t f = 0; f < 6; ++f) {
-                                const uint32_t src = (mono >> (5 * f)) & 31u;
-                                if (src == cop::kSrcNone) break;
-                                const uint32_t v =
-                                    (src & cop::kSrcReg)
-                                        ? static_cast<uint32_t>(0xFF00F0F0CCCCAAAAull >> (16 * (src & 3u))) & 0xffffu
-                                        : (((tb >> src) & 1u) ? 0xffffu : 0u);
-                                mm &= v;
-                            }
-                            M ^= mm;
+                            const uint32_t tm = mono >> 16;
+                            M ^= (tb & tm) == tm ? (mono & 0xffffu) : 0u;
                         }
 #pragma unroll
-                        for (int j = 0; j < kNA; ++j) a[j] = cneg_if(a[j], (M >> j) & 1u);
+                        for (int j = 0; j < kNA; ++j) a[j] = cneg_mask(a[j], (M << (31 - j)) & 0x80000000u);
                     } break;
                     default: {  // cop::kDiagK: any k, entry index per amplitude
                         if constexpr (!FULL) break;

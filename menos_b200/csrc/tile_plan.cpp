@@ -133,13 +133,190 @@ uint32_t push_matrix(std::vector<double>& data, const std::vector<Cd>& m) {
 
 }  // namespace
 
+// Passes over a topological order of the blocks' dependencies (two blocks
+// depend when they share a qubit; blocks on disjoint qubits commute), for
+// the paths that are not bitwise the reference's sweep (complex64).  Each
+// pass picks its tile greedily: the qubits of the earliest unapplied block,
+// the fixed low qubits, then one qubit at a time the one that lets the most
+// blocks run (ties: the one most blocked blocks wait for).  Inside the pass
+// the blocks are ordered phase by phase: every ready block that a register
+// set of four qubits (or no register at all: diagonals) can take, then the
+// next set from the ready dense blocks, so the kernel changes phase rarely.
+std::vector<PassSel> select_passes_commuting(const std::vector<Block>& blocks, uint32_t n, uint32_t m,
+                                             uint32_t fixed_low) {
+    std::vector<PassSel> passes;
+    uint32_t widest = 1;
+    for (const Block& b : blocks) widest = std::max(widest, b.k);
+    const uint32_t mt = std::min(m, n);
+    if (widest > mt) throw std::invalid_argument("a block is wider than the tile");
+    const uint32_t fixed = std::min(fixed_low, mt - widest);
+    const uint32_t nb = static_cast<uint32_t>(blocks.size());
+    std::vector<std::vector<uint32_t>> lists(n);
+    for (uint32_t i = 0; i < nb; ++i)
+        for (uint32_t t = 0; t < blocks[i].k; ++t) lists[blocks[i].q[t]].push_back(i);
+    std::vector<uint32_t> head(n, 0);
+    auto at_head = [&](const std::vector<uint32_t>& h, uint32_t i) {
+        for (uint32_t t = 0; t < blocks[i].k; ++t) {
+            const uint32_t y = blocks[i].q[t];
+            if (h[y] >= lists[y].size() || lists[y][h[y]] != i) return false;
+        }
+        return true;
+    };
+    // Blocks that can run inside tile s from heads h, in a dependency order
+    // (h advances past them); stops at the pass limits when `limit`.
+    std::vector<uint32_t> work;
+    auto closure = [&](uint64_t s, std::vector<uint32_t>& h, std::vector<uint32_t>* out, bool limit) {
+        uint32_t count = 0;
+        size_t staged = 0;
+        work.clear();
+        for (uint32_t x = 0; x < n; ++x)
+            if ((s >> x) & 1u) work.push_back(x);
+        while (!work.empty()) {
+            const uint32_t x = work.back();
+            work.pop_back();
+            if (h[x] >= lists[x].size()) continue;
+            const uint32_t i = lists[x][h[x]];
+            if ((blocks[i].mask() & ~s) != 0 || !at_head(h, i)) continue;
+            if (limit && (count >= kMaxBlocksPerPass ||
+                          (count > 0 && staged + staged_bytes(blocks[i]) > kMaxStagedBytes)))
+                break;
+            staged += staged_bytes(blocks[i]);
+            ++count;
+            if (out) out->push_back(i);
+            for (uint32_t t = 0; t < blocks[i].k; ++t) {
+                ++h[blocks[i].q[t]];
+                work.push_back(blocks[i].q[t]);
+            }
+        }
+        return count;
+    };
+    uint32_t applied = 0, first = 0;
+    std::vector<uint8_t> done(nb, 0);
+    std::vector<uint32_t> h;
+    while (applied < nb) {
+        while (done[first]) ++first;
+        uint64_t s = blocks[first].mask();
+        for (uint32_t q = 0; q < fixed; ++q) s |= uint64_t{1} << q;
+        while (static_cast<uint32_t>(std::popcount(s)) < mt) {
+            uint64_t best_score = 0;
+            uint32_t best = n;
+            for (uint32_t x = 0; x < n; ++x) {
+                if ((s >> x) & 1u) continue;
+                h = head;
+                const uint64_t runs = closure(s | (uint64_t{1} << x), h, nullptr, false);
+                // Blocked blocks at the tile's heads that wait for x.
+                uint32_t waits = 0;
+                for (uint32_t y = 0; y < n; ++y)
+                    if (((s >> y) & 1u) && head[y] < lists[y].size() &&
+                        ((blocks[lists[y][head[y]]].mask() >> x) & 1u))
+                        ++waits;
+                const uint64_t score = (runs << 16) | waits;
+                if (best == n || score > best_score) {
+                    best_score = score;
+                    best = x;
+                }
+            }
+            s |= uint64_t{1} << best;
+        }
+        std::vector<uint32_t> members;
+        h = head;
+        closure(s, h, &members, true);
+        if (members.empty()) throw std::logic_error("tile selection made no progress");
+        // Phase-by-phase order of the members.
+        PassSel sel;
+        sel.smask = s;
+        std::vector<uint8_t> in_pass(nb, 0);
+        for (uint32_t i : members) in_pass[i] = 1;
+        std::vector<uint32_t> ph = head, sim;
+        std::vector<uint8_t> sim_in;
+        // Runs every member that register set `regs` can take (diagonals and
+        // wide blocks need none), from heads hh, in waves: the ready dense
+        // blocks, then the ready diagonals (so that the diagonals of one
+        // layer are consecutive and merge), and so on; returns the dense
+        // ones run.
+        auto run = [&](uint64_t regs, std::vector<uint32_t>& hh, std::vector<uint8_t>& in, std::vector<uint32_t>* out) {
+            uint32_t dense = 0;
+            for (bool any = true; any;) {
+                any = false;
+                for (const bool diag : {false, true}) {
+                    work.clear();
+                    for (uint32_t x = 0; x < n; ++x)
+                        if ((s >> x) & 1u) work.push_back(x);
+                    while (!work.empty()) {
+                        const uint32_t x = work.back();
+                        work.pop_back();
+                        if (hh[x] >= lists[x].size()) continue;
+                        const uint32_t i = lists[x][hh[x]];
+                        const Block& b = blocks[i];
+                        if (!in[i] || b.diagonal != diag || !at_head(hh, i) ||
+                            !(b.diagonal || b.k > 2 || (b.mask() & ~regs) == 0))
+                            continue;
+                        in[i] = 0;
+                        any = true;
+                        if (!b.diagonal && b.k <= 2) ++dense;
+                        if (out) out->push_back(i);
+                        for (uint32_t t = 0; t < b.k; ++t) {
+                            ++hh[b.q[t]];
+                            work.push_back(b.q[t]);
+                        }
+                    }
+                }
+            }
+            return dense;
+        };
+        size_t left = members.size();
+        uint64_t regs = 0;
+        for (;;) {
+            const size_t before = sel.gates.size();
+            run(regs, ph, in_pass, &sel.gates);
+            left -= sel.gates.size() - before;
+            if (left == 0) break;
+            // Next register set: grown one qubit at a time by the qubit that
+            // lets the most dense blocks run (ties: the one most ready dense
+            // blocks use, then the lowest).
+            uint64_t cand = 0;
+            for (uint32_t i : members)
+                if (in_pass[i] && !blocks[i].diagonal && blocks[i].k <= 2) cand |= blocks[i].mask();
+            regs = 0;
+            for (uint32_t r = 0; r < kRegQubits && (cand & ~regs) != 0; ++r) {
+                uint64_t best_score = 0;
+                uint32_t best = n;
+                for (uint32_t x = 0; x < n; ++x) {
+                    if (!((cand >> x) & 1u) || ((regs >> x) & 1u)) continue;
+                    sim = ph;
+                    sim_in = in_pass;
+                    const uint64_t runs = run(regs | (uint64_t{1} << x), sim, sim_in, nullptr);
+                    uint32_t uses = 0;
+                    for (uint32_t i : members)
+                        if (in_pass[i] && !blocks[i].diagonal && blocks[i].k <= 2 && ((blocks[i].mask() >> x) & 1u) &&
+                            at_head(ph, i))
+                            ++uses;
+                    const uint64_t score = (runs << 16) | uses;
+                    if (best == n || score > best_score) {
+                        best_score = score;
+                        best = x;
+                    }
+                }
+                regs |= uint64_t{1} << best;
+            }
+            if (regs == 0) throw std::logic_error("phase ordering made no progress");
+        }
+        for (uint32_t i : sel.gates) done[i] = 1;
+        applied += static_cast<uint32_t>(sel.gates.size());
+        head = ph;
+        passes.push_back(std::move(sel));
+    }
+    return passes;
+}
+
 TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint32_t m, uint32_t fixed_low,
-                              const std::vector<uint8_t>* parametric) {
+                              const std::vector<uint8_t>* parametric, bool commuting) {
     if (m < kMinTileQubits || m > kMaxTileQubitsC64) throw std::invalid_argument("tile width out of range");
     TileProgram prog;
     const uint32_t mt = std::min(m, n);
     if (mt < kRegQubits) throw std::invalid_argument("state too small for the tile kernel");
-    const std::vector<PassSel> sels = select_passes(blocks, n, mt, fixed_low);
+    const std::vector<PassSel> sels =
+        commuting ? select_passes_commuting(blocks, n, mt, fixed_low) : select_passes(blocks, n, mt, fixed_low);
     prog.param_offsets.assign(blocks.size(), 0);
     auto param_flags = [&](uint32_t bi) -> uint8_t { return parametric ? (*parametric)[bi] : uint8_t{0}; };
     // A parametric block's data goes to the per-binding record.

@@ -79,7 +79,7 @@ def test_workload_shapes():
     assert len(ps) == 64 and all(x < (1 << 30) and z < (1 << 30) for x, z in ps)
 
 
-def schedule(circ, n, fuse=True, tile=0, per_gate=False):
+def schedule(circ, n, fuse=True, tile=0, per_gate=False, precision=_lib.C128):
     arr, keep = to_mb2_ops(circ)
     opts = _lib.SweepOptions(1 if fuse else 0, 0, tile, 1 if per_gate else 0)
     cap = 4 * len(circ.ops) + 4
@@ -90,7 +90,7 @@ def schedule(circ, n, fuse=True, tile=0, per_gate=False):
     nb = C.c_uint64(cap)
     ml = C.c_uint64(mats.size)
     rc = _lib.lib().mb2_debug_schedule(arr, len(circ.ops), C.byref(opts), n, pas.ctypes.data, ks.ctypes.data,
-                                       qs.ctypes.data, mats.ctypes.data, C.byref(nb), C.byref(ml))
+                                       qs.ctypes.data, mats.ctypes.data, C.byref(nb), C.byref(ml), precision)
     assert rc == 0
     out, off = [], 0
     for i in range(nb.value):
@@ -124,6 +124,42 @@ def test_tiled_schedule_is_bitwise_the_plain_sweep(oracle, tile):
                 oracle.apply_generic(state, m, qs)
             expect = oracle.run(as_oracle_circuit(c), fuse_gates=fuse)
             assert bits_equal(state, expect), (n, fuse, tile)
+
+
+@pytest.mark.parametrize("tile", [4, 5, 7, 12, 13])
+def test_complex64_schedule_is_a_dependency_order(oracle, tile):
+    # The complex64 planner reorders blocks on disjoint qubits: every qubit
+    # sees its blocks in plan order, and the state is the in-order one up to
+    # rounding.
+    rng = np.random.default_rng(100 + tile)
+    for n in (4, 6, 9, 13, 16):
+        for fuse in (True, False):
+            c = random_circuit(n, 80, rng)
+            c.num_clbits = 0
+            plain = schedule(c, n, fuse=fuse, tile=tile)
+            reord = schedule(c, n, fuse=fuse, tile=tile, precision=_lib.C64)
+            assert len(plain) == len(reord)
+            passes = [p for p, _, _ in reord]
+            assert passes == sorted(passes)
+            key = lambda qs, m: (tuple(int(q) for q in qs), m.tobytes())
+            for q in range(n):
+                seq_p = [key(qs, m) for _, qs, m in plain if q in qs]
+                seq_r = [key(qs, m) for _, qs, m in reord if q in qs]
+                assert seq_p == seq_r, (n, fuse, tile, q)
+            state = oracle.initialize(n, c.global_phase)
+            for _p, qs, m in reord:
+                oracle.apply_generic(state, m, qs)
+            expect = oracle.run(as_oracle_circuit(c), fuse_gates=fuse)
+            assert np.max(np.abs(state - expect)) < 1e-12, (n, fuse, tile)
+
+
+def test_complex64_brick_schedule_has_few_passes():
+    # Light-cone tiles: a 12-qubit tile runs several brick layers of its
+    # qubits before the next tile, instead of one run of consecutive blocks.
+    c = workloads.brick(28, 32, 5)
+    plain = max(p for p, _, _ in schedule(c, 28, tile=12)) + 1
+    reord = max(p for p, _, _ in schedule(c, 28, tile=12, precision=_lib.C64)) + 1
+    assert reord <= 40 and 4 * reord <= plain, (reord, plain)
 
 
 def test_brick_schedule_pass_count():
