@@ -28,6 +28,12 @@ static_assert(kR == 4, "written for 4 register qubits");
 struct Cf {
     float r, i;
 };
+// Entry e of a matrix staged as FP32 pairs (rounded once from the FP64
+// composition when the pass's data is staged), or read from FP64 data.
+__device__ __forceinline__ Cf entry(const float* md, uint32_t e) {
+    const float2 d = reinterpret_cast<const float2*>(md)[e];
+    return Cf{d.x, d.y};
+}
 __device__ __forceinline__ Cf entry(const double* md, uint32_t e) {
     const double2 d = reinterpret_cast<const double2*>(md)[e];
     return Cf{static_cast<float>(d.x), static_cast<float>(d.y)};
@@ -42,20 +48,30 @@ __device__ __forceinline__ float2 fneg_if(float2 v, uint32_t flip) {
     return make_float2(__uint_as_float(__float_as_uint(v.x) ^ msk), __uint_as_float(__float_as_uint(v.y) ^ msk));
 }
 
-template <int P>
-__device__ __forceinline__ void g1(float2 (&a)[kNA], const double* md) {
+// A dense 2x2 on register slot P.  KIND: 0 general, 1 entry (0,0) real
+// (U3), 2 every entry real; the known-zero imaginary parts are skipped.
+template <int P, int KIND = 0>
+__device__ __forceinline__ void g1(float2 (&a)[kNA], const float* md) {
     const Cf m00 = entry(md, 0), m01 = entry(md, 1), m10 = entry(md, 2), m11 = entry(md, 3);
 #pragma unroll
     for (int j = 0; j < kNA; ++j) {
         if (j & (1 << P)) continue;
         const float2 x = a[j], y = a[j | (1 << P)];
-        a[j] = cfma(m01, y, cmulf(m00, x));
-        a[j | (1 << P)] = cfma(m11, y, cmulf(m10, x));
+        if constexpr (KIND == 2) {
+            a[j] = make_float2(fmaf(m01.r, y.x, m00.r * x.x), fmaf(m01.r, y.y, m00.r * x.y));
+            a[j | (1 << P)] = make_float2(fmaf(m11.r, y.x, m10.r * x.x), fmaf(m11.r, y.y, m10.r * x.y));
+        } else if constexpr (KIND == 1) {
+            a[j] = cfma(m01, y, make_float2(m00.r * x.x, m00.r * x.y));
+            a[j | (1 << P)] = cfma(m11, y, cmulf(m10, x));
+        } else {
+            a[j] = cfma(m01, y, cmulf(m00, x));
+            a[j | (1 << P)] = cfma(m11, y, cmulf(m10, x));
+        }
     }
 }
 
 template <int P0, int P1>
-__device__ __forceinline__ void g2(float2 (&a)[kNA], const double* md) {
+__device__ __forceinline__ void g2(float2 (&a)[kNA], const float* md) {
     if constexpr (P0 == P1) {
         return;
     } else {
@@ -112,7 +128,7 @@ __device__ __forceinline__ void perm2(float2 (&a)[kNA]) {
 // thread bit of value v_b).  Entry e multiplies the amplitudes whose operand
 // bits spell e; class 0 entries (exactly 1) are skipped.
 template <int P0, int P1>
-__device__ __forceinline__ void diag_regs(float2 (&a)[kNA], const double* md, uint32_t k, uint32_t cls, uint32_t v0,
+__device__ __forceinline__ void diag_regs(float2 (&a)[kNA], const float* md, uint32_t k, uint32_t cls, uint32_t v0,
                                           uint32_t v1) {
 #pragma unroll
     for (uint32_t e = 0; e < 4; ++e) {
@@ -158,10 +174,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
     const uint32_t tbits = m - kRegQubits;
     const uint32_t tile_amps = 1u << m;
     uint32_t* sw = reinterpret_cast<uint32_t*>(smem_f + stages * tile_amps);
-    double* sd = reinterpret_cast<double*>(sw + nwords);
+    // The pass's data is staged as FP32 (each FP64-composed entry rounded once).
+    float* sd = reinterpret_cast<float*>(sw + nwords);
     for (uint32_t i = tid; i < nwords / 4; i += blockDim.x)
         reinterpret_cast<uint4*>(sw)[i] = __ldg(reinterpret_cast<const uint4*>(words) + i);
-    for (uint32_t i = tid; i < nsdata; i += blockDim.x) sd[i] = __ldg(sdata + i);
+    for (uint32_t i = tid; i < nsdata; i += blockDim.x) sd[i] = static_cast<float>(__ldg(sdata + i));
     IDX off_lo = 0, hib0 = 0, hib1 = 0, hib2 = 0, hib3 = 0;
     {
         uint32_t b = 0;
@@ -215,9 +232,9 @@ __global__ void __launch_bounds__(MAXT, MINB)
         cur = cur + 1 == stages ? 0u : cur + 1;
         nxt = nxt + 1 == stages ? 0u : nxt + 1;
         if (param_len != 0) {  // a batched sweep: this tile's binding is t >> bshift
-            const double2* src = reinterpret_cast<const double2*>(pdata + (t >> bshift) * pstride + param_lo);
-            double2* dst = reinterpret_cast<double2*>(sd + nsdata);
-            for (uint32_t i = tid; i < param_len / 2; i += blockDim.x) dst[i] = __ldg(src + i);
+            const double* src = pdata + (t >> bshift) * pstride + param_lo;
+            float* dst = sd + nsdata;
+            for (uint32_t i = tid; i < param_len; i += blockDim.x) dst[i] = static_cast<float>(__ldg(src + i));
         }
         if (stages == 3) cp_async_wait<2>();
         else cp_async_wait<1>();
@@ -252,7 +269,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
                     const uint32_t op = w & 0xffu;
                     if (op == cop::kEnd) break;
                     const uint32_t aux = (w >> 8) & 0xffu;
-                    const double* md = sd + ((w >> 20) << 1);
+                    const float* md = sd + ((w >> 20) << 1);
                     const uint32_t tv = (tb >> ((w >> 16) & 15u)) & 1u;
                     switch (op) {
 #define MB2_CASE4(BASE, ...) \
@@ -274,30 +291,30 @@ __global__ void __launch_bounds__(MAXT, MINB)
     case BASE + 10: { constexpr int P0 = 3, P1 = 1; __VA_ARGS__; } break; \
     case BASE + 11: { constexpr int P0 = 3, P1 = 2; __VA_ARGS__; } break;
                         // Every dense 1q kind is the general 2x2 in FP32.
-                        MB2_CASE4(cop::kU3, (g1<P>(a, md)))
+                        MB2_CASE4(cop::kU3, (g1<P, 1>(a, md)))
                         MB2_CASE4(cop::kGen1, (g1<P>(a, md)))
-                        MB2_CASE4(cop::kReal1, (g1<P>(a, md)))
+                        MB2_CASE4(cop::kReal1, (g1<P, 2>(a, md)))
                         MB2_CASE4(cop::kMono1, (g1<P>(a, md)))
                         MB2_CASE4(cop::kX1, if constexpr (FULL) perm1<P>(a))
                         case cop::kU3Run0123:
-                            g1<0>(a, md);
-                            g1<1>(a, md + 8);
-                            g1<2>(a, md + 16);
-                            g1<3>(a, md + 24);
+                            g1<0, 1>(a, md);
+                            g1<1, 1>(a, md + 8);
+                            g1<2, 1>(a, md + 16);
+                            g1<3, 1>(a, md + 24);
                             break;
                         case cop::kU3Run01:
-                            g1<0>(a, md);
-                            g1<1>(a, md + 8);
+                            g1<0, 1>(a, md);
+                            g1<1, 1>(a, md + 8);
                             break;
                         case cop::kU3Run123:
-                            g1<1>(a, md);
-                            g1<2>(a, md + 8);
-                            g1<3>(a, md + 16);
+                            g1<1, 1>(a, md);
+                            g1<2, 1>(a, md + 8);
+                            g1<3, 1>(a, md + 16);
                             break;
                         case cop::kU3Run012:
-                            g1<0>(a, md);
-                            g1<1>(a, md + 8);
-                            g1<2>(a, md + 16);
+                            g1<0, 1>(a, md);
+                            g1<1, 1>(a, md + 8);
+                            g1<2, 1>(a, md + 16);
                             break;
                         MB2_CASE12(cop::kGen2, if constexpr (FULL) g2<P0, P1>(a, md))
                         MB2_CASE12(cop::kMono2, if constexpr (FULL) { ++pc; g2<P0, P1>(a, md); })
@@ -460,7 +477,7 @@ int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uin
     // buffers each.
     L.stages = pass.m == kMaxTileQubitsC64 ? 3u : 2u;
     L.smem = L.stages * (size_t{1} << pass.m) * sizeof(float2) + size_t{pass.word_count} * 4 +
-             (size_t{pass.sdata_count} + pass.param_len) * sizeof(double);
+             (size_t{pass.sdata_count} + pass.param_len) * sizeof(float);
     L.ntiles = (uint64_t{1} << n) >> pass.m;
     L.n_all = n;
     if (batch != nullptr) {
