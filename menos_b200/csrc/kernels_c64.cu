@@ -94,17 +94,6 @@ __device__ __forceinline__ void g2(float2 (&a)[kNA], const float* md) {
     }
 }
 
-template <int P>
-__device__ __forceinline__ void perm1(float2 (&a)[kNA]) {
-#pragma unroll
-    for (int j = 0; j < kNA; ++j) {
-        if (j & (1 << P)) continue;
-        const float2 t = a[j];
-        a[j] = a[j | (1 << P)];
-        a[j | (1 << P)] = t;
-    }
-}
-
 template <int P0, int P1, int KIND>
 __device__ __forceinline__ void perm2(float2 (&a)[kNA]) {
     if constexpr (P0 == P1) {
@@ -294,8 +283,6 @@ __global__ void __launch_bounds__(MAXT, MINB)
                         MB2_CASE4(cop::kU3, (g1<P, 1>(a, md)))
                         MB2_CASE4(cop::kGen1, (g1<P>(a, md)))
                         MB2_CASE4(cop::kReal1, (g1<P, 2>(a, md)))
-                        MB2_CASE4(cop::kMono1, (g1<P>(a, md)))
-                        MB2_CASE4(cop::kX1, if constexpr (FULL) perm1<P>(a))
                         case cop::kU3Run0123:
                             g1<0, 1>(a, md);
                             g1<1, 1>(a, md + 8);

@@ -133,8 +133,7 @@ constexpr uint32_t kEnd = 0;     // end of a phase
 constexpr uint32_t kU3 = 1;      // + slot
 constexpr uint32_t kGen1 = 5;    // + slot
 constexpr uint32_t kReal1 = 9;   // + slot
-constexpr uint32_t kMono1 = 13;  // + slot; aux = source rows (3 bits each)
-constexpr uint32_t kX1 = 17;     // + slot
+// 13-20 are unused (one-qubit monomials and X are written as kGen1/kReal1).
 constexpr uint32_t kGen2 = 21;   // + pair
 constexpr uint32_t kMono2 = 33;  // + pair; extra word = source rows (3 bits each)
 constexpr uint32_t kSw12 = 45;   // + pair

@@ -176,17 +176,6 @@ __device__ __forceinline__ void gen2_if(double2 (&a)[kNA], const double* md) {
 // Exact permutations (every nonzero entry (1,0)): register moves only.
 // TK_X: 1q swap; TK_SW12 / TK_SW13 / TK_SW23: 2q, exchange local indices
 // (1,2) (SWAP), (1,3) (CX, control = operand 0), (2,3) (CX, control = operand 1).
-template <int P>
-__device__ __forceinline__ void perm1(double2 (&a)[kNA]) {
-#pragma unroll
-    for (int j = 0; j < kNA; ++j) {
-        if (j & (1 << P)) continue;
-        const double2 t = a[j];
-        a[j] = a[j | (1 << P)];
-        a[j | (1 << P)] = t;
-    }
-}
-
 template <int P0, int P1, int KIND>
 __device__ __forceinline__ void perm2(double2 (&a)[kNA]) {
     if constexpr (P0 == P1) {
@@ -292,8 +281,6 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
                     MB2_CASE4(cop::kU3, (g1<P, TK_U3>(a, md, 0u)))
                     MB2_CASE4(cop::kGen1, (g1<P, TK_GEN>(a, md, 0u)))
                     MB2_CASE4(cop::kReal1, (g1<P, TK_REAL>(a, md, 0u)))
-                    MB2_CASE4(cop::kMono1, if constexpr (FULL) g1<P, TK_MONO>(a, md, aux))
-                    MB2_CASE4(cop::kX1, if constexpr (FULL) perm1<P>(a))
                     MB2_CASE12(cop::kGen2, (gen2_if<P0, P1, FULL>(a, md)))
                     MB2_CASE12(cop::kMono2, if constexpr (FULL) g2<P0, P1, TK_MONO>(a, md, sw[pc++]))
                     MB2_CASE12(cop::kSw12, if constexpr (FULL) perm2<P0, P1, TK_SW12>(a))
