@@ -7,7 +7,9 @@
 // reference computes for that binding alone.  All bindings share one tile
 // program; blocks whose matrices differ between bindings read their entries
 // from a per-binding record selected by the tile's binding index.  The
-// expectation runs one 8-CTA cluster per binding (kernels_batch.cu).
+// expectation is the grouped Pauli reduction over every binding's state
+// (kernels_reduce.cu); states under 11 qubits take one 8-CTA cluster per
+// binding (kernels_batch.cu).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -25,6 +27,12 @@ int launch_batch_init(void* amps, uint32_t n, uint64_t bindings, double re, doub
 int launch_batch_expect(const void* amps, uint32_t n, uint64_t bindings, const uint64_t* dev_x,
                         const uint64_t* dev_z, const double* dev_coefs, uint32_t num_terms, double* dev_out,
                         void* stream, int precision);
+int launch_pauli_group_batch(const void* amps, uint32_t n, uint32_t c, uint32_t d, const uint64_t* dev_span,
+                             uint64_t free_mask, const void* dev_terms, uint32_t nterms, uint64_t bindings,
+                             uint32_t per, double* dev_partials, int sm_count, void* stream, int precision);
+int launch_batch_group_finish(const double* dev_partials, uint64_t bindings, uint32_t per, const uint64_t* dev_x,
+                              const uint64_t* dev_z, const double* dev_coefs, uint32_t num_terms, double* dev_out,
+                              void* stream);
 }  // namespace mb2
 
 namespace {
@@ -249,8 +257,23 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
     auto al = [](size_t v) { return (v + 255) & ~size_t{255}; };
     const size_t ib = prog.words.size() * sizeof(uint32_t), sb = prog.data.size() * 8,
                  gb = prog.gdata.size() * 8, pb = pdata.size() * 8, tb = size_t{num_terms} * 8;
+    // <H> per binding: with at least kPauliTileQubits qubits, the grouped
+    // reduction (terms sharing a GF(2) span read each state once, `per`
+    // CTAs per binding); smaller states: one 8-CTA cluster per binding.
+    mb2::PauliPlan pplan;
+    bool grouped = num_terms > 0 && num_qubits >= mb2::kPauliTileQubits;
+    if (grouped) {
+        pplan = mb2::plan_pauli_groups(x_masks, z_masks, num_terms, num_qubits);
+        for (const mb2::PauliGroupPlan& g : pplan.groups)
+            if (g.c + g.d < mb2::kPauliMinTileQubits) grouped = false;
+    }
+    const uint32_t gper = std::min<uint32_t>(4u, 1u << std::min<uint32_t>(2u, num_qubits - mb2::kPauliTileQubits));
+    const size_t spb = grouped ? pplan.spans.size() * 8 : 0,
+                 trb = grouped ? pplan.terms.size() * sizeof(mb2::PauliGroupTerm) : 0,
+                 prb = grouped ? size_t{num_terms} * num_bindings * gper * 16 : 0;
     const size_t o_s = al(ib), o_g = o_s + al(sb), o_p = o_g + al(gb), o_x = o_p + al(pb), o_z = o_x + al(tb),
-                 o_c = o_z + al(tb), o_o = o_c + al(tb), total = o_o + al(size_t{num_bindings} * 8);
+                 o_c = o_z + al(tb), o_sp = o_c + al(tb), o_tr = o_sp + al(spb), o_o = o_tr + al(trb),
+                 o_pr = o_o + al(size_t{num_bindings} * 8), total = o_pr + al(prb);
     if (cudaMalloc(&r.state, state_bytes) != cudaSuccess || cudaMalloc(&r.work, total) != cudaSuccess) {
         cudaGetLastError();
         return MB2_ERR_RESOURCE;
@@ -266,6 +289,8 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
         std::memcpy(host.data() + o_z, z_masks, tb);
         std::memcpy(host.data() + o_c, coefs, tb);
     }
+    if (spb) std::memcpy(host.data() + o_sp, pplan.spans.data(), spb);
+    if (trb) std::memcpy(host.data() + o_tr, pplan.terms.data(), trb);
     if (cudaMemcpyAsync(w, host.data(), host.size(), cudaMemcpyHostToDevice, r.stream) != cudaSuccess)
         return MB2_ERR_CUDA;
     const mb2::Cd ph = mb2::initial_phase(0.0);
@@ -287,10 +312,25 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
         if (rc != MB2_OK) return MB2_ERR_CUDA;
     }
     if (num_terms > 0) {
-        if (mb2::launch_batch_expect(r.state, num_qubits, num_bindings, reinterpret_cast<const uint64_t*>(w + o_x),
-                                     reinterpret_cast<const uint64_t*>(w + o_z), reinterpret_cast<const double*>(w + o_c),
-                                     num_terms, reinterpret_cast<double*>(w + o_o), r.stream, o.precision) != MB2_OK)
+        const auto* dx = reinterpret_cast<const uint64_t*>(w + o_x);
+        const auto* dz = reinterpret_cast<const uint64_t*>(w + o_z);
+        const auto* dc = reinterpret_cast<const double*>(w + o_c);
+        auto* dout = reinterpret_cast<double*>(w + o_o);
+        if (grouped) {
+            auto* parts = reinterpret_cast<double*>(w + o_pr);
+            for (const mb2::PauliGroupPlan& g : pplan.groups)
+                if (mb2::launch_pauli_group_batch(
+                        r.state, num_qubits, g.c, g.d, reinterpret_cast<const uint64_t*>(w + o_sp) + g.span_off,
+                        g.free_mask, w + o_tr + size_t{g.term_off} * sizeof(mb2::PauliGroupTerm), g.nterms,
+                        num_bindings, gper, parts, sm, r.stream, o.precision) != MB2_OK)
+                    return MB2_ERR_CUDA;
+            if (mb2::launch_batch_group_finish(parts, num_bindings, gper, dx, dz, dc, num_terms, dout, r.stream) !=
+                MB2_OK)
+                return MB2_ERR_CUDA;
+        } else if (mb2::launch_batch_expect(r.state, num_qubits, num_bindings, dx, dz, dc, num_terms, dout, r.stream,
+                                            o.precision) != MB2_OK) {
             return MB2_ERR_CUDA;
+        }
         if (cudaMemcpyAsync(out, w + o_o, size_t{num_bindings} * 8, cudaMemcpyDeviceToHost, r.stream) != cudaSuccess)
             return MB2_ERR_CUDA;
     } else {

@@ -12,6 +12,7 @@
 // bitwise the CPU's sequential sum; the parity tests bound the difference.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -152,6 +153,141 @@ __device__ __forceinline__ void cp_async_amp(float2* smem, const float2* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
+// Per-group tables in shared memory: the span, each term's low/high parts
+// and mode, and the parity of z_hi & span[k] per chunk k.
+struct GroupShared {
+    uint64_t sspan[1u << kPauliMaxSpan];
+    uint32_t cpar[kMaxGroupTerms][kChunkWords];  // parity of z_hi & span[k], bit k
+    uint32_t tdl[kMaxGroupTerms], tzl[kMaxGroupTerms], tmode[kMaxGroupTerms];
+    uint64_t tzh[kMaxGroupTerms];
+    double red[kThreads / 32];
+};
+
+__device__ __forceinline__ void group_setup(GroupShared& g, uint32_t c, uint32_t d, const uint64_t* __restrict__ span,
+                                            const GroupTerm* __restrict__ terms, uint32_t nterms) {
+    const uint32_t nchunks = 1u << d;
+    for (uint32_t i = threadIdx.x; i < nchunks; i += kThreads) g.sspan[i] = span[i];
+    for (uint32_t t = threadIdx.x; t < nterms; t += kThreads) {
+        const GroupTerm T = terms[t];
+        g.tdl[t] = (T.kx << c) | T.xl;
+        g.tzl[t] = static_cast<uint32_t>(T.z & ((uint64_t{1} << c) - 1));
+        g.tzh[t] = T.z >> c;
+        // 0: a Z string (x = 0); 1: real pair sum; 2: imaginary pair sum
+        g.tmode[t] = T.x == 0 ? 0u : ((__popcll(T.x & T.z) & 1) ? 2u : 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kMaxGroupTerms * kChunkWords; i += kThreads) {
+        const uint32_t t = i / kChunkWords, w = i % kChunkWords;
+        uint32_t bits = 0;
+        if (t < nterms)
+            for (uint32_t b = 0; b < 32 && w * 32 + b < nchunks; ++b)
+                bits |= static_cast<uint32_t>(__popcll(g.tzh[t] & g.sspan[w * 32 + b]) & 1) << b;
+        g.cpar[t][w] = bits;
+    }
+    __syncthreads();
+}
+
+// Adds one gathered coset tile (representative rep) to every term's two
+// accumulators.
+template <typename A>
+__device__ __forceinline__ void group_tile(const GroupShared& g, const A* __restrict__ cur, uint64_t rep, uint32_t c,
+                                           uint32_t tile_amps, uint32_t nterms, double (&acc0)[kMaxGroupTerms],
+                                           double (&acc1)[kMaxGroupTerms]) {
+#pragma unroll
+    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
+        if (t < nterms) {
+            const uint32_t dl = g.tdl[t], zl = g.tzl[t], mode = g.tmode[t];
+            const uint32_t rp = static_cast<uint32_t>(__popcll(g.tzh[t] & rep)) & 1u;
+            const uint32_t* cp = g.cpar[t];
+            if (mode == 0) {
+                for (uint32_t L = threadIdx.x; L < tile_amps; L += 2 * kThreads) {
+                    const uint32_t L1 = L + kThreads;
+                    const uint32_t k0 = L >> c, k1 = L1 >> c;
+                    const uint32_t n0 = rp ^ (cp[k0 >> 5] >> (k0 & 31)) ^ __popc(zl & L);
+                    const uint32_t n1 = rp ^ (cp[k1 >> 5] >> (k1 & 31)) ^ __popc(zl & L1);
+                    const double2 a0 = as_d2(cur[L]), a1 = as_d2(cur[L1]);
+                    const double p0 = __dadd_rn(__dmul_rn(a0.x, a0.x), __dmul_rn(a0.y, a0.y));
+                    const double p1 = __dadd_rn(__dmul_rn(a1.x, a1.x), __dmul_rn(a1.y, a1.y));
+                    acc0[t] = (n0 & 1) ? __dsub_rn(acc0[t], p0) : __dadd_rn(acc0[t], p0);
+                    acc1[t] = (n1 & 1) ? __dsub_rn(acc1[t], p1) : __dadd_rn(acc1[t], p1);
+                }
+            } else {
+                const uint32_t hb = 31 - __clz(dl);
+                const uint32_t below = (1u << hb) - 1;
+                for (uint32_t q = threadIdx.x; q < tile_amps / 2; q += 2 * kThreads) {
+                    const uint32_t q1 = q + kThreads;
+                    const uint32_t L0 = ((q & ~below) << 1) | (q & below);
+                    const uint32_t L1 = ((q1 & ~below) << 1) | (q1 & below);
+                    const uint32_t k0 = L0 >> c, k1 = L1 >> c;
+                    const uint32_t n0 = rp ^ (cp[k0 >> 5] >> (k0 & 31)) ^ __popc(zl & L0);
+                    const uint32_t n1 = rp ^ (cp[k1 >> 5] >> (k1 & 31)) ^ __popc(zl & L1);
+                    const double2 a0 = as_d2(cur[L0]), b0 = as_d2(cur[L0 ^ dl]);
+                    const double2 a1 = as_d2(cur[L1]), b1 = as_d2(cur[L1 ^ dl]);
+                    const double v0 = mode == 1 ? __dadd_rn(__dmul_rn(a0.x, b0.x), __dmul_rn(a0.y, b0.y))
+                                                : __dsub_rn(__dmul_rn(a0.x, b0.y), __dmul_rn(a0.y, b0.x));
+                    const double v1 = mode == 1 ? __dadd_rn(__dmul_rn(a1.x, b1.x), __dmul_rn(a1.y, b1.y))
+                                                : __dsub_rn(__dmul_rn(a1.x, b1.y), __dmul_rn(a1.y, b1.x));
+                    acc0[t] = (n0 & 1) ? __dsub_rn(acc0[t], v0) : __dadd_rn(acc0[t], v0);
+                    acc1[t] = (n1 & 1) ? __dsub_rn(acc1[t], v1) : __dadd_rn(acc1[t], v1);
+                }
+            }
+        }
+    }
+}
+
+// Per term: this CTA's sum in a fixed order (the two accumulators, lanes,
+// then warps), written to slot_of(t) as (re, im) of the pair sum before the
+// i^popcount(x & z) factor; the accumulators are cleared.
+template <typename SLOT>
+__device__ __forceinline__ void group_write(GroupShared& g, const GroupTerm* __restrict__ terms, uint32_t nterms,
+                                            double (&acc0)[kMaxGroupTerms], double (&acc1)[kMaxGroupTerms],
+                                            SLOT slot_of) {
+#pragma unroll
+    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
+        if (t < nterms) {
+            double r = __dadd_rn(acc0[t], acc1[t]);
+            for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+            __syncthreads();
+            if ((threadIdx.x & 31) == 0) g.red[threadIdx.x >> 5] = r;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double sum = 0.0;
+                for (int w = 0; w < kThreads / 32; ++w) sum += g.red[w];
+                double* p = slot_of(terms[t].out);
+                const uint32_t mode = g.tmode[t];
+                p[0] = mode == 0 ? sum : mode == 1 ? 2.0 * sum : 0.0;
+                p[1] = mode == 2 ? -2.0 * sum : 0.0;
+            }
+        }
+        acc0[t] = 0.0;
+        acc1[t] = 0.0;
+    }
+}
+
+// Coset representative: the coset number deposited on the free (non-pivot)
+// high bits.
+__device__ __forceinline__ uint64_t deposit_bits(uint64_t v, uint64_t mask) {
+    uint64_t r = 0;
+    while (mask != 0) {
+        const uint64_t low = mask & (~mask + 1);
+        if (v & 1) r |= low;
+        v >>= 1;
+        mask ^= low;
+    }
+    return r;
+}
+
+template <typename A>
+__device__ __forceinline__ void group_gather(const A* __restrict__ st, uint64_t rep, A* buf, const GroupShared& g,
+                                             uint32_t c, uint32_t tile_amps) {
+    const uint32_t lowmask = (1u << c) - 1;
+    for (uint32_t L = threadIdx.x; L < tile_amps; L += kThreads) {
+        const uint64_t m = ((rep ^ g.sspan[L >> c]) << c) | (L & lowmask);
+        cp_async_amp(buf + L, st + m);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
 // Cosets are processed with two shared-memory buffers: the next coset's
 // amplitudes are gathered with cp.async while this one is reduced.  Each
 // thread keeps two accumulators per term (alternate pairs) so consecutive
@@ -162,112 +298,31 @@ __global__ void __launch_bounds__(kThreads, 2)
                   uint64_t free_mask, const GroupTerm* __restrict__ terms, uint32_t nterms, uint64_t ncosets,
                   double* __restrict__ partials) {
     extern __shared__ __align__(16) unsigned char gsm[];
-    __shared__ uint64_t sspan[1u << kPauliMaxSpan];
-    __shared__ uint32_t cpar[kMaxGroupTerms][kChunkWords];  // parity of z_hi & span[k], bit k
-    __shared__ uint32_t tdl[kMaxGroupTerms], tzl[kMaxGroupTerms], tmode[kMaxGroupTerms];
-    __shared__ uint64_t tzh[kMaxGroupTerms];
-    __shared__ double red[kThreads / 32];
+    __shared__ GroupShared g;
     const uint32_t tile_amps = 1u << (c + d);
-    const uint32_t nchunks = 1u << d;
     A* buf0 = reinterpret_cast<A*>(gsm);
     A* buf1 = buf0 + tile_amps;
-    for (uint32_t i = threadIdx.x; i < nchunks; i += kThreads) sspan[i] = span[i];
-    for (uint32_t t = threadIdx.x; t < nterms; t += kThreads) {
-        const GroupTerm T = terms[t];
-        tdl[t] = (T.kx << c) | T.xl;
-        tzl[t] = static_cast<uint32_t>(T.z & ((uint64_t{1} << c) - 1));
-        tzh[t] = T.z >> c;
-        // 0: a Z string (x = 0); 1: real pair sum; 2: imaginary pair sum
-        tmode[t] = T.x == 0 ? 0u : ((__popcll(T.x & T.z) & 1) ? 2u : 1u);
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < kMaxGroupTerms * kChunkWords; i += kThreads) {
-        const uint32_t t = i / kChunkWords, w = i % kChunkWords;
-        uint32_t bits = 0;
-        if (t < nterms)
-            for (uint32_t b = 0; b < 32 && w * 32 + b < nchunks; ++b)
-                bits |= static_cast<uint32_t>(__popcll(tzh[t] & sspan[w * 32 + b]) & 1) << b;
-        cpar[t][w] = bits;
-    }
-    const uint32_t lowmask = (1u << c) - 1;
-    // Coset representatives: the coset number deposited on the free (non-
-    // pivot) high bits; moving gridDim.x cosets on is a masked add.
-    auto deposit = [&](uint64_t v) {
-        uint64_t r = 0, mask = free_mask;
-        while (mask != 0) {
-            const uint64_t low = mask & (~mask + 1);
-            if (v & 1) r |= low;
-            v >>= 1;
-            mask ^= low;
-        }
-        return r;
-    };
-    const uint64_t rstep = deposit(gridDim.x);
+    group_setup(g, c, d, span, terms, nterms);
+    // Moving gridDim.x cosets on is a masked add on the free bits.
+    const uint64_t rstep = deposit_bits(gridDim.x, free_mask);
     auto advance = [&](uint64_t r) { return ((r | ~free_mask) + rstep) & free_mask; };
-    auto gather = [&](uint64_t rep, A* buf) {
-        for (uint32_t L = threadIdx.x; L < tile_amps; L += kThreads) {
-            const uint64_t m = ((rep ^ sspan[L >> c]) << c) | (L & lowmask);
-            cp_async_amp(buf + L, st + m);
-        }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-    };
-    __syncthreads();  // sspan, cpar ready
     double acc0[kMaxGroupTerms], acc1[kMaxGroupTerms];
 #pragma unroll
     for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
         acc0[t] = 0.0;
         acc1[t] = 0.0;
     }
-    uint64_t rep = deposit(blockIdx.x);
-    if (blockIdx.x < ncosets) gather(rep, buf0);
+    uint64_t rep = deposit_bits(blockIdx.x, free_mask);
+    if (blockIdx.x < ncosets) group_gather(st, rep, buf0, g, c, tile_amps);
     A* cur = buf0;
     A* nxt = buf1;
     for (uint64_t cs = blockIdx.x; cs < ncosets; cs += gridDim.x) {
         const uint64_t rep_next = advance(rep);
-        if (cs + gridDim.x < ncosets) gather(rep_next, nxt);
+        if (cs + gridDim.x < ncosets) group_gather(st, rep_next, nxt, g, c, tile_amps);
         else asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         __syncthreads();
-#pragma unroll
-        for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
-            if (t < nterms) {
-                const uint32_t dl = tdl[t], zl = tzl[t], mode = tmode[t];
-                const uint32_t rp = static_cast<uint32_t>(__popcll(tzh[t] & rep)) & 1u;
-                const uint32_t* cp = cpar[t];
-                if (mode == 0) {
-                    for (uint32_t L = threadIdx.x; L < tile_amps; L += 2 * kThreads) {
-                        const uint32_t L1 = L + kThreads;
-                        const uint32_t k0 = L >> c, k1 = L1 >> c;
-                        const uint32_t n0 = rp ^ (cp[k0 >> 5] >> (k0 & 31)) ^ __popc(zl & L);
-                        const uint32_t n1 = rp ^ (cp[k1 >> 5] >> (k1 & 31)) ^ __popc(zl & L1);
-                        const double2 a0 = as_d2(cur[L]), a1 = as_d2(cur[L1]);
-                        const double p0 = __dadd_rn(__dmul_rn(a0.x, a0.x), __dmul_rn(a0.y, a0.y));
-                        const double p1 = __dadd_rn(__dmul_rn(a1.x, a1.x), __dmul_rn(a1.y, a1.y));
-                        acc0[t] = (n0 & 1) ? __dsub_rn(acc0[t], p0) : __dadd_rn(acc0[t], p0);
-                        acc1[t] = (n1 & 1) ? __dsub_rn(acc1[t], p1) : __dadd_rn(acc1[t], p1);
-                    }
-                } else {
-                    const uint32_t hb = 31 - __clz(dl);
-                    const uint32_t below = (1u << hb) - 1;
-                    for (uint32_t q = threadIdx.x; q < tile_amps / 2; q += 2 * kThreads) {
-                        const uint32_t q1 = q + kThreads;
-                        const uint32_t L0 = ((q & ~below) << 1) | (q & below);
-                        const uint32_t L1 = ((q1 & ~below) << 1) | (q1 & below);
-                        const uint32_t k0 = L0 >> c, k1 = L1 >> c;
-                        const uint32_t n0 = rp ^ (cp[k0 >> 5] >> (k0 & 31)) ^ __popc(zl & L0);
-                        const uint32_t n1 = rp ^ (cp[k1 >> 5] >> (k1 & 31)) ^ __popc(zl & L1);
-                        const double2 a0 = as_d2(cur[L0]), b0 = as_d2(cur[L0 ^ dl]);
-                        const double2 a1 = as_d2(cur[L1]), b1 = as_d2(cur[L1 ^ dl]);
-                        const double v0 = mode == 1 ? __dadd_rn(__dmul_rn(a0.x, b0.x), __dmul_rn(a0.y, b0.y))
-                                                    : __dsub_rn(__dmul_rn(a0.x, b0.y), __dmul_rn(a0.y, b0.x));
-                        const double v1 = mode == 1 ? __dadd_rn(__dmul_rn(a1.x, b1.x), __dmul_rn(a1.y, b1.y))
-                                                    : __dsub_rn(__dmul_rn(a1.x, b1.y), __dmul_rn(a1.y, b1.x));
-                        acc0[t] = (n0 & 1) ? __dsub_rn(acc0[t], v0) : __dadd_rn(acc0[t], v0);
-                        acc1[t] = (n1 & 1) ? __dsub_rn(acc1[t], v1) : __dadd_rn(acc1[t], v1);
-                    }
-                }
-            }
-        }
+        group_tile(g, cur, rep, c, tile_amps, nterms, acc0, acc1);
         __syncthreads();  // this buffer is the target of the gather after next
         rep = rep_next;
         A* tmp = cur;
@@ -275,26 +330,102 @@ __global__ void __launch_bounds__(kThreads, 2)
         nxt = tmp;
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    // Per term: this CTA's sum in a fixed order (the two accumulators, lanes,
-    // then warps), written as (re, im) of the pair sum before the
-    // i^popcount(x & z) factor.
+    group_write(g, terms, nterms, acc0, acc1, [&](uint32_t out) {
+        return partials + 2 * (static_cast<uint64_t>(out) * gridDim.x + blockIdx.x);
+    });
+}
+
+// The same grouped reduction over a batch of states (binding b's 2^n
+// amplitudes at b * 2^n).  `per` CTAs share a binding: CTA slot s takes the
+// binding's cosets s, s + per, ...; bindings are taken gridDim.x / per
+// apart.  Partial (term, binding, slot) lands at
+// partials[2 * ((term * bindings + b) * per + s)], so a binding's value
+// depends only on its own state and on `per`.
+template <typename A>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_pauli_group_batch(const A* __restrict__ st, uint32_t n, uint32_t c, uint32_t d,
+                        const uint64_t* __restrict__ span, uint64_t free_mask, const GroupTerm* __restrict__ terms,
+                        uint32_t nterms, uint64_t bindings, uint32_t per, double* __restrict__ partials) {
+    extern __shared__ __align__(16) unsigned char gsm[];
+    __shared__ GroupShared g;
+    const uint32_t tile_amps = 1u << (c + d);
+    A* buf0 = reinterpret_cast<A*>(gsm);
+    A* buf1 = buf0 + tile_amps;
+    group_setup(g, c, d, span, terms, nterms);
+    const uint64_t ncosets = uint64_t{1} << (n - c - d);
+    const uint32_t slot = blockIdx.x % per;
+    const uint64_t b0 = blockIdx.x / per, bstep = gridDim.x / per;
+    if (b0 >= bindings) return;  // (uniform over the CTA)
+    // This CTA's cosets in each binding, and its work items in order:
+    // item f = (binding b0 + (f / mine) * bstep, coset slot + (f % mine) * per).
+    const uint64_t mine = ncosets > slot ? (ncosets - slot + per - 1) / per : 0;
+    const uint64_t nb = (bindings - b0 + bstep - 1) / bstep;
+    double acc0[kMaxGroupTerms], acc1[kMaxGroupTerms];
 #pragma unroll
     for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
-        if (t < nterms) {
-            double r = __dadd_rn(acc0[t], acc1[t]);
-            for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
-            __syncthreads();
-            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double sum = 0.0;
-                for (int w = 0; w < kThreads / 32; ++w) sum += red[w];
-                double* p = partials + 2 * (static_cast<uint64_t>(terms[t].out) * gridDim.x + blockIdx.x);
-                const uint32_t mode = tmode[t];
-                p[0] = mode == 0 ? sum : mode == 1 ? 2.0 * sum : 0.0;
-                p[1] = mode == 2 ? -2.0 * sum : 0.0;
-            }
+        acc0[t] = 0.0;
+        acc1[t] = 0.0;
+    }
+    auto write = [&](uint64_t b) {
+        group_write(g, terms, nterms, acc0, acc1, [&](uint32_t out) {
+            return partials + 2 * ((static_cast<uint64_t>(out) * bindings + b) * per + slot);
+        });
+    };
+    if (mine == 0) {  // more slots than cosets: this slot's partials are zero
+        for (uint64_t i = 0; i < nb; ++i) write(b0 + i * bstep);
+        return;
+    }
+    const uint64_t items = nb * mine;
+    auto item = [&](uint64_t f, uint64_t& b, uint64_t& rep) {
+        b = b0 + (f / mine) * bstep;
+        rep = deposit_bits(slot + (f % mine) * per, free_mask);
+    };
+    uint64_t b = 0, rep = 0;
+    item(0, b, rep);
+    group_gather(st + (b << n), rep, buf0, g, c, tile_amps);
+    A* cur = buf0;
+    A* nxt = buf1;
+    for (uint64_t f = 0; f < items; ++f) {
+        uint64_t bn = 0, repn = 0;
+        if (f + 1 < items) {
+            item(f + 1, bn, repn);
+            group_gather(st + (bn << n), repn, nxt, g, c, tile_amps);
+        } else {
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
         }
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        __syncthreads();
+        group_tile(g, cur, rep, c, tile_amps, nterms, acc0, acc1);
+        __syncthreads();  // this buffer is the target of the gather after next
+        if ((f + 1) % mine == 0) write(b);
+        b = bn;
+        rep = repn;
+        A* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// <H> per binding: sum over terms in term order of coef * Re(i^popcount(x&z)
+// * (sum over the binding's slots, in slot order, of the partials)).
+__global__ void k_batch_group_finish(const double* __restrict__ partials, uint64_t bindings, uint32_t per,
+                                     const uint64_t* __restrict__ xs, const uint64_t* __restrict__ zs,
+                                     const double* __restrict__ coefs, uint32_t num_terms, double* __restrict__ out) {
+    for (uint64_t b = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < bindings;
+         b += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        double total = 0.0;
+        for (uint32_t t = 0; t < num_terms; ++t) {
+            const double* p = partials + 2 * ((static_cast<uint64_t>(t) * bindings + b) * per);
+            double re = 0.0, im = 0.0;
+            for (uint32_t s = 0; s < per; ++s) {
+                re += p[2 * s];
+                im += p[2 * s + 1];
+            }
+            const int ph = __popcll(xs[t] & zs[t]) & 3;
+            total += coefs[t] * (ph == 0 ? re : ph == 1 ? -im : ph == 2 ? -re : im);
+        }
+        out[b] = total;
     }
 }
 
@@ -325,6 +456,49 @@ int launch_pauli_group(const void* amps, uint32_t n, uint32_t c, uint32_t d, con
     else
         k_pauli_group<double2><<<grid, kThreads, smem, s>>>(static_cast<const double2*>(amps), c, d, dev_span,
                                                             free_mask, terms, nterms, ncosets, dev_partials);
+    note_launches(1);
+    return launch_status();
+}
+
+int launch_pauli_group_batch(const void* amps, uint32_t n, uint32_t c, uint32_t d, const uint64_t* dev_span,
+                             uint64_t free_mask, const void* dev_terms, uint32_t nterms, uint64_t bindings,
+                             uint32_t per, double* dev_partials, int sm_count, void* stream, int precision) {
+    if (nterms == 0) return MB2_OK;
+    if (nterms > kMaxGroupTerms || c + d > kPauliTileQubits || d > kPauliMaxSpan || c + d > n || per == 0 ||
+        c + d < kPauliMinTileQubits)
+        return MB2_ERR_INVALID;
+    const size_t smem = 2 * (size_t{1} << (c + d)) * (precision == MB2_C64 ? sizeof(float2) : sizeof(double2));
+    static const bool attr = [] {  // once, thread-safe
+        return cudaFuncSetAttribute(k_pauli_group_batch<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    128 * 1024) == cudaSuccess &&
+               cudaFuncSetAttribute(k_pauli_group_batch<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    128 * 1024) == cudaSuccess;
+    }();
+    if (!attr) return launch_status();
+    // Two CTAs per SM, a multiple of `per`, no more binding lanes than bindings.
+    uint64_t lanes = std::max<uint64_t>(1, (2ull * static_cast<uint64_t>(sm_count)) / per);
+    lanes = std::min<uint64_t>(lanes, bindings);
+    const unsigned grid = static_cast<unsigned>(lanes * per);
+    const auto s = static_cast<cudaStream_t>(stream);
+    const auto* terms = static_cast<const GroupTerm*>(dev_terms);
+    if (precision == MB2_C64)
+        k_pauli_group_batch<float2><<<grid, kThreads, smem, s>>>(static_cast<const float2*>(amps), n, c, d, dev_span,
+                                                                 free_mask, terms, nterms, bindings, per, dev_partials);
+    else
+        k_pauli_group_batch<double2><<<grid, kThreads, smem, s>>>(static_cast<const double2*>(amps), n, c, d,
+                                                                  dev_span, free_mask, terms, nterms, bindings, per,
+                                                                  dev_partials);
+    note_launches(1);
+    return launch_status();
+}
+
+int launch_batch_group_finish(const double* dev_partials, uint64_t bindings, uint32_t per, const uint64_t* dev_x,
+                              const uint64_t* dev_z, const double* dev_coefs, uint32_t num_terms, double* dev_out,
+                              void* stream) {
+    const uint64_t blocks = (bindings + 127) / 128;
+    k_batch_group_finish<<<static_cast<unsigned>(blocks < 1024 ? blocks : 1024), 128, 0,
+                           static_cast<cudaStream_t>(stream)>>>(dev_partials, bindings, per, dev_x, dev_z, dev_coefs,
+                                                                num_terms, dev_out);
     note_launches(1);
     return launch_status();
 }

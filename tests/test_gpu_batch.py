@@ -71,3 +71,20 @@ def test_batch_complex64_within_tolerance(ctx):
     assert stats.parametric_blocks > 0
     assert np.max(np.abs(lo - hi)) <= 1e-6
     assert np.max(np.abs(s_lo - s_hi)) <= 1e-5
+
+
+@pytest.mark.parametrize("n", [11, 12])
+def test_batch_grouped_expectation_many_bindings(ctx, ref, n):
+    # More bindings than the grouped reduction has binding lanes (each lane
+    # takes several bindings in turn), at the smallest grouped sizes (one and
+    # two CTAs per binding).
+    layers, B = 3, 333
+    rows = workloads.hea_bindings(n, layers, B, 400 + n)
+    paulis = workloads.pauli_strings(n, 32, 401 + n)
+    coefs = workloads.weights(32, 402 + n)
+    vals, _, _ = sweep_batch(ctx, workloads.hea(n, layers, 0), rows, paulis, coefs)
+    for b in (0, 1, 147, 295, 296, 297, 332):
+        c = as_oracle_circuit(bound_circuit(n, layers, rows[b]))
+        r = ref.run(c, fuse_gates=True, paulis=paulis)
+        h = sum(w * t for w, t in zip(coefs, r["terms"]))
+        assert abs(vals[b] - h.real) <= 1e-11, (b, vals[b], h)
