@@ -126,12 +126,21 @@ __device__ __forceinline__ void diag_regs(float2 (&a)[kNA], const float* md, uin
         if (P1 < 0 && k > 1 && ((e >> 1) & 1u) != v1) continue;
         const uint32_t c = (cls >> (2 * e)) & 3u;
         if (c == 0u) continue;
+        if (c == 1u) {  // -1: sign flips only
+#pragma unroll
+            for (int j = 0; j < kNA; ++j) {
+                if (P0 >= 0 && ((j >> (P0 < 0 ? 0 : P0)) & 1) != static_cast<int>(e & 1u)) continue;
+                if (P1 >= 0 && ((j >> (P1 < 0 ? 0 : P1)) & 1) != static_cast<int>((e >> 1) & 1u)) continue;
+                a[j] = fneg_if(a[j], 1u);
+            }
+            continue;
+        }
         const Cf d = entry(md, e);
 #pragma unroll
         for (int j = 0; j < kNA; ++j) {
             if (P0 >= 0 && ((j >> (P0 < 0 ? 0 : P0)) & 1) != static_cast<int>(e & 1u)) continue;
             if (P1 >= 0 && ((j >> (P1 < 0 ? 0 : P1)) & 1) != static_cast<int>((e >> 1) & 1u)) continue;
-            a[j] = c == 1u ? fneg_if(a[j], 1u) : cmulf(d, a[j]);
+            a[j] = cmulf(d, a[j]);
         }
     }
 }

@@ -105,9 +105,41 @@ void encode_compact(TileProgram& prog) {
         auto& w = prog.words;
         bool heavy = false;
         uint32_t reg[kRegQubits] = {0, 1, 2, 3};
-        // Pending sign monomials (canonical words), toggled so pairs cancel.
+        // A diagonal of at most two operands by entry class.
+        auto emit_dsmall = [&](const TileInstr& g, uint32_t off) {
+            const uint32_t c0 = g.pos[4], c1 = g.pos[5];
+            const bool r0 = (c0 & 0x80u) != 0, r1 = (c1 & 0x80u) != 0;
+            const uint32_t cls = g.aux & 255u;
+            if (g.k == 1) {
+                if (r0) w.push_back(header(cop::kDs1R + (c0 & 3u), cls, 0, off));
+                else w.push_back(header(cop::kDs1T, cls, c0, off));
+            } else if (r0 && r1) {
+                w.push_back(header(cop::kDs2RR + pair_index(c0 & 3u, c1 & 3u), cls, 0, off));
+            } else if (r0) {
+                w.push_back(header(cop::kDs2RT + 2 * (c0 & 3u) + 1, cls, c1, off));
+            } else if (r1) {
+                w.push_back(header(cop::kDs2RT + 2 * (c1 & 3u), cls, c0, off));
+            } else {
+                w.push_back(header(cop::kDs2TT, cls, 0, off));
+                w.push_back(c0 | (c1 << 4));
+            }
+        };
+        // Pending sign monomials (canonical words), toggled so pairs cancel,
+        // and the +-1 diagonals they come from.
         std::map<uint32_t, bool> signs;
+        std::vector<const TileInstr*> sign_run;
         auto flush_signs = [&]() {
+            if (sign_run.size() == 1 && sign_run[0]->kind == TK_DSMALL) {
+                // A lone +-1 diagonal of at most two operands keeps its
+                // entry-class instruction: it negates only the amplitudes it
+                // selects, where a sign instruction passes over all 16.
+                const TileInstr& g = *sign_run[0];
+                signs.clear();
+                sign_run.clear();
+                emit_dsmall(g, data_off(g));
+                return;
+            }
+            sign_run.clear();
             std::vector<uint32_t> live;
             for (const auto& [mono, on] : signs)
                 if (on) live.push_back(mono);
@@ -162,6 +194,7 @@ void encode_compact(TileProgram& prog) {
                     uint32_t pos[8];
                     for (uint32_t t = 0; t < g.k; ++t) pos[t] = g.pos[t];
                     add_signs(g.k, pos, neg);
+                    sign_run.push_back(&g);
                     continue;
                 }
             }
@@ -247,22 +280,7 @@ void encode_compact(TileProgram& prog) {
                 }
                 case TOP_DIAG: {
                     if (g.kind == TK_DSMALL) {
-                        const uint32_t c0 = g.pos[4], c1 = g.pos[5];
-                        const bool r0 = (c0 & 0x80u) != 0, r1 = (c1 & 0x80u) != 0;
-                        const uint32_t cls = g.aux & 255u;
-                        if (g.k == 1) {
-                            if (r0) w.push_back(header(cop::kDs1R + (c0 & 3u), cls, 0, off));
-                            else w.push_back(header(cop::kDs1T, cls, c0, off));
-                        } else if (r0 && r1) {
-                            w.push_back(header(cop::kDs2RR + pair_index(c0 & 3u, c1 & 3u), cls, 0, off));
-                        } else if (r0) {
-                            w.push_back(header(cop::kDs2RT + 2 * (c0 & 3u) + 1, cls, c1, off));
-                        } else if (r1) {
-                            w.push_back(header(cop::kDs2RT + 2 * (c1 & 3u), cls, c0, off));
-                        } else {
-                            w.push_back(header(cop::kDs2TT, cls, 0, off));
-                            w.push_back(c0 | (c1 << 4));
-                        }
+                        emit_dsmall(g, off);
                     } else {
                         heavy = true;
                         uint32_t packed = 0;
