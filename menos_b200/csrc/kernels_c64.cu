@@ -157,9 +157,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // `stages - 1` ahead in flight, masked-add tile bases, the pass's words and
 // data staged in shared memory, a batch's parametric slice per tile) with
 // FP32 gates.  MT > 0 fixes the tile width; IDX is the index type.
-// FULL = false: the lean variant without register-moving and rare heavy
-// instructions (as the complex128 kernel's), for passes without them.
-template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
+// V: 0 the lean variant without register-moving and rare heavy
+// instructions (as the complex128 kernel's), for passes without them;
+// 1 adds general dense two-qubit blocks (ansatz layers) and nothing else;
+// 2 the full set.
+template <int MAXT, int MINB, int MT, typename IDX, int V>
 __global__ void __launch_bounds__(MAXT, MINB)
     k_tile_pass_c64(float2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask,
                     const uint32_t* __restrict__ words, uint32_t nwords, const double* __restrict__ sdata,
@@ -312,11 +314,11 @@ __global__ void __launch_bounds__(MAXT, MINB)
                             g1<1, 1>(a, md + 8);
                             g1<2, 1>(a, md + 16);
                             break;
-                        MB2_CASE12(cop::kGen2, if constexpr (FULL) g2<P0, P1>(a, md))
-                        MB2_CASE12(cop::kMono2, if constexpr (FULL) { ++pc; g2<P0, P1>(a, md); })
-                        MB2_CASE12(cop::kSw12, if constexpr (FULL) perm2<P0, P1, TK_SW12>(a))
-                        MB2_CASE12(cop::kSw13, if constexpr (FULL) perm2<P0, P1, TK_SW13>(a))
-                        MB2_CASE12(cop::kSw23, if constexpr (FULL) perm2<P0, P1, TK_SW23>(a))
+                        MB2_CASE12(cop::kGen2, if constexpr (V >= 1) g2<P0, P1>(a, md))
+                        MB2_CASE12(cop::kMono2, if constexpr (V == 2) { ++pc; g2<P0, P1>(a, md); })
+                        MB2_CASE12(cop::kSw12, if constexpr (V == 2) perm2<P0, P1, TK_SW12>(a))
+                        MB2_CASE12(cop::kSw13, if constexpr (V == 2) perm2<P0, P1, TK_SW13>(a))
+                        MB2_CASE12(cop::kSw23, if constexpr (V == 2) perm2<P0, P1, TK_SW23>(a))
                         MB2_CASE4(cop::kDs1R, (diag_regs<P, -1>(a, md, 1, aux, 0u, 0u)))
                         MB2_CASE12(cop::kDs2RR, (diag_regs<P0, P1>(a, md, 2, aux, 0u, 0u)))
 #undef MB2_CASE4
@@ -351,7 +353,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
                             }
                         } break;
                         default: {  // cop::kDiagK: entry per amplitude
-                            if constexpr (!FULL) break;
+                            if constexpr (V != 2) break;
                             const uint32_t pos = sw[pc++];
                             uint32_t et = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
                             for (uint32_t b = 0; b < aux; ++b) {
@@ -374,7 +376,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 #pragma unroll
                 for (int j = 0; j < kNA; ++j) at(j) = a[j];
                 __syncthreads();
-            } else if (FULL && op0 == cop::kSmem) {
+            } else if (V == 2 && op0 == cop::kSmem) {
                 const uint32_t k = (w0 >> 8) & 0xffu, dim = 1u << k;
                 const uint32_t pos = sw[pc + 1];
                 const double* md = gdata + sw[pc + 2];
@@ -413,7 +415,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
 }
 
-template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
+template <int MAXT, int MINB, int MT, typename IDX, int V>
 int launch_c64_instance(const TileLaunch& L) {
     // The dynamic limit is what the static shared memory leaves of the
     // per-block maximum; it is raised once, by whichever thread launches
@@ -421,16 +423,16 @@ int launch_c64_instance(const TileLaunch& L) {
     // initialisation is thread-safe and every thread sees it complete).
     static const size_t dyn_max = [] {
         cudaFuncAttributes fa{};
-        if (cudaFuncGetAttributes(&fa, k_tile_pass_c64<MAXT, MINB, MT, IDX, FULL>) != cudaSuccess) return size_t{0};
+        if (cudaFuncGetAttributes(&fa, k_tile_pass_c64<MAXT, MINB, MT, IDX, V>) != cudaSuccess) return size_t{0};
         const size_t v = kTileSmemMax - fa.sharedSizeBytes;
-        if (cudaFuncSetAttribute(k_tile_pass_c64<MAXT, MINB, MT, IDX, FULL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_tile_pass_c64<MAXT, MINB, MT, IDX, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(v)) != cudaSuccess)
             return size_t{0};
         return v;
     }();
     if (dyn_max == 0) return launch_status();
     if (L.smem > dyn_max) return MB2_ERR_INVALID;
-    k_tile_pass_c64<MAXT, MINB, MT, IDX, FULL><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
+    k_tile_pass_c64<MAXT, MINB, MT, IDX, V><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
         static_cast<float2*>(L.amps), L.n_all, L.m, L.smask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata, L.ntiles,
         L.pdata, L.pstride, L.param_lo, L.param_len, L.bshift, L.stages);
     return launch_status();
@@ -483,20 +485,26 @@ int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uin
     const uint64_t cap = static_cast<uint64_t>(sm_count) * (pass.m == kMaxTileQubitsC64 ? 1u : 2u);
     L.grid = static_cast<int>(L.ntiles < cap ? L.ntiles : cap);
     int rc;
-    if (pass.m == kMaxTileQubitsC64 && !pass.heavy)
-        rc = L.n_all <= 32 ? launch_c64_instance<512, 1, 13, uint32_t, false>(L)
-                           : launch_c64_instance<512, 1, 13, uint64_t, false>(L);
-    else if (pass.m == kMaxTileQubitsC64)
-        rc = L.n_all <= 32 ? launch_c64_instance<512, 1, 13, uint32_t, true>(L)
-                           : launch_c64_instance<512, 1, 13, uint64_t, true>(L);
-    else if (pass.m == 12 && !pass.heavy)
-        rc = L.n_all <= 32 ? launch_c64_instance<256, 2, 12, uint32_t, false>(L)
-                           : launch_c64_instance<256, 2, 12, uint64_t, false>(L);
-    else if (pass.m == 12)
-        rc = L.n_all <= 32 ? launch_c64_instance<256, 2, 12, uint32_t, true>(L)
-                           : launch_c64_instance<256, 2, 12, uint64_t, true>(L);
-    else
-        rc = launch_c64_instance<512, 1, 0, uint64_t, true>(L);
+    // Variant: lean, lean + dense two-qubit blocks, or full (TilePass::heavy/mid).
+    const int v = !pass.heavy ? 0 : pass.mid ? 1 : 2;
+    const bool i32 = L.n_all <= 32;
+    if (pass.m == kMaxTileQubitsC64) {
+        if (v == 0)
+            rc = i32 ? launch_c64_instance<512, 1, 13, uint32_t, 0>(L) : launch_c64_instance<512, 1, 13, uint64_t, 0>(L);
+        else if (v == 1)
+            rc = i32 ? launch_c64_instance<512, 1, 13, uint32_t, 1>(L) : launch_c64_instance<512, 1, 13, uint64_t, 1>(L);
+        else
+            rc = i32 ? launch_c64_instance<512, 1, 13, uint32_t, 2>(L) : launch_c64_instance<512, 1, 13, uint64_t, 2>(L);
+    } else if (pass.m == 12) {
+        if (v == 0)
+            rc = i32 ? launch_c64_instance<256, 2, 12, uint32_t, 0>(L) : launch_c64_instance<256, 2, 12, uint64_t, 0>(L);
+        else if (v == 1)
+            rc = i32 ? launch_c64_instance<256, 2, 12, uint32_t, 1>(L) : launch_c64_instance<256, 2, 12, uint64_t, 1>(L);
+        else
+            rc = i32 ? launch_c64_instance<256, 2, 12, uint32_t, 2>(L) : launch_c64_instance<256, 2, 12, uint64_t, 2>(L);
+    } else {
+        rc = launch_c64_instance<512, 1, 0, uint64_t, 2>(L);
+    }
     note_launches(1);
     return rc;
 }

@@ -119,6 +119,7 @@ struct TilePass {
     uint32_t param_lo = 0;
     uint32_t param_len = 0;
     bool heavy = false;  // has two-qubit dense/monomial/permutation, kDiagK or kSmem words
+    bool mid = false;    // heavy, but only through general dense two-qubit words (kGen2)
 };
 
 // Compact instruction stream of the complex128 tile kernel, written from the

@@ -103,7 +103,7 @@ void encode_compact(TileProgram& prog) {
             return is_param(g) ? pass.sdata_count + (g.data - pass.param_lo) : g.data;
         };
         auto& w = prog.words;
-        bool heavy = false;
+        bool heavy = false, heavy_other = false;  // other: beyond general dense 2q
         uint32_t reg[kRegQubits] = {0, 1, 2, 3};
         // A diagonal of at most two operands by entry class.
         auto emit_dsmall = [&](const TileInstr& g, uint32_t off) {
@@ -234,7 +234,7 @@ void encode_compact(TileProgram& prog) {
                     w.push_back(cop::kEnd);
                     break;
                 case TOP_SMEM: {
-                    heavy = true;
+                    heavy = heavy_other = true;
                     uint32_t packed = 0;
                     for (uint32_t t = 0; t < g.k; ++t) packed |= static_cast<uint32_t>(g.pos[t]) << (4 * t);
                     w.push_back(cop::kSmem | (static_cast<uint32_t>(g.k) << 8));
@@ -266,6 +266,7 @@ void encode_compact(TileProgram& prog) {
                 case TOP_G2: {
                     heavy = true;  // permutations and monomials move registers: full variant
                     const uint32_t pr = pair_index(g.pos[0], g.pos[1]);
+                    if (g.kind != TK_GEN) heavy_other = true;
                     switch (g.kind) {
                         case TK_SW12: w.push_back(header(cop::kSw12 + pr, 0, 0, 0)); break;
                         case TK_SW13: w.push_back(header(cop::kSw13 + pr, 0, 0, 0)); break;
@@ -282,7 +283,7 @@ void encode_compact(TileProgram& prog) {
                     if (g.kind == TK_DSMALL) {
                         emit_dsmall(g, off);
                     } else {
-                        heavy = true;
+                        heavy = heavy_other = true;
                         uint32_t packed = 0;
                         for (uint32_t t = 0; t < g.k; ++t) packed |= static_cast<uint32_t>(g.pos[t]) << (4 * t);
                         w.push_back(header(cop::kDiagK, g.k, 0, off));
@@ -297,6 +298,7 @@ void encode_compact(TileProgram& prog) {
         flush_signs();
         fuse_u3_runs(w, pass.word_begin);
         pass.heavy = heavy;
+        pass.mid = heavy && !heavy_other;
         while (w.size() & 3u) w.push_back(cop::kEnd);  // 16-byte multiple: the staged data follows
         pass.word_count = static_cast<uint32_t>(w.size()) - pass.word_begin;
     }
