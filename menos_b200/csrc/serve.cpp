@@ -189,6 +189,17 @@ int mb2_server_create(mb2_context* ctx, const mb2_server_options* opts, mb2_serv
         }
         s->streams.push_back(st);
     }
+    // The admission budget is mapped into the device's stream-ordered pool
+    // once, up front (the pool keeps freed memory, and the server gives it
+    // back when it is destroyed): requests then take memory that is already
+    // mapped, instead of the first ones mapping fresh memory while others
+    // run.  A budget the pool cannot map at once is simply not warmed.
+    {
+        void* p = nullptr;
+        if (cudaMallocAsync(&p, s->budget, s->streams[0]) == cudaSuccess) cudaFreeAsync(p, s->streams[0]);
+        else cudaGetLastError();
+        cudaStreamSynchronize(s->streams[0]);
+    }
     for (uint32_t i = 0; i < slots; ++i) s->workers.emplace_back(worker, s, i);
     *out = s;
     return MB2_OK;
@@ -286,6 +297,9 @@ int mb2_server_destroy(mb2_server* s) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
     }
+    // Return the pool's unused memory (the warmed budget) to the device.
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, mb2::context_device(s->ctx)) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
     delete s;
     return MB2_OK;
 }
