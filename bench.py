@@ -75,6 +75,8 @@ def parse():
     p.add_argument("--terms", type=int, default=64)
     p.add_argument("--tile", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--validate-cpu", action="store_true",
+                   help="with --impl reference: the extrapolated CPU job time against a whole reference run")
     p.add_argument("--mode", default="job", choices=["job", "serve", "batch", "c64"])
     p.add_argument("--requests", type=int, default=600)
     p.add_argument("--load", type=float, default=4.0, help="serve: arrival rate / plain-loop capacity")
@@ -172,9 +174,11 @@ def cpu_reference_sample(n, circ, paulis, shots, seed):
     import pyoracle
     ref = pyoracle.RefLib()
     threads = ref.default_threads()
-    state = np.zeros(1 << n, np.complex128)
+    state = np.empty(1 << n, np.complex128)
+    state.fill(0.0)  # every page touched before anything is timed
     state[0] = 1.0
-    # U3 and CZ timings from one brick layer; CP / H / SWAP timed once each.
+    # U3 and CZ timings from one brick layer; CP / H / SWAP timed once each;
+    # each gate applied twice and the second (warm) application timed.
     per_kind = {}
     sample_ops = circ.ops[:n + n // 2]
     extra = []
@@ -185,6 +189,7 @@ def cpu_reference_sample(n, circ, paulis, shots, seed):
                 break
     for oc, qs, ps, _m, _c in sample_ops + extra:
         m = ref.gate_matrix(oc, list(ps) + [0.0] * (3 - len(ps)))
+        ref.apply_matrix(state, m, list(qs), threads=threads)
         t0 = time.perf_counter()
         ref.apply_matrix(state, m, list(qs), threads=threads)
         per_kind.setdefault(oc, []).append(time.perf_counter() - t0)
@@ -580,9 +585,34 @@ def main_c64(args, local):
     print(json.dumps(line), flush=True)
 
 
+def validate_cpu_baseline(args):
+    """The extrapolated CPU figure against one whole job run through the
+    reference's DenseEngine::execute (oracle/_ref), both at --qubits (26 by
+    default for this check: a full 30-qubit run takes hours)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from menos_b200 import workloads
+    n = args.qubits
+    circ = workloads.config_c2(n=n, depth=args.depth)
+    paulis = workloads.pauli_strings(n, args.terms, 7)
+    v, detail, cores, sampled = cpu_reference_sample(n, circ, paulis, args.shots, 1234)
+    ref = pyoracle.RefLib()
+    oc = pyoracle.Circuit(n)
+    oc.ops = list(circ.ops)
+    t0 = time.perf_counter()
+    ref.run(oc, fuse_gates=True, statevector=False, shots=args.shots, seed=1234,
+            targets=[(q, q) for q in range(n)], width=n, paulis=[(0, 0)] + list(paulis))
+    whole = time.perf_counter() - t0
+    print(json.dumps({"check": "cpu baseline extrapolation vs whole DenseEngine::execute", "qubits": n,
+                      "extrapolated_s": round(1.0 / v, 3), "measured_s": round(whole, 3),
+                      "ratio": round((1.0 / v) / whole, 3), "threads": cores, "detail": detail}), flush=True)
+
+
 def main_reference(args, rank, world):
     if rank != 0:
         return
+    if args.validate_cpu:
+        return validate_cpu_baseline(args)
     from menos_b200 import workloads
     n = args.qubits
     circ = workloads.config_c2(n=n, depth=args.depth)

@@ -178,8 +178,11 @@ int mb2_expectation(mb2_state* state, const uint64_t* x_masks, const uint64_t* z
  * num_terms above MB2_NOALLOC_MAX_TERMS returns MB2_ERR_RESOURCE and does
  * nothing.  The first call on a device looks the array's device address up
  * (cudaGetSymbolAddress, with that device current); make it before any
- * stream capture.  Calls share the one array: calls that overlap on the GPU
- * (on different streams) race.  Synchronous.  No counterpart in the
+ * stream capture.  After a device reset the kept address is stale: the next
+ * call sees its first copy refused and looks the address up again.  Calls
+ * share the one array: calls that overlap on the GPU (on different streams)
+ * race.  A CUDA failure returns MB2_ERR_CUDA with its message kept for the
+ * thread, as for launches.  Synchronous.  No counterpart in the
  * reference, which allocates its partial sums per term
  * (src/kernels/cuda/dense_kernels.cu:378-399). */
 #define MB2_NOALLOC_MAX_TERMS 64
@@ -199,6 +202,14 @@ int mb2_normalize(mb2_state* state, double* norm_before);
  * outcomes/counts, out: distinct outcomes written.  Synchronous. */
 int mb2_sample(mb2_state* state, uint64_t shots, uint64_t seed, const uint32_t* targets,
                uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes);
+/* For each uniform (any order, each in [0, 1)), the basis state a draw of it
+ * lands on: the first index whose sequential FP64 cumulative sum of |a|^2
+ * exceeds it, the last index when none does.  The answers of the reference's
+ * CumulativeDistribution::sample_one(double) for a region's state
+ * (src/engines/dense/cumulative_distribution.cpp:3-124), computed on the
+ * device without copying the state back; basis_out[i] belongs to
+ * uniforms[i].  Synchronous. */
+int mb2_sample_basis(mb2_state* state, const double* uniforms, uint64_t n, uint64_t* basis_out);
 /* Copies the amplitudes to host memory (interleaved; 2 doubles or 2 floats
  * per amplitude by precision).  Replaces: DeviceBuffer::copy_to_host
  * (src/kernels/cuda/device_buffer.cpp:60-63).  Synchronous. */

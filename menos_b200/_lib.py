@@ -120,6 +120,7 @@ SIGNATURES = {
     "mb2_norm": (C.c_int, [_VP, C.POINTER(C.c_double)]),
     "mb2_normalize": (C.c_int, [_VP, C.POINTER(C.c_double)]),
     "mb2_sample": (C.c_int, [_VP, C.c_uint64, C.c_uint64, _VP, C.c_uint32, _VP, _VP, C.POINTER(C.c_uint64)]),
+    "mb2_sample_basis": (C.c_int, [_VP, _VP, C.c_uint64, _VP]),
     "mb2_copy_out": (C.c_int, [_VP, _VP, C.c_uint64]),
     "mb2_copy_in": (C.c_int, [_VP, _VP, C.c_uint64]),
     "mb2_synchronize": (C.c_int, [_VP]),

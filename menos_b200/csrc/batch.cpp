@@ -172,6 +172,12 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
                 m00_real = m00_real && acc[w][4 * i + 2];
                 all_diag = all_diag && acc[w][4 * i + 3];
             }
+            // A block that is diagonal for some bindings only (an angle of 0)
+            // runs through the dense path for every binding.  For such a
+            // binding each output is d*a plus products with exactly-zero
+            // entries: the diagonal kernel's value except possibly for the
+            // sign of a zero result, and every stored zero is canonical (+0)
+            // on both paths, so the state's bits are the same.
             shape[i].diagonal = shape[i].diagonal && all_diag;
             if (differs) {
                 flags[i] = mb2::kParamBlock | (all_real ? mb2::kParamAllReal : 0) | (m00_real ? mb2::kParamM00Real : 0);
@@ -250,8 +256,10 @@ extern "C" int mb2_sweep_batch(mb2_context* ctx, const mb2_op* ops, uint32_t num
 
     // ---- device
     Runner r{0};
-    int dev = 0;
-    cudaGetDevice(&dev);
+    // Everything below runs on the context's device, whichever device the
+    // calling thread had selected.
+    const int dev = mb2::context_device(ctx);
+    if (cudaSetDevice(dev) != cudaSuccess) return MB2_ERR_CUDA;
     if (cudaStreamCreateWithFlags(&r.stream, cudaStreamNonBlocking) != cudaSuccess) return MB2_ERR_CUDA;
     const size_t state_bytes = (size_t{num_bindings} << num_qubits) * (c64 ? 8 : sizeof(mb2::Cd));
     auto al = [](size_t v) { return (v + 255) & ~size_t{255}; };

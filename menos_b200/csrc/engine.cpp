@@ -101,6 +101,27 @@ int check_operands(mb2_state* s, const uint32_t* q, uint32_t k) {
     return MB2_OK;
 }
 
+// The reference's walk (src/engines/dense/sample.cpp:55-69), reproduced
+// exactly on the device: basis[i] = the first basis state whose sequential
+// FP64 cumulative |a|^2 exceeds the sorted uniform u[i] (the last state when
+// none does).  Synchronous.
+int walk_sorted(mb2_state* s, const std::vector<double>& u, uint64_t* basis) {
+    const uint64_t shots = u.size();
+    const size_t al_u = (shots * 8 + 255) & ~size_t{255};
+    const size_t need = 2 * al_u + mb2::sample_scratch_bytes(s->n, shots);
+    if (int e = ensure_scratch(s, need); e != MB2_OK) return e;
+    auto* base = static_cast<unsigned char*>(s->scratch);
+    auto* dev_u = reinterpret_cast<double*>(base);
+    auto* dev_basis = reinterpret_cast<uint64_t*>(base + al_u);
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(dev_u, u.data(), shots * 8, cudaMemcpyHostToDevice, s->stream));
+    const int rc =
+        mb2::launch_sample(s->amps, s->n, dev_u, shots, base + 2 * al_u, dev_basis, s->stream, s->precision);
+    if (rc != MB2_OK) return fail(s->ctx, rc, std::string("sample launch: ") + mb2::last_cuda_error_string());
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(basis, dev_basis, shots * 8, cudaMemcpyDeviceToHost, s->stream));
+    MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+    return MB2_OK;
+}
+
 // One block through the per-gate kernels (the reference's apply_matrix
 // dispatch, src/kernels/cpu/dense_kernels.cpp:427-463: diagonal, 1q, 2q,
 // generic).
@@ -147,6 +168,28 @@ uint32_t tile_width(uint32_t requested, uint32_t n, const std::vector<mb2::Block
 }  // namespace
 
 namespace mb2 {
+uint64_t scratch_bound(uint32_t n, const mb2_op* ops, uint32_t num_ops, uint64_t shots, uint32_t terms) {
+    auto up = [](uint64_t v) { return (v + 255) & ~uint64_t{255}; };
+    // The sweep's upload (mb2_apply_program_monitored): per block at most a
+    // phase record, a few gate words and pass padding (144 bytes) and its
+    // matrix (16 * 4^k, staged or global-only); blocks never outnumber ops.
+    uint64_t program = 4 * 256;
+    for (uint32_t i = 0; i < num_ops; ++i)
+        if (ops[i].opcode != MB2_MEASURE) program += 144 + (16ull << (2 * ops[i].num_qubits));
+    // The sampler (walk_sorted): uniforms, per-shot basis, the walk's scratch.
+    const uint64_t sample = shots == 0 ? 0 : 2 * up(8 * shots) + sample_scratch_bytes(n, shots);
+    // The expectation (mb2_expectation): masks, partials, results, the
+    // groups' span vectors (at most 2^kPauliMaxSpan per group) and terms.
+    const uint64_t t = terms;
+    const uint64_t expect = terms == 0 ? 0
+                                       : 2 * up(8 * t) + up(16 * kExpBlocks * t + 16 * t) +
+                                             up(8 * t << kPauliMaxSpan) + sizeof(PauliGroupTerm) * t;
+    const uint64_t need = std::max({program, sample, expect});
+    uint64_t rounded = uint64_t{1} << 20;  // ensure_scratch's power-of-two growth
+    while (rounded < need) rounded <<= 1;
+    return rounded;
+}
+
 int context_device(const mb2_context* ctx) { return ctx == nullptr ? 0 : ctx->device; }
 
 // A state whose work is queued on a stream the caller owns (the serving
@@ -579,20 +622,8 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
         sort_range(0);
         for (auto& th : pool) th.join();
     }
-    // The walk (sample.cpp:55-69), reproduced exactly on the device.
-    const size_t al_u = (shots * 8 + 255) & ~size_t{255};
-    const size_t need = 2 * al_u + mb2::sample_scratch_bytes(s->n, shots);
-    if (int e = ensure_scratch(s, need); e != MB2_OK) return e;
-    auto* base = static_cast<unsigned char*>(s->scratch);
-    auto* dev_u = reinterpret_cast<double*>(base);
-    auto* dev_basis = reinterpret_cast<uint64_t*>(base + al_u);
-    MB2_CUDA(s->ctx, cudaMemcpyAsync(dev_u, u.data(), shots * 8, cudaMemcpyHostToDevice, s->stream));
-    const int rc =
-        mb2::launch_sample(s->amps, s->n, dev_u, shots, base + 2 * al_u, dev_basis, s->stream, s->precision);
-    if (rc != MB2_OK) return fail(s->ctx, rc, std::string("sample launch: ") + mb2::last_cuda_error_string());
     std::vector<uint64_t> basis(shots);
-    MB2_CUDA(s->ctx, cudaMemcpyAsync(basis.data(), dev_basis, shots * 8, cudaMemcpyDeviceToHost, s->stream));
-    MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+    if (int e = walk_sorted(s, u, basis.data()); e != MB2_OK) return e;
     // Outcomes through the measure targets, ascending, with counts.  The walk
     // gives non-decreasing basis indices (sorted uniforms against the
     // cumulative sum), so runs are counted first; the distinct outcomes are
@@ -643,6 +674,24 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
         ++d;
     }
     *num_outcomes = d;
+    return MB2_OK;
+}
+
+int mb2_sample_basis(mb2_state* s, const double* uniforms, uint64_t n, uint64_t* basis_out) {
+    if (s == nullptr || (n != 0 && (uniforms == nullptr || basis_out == nullptr))) return MB2_ERR_INVALID;
+    if (n == 0) return MB2_OK;
+    for (uint64_t i = 0; i < n; ++i)
+        if (!(uniforms[i] >= 0.0 && uniforms[i] < 1.0))
+            return fail(s->ctx, MB2_ERR_INVALID, "uniforms must lie in [0, 1)");
+    // Draw order -> ascending order (ties keep draw order), one walk, back.
+    std::vector<uint64_t> order(n);
+    for (uint64_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return uniforms[a] < uniforms[b]; });
+    std::vector<double> u(n);
+    for (uint64_t i = 0; i < n; ++i) u[i] = uniforms[order[i]];
+    std::vector<uint64_t> basis(n);
+    if (int e = walk_sorted(s, u, basis.data()); e != MB2_OK) return e;
+    for (uint64_t i = 0; i < n; ++i) basis_out[order[i]] = basis[i];
     return MB2_OK;
 }
 

@@ -278,6 +278,14 @@ int launch_status() {
     return MB2_ERR_CUDA;
 }
 
+int record_cuda_error(int cuda_error) {
+    const auto e = static_cast<cudaError_t>(cuda_error);
+    if (e == cudaSuccess) return MB2_OK;
+    cudaGetLastError();  // clear a non-sticky error; the message is kept here
+    t_launch_error = e;
+    return MB2_ERR_CUDA;
+}
+
 const char* last_cuda_error_string() {
     cudaError_t e = t_launch_error;
     t_launch_error = cudaSuccess;

@@ -574,17 +574,20 @@ unsigned char* g_noalloc_ptr[kMaxDevices] = {};
 
 // The device address of g_noalloc_scratch on the current device.  In host
 // code the symbol names a host-side stand-in, not device memory, so the
-// address is looked up once per device (with that device current) and kept.
-int noalloc_scratch(unsigned char** out) {
+// address is looked up once per device (with that device current) and kept;
+// `refresh` looks it up again (after a device reset the module is loaded
+// anew and the kept address is stale).
+int noalloc_scratch(unsigned char** out, bool refresh = false) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MB2_ERR_NO_DEVICE;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return MB2_ERR_NO_DEVICE;
+    }
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (g_noalloc_ptr[dev] == nullptr) {
+    if (g_noalloc_ptr[dev] == nullptr || refresh) {
         void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) {
-            cudaGetLastError();
-            return MB2_ERR_CUDA;
-        }
+        if (const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch); e != cudaSuccess)
+            return record_cuda_error(e);
         g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
     }
     *out = g_noalloc_ptr[dev];
@@ -614,15 +617,25 @@ extern "C" int mb2_expectation_noalloc(const void* dev_amps, uint32_t num_qubits
     auto* dout = reinterpret_cast<double*>(base + 2 * kNoAllocMasks + kNoAllocPartials);
     const auto s = static_cast<cudaStream_t>(stream);
     const size_t mb = size_t{num_terms} * sizeof(uint64_t);
-    if (cudaMemcpyAsync(dx, x_masks, mb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(dz, z_masks, mb, cudaMemcpyHostToDevice, s) != cudaSuccess)
-        return MB2_ERR_CUDA;
+    cudaError_t e = cudaMemcpyAsync(dx, x_masks, mb, cudaMemcpyHostToDevice, s);
+    if (e == cudaErrorInvalidValue) {
+        // A kept address from before a device reset: look it up again, once.
+        cudaGetLastError();
+        if (int rc = noalloc_scratch(&base, true); rc != MB2_OK) return rc;
+        dx = reinterpret_cast<uint64_t*>(base);
+        dz = reinterpret_cast<uint64_t*>(base + kNoAllocMasks);
+        partials = reinterpret_cast<double*>(base + 2 * kNoAllocMasks);
+        dout = reinterpret_cast<double*>(base + 2 * kNoAllocMasks + kNoAllocPartials);
+        e = cudaMemcpyAsync(dx, x_masks, mb, cudaMemcpyHostToDevice, s);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dz, z_masks, mb, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return record_cuda_error(e);
     // Every partial and every output slot is written before it is read, so
     // nothing left in the array by an earlier call needs clearing.
     if (launch_expectation(dev_amps, num_qubits, dx, dz, num_terms, partials, dout, stream) != MB2_OK)
         return MB2_ERR_CUDA;
-    if (cudaMemcpyAsync(out, dout, size_t{num_terms} * 2 * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
-        return MB2_ERR_CUDA;
-    return cudaStreamSynchronize(s) == cudaSuccess ? MB2_OK : MB2_ERR_CUDA;
+    e = cudaMemcpyAsync(out, dout, size_t{num_terms} * 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return record_cuda_error(e);
 }
 

@@ -288,6 +288,11 @@ int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uin
                          const BatchLayout* batch = nullptr);
 int launch_scale_c64(void* amps, uint64_t n_amps, float s, void* stream);
 int context_device(const mb2_context* ctx);
+// The most staging memory a state's calls can hold for a sweep of these ops,
+// `shots` counts and `terms` Pauli terms, rounded as the state's grow-only
+// staging buffer rounds its size (engine.cpp): what an admission must charge
+// beside the state itself.
+uint64_t scratch_bound(uint32_t n, const mb2_op* ops, uint32_t num_ops, uint64_t shots, uint32_t terms);
 // A complex128 state on a caller-owned stream (engine.cpp).
 int state_on_stream(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, void* stream, mb2_state** out,
                     int precision = MB2_C128);
@@ -333,6 +338,11 @@ int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const
 // last_cuda_error_string() (which reports and clears it).
 int launch_status();
 const char* last_cuda_error_string();
+// Keeps a failed runtime call's error for last_cuda_error_string() (as
+// launch_status does for launches) and returns MB2_ERR_CUDA; MB2_OK for
+// cudaSuccess.  The error is passed as an int (a cudaError_t value) so that
+// host-only translation units need no CUDA header.
+int record_cuda_error(int cuda_error);
 // Counts kernels this library launched (process-wide; mb2_kernel_launches).
 void note_launches(uint32_t k);
 

@@ -57,14 +57,18 @@ struct Done {
     std::vector<uint64_t> outcomes, counts;
 };
 
+// What a request holds on the device while it runs: its state and the
+// state's staging buffer at its largest (the same layout and rounding the
+// engine's calls use), each allocation rounded up to the stream-ordered
+// pool's 2 MiB granularity.
 uint64_t admission_bytes(const Request& r) {
+    auto pool = [](uint64_t v) { return (v + (2ull << 20) - 1) & ~((2ull << 20) - 1); };
     const uint64_t state = (uint64_t{1} << r.n) * (r.precision == MB2_C64 ? 8 : 16);
-    const uint64_t nchunks = std::max<uint64_t>(1, (uint64_t{1} << r.n) / mb2::kSampleChunk);
-    const uint64_t sampler = r.output == MB2_OUT_COUNTS ? 16 * r.shots + 128 * nchunks : 0;
-    const uint64_t expect = 16ull * mb2::kExpBlocks * std::max<size_t>(1, r.xs.size());
-    // program staging (instructions + matrices), rounded as the state rounds it
-    const uint64_t program = 128ull * r.ops.size() + (1ull << 20);
-    return state + std::max(sampler, expect) + program + (2ull << 20);
+    const uint64_t staging =
+        mb2::scratch_bound(r.n, r.ops.data(), static_cast<uint32_t>(r.ops.size()),
+                           r.output == MB2_OUT_COUNTS ? r.shots : 0,
+                           r.output == MB2_OUT_EXPECTATION ? static_cast<uint32_t>(r.xs.size()) : 0);
+    return pool(state) + pool(staging);
 }
 
 }  // namespace

@@ -1,0 +1,278 @@
+// adapter_harness.cpp -- TEST INFRASTRUCTURE, not product code.
+//
+// Drives the reference-side binding (menos_b200/integration/
+// b200_dense_engine.cpp, the menos::SimulationEngine the reference would
+// register) and the reference's own CPU DenseEngine
+// (src/engines/dense/dense_engine.cpp:333-400) through one request shape, so
+// tests can run the reference's CPU/CUDA differential cases
+// (tests/api/cpu_cuda_differential_test.cpp:132-421) against the adapter
+// itself.  oracle/Makefile links it with the adapter, the reference's CPU
+// engine objects and libmenos_b200.so into oracle/_ref/libmenos_adapter.so.
+//
+//   ah_execute       one EngineExecutionRequest through either engine, under
+//                    an installed MemoryLedger (peaks reported), with an
+//                    optional monitor that abandons at a boundary count; a
+//                    Factorized region's sampler is drawn from with its own Rng
+//   ah_estimate      EngineEstimateRequest through either engine
+//   ah_calibration   measure_b200_calibration()
+#include <chrono>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <span>
+#include <string>
+#include <vector>
+
+#include "common/error.h"
+#include "common/memory_ledger.h"
+#include "common/rng.h"
+#include "engines/dense/dense_engine.h"
+#include "ir/gate_table.h"
+#include "menos/bitstring.h"
+#include "menos/circuit.h"
+#include "menos/observable.h"
+#include "menos/simulation_engine.h"
+#include "plan/cuda_calibration.h"
+
+#include "../include/mb2.h"
+
+namespace menos::engines::dense_b200 {
+const SimulationEngine& b200_dense_engine();
+plan::CudaCalibration measure_b200_calibration();
+}  // namespace menos::engines::dense_b200
+
+namespace {
+
+using C = std::complex<double>;
+
+menos::Operation to_operation(const mb2_op& op) {
+    if (op.opcode == MB2_MEASURE) return menos::MeasureOp{op.qubits[0], op.clbit};
+    std::vector<menos::QubitId> qubits(op.qubits, op.qubits + op.num_qubits);
+    if (op.opcode == MB2_UNITARY) {
+        const std::size_t dim = std::size_t{1} << op.num_qubits;
+        std::vector<C> m(dim * dim);
+        for (std::size_t i = 0; i < dim * dim; ++i) m[i] = C{op.matrix[2 * i], op.matrix[2 * i + 1]};
+        return menos::UnitaryOp{std::move(qubits), std::move(m)};
+    }
+    const auto opcode = static_cast<menos::Opcode>(op.opcode);
+    const int np = menos::ir::gate_info(opcode).num_params;
+    return menos::GateOp{opcode, std::move(qubits), std::vector<double>(op.params, op.params + np)};
+}
+
+std::uint64_t bits_of(const menos::BitString& b) {
+    std::uint64_t v = 0;
+    for (std::uint32_t i = 0; i < b.num_bits() && i < 64; ++i)
+        if (b.test(i)) v |= std::uint64_t{1} << i;
+    return v;
+}
+
+// Abandons at the safe boundary whose count reaches `at` (the reference's
+// ExecutionMonitor contract: throw to abandon).
+class CountingMonitor final : public menos::ExecutionMonitor {
+public:
+    explicit CountingMonitor(std::int64_t at) : at_(at) {}
+    void at_safe_boundary(std::uint64_t crossed) const override {
+        ++calls_;
+        if (at_ >= 0 && static_cast<std::int64_t>(crossed) >= at_) throw menos::common::InternalError("abandoned");
+    }
+    mutable std::uint64_t calls_ = 0;
+
+private:
+    std::int64_t at_;
+};
+
+const menos::SimulationEngine& engine_of(int which) {
+    static const menos::engines::dense::DenseEngine cpu;
+    if (which == 0) return cpu;
+    return menos::engines::dense_b200::b200_dense_engine();
+}
+
+void set_error(char* err, std::size_t len, const char* what) {
+    if (err == nullptr || len == 0) return;
+    std::strncpy(err, what, len - 1);
+    err[len - 1] = '\0';
+}
+
+}  // namespace
+
+extern "C" {
+
+// The request, as plain C.  abandon_at < 0: no monitor.
+typedef struct ah_request {
+    std::uint32_t num_qubits;
+    std::uint32_t num_ops;
+    const mb2_op* ops;
+    std::int32_t fuse_gates, want_statevector, want_counts, want_expectation, is_sole_region, reserved;
+    std::uint64_t shots, seed;
+    const std::uint32_t* targets;  // (qubit, clbit) pairs
+    std::uint32_t num_targets, bitstring_width;
+    double global_phase;
+    std::uint64_t budget_bytes;
+    const std::uint64_t* x_masks;
+    const std::uint64_t* z_masks;
+    std::uint32_t num_terms, reserved2;
+    std::int64_t abandon_at;
+} ah_request;
+
+typedef struct ah_result {
+    double* statevector;          // 2 * 2^n doubles, or NULL
+    std::uint64_t* outcomes;      // sole region: histogram keys (ascending)
+    std::uint64_t* counts;
+    std::uint64_t capacity;       // of outcomes/counts and of draws
+    std::uint64_t num_outcomes;
+    double* expectation;          // 2 * num_terms doubles
+    std::uint64_t draws;          // Factorized region: draws from counts_sampler with Rng(draw_seed)
+    std::uint64_t draw_seed;
+    std::uint64_t* drawn;         // the drawn outcomes, in draw order
+    std::uint64_t actual_bytes, peak_host, peak_device, monitor_calls;
+    std::int32_t has_statevector, has_counts, has_sampler, has_expectation;
+    double seconds;               // wall time of execute()
+} ah_result;
+
+// 0 ok; 1 ResourceExceeded; 2 InternalError (the monitor's abandon included);
+// 3 any other exception.
+int ah_execute(int which, const ah_request* rq, ah_result* res, char* err, std::size_t errlen) {
+    try {
+        std::vector<menos::Operation> ops;
+        for (std::uint32_t i = 0; i < rq->num_ops; ++i) ops.push_back(to_operation(rq->ops[i]));
+        std::vector<std::pair<menos::QubitId, menos::ClbitId>> targets;
+        for (std::uint32_t t = 0; t < rq->num_targets; ++t)
+            targets.emplace_back(rq->targets[2 * t], rq->targets[2 * t + 1]);
+        menos::Observable obs;
+        for (std::uint32_t t = 0; t < rq->num_terms; ++t) {
+            menos::PauliString p;
+            p.num_qubits = rq->num_qubits;
+            p.x_words.assign(1, rq->x_masks[t]);
+            p.z_words.assign(1, rq->z_masks[t]);
+            obs.terms.emplace_back(std::move(p), C{1.0, 0.0});
+        }
+        CountingMonitor monitor(rq->abandon_at);
+        menos::EngineExecutionRequest request{
+            .num_qubits = rq->num_qubits,
+            .operations = ops,
+            .want_statevector = rq->want_statevector != 0,
+            .want_counts = rq->want_counts != 0,
+            .want_expectation = rq->want_expectation != 0,
+            .shots = rq->shots,
+            .measure_targets = targets,
+            .bitstring_width = rq->bitstring_width,
+            .seed = rq->seed,
+            .global_phase = rq->global_phase,
+            .budget_bytes = rq->budget_bytes,
+            .is_sole_region = rq->is_sole_region != 0,
+            .observable = rq->want_expectation ? &obs : nullptr,
+        };
+        request.fuse_gates = rq->fuse_gates != 0;
+        if (rq->abandon_at >= 0) request.monitor = &monitor;
+        menos::common::MemoryLedger ledger;
+        {
+            menos::common::MemoryLedger::Scope scope(ledger);
+            menos::EngineExecutionResult r;
+            try {
+                const auto t0 = std::chrono::steady_clock::now();
+                r = engine_of(which).execute(request);
+                res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            } catch (...) {
+                res->monitor_calls = monitor.calls_;
+                throw;
+            }
+            res->monitor_calls = monitor.calls_;
+            res->actual_bytes = r.actual_bytes;
+            res->has_statevector = r.statevector.has_value();
+            if (r.statevector && res->statevector)
+                std::memcpy(res->statevector, r.statevector->data(), r.statevector->size() * sizeof(C));
+            res->has_counts = r.counts.has_value();
+            res->num_outcomes = 0;
+            if (r.counts) {
+                for (const auto& [key, c] : *r.counts) {
+                    if (res->num_outcomes >= res->capacity) break;
+                    res->outcomes[res->num_outcomes] = bits_of(key);
+                    res->counts[res->num_outcomes] = c;
+                    ++res->num_outcomes;
+                }
+            }
+            res->has_sampler = r.counts_sampler != nullptr;
+            if (r.counts_sampler && res->drawn) {
+                menos::common::Rng rng(res->draw_seed);
+                for (std::uint64_t i = 0; i < res->draws && i < res->capacity; ++i)
+                    res->drawn[i] = bits_of(r.counts_sampler->sample_one(rng));
+            }
+            res->has_expectation = r.expectation_terms.has_value();
+            if (r.expectation_terms && res->expectation)
+                std::memcpy(res->expectation, r.expectation_terms->data(), r.expectation_terms->size() * sizeof(C));
+        }
+        res->peak_host = ledger.peak_host_bytes();
+        res->peak_device = ledger.peak_device_bytes();
+        return 0;
+    } catch (const menos::common::ResourceExceeded& e) {
+        set_error(err, errlen, e.what());
+        return 1;
+    } catch (const menos::common::InternalError& e) {
+        set_error(err, errlen, e.what());
+        return 2;
+    } catch (const std::exception& e) {
+        set_error(err, errlen, e.what());
+        return 3;
+    }
+}
+
+// out: feasible, estimated_peak_bytes, estimated_work_units, device_bytes,
+// h2d_bytes, d2h_bytes, kernel_launches, host pass count (time component 0).
+int ah_estimate(int which, const ah_request* rq, std::uint64_t* out, char* reason, std::size_t len) {
+    try {
+        std::vector<menos::Operation> ops;
+        for (std::uint32_t i = 0; i < rq->num_ops; ++i) ops.push_back(to_operation(rq->ops[i]));
+        menos::Observable obs;
+        for (std::uint32_t t = 0; t < rq->num_terms; ++t) {
+            menos::PauliString p;
+            p.num_qubits = rq->num_qubits;
+            p.x_words.assign(1, rq->x_masks[t]);
+            p.z_words.assign(1, rq->z_masks[t]);
+            obs.terms.emplace_back(std::move(p), C{1.0, 0.0});
+        }
+        menos::EngineEstimateRequest request{
+            .num_qubits = rq->num_qubits,
+            .operations = &ops,
+            .want_statevector = rq->want_statevector != 0,
+            .want_counts = rq->want_counts != 0,
+            .want_expectation = rq->want_expectation != 0,
+            .observable = rq->want_expectation ? &obs : nullptr,
+        };
+        request.shots = rq->shots;
+        request.bitstring_width = rq->bitstring_width;
+        request.is_sole_region = rq->is_sole_region != 0;
+        request.fuse_gates = rq->fuse_gates != 0;
+        const menos::CostEstimate e = engine_of(which).estimate(request);
+        out[0] = e.feasible;
+        out[1] = e.estimated_peak_bytes;
+        out[2] = e.estimated_work_units;
+        out[3] = e.device.device_bytes;
+        out[4] = e.device.host_to_device_bytes;
+        out[5] = e.device.device_to_host_bytes;
+        out[6] = e.device.kernel_launches;
+        out[7] = static_cast<std::uint64_t>(e.time.counts[static_cast<std::size_t>(menos::Engine::Dense)][0]);
+        set_error(reason, len, e.infeasible_reason.c_str());
+        return 0;
+    } catch (const std::exception& e) {
+        set_error(reason, len, e.what());
+        return 3;
+    }
+}
+
+// out: present, device_total_bytes, device_available_bytes, h2d B/s, d2h B/s,
+// kernel_launch_seconds, execution_seconds, device_work_units_per_second.
+int ah_calibration(double* out) {
+    const menos::plan::CudaCalibration c = menos::engines::dense_b200::measure_b200_calibration();
+    out[0] = c.present ? 1.0 : 0.0;
+    out[1] = static_cast<double>(c.device_total_bytes);
+    out[2] = static_cast<double>(c.device_available_bytes);
+    out[3] = c.host_to_device_bytes_per_second;
+    out[4] = c.device_to_host_bytes_per_second;
+    out[5] = c.kernel_launch_seconds;
+    out[6] = c.execution_seconds;
+    out[7] = c.device_work_units_per_second;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,206 @@
+"""The drop-in itself on the GPU: the reference-side binding
+(menos_b200/integration/b200_dense_engine.cpp) executed through
+menos::SimulationEngine::execute beside the reference's own CPU DenseEngine,
+in the shape of the reference's CPU/CUDA differential suite
+(tests/api/cpu_cuda_differential_test.cpp:132-421): statevectors bitwise,
+counts identical for the same seed, expectation terms within 1e-12, a
+monitor that abandons, an over-budget refusal, the ledger's peaks, a
+Factorized region's sampler drawn from on the device, and the estimate and
+calibration the planner reads."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+ADAPTER_SO = os.path.join(ROOT, "oracle", "_ref", "libmenos_adapter.so")
+
+
+@pytest.fixture(scope="module")
+def harness():
+    if not os.path.exists(ADAPTER_SO):
+        pytest.skip("adapter library not built (oracle/_ref)")
+    import pyadapter
+    return pyadapter.AdapterHarness()
+
+
+def both(h, circ, **kw):
+    import pyadapter
+    ref = h.execute(pyadapter.REFERENCE_CPU, circ, **kw)
+    b2 = h.execute(pyadapter.B200, circ, **kw)
+    return ref, b2
+
+
+def same_bits(a, b):
+    return np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def random_circuit(n, layers, seed):
+    """H / T / RX / RY / RZ per qubit from a seeded stream, then a CX brick."""
+    from pyoracle import Circuit
+    from menos_b200.workloads import MT19937_64
+    rng = MT19937_64(seed)
+    c = Circuit(n)
+    for layer in range(layers):
+        for q in range(n):
+            kind = rng.next_word() % 5
+            angle = 2.0 * math.pi * rng.uniform()
+            if kind == 0:
+                c.gate("h", [q])
+            elif kind == 1:
+                c.gate("t", [q])
+            else:
+                c.gate(["rx", "ry", "rz"][kind - 2], [q], [angle])
+        for q in range(layer % 2, n - 1, 2):
+            c.gate("cx", [q, q + 1])
+    return c
+
+
+@pytest.mark.parametrize("fuse", [True, False])
+def test_random_circuits_bitwise_across_qubit_counts(harness, fuse):
+    for n in range(4, 13):
+        c = random_circuit(n, 6, 20260929 + n)
+        ref, b2 = both(harness, c, statevector=True, fuse=fuse)
+        assert ref["rc"] == 0 and b2["rc"] == 0, (ref["error"], b2["error"])
+        assert same_bits(ref["statevector"], b2["statevector"]), f"n={n}"
+
+
+def test_gates_phases_and_unitaries_bitwise(harness):
+    from pyoracle import Circuit
+    rs = np.random.default_rng(987654321)
+    for phase in (0.0, 0.7, -2.3, math.pi):
+        c = Circuit(3, phase).gate("h", [0]).gate("cx", [0, 1]).gate("t", [2])
+        ref, b2 = both(harness, c, statevector=True)
+        assert same_bits(ref["statevector"], b2["statevector"])
+    for k in range(1, 6):
+        n = k + 2
+        m = rs.standard_normal((1 << k, 1 << k)) + 1j * rs.standard_normal((1 << k, 1 << k))
+        q, _ = np.linalg.qr(m)
+        c = Circuit(n)
+        for j in range(n):
+            c.gate("h", [j])
+        c.gate("t", [0])
+        c.unitary(list(rs.permutation(n)[:k]), q)
+        ref, b2 = both(harness, c, statevector=True)
+        assert same_bits(ref["statevector"], b2["statevector"]), f"k={k}"
+    for oc in ("cx", "cz", "swap"):
+        for rev in (False, True):
+            c = Circuit(4)
+            for j in range(4):
+                c.gate("h", [j])
+            c.gate("t", [1])
+            c.gate(oc, [2, 0] if rev else [0, 2])
+            ref, b2 = both(harness, c, statevector=True)
+            assert same_bits(ref["statevector"], b2["statevector"])
+
+
+def test_counts_identical_for_the_same_seed(harness):
+    from menos_b200 import workloads
+    from pyoracle import Circuit
+    c6 = Circuit(6)
+    for q in range(6):
+        c6.gate("h", [q])
+    c6.gate("t", [0])
+    for q in range(0, 5, 2):
+        c6.gate("cx", [q, q + 1])
+    for circ, shots, seed in ((c6, 4096, 424242), (workloads.brick(16, 8, 5), 100000, 1234)):
+        n = circ.num_qubits
+        targets = [(q, q) for q in range(n)]
+        ref, b2 = both(harness, circ, shots=shots, seed=seed, targets=targets)
+        assert ref["rc"] == 0 and b2["rc"] == 0, (ref["error"], b2["error"])
+        assert ref["counts"] == b2["counts"]
+        # A measured subset mapped to other clbits.
+        sub = [(1, 0), (n - 1, 3), (2, 1)]
+        ref, b2 = both(harness, circ, shots=shots, seed=seed + 1, targets=sub, width=5)
+        assert ref["counts"] == b2["counts"]
+
+
+def test_expectation_terms_within_tolerance(harness):
+    from menos_b200 import workloads
+    circ = workloads.brick(12, 6, 3)
+    paulis = workloads.pauli_strings(12, 24, 9)
+    ref, b2 = both(harness, circ, paulis=paulis)
+    assert ref["rc"] == 0 and b2["rc"] == 0
+    assert np.max(np.abs(ref["terms"] - b2["terms"])) <= 1e-12
+
+
+def test_factorized_region_sampler_draws_identically(harness):
+    """A non-sole region returns a sampler that combine_counts draws from
+    (src/runtime/combine_counts.cpp): the adapter's keeps the state on the
+    device and gives the reference CumulativeDistribution's draws; it holds
+    no host memory, the reference holds its 8 * 2^n cumulative array."""
+    from menos_b200 import workloads
+    circ = workloads.brick(14, 6, 11)
+    targets = [(q, q) for q in range(0, 14, 2)]
+    kw = dict(shots=3000, seed=0, targets=targets, sole=False, draws=3000, draw_seed=77)
+    ref, b2 = both(harness, circ, **kw)
+    assert ref["rc"] == 0 and b2["rc"] == 0, (ref["error"], b2["error"])
+    assert ref["has_sampler"] and b2["has_sampler"]
+    assert np.array_equal(ref["drawn"], b2["drawn"])
+    assert ref["peak_host"] >= 8 << 14
+    assert b2["peak_host"] == 0
+    assert b2["peak_device"] == 16 << 14
+    # Draws past the precomputed batch continue identically.
+    kw.update(draws=4500, shots=2000)
+    ref, b2 = both(harness, circ, **kw)
+    assert np.array_equal(ref["drawn"], b2["drawn"])
+
+
+def test_monitor_abandons_and_budget_refuses(harness):
+    import pyadapter
+    from menos_b200 import workloads
+    circ = workloads.brick(16, 10, 4)
+    ref, b2 = both(harness, circ, statevector=True, abandon_at=2)
+    assert ref["rc"] == pyadapter.INTERNAL_ERROR and b2["rc"] == pyadapter.INTERNAL_ERROR
+    # The reference's boundaries are blocks; the adapter's are passes, each
+    # reporting the blocks done so far, so it abandons after its first pass.
+    assert "abandoned" in b2["error"] and b2["monitor_calls"] >= 1 and ref["monitor_calls"] == 2
+    # A statevector over the host budget: ResourceExceeded, before any host copy.
+    ref, b2 = both(harness, circ, statevector=True, budget=(16 << 16) - 1)
+    assert ref["rc"] == pyadapter.RESOURCE_EXCEEDED and b2["rc"] == pyadapter.RESOURCE_EXCEEDED
+    assert "the host copy needs" in b2["error"]
+    assert b2["peak_host"] == 0
+
+
+def test_ledger_peaks(harness):
+    from menos_b200 import workloads
+    circ = workloads.brick(18, 4, 2)
+    ref, b2 = both(harness, circ, statevector=True)
+    assert b2["peak_device"] == 16 << 18
+    assert b2["peak_host"] == 16 << 18
+    assert ref["peak_device"] == 0 and ref["peak_host"] >= 16 << 18
+    e = both(harness, circ, paulis=workloads.pauli_strings(18, 4, 1))[1]
+    assert e["peak_device"] == 16 << 18 and e["peak_host"] == 0
+
+
+def test_estimate_and_calibration_feed_the_time_model(harness):
+    """The planner prices a CUDA candidate as execution + launches * launch
+    + work_units / device_work_units_per_second + transfers
+    (src/plan/planner.cpp:415-433).  With the adapter's calibration and
+    estimate -- the sweep priced by the engine's autotuned per-pass time
+    model -- that price is within 2x of the adapter's measured execute()."""
+    import pyadapter
+    from menos_b200 import workloads
+    cal = harness.calibration()
+    assert cal["present"] == 1.0
+    for key in ("device_total_bytes", "device_available_bytes", "h2d_bytes_per_s", "d2h_bytes_per_s",
+                "kernel_launch_seconds", "device_work_units_per_second"):
+        assert cal[key] > 0, key
+    assert cal["execution_seconds"] >= 0
+    for circ in (workloads.brick(26, 12, 8), workloads.qft(25)):
+        paulis = workloads.pauli_strings(circ.num_qubits, 8, 3)
+        est = harness.estimate(pyadapter.B200, circ, paulis=paulis)
+        assert est["feasible"] and est["work_units"] > 0 and est["launches"] > 1
+        assert est["device_bytes"] >= 16 << circ.num_qubits
+        assert est["peak_bytes"] == 0 and est["d2h_bytes"] == 16 * len(paulis)
+        priced = (cal["execution_seconds"] + est["launches"] * cal["kernel_launch_seconds"] +
+                  est["work_units"] / cal["device_work_units_per_second"] +
+                  est["h2d_bytes"] / cal["h2d_bytes_per_s"] + est["d2h_bytes"] / cal["d2h_bytes_per_s"])
+        harness.execute(pyadapter.B200, circ, paulis=paulis)  # warm
+        run = harness.execute(pyadapter.B200, circ, paulis=paulis)
+        assert run["rc"] == 0, run["error"]
+        assert 0.5 <= priced / run["seconds"] <= 2.0, (priced, run["seconds"])

@@ -88,3 +88,23 @@ def test_batch_grouped_expectation_many_bindings(ctx, ref, n):
         r = ref.run(c, fuse_gates=True, paulis=paulis)
         h = sum(w * t for w, t in zip(coefs, r["terms"]))
         assert abs(vals[b] - h.real) <= 1e-11, (b, vals[b], h)
+
+
+@pytest.mark.parametrize("fuse", [False, True])
+def test_batch_binding_at_angle_zero_bitwise(ctx, ref, fuse):
+    # RY(0) and RZ(0) are diagonal (the identity) for one binding only: that
+    # binding still runs the dense path the others need, and its state is
+    # bitwise the reference's, whose dispatch takes the diagonal kernel.
+    n, layers, B = 10, 3, 4
+    rows = workloads.hea_bindings(n, layers, B, 123)
+    rows[1][0] = 0.0          # RY(0) on qubit 0, first layer
+    rows[1][3] = 0.0          # RZ(0) on qubit 1
+    rows[2] = [0.0] * len(rows[2])
+    paulis = workloads.pauli_strings(n, 8, 5)
+    coefs = workloads.weights(8, 6)
+    vals, states, _ = sweep_batch(ctx, workloads.hea(n, layers, 0), rows, paulis, coefs, fuse_gates=fuse,
+                                  want_states=True)
+    for b in range(B):
+        c = as_oracle_circuit(bound_circuit(n, layers, rows[b]))
+        r = ref.run(c, fuse_gates=fuse, statevector=True)
+        assert bits_equal(states[b], r["statevector"]), b

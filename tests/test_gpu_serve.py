@@ -68,6 +68,30 @@ def test_admission_budget(ctx):
     srv.close()
 
 
+def test_admission_charges_the_sampler_staging(ctx):
+    # A counts request holds its state and, while it samples, the uniforms,
+    # the per-shot basis and the walk's scratch in the state's staging buffer
+    # (rounded up to a power of two): the admission charge covers all of it,
+    # so a budget that holds the state but not that staging refuses the
+    # request up front, and a larger one runs such requests side by side.
+    c = workloads.brick(20, 2, 1)
+    shots = 1 << 21  # 16 MiB of uniforms and 16 MiB of basis indices
+    targets = [(q, q) for q in range(20)]
+    srv = Server(ctx, budget_bytes=60 << 20, slots=2)
+    with pytest.raises(ResourceExceeded):
+        srv.submit(c, "counts", shots=shots, seed=1, targets=targets)
+    srv.close()
+    srv = Server(ctx, budget_bytes=200 << 20, slots=4)
+    reqs = {srv.submit(c, "counts", shots=shots, seed=s, targets=targets): s for s in range(4)}
+    got = collect(srv, len(reqs))
+    assert srv.stats()["held_bytes"] == 0
+    srv.close()
+    assert sorted(got) == sorted(reqs)
+    for t, seed in reqs.items():
+        assert got[t]["status"] == 0
+        assert got[t]["counts"] == alone(ctx, {"circuit": c, "output": "counts", "shots": shots, "seed": seed})
+
+
 def test_poll_times_out_when_idle(ctx):
     srv = Server(ctx, slots=2)
     assert srv.poll(timeout_ms=50) == []
