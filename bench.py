@@ -82,6 +82,8 @@ def parse():
     p.add_argument("--load", type=float, default=4.0, help="serve: arrival rate / plain-loop capacity")
     p.add_argument("--bindings", type=int, default=4096)
     p.add_argument("--precision", default="c128", choices=["c128", "c64"], help="serve/batch: state precision")
+    p.add_argument("--c64-kernel", default="tensor", choices=["tensor", "simt"],
+                   help="complex64 passes: tensor cores (split-TF32 GEMMs) or FP32 SIMT gates")
     return p.parse_args()
 
 
@@ -545,7 +547,7 @@ def main_c64(args, local):
     ref.free()
     lo = DeviceState(ctx, 28, precision=C64)
     lo.init(0.0)
-    lo.apply_program(circ28)
+    lo.apply_program(circ28, tile_qubits=args.tile, c64_kernel=args.c64_kernel)
     lo.normalize()
     lo_amps = lo.copy_out()
     lo_exp = lo.expectation(paulis)
@@ -558,7 +560,7 @@ def main_c64(args, local):
     st = DeviceState(ctx, n, precision=C64)
     stream = torch.cuda.ExternalStream(st.stream_handle())
     st.init(0.0)
-    st.apply_program(circ)
+    st.apply_program(circ, tile_qubits=args.tile, c64_kernel=args.c64_kernel)
     st.synchronize()
     ts = []
     for _ in range(max(1, args.steps)):
@@ -566,7 +568,7 @@ def main_c64(args, local):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        stats = st.apply_program(circ)
+        stats = st.apply_program(circ, tile_qubits=args.tile, c64_kernel=args.c64_kernel)
         st.normalize()
         b.record(stream)
         b.synchronize()
@@ -579,7 +581,8 @@ def main_c64(args, local):
         "passes": int(stats.passes), "hbm_gbs_per_pass": round(2 * (8 << n) / (per_pass * 1e-3) / 1e9, 1),
         "error_28q_vs_complex128": {"max_abs_amp": d_amp, "max_abs_pauli": d_exp, "paulis": 64},
         "dtype": "c64 (f32 amplitudes, f64 reductions)",
-        "config": {"workload": f"brick({n}, 32), state {8 << n >> 30} GiB", "seed": 20260929},
+        "config": {"workload": f"brick({n}, 32), state {8 << n >> 30} GiB", "seed": 20260929,
+                   "c64_kernel": args.c64_kernel, "tile_qubits": args.tile or 12},
         "data": "synthetic (seeded circuit)",
     }
     print(json.dumps(line), flush=True)

@@ -15,9 +15,13 @@
  *   - the global phase is part of the state: init writes exp(i*phase)|0..0>;
  *   - Pauli strings use Y = i*X*Z (x/z bit masks, one 64-bit word).
  *
- * The complex64 precision path (MB2_C64 states) runs the same sweep with FP32
- * fused multiply-adds on gate matrices composed in FP64; norms, expectations
- * and sampling probabilities accumulate in FP64.
+ * The complex64 precision path (MB2_C64 states) runs the same tiled sweep with
+ * gate matrices composed in FP64: each phase's gates on its four register
+ * qubits compose into one 16x16 complex matrix applied on the tcgen05 tensor
+ * cores as a split-precision GEMM (TF32 high and low parts of both operands,
+ * FP32 accumulation), or, per option, gate by gate with FP32 fused
+ * multiply-adds; norms, expectations and sampling probabilities accumulate
+ * in FP64.
  *
  * The plain complex128 path is bitwise identical to the reference's generic
  * CPU kernel (src/kernels/cpu/dense_kernels.cpp:465-524): every output
@@ -118,6 +122,8 @@ typedef struct mb2_sweep_options {
     int32_t low_qubits;      /* qubits 0..low-1 held in every tile (contiguous runs); -1 = none, 0 = default 3 */
     int32_t tile_qubits;     /* qubits per multi-gate tile pass; 0 = autotuned */
     int32_t per_gate;        /* 1: one launch per block, no tiling (the reference's sweep shape) */
+    int32_t c64_kernel;      /* complex64 states: 0 = tensor cores (split-TF32 GEMMs of each phase's
+                                composed 16x16 matrix) wherever a pass allows, 1 = FP32 SIMT gates only */
 } mb2_sweep_options;
 
 /* Applies a whole operation list (MeasureOps skipped) as a sequence of
@@ -374,6 +380,29 @@ int mb2_gate_matrix(int32_t opcode, const double* params, double* out, uint32_t 
 int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
                        uint32_t num_qubits, uint32_t* pass, uint32_t* k, uint32_t* qubits,
                        double* matrices, uint64_t* num_blocks, uint64_t* matrix_len, int32_t precision);
+
+/* Runs the tiled program mb2_apply_program would plan for these ops on a
+ * num_qubits state (precision MB2_C64: the commuting plan and, unless
+ * opts->c64_kernel says otherwise, its tensor-core form) on the host, in
+ * FP64, instruction by instruction (phase matrices exact): state (2 * 2^n
+ * doubles) in and out.  stats (5 words, optional): passes, tensor-core
+ * passes, phase matrices, tile qubits, the largest dynamic shared memory
+ * (bytes) a tensor-core pass launches with.  Lets tests check the plan -- the
+ * order of every block, each phase's composed matrix, the placement of
+ * elementwise diagonals -- against the oracle on the CPU.  state NULL: the
+ * stats only (up to 40 qubits); otherwise at most 28 qubits.  Has no
+ * counterpart in the reference. */
+int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
+                       int32_t precision, double* state, uint64_t* stats);
+
+/* The complex64 tensor-core step alone, on the context's device: 256 rows of
+ * 16 complex64 amplitudes (rows: 256 * 32 floats, interleaved) times the
+ * 16x16 complex matrix (row-major, interleaved doubles) as the tile pass
+ * applies a phase -- split-TF32 operands, FP32 accumulation -- into out
+ * (256 * 32 floats): out_row = matrix * in_row.  Lets tests check the
+ * tensor-memory and operand layouts in isolation.  Has no counterpart in the
+ * reference. */
+int mb2_debug_tc_probe(mb2_context* ctx, const float* rows, const double* matrix, float* out);
 
 /* The grouping mb2_expectation uses for these terms on a num_qubits state,
  * as 64-bit words: the group count, then per group c, d, free_mask, nterms,

@@ -413,48 +413,79 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
         return MB2_OK;
     }
     mb2::TileProgram prog;
+    // complex64 passes on the tensor cores: 12- or 13-qubit tiles.
+    const bool tc = c64 && o.c64_kernel == 0 && (m == 12 || m == 13);
     try {
         const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
                                                                          : static_cast<uint32_t>(o.low_qubits));
         // complex64 results are not bitwise the reference's: commuting
         // blocks may be reordered into fewer passes.
         prog = mb2::plan_tile_program(blocks, s->n, m, low, nullptr, c64);
+        if (tc) mb2::make_tensor_core_program(prog, m == 12 ? mb2::kTcMaxPhasesTwoCtas : mb2::kTcMaxPhasesOneCta);
     } catch (const std::exception& e) {
         return fail(s->ctx, MB2_ERR_INVALID, e.what());
     }
-    // One upload: the compact word stream, staged data, global-only data
-    // (256-byte aligned parts).
+    // One upload: the compact word stream, staged data, global-only data,
+    // the tensor-core phase matrices and their error word (256-byte aligned
+    // parts).
     const size_t ibytes = prog.words.size() * sizeof(uint32_t);
     const size_t dbytes = prog.data.size() * sizeof(double);
     const size_t gbytes = prog.gdata.size() * sizeof(double);
+    const size_t tbytes = prog.tcdata.size() * sizeof(float);
     const size_t doff = (ibytes + 255) & ~size_t{255};
     const size_t goff = (doff + dbytes + 255) & ~size_t{255};
-    if (int e = ensure_scratch(s, goff + gbytes + 256); e != MB2_OK) return e;
-    std::vector<unsigned char> host(goff + gbytes);
+    const size_t toff = (goff + gbytes + 255) & ~size_t{255};
+    const size_t eoff = (toff + tbytes + 255) & ~size_t{255};
+    if (int e = ensure_scratch(s, eoff + 256); e != MB2_OK) return e;
+    std::vector<unsigned char> host(eoff + sizeof(int), 0);
     std::memcpy(host.data(), prog.words.data(), ibytes);
     if (dbytes) std::memcpy(host.data() + doff, prog.data.data(), dbytes);
     if (gbytes) std::memcpy(host.data() + goff, prog.gdata.data(), gbytes);
+    if (tbytes) std::memcpy(host.data() + toff, prog.tcdata.data(), tbytes);
     MB2_CUDA(s->ctx, cudaMemcpyAsync(s->scratch, host.data(), host.size(), cudaMemcpyHostToDevice, s->stream));
-    const auto* dev_words = static_cast<const uint32_t*>(s->scratch);
-    const auto* dev_sdata = reinterpret_cast<const double*>(static_cast<unsigned char*>(s->scratch) + doff);
-    const auto* dev_gdata = reinterpret_cast<const double*>(static_cast<unsigned char*>(s->scratch) + goff);
+    auto* base = static_cast<unsigned char*>(s->scratch);
+    const auto* dev_words = reinterpret_cast<const uint32_t*>(base);
+    const auto* dev_sdata = reinterpret_cast<const double*>(base + doff);
+    const auto* dev_gdata = reinterpret_cast<const double*>(base + goff);
+    const auto* dev_tc = reinterpret_cast<const float*>(base + toff);
+    auto* dev_err = reinterpret_cast<int*>(base + eoff);
     s->stats.fp64_ops_per_amp = prog.fp64_per_amp;
     uint64_t done = 0;
+    bool any_tc = false;
+    // A bounded wait on the tensor core that ran out leaves a nonzero code
+    // in the error word; read it whenever the sweep synchronises.
+    auto check_tc = [&]() -> int {
+        if (!any_tc) return MB2_OK;
+        int err = 0;
+        MB2_CUDA(s->ctx, cudaMemcpyAsync(&err, dev_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+        if (err != 0) return fail(s->ctx, MB2_ERR_CUDA, "tensor-core pass: a bounded wait ran out");
+        return MB2_OK;
+    };
     for (const mb2::TilePass& pass : prog.passes) {
-        const int rc = c64 ? mb2::launch_tile_pass_c64(s->amps, s->n, pass, dev_words, dev_sdata, dev_gdata,
-                                                       s->ctx->sm_count, s->stream)
-                           : mb2::launch_tile_pass(s->amps, s->n, pass, dev_words, dev_sdata, dev_gdata,
-                                                   s->ctx->sm_count, s->stream);
+        int rc;
+        if (pass.tc) {
+            any_tc = true;
+            rc = mb2::launch_tile_pass_tc(s->amps, s->n, pass, dev_words, dev_sdata, dev_tc, dev_err,
+                                          s->ctx->sm_count, s->stream);
+        } else if (c64) {
+            rc = mb2::launch_tile_pass_c64(s->amps, s->n, pass, dev_words, dev_sdata, dev_gdata, s->ctx->sm_count,
+                                           s->stream);
+        } else {
+            rc = mb2::launch_tile_pass(s->amps, s->n, pass, dev_words, dev_sdata, dev_gdata, s->ctx->sm_count,
+                                       s->stream);
+        }
         if (rc != MB2_OK) return fail(s->ctx, rc, std::string("tile pass launch: ") + mb2::last_cuda_error_string());
         s->stats.passes += 1;
         s->stats.launches += 1;
         done += pass.gates;
         if (boundary != nullptr) {
             MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+            if (int e = check_tc(); e != MB2_OK) return e;
             if (boundary(user, done) != 0) return fail(s->ctx, MB2_ERR_ABANDONED, "sweep abandoned");
         }
     }
-    return MB2_OK;
+    return check_tc();
 }
 
 int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts) {
@@ -716,6 +747,82 @@ int mb2_copy_in(mb2_state* s, const void* host, uint64_t num_amplitudes) {
 int mb2_synchronize(mb2_state* s) {
     if (s == nullptr) return MB2_ERR_INVALID;
     MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
+    return MB2_OK;
+}
+
+int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
+                       int32_t precision, double* state, uint64_t* stats) {
+    if ((ops == nullptr && num_ops != 0) || num_qubits < 1 || num_qubits > 40 || (state != nullptr && num_qubits > 28) ||
+        (precision != MB2_C128 && precision != MB2_C64))
+        return MB2_ERR_INVALID;
+    mb2_sweep_options o{1, 0, 0, 0, 0};
+    if (opts != nullptr) o = *opts;
+    try {
+        const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+        if (blocks.empty()) return MB2_OK;
+        const bool c64 = precision == MB2_C64;
+        uint32_t m = c64 ? (o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : mb2::kDefaultTileQubitsC64)
+                         : tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, num_qubits, blocks);
+        for (const mb2::Block& b : blocks) m = std::max(m, b.k);
+        m = std::min(std::max(m, mb2::kMinTileQubits), num_qubits);
+        const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
+                                                                         : static_cast<uint32_t>(o.low_qubits));
+        mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m, low, nullptr, c64);
+        const bool tc = c64 && o.c64_kernel == 0 && (m == 12 || m == 13);
+        if (tc) mb2::make_tensor_core_program(prog, m == 12 ? mb2::kTcMaxPhasesTwoCtas : mb2::kTcMaxPhasesOneCta);
+        if (state != nullptr) mb2::run_program_on_host(prog, num_qubits, reinterpret_cast<mb2::Cd*>(state));
+        if (stats != nullptr) {
+            uint64_t tcp = 0, smem = 0;
+            for (const mb2::TilePass& p : prog.passes) {
+                if (!p.tc) continue;
+                tcp += 1;
+                smem = std::max<uint64_t>(smem, 2 * (8ull << p.m) + uint64_t{p.tc_phases} * mb2::kTcMatrixFloats * 4 +
+                                                    4ull * p.word_count + 4ull * p.sdata_count);
+            }
+            stats[0] = prog.passes.size();
+            stats[1] = tcp;
+            stats[2] = prog.tcmatrices.size() / 256;
+            stats[3] = m;
+            stats[4] = smem;
+        }
+    } catch (const std::exception&) {
+        return MB2_ERR_INVALID;
+    }
+    return MB2_OK;
+}
+
+int mb2_debug_tc_probe(mb2_context* ctx, const float* rows, const double* matrix, float* out) {
+    if (ctx == nullptr || rows == nullptr || matrix == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    MB2_CUDA(ctx, cudaSetDevice(ctx->device));
+    std::vector<float> b(mb2::kTcMatrixFloats);
+    mb2::tc_operands(reinterpret_cast<const mb2::Cd*>(matrix), b.data());
+    constexpr size_t kRowBytes = 256 * 32 * sizeof(float);
+    const size_t bytes = 2 * kRowBytes + b.size() * sizeof(float) + 256;
+    cudaStream_t stream = nullptr;
+    MB2_CUDA(ctx, cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    unsigned char* dev = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&dev), bytes, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dev, 0, bytes, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dev, rows, kRowBytes, cudaMemcpyHostToDevice, stream);
+    float* dev_b = reinterpret_cast<float*>(dev + 2 * kRowBytes);
+    int* dev_err = reinterpret_cast<int*>(dev + 2 * kRowBytes + b.size() * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dev_b, b.data(), b.size() * sizeof(float), cudaMemcpyHostToDevice, stream);
+    int rc = MB2_OK;
+    if (e == cudaSuccess) {
+        rc = mb2::launch_tc_probe(reinterpret_cast<const float*>(dev), dev_b, reinterpret_cast<float*>(dev + kRowBytes),
+                                  dev_err, stream);
+        if (rc != MB2_OK) rc = fail(ctx, rc, std::string("tc probe launch: ") + mb2::last_cuda_error_string());
+    }
+    int err = 0;
+    if (e == cudaSuccess && rc == MB2_OK) e = cudaMemcpyAsync(out, dev + kRowBytes, kRowBytes, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && rc == MB2_OK) e = cudaMemcpyAsync(&err, dev_err, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (dev != nullptr) cudaFreeAsync(dev, stream);
+    const cudaError_t se = cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "tc probe");
+    if (se != cudaSuccess) return cuda_fail(ctx, se, "tc probe");
+    if (rc != MB2_OK) return rc;
+    if (err != 0) return fail(ctx, MB2_ERR_CUDA, "tc probe: a bounded wait ran out");
     return MB2_OK;
 }
 

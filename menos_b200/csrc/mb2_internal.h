@@ -78,7 +78,8 @@ enum TileOp : uint8_t {
     TOP_G1 = 3,       // 1-qubit dense gate on register slot pos[0]
     TOP_G2 = 4,       // 2-qubit dense gate on register slots (pos[0], pos[1])
     TOP_DIAG = 5,     // diagonal on tile bits pos[0..k-1]
-    TOP_SMEM = 6      // k-qubit dense gate applied from shared memory (own phase)
+    TOP_SMEM = 6,     // k-qubit dense gate applied from shared memory (own phase)
+    TOP_MMA = 7       // tensor-core pass: the phase's composed 16x16 matrix number `aux` (tile_tc.cpp)
 };
 enum TileKind : uint8_t {
     TK_GEN = 0,   // every entry general
@@ -120,6 +121,11 @@ struct TilePass {
     uint32_t param_len = 0;
     bool heavy = false;  // has two-qubit dense/monomial/permutation, kDiagK or kSmem words
     bool mid = false;    // heavy, but only through general dense two-qubit words (kGen2)
+    // Tensor-core form (complex64, tile_tc.cpp): the pass's composed phase
+    // matrices are tcdata[tc_begin, tc_begin + tc_phases * kTcMatrixFloats).
+    bool tc = false;
+    uint32_t tc_begin = 0;
+    uint32_t tc_phases = 0;
 };
 
 // Compact instruction stream of the complex128 tile kernel, written from the
@@ -161,6 +167,9 @@ constexpr uint32_t kU3Run012 = 112;
 constexpr uint32_t kPhase = 200;
 constexpr uint32_t kPhaseWords = 29;
 constexpr uint32_t kSmem = 201;  // aux = k; extra words: tile positions, gdata offset (doubles)
+// Tensor-core pass: apply the pass's composed phase matrix number aux (its
+// split-TF32 operands staged in shared memory) to the registers' amplitudes.
+constexpr uint32_t kMma = 202;
 // A sign monomial word: bits 0-15 the register slots j (of 16) whose
 // register-bit factors are all 1 (0xffff: no register factor), bits 16-31
 // the tile bits of its thread-bit factors.  The amplitudes of slots j in
@@ -184,9 +193,29 @@ struct TileProgram {
     std::vector<double> data;
     std::vector<uint32_t> words;  // compact stream of every pass (complex128 kernel)
     uint64_t fp64_per_amp = 0;    // modelled FP64 instructions per amplitude
+    // Tensor-core passes: per composed phase matrix, its real 32x32 form as
+    // TF32 high and low parts in the MMA's shared-memory layout (tile_tc.cpp),
+    // and the matrix itself (16x16 complex, FP64) for the host interpreter.
+    std::vector<float> tcdata;
+    std::vector<Cd> tcmatrices;
 };
 // Writes prog.words and each pass's word range and parametric slice.
 void encode_compact(TileProgram& prog);
+
+// The complex64 tensor-core form of a planned program (tile_tc.cpp): each
+// pass without wide (k > 2) or parametric blocks becomes phases whose dense
+// gates on the four register qubits compose (in FP64) into one 16x16
+// complex matrix, applied as a split-TF32 tensor-core GEMM, with diagonals
+// that involve other tile qubits applied elementwise before or after it.  A
+// pass needing more than `max_phases` matrices is split into several passes
+// on the same tile.  Rewrites the passes, the staged data and the word stream.
+constexpr uint32_t kTcMatrixFloats = 2 * 32 * 32;  // TF32 high + low, 32x32 real each
+void make_tensor_core_program(TileProgram& prog, uint32_t max_phases);
+
+// Applies a planned program's passes to a host state in FP64, instruction by
+// instruction (phase matrices exact, not split): the arithmetic the tile
+// kernels carry out, up to their precision, for checking plans on the CPU.
+void run_program_on_host(const TileProgram& prog, uint32_t n, Cd* state);
 
 // Register qubits per thread in the tile kernel (16 amplitudes per thread).
 constexpr uint32_t kRegQubits = 4;
@@ -287,6 +316,20 @@ int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uin
                          const double* dev_sdata, const double* dev_gdata, int sm_count, void* stream,
                          const BatchLayout* batch = nullptr);
 int launch_scale_c64(void* amps, uint64_t n_amps, float s, void* stream);
+// The tensor-core complex64 pass (kernels_tc.cu) of a pass in tensor-core
+// form (TilePass::tc).  dev_tc: the program's tcdata on the device; dev_err:
+// a device word the kernel sets to a nonzero code if a bounded wait on the
+// tensor core ran out (the pass's result is then invalid).
+constexpr uint32_t kTcMaxPhasesTwoCtas = 5;   // 12-qubit tiles, two CTAs per SM
+constexpr uint32_t kTcMaxPhasesOneCta = 11;   // 13-qubit tiles, one CTA per SM
+int launch_tile_pass_tc(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
+                        const double* dev_sdata, const float* dev_tc, int* dev_err, int sm_count, void* stream);
+// Debug probe of the tensor-core step alone: one CTA applies the split-TF32
+// operands b (kTcMatrixFloats floats, tile_tc.cpp's layout) to 256 rows of
+// 16 complex64 amplitudes (in -> out, device pointers).
+int launch_tc_probe(const float* in, const float* b, float* out, int* dev_err, void* stream);
+// Writes U (16x16 complex, row-major) as split-TF32 operands (kTcMatrixFloats floats).
+void tc_operands(const Cd* u, float* out);
 int context_device(const mb2_context* ctx);
 // The most staging memory a state's calls can hold for a sweep of these ops,
 // `shots` counts and `terms` Pauli terms, rounded as the state's grow-only

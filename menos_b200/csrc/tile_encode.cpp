@@ -31,7 +31,9 @@ uint32_t header(uint32_t op, uint32_t aux, uint32_t tbit, uint32_t off_doubles) 
     return op | (aux << 8) | (tbit << 16) | (off << 20);
 }
 
-bool is_param(const TileInstr& g) { return g.op != TOP_PHASE && g.op != TOP_END && g.nthread != 0; }
+bool is_param(const TileInstr& g) {
+    return g.op != TOP_PHASE && g.op != TOP_END && g.op != TOP_MMA && g.nthread != 0;
+}
 
 // Doubles of a parametric instruction's per-binding record.
 uint32_t param_doubles(const TileInstr& g) {
@@ -199,7 +201,8 @@ void encode_compact(TileProgram& prog) {
                 }
             }
             flush_signs();
-            const uint32_t off = (g.op == TOP_PHASE || g.op == TOP_END || g.op == TOP_SMEM) ? 0u : data_off(g);
+            const uint32_t off =
+                (g.op == TOP_PHASE || g.op == TOP_END || g.op == TOP_SMEM || g.op == TOP_MMA) ? 0u : data_off(g);
             switch (g.op) {
                 case TOP_PHASE: {
                     uint32_t packed = 0;
@@ -232,6 +235,10 @@ void encode_compact(TileProgram& prog) {
                 }
                 case TOP_END:
                     w.push_back(cop::kEnd);
+                    break;
+                case TOP_MMA:
+                    if (g.aux > 255u) throw std::invalid_argument("too many phase matrices in a pass");
+                    w.push_back(cop::kMma | (g.aux << 8));
                     break;
                 case TOP_SMEM: {
                     heavy = heavy_other = true;

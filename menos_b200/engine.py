@@ -70,6 +70,16 @@ class Context:
         self.h = h
         self.device = device
 
+    def tc_probe(self, rows: np.ndarray, matrix: np.ndarray) -> np.ndarray:
+        """The tensor-core step alone (mb2_debug_tc_probe): rows (256 x 16
+        complex64) times matrix^T (16 x 16 complex), split-TF32 on tcgen05."""
+        r = np.ascontiguousarray(np.asarray(rows, np.complex64).reshape(256, 16))
+        m = np.ascontiguousarray(np.asarray(matrix, np.complex128).reshape(16, 16))
+        out = np.zeros((256, 16), np.complex64)
+        check(lib().mb2_debug_tc_probe(self.h, r.ctypes.data, m.ctypes.data, out.ctypes.data), self.h,
+              "mb2_debug_tc_probe")
+        return out
+
     def close(self) -> None:
         if self.h:
             lib().mb2_context_destroy(self.h)
@@ -159,9 +169,15 @@ class DeviceState:
         self._chk(f(self.h, m.ctypes.data, q.ctypes.data, len(q)), "mb2_apply_matrix")
 
     def apply_program(self, circ: Circuit, fuse_gates: bool = True, tile_qubits: int = 0,
-                      per_gate: bool = False, low_qubits: int = 0) -> SweepStats:
+                      per_gate: bool = False, low_qubits: int = 0, c64_kernel: str = "tensor") -> SweepStats:
+        """c64_kernel (complex64 states): "tensor" -- each phase's gates as one
+        split-TF32 tensor-core GEMM wherever a pass allows; "simt" -- FP32
+        gates one by one."""
         arr, keep = to_mb2_ops(circ)
-        opts = SweepOptions(1 if fuse_gates else 0, low_qubits, tile_qubits, 1 if per_gate else 0)
+        if c64_kernel not in ("tensor", "simt"):
+            raise ValueError("c64_kernel is 'tensor' or 'simt'")
+        opts = SweepOptions(1 if fuse_gates else 0, low_qubits, tile_qubits, 1 if per_gate else 0,
+                            0 if c64_kernel == "tensor" else 1)
         self._chk(lib().mb2_apply_program(self.h, arr, len(circ.ops), C.byref(opts)), "mb2_apply_program")
         del keep
         return self.stats()

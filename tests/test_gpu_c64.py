@@ -12,14 +12,15 @@ from test_oracle_pin import random_circuit
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("kernel", ["tensor", "simt"])
 @pytest.mark.parametrize("n", [4, 7, 11, 14])
-def test_c64_random_circuits_within_fp32_error(ctx, oracle, n):
+def test_c64_random_circuits_within_fp32_error(ctx, oracle, n, kernel):
     rng = np.random.default_rng(n)
     for fuse in (True, False):
         c = random_circuit(n, 120, rng)
         st = DeviceState(ctx, n, precision=C64)
         st.init(c.global_phase)
-        st.apply_program(c, fuse_gates=fuse)
+        st.apply_program(c, fuse_gates=fuse, c64_kernel=kernel)
         got = st.copy_out().astype(np.complex128)
         expect = oracle.run(as_oracle_circuit(c), fuse_gates=fuse)
         assert np.max(np.abs(got - expect)) < 2e-5, (n, fuse)
