@@ -421,7 +421,7 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
         // complex64 results are not bitwise the reference's: commuting
         // blocks may be reordered into fewer passes.
         prog = mb2::plan_tile_program(blocks, s->n, m, low, nullptr, c64);
-        if (tc) mb2::make_tensor_core_program(prog, m == 12 ? mb2::kTcMaxPhasesTwoCtas : mb2::kTcMaxPhasesOneCta);
+        if (tc) mb2::make_tensor_core_program(prog, blocks, m == 12 ? mb2::kTcMaxPhasesTwoCtas : mb2::kTcMaxPhasesOneCta);
     } catch (const std::exception& e) {
         return fail(s->ctx, MB2_ERR_INVALID, e.what());
     }
@@ -431,7 +431,7 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     const size_t ibytes = prog.words.size() * sizeof(uint32_t);
     const size_t dbytes = prog.data.size() * sizeof(double);
     const size_t gbytes = prog.gdata.size() * sizeof(double);
-    const size_t tbytes = prog.tcdata.size() * sizeof(float);
+    const size_t tbytes = prog.tcdata.size() * sizeof(uint32_t);
     const size_t doff = (ibytes + 255) & ~size_t{255};
     const size_t goff = (doff + dbytes + 255) & ~size_t{255};
     const size_t toff = (goff + gbytes + 255) & ~size_t{255};
@@ -447,7 +447,7 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     const auto* dev_words = reinterpret_cast<const uint32_t*>(base);
     const auto* dev_sdata = reinterpret_cast<const double*>(base + doff);
     const auto* dev_gdata = reinterpret_cast<const double*>(base + goff);
-    const auto* dev_tc = reinterpret_cast<const float*>(base + toff);
+    const auto* dev_tc = reinterpret_cast<const uint32_t*>(base + toff);
     auto* dev_err = reinterpret_cast<int*>(base + eoff);
     s->stats.fp64_ops_per_amp = prog.fp64_per_amp;
     uint64_t done = 0;
@@ -769,14 +769,14 @@ int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
                                                                          : static_cast<uint32_t>(o.low_qubits));
         mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m, low, nullptr, c64);
         const bool tc = c64 && o.c64_kernel == 0 && (m == 12 || m == 13);
-        if (tc) mb2::make_tensor_core_program(prog, m == 12 ? mb2::kTcMaxPhasesTwoCtas : mb2::kTcMaxPhasesOneCta);
+        if (tc) mb2::make_tensor_core_program(prog, blocks, m == 12 ? mb2::kTcMaxPhasesTwoCtas : mb2::kTcMaxPhasesOneCta);
         if (state != nullptr) mb2::run_program_on_host(prog, num_qubits, reinterpret_cast<mb2::Cd*>(state));
         if (stats != nullptr) {
             uint64_t tcp = 0, smem = 0;
             for (const mb2::TilePass& p : prog.passes) {
                 if (!p.tc) continue;
                 tcp += 1;
-                smem = std::max<uint64_t>(smem, 2 * (8ull << p.m) + uint64_t{p.tc_phases} * mb2::kTcMatrixFloats * 4 +
+                smem = std::max<uint64_t>(smem, 2 * (8ull << p.m) + uint64_t{p.tc_phases} * mb2::kTcOperandWords * 4 +
                                                     4ull * p.word_count + 4ull * p.sdata_count);
             }
             stats[0] = prog.passes.size();
@@ -794,19 +794,19 @@ int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
 int mb2_debug_tc_probe(mb2_context* ctx, const float* rows, const double* matrix, float* out) {
     if (ctx == nullptr || rows == nullptr || matrix == nullptr || out == nullptr) return MB2_ERR_INVALID;
     MB2_CUDA(ctx, cudaSetDevice(ctx->device));
-    std::vector<float> b(mb2::kTcMatrixFloats);
+    std::vector<uint32_t> b(mb2::kTcOperandWords);
     mb2::tc_operands(reinterpret_cast<const mb2::Cd*>(matrix), b.data());
     constexpr size_t kRowBytes = 256 * 32 * sizeof(float);
-    const size_t bytes = 2 * kRowBytes + b.size() * sizeof(float) + 256;
+    const size_t bytes = 2 * kRowBytes + b.size() * sizeof(uint32_t) + 256;
     cudaStream_t stream = nullptr;
     MB2_CUDA(ctx, cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     unsigned char* dev = nullptr;
     cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&dev), bytes, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(dev, 0, bytes, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dev, rows, kRowBytes, cudaMemcpyHostToDevice, stream);
-    float* dev_b = reinterpret_cast<float*>(dev + 2 * kRowBytes);
-    int* dev_err = reinterpret_cast<int*>(dev + 2 * kRowBytes + b.size() * sizeof(float));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dev_b, b.data(), b.size() * sizeof(float), cudaMemcpyHostToDevice, stream);
+    auto* dev_b = reinterpret_cast<uint32_t*>(dev + 2 * kRowBytes);
+    int* dev_err = reinterpret_cast<int*>(dev + 2 * kRowBytes + b.size() * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dev_b, b.data(), b.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream);
     int rc = MB2_OK;
     if (e == cudaSuccess) {
         rc = mb2::launch_tc_probe(reinterpret_cast<const float*>(dev), dev_b, reinterpret_cast<float*>(dev + kRowBytes),

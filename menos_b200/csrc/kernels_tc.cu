@@ -6,19 +6,22 @@
 // phase's dense gates are applied as one composed 16x16 complex matrix U on
 // the tensor cores (tile_tc.cpp builds the program):
 //
-//   each thread splits its row (32 floats, interleaved re/im) into TF32 high
-//   and low parts and stores both into tensor memory (TMEM lane = row within
-//   a 128-row block, one 32-bit column per element); one thread issues, per
-//   128-row block, tcgen05.mma kind::tf32 with A from tensor memory and U's
-//   split real form B (32x32, in shared memory) accumulating hi*lo, lo*hi and
-//   hi*hi into an FP32 accumulator in tensor memory (M = 128, N = 32, four
-//   K-steps of 8 each); tcgen05.commit signals an mbarrier; every thread
-//   reads its row of the product back (tcgen05.ld) and applies the phase's
-//   elementwise diagonals on registers.
+//   each thread scales its row (32 floats, interleaved re/im) by a power of
+//   two that puts the row's largest magnitude in [2^13, 2^14), splits it into
+//   FP16 high and low parts and stores both into tensor memory (TMEM lane =
+//   row within a 128-row block, two FP16 values per 32-bit column); one
+//   thread issues, per 128-row block, tcgen05.mma kind::f16 with A from
+//   tensor memory and B = U's operand in shared memory (FP16 high parts over
+//   low parts, N = 64): A_hi x [B_hi; B_lo] into 64 FP32 accumulator columns,
+//   then A_lo x B_hi accumulated into the first 32 (two K-steps of 16 each);
+//   tcgen05.commit signals an mbarrier; every thread reads its row back
+//   (tcgen05.ld), adds the two 32-column halves, undoes the scale and applies
+//   the phase's elementwise diagonals on registers.
 //
 // Every wait on the tensor core is bounded: a wait that runs out sets the
 // caller's error word, the CTA stops issuing work, frees its tensor memory
 // and returns.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -81,13 +84,13 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_addr(bar))
                  : "memory");
 }
-// D (TMEM) [+]= A (TMEM) * B (shared memory, descriptor), kind::tf32.
-__device__ __forceinline__ void mma_tf32(uint32_t d, uint32_t a, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+// D (TMEM) [+]= A (TMEM) * B (shared memory, descriptor), kind::f16.
+__device__ __forceinline__ void mma_f16(uint32_t d, uint32_t a, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n"
         ".reg .pred p;\n"
         "setp.ne.b32 p, %4, 0;\n"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n"
         "}\n" ::"r"(d),
         "r"(a), "l"(bdesc), "r"(idesc), "r"(acc)
         : "memory");
@@ -95,13 +98,13 @@ __device__ __forceinline__ void mma_tf32(uint32_t d, uint32_t a, uint64_t bdesc,
 
 #define MB2_R8(i) "r"(v[i]), "r"(v[i + 1]), "r"(v[i + 2]), "r"(v[i + 3]), "r"(v[i + 4]), "r"(v[i + 5]), "r"(v[i + 6]), "r"(v[i + 7])
 #define MB2_W8(i) "=r"(v[i]), "=r"(v[i + 1]), "=r"(v[i + 2]), "=r"(v[i + 3]), "=r"(v[i + 4]), "=r"(v[i + 5]), "=r"(v[i + 6]), "=r"(v[i + 7])
-// 32 consecutive 32-bit columns of this thread's lane (warp w reaches lanes
+// Consecutive 32-bit columns of this thread's lane (warp w reaches lanes
 // 32 (w % 4) .. + 31; taddr carries the lane in bits 16-31).
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16]) {
     asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};\n" ::"r"(taddr),
-        MB2_R8(0), MB2_R8(8), MB2_R8(16), MB2_R8(24)
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};\n" ::"r"(taddr),
+        MB2_R8(0), MB2_R8(8)
         : "memory");
 }
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
@@ -117,22 +120,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
-__device__ __forceinline__ uint32_t tf32_round(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
-    return r;
-}
+__device__ __forceinline__ uint32_t half2_bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 
-// tcgen05.mma kind::tf32 instruction descriptor: D FP32 (bits 4-5 = 1),
-// A and B TF32 (bits 7-9, 10-12 = 2), both K-major, N >> 3 at bit 17,
-// M >> 4 at bit 24; M = 128 rows, N = 32 (16 complex outputs).
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+// tcgen05.mma kind::f16 instruction descriptors: D FP32 (bits 4-5 = 1),
+// A and B FP16 (bits 7-9, 10-12 = 0), both K-major, N >> 3 at bit 17,
+// M >> 4 at bit 24; M = 128 rows, N = 64 (the stacked high and low parts of
+// U's 32 output rows) or N = 32 (the high parts only).
+constexpr uint32_t kIdescN64 = (1u << 4) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kIdescN32 = (1u << 4) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
 // Shared-memory descriptor of B: start address >> 4 (bits 0-13), leading
-// (K) byte offset 128 >> 4 (bits 16-29), stride (N) byte offset 1024 >> 4
+// (K) byte offset 128 >> 4 (bits 16-29), stride (N) byte offset 512 >> 4
 // (bits 32-45), descriptor version 1 (bits 46-47), no swizzle (bits 61-63 = 0).
 __device__ __forceinline__ uint64_t b_desc(uint32_t saddr) {
     return static_cast<uint64_t>((saddr >> 4) & 0x3fffu) | (uint64_t{128u >> 4} << 16) |
-           (uint64_t{1024u >> 4} << 32) | (uint64_t{1} << 46);
+           (uint64_t{512u >> 4} << 32) | (uint64_t{1} << 46);
 }
 
 // The block state of the tensor-core step: TMEM base, mbarrier, its phase
@@ -145,28 +146,37 @@ struct TcCtx {
     int* err;
 };
 
-// a <- U a for this thread's row, U's split operands at shared addresses
-// bhi / blo (each 32x32 TF32, the layout of tile_tc.cpp).  ROWS threads,
-// ROWS / 128 row blocks; TMEM columns: [0, 32 NB) high parts, [32 NB, 64 NB)
-// low parts, [64 NB, 96 NB) the products.  All threads of the CTA call it.
+// a <- U a for this thread's row, U's operand (kTcOperandWords words, the
+// layout of tile_tc.cpp) at shared address b.  ROWS threads, ROWS / 128 row
+// blocks; TMEM columns: [0, 16 NB) high parts, [16 NB, 32 NB) low parts,
+// [32 NB, 96 NB) the products (64 per block).  All threads of the CTA call it.
 template <int ROWS>
-__device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t bhi, uint32_t blo, TcCtx& c) {
+__device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c) {
     constexpr uint32_t NB = ROWS / 128;
     const uint32_t tid = threadIdx.x;
     const uint32_t blk = tid >> 7;
     const uint32_t lane = (tid & 0x60u) << 16;  // this warp's lane quarter
+    // The row's scale: 2^e puts its largest magnitude in [2^13, 2^14)
+    // (e <= 126 keeps 2^-e a normal float; an all-zero row keeps e = 0).
+    float mx = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kNA; ++j) mx = fmaxf(mx, fmaxf(fabsf(a[j].x), fabsf(a[j].y)));
+    const int ex = static_cast<int>((__float_as_uint(mx) >> 23) & 0xffu);
+    const int e = ex == 0 ? 0 : min(140 - ex, 126);
+    const float scale = __uint_as_float(static_cast<uint32_t>(127 + e) << 23);
+    const float unscale = __uint_as_float(static_cast<uint32_t>(127 - e) << 23);
     {
-        uint32_t hi[32], lo[32];
+        uint32_t hi[16], lo[16];
 #pragma unroll
         for (int j = 0; j < kNA; ++j) {
-            const uint32_t hr = tf32_round(a[j].x), hi_ = tf32_round(a[j].y);
-            hi[2 * j] = hr;
-            hi[2 * j + 1] = hi_;
-            lo[2 * j] = tf32_round(a[j].x - __uint_as_float(hr));
-            lo[2 * j + 1] = tf32_round(a[j].y - __uint_as_float(hi_));
+            const float x = a[j].x * scale, y = a[j].y * scale;
+            const __half2 h = __floats2half2_rn(x, y);
+            const float2 hf = __half22float2(h);
+            hi[j] = half2_bits(h);
+            lo[j] = half2_bits(__floats2half2_rn(x - hf.x, y - hf.y));
         }
-        tmem_st32(c.tmem + lane + 32 * blk, hi);
-        tmem_st32(c.tmem + lane + 32 * NB + 32 * blk, lo);
+        tmem_st16(c.tmem + lane + 16 * blk, hi);
+        tmem_st16(c.tmem + lane + 16 * NB + 16 * blk, lo);
     }
     tmem_wait_st();
     tc_fence_before();
@@ -174,16 +184,14 @@ __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t bhi, uint32_
     const bool abort = *c.abort != 0;
     if (!abort && tid == 0) {
         tc_fence_after();
+        const uint64_t d0 = b_desc(b), d1 = b_desc(b + 256);
 #pragma unroll
-        for (uint32_t b = 0; b < NB; ++b) {
-            const uint32_t ah = c.tmem + 32 * b, al = c.tmem + 32 * NB + 32 * b, d = c.tmem + 64 * NB + 32 * b;
-            // Small products first: hi*lo, lo*hi, then hi*hi.
-#pragma unroll
-            for (uint32_t s = 0; s < 4; ++s) mma_tf32(d, ah + 8 * s, b_desc(blo + 256 * s), kIdesc, s);
-#pragma unroll
-            for (uint32_t s = 0; s < 4; ++s) mma_tf32(d, al + 8 * s, b_desc(bhi + 256 * s), kIdesc, 1);
-#pragma unroll
-            for (uint32_t s = 0; s < 4; ++s) mma_tf32(d, ah + 8 * s, b_desc(bhi + 256 * s), kIdesc, 1);
+        for (uint32_t k = 0; k < NB; ++k) {
+            const uint32_t ah = c.tmem + 16 * k, al = c.tmem + 16 * NB + 16 * k, d = c.tmem + 32 * NB + 64 * k;
+            mma_f16(d, ah, d0, kIdescN64, 0);
+            mma_f16(d, ah + 8, d1, kIdescN64, 1);
+            mma_f16(d, al, d0, kIdescN32, 1);
+            mma_f16(d, al + 8, d1, kIdescN32, 1);
         }
         mma_commit(c.bar);
     }
@@ -195,11 +203,14 @@ __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t bhi, uint32_
         c.parity ^= 1u;
     }
     tc_fence_after();
-    uint32_t v[32];
-    tmem_ld32(c.tmem + lane + 64 * NB + 32 * blk, v);
+    uint32_t v0[32], v1[32];
+    tmem_ld32(c.tmem + lane + 32 * NB + 64 * blk, v0);
+    tmem_ld32(c.tmem + lane + 32 * NB + 64 * blk + 32, v1);
     tmem_wait_ld();
 #pragma unroll
-    for (int j = 0; j < kNA; ++j) a[j] = make_float2(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1]));
+    for (int j = 0; j < kNA; ++j)
+        a[j] = make_float2((__uint_as_float(v0[2 * j]) + __uint_as_float(v1[2 * j])) * unscale,
+                           (__uint_as_float(v0[2 * j + 1]) + __uint_as_float(v1[2 * j + 1])) * unscale);
 }
 
 // Sets up TMEM (warp 0), the mbarrier and the abort flag; the caller's
@@ -227,20 +238,20 @@ __device__ __forceinline__ void tc_teardown(const TcCtx& c) {
 }
 
 // ---- probe: the tensor-core step alone, on 256 rows -------------------------
-__global__ void __launch_bounds__(256, 1) k_tc_probe(const float2* __restrict__ in, const float* __restrict__ b,
+__global__ void __launch_bounds__(256, 1) k_tc_probe(const float2* __restrict__ in, const uint32_t* __restrict__ b,
                                                      float2* __restrict__ out, int* err) {
-    __shared__ __align__(128) float sb[kTcMatrixFloats];
+    __shared__ __align__(128) uint32_t sb[kTcOperandWords];
     __shared__ uint32_t s_tmem;
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ int s_abort;
-    for (uint32_t i = threadIdx.x; i < kTcMatrixFloats / 4; i += blockDim.x)
-        reinterpret_cast<float4*>(sb)[i] = reinterpret_cast<const float4*>(b)[i];
+    for (uint32_t i = threadIdx.x; i < kTcOperandWords / 4; i += blockDim.x)
+        reinterpret_cast<uint4*>(sb)[i] = reinterpret_cast<const uint4*>(b)[i];
     fence_async_smem();
     TcCtx c = tc_setup<256>(&s_tmem, &s_bar, &s_abort, err);
     float2 a[kNA];
 #pragma unroll
     for (int j = 0; j < kNA; ++j) a[j] = in[threadIdx.x * kNA + j];
-    tc_apply<256>(a, smem_addr(sb), smem_addr(sb + kTcMatrixFloats / 2), c);
+    tc_apply<256>(a, smem_addr(sb), c);
 #pragma unroll
     for (int j = 0; j < kNA; ++j) out[threadIdx.x * kNA + j] = a[j];
     tc_teardown<256>(c);
@@ -254,7 +265,7 @@ template <int MT, int MINB, typename IDX>
 __global__ void __launch_bounds__(1 << (MT - 4), MINB)
     k_tile_pass_tc(float2* __restrict__ st, uint32_t n, uint64_t smask, const uint32_t* __restrict__ words,
                    uint32_t nwords, const double* __restrict__ sdata, uint32_t nsdata,
-                   const float* __restrict__ tcm, uint32_t nphases, uint64_t ntiles, uint32_t stages, int* err) {
+                   const uint32_t* __restrict__ tcm, uint32_t nphases, uint64_t ntiles, uint32_t stages, int* err) {
     constexpr uint32_t kRows = 1u << (MT - 4);
     constexpr uint32_t kCols = kRows == 256 ? 256 : 512;
     extern __shared__ __align__(128) float2 smem_f[];
@@ -265,11 +276,11 @@ __global__ void __launch_bounds__(1 << (MT - 4), MINB)
     constexpr uint32_t m = MT;
     constexpr uint32_t tbits = m - kRegQubits;
     constexpr uint32_t tile_amps = 1u << m;
-    float* sb = reinterpret_cast<float*>(smem_f + stages * tile_amps);
-    uint32_t* sw = reinterpret_cast<uint32_t*>(sb + nphases * kTcMatrixFloats);
+    uint32_t* sb = reinterpret_cast<uint32_t*>(smem_f + stages * tile_amps);
+    uint32_t* sw = sb + nphases * kTcOperandWords;
     float* sd = reinterpret_cast<float*>(sw + nwords);
-    for (uint32_t i = tid; i < nphases * (kTcMatrixFloats / 4); i += kRows)
-        reinterpret_cast<float4*>(sb)[i] = __ldg(reinterpret_cast<const float4*>(tcm) + i);
+    for (uint32_t i = tid; i < nphases * (kTcOperandWords / 4); i += kRows)
+        reinterpret_cast<uint4*>(sb)[i] = __ldg(reinterpret_cast<const uint4*>(tcm) + i);
     for (uint32_t i = tid; i < nwords / 4; i += kRows)
         reinterpret_cast<uint4*>(sw)[i] = __ldg(reinterpret_cast<const uint4*>(words) + i);
     for (uint32_t i = tid; i < nsdata; i += kRows) sd[i] = static_cast<float>(__ldg(sdata + i));
@@ -361,8 +372,7 @@ __global__ void __launch_bounds__(1 << (MT - 4), MINB)
                 const uint32_t op = w & 0xffu;
                 if (op == cop::kEnd) break;
                 if (op == cop::kMma) {
-                    const uint32_t b0 = sb_addr + ((w >> 8) & 0xffu) * (kTcMatrixFloats * 4);
-                    tc_apply<kRows>(a, b0, b0 + kTcMatrixFloats * 2, c);
+                    tc_apply<kRows>(a, sb_addr + ((w >> 8) & 0xffu) * (kTcOperandWords * 4), c);
                     continue;
                 }
                 const uint32_t aux = (w >> 8) & 0xffu;
@@ -445,7 +455,7 @@ __global__ void __launch_bounds__(1 << (MT - 4), MINB)
 }
 
 template <int MT, int MINB, typename IDX>
-int launch_tc_instance(const TileLaunch& L, const float* tcm, uint32_t nphases, int* err) {
+int launch_tc_instance(const TileLaunch& L, const uint32_t* tcm, uint32_t nphases, int* err) {
     static const size_t dyn_max = [] {
         cudaFuncAttributes fa{};
         if (cudaFuncGetAttributes(&fa, k_tile_pass_tc<MT, MINB, IDX>) != cudaSuccess) return size_t{0};
@@ -466,7 +476,7 @@ int launch_tc_instance(const TileLaunch& L, const float* tcm, uint32_t nphases, 
 }  // namespace
 
 int launch_tile_pass_tc(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
-                        const double* dev_sdata, const float* dev_tc, int* dev_err, int sm_count, void* stream) {
+                        const double* dev_sdata, const uint32_t* dev_tc, int* dev_err, int sm_count, void* stream) {
     if (!pass.tc || (pass.m != 12 && pass.m != 13) || (pass.word_count & 3u) != 0) return MB2_ERR_INVALID;
     TileLaunch L;
     L.amps = amps;
@@ -478,14 +488,14 @@ int launch_tile_pass_tc(void* amps, uint32_t n, const TilePass& pass, const uint
     L.nsdata = pass.sdata_count;
     L.stream = stream;
     L.stages = 2;
-    L.smem = L.stages * (size_t{1} << pass.m) * sizeof(float2) + size_t{pass.tc_phases} * kTcMatrixFloats * 4 +
+    L.smem = L.stages * (size_t{1} << pass.m) * sizeof(float2) + size_t{pass.tc_phases} * kTcOperandWords * 4 +
              size_t{pass.word_count} * 4 + size_t{pass.sdata_count} * 4;
     L.ntiles = (uint64_t{1} << n) >> pass.m;
     L.n_all = n;
     const bool two = pass.m == 12;
     const uint64_t cap = static_cast<uint64_t>(sm_count) * (two ? 2u : 1u);
     L.grid = static_cast<int>(L.ntiles < cap ? L.ntiles : cap);
-    const float* tcm = dev_tc + pass.tc_begin;
+    const uint32_t* tcm = dev_tc + pass.tc_begin;
     int rc;
     if (two) rc = n <= 32 ? launch_tc_instance<12, 2, uint32_t>(L, tcm, pass.tc_phases, dev_err)
                           : launch_tc_instance<12, 2, uint64_t>(L, tcm, pass.tc_phases, dev_err);
@@ -495,7 +505,7 @@ int launch_tile_pass_tc(void* amps, uint32_t n, const TilePass& pass, const uint
     return rc;
 }
 
-int launch_tc_probe(const float* in, const float* b, float* out, int* dev_err, void* stream) {
+int launch_tc_probe(const float* in, const uint32_t* b, float* out, int* dev_err, void* stream) {
     k_tc_probe<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(reinterpret_cast<const float2*>(in), b,
                                                                  reinterpret_cast<float2*>(out), dev_err);
     note_launches(1);

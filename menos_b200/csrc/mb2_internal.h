@@ -122,7 +122,7 @@ struct TilePass {
     bool heavy = false;  // has two-qubit dense/monomial/permutation, kDiagK or kSmem words
     bool mid = false;    // heavy, but only through general dense two-qubit words (kGen2)
     // Tensor-core form (complex64, tile_tc.cpp): the pass's composed phase
-    // matrices are tcdata[tc_begin, tc_begin + tc_phases * kTcMatrixFloats).
+    // matrices are tcdata[tc_begin, tc_begin + tc_phases * kTcOperandWords).
     bool tc = false;
     uint32_t tc_begin = 0;
     uint32_t tc_phases = 0;
@@ -194,23 +194,31 @@ struct TileProgram {
     std::vector<uint32_t> words;  // compact stream of every pass (complex128 kernel)
     uint64_t fp64_per_amp = 0;    // modelled FP64 instructions per amplitude
     // Tensor-core passes: per composed phase matrix, its real 32x32 form as
-    // TF32 high and low parts in the MMA's shared-memory layout (tile_tc.cpp),
+    // FP16 high and low parts in the MMA's shared-memory layout (tile_tc.cpp),
     // and the matrix itself (16x16 complex, FP64) for the host interpreter.
-    std::vector<float> tcdata;
+    std::vector<uint32_t> tcdata;
     std::vector<Cd> tcmatrices;
 };
 // Writes prog.words and each pass's word range and parametric slice.
 void encode_compact(TileProgram& prog);
 
 // The complex64 tensor-core form of a planned program (tile_tc.cpp): each
-// pass without wide (k > 2) or parametric blocks becomes phases whose dense
-// gates on the four register qubits compose (in FP64) into one 16x16
-// complex matrix, applied as a split-TF32 tensor-core GEMM, with diagonals
-// that involve other tile qubits applied elementwise before or after it.  A
-// pass needing more than `max_phases` matrices is split into several passes
-// on the same tile.  Rewrites the passes, the staged data and the word stream.
-constexpr uint32_t kTcMatrixFloats = 2 * 32 * 32;  // TF32 high + low, 32x32 real each
-void make_tensor_core_program(TileProgram& prog, uint32_t max_phases);
+// pass without wide (k > 2), parametric or non-contractive blocks becomes
+// phases whose dense gates on the four register qubits compose (in FP64)
+// into one 16x16 complex matrix, applied as a split-FP16 tensor-core GEMM,
+// with diagonals that involve other tile qubits applied elementwise before
+// or after it.  A pass needing more than `max_phases` matrices is split into
+// several passes on the same tile.  Rewrites the passes, the staged data and
+// the word stream.
+// One phase matrix's operand: U's real 32x32 form as FP16 high parts (rows
+// 0-31) over FP16 low parts (rows 32-63), 4096 bytes.
+constexpr uint32_t kTcOperandWords = 1024;
+void make_tensor_core_program(TileProgram& prog, const std::vector<Block>& blocks, uint32_t max_phases);
+// Thread-bit order of a phase whose register bits are reg[0..nreg) (tile
+// positions): tperm[0..nthread) lists the other tile positions, the first
+// three of distinct residues mod 3 when possible (conflict-free shared-memory
+// slots under the tile kernels' XOR-fold swizzle).
+void thread_bit_order(uint32_t m, const uint32_t* reg, uint32_t nreg, uint8_t* tperm, uint8_t& nthread);
 
 // Applies a planned program's passes to a host state in FP64, instruction by
 // instruction (phase matrices exact, not split): the arithmetic the tile
@@ -320,16 +328,16 @@ int launch_scale_c64(void* amps, uint64_t n_amps, float s, void* stream);
 // form (TilePass::tc).  dev_tc: the program's tcdata on the device; dev_err:
 // a device word the kernel sets to a nonzero code if a bounded wait on the
 // tensor core ran out (the pass's result is then invalid).
-constexpr uint32_t kTcMaxPhasesTwoCtas = 5;   // 12-qubit tiles, two CTAs per SM
-constexpr uint32_t kTcMaxPhasesOneCta = 11;   // 13-qubit tiles, one CTA per SM
+constexpr uint32_t kTcMaxPhasesTwoCtas = 10;  // 12-qubit tiles, two CTAs per SM
+constexpr uint32_t kTcMaxPhasesOneCta = 22;   // 13-qubit tiles, one CTA per SM
 int launch_tile_pass_tc(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
-                        const double* dev_sdata, const float* dev_tc, int* dev_err, int sm_count, void* stream);
-// Debug probe of the tensor-core step alone: one CTA applies the split-TF32
-// operands b (kTcMatrixFloats floats, tile_tc.cpp's layout) to 256 rows of
-// 16 complex64 amplitudes (in -> out, device pointers).
-int launch_tc_probe(const float* in, const float* b, float* out, int* dev_err, void* stream);
-// Writes U (16x16 complex, row-major) as split-TF32 operands (kTcMatrixFloats floats).
-void tc_operands(const Cd* u, float* out);
+                        const double* dev_sdata, const uint32_t* dev_tc, int* dev_err, int sm_count, void* stream);
+// Debug probe of the tensor-core step alone: one CTA applies the split-FP16
+// operand b (kTcOperandWords words, tile_tc.cpp's layout) to 256 rows of 16
+// complex64 amplitudes (in -> out, device pointers).
+int launch_tc_probe(const float* in, const uint32_t* b, float* out, int* dev_err, void* stream);
+// Writes U (16x16 complex, row-major) as the split-FP16 operand (kTcOperandWords words).
+void tc_operands(const Cd* u, uint32_t* out);
 int context_device(const mb2_context* ctx);
 // The most staging memory a state's calls can hold for a sweep of these ops,
 // `shots` counts and `terms` Pauli terms, rounded as the state's grow-only

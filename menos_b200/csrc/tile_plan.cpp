@@ -99,11 +99,22 @@ std::vector<PassSel> select_passes(const std::vector<Block>& blocks, uint32_t n,
     return passes;
 }
 
+uint32_t push_matrix(std::vector<double>& data, const std::vector<Cd>& m) {
+    const uint32_t off = static_cast<uint32_t>(data.size());
+    for (const Cd& c : m) {
+        data.push_back(c.real());
+        data.push_back(c.imag());
+    }
+    return off;
+}
+
+}  // namespace
+
 // Thread-bit order for a phase whose register bits are `reg` (tile-local
 // positions): the first three thread bits get distinct residues mod 3 when
 // possible, so that the eight threads of a quarter warp hit eight distinct
 // 16-byte bank groups under the kernel's XOR-fold swizzle.
-void thread_order(uint32_t m, const uint32_t* reg, uint32_t nreg, uint8_t* tperm, uint8_t& nthread) {
+void thread_bit_order(uint32_t m, const uint32_t* reg, uint32_t nreg, uint8_t* tperm, uint8_t& nthread) {
     std::vector<uint32_t> free_pos;
     for (uint32_t p = 0; p < m; ++p)
         if (std::find(reg, reg + nreg, p) == reg + nreg) free_pos.push_back(p);
@@ -121,17 +132,6 @@ void thread_order(uint32_t m, const uint32_t* reg, uint32_t nreg, uint8_t* tperm
     nthread = static_cast<uint8_t>(order.size());
     for (size_t i = 0; i < order.size(); ++i) tperm[i] = static_cast<uint8_t>(order[i]);
 }
-
-uint32_t push_matrix(std::vector<double>& data, const std::vector<Cd>& m) {
-    const uint32_t off = static_cast<uint32_t>(data.size());
-    for (const Cd& c : m) {
-        data.push_back(c.real());
-        data.push_back(c.imag());
-    }
-    return off;
-}
-
-}  // namespace
 
 // Passes over a topological order of the blocks' dependencies (two blocks
 // depend when they share a qubit; blocks on disjoint qubits commute), for
@@ -378,7 +378,7 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
             TileInstr ph{};
             ph.op = TOP_PHASE;
             for (uint32_t s = 0; s < kRegQubits; ++s) ph.pos[s] = static_cast<uint8_t>(reg[s]);
-            thread_order(mt, reg, kRegQubits, ph.tperm, ph.nthread);
+            thread_bit_order(mt, reg, kRegQubits, ph.tperm, ph.nthread);
             prog.instrs.push_back(ph);
             open = true;
         };
