@@ -385,9 +385,10 @@ int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
  * num_qubits state (precision MB2_C64: the commuting plan and, unless
  * opts->c64_kernel says otherwise, its tensor-core form) on the host, in
  * FP64, instruction by instruction (phase matrices exact): state (2 * 2^n
- * doubles) in and out.  stats (5 words, optional): passes, tensor-core
+ * doubles) in and out.  stats (6 words, optional): passes, tensor-core
  * passes, phase matrices, tile qubits, the largest dynamic shared memory
- * (bytes) a tensor-core pass launches with.  Lets tests check the plan -- the
+ * (bytes) a tensor-core pass launches with, register layouts the
+ * tensor-core passes load.  Lets tests check the plan -- the
  * order of every block, each phase's composed matrix, the placement of
  * elementwise diagonals -- against the oracle on the CPU.  state NULL: the
  * stats only (up to 40 qubits); otherwise at most 28 qubits.  Has no

@@ -413,15 +413,15 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
         return MB2_OK;
     }
     mb2::TileProgram prog;
-    // complex64 passes on the tensor cores: 12- or 13-qubit tiles.
-    const bool tc = c64 && o.c64_kernel == 0 && (m == 12 || m == 13);
+    // complex64 passes on the tensor cores: 11- to 13-qubit tiles.
+    const bool tc = c64 && o.c64_kernel == 0 && m >= 11 && m <= 13;
     try {
         const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
                                                                          : static_cast<uint32_t>(o.low_qubits));
         // complex64 results are not bitwise the reference's: commuting
         // blocks may be reordered into fewer passes.
         prog = mb2::plan_tile_program(blocks, s->n, m, low, nullptr, c64);
-        if (tc) mb2::make_tensor_core_program(prog, blocks, m == 12 ? mb2::kTcMaxPhasesTwoCtas : mb2::kTcMaxPhasesOneCta);
+        if (tc) mb2::make_tensor_core_program(prog, blocks, mb2::tc_max_phases(m));
     } catch (const std::exception& e) {
         return fail(s->ctx, MB2_ERR_INVALID, e.what());
     }
@@ -768,14 +768,15 @@ int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
         const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
                                                                          : static_cast<uint32_t>(o.low_qubits));
         mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m, low, nullptr, c64);
-        const bool tc = c64 && o.c64_kernel == 0 && (m == 12 || m == 13);
-        if (tc) mb2::make_tensor_core_program(prog, blocks, m == 12 ? mb2::kTcMaxPhasesTwoCtas : mb2::kTcMaxPhasesOneCta);
+        const bool tc = c64 && o.c64_kernel == 0 && m >= 11 && m <= 13;
+        if (tc) mb2::make_tensor_core_program(prog, blocks, mb2::tc_max_phases(m));
         if (state != nullptr) mb2::run_program_on_host(prog, num_qubits, reinterpret_cast<mb2::Cd*>(state));
         if (stats != nullptr) {
-            uint64_t tcp = 0, smem = 0;
+            uint64_t tcp = 0, smem = 0, layouts = 0;
             for (const mb2::TilePass& p : prog.passes) {
                 if (!p.tc) continue;
                 tcp += 1;
+                for (uint32_t i = 0; i < p.prog_count; ++i) layouts += prog.instrs[p.prog_begin + i].op == mb2::TOP_PHASE;
                 smem = std::max<uint64_t>(smem, 2 * (8ull << p.m) + uint64_t{p.tc_phases} * mb2::kTcOperandWords * 4 +
                                                     4ull * p.word_count + 4ull * p.sdata_count);
             }
@@ -784,6 +785,7 @@ int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
             stats[2] = prog.tcmatrices.size() / 256;
             stats[3] = m;
             stats[4] = smem;
+            stats[5] = layouts;
         }
     } catch (const std::exception&) {
         return MB2_ERR_INVALID;

@@ -6,17 +6,20 @@
 // phase's dense gates are applied as one composed 16x16 complex matrix U on
 // the tensor cores (tile_tc.cpp builds the program):
 //
-//   each thread scales its row (32 floats, interleaved re/im) by a power of
-//   two that puts the row's largest magnitude in [2^13, 2^14), splits it into
-//   FP16 high and low parts and stores both into tensor memory (TMEM lane =
+//   a tile is scaled once, at its first phase, by the power of two that puts
+//   its norm in [2^13, 2^14) (unitary gates on tile qubits keep every
+//   amplitude below the norm), and unscaled when it is stored; each thread
+//   splits its row (32 floats, interleaved re/im) into FP16 high and low
+//   parts and stores both into tensor memory (TMEM lane =
 //   row within a 128-row block, two FP16 values per 32-bit column); one
 //   thread issues, per 128-row block, tcgen05.mma kind::f16 with A from
 //   tensor memory and B = U's operand in shared memory (FP16 high parts over
 //   low parts, N = 64): A_hi x [B_hi; B_lo] into 64 FP32 accumulator columns,
 //   then A_lo x B_hi accumulated into the first 32 (two K-steps of 16 each);
-//   tcgen05.commit signals an mbarrier; every thread reads its row back
-//   (tcgen05.ld), adds the two 32-column halves, undoes the scale and applies
-//   the phase's elementwise diagonals on registers.
+//   tcgen05.commit signals an mbarrier the issuing thread waits on; after a
+//   CTA barrier every thread reads its row back (tcgen05.ld), adds the two
+//   32-column halves and applies the phase's elementwise diagonals on
+//   registers.
 //
 // Every wait on the tensor core is bounded: a wait that runs out sets the
 // caller's error word, the CTA stops issuing work, frees its tensor memory
@@ -146,34 +149,47 @@ struct TcCtx {
     int* err;
 };
 
+// The power-of-two scale of a tile: 2^e puts the norm of the CTA's rows
+// in [2^13, 2^14), so every amplitude -- at most the norm, which the pass's
+// unitary gates on tile qubits preserve -- stays in FP16's range through all
+// phases (e <= 126 keeps 2^-e a normal float; a zero tile keeps e = 0).
+// Every thread of the CTA calls it; red: shared scratch of one float per warp.
+__device__ __forceinline__ int tile_scale_exp(const float2 (&a)[kNA], float* red) {
+    float ss = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kNA; ++j) ss = fmaf(a[j].x, a[j].x, fmaf(a[j].y, a[j].y, ss));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    if ((threadIdx.x & 31u) == 0) red[threadIdx.x >> 5] = ss;
+    __syncthreads();
+    float tot = 0.0f;
+    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) tot += red[w];
+    __syncthreads();  // red is free again
+    const int ex = static_cast<int>((__float_as_uint(sqrtf(tot)) >> 23) & 0xffu);
+    return ex == 0 ? 0 : max(-126, min(140 - ex, 126));
+}
+__device__ __forceinline__ float pow2f(int e) { return __uint_as_float(static_cast<uint32_t>(127 + e) << 23); }
+
 // a <- U a for this thread's row, U's operand (kTcOperandWords words, the
-// layout of tile_tc.cpp) at shared address b.  ROWS threads, ROWS / 128 row
-// blocks; TMEM columns: [0, 16 NB) high parts, [16 NB, 32 NB) low parts,
-// [32 NB, 96 NB) the products (64 per block).  All threads of the CTA call it.
+// layout of tile_tc.cpp) at shared address b; the row is already scaled
+// into FP16's range (tile_scale_exp).  ROWS threads, ROWS / 128 row blocks;
+// TMEM columns: [0, 16 NB) high parts, [16 NB, 32 NB) low parts,
+// [32 NB, 96 NB) the products (64 per block).  All threads of the CTA call
+// it; thread 0 issues the MMAs and waits for them.
 template <int ROWS>
 __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c) {
     constexpr uint32_t NB = ROWS / 128;
     const uint32_t tid = threadIdx.x;
     const uint32_t blk = tid >> 7;
     const uint32_t lane = (tid & 0x60u) << 16;  // this warp's lane quarter
-    // The row's scale: 2^e puts its largest magnitude in [2^13, 2^14)
-    // (e <= 126 keeps 2^-e a normal float; an all-zero row keeps e = 0).
-    float mx = 0.0f;
-#pragma unroll
-    for (int j = 0; j < kNA; ++j) mx = fmaxf(mx, fmaxf(fabsf(a[j].x), fabsf(a[j].y)));
-    const int ex = static_cast<int>((__float_as_uint(mx) >> 23) & 0xffu);
-    const int e = ex == 0 ? 0 : min(140 - ex, 126);
-    const float scale = __uint_as_float(static_cast<uint32_t>(127 + e) << 23);
-    const float unscale = __uint_as_float(static_cast<uint32_t>(127 - e) << 23);
     {
         uint32_t hi[16], lo[16];
 #pragma unroll
         for (int j = 0; j < kNA; ++j) {
-            const float x = a[j].x * scale, y = a[j].y * scale;
-            const __half2 h = __floats2half2_rn(x, y);
+            const __half2 h = __floats2half2_rn(a[j].x, a[j].y);
             const float2 hf = __half22float2(h);
             hi[j] = half2_bits(h);
-            lo[j] = half2_bits(__floats2half2_rn(x - hf.x, y - hf.y));
+            lo[j] = half2_bits(__floats2half2_rn(a[j].x - hf.x, a[j].y - hf.y));
         }
         tmem_st16(c.tmem + lane + 16 * blk, hi);
         tmem_st16(c.tmem + lane + 16 * NB + 16 * blk, lo);
@@ -194,14 +210,14 @@ __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c)
             mma_f16(d, al + 8, d1, kIdescN32, 1);
         }
         mma_commit(c.bar);
-    }
-    if (!abort) {
         if (!mbar_wait(c.bar, c.parity)) {
             *c.abort = 1;
             atomicExch(c.err, 1);
         }
-        c.parity ^= 1u;
     }
+    if (!abort) c.parity ^= 1u;
+    tc_fence_before();
+    __syncthreads();
     tc_fence_after();
     uint32_t v0[32], v1[32];
     tmem_ld32(c.tmem + lane + 32 * NB + 64 * blk, v0);
@@ -209,8 +225,8 @@ __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c)
     tmem_wait_ld();
 #pragma unroll
     for (int j = 0; j < kNA; ++j)
-        a[j] = make_float2((__uint_as_float(v0[2 * j]) + __uint_as_float(v1[2 * j])) * unscale,
-                           (__uint_as_float(v0[2 * j + 1]) + __uint_as_float(v1[2 * j + 1])) * unscale);
+        a[j] = make_float2(__uint_as_float(v0[2 * j]) + __uint_as_float(v1[2 * j]),
+                           __uint_as_float(v0[2 * j + 1]) + __uint_as_float(v1[2 * j + 1]));
 }
 
 // Sets up TMEM (warp 0), the mbarrier and the abort flag; the caller's
@@ -248,17 +264,23 @@ __global__ void __launch_bounds__(256, 1) k_tc_probe(const float2* __restrict__ 
         reinterpret_cast<uint4*>(sb)[i] = reinterpret_cast<const uint4*>(b)[i];
     fence_async_smem();
     TcCtx c = tc_setup<256>(&s_tmem, &s_bar, &s_abort, err);
+    __shared__ float s_red[8];
     float2 a[kNA];
 #pragma unroll
     for (int j = 0; j < kNA; ++j) a[j] = in[threadIdx.x * kNA + j];
+    const int e = tile_scale_exp(a, s_red);
+    const float scale = pow2f(e), unscale = pow2f(-e);
+#pragma unroll
+    for (int j = 0; j < kNA; ++j) a[j] = make_float2(a[j].x * scale, a[j].y * scale);
     tc_apply<256>(a, smem_addr(sb), c);
 #pragma unroll
-    for (int j = 0; j < kNA; ++j) out[threadIdx.x * kNA + j] = a[j];
+    for (int j = 0; j < kNA; ++j) out[threadIdx.x * kNA + j] = make_float2(a[j].x * unscale, a[j].y * unscale);
     tc_teardown<256>(c);
 }
 
 // ---- the pass ----------------------------------------------------------------
-// MT: tile qubits (12: 256 threads, two CTAs per SM; 13: 512 threads, one);
+// MT: tile qubits (11: 128 threads, four CTAs per SM; 12: 256 threads, two;
+// 13: 512 threads, one);
 // IDX: the amplitude index type.  Dynamic shared memory: `stages` tile
 // buffers, the pass's phase matrices, its words, its diagonal data (FP32).
 template <int MT, int MINB, typename IDX>
@@ -267,11 +289,12 @@ __global__ void __launch_bounds__(1 << (MT - 4), MINB)
                    uint32_t nwords, const double* __restrict__ sdata, uint32_t nsdata,
                    const uint32_t* __restrict__ tcm, uint32_t nphases, uint64_t ntiles, uint32_t stages, int* err) {
     constexpr uint32_t kRows = 1u << (MT - 4);
-    constexpr uint32_t kCols = kRows == 256 ? 256 : 512;
+    constexpr uint32_t kCols = kRows == 128 ? 128 : (kRows == 256 ? 256 : 512);
     extern __shared__ __align__(128) float2 smem_f[];
     __shared__ uint32_t s_tmem;
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ int s_abort;
+    __shared__ float s_red[kRows / 32];
     const uint32_t tid = threadIdx.x;
     constexpr uint32_t m = MT;
     constexpr uint32_t tbits = m - kRegQubits;
@@ -346,6 +369,9 @@ __global__ void __launch_bounds__(1 << (MT - 4), MINB)
 
         float2 a[kNA];
         uint32_t pc = 0;
+        // The tile's scale, set at its first phase; the tile is stored unscaled.
+        float unscale = 1.0f;
+        bool first = true;
         while (pc < nwords) {
             const uint32_t w0 = sw[pc];
             if ((w0 & 0xffu) != cop::kPhase) break;  // padding after the last phase
@@ -367,6 +393,14 @@ __global__ void __launch_bounds__(1 << (MT - 4), MINB)
             };
 #pragma unroll
             for (int j = 0; j < kNA; ++j) a[j] = at(j);
+            if (first) {
+                first = false;
+                const int e = tile_scale_exp(a, s_red);
+                const float scale = pow2f(e);
+                unscale = pow2f(-e);
+#pragma unroll
+                for (int j = 0; j < kNA; ++j) a[j] = make_float2(a[j].x * scale, a[j].y * scale);
+            }
             for (;;) {
                 const uint32_t w = sw[pc++];
                 const uint32_t op = w & 0xffu;
@@ -445,7 +479,10 @@ __global__ void __launch_bounds__(1 << (MT - 4), MINB)
         }
         const IDX b0 = cbase + off_lo;
 #pragma unroll
-        for (int j = 0; j < kNA; ++j) st[b0 + reg_off(j)] = tile[slot(j)];
+        for (int j = 0; j < kNA; ++j) {
+            const float2 v = tile[slot(j)];
+            st[b0 + reg_off(j)] = make_float2(v.x * unscale, v.y * unscale);
+        }
         cbase = advance(cbase);
         __syncthreads();
         if (*c.abort) break;
@@ -477,7 +514,7 @@ int launch_tc_instance(const TileLaunch& L, const uint32_t* tcm, uint32_t nphase
 
 int launch_tile_pass_tc(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
                         const double* dev_sdata, const uint32_t* dev_tc, int* dev_err, int sm_count, void* stream) {
-    if (!pass.tc || (pass.m != 12 && pass.m != 13) || (pass.word_count & 3u) != 0) return MB2_ERR_INVALID;
+    if (!pass.tc || pass.m < 11 || pass.m > 13 || (pass.word_count & 3u) != 0) return MB2_ERR_INVALID;
     TileLaunch L;
     L.amps = amps;
     L.m = pass.m;
@@ -492,15 +529,20 @@ int launch_tile_pass_tc(void* amps, uint32_t n, const TilePass& pass, const uint
              size_t{pass.word_count} * 4 + size_t{pass.sdata_count} * 4;
     L.ntiles = (uint64_t{1} << n) >> pass.m;
     L.n_all = n;
-    const bool two = pass.m == 12;
-    const uint64_t cap = static_cast<uint64_t>(sm_count) * (two ? 2u : 1u);
+    // Resident CTAs per SM: tensor memory (128, 256 or 512 columns per CTA)
+    // and shared memory allow four, two or one.
+    const uint32_t per_sm = pass.m == 11 ? 4u : (pass.m == 12 ? 2u : 1u);
+    const uint64_t cap = static_cast<uint64_t>(sm_count) * per_sm;
     L.grid = static_cast<int>(L.ntiles < cap ? L.ntiles : cap);
     const uint32_t* tcm = dev_tc + pass.tc_begin;
+    const bool i32 = n <= 32;
     int rc;
-    if (two) rc = n <= 32 ? launch_tc_instance<12, 2, uint32_t>(L, tcm, pass.tc_phases, dev_err)
-                          : launch_tc_instance<12, 2, uint64_t>(L, tcm, pass.tc_phases, dev_err);
-    else rc = n <= 32 ? launch_tc_instance<13, 1, uint32_t>(L, tcm, pass.tc_phases, dev_err)
-                      : launch_tc_instance<13, 1, uint64_t>(L, tcm, pass.tc_phases, dev_err);
+    if (pass.m == 11) rc = i32 ? launch_tc_instance<11, 4, uint32_t>(L, tcm, pass.tc_phases, dev_err)
+                               : launch_tc_instance<11, 4, uint64_t>(L, tcm, pass.tc_phases, dev_err);
+    else if (pass.m == 12) rc = i32 ? launch_tc_instance<12, 2, uint32_t>(L, tcm, pass.tc_phases, dev_err)
+                                    : launch_tc_instance<12, 2, uint64_t>(L, tcm, pass.tc_phases, dev_err);
+    else rc = i32 ? launch_tc_instance<13, 1, uint32_t>(L, tcm, pass.tc_phases, dev_err)
+                  : launch_tc_instance<13, 1, uint64_t>(L, tcm, pass.tc_phases, dev_err);
     note_launches(1);
     return rc;
 }

@@ -203,7 +203,7 @@ struct TileProgram {
 void encode_compact(TileProgram& prog);
 
 // The complex64 tensor-core form of a planned program (tile_tc.cpp): each
-// pass without wide (k > 2), parametric or non-contractive blocks becomes
+// pass without wide (k > 2), parametric or non-unitary blocks becomes
 // phases whose dense gates on the four register qubits compose (in FP64)
 // into one 16x16 complex matrix, applied as a split-FP16 tensor-core GEMM,
 // with diagonals that involve other tile qubits applied elementwise before
@@ -328,8 +328,12 @@ int launch_scale_c64(void* amps, uint64_t n_amps, float s, void* stream);
 // form (TilePass::tc).  dev_tc: the program's tcdata on the device; dev_err:
 // a device word the kernel sets to a nonzero code if a bounded wait on the
 // tensor core ran out (the pass's result is then invalid).
+constexpr uint32_t kTcMaxPhasesFourCtas = 5;  // 11-qubit tiles, four CTAs per SM
 constexpr uint32_t kTcMaxPhasesTwoCtas = 10;  // 12-qubit tiles, two CTAs per SM
 constexpr uint32_t kTcMaxPhasesOneCta = 22;   // 13-qubit tiles, one CTA per SM
+inline uint32_t tc_max_phases(uint32_t m) {
+    return m == 11 ? kTcMaxPhasesFourCtas : (m == 12 ? kTcMaxPhasesTwoCtas : kTcMaxPhasesOneCta);
+}
 int launch_tile_pass_tc(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
                         const double* dev_sdata, const uint32_t* dev_tc, int* dev_err, int sm_count, void* stream);
 // Debug probe of the tensor-core step alone: one CTA applies the split-FP16

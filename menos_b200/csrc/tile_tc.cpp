@@ -21,9 +21,11 @@
 // times U^T, as real operands rows x 32 and 32 x 32 (interleaved re/im).
 // The kernel (kernels_tc.cu) runs it on tcgen05 tensor cores with FP16
 // operands and FP32 accumulation, each operand split into an FP16 high part
-// and an FP16 low part (x = hi + lo to 22 bits; the rows are scaled by a
-// power of two first, so their magnitudes sit in FP16's range) and the
-// products hi*hi + hi*lo + lo*hi summed.  This file writes U's operand:
+// and an FP16 low part (x = hi + lo to 22 bits; the amplitudes are scaled by
+// a power of two first, so their magnitudes sit in FP16's range) and the
+// products hi*hi + hi*lo + lo*hi summed; the tile is scaled by a power of
+// two once per pass, which needs every block of a tensor-core pass to be
+// unitary (it keeps the tile's norm).  This file writes U's operand:
 // 64 rows of 32 FP16 values -- rows 0-31 the high parts of U's real form
 // (row = output re/im, column = input re/im), rows 32-63 the low parts --
 // K-major, no swizzle, in 8-row x 16-byte core matrices: element (n, k) at
@@ -104,6 +106,17 @@ void left_diag(std::vector<Cd>& u, const Cd* d, const uint32_t* sl, uint32_t k) 
         for (uint32_t t = 0; t < k; ++t) e |= ((r >> sl[t]) & 1u) << t;
         for (uint32_t c = 0; c < kDim; ++c) u[r * kDim + c] *= d[e];
     }
+}
+
+bool is_unitary(const Block& b) {
+    const uint32_t dim = 1u << b.k;
+    for (uint32_t r = 0; r < dim; ++r)
+        for (uint32_t c = 0; c < dim; ++c) {
+            Cd dot = 0.0;
+            for (uint32_t i = 0; i < dim; ++i) dot += std::conj(b.m[i * dim + r]) * b.m[i * dim + c];
+            if (std::abs(dot - (r == c ? Cd(1.0, 0.0) : Cd(0.0, 0.0))) > 1e-10) return false;
+        }
+    return true;
 }
 
 }  // namespace
@@ -263,15 +276,14 @@ void make_tensor_core_program(TileProgram& prog, const std::vector<Block>& block
     for (size_t pi = 0; pi < prog.passes.size(); ++pi) {
         const TilePass& src = prog.passes[pi];
         const std::vector<uint32_t>& mem = members[pi];
-        // Convertible: no wide dense or parametric blocks, and every entry of
-        // at most unit modulus (products of such matrices stay in the FP16
-        // operand's range; unitary gates always are).
+        // Convertible: no wide dense or parametric blocks, and every block
+        // unitary (to 1e-10): the pass then preserves each tile's norm, which
+        // the kernel's FP16 scaling relies on.
         bool convertible = src.param_len == 0 && !mem.empty();
         for (uint32_t i : mem) {
             const Block& b = blocks[i];
             if (!b.diagonal && b.k > 2) convertible = false;
-            for (const Cd& z : b.m)
-                if (std::abs(z) > 1.0 + 1e-9) convertible = false;
+            if (convertible && !is_unitary(b)) convertible = false;
         }
         if (!convertible) {  // kept as it is, for the FP32 SIMT kernel
             const TileInstr* ins = prog.instrs.data() + src.prog_begin;

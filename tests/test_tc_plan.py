@@ -20,7 +20,7 @@ def run_plan(circ, tile=0, kernel=0, fuse=True):
     n = circ.num_qubits
     st = np.zeros(1 << n, np.complex128)
     st[0] = 1.0
-    stats = np.zeros(5, np.uint64)
+    stats = np.zeros(6, np.uint64)
     opts = _lib.SweepOptions(1 if fuse else 0, 0, tile, 0, kernel)
     rc = _lib.lib().mb2_debug_run_plan(arr, len(circ.ops), C.byref(opts), n, C64, st.ctypes.data, stats.ctypes.data)
     assert rc == 0
