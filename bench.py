@@ -82,8 +82,8 @@ def parse():
     p.add_argument("--load", type=float, default=4.0, help="serve: arrival rate / plain-loop capacity")
     p.add_argument("--bindings", type=int, default=4096)
     p.add_argument("--precision", default="c128", choices=["c128", "c64"], help="serve/batch: state precision")
-    p.add_argument("--c64-kernel", default="tensor", choices=["tensor", "simt"],
-                   help="complex64 passes: tensor cores (split-TF32 GEMMs) or FP32 SIMT gates")
+    p.add_argument("--c64-kernel", default="auto", choices=["auto", "tensor", "simt"],
+                   help="complex64 passes: tensor cores (split-FP16 GEMMs), FP32 SIMT gates, or automatic")
     return p.parse_args()
 
 
@@ -582,7 +582,7 @@ def main_c64(args, local):
         "error_28q_vs_complex128": {"max_abs_amp": d_amp, "max_abs_pauli": d_exp, "paulis": 64},
         "dtype": "c64 (f32 amplitudes, f64 reductions)",
         "config": {"workload": f"brick({n}, 32), state {8 << n >> 30} GiB", "seed": 20260929,
-                   "c64_kernel": args.c64_kernel, "tile_qubits": args.tile or 12},
+                   "c64_kernel": args.c64_kernel, "tile_qubits": args.tile or "auto"},
         "data": "synthetic (seeded circuit)",
     }
     print(json.dumps(line), flush=True)

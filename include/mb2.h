@@ -122,8 +122,11 @@ typedef struct mb2_sweep_options {
     int32_t low_qubits;      /* qubits 0..low-1 held in every tile (contiguous runs); -1 = none, 0 = default 3 */
     int32_t tile_qubits;     /* qubits per multi-gate tile pass; 0 = autotuned */
     int32_t per_gate;        /* 1: one launch per block, no tiling (the reference's sweep shape) */
-    int32_t c64_kernel;      /* complex64 states: 0 = tensor cores (split-TF32 GEMMs of each phase's
-                                composed 16x16 matrix) wherever a pass allows, 1 = FP32 SIMT gates only */
+    int32_t c64_kernel;      /* complex64 states: 0 = automatic (tensor cores for states of more than
+                                2^24 amplitudes, which stream from HBM; FP32 SIMT gates below, where
+                                the state stays in L2), 1 = FP32 SIMT gates only, 2 = tensor cores
+                                (split-FP16 GEMMs of each phase's composed 16x16 matrix) wherever a
+                                pass allows */
 } mb2_sweep_options;
 
 /* Applies a whole operation list (MeasureOps skipped) as a sequence of

@@ -165,6 +165,25 @@ uint32_t tile_width(uint32_t requested, uint32_t n, const std::vector<mb2::Block
     return std::min(m, mb2::kMaxTileQubits);
 }
 
+// A complex64 sweep's tile width and kernel.  Automatic: the tensor-core
+// pass for states of more than 2^24 amplitudes (which stream from HBM, where
+// it is the faster one) at 11-qubit tiles up to 28 qubits and 12 above; the
+// FP32 SIMT pass below, at the context's complex64 tile width.
+struct C64Choice {
+    uint32_t m;
+    bool tc;
+};
+C64Choice c64_choice(const mb2_sweep_options& o, uint32_t n, uint32_t default_tile,
+                     const std::vector<mb2::Block>& blocks) {
+    const bool want_tc = o.c64_kernel == 2 || (o.c64_kernel == 0 && n > 24);
+    uint32_t m = o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits)
+                                   : (want_tc && o.c64_kernel == 0 ? (n <= 28 ? 11u : 12u) : default_tile);
+    m = std::min(std::min(m, mb2::kMaxTileQubitsC64), n);
+    for (const mb2::Block& b : blocks) m = std::max(m, b.k);
+    m = std::max(m, mb2::kMinTileQubits);
+    return {m, want_tc && m >= 11 && m <= 13};
+}
+
 }  // namespace
 
 namespace mb2 {
@@ -390,16 +409,14 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     const bool c64 = s->precision == MB2_C64;
     uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : s->ctx->tile_c128.load(), s->n,
                             blocks);
+    bool tc = false;
     if (c64) {
-        // 8-byte amplitudes: up to 13-qubit tiles fit the same shared memory;
-        // 12 by default (two CTAs per SM).
-        m = o.tile_qubits > 0 ? std::min<uint32_t>(static_cast<uint32_t>(o.tile_qubits), mb2::kMaxTileQubitsC64)
-                              : std::min<uint32_t>(s->ctx->tile_c64.load() ? s->ctx->tile_c64.load()
-                                                                            : mb2::kDefaultTileQubitsC64,
-                                                   s->n);
-        for (const mb2::Block& b : blocks) m = std::max(m, b.k);
-        m = std::max(m, mb2::kMinTileQubits);
+        // 8-byte amplitudes: up to 13-qubit tiles fit the same shared memory.
         if (s->n < mb2::kMinTileQubits) return fail(s->ctx, MB2_ERR_UNSUPPORTED, "complex64 states need >= 4 qubits");
+        const uint32_t tile64 = s->ctx->tile_c64.load() ? s->ctx->tile_c64.load() : mb2::kDefaultTileQubitsC64;
+        const C64Choice ch = c64_choice(o, s->n, tile64, blocks);
+        m = ch.m;
+        tc = ch.tc;
     }
     if (!c64 && (o.per_gate != 0 || s->n < mb2::kMinTileQubits)) {
         for (const mb2::Block& b : blocks) {
@@ -413,8 +430,6 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
         return MB2_OK;
     }
     mb2::TileProgram prog;
-    // complex64 passes on the tensor cores: 11- to 13-qubit tiles.
-    const bool tc = c64 && o.c64_kernel == 0 && m >= 11 && m <= 13;
     try {
         const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
                                                                          : static_cast<uint32_t>(o.low_qubits));
@@ -761,14 +776,18 @@ int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
         const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
         if (blocks.empty()) return MB2_OK;
         const bool c64 = precision == MB2_C64;
-        uint32_t m = c64 ? (o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : mb2::kDefaultTileQubitsC64)
-                         : tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, num_qubits, blocks);
-        for (const mb2::Block& b : blocks) m = std::max(m, b.k);
+        uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, num_qubits, blocks);
+        bool tc = false;
+        if (c64) {
+            if (num_qubits < mb2::kMinTileQubits) return MB2_ERR_UNSUPPORTED;
+            const C64Choice ch = c64_choice(o, num_qubits, mb2::kDefaultTileQubitsC64, blocks);
+            m = ch.m;
+            tc = ch.tc;
+        }
         m = std::min(std::max(m, mb2::kMinTileQubits), num_qubits);
         const uint32_t low = o.low_qubits < 0 ? 0u : (o.low_qubits == 0 ? mb2::kDefaultFixedLow
                                                                          : static_cast<uint32_t>(o.low_qubits));
         mb2::TileProgram prog = mb2::plan_tile_program(blocks, num_qubits, m, low, nullptr, c64);
-        const bool tc = c64 && o.c64_kernel == 0 && m >= 11 && m <= 13;
         if (tc) mb2::make_tensor_core_program(prog, blocks, mb2::tc_max_phases(m));
         if (state != nullptr) mb2::run_program_on_host(prog, num_qubits, reinterpret_cast<mb2::Cd*>(state));
         if (stats != nullptr) {

@@ -13,13 +13,13 @@
 //   parts and stores both into tensor memory (TMEM lane =
 //   row within a 128-row block, two FP16 values per 32-bit column); one
 //   thread issues, per 128-row block, tcgen05.mma kind::f16 with A from
-//   tensor memory and B = U's operand in shared memory (FP16 high parts over
-//   low parts, N = 64): A_hi x [B_hi; B_lo] into 64 FP32 accumulator columns,
+//   tensor memory and B = 2^12 U's operand in shared memory (FP16 high parts
+//   over low parts, N = 64): A_hi x [B_hi; B_lo] into 64 FP32 accumulator columns,
 //   then A_lo x B_hi accumulated into the first 32 (two K-steps of 16 each);
 //   tcgen05.commit signals an mbarrier the issuing thread waits on; after a
 //   CTA barrier every thread reads its row back (tcgen05.ld), adds the two
-//   32-column halves and applies the phase's elementwise diagonals on
-//   registers.
+//   32-column halves, takes out the 2^12 and applies the phase's elementwise
+//   diagonals on registers.
 //
 // Every wait on the tensor core is bounded: a wait that runs out sets the
 // caller's error word, the CTA stops issuing work, frees its tensor memory
@@ -223,10 +223,11 @@ __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c)
     tmem_ld32(c.tmem + lane + 32 * NB + 64 * blk, v0);
     tmem_ld32(c.tmem + lane + 32 * NB + 64 * blk + 32, v1);
     tmem_wait_ld();
+    constexpr float kUnscale = static_cast<float>(1.0 / kTcOperandScale);
 #pragma unroll
     for (int j = 0; j < kNA; ++j)
-        a[j] = make_float2(__uint_as_float(v0[2 * j]) + __uint_as_float(v1[2 * j]),
-                           __uint_as_float(v0[2 * j + 1]) + __uint_as_float(v1[2 * j + 1]));
+        a[j] = make_float2((__uint_as_float(v0[2 * j]) + __uint_as_float(v1[2 * j])) * kUnscale,
+                           (__uint_as_float(v0[2 * j + 1]) + __uint_as_float(v1[2 * j + 1])) * kUnscale);
 }
 
 // Sets up TMEM (warp 0), the mbarrier and the abort flag; the caller's

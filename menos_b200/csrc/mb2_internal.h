@@ -213,6 +213,7 @@ void encode_compact(TileProgram& prog);
 // One phase matrix's operand: U's real 32x32 form as FP16 high parts (rows
 // 0-31) over FP16 low parts (rows 32-63), 4096 bytes.
 constexpr uint32_t kTcOperandWords = 1024;
+constexpr double kTcOperandScale = 4096.0;  // U's operand is 2^12 U
 void make_tensor_core_program(TileProgram& prog, const std::vector<Block>& blocks, uint32_t max_phases);
 // Thread-bit order of a phase whose register bits are reg[0..nreg) (tile
 // positions): tperm[0..nthread) lists the other tile positions, the first

@@ -67,7 +67,7 @@ uint64_t admission_bytes(const Request& r) {
     const uint64_t staging =
         mb2::scratch_bound(r.n, r.ops.data(), static_cast<uint32_t>(r.ops.size()),
                            r.output == MB2_OUT_COUNTS ? r.shots : 0,
-                           r.output == MB2_OUT_EXPECTATION ? static_cast<uint32_t>(r.xs.size()) : 0);
+                           r.output == MB2_OUT_EXPECTATION ? static_cast<uint32_t>(r.xs.size()) + 1 : 1);
     return pool(state) + pool(staging);
 }
 
@@ -119,18 +119,31 @@ void run_request(mb2_server* s, cudaStream_t stream, Request& r, Done& d) {
         mb2_sweep_options o{r.fuse, 0, 0, 0};
         rc = mb2_apply_program(st, r.ops.data(), static_cast<uint32_t>(r.ops.size()), &o);
     }
+    // A complex64 state is renormalised in FP64 (its norm drifts by FP32
+    // roundings over a deep circuit): <H> is divided by the norm, read in the
+    // same grouped pass as the terms (the identity term); counts are drawn
+    // from the rescaled state.  complex128 results stay the reference's.
+    const bool c64 = r.precision == MB2_C64;
     if (rc == MB2_OK && r.output == MB2_OUT_EXPECTATION) {
-        std::vector<double> terms(2 * r.xs.size());
-        rc = mb2_expectation(st, r.xs.data(), r.zs.data(), static_cast<uint32_t>(r.xs.size()), terms.data());
+        std::vector<uint64_t> xs(r.xs), zs(r.zs);
+        if (c64) {
+            xs.push_back(0);
+            zs.push_back(0);
+        }
+        std::vector<double> terms(2 * xs.size());
+        rc = mb2_expectation(st, xs.data(), zs.data(), static_cast<uint32_t>(xs.size()), terms.data());
         double total = 0.0;
         for (size_t t = 0; t < r.xs.size() && rc == MB2_OK; ++t) total += r.coefs[t] * terms[2 * t];
+        if (c64 && rc == MB2_OK) total /= terms[2 * r.xs.size()];
         d.c.value = total;
     } else if (rc == MB2_OK && r.output == MB2_OUT_COUNTS) {
+        if (c64) rc = mb2_normalize(st, nullptr);
         d.outcomes.resize(std::max<uint64_t>(1, r.shots));
         d.counts.resize(std::max<uint64_t>(1, r.shots));
         uint64_t distinct = d.outcomes.size();
-        rc = mb2_sample(st, r.shots, r.seed, r.targets.data(), static_cast<uint32_t>(r.targets.size() / 2),
-                        d.outcomes.data(), d.counts.data(), &distinct);
+        if (rc == MB2_OK)
+            rc = mb2_sample(st, r.shots, r.seed, r.targets.data(), static_cast<uint32_t>(r.targets.size() / 2),
+                            d.outcomes.data(), d.counts.data(), &distinct);
         d.outcomes.resize(rc == MB2_OK ? distinct : 0);
         d.counts.resize(rc == MB2_OK ? distinct : 0);
         d.c.num_outcomes = rc == MB2_OK ? distinct : 0;

@@ -25,7 +25,9 @@
 // a power of two first, so their magnitudes sit in FP16's range) and the
 // products hi*hi + hi*lo + lo*hi summed; the tile is scaled by a power of
 // two once per pass, which needs every block of a tensor-core pass to be
-// unitary (it keeps the tile's norm).  This file writes U's operand:
+// unitary (it keeps the tile's norm), and U by 2^12 (kTcOperandScale: the
+// low part of an entry as small as 2^-14 is still an FP16 normal), undone
+// when the product is read back.  This file writes U's operand:
 // 64 rows of 32 FP16 values -- rows 0-31 the high parts of U's real form
 // (row = output re/im, column = input re/im), rows 32-63 the low parts --
 // K-major, no swizzle, in 8-row x 16-byte core matrices: element (n, k) at
@@ -125,10 +127,11 @@ void tc_operands(const Cd* u, uint32_t* out) {
     auto* h = reinterpret_cast<uint16_t*>(out);  // little-endian: element k even in a word's low half
     for (uint32_t n = 0; n < 32; ++n) {
         for (uint32_t k = 0; k < 32; ++k) {
-            // Real form of U: out_re = Re U in_re - Im U in_im, out_im = Im U in_re + Re U in_im.
+            // Real form of U: out_re = Re U in_re - Im U in_im, out_im = Im U in_re + Re U in_im,
+            // scaled by kTcOperandScale so that the low parts of small entries stay FP16 normals.
             const Cd z = u[(n >> 1) * kDim + (k >> 1)];
             const uint32_t cn = n & 1u, ck = k & 1u;
-            const double v = cn == ck ? z.real() : (cn == 0 ? -z.imag() : z.imag());
+            const double v = (cn == ck ? z.real() : (cn == 0 ? -z.imag() : z.imag())) * kTcOperandScale;
             const uint16_t hi = to_half(v);
             const uint16_t lo = to_half(v - from_half(hi));
             auto at = [&](uint32_t row) { return (row / 8) * 256 + (k / 8) * 64 + (row % 8) * 8 + (k % 8); };

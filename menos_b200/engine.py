@@ -169,15 +169,17 @@ class DeviceState:
         self._chk(f(self.h, m.ctypes.data, q.ctypes.data, len(q)), "mb2_apply_matrix")
 
     def apply_program(self, circ: Circuit, fuse_gates: bool = True, tile_qubits: int = 0,
-                      per_gate: bool = False, low_qubits: int = 0, c64_kernel: str = "tensor") -> SweepStats:
+                      per_gate: bool = False, low_qubits: int = 0, c64_kernel: str = "auto") -> SweepStats:
         """c64_kernel (complex64 states): "tensor" -- each phase's gates as one
-        split-TF32 tensor-core GEMM wherever a pass allows; "simt" -- FP32
-        gates one by one."""
+        split-FP16 tensor-core GEMM wherever a pass allows; "simt" -- FP32
+        gates one by one; "auto" -- tensor cores for states of more than 2^24
+        amplitudes, SIMT below."""
         arr, keep = to_mb2_ops(circ)
-        if c64_kernel not in ("tensor", "simt"):
-            raise ValueError("c64_kernel is 'tensor' or 'simt'")
+        kernels = {"auto": 0, "simt": 1, "tensor": 2}
+        if c64_kernel not in kernels:
+            raise ValueError("c64_kernel is 'auto', 'tensor' or 'simt'")
         opts = SweepOptions(1 if fuse_gates else 0, low_qubits, tile_qubits, 1 if per_gate else 0,
-                            0 if c64_kernel == "tensor" else 1)
+                            kernels[c64_kernel])
         self._chk(lib().mb2_apply_program(self.h, arr, len(circ.ops), C.byref(opts)), "mb2_apply_program")
         del keep
         return self.stats()

@@ -100,7 +100,9 @@ def test_poll_times_out_when_idle(ctx):
 
 def test_complex64_requests_same_alone_and_in_the_mix(ctx):
     # The precision path through the server: each result equals the same
-    # request run alone in complex64, and <H> is within 1e-6 of complex128.
+    # request run alone in complex64 -- renormalised in FP64: <H> divided by
+    # the norm read with the terms, counts from the rescaled state -- and <H>
+    # is within 1e-6 of complex128.
     from menos_b200._lib import C64
     reqs = workloads.serving_stream(24, 1000.0, 11, nmin=8, nmax=18, dmin=2, dmax=10, shots=2048, terms=16)
     srv = Server(ctx, slots=8)
@@ -121,10 +123,12 @@ def test_complex64_requests_same_alone_and_in_the_mix(ctx):
         st.init(circ.global_phase)
         st.apply_program(circ)
         if r["output"] == "counts":
+            st.normalize()
             assert c["counts"] == st.sample(r["shots"], r["seed"], [(q, q) for q in range(circ.num_qubits)])
         else:
-            terms = st.expectation(r["paulis"])
-            assert c["value"] == sum(w * v.real for w, v in zip(r["coefs"], terms))
+            terms = st.expectation(list(r["paulis"]) + [(0, 0)])
+            value = sum(w * v.real for w, v in zip(r["coefs"], terms)) / terms[-1].real
+            assert c["value"] == value
             assert abs(c["value"] - alone(ctx, r)) <= 1e-6
 
 

@@ -15,7 +15,7 @@ from menos_b200.engine import C64
 from test_host import as_oracle_circuit
 
 
-def run_plan(circ, tile=0, kernel=0, fuse=True):
+def run_plan(circ, tile=0, kernel=2, fuse=True):
     arr, keep = to_mb2_ops(circ)
     n = circ.num_qubits
     st = np.zeros(1 << n, np.complex128)
