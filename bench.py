@@ -74,12 +74,14 @@ def parse():
     p.add_argument("--shots", type=int, default=1_000_000)
     p.add_argument("--terms", type=int, default=64)
     p.add_argument("--tile", type=int, default=0)
+    p.add_argument("--fusion", type=int, default=0,
+                   help="job: 0 = the reference's containment fusion; 2..6 = blocks of up to that many qubits")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--validate-cpu", action="store_true",
                    help="with --impl reference: the extrapolated CPU job time against a whole reference run")
     p.add_argument("--mode", default="job", choices=["job", "serve", "batch", "c64"])
     p.add_argument("--requests", type=int, default=600)
-    p.add_argument("--load", type=float, default=4.0, help="serve: arrival rate / plain-loop capacity")
+    p.add_argument("--load", default="4", help="serve: arrival rate / plain-loop capacity (comma list: a sweep)")
     p.add_argument("--bindings", type=int, default=4096)
     p.add_argument("--precision", default="c128", choices=["c128", "c64"], help="serve/batch: state precision")
     p.add_argument("--c64-kernel", default="auto", choices=["auto", "tensor", "simt"],
@@ -240,7 +242,7 @@ def main():
 
     def step():
         st.init(0.0)
-        stats = st.apply_program(circ, tile_qubits=args.tile)
+        stats = st.apply_program(circ, tile_qubits=args.tile, fusion_width=args.fusion)
         norm = st.norm()
         terms = st.expectation(paulis)
         counts = st.sample(args.shots, 1234, targets)
@@ -275,7 +277,7 @@ def main():
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        stats = st.apply_program(circ, tile_qubits=args.tile)
+        stats = st.apply_program(circ, tile_qubits=args.tile, fusion_width=args.fusion)
         b.record(stream)
         b.synchronize()
         sweep_ms.append(a.elapsed_time(b))
@@ -286,7 +288,7 @@ def main():
 
     # ---- end to end through the engine's public API (host circuit in, host results out)
     from menos_b200 import B200DenseEngine, EngineExecutionRequest, PauliTerm
-    eng = B200DenseEngine(local, tile_qubits=args.tile)
+    eng = B200DenseEngine(local, tile_qubits=args.tile, fusion_width=args.fusion)
     req = EngineExecutionRequest(num_qubits=n, operations=circ, want_counts=True, want_expectation=True,
                                  shots=args.shots, seed=1234, measure_targets=targets, bitstring_width=n,
                                  observable=[PauliTerm(0, 0)] + [PauliTerm(x, z) for x, z in paulis])
@@ -318,7 +320,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": round(job_ms / args.steps, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded circuit)",
         "config": {"workload": f"{n}q complex128: brick depth {args.depth} + QFT ({len(circ.ops)} gates), "
-                               f"fusion=containment, norm + {args.terms} Paulis + {args.shots} shots",
+                               (f"fusion=containment" if args.fusion == 0 else f"fusion<={args.fusion} qubits") +
+                               f", norm + {args.terms} Paulis + {args.shots} shots",
                    "qubits": n, "parallelism": f"replicas x{world}", "l2": "state 16 GiB >> L2 (no flush)",
                    "passes": passes, "blocks": int(stats.blocks), "sweep_ms": round(sweep_avg, 2),
                    "tile_qubits": args.tile or 11},
@@ -389,17 +392,15 @@ def main_serve(args, local):
         service.append(time.perf_counter() - t0)
     plain_total = time.perf_counter() - t_all
     plain_rate = len(reqs) / plain_total
-    rate = args.load * plain_rate
-    arrivals = [r["arrival_s"] / rate for r in reqs]  # the stream was drawn at rate 1
+    loads = [float(x) for x in str(args.load).split(",")]
 
-    def fifo_latencies():
+    def fifo_latencies(arrivals):
         lat, free_at = [], 0.0
         for a, s in zip(arrivals, service):
             start = max(a, free_at)
             free_at = start + s
             lat.append(free_at - a)
-        return lat, free_at
-    plain_lat, plain_end = fifo_latencies()
+        return lat
 
     from menos_b200._lib import C64, C128
     prec = C64 if args.precision == "c64" else C128
@@ -434,32 +435,43 @@ def main_serve(args, local):
         return done, results, total, failed
 
     burst_done, burst_res, burst_total, burst_failed = serve(None)
-    live_done, live_res, live_total, live_failed = serve(arrivals)
-    # Each result the same in the burst and in the live mix; against the
+    # The live stream at each load: Poisson arrivals at load x the plain
+    # loop's capacity (the stream was drawn at rate 1 and is rescaled).
+    live, live_failed, mix_same = [], {}, True
+    for load in loads:
+        rate = load * plain_rate
+        arrivals = [r["arrival_s"] / rate for r in reqs]
+        done, res, total, failed = serve(arrivals)
+        live_failed.update(failed)
+        for k in range(len(reqs)):
+            if k not in burst_failed and k not in failed:
+                mix_same = mix_same and (burst_res[k] == res[k])
+        lat = [done[k] for k in range(len(reqs))]
+        plain_lat = fifo_latencies(arrivals)
+        live.append({"arrival_rate_per_s": round(rate, 2), "load_vs_plain_capacity": load,
+                     "circuits_per_s": round(len(reqs) / total, 2),
+                     "p50_ms": round(1e3 * percentile(lat, 50), 2), "p99_ms": round(1e3 * percentile(lat, 99), 2),
+                     "plain_fifo_p50_ms": round(1e3 * percentile(plain_lat, 50), 2),
+                     "plain_fifo_p99_ms": round(1e3 * percentile(plain_lat, 99), 2)})
+    # Each result the same in the burst and in the live mixes; against the
     # complex128 plain loop: identical counts and <H> (complex128), or <H>
     # within the precision path's error (complex64; counts then follow the
     # complex64 probabilities).
-    worst_exp, counts_same, mix_same = 0.0, True, True
+    worst_exp, counts_same = 0.0, True
     for k, r in enumerate(reqs):
         if k in burst_failed or k in live_failed:
             continue
-        mix_same = mix_same and (burst_res[k] == live_res[k])
         if r["output"] == "counts":
             counts_same = counts_same and (burst_res[k] == plain_out[k])
         else:
             worst_exp = max(worst_exp, abs(burst_res[k] - plain_out[k]))
-    live_lat = [live_done[k] for k in range(len(reqs))]
     line = {
         "metric": "served circuits/s (continuous batching) vs sequential plain loop", "unit": "circuits/s",
         "mode": "serve", "requests": len(reqs), "higher_is_better": True,
         "value": round(len(reqs) / burst_total, 2),
         "plain_loop": {"circuits_per_s": round(plain_rate, 2), "total_s": round(plain_total, 3)},
         "speedup_vs_plain": round(plain_total / burst_total, 2),
-        "live": {"arrival_rate_per_s": round(rate, 2), "load_vs_plain_capacity": args.load,
-                 "circuits_per_s": round(len(reqs) / live_total, 2),
-                 "p50_ms": round(1e3 * percentile(live_lat, 50), 2), "p99_ms": round(1e3 * percentile(live_lat, 99), 2),
-                 "plain_fifo_p50_ms": round(1e3 * percentile(plain_lat, 50), 2),
-                 "plain_fifo_p99_ms": round(1e3 * percentile(plain_lat, 99), 2)},
+        "live": live,
         "failed_requests": {"burst": len(burst_failed), "live": len(live_failed),
                             "statuses": sorted(set(burst_failed.values()) | set(live_failed.values()))},
         "results": {"burst_equals_live": mix_same, "counts_identical_to_plain_c128": counts_same,

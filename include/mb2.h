@@ -127,6 +127,9 @@ typedef struct mb2_sweep_options {
                                 the state stays in L2), 1 = FP32 SIMT gates only, 2 = tensor cores
                                 (split-FP16 GEMMs of each phase's composed 16x16 matrix) wherever a
                                 pass allows */
+    int32_t fusion_width;    /* with fuse_gates: 0 = the reference's containment rule; 2..6 = the same
+                                plan structure, a gate joining while its block spans at most this
+                                many qubits (mb2_fusion_plan gives the plan) */
 } mb2_sweep_options;
 
 /* Applies a whole operation list (MeasureOps skipped) as a sequence of
@@ -144,6 +147,18 @@ int mb2_apply_program(mb2_state* state, const mb2_op* ops, uint32_t num_ops,
 typedef int (*mb2_boundary_fn)(void* user, uint64_t blocks_done);
 int mb2_apply_program_monitored(mb2_state* state, const mb2_op* ops, uint32_t num_ops,
                                 const mb2_sweep_options* opts, mb2_boundary_fn boundary, void* user);
+
+/* The fusion plan a sweep with these options applies, in the arrays of the
+ * reference's ir::FusionPlan (src/ir/fuse_gates.h:38-76): block b is the ops
+ * order[block_begin[b] .. block_begin[b+1]) on the qubits
+ * block_qubits[qubits_begin[b] .. qubits_begin[b+1]) (ascending; empty for a
+ * MeasureOp barrier).  Handing it to the reference's block sweep
+ * (engines::dense::apply_blocks) reproduces this engine's complex128 state
+ * bit for bit.  Capacities in, sizes out: *num_blocks (blocks), *num_order
+ * (entries of order, = num_ops), *num_block_qubits.  Host only. */
+int mb2_fusion_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t* order,
+                    uint32_t* block_begin, uint32_t* block_qubits, uint32_t* qubits_begin, uint64_t* num_blocks,
+                    uint64_t* num_block_qubits);
 
 /* What a sweep of these ops on a num_qubits state costs the device, without
  * running it: the planner's DeviceCost (include/menos/plan.h:117-122) and the

@@ -21,7 +21,7 @@ C128, C64 = 0, 1
 
 class SweepOptions(C.Structure):
     _fields_ = [("fuse_gates", C.c_int32), ("low_qubits", C.c_int32), ("tile_qubits", C.c_int32),
-                ("per_gate", C.c_int32), ("c64_kernel", C.c_int32)]
+                ("per_gate", C.c_int32), ("c64_kernel", C.c_int32), ("fusion_width", C.c_int32)]
 
 
 class SweepEstimate(C.Structure):
@@ -122,6 +122,8 @@ SIGNATURES = {
     "mb2_sample": (C.c_int, [_VP, C.c_uint64, C.c_uint64, _VP, C.c_uint32, _VP, _VP, C.POINTER(C.c_uint64)]),
     "mb2_sample_basis": (C.c_int, [_VP, _VP, C.c_uint64, _VP]),
     "mb2_debug_tc_probe": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "mb2_fusion_plan": (C.c_int, [C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions), _VP, _VP, _VP, _VP,
+                                  C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "mb2_debug_run_plan": (C.c_int, [C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions), C.c_uint32, C.c_int32,
                                      _VP, _VP]),
     "mb2_copy_out": (C.c_int, [_VP, _VP, C.c_uint64]),

@@ -399,7 +399,7 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     }
     std::vector<mb2::Block> blocks;
     try {
-        blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+        blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0, static_cast<uint32_t>(o.fusion_width));
     } catch (const std::exception& e) {
         return fail(s->ctx, MB2_ERR_INVALID, e.what());
     }
@@ -507,6 +507,33 @@ int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const m
     return mb2_apply_program_monitored(s, ops, num_ops, opts, nullptr, nullptr);
 }
 
+int mb2_fusion_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t* order,
+                    uint32_t* block_begin, uint32_t* block_qubits, uint32_t* qubits_begin, uint64_t* num_blocks,
+                    uint64_t* num_block_qubits) {
+    if ((ops == nullptr && num_ops != 0) || num_blocks == nullptr || num_block_qubits == nullptr)
+        return MB2_ERR_INVALID;
+    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
+    if (opts != nullptr) o = *opts;
+    mb2::FusionPlanArrays plan;
+    try {
+        mb2::build_blocks(ops, num_ops, true, static_cast<uint32_t>(o.fusion_width), &plan);
+    } catch (const std::exception&) {
+        return MB2_ERR_INVALID;
+    }
+    const uint64_t blocks = plan.block_begin.size() - 1;
+    const uint64_t cap_b = *num_blocks, cap_q = *num_block_qubits;
+    *num_blocks = blocks;
+    *num_block_qubits = plan.block_qubits.size();
+    if (order == nullptr || block_begin == nullptr || qubits_begin == nullptr ||
+        (block_qubits == nullptr && !plan.block_qubits.empty()) || cap_b < blocks || cap_q < plan.block_qubits.size())
+        return MB2_ERR_INVALID;
+    std::copy(plan.order.begin(), plan.order.end(), order);
+    std::copy(plan.block_begin.begin(), plan.block_begin.end(), block_begin);
+    std::copy(plan.block_qubits.begin(), plan.block_qubits.end(), block_qubits);
+    std::copy(plan.qubits_begin.begin(), plan.qubits_begin.end(), qubits_begin);
+    return MB2_OK;
+}
+
 int mb2_estimate_sweep(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
                        mb2_sweep_estimate* out) {
     if (out == nullptr || (ops == nullptr && num_ops != 0) || num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
@@ -514,7 +541,7 @@ int mb2_estimate_sweep(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
     if (opts != nullptr) o = *opts;
     *out = mb2_sweep_estimate{};
     try {
-        const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+        const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0, static_cast<uint32_t>(o.fusion_width));
         out->blocks = blocks.size();
         out->work_units = uint64_t{1} << num_qubits;
         for (const mb2::Block& b : blocks) out->work_units += uint64_t{1} << (num_qubits + b.k);
@@ -773,7 +800,7 @@ int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
     mb2_sweep_options o{1, 0, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     try {
-        const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+        const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0, static_cast<uint32_t>(o.fusion_width));
         if (blocks.empty()) return MB2_OK;
         const bool c64 = precision == MB2_C64;
         uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, num_qubits, blocks);
@@ -859,7 +886,7 @@ int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
     std::vector<mb2::Block> blocks;
     std::vector<uint32_t> order, order_pass;
     try {
-        blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+        blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0, static_cast<uint32_t>(o.fusion_width));
         uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : 0, num_qubits, blocks);
         if (c64) {
             m = o.tile_qubits > 0 ? std::min<uint32_t>(static_cast<uint32_t>(o.tile_qubits), mb2::kMaxTileQubitsC64)
@@ -1074,7 +1101,7 @@ int mb2_estimate_sweep_time(mb2_context* ctx, const mb2_op* ops, uint32_t num_op
     }
     const bool c64 = precision == MB2_C64;
     try {
-        const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0);
+        const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0, static_cast<uint32_t>(o.fusion_width));
         double total = 0.0;
         if (o.per_gate != 0 || num_qubits < mb2::kMinTileQubits || blocks.empty()) {
             for (size_t i = 0; i < blocks.size(); ++i) total += pass_seconds(t, c64, blocks, i, i + 1, num_qubits);

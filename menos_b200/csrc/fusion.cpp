@@ -4,6 +4,16 @@
 // blocks this engine applies are the same matrices on the same operands as
 // the reference CPU and CUDA engines apply: results stay bitwise identical
 // with fusion on.
+//
+// Wider fusion (width k >= 2) keeps the plan's structure -- a gate joins the
+// newest open block that shares a qubit with it, blocks run in the order they
+// opened, a MeasureOp closes every block -- and only changes the join rule:
+// the gate joins when the block and the gate together span at most k qubits.
+// The structure is what makes any join rule sound: every block opened after
+// the one the gate joins is on qubits disjoint from the gate's, so it
+// commutes with it.  The plan (FusionPlan's arrays) can be handed to the
+// reference's own block sweep (engines::dense::apply_blocks), which then
+// computes the same bits.
 #include <algorithm>
 #include <array>
 #include <stdexcept>
@@ -119,7 +129,9 @@ bool may_join(uint64_t block, bool block_diagonal, uint64_t gate, bool gate_diag
 
 }  // namespace
 
-std::vector<Block> build_blocks(const mb2_op* ops, uint32_t n_ops, bool fuse_gates) {
+std::vector<Block> build_blocks(const mb2_op* ops, uint32_t n_ops, bool fuse_gates, uint32_t width,
+                                FusionPlanArrays* plan_out) {
+    if (width == 1 || width > MB2_MAX_OP_QUBITS) throw std::invalid_argument("fusion width must be 0 or 2..6");
     std::vector<OpView> views;
     views.reserve(n_ops);
     for (uint32_t i = 0; i < n_ops; ++i) views.push_back(view_of(ops[i], i));
@@ -163,7 +175,11 @@ std::vector<Block> build_blocks(const mb2_op* ops, uint32_t n_ops, bool fuse_gat
             if (b != kNone && (dep == kNone || b > dep)) dep = b;
         }
         uint32_t b;
-        if (dep != kNone && may_join(block_mask[dep], block_diag[dep] != 0, v.mask, v.fusion_diagonal)) {
+        const bool join = dep != kNone && (width == 0 ? may_join(block_mask[dep], block_diag[dep] != 0, v.mask,
+                                                                  v.fusion_diagonal)
+                                                       : __builtin_popcountll(block_mask[dep] | v.mask) <=
+                                                             static_cast<int>(width));
+        if (join) {
             b = dep;
             block_mask[b] |= v.mask;
             block_diag[b] = static_cast<unsigned char>(block_diag[b] != 0 && v.fusion_diagonal);
@@ -180,6 +196,18 @@ std::vector<Block> build_blocks(const mb2_op* ops, uint32_t n_ops, bool fuse_gat
     const uint32_t blocks = static_cast<uint32_t>(block_mask.size());
     std::vector<std::vector<uint32_t>> members(blocks);
     for (uint32_t i = 0; i < n_ops; ++i) members[block_of[i]].push_back(i);
+    if (plan_out != nullptr) {
+        *plan_out = FusionPlanArrays{};
+        plan_out->block_begin.push_back(0);
+        plan_out->qubits_begin.push_back(0);
+        for (uint32_t b = 0; b < blocks; ++b) {
+            plan_out->order.insert(plan_out->order.end(), members[b].begin(), members[b].end());
+            plan_out->block_begin.push_back(static_cast<uint32_t>(plan_out->order.size()));
+            for (uint64_t rest = block_mask[b]; rest != 0; rest &= rest - 1)
+                plan_out->block_qubits.push_back(static_cast<uint32_t>(__builtin_ctzll(rest)));
+            plan_out->qubits_begin.push_back(static_cast<uint32_t>(plan_out->block_qubits.size()));
+        }
+    }
 
     for (uint32_t b = 0; b < blocks; ++b) {
         if (block_mask[b] == 0) continue;  // barrier

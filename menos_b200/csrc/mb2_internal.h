@@ -59,11 +59,17 @@ bool is_diagonal(const std::vector<Cd>& m, uint32_t dim);
 
 // ---- fusion (fusion.cpp) ----------------------------------------------------
 // The operations as blocks: with fuse_gates, the reference's containment plan
-// (src/ir/fuse_gates.cpp:190-283) and its block matrices
-// (src/engines/dense/fused_block.cpp:61-99); without, one block per gate.
-// MeasureOps are dropped (they apply nothing).  Throws std::invalid_argument
-// on a malformed op.
-std::vector<Block> build_blocks(const mb2_op* ops, uint32_t n_ops, bool fuse_gates);
+// (src/ir/fuse_gates.cpp:190-283), or with width >= 2 the same plan structure
+// joining while the block spans at most `width` qubits (fusion.cpp), and the
+// reference's block matrices (src/engines/dense/fused_block.cpp:61-99);
+// without, one block per gate.  MeasureOps are dropped (they apply nothing).
+// plan_out (optional): the plan as ir::FusionPlan's arrays.  Throws
+// std::invalid_argument on a malformed op.
+struct FusionPlanArrays {
+    std::vector<uint32_t> order, block_begin, block_qubits, qubits_begin;
+};
+std::vector<Block> build_blocks(const mb2_op* ops, uint32_t n_ops, bool fuse_gates, uint32_t width = 0,
+                                FusionPlanArrays* plan_out = nullptr);
 
 // The generic kernel on a host vector (the fused-matrix builder's tool):
 // bitwise kernels::cpu::apply_matrix_generic.

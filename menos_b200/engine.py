@@ -169,17 +169,20 @@ class DeviceState:
         self._chk(f(self.h, m.ctypes.data, q.ctypes.data, len(q)), "mb2_apply_matrix")
 
     def apply_program(self, circ: Circuit, fuse_gates: bool = True, tile_qubits: int = 0,
-                      per_gate: bool = False, low_qubits: int = 0, c64_kernel: str = "auto") -> SweepStats:
+                      per_gate: bool = False, low_qubits: int = 0, c64_kernel: str = "auto",
+                      fusion_width: int = 0) -> SweepStats:
         """c64_kernel (complex64 states): "tensor" -- each phase's gates as one
         split-FP16 tensor-core GEMM wherever a pass allows; "simt" -- FP32
         gates one by one; "auto" -- tensor cores for states of more than 2^24
-        amplitudes, SIMT below."""
+        amplitudes, SIMT below.  fusion_width (with fuse_gates): 0 -- the
+        reference's containment rule; 2..6 -- blocks of up to that many qubits
+        (fusion_plan gives the plan)."""
         arr, keep = to_mb2_ops(circ)
         kernels = {"auto": 0, "simt": 1, "tensor": 2}
         if c64_kernel not in kernels:
             raise ValueError("c64_kernel is 'auto', 'tensor' or 'simt'")
         opts = SweepOptions(1 if fuse_gates else 0, low_qubits, tile_qubits, 1 if per_gate else 0,
-                            kernels[c64_kernel])
+                            kernels[c64_kernel], fusion_width)
         self._chk(lib().mb2_apply_program(self.h, arr, len(circ.ops), C.byref(opts)), "mb2_apply_program")
         del keep
         return self.stats()
@@ -307,9 +310,10 @@ class B200DenseEngine:
     """The dense statevector engine on one B200: {Dense, Cuda, InMemory}
     (the triple src/plan/execution_engines.cpp:37-45 resolves)."""
 
-    def __init__(self, device: int = 0, tile_qubits: int = 0):
+    def __init__(self, device: int = 0, tile_qubits: int = 0, fusion_width: int = 0):
         self.ctx = Context(device)
         self.tile_qubits = tile_qubits
+        self.fusion_width = fusion_width
 
     def name(self) -> str:
         return "dense_b200"
@@ -335,7 +339,8 @@ class B200DenseEngine:
         st = DeviceState(self.ctx, req.num_qubits, C128, req.budget_bytes)
         try:
             st.init(req.global_phase)
-            stats = st.apply_program(req.operations, fuse_gates=req.fuse_gates, tile_qubits=self.tile_qubits)
+            stats = st.apply_program(req.operations, fuse_gates=req.fuse_gates, tile_qubits=self.tile_qubits,
+                                     fusion_width=self.fusion_width)
             res = EngineExecutionResult(actual_bytes=16 << req.num_qubits,
                                         sweep={"blocks": stats.blocks, "passes": stats.passes,
                                                "launches": stats.launches})
@@ -349,3 +354,23 @@ class B200DenseEngine:
             return res
         finally:
             st.free()
+
+
+def fusion_plan(circ: Circuit, fusion_width: int = 0):
+    """The fusion plan a sweep applies (mb2_fusion_plan), as the reference's
+    ir::FusionPlan arrays: (order, block_begin, block_qubits, qubits_begin)."""
+    arr, keep = to_mb2_ops(circ)
+    n = len(circ.ops)
+    order = np.zeros(max(n, 1), np.uint32)
+    bb = np.zeros(n + 2, np.uint32)
+    qb = np.zeros(n + 2, np.uint32)
+    bq = np.zeros(max(6 * n, 1), np.uint32)
+    nb = C.c_uint64(n + 1)
+    nq = C.c_uint64(bq.size)
+    opts = SweepOptions(1, 0, 0, 0, 0, fusion_width)
+    rc = lib().mb2_fusion_plan(arr, n, C.byref(opts), order.ctypes.data, bb.ctypes.data, bq.ctypes.data,
+                               qb.ctypes.data, C.byref(nb), C.byref(nq))
+    check(rc, None, "mb2_fusion_plan")
+    del keep
+    b = nb.value
+    return order[:n].copy(), bb[:b + 1].copy(), bq[:nq.value].copy(), qb[:b + 1].copy()

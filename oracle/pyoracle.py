@@ -234,6 +234,9 @@ class RefLib:
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                     C.c_void_p, C.c_void_p]
         L.ref_run_dense.restype = C.c_int
+        L.ref_run_plan.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+        L.ref_run_plan.restype = C.c_int
         L.ref_last_error.restype = C.c_char_p
         L.ref_default_threads.restype = C.c_uint32
         L.ref_kernel_isa.restype = C.c_int
@@ -327,6 +330,20 @@ class RefLib:
             "terms": terms[:2 * len(paulis)].view(np.complex128).copy() if paulis else None,
             "seconds": float(secs[0]),
         }
+
+    def run_plan(self, circ, plan, threads=0) -> np.ndarray:
+        """The dense engine's fused sweep over an explicit plan (order,
+        block_begin, block_qubits, qubits_begin): the statevector."""
+        arr, keep = ops_struct_array(circ)
+        order, bb, bq, qb = (np.ascontiguousarray(a, np.uint32) for a in plan)
+        n = circ.num_qubits
+        sv = np.zeros(1 << n, np.complex128)
+        rc = self.L.ref_run_plan(n, C.addressof(arr), len(circ.ops), circ.global_phase, order.ctypes.data,
+                                 bb.ctypes.data, bq.ctypes.data if bq.size else None, qb.ctypes.data, len(bb) - 1,
+                                 threads, sv.ctypes.data)
+        assert rc == 0, self.L.ref_last_error()
+        del keep
+        return sv
 
     def default_threads(self) -> int:
         return int(self.L.ref_default_threads())

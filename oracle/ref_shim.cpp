@@ -15,6 +15,9 @@
 //   ref_plan_fusion          -> ir::plan_fusion            (src/ir/fuse_gates.cpp:190)
 //   ref_fused_block_matrix   -> engines::dense::fused_block_matrix (src/engines/dense/fused_block.cpp:61)
 //   ref_run_dense            -> engines::dense::DenseEngine::execute (src/engines/dense/dense_engine.cpp:333)
+//   ref_run_plan             -> initialize + engines::dense::apply_blocks with the dense
+//                               engine's apply_matrix, for a plan given as ir::FusionPlan's
+//                               arrays (src/engines/dense/dense_engine.cpp:100-112)
 #include <algorithm>
 #include <chrono>
 #include <complex>
@@ -26,6 +29,7 @@
 #include <vector>
 
 #include "common/rng.h"
+#include "engines/dense/apply_matrix.h"
 #include "engines/dense/dense_engine.h"
 #include "engines/dense/fused_block.h"
 #include "engines/dense/sample.h"
@@ -283,6 +287,35 @@ int ref_run_dense(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_o
                 terms_out[2 * i + 1] = (*res.expectation_terms)[i].imag();
             }
         }
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// The dense engine's fused sweep (apply_fused, src/engines/dense/dense_engine.cpp:
+// 100-112) over the plan given as ir::FusionPlan's arrays, from
+// initialize(global_phase); the state (2 * 2^n doubles) out.
+int ref_run_plan(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_ops, double global_phase,
+                 const std::uint32_t* order, const std::uint32_t* block_begin, const std::uint32_t* block_qubits,
+                 const std::uint32_t* qubits_begin, std::uint32_t n_blocks, std::uint32_t threads,
+                 double* statevector) {
+    try {
+        std::vector<menos::Operation> v;
+        for (std::uint32_t i = 0; i < n_ops; ++i) v.push_back(to_operation(ops[i]));
+        menos::ir::FusionPlan plan;
+        plan.order.assign(order, order + block_begin[n_blocks]);
+        plan.block_begin.assign(block_begin, block_begin + n_blocks + 1);
+        plan.qubits_begin.assign(qubits_begin, qubits_begin + n_blocks + 1);
+        plan.block_qubits.assign(block_qubits, block_qubits + qubits_begin[n_blocks]);
+        auto state = as_span(statevector, std::uint64_t{1} << num_qubits);
+        menos::kernels::cpu::initialize(state, global_phase);
+        const std::uint32_t t = threads == 0 ? menos::common::default_thread_count() : threads;
+        menos::engines::dense::apply_blocks(
+            plan, v, nullptr, [&](std::span<const C> matrix, std::span<const menos::QubitId> operands) {
+                menos::engines::dense::apply_matrix(state, matrix, operands, t);
+            });
         return 0;
     } catch (const std::exception& e) {
         g_error = e.what();
