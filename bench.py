@@ -319,8 +319,8 @@ def main():
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(job_ms / args.steps, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded circuit)",
-        "config": {"workload": f"{n}q complex128: brick depth {args.depth} + QFT ({len(circ.ops)} gates), "
-                               (f"fusion=containment" if args.fusion == 0 else f"fusion<={args.fusion} qubits") +
+        "config": {"workload": f"{n}q complex128: brick depth {args.depth} + QFT ({len(circ.ops)} gates), " +
+                               ("fusion=containment" if args.fusion == 0 else f"fusion<={args.fusion} qubits") +
                                f", norm + {args.terms} Paulis + {args.shots} shots",
                    "qubits": n, "parallelism": f"replicas x{world}", "l2": "state 16 GiB >> L2 (no flush)",
                    "passes": passes, "blocks": int(stats.blocks), "sweep_ms": round(sweep_avg, 2),
