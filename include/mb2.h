@@ -57,7 +57,10 @@ enum { MB2_C128 = 0, MB2_C64 = 1 };
 enum {
     MB2_X = 0, MB2_Y, MB2_Z, MB2_H, MB2_S, MB2_SDG, MB2_T, MB2_TDG, MB2_SX, MB2_SXDG,
     MB2_RX, MB2_RY, MB2_RZ, MB2_P, MB2_U, MB2_CX, MB2_CZ, MB2_SWAP, MB2_CP, MB2_RZZ,
-    MB2_CCX, MB2_UNITARY, MB2_MEASURE
+    MB2_CCX, MB2_UNITARY, MB2_MEASURE,
+    MB2_CHANNEL  /* a noise channel (the reference's ChannelOp, include/menos/circuit.h:85-88):
+                    `reserved` Kraus operators of 4^k entries each, consecutive at `matrix`;
+                    applied by the density-matrix path only */
 };
 
 /* The widest operation carried: the reference caps UnitaryOp at 5 qubits
@@ -242,6 +245,25 @@ int mb2_copy_out(mb2_state* state, void* host, uint64_t num_amplitudes);
 int mb2_copy_in(mb2_state* state, const void* host, uint64_t num_amplitudes);
 /* Waits for all work queued on the state's stream. */
 int mb2_synchronize(mb2_state* state);
+
+/* ---- density matrices (noisy circuits) ---------------------------------- */
+/* The reference's density-matrix engine (src/engines/density_matrix/
+ * density_matrix_engine.cpp) on the device.  rho for n qubits is a
+ * complex128 state of 2n qubits (mb2_state_alloc(ctx, 2n, MB2_C128, ...)),
+ * entry (r, c) at index r | c << n; mb2_init(rho, 0.0) sets |0..0><0..0|.
+ * mb2_dm_apply_program applies each gate as U on qubits q and conj(U) on
+ * q + n, each MB2_CHANNEL as its superoperator (sum over Kraus K of
+ * K (x) conj(K), rows r | c << k) on q and q + n, operation by operation:
+ * bitwise the reference engine's rho.  mb2_dm_expectation: Tr(P_t rho) per
+ * term (within 1e-12 of the reference's sequential sum).  mb2_dm_sample:
+ * counts by the reference's sort-then-walk over rho's diagonal (identical
+ * counts); outcomes as mb2_sample's.  n <= 15.  MeasureOps carry no readout
+ * error across this ABI. */
+int mb2_dm_apply_program(mb2_state* rho, uint32_t num_qubits, const mb2_op* ops, uint32_t num_ops);
+int mb2_dm_expectation(mb2_state* rho, uint32_t num_qubits, const uint64_t* x_masks, const uint64_t* z_masks,
+                       uint32_t num_terms, double* out);
+int mb2_dm_sample(mb2_state* rho, uint32_t num_qubits, uint64_t shots, uint64_t seed, const uint32_t* targets,
+                  uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes);
 
 /* ---- batched parameter sweep ------------------------------------------- */
 /* One circuit structure under many parameter bindings, in one device job:

@@ -6,8 +6,8 @@ CUDA for sm_100a with a C++ host layer.  This package is its Python face:
 ``circuit`` (KIR operations) and ``workloads`` (seeded benchmark circuits).
 """
 from .circuit import OP, Circuit
-from .engine import (B200DenseEngine, Context, DeviceState, EngineExecutionRequest, EngineExecutionResult,
-                     PauliTerm)
+from .engine import (B200DenseEngine, Context, DensityMatrix, DeviceState, EngineExecutionRequest,
+                     EngineExecutionResult, PauliTerm)
 
-__all__ = ["OP", "Circuit", "B200DenseEngine", "Context", "DeviceState", "EngineExecutionRequest",
+__all__ = ["OP", "Circuit", "B200DenseEngine", "Context", "DensityMatrix", "DeviceState", "EngineExecutionRequest",
            "EngineExecutionResult", "PauliTerm"]

@@ -2,7 +2,8 @@
 
 ``Circuit`` mirrors the reference's ``menos::Circuit`` operation list
 (include/menos/circuit.h:50-150): named gates by opcode (the reference's
-``menos::Opcode`` order), explicit unitaries, and measurements.  ``ops`` is a
+``menos::Opcode`` order), explicit unitaries, measurements and noise
+channels.  ``ops`` is a
 list of ``(opcode, qubits, params, matrix, clbit)`` tuples; ``to_mb2_ops``
 packs it into the C ABI's ``mb2_op`` array.
 """
@@ -13,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 OPCODES = ["x", "y", "z", "h", "s", "sdg", "t", "tdg", "sx", "sxdg", "rx", "ry", "rz", "p",
-           "u", "cx", "cz", "swap", "cp", "rzz", "ccx", "unitary", "measure"]
+           "u", "cx", "cz", "swap", "cp", "rzz", "ccx", "unitary", "measure", "channel"]
 OP = {name: i for i, name in enumerate(OPCODES)}
 NUM_QUBITS = {**{i: 1 for i in range(15)}, 15: 2, 16: 2, 17: 2, 18: 2, 19: 2, 20: 3}
 NUM_PARAMS = {10: 1, 11: 1, 12: 1, 13: 1, 14: 3, 18: 1, 19: 1}
@@ -53,6 +54,18 @@ class Circuit:
         self.ops.append((OP["unitary"], qs, (), m, 0))
         return self
 
+    def channel(self, qubits, kraus) -> "Circuit":
+        """A noise channel (the reference's ChannelOp, include/menos/circuit.h:
+        85-88): Kraus operators as a (count, 2^k, 2^k) array, k <= 5 (the
+        reference's kMaxUnitaryQubits).  Only the density-matrix path
+        (DensityMatrix.apply) takes it."""
+        qs = tuple(int(q) for q in qubits)
+        m = np.ascontiguousarray(np.asarray(kraus, dtype=np.complex128))
+        if m.ndim != 3 or m.shape[0] < 1 or m.shape[1:] != (1 << len(qs), 1 << len(qs)) or not 1 <= len(qs) <= 5:
+            raise ValueError("a channel takes 1..5 qubits and Kraus operators of shape (count, 2^k, 2^k)")
+        self.ops.append((OP["channel"], qs, (), m, 0))
+        return self
+
     def measure(self, qubit: int, clbit: int) -> "Circuit":
         self.ops.append((OP["measure"], (int(qubit),), (), None, int(clbit)))
         self.num_clbits = max(self.num_clbits, int(clbit) + 1)
@@ -88,5 +101,7 @@ def to_mb2_ops(circ: Circuit):
             buf = np.ascontiguousarray(m.view(np.float64).ravel())
             keep.append(buf)
             o.matrix = buf.ctypes.data_as(C.POINTER(C.c_double))
+            if oc == OP["channel"]:
+                o.reserved = m.shape[0]
         o.clbit = cl
     return arr, keep

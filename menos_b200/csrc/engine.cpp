@@ -654,21 +654,16 @@ int mb2_norm(mb2_state* s, double* out) {
     return MB2_OK;
 }
 
-int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targets, uint32_t num_targets,
-               uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes) {
-    if (s == nullptr || num_outcomes == nullptr) return MB2_ERR_INVALID;
-    for (uint32_t t = 0; t < num_targets; ++t)
-        if (targets[2 * t] >= s->n || targets[2 * t + 1] >= 64)
-            return fail(s->ctx, MB2_ERR_INVALID, "measure target out of range");
-    if (shots == 0) {
-        *num_outcomes = 0;
-        return MB2_OK;
-    }
-    // Uniforms exactly as common::Rng (src/common/rng.cpp:176-186), sorted
-    // (src/engines/dense/sample.cpp:37-42).  u = k * 2^-53 with k the top 53
-    // bits of a word, so sorting the integers k sorts the uniforms: one
-    // counting pass on the top 12 bits, then the buckets (about shots / 4096
-    // keys each, uniform) sorted independently on a few host threads.
+}  // extern "C"
+
+namespace {
+
+// Uniforms exactly as common::Rng (src/common/rng.cpp:176-186), sorted
+// (src/engines/dense/sample.cpp:37-42).  u = k * 2^-53 with k the top 53
+// bits of a word, so sorting the integers k sorts the uniforms: one
+// counting pass on the top 12 bits, then the buckets (about shots / 4096
+// keys each, uniform) sorted independently on a few host threads.
+std::vector<double> sorted_uniforms(uint64_t shots, uint64_t seed) {
     std::vector<double> u(shots);
     {
         std::vector<uint64_t> key(shots), sorted(shots);
@@ -695,8 +690,14 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
         sort_range(0);
         for (auto& th : pool) th.join();
     }
-    std::vector<uint64_t> basis(shots);
-    if (int e = walk_sorted(s, u, basis.data()); e != MB2_OK) return e;
+    return u;
+}
+
+// The walk's basis states (non-decreasing) as counts of the measured
+// outcomes, ascending: mb2_sample's output.
+int histogram(mb2_state* s, uint32_t n, const std::vector<uint64_t>& basis, const uint32_t* targets,
+              uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes) {
+    const uint64_t shots = basis.size();
     // Outcomes through the measure targets, ascending, with counts.  The walk
     // gives non-decreasing basis indices (sorted uniforms against the
     // cumulative sum), so runs are counted first; the distinct outcomes are
@@ -704,7 +705,7 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
     // Outcome of a basis index: one table per byte of the index (the OR of
     // the target bits that byte carries), or the index itself when every
     // qubit is read into the clbit of its own number.
-    bool identity = num_targets == s->n;
+    bool identity = num_targets == n;
     std::vector<uint64_t> table(8 * 256, 0);
     for (uint32_t t = 0; t < num_targets; ++t) {
         const uint32_t q = targets[2 * t], c = targets[2 * t + 1];
@@ -715,9 +716,9 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
     if (identity) {
         uint64_t seen = 0;
         for (uint32_t t = 0; t < num_targets; ++t) seen |= uint64_t{1} << targets[2 * t];
-        identity = seen == ((s->n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << s->n) - 1));
+        identity = seen == ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1));
     }
-    const uint32_t nbytes = (s->n + 7) / 8;
+    const uint32_t nbytes = (n + 7) / 8;
     auto outcome_of = [&](uint64_t b) {
         if (identity) return b;
         uint64_t o = 0;
@@ -725,7 +726,7 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
         return o;
     };
     std::vector<std::pair<uint64_t, uint64_t>> oc;
-    oc.reserve(std::min<uint64_t>(shots, uint64_t{1} << std::min<uint32_t>(s->n, 30)));
+    oc.reserve(std::min<uint64_t>(shots, uint64_t{1} << std::min<uint32_t>(n, 30)));
     for (uint64_t i = 0; i < shots;) {
         uint64_t j = i + 1;
         while (j < shots && basis[j] == basis[i]) ++j;
@@ -750,6 +751,26 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
     return MB2_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targets, uint32_t num_targets,
+               uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes) {
+    if (s == nullptr || num_outcomes == nullptr) return MB2_ERR_INVALID;
+    for (uint32_t t = 0; t < num_targets; ++t)
+        if (targets[2 * t] >= s->n || targets[2 * t + 1] >= 64)
+            return fail(s->ctx, MB2_ERR_INVALID, "measure target out of range");
+    if (shots == 0) {
+        *num_outcomes = 0;
+        return MB2_OK;
+    }
+    const std::vector<double> u = sorted_uniforms(shots, seed);
+    std::vector<uint64_t> basis(shots);
+    if (int e = walk_sorted(s, u, basis.data()); e != MB2_OK) return e;
+    return histogram(s, s->n, basis, targets, num_targets, outcomes, counts, num_outcomes);
+}
+
 int mb2_sample_basis(mb2_state* s, const double* uniforms, uint64_t n, uint64_t* basis_out) {
     if (s == nullptr || (n != 0 && (uniforms == nullptr || basis_out == nullptr))) return MB2_ERR_INVALID;
     if (n == 0) return MB2_OK;
@@ -766,6 +787,188 @@ int mb2_sample_basis(mb2_state* s, const double* uniforms, uint64_t n, uint64_t*
     if (int e = walk_sorted(s, u, basis.data()); e != MB2_OK) return e;
     for (uint64_t i = 0; i < n; ++i) basis_out[order[i]] = basis[i];
     return MB2_OK;
+}
+
+// ---- density matrices ------------------------------------------------------
+// The reference's density-matrix engine (src/engines/density_matrix/
+// density_matrix_engine.cpp): rho as a 2n-qubit vector, entry (r, c) at
+// r | c << n.
+
+}  // extern "C"
+
+namespace {
+
+// A channel's superoperator on (q, q + n): S[(r | c << k), (r2 | c2 << k)] =
+// sum over the Kraus operators K, in order, of K[r][r2] conj(K[c][c2]) --
+// the reference's construction and summation order (superoperator(),
+// density_matrix_engine.cpp), so its bits are the reference's.
+std::vector<mb2::Cd> superoperator(const std::vector<std::vector<mb2::Cd>>& kraus, uint32_t k) {
+    const size_t dim = size_t{1} << k, sdim = dim * dim;
+    std::vector<mb2::Cd> sop(sdim * sdim, mb2::Cd{0.0, 0.0});
+    for (const std::vector<mb2::Cd>& op : kraus)
+        for (size_t r = 0; r < dim; ++r)
+            for (size_t c = 0; c < dim; ++c) {
+                const size_t row = r | (c << k);
+                for (size_t r2 = 0; r2 < dim; ++r2)
+                    for (size_t c2 = 0; c2 < dim; ++c2)
+                        sop[row * sdim + (r2 | (c2 << k))] += op[r * dim + r2] * std::conj(op[c * dim + c2]);
+            }
+    return sop;
+}
+
+int check_rho(mb2_state* rho, uint32_t n) {
+    if (rho == nullptr) return MB2_ERR_INVALID;
+    if (n < 1 || n > 15 || rho->n != 2 * n || rho->precision != MB2_C128)
+        return fail(rho->ctx, MB2_ERR_INVALID, "a density matrix of n qubits is a complex128 state of 2n qubits, n <= 15");
+    return MB2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mb2_dm_apply_program(mb2_state* rho, uint32_t n, const mb2_op* ops, uint32_t num_ops) {
+    if (int e = check_rho(rho, n); e != MB2_OK) return e;
+    if (ops == nullptr && num_ops != 0) return MB2_ERR_INVALID;
+    // Each operation as 2n-qubit blocks, applied one by one in order (the
+    // reference fuses nothing here): a gate U on q and conj(U) on q + n; a
+    // channel's superoperator on q and q + n.  Runs of blocks of up to six
+    // operands go through the sweep; a 4- or 5-qubit channel's 8- or
+    // 10-operand superoperator through the wide generic kernel.
+    std::vector<mb2_op> out;
+    std::vector<std::vector<double>> keep;
+    auto block = [&](const std::vector<mb2::Cd>& m, const uint32_t* q, uint32_t k) {
+        mb2_op o{};
+        o.opcode = MB2_UNITARY;
+        o.num_qubits = k;
+        std::copy(q, q + k, o.qubits);
+        keep.emplace_back(2 * m.size());
+        std::memcpy(keep.back().data(), m.data(), m.size() * sizeof(mb2::Cd));
+        out.push_back(o);
+    };
+    auto flush = [&]() -> int {
+        if (out.empty()) return MB2_OK;
+        for (size_t i = 0; i < out.size(); ++i) out[i].matrix = keep[i].data();
+        mb2_sweep_options o{0, 0, 0, 0, 0, 0};
+        const int rc = mb2_apply_program(rho, out.data(), static_cast<uint32_t>(out.size()), &o);
+        out.clear();
+        keep.clear();
+        return rc;
+    };
+    try {
+        for (uint32_t i = 0; i < num_ops; ++i) {
+            const mb2_op& op = ops[i];
+            if (op.opcode == MB2_MEASURE) continue;
+            const uint32_t k = op.num_qubits;
+            const bool channel = op.opcode == MB2_CHANNEL;
+            if (k == 0 || k > (channel ? 5u : static_cast<uint32_t>(MB2_MAX_OP_QUBITS)))
+                return fail(rho->ctx, MB2_ERR_INVALID, "operation " + std::to_string(i) + ": operand count");
+            uint32_t both[10];
+            uint64_t seen = 0;
+            for (uint32_t j = 0; j < k; ++j) {
+                if (op.qubits[j] >= n) return fail(rho->ctx, MB2_ERR_INVALID, "operand out of range");
+                if (seen >> op.qubits[j] & 1u) return fail(rho->ctx, MB2_ERR_INVALID, "repeated operand");
+                seen |= uint64_t{1} << op.qubits[j];
+                both[j] = op.qubits[j];
+                both[k + j] = op.qubits[j] + n;
+            }
+            const uint32_t dim = 1u << k;
+            if (channel) {
+                if (op.matrix == nullptr || op.reserved == 0)
+                    return fail(rho->ctx, MB2_ERR_INVALID, "operation " + std::to_string(i) + ": channel without Kraus operators");
+                std::vector<std::vector<mb2::Cd>> kraus(op.reserved, std::vector<mb2::Cd>(size_t{dim} * dim));
+                for (uint32_t t = 0; t < op.reserved; ++t)
+                    for (size_t e = 0; e < size_t{dim} * dim; ++e) {
+                        const double* z = op.matrix + 2 * (size_t{t} * dim * dim + e);
+                        kraus[t][e] = mb2::Cd{z[0], z[1]};
+                    }
+                const std::vector<mb2::Cd> sop = superoperator(kraus, k);
+                if (2 * k <= MB2_MAX_OP_QUBITS) {
+                    block(sop, both, 2 * k);
+                    continue;
+                }
+                if (int rc = flush(); rc != MB2_OK) return rc;
+                const size_t sd = size_t{dim} * dim;
+                std::vector<mb2::Cd> mt(sd * sd);
+                for (size_t r = 0; r < sd; ++r)
+                    for (size_t c = 0; c < sd; ++c) mt[c * sd + r] = sop[r * sd + c];
+                if (int e = ensure_scratch(rho, mt.size() * sizeof(mb2::Cd)); e != MB2_OK) return e;
+                MB2_CUDA(rho->ctx, cudaMemcpyAsync(rho->scratch, mt.data(), mt.size() * sizeof(mb2::Cd),
+                                                   cudaMemcpyHostToDevice, rho->stream));
+                const int rc = mb2::launch_apply_wide(rho->amps, 2 * n, both, 2 * k,
+                                                      static_cast<const double*>(rho->scratch), rho->stream);
+                if (rc != MB2_OK) return fail(rho->ctx, rc, std::string("wide apply: ") + mb2::last_cuda_error_string());
+                // The host copy of the matrix must outlive the transfer.
+                MB2_CUDA(rho->ctx, cudaStreamSynchronize(rho->stream));
+                continue;
+            }
+            std::vector<mb2::Cd> m;
+            if (op.opcode == MB2_UNITARY) {
+                if (op.matrix == nullptr) return fail(rho->ctx, MB2_ERR_INVALID, "unitary without a matrix");
+                m.resize(size_t{dim} * dim);
+                for (size_t e = 0; e < m.size(); ++e) m[e] = mb2::Cd{op.matrix[2 * e], op.matrix[2 * e + 1]};
+            } else if (mb2::gate_matrix(op.opcode, op.params, m) != static_cast<int>(dim)) {
+                return fail(rho->ctx, MB2_ERR_INVALID, "operation " + std::to_string(i) + ": unknown gate");
+            }
+            std::vector<mb2::Cd> mc(m.size());
+            for (size_t e = 0; e < m.size(); ++e) mc[e] = std::conj(m[e]);
+            block(m, both, k);
+            block(mc, both + k, k);
+        }
+    } catch (const std::exception& e) {
+        return fail(rho->ctx, MB2_ERR_INVALID, e.what());
+    }
+    return flush();
+}
+
+int mb2_dm_expectation(mb2_state* rho, uint32_t n, const uint64_t* x_masks, const uint64_t* z_masks,
+                       uint32_t num_terms, double* out) {
+    if (int e = check_rho(rho, n); e != MB2_OK) return e;
+    if (num_terms == 0) return MB2_OK;
+    if (x_masks == nullptr || z_masks == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    const uint64_t lim = (uint64_t{1} << n) - 1;
+    for (uint32_t t = 0; t < num_terms; ++t)
+        if ((x_masks[t] | z_masks[t]) & ~lim) return fail(rho->ctx, MB2_ERR_INVALID, "Pauli mask beyond the qubits");
+    auto up = [](size_t v) { return (v + 255) & ~size_t{255}; };
+    const size_t mb = size_t{num_terms} * 8;
+    const size_t off_z = up(mb), off_p = off_z + up(mb), off_o = off_p + size_t{num_terms} * mb2::kExpBlocks * 16;
+    if (int e = ensure_scratch(rho, off_o + size_t{num_terms} * 16); e != MB2_OK) return e;
+    auto* base = static_cast<unsigned char*>(rho->scratch);
+    MB2_CUDA(rho->ctx, cudaMemcpyAsync(base, x_masks, mb, cudaMemcpyHostToDevice, rho->stream));
+    MB2_CUDA(rho->ctx, cudaMemcpyAsync(base + off_z, z_masks, mb, cudaMemcpyHostToDevice, rho->stream));
+    const int rc = mb2::launch_dm_trace(rho->amps, n, reinterpret_cast<const uint64_t*>(base),
+                                        reinterpret_cast<const uint64_t*>(base + off_z), num_terms,
+                                        reinterpret_cast<double*>(base + off_p), reinterpret_cast<double*>(base + off_o),
+                                        rho->stream);
+    if (rc != MB2_OK) return fail(rho->ctx, rc, std::string("trace launch: ") + mb2::last_cuda_error_string());
+    MB2_CUDA(rho->ctx, cudaMemcpyAsync(out, base + off_o, size_t{num_terms} * 16, cudaMemcpyDeviceToHost, rho->stream));
+    MB2_CUDA(rho->ctx, cudaStreamSynchronize(rho->stream));
+    return MB2_OK;
+}
+
+int mb2_dm_sample(mb2_state* rho, uint32_t n, uint64_t shots, uint64_t seed, const uint32_t* targets,
+                  uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes) {
+    if (int e = check_rho(rho, n); e != MB2_OK) return e;
+    if (num_outcomes == nullptr) return MB2_ERR_INVALID;
+    for (uint32_t t = 0; t < num_targets; ++t)
+        if (targets[2 * t] >= n || targets[2 * t + 1] >= 64)
+            return fail(rho->ctx, MB2_ERR_INVALID, "measure target out of range");
+    if (shots == 0) {
+        *num_outcomes = 0;
+        return MB2_OK;
+    }
+    const std::vector<double> u = sorted_uniforms(shots, seed);
+    const size_t al_u = (shots * 8 + 255) & ~size_t{255};
+    if (int e = ensure_scratch(rho, 2 * al_u); e != MB2_OK) return e;
+    auto* base = static_cast<unsigned char*>(rho->scratch);
+    MB2_CUDA(rho->ctx, cudaMemcpyAsync(base, u.data(), shots * 8, cudaMemcpyHostToDevice, rho->stream));
+    const int rc = mb2::launch_dm_walk(rho->amps, n, reinterpret_cast<const double*>(base), shots,
+                                       reinterpret_cast<uint64_t*>(base + al_u), rho->stream);
+    if (rc != MB2_OK) return fail(rho->ctx, rc, std::string("walk launch: ") + mb2::last_cuda_error_string());
+    std::vector<uint64_t> basis(shots);
+    MB2_CUDA(rho->ctx, cudaMemcpyAsync(basis.data(), base + al_u, shots * 8, cudaMemcpyDeviceToHost, rho->stream));
+    MB2_CUDA(rho->ctx, cudaStreamSynchronize(rho->stream));
+    return histogram(rho, n, basis, targets, num_targets, outcomes, counts, num_outcomes);
 }
 
 int mb2_copy_out(mb2_state* s, void* host, uint64_t num_amplitudes) {

@@ -92,6 +92,9 @@ struct OpView {
 OpView view_of(const mb2_op& op, uint32_t index) {
     OpView v;
     if (op.opcode == MB2_MEASURE) return v;
+    if (op.opcode == MB2_CHANNEL)
+        throw std::invalid_argument("operation " + std::to_string(index) +
+                                    ": a noise channel needs the density-matrix path (mb2_dm_apply_program)");
     if (op.opcode < 0 || op.opcode > MB2_UNITARY)
         throw std::invalid_argument("operation " + std::to_string(index) + ": unknown opcode");
     if (op.opcode == MB2_UNITARY) {

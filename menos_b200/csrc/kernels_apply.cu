@@ -150,6 +150,48 @@ __global__ void __launch_bounds__(256) k_apply_generic(double2* __restrict__ st,
     }
 }
 
+// The generic kernel for 7..10 operands (a density matrix's superoperator of
+// a 4- or 5-qubit channel): one CTA per group of 2^k amplitudes, gathered
+// into shared memory; thread `out` forms sum over `in` (increasing) of
+// m[out][in] * a[in] exactly as k_apply_generic, reading the matrix
+// transposed (mt[in * dim + out], so a warp's reads are contiguous) from
+// global memory, where it stays in L2.
+struct Q10 {
+    uint32_t q[10];
+};
+
+__global__ void __launch_bounds__(256) k_apply_wide(double2* __restrict__ st, uint32_t n, uint32_t k, Q10 ops,
+                                                    const double2* __restrict__ mt) {
+    extern __shared__ double2 grp[];
+    const uint32_t dim = 1u << k;
+    uint64_t opmask = 0;
+    for (uint32_t j = 0; j < k; ++j) opmask |= uint64_t{1} << ops.q[j];
+    const uint64_t rest = ((uint64_t{1} << n) - 1) & ~opmask;
+    const uint64_t ngroups = (uint64_t{1} << n) >> k;
+    for (uint64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const uint64_t base = pdep64(g, rest);
+        __syncthreads();
+        for (uint32_t l = threadIdx.x; l < dim; l += blockDim.x) {
+            uint64_t idx = base;
+            for (uint32_t j = 0; j < k; ++j)
+                if ((l >> j) & 1u) idx |= uint64_t{1} << ops.q[j];
+            grp[l] = st[idx];
+        }
+        __syncthreads();
+        for (uint32_t out = threadIdx.x; out < dim; out += blockDim.x) {
+            double2 acc = cmul(mt[out].x, mt[out].y, grp[0]);
+            for (uint32_t in = 1; in < dim; ++in) {
+                const double2 e = mt[static_cast<size_t>(in) * dim + out];
+                acc = cadd(acc, cmul(e.x, e.y, grp[in]));
+            }
+            uint64_t idx = base;
+            for (uint32_t j = 0; j < k; ++j)
+                if ((out >> j) & 1u) idx |= uint64_t{1} << ops.q[j];
+            st[idx] = canon(acc);
+        }
+    }
+}
+
 int grid_for(uint64_t work, int threads) {
     const uint64_t blocks = (work + threads - 1) / threads;
     return static_cast<int>(blocks < 148ull * 16 ? (blocks == 0 ? 1 : blocks) : 148ull * 16);
@@ -219,6 +261,19 @@ int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, 
     k_apply_generic<<<grid, 256, smem, static_cast<cudaStream_t>(stream)>>>(
         static_cast<double2*>(amps), n, k, qq[0], qq[1], qq[2], qq[3], qq[4], qq[5],
         reinterpret_cast<const double2*>(dev_matrix));
+    note_launches(1);
+    return launch_status();
+}
+
+int launch_apply_wide(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* dev_matrix_t,
+                      void* stream) {
+    if (k < 1 || k > 10 || k > n) return MB2_ERR_INVALID;
+    Q10 ops{};
+    for (uint32_t j = 0; j < k; ++j) ops.q[j] = q[j];
+    const uint64_t ngroups = (uint64_t{1} << n) >> k;
+    const int grid = static_cast<int>(ngroups < 148ull * 8 ? ngroups : 148ull * 8);
+    k_apply_wide<<<grid, 256, (size_t{1} << k) * sizeof(double2), static_cast<cudaStream_t>(stream)>>>(
+        static_cast<double2*>(amps), n, k, ops, reinterpret_cast<const double2*>(dev_matrix_t));
     note_launches(1);
     return launch_status();
 }

@@ -503,10 +503,77 @@ int launch_batch_group_finish(const double* dev_partials, uint64_t bindings, uin
     return launch_status();
 }
 
+// ---- density matrices ---------------------------------------------------
+// rho as a 2n-qubit vector, entry (r, c) at r | c << n.  Tr(P rho) partials:
+// the sum over c of (-1)^popcount(c & z) rho[c | (c ^ x) << n] (the
+// reference's trace_with_pauli, src/engines/density_matrix/
+// density_matrix_engine.cpp); k_expectation_finish adds the partials in
+// block order and applies i^popcount(x & z).
+__global__ void __launch_bounds__(kThreads)
+    k_dm_trace(const double2* __restrict__ rho, uint32_t n, const uint64_t* __restrict__ xs,
+               const uint64_t* __restrict__ zs, double* __restrict__ partials) {
+    const uint32_t term = blockIdx.y;
+    const uint64_t x = xs[term], z = zs[term];
+    const uint64_t dim = uint64_t{1} << n;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+    double re = 0.0, im = 0.0;
+    for (uint64_t c = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < dim; c += stride) {
+        const double2 e = rho[c | ((c ^ x) << n)];
+        if (__popcll(c & z) & 1) {
+            re = __dsub_rn(re, e.x);
+            im = __dsub_rn(im, e.y);
+        } else {
+            re = __dadd_rn(re, e.x);
+            im = __dadd_rn(im, e.y);
+        }
+    }
+    block_reduce2(re, im);
+    if (threadIdx.x == 0) {
+        double* p = partials + 2 * (static_cast<uint64_t>(term) * gridDim.x + blockIdx.x);
+        p[0] = re;
+        p[1] = im;
+    }
+}
+
+// The reference's sort-then-walk over rho's diagonal, strictly in order
+// (src/engines/dense/sample.cpp:55-69 over probabilities Re rho[x | x << n]):
+// one thread, for the density matrices this path holds (n <= 15).
+__global__ void k_dm_walk(const double2* __restrict__ rho, uint32_t n, const double* __restrict__ u, uint64_t shots,
+                          uint64_t* __restrict__ basis) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const uint64_t dim = uint64_t{1} << n;
+    double cumulative = 0.0;
+    uint64_t s = 0;
+    for (uint64_t b = 0; b < dim && s < shots; ++b) {
+        cumulative = __dadd_rn(cumulative, rho[b * (dim + 1)].x);
+        while (s < shots && u[s] < cumulative) basis[s++] = b;
+    }
+    for (; s < shots; ++s) basis[s] = dim - 1;
+}
+
 int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const uint64_t* dev_x,
                               const uint64_t* dev_z, uint32_t num_terms, double* dev_out, void* stream) {
     k_expectation_finish<<<(num_terms + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
         dev_partials, blocks, dev_x, dev_z, num_terms, dev_out);
+    note_launches(1);
+    return launch_status();
+}
+
+int launch_dm_trace(const void* rho, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z, uint32_t num_terms,
+                    double* dev_partials, double* dev_out, void* stream) {
+    if (num_terms == 0) return MB2_OK;
+    const auto s = static_cast<cudaStream_t>(stream);
+    k_dm_trace<<<dim3(kExpBlocks, num_terms), kThreads, 0, s>>>(static_cast<const double2*>(rho), n, dev_x, dev_z,
+                                                               dev_partials);
+    note_launches(1);
+    if (int rc = launch_status(); rc != MB2_OK) return rc;
+    return launch_expectation_finish(dev_partials, kExpBlocks, dev_x, dev_z, num_terms, dev_out, stream);
+}
+
+int launch_dm_walk(const void* rho, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots,
+                   uint64_t* dev_basis, void* stream) {
+    k_dm_walk<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const double2*>(rho), n,
+                                                              dev_uniforms_sorted, shots, dev_basis);
     note_launches(1);
     return launch_status();
 }

@@ -263,6 +263,10 @@ int launch_apply_diag(void* amps, uint32_t n, const uint32_t* q, uint32_t k, con
                       void* stream);
 int launch_apply_generic(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* dev_matrix,
                          void* stream);
+// k = 1..10 operands, the matrix transposed (entry (out, in) at in * 2^k +
+// out) in device memory; same sums as launch_apply_generic.
+int launch_apply_wide(void* amps, uint32_t n, const uint32_t* q, uint32_t k, const double* dev_matrix_t,
+                      void* stream);
 // A batched sweep: `bindings` states of 2^n amplitudes back to back; the
 // data of a parametric instruction for binding b is at pdata + b * pstride
 // + instr.data (doubles).
@@ -396,6 +400,14 @@ int launch_expectation_partials(const void* amps, uint32_t n, const uint64_t* de
                                 uint32_t num_terms, double* dev_partials, void* stream, int precision);
 int launch_expectation_finish(const double* dev_partials, uint32_t blocks, const uint64_t* dev_x,
                               const uint64_t* dev_z, uint32_t num_terms, double* dev_out, void* stream);
+// Density matrices (kernels_reduce.cu): rho as a 2n-qubit complex128 vector,
+// entry (r, c) at r | c << n.  Tr(P rho) per term (partials as
+// launch_expectation's, then the finish); the exact walk of the sorted
+// uniforms over rho's diagonal (one thread; n <= 15).
+int launch_dm_trace(const void* rho, uint32_t n, const uint64_t* dev_x, const uint64_t* dev_z, uint32_t num_terms,
+                    double* dev_partials, double* dev_out, void* stream);
+int launch_dm_walk(const void* rho, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots,
+                   uint64_t* dev_basis, void* stream);
 // MB2_OK after a clean launch, else MB2_ERR_CUDA with the error kept for
 // last_cuda_error_string() (which reports and clears it).
 int launch_status();

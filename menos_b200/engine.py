@@ -240,6 +240,65 @@ class DeviceState:
         self._chk(lib().mb2_synchronize(self.h), "mb2_synchronize")
 
 
+class DensityMatrix:
+    """A density matrix of n qubits on the device: the reference's
+    density-matrix engine (src/engines/density_matrix/
+    density_matrix_engine.cpp).  rho is a complex128 state of 2n qubits,
+    entry (r, c) at r | c << n; gates act as U on the row qubits and conj(U)
+    on the column qubits, channels as their superoperators."""
+
+    def __init__(self, ctx: Context, num_qubits: int, budget_bytes: int = 2 ** 64 - 1):
+        if not 1 <= num_qubits <= 15:
+            raise ValueError("a density matrix holds 1..15 qubits")
+        self.n = num_qubits
+        self.state = DeviceState(ctx, 2 * num_qubits, C128, budget_bytes)
+
+    def _chk(self, rc, what):
+        check(rc, self.state.ctx.h, what)
+
+    def init(self) -> None:
+        """|0..0><0..0| (a global phase cancels in rho)."""
+        self.state.init(0.0)
+
+    def apply(self, circ: Circuit) -> None:
+        if circ.num_qubits != self.n:
+            raise ValueError("circuit and density matrix differ in qubit count")
+        arr, keep = to_mb2_ops(circ)
+        self._chk(lib().mb2_dm_apply_program(self.state.h, self.n, arr, len(circ.ops)), "mb2_dm_apply_program")
+        del keep
+
+    def expectation(self, paulis: Sequence[tuple]) -> np.ndarray:
+        """Tr(P rho) per (x_mask, z_mask) pair -> complex128 array."""
+        if len(paulis) == 0:
+            return np.zeros(0, np.complex128)
+        xs = np.ascontiguousarray([int(p[0]) for p in paulis], dtype=np.uint64)
+        zs = np.ascontiguousarray([int(p[1]) for p in paulis], dtype=np.uint64)
+        out = np.zeros(2 * len(paulis), np.float64)
+        self._chk(lib().mb2_dm_expectation(self.state.h, self.n, xs.ctypes.data, zs.ctypes.data, len(paulis),
+                                           out.ctypes.data), "mb2_dm_expectation")
+        return out.view(np.complex128).copy()
+
+    def sample(self, shots: int, seed: int, targets) -> "Counts":
+        t = np.ascontiguousarray(np.asarray(targets, np.uint32).ravel())
+        cap = max(int(shots), 1)
+        outc = np.zeros(cap, np.uint64)
+        cnt = np.zeros(cap, np.uint64)
+        nout = C.c_uint64(cap)
+        self._chk(lib().mb2_dm_sample(self.state.h, self.n, shots, seed, t.ctypes.data if len(t) else None,
+                                      len(t) // 2, outc.ctypes.data, cnt.ctypes.data, C.byref(nout)),
+                  "mb2_dm_sample")
+        d = nout.value
+        return Counts(outc[:d].copy(), cnt[:d].copy())
+
+    def matrix(self) -> np.ndarray:
+        """rho as a (2^n, 2^n) array, rho[r, c]."""
+        dim = 1 << self.n
+        return self.state.copy_out().reshape(dim, dim).T.copy()
+
+    def free(self) -> None:
+        self.state.free()
+
+
 def sweep_batch(ctx: Context, circ: Circuit, params, paulis, coefs, fuse_gates: bool = False, tile_qubits: int = 0,
                 want_states: bool = False, precision: int = C128):
     """mb2_sweep_batch: <H> per binding for params[b] (one row per binding,

@@ -23,7 +23,7 @@ REF_SO = os.path.join(HERE, "_ref", "libmenos_ref.so")
 
 # Opcodes: the reference's menos::Opcode order (include/menos/circuit.h:17-41).
 OPCODES = ["x", "y", "z", "h", "s", "sdg", "t", "tdg", "sx", "sxdg", "rx", "ry", "rz", "p",
-           "u", "cx", "cz", "swap", "cp", "rzz", "ccx", "unitary", "measure"]
+           "u", "cx", "cz", "swap", "cp", "rzz", "ccx", "unitary", "measure", "channel"]
 OP = {name: i for i, name in enumerate(OPCODES)}
 NUM_PARAMS = {10: 1, 11: 1, 12: 1, 13: 1, 14: 3, 18: 1, 19: 1}
 
@@ -58,6 +58,12 @@ class Circuit:
 
     def measure(self, qubit: int, clbit: int):
         self.ops.append((OP["measure"], (int(qubit),), (), None, int(clbit)))
+        return self
+
+    def channel(self, qubits, kraus):
+        """A noise channel: Kraus operators (count, 2^k, 2^k)."""
+        m = np.ascontiguousarray(np.asarray(kraus, dtype=np.complex128))
+        self.ops.append((OP["channel"], tuple(int(q) for q in qubits), (), m, 0))
         return self
 
     def arrays(self):
@@ -108,6 +114,8 @@ def ops_struct_array(circ: Circuit):
             buf = np.ascontiguousarray(m.view(np.float64).ravel())
             keep.append(buf)
             o.matrix = buf.ctypes.data_as(C.POINTER(C.c_double))
+            if oc == OP["channel"]:
+                o.reserved = m.shape[0]
         o.clbit = cl
     return arr, keep
 
@@ -237,6 +245,10 @@ class RefLib:
         L.ref_run_plan.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
         L.ref_run_plan.restype = C.c_int
+        L.ref_run_dm.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64,
+                                 C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        L.ref_run_dm.restype = C.c_int
         L.ref_last_error.restype = C.c_char_p
         L.ref_default_threads.restype = C.c_uint32
         L.ref_kernel_isa.restype = C.c_int
@@ -326,6 +338,34 @@ class RefLib:
         d = int(nout[0]) if shots else 0
         return {
             "statevector": sv,
+            "counts": {int(o): int(c) for o, c in zip(outc[:d], cnt[:d])},
+            "terms": terms[:2 * len(paulis)].view(np.complex128).copy() if paulis else None,
+            "seconds": float(secs[0]),
+        }
+
+    def run_dm(self, circ: Circuit, threads=0, shots=0, seed=0, targets=(), width=None, paulis=()):
+        """DensityMatrixEngine::execute; returns dict(counts, terms, seconds)."""
+        arr, keep = ops_struct_array(circ)
+        t = np.asarray(targets, np.uint32).ravel()
+        if width is None:
+            width = int(max(t[1::2]) + 1) if len(t) else 0
+        cap = max(shots, 1)
+        outc = np.zeros(cap, np.uint64)
+        cnt = np.zeros(cap, np.uint64)
+        nout = np.array([cap], np.uint64)
+        xs = np.array([p[0] for p in paulis] or [0], np.uint64)
+        zs = np.array([p[1] for p in paulis] or [0], np.uint64)
+        terms = np.zeros(2 * max(len(paulis), 1), np.float64)
+        secs = np.zeros(1, np.float64)
+        rc = self.L.ref_run_dm(
+            circ.num_qubits, C.addressof(arr), len(circ.ops), threads, shots, seed,
+            t.ctypes.data if len(t) else None, len(t) // 2, width, outc.ctypes.data if shots else None,
+            cnt.ctypes.data, nout.ctypes.data, xs.ctypes.data, zs.ctypes.data, len(paulis),
+            terms.ctypes.data if paulis else None, secs.ctypes.data)
+        assert rc == 0, self.L.ref_last_error()
+        del keep
+        d = int(nout[0]) if shots else 0
+        return {
             "counts": {int(o): int(c) for o, c in zip(outc[:d], cnt[:d])},
             "terms": terms[:2 * len(paulis)].view(np.complex128).copy() if paulis else None,
             "seconds": float(secs[0]),

@@ -30,6 +30,7 @@
 
 #include "common/rng.h"
 #include "engines/dense/apply_matrix.h"
+#include "engines/density_matrix/density_matrix_engine.h"
 #include "engines/dense/dense_engine.h"
 #include "engines/dense/fused_block.h"
 #include "engines/dense/sample.h"
@@ -61,6 +62,17 @@ menos::Operation to_operation(const mb2_op& op) {
         return menos::MeasureOp{op.qubits[0], op.clbit};
     }
     std::vector<menos::QubitId> qubits(op.qubits, op.qubits + op.num_qubits);
+    if (op.opcode == MB2_CHANNEL) {
+        const std::size_t entries = std::size_t{1} << (2 * op.num_qubits);
+        std::vector<std::vector<C>> kraus(op.reserved, std::vector<C>(entries));
+        for (std::size_t t = 0; t < op.reserved; ++t) {
+            for (std::size_t i = 0; i < entries; ++i) {
+                const double* z = op.matrix + 2 * (t * entries + i);
+                kraus[t][i] = C{z[0], z[1]};
+            }
+        }
+        return menos::ChannelOp{std::move(qubits), std::move(kraus)};
+    }
     if (op.opcode == MB2_UNITARY) {
         const std::size_t dim = std::size_t{1} << op.num_qubits;
         std::vector<C> m(dim * dim);
@@ -267,6 +279,77 @@ int ref_run_dense(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_o
         }
         if (statevector != nullptr) {
             std::memcpy(statevector, res.statevector->data(), res.statevector->size() * sizeof(C));
+        }
+        if (req.want_counts) {
+            std::uint64_t i = 0;
+            for (const auto& [key, count] : *res.counts) {
+                if (i >= *n_outcomes) {
+                    g_error = "outcome capacity exceeded";
+                    return -1;
+                }
+                out_outcomes[i] = bits_of(key);
+                out_counts[i] = count;
+                ++i;
+            }
+            *n_outcomes = i;
+        }
+        if (req.want_expectation) {
+            for (std::uint32_t i = 0; i < n_terms; ++i) {
+                terms_out[2 * i] = (*res.expectation_terms)[i].real();
+                terms_out[2 * i + 1] = (*res.expectation_terms)[i].imag();
+            }
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// DensityMatrixEngine::execute on ops (src/engines/density_matrix/
+// density_matrix_engine.cpp): counts (capacity *n_outcomes, updated) and
+// expectation terms (2 * n_terms doubles) when their pointers are non-null;
+// seconds_out (optional) the wall time of execute() alone.
+int ref_run_dm(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_ops, std::uint32_t threads,
+               std::uint64_t shots, std::uint64_t seed, const std::uint32_t* targets, std::uint32_t n_targets,
+               std::uint32_t width, std::uint64_t* out_outcomes, std::uint64_t* out_counts,
+               std::uint64_t* n_outcomes, const std::uint64_t* x_masks, const std::uint64_t* z_masks,
+               std::uint32_t n_terms, double* terms_out, double* seconds_out) {
+    try {
+        std::vector<menos::Operation> v;
+        v.reserve(n_ops);
+        for (std::uint32_t i = 0; i < n_ops; ++i) {
+            v.push_back(to_operation(ops[i]));
+        }
+        std::vector<std::pair<menos::QubitId, menos::ClbitId>> t(n_targets);
+        for (std::uint32_t i = 0; i < n_targets; ++i) {
+            t[i] = {targets[2 * i], targets[2 * i + 1]};
+        }
+        menos::Observable obs;
+        for (std::uint32_t i = 0; i < n_terms; ++i) {
+            menos::PauliString p{num_qubits, {x_masks[i]}, {z_masks[i]}};
+            obs.terms.emplace_back(std::move(p), C{1.0, 0.0});
+        }
+        menos::EngineExecutionRequest req{};
+        req.num_qubits = num_qubits;
+        req.operations = v;
+        req.want_statevector = false;
+        req.want_counts = out_outcomes != nullptr && shots > 0;
+        req.want_expectation = terms_out != nullptr && n_terms > 0;
+        req.shots = shots;
+        req.measure_targets = t;
+        req.bitstring_width = width;
+        req.seed = seed;
+        req.budget_bytes = ~std::uint64_t{0};
+        req.is_sole_region = true;
+        req.observable = req.want_expectation ? &obs : nullptr;
+        req.max_threads = threads == 0 ? menos::common::default_thread_count() : threads;
+        menos::engines::density_matrix::DensityMatrixEngine engine;
+        const auto t0 = std::chrono::steady_clock::now();
+        menos::EngineExecutionResult res = engine.execute(req);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (seconds_out != nullptr) {
+            *seconds_out = std::chrono::duration<double>(t1 - t0).count();
         }
         if (req.want_counts) {
             std::uint64_t i = 0;
