@@ -1191,6 +1191,9 @@ int time_sweep(mb2_state* st, const std::vector<mb2_op>& ops, uint32_t tile, dou
 // memory and the fixed launch cost from an empty pass at n and n - 2 qubits,
 // compute from passes of many unfused blocks (compute-bound by construction):
 // a dense one-qubit block and a two-qubit diagonal block.
+// The state whose pass times the per-pass fixed cost (launch, ramp, tail).
+constexpr uint32_t kFixedCostQubits = 14;
+
 int measure_costs(mb2_state* st, mb2_state* small, uint32_t m, double* fixed, double* pass, double* dense1,
                   double* diag) {
     const uint32_t n = st->n;
@@ -1207,7 +1210,9 @@ int measure_costs(mb2_state* st, mb2_state* small, uint32_t m, double* fixed, do
     if (int rc = time_sweep(st, u.ops, m, &tu, 0); rc != MB2_OK) return rc;
     if (int rc = time_sweep(st, d.ops, m, &td, 0); rc != MB2_OK) return rc;
     const double amps = static_cast<double>(uint64_t{1} << n);
-    const double f = std::max(0.0, (4.0 * tes - te) / 3.0) * 1e-3;  // te = f + A p, tes = f + A p / 4
+    // The small state's pass is all fixed cost (its bytes take well under a
+    // microsecond); te = f + A p.
+    const double f = tes * 1e-3;
     *fixed = f;
     *pass = std::max(0.0, te * 1e-3 - f) / amps;
     *dense1 = std::max(0.0, tu * 1e-3 - f) / (amps * static_cast<double>(u.ops.size()));
@@ -1239,7 +1244,7 @@ int mb2_autotune(mb2_context* ctx, uint32_t probe_qubits, mb2_tuning* out) {
         mb2_state* st = nullptr;
         mb2_state* small = nullptr;
         if (int rc = mb2_state_alloc(ctx, n, prec, ~uint64_t{0}, &st); rc != MB2_OK) return rc;
-        if (int rc = mb2_state_alloc(ctx, n - 2, prec, ~uint64_t{0}, &small); rc != MB2_OK) {
+        if (int rc = mb2_state_alloc(ctx, kFixedCostQubits, prec, ~uint64_t{0}, &small); rc != MB2_OK) {
             mb2_state_free(st);
             return rc;
         }

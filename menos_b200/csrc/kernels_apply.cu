@@ -288,6 +288,7 @@ int launch_tile_pass(void* amps, uint32_t n, const TilePass& pass, const uint32_
     L.amps = amps;
     L.m = pass.m;
     L.smask = pass.smask;
+    L.gmask = pass.gmask;
     L.words = dev_words + pass.word_begin;
     L.nwords = pass.word_count;
     L.sdata = dev_sdata + pass.sdata_begin;

@@ -391,6 +391,7 @@ int launch_tile_pass_c64(void* amps, uint32_t n, const TilePass& pass, const uin
                          const BatchLayout* batch) {
     if (pass.m > kMaxTileQubitsC64 || pass.m < kMinTileQubits) return MB2_ERR_INVALID;
     if ((pass.word_count & 3u) != 0 || (pass.param_len != 0 && batch == nullptr)) return MB2_ERR_INVALID;
+    if (pass.gmask != 0) return MB2_ERR_INVALID;  // the complex64 kernels read operands inside the tile only
     TileLaunch L;
     L.amps = amps;
     L.m = pass.m;

@@ -515,7 +515,8 @@ int launch_tc_instance(const TileLaunch& L, const uint32_t* tcm, uint32_t nphase
 
 int launch_tile_pass_tc(void* amps, uint32_t n, const TilePass& pass, const uint32_t* dev_words,
                         const double* dev_sdata, const uint32_t* dev_tc, int* dev_err, int sm_count, void* stream) {
-    if (!pass.tc || pass.m < 11 || pass.m > 13 || (pass.word_count & 3u) != 0) return MB2_ERR_INVALID;
+    if (!pass.tc || pass.m < 11 || pass.m > 13 || (pass.word_count & 3u) != 0 || pass.gmask != 0)
+        return MB2_ERR_INVALID;
     TileLaunch L;
     L.amps = amps;
     L.m = pass.m;

@@ -110,9 +110,16 @@ struct TileInstr {
 };
 static_assert(sizeof(TileInstr) == 32, "TileInstr is 32 bytes");
 
+// Diagonal operands outside a pass's tile: at most kMaxGlobalQubits per
+// pass; in instructions, the operand at rank r among them is position
+// kGlobalPos0 + r (tile positions are below 16).
+constexpr uint32_t kMaxGlobalQubits = 16;
+constexpr uint32_t kGlobalPos0 = 16;
+
 struct TilePass {
     uint32_t m = 0;          // tile qubits
     uint64_t smask = 0;      // global qubits in the tile
+    uint64_t gmask = 0;      // qubits outside the tile whose bits diagonals read (complex128 plain path)
     uint32_t prog_begin = 0; // first instruction
     uint32_t prog_count = 0;
     uint32_t sdata_begin = 0;  // this pass's staged data (doubles), copied to shared memory
@@ -153,10 +160,14 @@ constexpr uint32_t kSw12 = 45;   // + pair
 constexpr uint32_t kSw13 = 57;   // + pair
 constexpr uint32_t kSw23 = 69;   // + pair
 constexpr uint32_t kDs1R = 81;   // + slot; aux = entry classes
-constexpr uint32_t kDs1T = 85;   // aux = classes; the operand's tile bit in bits 16-19
+// An operand position (0-31) in a header word: bits 16-19 and bit 31 (the
+// staged data offset, bits 20-30, stays below 2048 16-byte units).
+constexpr uint32_t kDs1T = 85;   // aux = classes; the operand's position in bits 16-19, 31
 constexpr uint32_t kDs2RR = 86;  // + pair; aux = classes
-constexpr uint32_t kDs2RT = 98;  // + 2 * slot + (index of the thread-bit operand); tile bit in bits 16-19
-constexpr uint32_t kDs2TT = 106; // aux = classes; extra word = the two tile bits (4 bits each)
+constexpr uint32_t kDs2RT = 98;  // + 2 * slot + (index of the bit-value operand); its position in bits 16-19, 31
+// aux = classes; extra word = the two operand positions: low 4 bits at 0-3
+// and 4-7, their bit 4 at bits 8 and 9.
+constexpr uint32_t kDs2TT = 106;
 constexpr uint32_t kDiagK = 107; // aux = k; extra word = tile positions (4 bits each)
 constexpr uint32_t kSigns = 108; // aux = monomial count; one word per monomial
 // Runs of U3 blocks on consecutive register slots, their matrices
@@ -165,6 +176,10 @@ constexpr uint32_t kU3Run0123 = 109;
 constexpr uint32_t kU3Run01 = 110;
 constexpr uint32_t kU3Run123 = 111;
 constexpr uint32_t kU3Run012 = 112;
+// Sign monomials some of whose factors are qubits outside the tile: two
+// words per monomial, the register slots (bits 0-15) and the operand bits
+// (positions 0-31: tile bits, then the outside qubits from kGlobalPos0).
+constexpr uint32_t kSignsW = 113;
 // aux = thread bits; bits 16-31 register positions; then the phase record:
 // words 1-2 the byte offsets (16 bits each) of the four register bits' slots
 // with 16-byte slots, words 3-4 the same with 8-byte slots, words 5-28 a
@@ -284,6 +299,7 @@ struct TileLaunch {
     uint32_t n_all = 0;  // index bits, bindings included
     uint32_t m = 0;
     uint64_t smask = 0;
+    uint64_t gmask = 0;
     const uint32_t* words = nullptr;
     uint32_t nwords = 0;
     const double* sdata = nullptr;

@@ -23,12 +23,14 @@ namespace {
 
 uint32_t pair_index(uint32_t p0, uint32_t p1) { return p0 * 3 + (p1 < p0 ? p1 : p1 - 1); }
 
+// op, aux, an operand position (0-31: bits 16-19 and 31) and the staged data
+// offset in 16-byte units (bits 20-30).
 uint32_t header(uint32_t op, uint32_t aux, uint32_t tbit, uint32_t off_doubles) {
     if (off_doubles & 1u) throw std::logic_error("staged data offset is not 16-byte aligned");
     const uint32_t off = off_doubles / 2;
-    if (off >= 4096u || aux > 255u || tbit > 15u)
+    if (off >= 2048u || aux > 255u || tbit > 31u)
         throw std::invalid_argument("pass data beyond the compact stream's reach");
-    return op | (aux << 8) | (tbit << 16) | (off << 20);
+    return op | (aux << 8) | ((tbit & 15u) << 16) | (off << 20) | ((tbit >> 4) << 31);
 }
 
 bool is_param(const TileInstr& g) {
@@ -48,7 +50,7 @@ void fuse_u3_runs(std::vector<uint32_t>& w, size_t begin) {
     std::vector<uint32_t> out(w.begin(), w.begin() + static_cast<long>(begin));
     size_t i = begin;
     auto is_u3 = [&](size_t k, uint32_t slot) { return k < w.size() && (w[k] & 0xffu) == cop::kU3 + slot; };
-    auto off = [&](size_t k) { return w[k] >> 20; };
+    auto off = [&](size_t k) { return (w[k] >> 20) & 0x7ffu; };
     auto chain = [&](size_t k, uint32_t first, uint32_t len) {
         for (uint32_t t = 0; t < len; ++t) {
             if (!is_u3(k + t, first + t)) return false;
@@ -64,6 +66,7 @@ void fuse_u3_runs(std::vector<uint32_t>& w, size_t begin) {
         else if (op == cop::kSmem) len = 3;
         else if ((op >= cop::kMono2 && op < cop::kSw12) || op == cop::kDs2TT || op == cop::kDiagK) len = 2;
         else if (op == cop::kSigns) len = 1 + ((w[i] >> 8) & 0xffu);
+        else if (op == cop::kSignsW) len = 1 + 2 * ((w[i] >> 8) & 0xffu);
         if (op == cop::kU3 && chain(i, 0, 4)) {
             out.push_back((w[i] & ~0xffu) | cop::kU3Run0123);
             i += 4;
@@ -123,12 +126,12 @@ void encode_compact(TileProgram& prog) {
                 w.push_back(header(cop::kDs2RT + 2 * (c1 & 3u), cls, c0, off));
             } else {
                 w.push_back(header(cop::kDs2TT, cls, 0, off));
-                w.push_back(c0 | (c1 << 4));
+                w.push_back((c0 & 15u) | ((c1 & 15u) << 4) | ((c0 >> 4) << 8) | ((c1 >> 4) << 9));
             }
         };
-        // Pending sign monomials (canonical words), toggled so pairs cancel,
-        // and the +-1 diagonals they come from.
-        std::map<uint32_t, bool> signs;
+        // Pending sign monomials (register slots | operand bits << 16),
+        // toggled so pairs cancel, and the +-1 diagonals they come from.
+        std::map<uint64_t, bool> signs;
         std::vector<const TileInstr*> sign_run;
         auto flush_signs = [&]() {
             if (sign_run.size() == 1 && sign_run[0]->kind == TK_DSMALL) {
@@ -142,14 +145,25 @@ void encode_compact(TileProgram& prog) {
                 return;
             }
             sign_run.clear();
-            std::vector<uint32_t> live;
+            std::vector<uint64_t> live;
+            bool wide = false;  // a factor outside the tile: two words per monomial
             for (const auto& [mono, on] : signs)
-                if (on) live.push_back(mono);
+                if (on) {
+                    live.push_back(mono);
+                    wide = wide || (mono >> 32) != 0;
+                }
             signs.clear();
             for (size_t i = 0; i < live.size(); i += 255) {
                 const uint32_t cnt = static_cast<uint32_t>(std::min<size_t>(255, live.size() - i));
-                w.push_back(header(cop::kSigns, cnt, 0, 0));
-                w.insert(w.end(), live.begin() + static_cast<long>(i), live.begin() + static_cast<long>(i + cnt));
+                w.push_back(header(wide ? cop::kSignsW : cop::kSigns, cnt, 0, 0));
+                for (size_t t = i; t < i + cnt; ++t) {
+                    if (wide) {
+                        w.push_back(static_cast<uint32_t>(live[t] & 0xffffu));
+                        w.push_back(static_cast<uint32_t>(live[t] >> 16));
+                    } else {
+                        w.push_back(static_cast<uint32_t>(live[t]));
+                    }
+                }
             }
         };
         // Register slot of tile position p in the current phase, -1 for a thread bit.
@@ -170,14 +184,14 @@ void encode_compact(TileProgram& prog) {
             constexpr uint32_t kSlotBits[kRegQubits] = {0xAAAAu, 0xCCCCu, 0xF0F0u, 0xFF00u};
             for (uint32_t s = 0; s < dim; ++s) {
                 if (!c[s]) continue;
-                uint32_t slots = 0xffffu, tbits = 0;
+                uint64_t slots = 0xffffu, tbits = 0;
                 for (uint32_t t = 0; t < k; ++t) {
                     if (!(s & (1u << t))) continue;
                     const int r = slot_of(pos[t]);
                     if (r >= 0) slots &= kSlotBits[r];
-                    else tbits |= 1u << pos[t];
+                    else tbits |= uint64_t{1} << pos[t];
                 }
-                const uint32_t mono = slots | (tbits << 16);
+                const uint64_t mono = slots | (tbits << 16);
                 signs[mono] = !signs[mono];
             }
         };

@@ -219,7 +219,7 @@ template <int MT, bool FULL, typename SYNC>
 __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const uint32_t* __restrict__ sw,
                                              uint32_t nwords, const double* __restrict__ sd, uint32_t nsdata,
                                              uint32_t pshift, const double* __restrict__ gdata, uint32_t tid,
-                                             uint32_t m, SYNC sync) {
+                                             uint32_t m, uint32_t gbits, SYNC sync) {
     const uint32_t tbits = m - kRegQubits;
     const uint32_t s_tid = swz(tid);
     auto slot = [&](int j) -> uint32_t { return s_tid ^ swz(static_cast<uint32_t>(j) << tbits); };
@@ -244,6 +244,9 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
             // rather than held in 16 registers through the gates).
             const uint32_t z0 = swz(tb) << 4, z1 = rec[1] & 0xffffu, z2 = rec[1] >> 16, z3 = rec[2] & 0xffffu,
                            z4 = rec[2] >> 16;
+            // Operand bit values from here on: the tile bits, and from
+            // position kGlobalPos0 the tile's bits of the qubits outside it.
+            tb |= gbits;
             char* const tile_b = reinterpret_cast<char*>(tile);
             auto at = [&](int j) -> double2& {
                 return *reinterpret_cast<double2*>(
@@ -256,9 +259,10 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
                 const uint32_t op = w & 0xffu;
                 if (op == cop::kEnd) break;
                 const uint32_t aux = (w >> 8) & 0xffu;
-                const uint32_t off = (w >> 20) << 1;
+                const uint32_t off = ((w >> 20) & 0x7ffu) << 1;
                 const double* md = sd + off + (off >= nsdata ? pshift : 0u);
-                const uint32_t tv = (tb >> ((w >> 16) & 15u)) & 1u;  // the thread-bit operand's value
+                // The bit-value operand's value (position: bits 16-19, 31).
+                const uint32_t tv = (tb >> (((w >> 16) & 15u) | ((w >> 27) & 16u))) & 1u;
                 switch (op) {
 #define MB2_CASE4(BASE, ...) \
     case BASE + 0: { constexpr int P = 0; __VA_ARGS__; } break; \
@@ -325,7 +329,8 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
                     case cop::kDs2RT + 7: diag_rt<3>(a, load_diag(md, 2, aux), 0u, tv); break;
                     case cop::kDs2TT: {
                         const uint32_t cc = sw[pc++];
-                        const uint32_t e = ((tb >> (cc & 15u)) & 1u) | (((tb >> ((cc >> 4) & 15u)) & 1u) << 1);
+                        const uint32_t e = ((tb >> ((cc & 15u) | ((cc >> 4) & 16u))) & 1u) |
+                                           (((tb >> (((cc >> 4) & 15u) | ((cc >> 5) & 16u))) & 1u) << 1);
                         const Diag4 D = load_diag(md, 2, aux);
                         diag_set<-1, -1>(a, (aux >> (2 * e)) & 3u, diag_entry(D, e), 0, 0);
                     } break;
@@ -336,6 +341,16 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
                             const uint32_t mono = sw[pc++];
                             const uint32_t tm = mono >> 16;
                             M ^= (tb & tm) == tm ? (mono & 0xffffu) : 0u;
+                        }
+#pragma unroll
+                        for (int j = 0; j < kNA; ++j) a[j] = cneg_mask(a[j], (M << (31 - j)) & 0x80000000u);
+                    } break;
+                    case cop::kSignsW: {
+                        uint32_t M = 0;
+                        for (uint32_t i = 0; i < aux; ++i) {
+                            const uint32_t slots = sw[pc], bits = sw[pc + 1];
+                            pc += 2;
+                            M ^= (tb & bits) == bits ? slots : 0u;
                         }
 #pragma unroll
                         for (int j = 0; j < kNA; ++j) a[j] = cneg_mask(a[j], (M << (31 - j)) & 0x80000000u);
@@ -415,7 +430,7 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
 // ((base | ~nmask) + step) & nmask, step = deposit(gridDim.x).
 template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
 __global__ void __launch_bounds__(MAXT, MINB)
-    k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask,
+    k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask, uint64_t gmask,
                 const uint32_t* __restrict__ words, uint32_t nwords, const double* __restrict__ sdata,
                 uint32_t nsdata, const double* __restrict__ gdata, uint64_t ntiles, const double* __restrict__ pdata,
                 uint32_t pstride, uint32_t param_lo, uint32_t param_len, uint32_t bshift, uint32_t stages) {
@@ -501,7 +516,15 @@ __global__ void __launch_bounds__(MAXT, MINB)
         else cp_async_wait<1>();
         __syncthreads();
 
-        compute_tile<MT, FULL>(tile, sw, nwords, sd, nsdata, 0u, gdata, tid, m, [] { __syncthreads(); });
+        // The tile's bits of the qubits outside it that diagonals read, at
+        // positions kGlobalPos0 + rank.
+        uint32_t gbits = 0;
+        {
+            uint32_t r = kGlobalPos0;
+            for (uint64_t g = gmask; g != 0; g &= g - 1, ++r)
+                gbits |= static_cast<uint32_t>((static_cast<uint64_t>(cbase) >> (__ffsll(static_cast<long long>(g)) - 1)) & 1u) << r;
+        }
+        compute_tile<MT, FULL>(tile, sw, nwords, sd, nsdata, 0u, gdata, tid, m, gbits, [] { __syncthreads(); });
 
         // Store: canonical mapping, -0.0 normalised.
         const IDX b0 = cbase + off_lo;
@@ -531,7 +554,7 @@ int launch_instance(const TileLaunch& L) {
     if (dyn_max == 0) return launch_status();
     if (L.smem > dyn_max) return MB2_ERR_INVALID;
     k_tile_pass<MAXT, MINB, MT, IDX, FULL><<<L.grid, L.threads, L.smem, static_cast<cudaStream_t>(L.stream)>>>(
-        static_cast<double2*>(L.amps), L.n_all, L.m, L.smask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata,
+        static_cast<double2*>(L.amps), L.n_all, L.m, L.smask, L.gmask, L.words, L.nwords, L.sdata, L.nsdata, L.gdata,
         L.ntiles, L.pdata, L.pstride, L.param_lo, L.param_len, L.bshift, L.stages);
     return launch_status();
 }

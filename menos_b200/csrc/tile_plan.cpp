@@ -58,15 +58,44 @@ int mono_src(const std::vector<Cd>& m, uint32_t dim, uint32_t r) {
 
 struct PassSel {
     uint64_t smask;
+    uint64_t gmask = 0;           // qubits outside the tile that diagonals of the pass read
     std::vector<uint32_t> gates;  // block indices in application order
 };
 
+// A diagonal block's operands need not lie in the tile: an amplitude's entry
+// depends only on its operand bits, and a qubit outside the tile has one
+// value over the whole tile, which the kernel reads off the tile's base
+// index.  That holds for the instructions that take an operand as a bit
+// value -- diagonals of at most two operands and +-1 diagonals (sign
+// monomials) -- not for the wide entry-index diagonal (kDiagK).
+bool diagonal_any_operand(const Block& b, bool parametric) {
+    if (!b.diagonal) return false;
+    if (b.k <= 2) return true;
+    if (parametric) return false;
+    const uint32_t dim = 1u << b.k;
+    for (uint32_t e = 0; e < dim; ++e) {
+        const Cd& d = b.m[size_t{e} * dim + e];
+        if (d.imag() != 0.0 || (d.real() != 1.0 && d.real() != -1.0)) return false;
+    }
+    return true;
+}
+
+// A diagonal operand's instruction position: its tile position, or
+// kGlobalPos0 + its rank among the pass's outside qubits.
+uint32_t operand_pos(uint64_t smask, uint64_t gmask, uint32_t q) {
+    if ((smask >> q) & 1u) return local_pos(smask, q);
+    if (!((gmask >> q) & 1u)) throw std::logic_error("diagonal operand neither in the tile nor global");
+    return kGlobalPos0 + static_cast<uint32_t>(std::popcount(gmask & ((uint64_t{1} << q) - 1)));
+}
+
 // Passes are maximal runs of CONSECUTIVE blocks whose operands fit one
-// tile.  Blocks are never reordered, not even commuting ones: two gates on
-// disjoint qubits applied in the other order give the same state only up to
-// rounding, and the plain path is bitwise the reference's sweep, which
-// applies the blocks in plan order.
-std::vector<PassSel> select_passes(const std::vector<Block>& blocks, uint32_t n, uint32_t m, uint32_t fixed_low) {
+// tile -- diagonals read up to kMaxGlobalQubits qubits outside it.  Blocks
+// are never reordered, not even commuting ones: two gates on disjoint qubits
+// applied in the other order give the same state only up to rounding, and
+// the plain path is bitwise the reference's sweep, which applies the blocks
+// in plan order.
+std::vector<PassSel> select_passes(const std::vector<Block>& blocks, uint32_t n, uint32_t m, uint32_t fixed_low,
+                                   const std::vector<uint8_t>* parametric) {
     std::vector<PassSel> passes;
     uint32_t widest = 1;
     for (const Block& b : blocks) widest = std::max(widest, b.k);
@@ -75,25 +104,41 @@ std::vector<PassSel> select_passes(const std::vector<Block>& blocks, uint32_t n,
     // Low qubits kept in every tile so that tiles gather contiguous runs,
     // leaving room for the widest block.
     const uint32_t fixed = std::min(fixed_low, mt - widest);
+    // Qubits outside the tile that the diagonals read, once the tile is
+    // padded to mt qubits with them first.
+    auto outside = [&](uint64_t s, uint64_t d) {
+        return std::popcount(d & ~s) - (static_cast<int>(mt) - std::popcount(s));
+    };
     size_t i = 0;
     while (i < blocks.size()) {
-        uint64_t smask = 0;
+        uint64_t smask = 0, dmask = 0;  // the tile's qubits so far; the diagonals' operands
         for (uint32_t q = 0; q < fixed; ++q) smask |= uint64_t{1} << q;
         PassSel sel;
         size_t staged = 0;
         while (i < blocks.size() && sel.gates.size() < kMaxBlocksPerPass) {
-            const uint64_t grown = smask | blocks[i].mask();
-            if (static_cast<uint32_t>(std::popcount(grown)) > mt) break;
+            const bool param = parametric != nullptr && ((*parametric)[i] & kParamBlock) != 0;
+            uint64_t s2 = smask, d2 = dmask;
+            if (diagonal_any_operand(blocks[i], param)) d2 |= blocks[i].mask();
+            else s2 |= blocks[i].mask();
+            if (static_cast<uint32_t>(std::popcount(s2)) > mt) break;
+            if (outside(s2, d2) > static_cast<int>(kMaxGlobalQubits)) break;
             if (staged + staged_bytes(blocks[i]) > kMaxStagedBytes && !sel.gates.empty()) break;
             staged += staged_bytes(blocks[i]);
-            smask = grown;
+            smask = s2;
+            dmask = d2;
             sel.gates.push_back(static_cast<uint32_t>(i));
             ++i;
         }
-        // Pad the tile to exactly mt qubits with the lowest unused ones.
+        // Pad the tile to exactly mt qubits: first with the diagonals'
+        // operands the global limit leaves out, then with the lowest unused
+        // qubits (longer contiguous runs per tile).
+        for (uint64_t rest = dmask & ~smask; std::popcount(rest) > static_cast<int>(kMaxGlobalQubits);
+             rest &= rest - 1)
+            smask |= rest & (~rest + 1);
         for (uint32_t q = 0; q < n && static_cast<uint32_t>(std::popcount(smask)) < mt; ++q)
             smask |= uint64_t{1} << q;
         sel.smask = smask;
+        sel.gmask = dmask & ~smask;
         passes.push_back(std::move(sel));
     }
     return passes;
@@ -316,7 +361,8 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
     const uint32_t mt = std::min(m, n);
     if (mt < kRegQubits) throw std::invalid_argument("state too small for the tile kernel");
     const std::vector<PassSel> sels =
-        commuting ? select_passes_commuting(blocks, n, mt, fixed_low) : select_passes(blocks, n, mt, fixed_low);
+        commuting ? select_passes_commuting(blocks, n, mt, fixed_low)
+                  : select_passes(blocks, n, mt, fixed_low, parametric);
     prog.param_offsets.assign(blocks.size(), 0);
     auto param_flags = [&](uint32_t bi) -> uint8_t { return parametric ? (*parametric)[bi] : uint8_t{0}; };
     // A parametric block's data goes to the per-binding record.
@@ -330,6 +376,7 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
         TilePass pass;
         pass.m = mt;
         pass.smask = sel.smask;
+        pass.gmask = sel.gmask;
         pass.prog_begin = static_cast<uint32_t>(prog.instrs.size());
         pass.sdata_begin = static_cast<uint32_t>(prog.data.size());
         pass.gates = static_cast<uint32_t>(sel.gates.size());
@@ -401,7 +448,8 @@ TileProgram plan_tile_program(const std::vector<Block>& blocks, uint32_t n, uint
             if (b.diagonal) {
                 if (!open) open_phase({}, j + 1);
                 g.op = TOP_DIAG;
-                for (uint32_t t = 0; t < b.k; ++t) g.pos[t] = static_cast<uint8_t>(local_pos(sel.smask, b.q[t]));
+                for (uint32_t t = 0; t < b.k; ++t)
+                    g.pos[t] = static_cast<uint8_t>(operand_pos(sel.smask, sel.gmask, b.q[t]));
                 std::vector<Cd> d(dim);
                 for (uint32_t i = 0; i < dim; ++i) d[i] = b.m[i * dim + i];
                 if (param_flags(sel.gates[j]) & kParamBlock) {

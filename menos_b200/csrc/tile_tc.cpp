@@ -312,6 +312,7 @@ void make_tensor_core_program(TileProgram& prog, const std::vector<Block>& block
             cur = TilePass{};
             cur.m = src.m;
             cur.smask = src.smask;
+            cur.gmask = src.gmask;
             cur.tc = true;
             cur.prog_begin = static_cast<uint32_t>(instrs.size());
             cur.sdata_begin = static_cast<uint32_t>(data.size());
@@ -436,6 +437,12 @@ void run_program_on_host(const TileProgram& prog, uint32_t n, Cd* state) {
         std::vector<uint32_t> qubit;
         for (uint32_t q = 0; q < n; ++q)
             if ((pass.smask >> q) & 1u) qubit.push_back(q);
+        // A diagonal's operand position: a tile position, or kGlobalPos0 +
+        // rank among the outside qubits it reads.
+        std::vector<uint32_t> outside;
+        for (uint32_t q = 0; q < n; ++q)
+            if ((pass.gmask >> q) & 1u) outside.push_back(q);
+        auto qubit_at = [&](uint32_t p) { return p >= kGlobalPos0 ? outside.at(p - kGlobalPos0) : qubit.at(p); };
         const TileInstr* ins = prog.instrs.data() + pass.prog_begin;
         const double* sdata = prog.data.data() + pass.sdata_begin;
         uint32_t reg[kRegQubits] = {0, 1, 2, 3};
@@ -464,7 +471,7 @@ void run_program_on_host(const TileProgram& prog, uint32_t n, Cd* state) {
                     const uint32_t dim = 1u << g.k;
                     std::vector<Cd> m(size_t{dim} * dim, Cd(0.0, 0.0));
                     for (uint32_t e = 0; e < dim; ++e) m[e * dim + e] = Cd(sdata[g.data + 2 * e], sdata[g.data + 2 * e + 1]);
-                    for (uint32_t t = 0; t < g.k; ++t) ops[t] = qubit[g.pos[t]];
+                    for (uint32_t t = 0; t < g.k; ++t) ops[t] = qubit_at(g.pos[t]);
                     host_apply_generic(state, amps, m.data(), ops, g.k);
                     break;
                 }

@@ -159,7 +159,7 @@ def test_complex64_brick_schedule_has_few_passes():
     c = workloads.brick(28, 32, 5)
     plain = max(p for p, _, _ in schedule(c, 28, tile=12)) + 1
     reord = max(p for p, _, _ in schedule(c, 28, tile=12, precision=_lib.C64)) + 1
-    assert reord <= 40 and 4 * reord <= plain, (reord, plain)
+    assert reord <= 40 and 3 * reord <= plain, (reord, plain)
 
 
 def test_brick_schedule_pass_count():
@@ -167,6 +167,6 @@ def test_brick_schedule_pass_count():
     workloads.qft(30, c)
     sched = schedule(c, 30, fuse=True, tile=12)
     passes = max(p for p, _, _ in sched) + 1
-    # runs of consecutive blocks (never reordered): ~300 passes instead of
-    # one per block (2260 blocks)
-    assert passes < 400, passes
+    # runs of consecutive blocks (never reordered), diagonals reading qubits
+    # outside the tile: ~160 passes instead of one per block (2260 blocks)
+    assert passes < 200, passes
