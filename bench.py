@@ -51,10 +51,10 @@ def kernel_launches() -> int:
 
 def profiled_traffic(n: int):
     """DRAM bytes of one tile-pass launch, from the committed ncu summary
-    (measured at 26 qubits, scaled to 2^n: every tile is read and written
+    (measured at 28 qubits, scaled to 2^n: every tile is read and written
     once), or None when the summary is absent."""
     import re
-    path = os.path.join(ROOT, "profiles", "k_tile_pass_c2_26q_ncu_full.md")
+    path = os.path.join(ROOT, "profiles", "k_tile_pass_c2_28q_ncu_full.md")
     try:
         with open(path) as f:
             m = re.search(r"traffic_bytes_per_launch_30q:\s*([0-9.eE+]+)", f.read())
@@ -327,8 +327,8 @@ def main():
                    "tile_qubits": args.tile or 11},
         "roofline": {"bound": "hbm", "kernel": "k_tile_pass", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": profiled_traffic(n),
-                     "traffic_source": "ncu dram__bytes_read+write of one pass at 26 qubits, scaled by the "
-                                       "state size (profiles/k_tile_pass_c2_26q_ncu_full.md)",
+                     "traffic_source": "ncu dram__bytes_read+write of one pass at 28 qubits, scaled by the "
+                                       "state size (profiles/k_tile_pass_c2_28q_ncu_full.md)",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": 2 * state_bytes},
         "fp64": {"kernel": "k_tile_pass", "achieved_ops_per_s": round(stats.fp64_ops_per_amp * (1 << n) /
