@@ -77,6 +77,8 @@ def parse():
     p.add_argument("--fusion", type=int, default=0,
                    help="job: 0 = the reference's containment fusion; 2..6 = blocks of up to that many qubits")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-reference-gpu", action="store_true",
+                   help="with --impl reference: skip timing the reference's own CUDA engine")
     p.add_argument("--validate-cpu", action="store_true",
                    help="with --impl reference: the extrapolated CPU job time against a whole reference run")
     p.add_argument("--mode", default="job", choices=["job", "serve", "batch", "c64"])
@@ -623,6 +625,33 @@ def validate_cpu_baseline(args):
                       "ratio": round((1.0 / v) / whole, 3), "threads": cores, "detail": detail}), flush=True)
 
 
+def reference_gpu_job(n, circ, paulis, shots):
+    """The reference's own CUDA dense engine (CudaDenseEngine::execute, its
+    src/kernels/cuda built for sm_100a with its -fmad=false by
+    oracle/Makefile) on the whole job: wall time of one execute() for the
+    request the B200 engine's e2e leg runs (statevector norm as the identity
+    term, the Pauli terms, the shots), after a small warm-up run."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from menos_b200 import workloads
+    if not os.path.exists(pyoracle.REF_CUDA_SO):
+        return {"unavailable": "oracle/_ref/libmenos_ref_cuda.so is not built"}
+    ref = pyoracle.RefLib(pyoracle.REF_CUDA_SO)
+    warm = pyoracle.Circuit(16)
+    warm.ops = list(workloads.config_c2(n=16, depth=2).ops)
+    ref.run(warm, engine="cuda", statevector=False, shots=1000, seed=1, targets=[(q, q) for q in range(16)],
+            width=16, paulis=[(0, 0)])
+    oc = pyoracle.Circuit(n, circ.global_phase)
+    oc.ops = list(circ.ops)
+    r = ref.run(oc, engine="cuda", fuse_gates=True, statevector=False, shots=shots, seed=1234,
+                targets=[(q, q) for q in range(n)], width=n, paulis=[(0, 0)] + list(paulis))
+    s = r["seconds"]
+    return {"value": round(1.0 / s, 6), "unit": UNIT, "seconds": round(s, 3),
+            "engine": "reference CudaDenseEngine::execute (sm_100a, -fmad=false), containment fusion, "
+                      "host-side sampling walk",
+            "request": f"{n}q brick depth 40 + QFT, identity + {len(paulis)} Pauli terms, {shots} shots"}
+
+
 def main_reference(args, rank, world):
     if rank != 0:
         return
@@ -648,6 +677,13 @@ def main_reference(args, rank, world):
                                    f"full 1e6-shot walk; extrapolated to the job", "detail": detail},
         "e2e": {"value": round(v, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    # Beside the CPU arm, for reference: the reference's own GPU path.
+    try:
+        import torch
+        if torch.cuda.is_available() and not args.no_reference_gpu:
+            line["reference_gpu"] = reference_gpu_job(n, circ, paulis, args.shots)
+    except Exception as e:  # reported, never fatal to the CPU arm
+        line["reference_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     print(json.dumps(line), flush=True)
 
 

@@ -257,8 +257,9 @@ int mb2_synchronize(mb2_state* state);
  * bitwise the reference engine's rho.  mb2_dm_expectation: Tr(P_t rho) per
  * term (within 1e-12 of the reference's sequential sum).  mb2_dm_sample:
  * counts by the reference's sort-then-walk over rho's diagonal (identical
- * counts); outcomes as mb2_sample's.  n <= 15.  MeasureOps carry no readout
- * error across this ABI. */
+ * counts); outcomes as mb2_sample's.  n <= 15; channels of 1..5 qubits (4- and
+ * 5-qubit ones run as 8- and 10-operand blocks from global memory).
+ * MeasureOps carry no readout error across this ABI. */
 int mb2_dm_apply_program(mb2_state* rho, uint32_t num_qubits, const mb2_op* ops, uint32_t num_ops);
 int mb2_dm_expectation(mb2_state* rho, uint32_t num_qubits, const uint64_t* x_masks, const uint64_t* z_masks,
                        uint32_t num_terms, double* out);
@@ -353,6 +354,19 @@ int mb2_server_stats(mb2_server* server, uint64_t* pending, uint64_t* in_flight,
                      uint64_t* budget_bytes);
 /* Drops pending requests, waits for the running ones, frees everything. */
 int mb2_server_destroy(mb2_server* server);
+/* Admission through the caller's memory ledger (the reference's
+ * MemoryLedger, src/common/memory_ledger.h:37-117, Space::Device): a request
+ * is admitted when it fits the server's budget AND charge(user, bytes)
+ * returns nonzero (the ledger took the bytes: its state and staging, as the
+ * server counts them); release(user, bytes) is called when that memory is
+ * freed.  Both run on server threads, one call at a time, with the server's
+ * lock held (they must not call the server).  A refused request stays
+ * pending and is offered again within a few milliseconds.  Set before the
+ * first submit; null functions detach the ledger. */
+typedef int (*mb2_ledger_charge_fn)(void* user, uint64_t bytes);
+typedef void (*mb2_ledger_release_fn)(void* user, uint64_t bytes);
+int mb2_server_set_ledger(mb2_server* server, mb2_ledger_charge_fn charge, mb2_ledger_release_fn release,
+                          void* user);
 
 /* ---- calibration ------------------------------------------------------- */
 /* Measures the device's FP64 multiply/add issue rate (instructions per
@@ -366,11 +380,11 @@ int mb2_probe_rates(mb2_context* ctx, double* fp64_ops_per_s, double* copy_gbs);
  * Measures, on the context's device, which tile width runs a synthetic
  * brick sweep fastest (complex128: 10, 11, 12 qubits; complex64: 12, 13) at
  * probe_qubits (0: 24; 16..30) and the costs of the time model, in which a
- * pass takes  fixed + amplitudes * max(memory, sum of its blocks' compute):
- * the fixed launch cost and the memory cost of an empty pass (the state read
- * and written once, at probe_qubits and probe_qubits - 2), the compute of a
- * dense single-qubit block (a dense k-qubit block counts 2^(k-1) of them) and
- * of a diagonal block.  The widths become the context's defaults for
+ * pass takes  fixed + amplitudes * (memory + sum of its blocks' compute):
+ * the fixed cost of a pass (timed on a 14-qubit state), the memory cost of a
+ * near-empty pass (the state read and written once, at probe_qubits), the
+ * compute a dense single-qubit block adds to a pass (a dense k-qubit block
+ * counts 2^(k-1) of them) and that of a diagonal block.  The widths become the context's defaults for
  * sweeps with tile_qubits = 0; the costs feed mb2_estimate_sweep_time.
  * Replaces the reference's device microbenchmarks feeding CudaCalibration
  * (src/kernels/cuda/device_benchmarks.h:30-67, src/plan/cuda_calibration.h:9-48),

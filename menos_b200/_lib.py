@@ -80,6 +80,10 @@ class SweepStats(C.Structure):
 # Exported symbol -> (restype, argtypes); the list the C-ABI tests check
 # against include/mb2.h.
 _VP = C.c_void_p
+# mb2_ledger_charge_fn / mb2_ledger_release_fn
+LEDGER_CHARGE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64)
+LEDGER_RELEASE = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64)
+
 SIGNATURES = {
     "mb2_context_create": (C.c_int, [C.c_int, C.POINTER(_VP)]),
     "mb2_context_destroy": (C.c_int, [_VP]),
@@ -95,6 +99,7 @@ SIGNATURES = {
     "mb2_server_stats": (C.c_int, [_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                    C.POINTER(C.c_uint64)]),
     "mb2_server_destroy": (C.c_int, [_VP]),
+    "mb2_server_set_ledger": (C.c_int, [_VP, _VP, _VP, _VP]),
     "mb2_probe_rates": (C.c_int, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "mb2_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),
     "mb2_autotune": (C.c_int, [_VP, C.c_uint32, _VP]),

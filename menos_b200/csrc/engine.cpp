@@ -1187,10 +1187,11 @@ int time_sweep(mb2_state* st, const std::vector<mb2_op>& ops, uint32_t tile, dou
 }
 
 // The time model's costs at one precision and tile width.  A pass takes
-//   fixed + amps * max(memory, sum over its blocks of compute),
-// memory and the fixed launch cost from an empty pass at n and n - 2 qubits,
-// compute from passes of many unfused blocks (compute-bound by construction):
-// a dense one-qubit block and a two-qubit diagonal block.
+//   fixed + amps * (memory + sum over its blocks of compute),
+// the fixed cost from a pass over a 14-qubit state, memory from a
+// near-empty pass at n qubits, compute from one pass each of many unfused
+// blocks, less its memory time: a dense one-qubit block and a two-qubit
+// diagonal block.
 // The state whose pass times the per-pass fixed cost (launch, ramp, tail).
 constexpr uint32_t kFixedCostQubits = 14;
 
@@ -1215,12 +1216,18 @@ int measure_costs(mb2_state* st, mb2_state* small, uint32_t m, double* fixed, do
     const double f = tes * 1e-3;
     *fixed = f;
     *pass = std::max(0.0, te * 1e-3 - f) / amps;
-    *dense1 = std::max(0.0, tu * 1e-3 - f) / (amps * static_cast<double>(u.ops.size()));
-    *diag = std::max(0.0, td * 1e-3 - f) / (amps * static_cast<double>(d.ops.size()));
+    // The probes' blocks each fit one pass: what they add to its memory time
+    // is their compute, per amplitude and block.
+    *dense1 = std::max(0.0, (tu * 1e-3 - f) / amps - *pass) / static_cast<double>(u.ops.size());
+    *diag = std::max(0.0, (td * 1e-3 - f) / amps - *pass) / static_cast<double>(d.ops.size());
     return MB2_OK;
 }
 
-// Seconds for one pass of blocks [b0, b1) over 2^n amplitudes.
+// Seconds for one pass of blocks [b0, b1) over 2^n amplitudes: the fixed
+// cost, the memory time and the blocks' compute, added -- a pass with dense
+// blocks is bound by FP64 latency at the resident warps, so its loads and
+// stores overlap its arithmetic only in part (measured: a 28-qubit brick pass
+// of 8 U3s takes about its DRAM time plus its FP64 time at the measured rate).
 double pass_seconds(const mb2_tuning& t, bool c64, const std::vector<mb2::Block>& blocks, size_t b0, size_t b1,
                     uint32_t n) {
     const double mem = c64 ? t.pass_s_per_amp_c64 : t.pass_s_per_amp;
@@ -1229,7 +1236,7 @@ double pass_seconds(const mb2_tuning& t, bool c64, const std::vector<mb2::Block>
     double compute = 0.0;
     for (size_t i = b0; i < b1; ++i)  // a dense k-qubit block sums 2^k terms per amplitude
         compute += blocks[i].diagonal ? diag : dense1 * static_cast<double>(uint64_t{1} << (blocks[i].k - 1));
-    return (c64 ? t.pass_s_fixed_c64 : t.pass_s_fixed) + std::max(mem, compute) * static_cast<double>(uint64_t{1} << n);
+    return (c64 ? t.pass_s_fixed_c64 : t.pass_s_fixed) + (mem + compute) * static_cast<double>(uint64_t{1} << n);
 }
 
 }  // namespace

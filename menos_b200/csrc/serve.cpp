@@ -88,26 +88,37 @@ struct mb2_server {
     uint32_t in_flight = 0;
     std::vector<std::thread> workers;
     std::vector<cudaStream_t> streams;
+    // The caller's memory ledger (mb2_server_set_ledger), or none.
+    mb2_ledger_charge_fn ledger_charge = nullptr;
+    mb2_ledger_release_fn ledger_release = nullptr;
+    void* ledger_user = nullptr;
 };
 
 namespace {
 
-// The oldest pending request that fits the remaining budget; none if the
-// oldest has waited past the starvation limit and does not fit.
+// Whether a request of `bytes` can be admitted now: it fits what is left of
+// the budget and the caller's ledger (if any) takes the bytes -- a charge
+// that succeeds is kept, so call this only for a request about to be admitted.
+bool admit(mb2_server* s, uint64_t bytes) {
+    if (s->held + bytes > s->budget) return false;
+    return s->ledger_charge == nullptr || s->ledger_charge(s->ledger_user, bytes) != 0;
+}
+
+// The oldest pending request that can be admitted; none if the oldest has
+// waited past the starvation limit and cannot be.
 bool pick(mb2_server* s, Request& out) {
     if (s->pending.empty()) return false;
-    const Request& head = s->pending.front();
-    const bool head_fits = s->held + head.bytes <= s->budget;
-    const double head_wait = std::chrono::duration<double>(Clock::now() - head.submitted).count();
-    for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
-        if (s->held + it->bytes <= s->budget) {
-            if (it != s->pending.begin() && !head_fits && head_wait > s->starvation_s) return false;
-            out = std::move(*it);
-            s->pending.erase(it);
-            s->held += out.bytes;
-            return true;
-        }
-    }
+    auto take = [&](std::deque<Request>::iterator it) {
+        out = std::move(*it);
+        s->pending.erase(it);
+        s->held += out.bytes;
+        return true;
+    };
+    if (admit(s, s->pending.front().bytes)) return take(s->pending.begin());
+    const double head_wait = std::chrono::duration<double>(Clock::now() - s->pending.front().submitted).count();
+    if (head_wait > s->starvation_s) return false;
+    for (auto it = s->pending.begin() + 1; it != s->pending.end(); ++it)
+        if (admit(s, it->bytes)) return take(it);
     return false;
 }
 
@@ -159,7 +170,13 @@ void worker(mb2_server* s, uint32_t slot) {
         Clock::time_point admitted;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv_work.wait(lk, [&] { return s->stop || pick(s, r); });
+            // With a ledger, memory can free up outside the server: look again
+            // every few milliseconds as well as on submits and completions.
+            auto ready = [&] { return s->stop || pick(s, r); };
+            if (s->ledger_charge == nullptr) s->cv_work.wait(lk, ready);
+            else
+                while (!s->cv_work.wait_for(lk, std::chrono::milliseconds(4), ready)) {
+                }
             if (r.ticket == 0) return;  // stopped with nothing picked
             admitted = Clock::now();
             ++s->in_flight;
@@ -173,6 +190,7 @@ void worker(mb2_server* s, uint32_t slot) {
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->held -= r.bytes;
+            if (s->ledger_release != nullptr) s->ledger_release(s->ledger_user, r.bytes);
             --s->in_flight;
             s->done.push_back(std::move(d));
         }
@@ -282,6 +300,16 @@ int mb2_server_poll(mb2_server* s, mb2_completion* out, uint32_t capacity, uint3
         out[(*count)++] = kept.c;
     }
     return *count > 0 ? MB2_OK : MB2_ERR_TIMEOUT;
+}
+
+int mb2_server_set_ledger(mb2_server* s, mb2_ledger_charge_fn charge, mb2_ledger_release_fn release, void* user) {
+    if (s == nullptr || (charge == nullptr) != (release == nullptr)) return MB2_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->in_flight != 0) return MB2_ERR_INVALID;  // charges already taken would be released elsewhere
+    s->ledger_charge = charge;
+    s->ledger_release = release;
+    s->ledger_user = user;
+    return MB2_OK;
 }
 
 int mb2_server_release(mb2_server* s, uint64_t ticket) {

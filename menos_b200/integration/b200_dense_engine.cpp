@@ -32,6 +32,7 @@
 #include <variant>
 #include <vector>
 
+#include "b200_dense_engine.h"
 #include "common/error.h"
 #include "common/memory_ledger.h"
 #include "common/rng.h"
@@ -439,6 +440,23 @@ private:
 const SimulationEngine& b200_dense_engine() {
     static const B200DenseEngine engine;
     return engine;
+}
+
+int ServerLedger::attach(mb2_server* server) { return mb2_server_set_ledger(server, &charge, &release, this); }
+
+// Called by the server with its lock held, one call at a time.
+int ServerLedger::charge(void* user, uint64_t bytes) {
+    auto* self = static_cast<ServerLedger*>(user);
+    if (self->limit_ != 0 && self->ledger_.live_device_bytes() + bytes > self->limit_) return 0;
+    const common::MemoryLedger::Scope scope(self->ledger_);
+    self->live_.emplace(bytes, common::MemoryLedger::Charge(bytes, common::MemoryLedger::Space::Device));
+    return 1;
+}
+
+void ServerLedger::release(void* user, uint64_t bytes) {
+    auto* self = static_cast<ServerLedger*>(user);
+    const auto it = self->live_.find(bytes);
+    if (it != self->live_.end()) self->live_.erase(it);
 }
 
 }  // namespace menos::engines::dense_b200

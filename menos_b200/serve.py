@@ -67,6 +67,16 @@ class Server:
             check(rc, self.ctx.h, "mb2_server_poll")
         return out
 
+    def set_ledger(self, charge, release) -> None:
+        """Admission through a memory ledger: charge(bytes) -> bool is asked
+        before a request is admitted (False keeps it pending), release(bytes)
+        is called when its memory is freed.  Both run on server threads."""
+        self._ledger = (_lib.LEDGER_CHARGE(lambda _u, b: 1 if charge(int(b)) else 0),
+                        _lib.LEDGER_RELEASE(lambda _u, b: release(int(b))))
+        check(lib().mb2_server_set_ledger(self.h, C.cast(self._ledger[0], C.c_void_p),
+                                          C.cast(self._ledger[1], C.c_void_p), None),
+              self.ctx.h, "mb2_server_set_ledger")
+
     def stats(self):
         p, f, hb, bb = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
         lib().mb2_server_stats(self.h, C.byref(p), C.byref(f), C.byref(hb), C.byref(bb))

@@ -15,6 +15,8 @@
 //                    Factorized region's sampler is drawn from with its own Rng
 //   ah_estimate      EngineEstimateRequest through either engine
 //   ah_calibration   measure_b200_calibration()
+//   ah_serve_with_ledger  the serving loop admitting through the adapter's
+//                    ServerLedger (device bytes charged to a MemoryLedger)
 #include <chrono>
 #include <complex>
 #include <cstdint>
@@ -37,10 +39,7 @@
 
 #include "../include/mb2.h"
 
-namespace menos::engines::dense_b200 {
-const SimulationEngine& b200_dense_engine();
-plan::CudaCalibration measure_b200_calibration();
-}  // namespace menos::engines::dense_b200
+#include "../menos_b200/integration/b200_dense_engine.h"
 
 namespace {
 
@@ -273,6 +272,89 @@ int ah_calibration(double* out) {
     out[6] = c.execution_seconds;
     out[7] = c.device_work_units_per_second;
     return 0;
+}
+
+// The serving loop with its admissions charged to a MemoryLedger through the
+// adapter's ServerLedger: `count` requests (brick circuits of qubits[i]
+// qubits, depth 8, <Z_0> each) on a server of `slots` slots; the ledger
+// refuses beyond `device_limit`.  out: peak device bytes, live device bytes
+// after the last completion, completions with status 0, the largest single
+// admission's bytes (the server's own count).
+int ah_serve_with_ledger(const std::uint32_t* qubits, std::uint32_t count, std::uint32_t slots,
+                         std::uint64_t device_limit, std::uint64_t* out) {
+    mb2_context* ctx = nullptr;
+    if (mb2_context_create(0, &ctx) != MB2_OK) return -1;
+    menos::common::MemoryLedger ledger;
+    int rc = 0;
+    {
+        menos::engines::dense_b200::ServerLedger hook(ledger, device_limit);
+        mb2_server* srv = nullptr;
+        mb2_server_options so{0, slots, 0};
+        if (mb2_server_create(ctx, &so, &srv) != MB2_OK) {
+            mb2_context_destroy(ctx);
+            return -2;
+        }
+        if (hook.attach(srv) != MB2_OK) rc = -3;
+        std::vector<std::vector<mb2_op>> programs(count);
+        const std::uint64_t z0 = 1, x0 = 0;
+        const double one = 1.0;
+        std::uint64_t ok = 0;
+        for (std::uint32_t i = 0; i < count && rc == 0; ++i) {
+            const std::uint32_t n = qubits[i];
+            for (std::uint32_t layer = 0; layer < 8; ++layer) {
+                for (std::uint32_t q = 0; q < n; ++q) {
+                    mb2_op o{};
+                    o.opcode = MB2_U;
+                    o.num_qubits = 1;
+                    o.qubits[0] = q;
+                    o.params[0] = 0.1 * (q + 1) + layer;
+                    o.params[1] = 0.2 * q;
+                    o.params[2] = 0.3 * layer;
+                    programs[i].push_back(o);
+                }
+                for (std::uint32_t q = layer & 1u; q + 1 < n; q += 2) {
+                    mb2_op o{};
+                    o.opcode = MB2_CZ;
+                    o.num_qubits = 2;
+                    o.qubits[0] = q;
+                    o.qubits[1] = q + 1;
+                    programs[i].push_back(o);
+                }
+            }
+            mb2_request rq{};
+            rq.ops = programs[i].data();
+            rq.num_ops = static_cast<std::uint32_t>(programs[i].size());
+            rq.num_qubits = n;
+            rq.fuse_gates = 1;
+            rq.output = MB2_OUT_EXPECTATION;
+            rq.num_terms = 1;
+            rq.x_masks = &x0;
+            rq.z_masks = &z0;
+            rq.coefs = &one;
+            rq.precision = MB2_C128;
+            std::uint64_t ticket = 0;
+            if (mb2_server_submit(srv, &rq, &ticket) != MB2_OK) rc = -4;
+        }
+        std::uint32_t got_total = 0;
+        for (int spins = 0; got_total < count && rc == 0 && spins < 6000; ++spins) {
+            mb2_completion done[16];
+            std::uint32_t got = 0;
+            const int prc = mb2_server_poll(srv, done, 16, &got, 100);
+            if (prc != MB2_OK && prc != MB2_ERR_TIMEOUT) rc = -5;
+            for (std::uint32_t k = 0; k < got; ++k) {
+                if (done[k].status == MB2_OK) ++ok;
+                mb2_server_release(srv, done[k].ticket);
+            }
+            got_total += got;
+        }
+        mb2_server_destroy(srv);
+        out[0] = ledger.peak_device_bytes();
+        out[1] = ledger.live_device_bytes();
+        out[2] = ok;
+        out[3] = got_total;
+    }
+    mb2_context_destroy(ctx);
+    return rc;
 }
 
 }  // extern "C"

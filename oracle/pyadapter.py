@@ -52,6 +52,8 @@ class AdapterHarness:
         self.L.ah_estimate.argtypes = [C.c_int, C.POINTER(_Request), C.c_void_p, C.c_char_p, C.c_size_t]
         self.L.ah_calibration.restype = C.c_int
         self.L.ah_calibration.argtypes = [C.c_void_p]
+        self.L.ah_serve_with_ledger.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64, C.c_void_p]
+        self.L.ah_serve_with_ledger.restype = C.c_int
 
     def _request(self, circ, keep, *, fuse=True, statevector=False, shots=0, seed=0, targets=(), width=None,
                  sole=True, paulis=(), global_phase=None, budget=1 << 40, abandon_at=-1):
@@ -137,6 +139,14 @@ class AdapterHarness:
         d["feasible"] = bool(d["feasible"])
         d["reason"] = reason.value.decode(errors="replace")
         return d
+
+    def serve_with_ledger(self, qubits, slots, device_limit) -> dict:
+        """The serving loop admitting through the adapter's ServerLedger."""
+        q = np.ascontiguousarray(qubits, np.uint32)
+        out = np.zeros(4, np.uint64)
+        rc = self.L.ah_serve_with_ledger(q.ctypes.data, len(q), slots, device_limit, out.ctypes.data)
+        assert rc == 0, rc
+        return dict(zip(["peak_device_bytes", "live_device_bytes", "ok", "completed"], (int(v) for v in out)))
 
     def calibration(self) -> dict:
         out = np.zeros(8, np.float64)

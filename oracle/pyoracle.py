@@ -20,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmenos_ref.so")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libmenos_ref_cuda.so")
 
 # Opcodes: the reference's menos::Opcode order (include/menos/circuit.h:17-41).
 OPCODES = ["x", "y", "z", "h", "s", "sdg", "t", "tdg", "sx", "sxdg", "rx", "ry", "rz", "p",
@@ -242,6 +243,9 @@ class RefLib:
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                     C.c_void_p, C.c_void_p]
         L.ref_run_dense.restype = C.c_int
+        if hasattr(L, "ref_run_cuda"):  # the library with the reference's CUDA engine
+            L.ref_run_cuda.argtypes = L.ref_run_dense.argtypes
+            L.ref_run_cuda.restype = C.c_int
         L.ref_run_plan.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_double, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
         L.ref_run_plan.restype = C.c_int
@@ -312,8 +316,11 @@ class RefLib:
         return out[:2 * dim * dim].view(np.complex128).reshape(dim, dim).copy()
 
     def run(self, circ: Circuit, fuse_gates=True, threads=0, statevector=True, shots=0, seed=0, targets=(),
-            width=None, paulis=(), timing=False):
-        """DenseEngine::execute; returns dict(statevector, counts, terms, seconds)."""
+            width=None, paulis=(), timing=False, engine="cpu"):
+        """DenseEngine::execute (engine="cpu") or CudaDenseEngine::execute
+        (engine="cuda", a RefLib on REF_CUDA_SO); returns dict(statevector,
+        counts, terms, seconds)."""
+        run_fn = self.L.ref_run_cuda if engine == "cuda" else self.L.ref_run_dense
         arr, keep = ops_struct_array(circ)
         n = circ.num_qubits
         sv = np.zeros(1 << n, np.complex128) if statevector else None
@@ -328,7 +335,7 @@ class RefLib:
         zs = np.array([p[1] for p in paulis] or [0], np.uint64)
         terms = np.zeros(2 * max(len(paulis), 1), np.float64)
         secs = np.zeros(1, np.float64)
-        rc = self.L.ref_run_dense(
+        rc = run_fn(
             n, C.addressof(arr), len(circ.ops), circ.global_phase, 1 if fuse_gates else 0, threads,
             sv.ctypes.data if sv is not None else None, shots, seed, t.ctypes.data if len(t) else None,
             len(t) // 2, width, outc.ctypes.data if shots else None, cnt.ctypes.data, nout.ctypes.data,

@@ -32,6 +32,9 @@
 #include "engines/dense/apply_matrix.h"
 #include "engines/density_matrix/density_matrix_engine.h"
 #include "engines/dense/dense_engine.h"
+#ifdef MENOS_REF_CUDA
+#include "engines/dense_cuda/cuda_dense_engine.h"
+#endif
 #include "engines/dense/fused_block.h"
 #include "engines/dense/sample.h"
 #include "ir/fuse_gates.h"
@@ -231,14 +234,16 @@ int ref_fused_block_matrix(const mb2_op* ops, std::uint32_t n_ops, std::uint32_t
 // non-null: statevector (2 * 2^n doubles), counts (outcomes/counts with
 // capacity *n_outcomes, updated), expectation terms (2 * n_terms doubles).
 // seconds_out (optional) receives the wall time of execute() alone.
-int ref_run_dense(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_ops,
-                  double global_phase, int fuse_gates, std::uint32_t threads,
-                  double* statevector, std::uint64_t shots, std::uint64_t seed,
-                  const std::uint32_t* targets, std::uint32_t n_targets, std::uint32_t width,
-                  std::uint64_t* out_outcomes, std::uint64_t* out_counts,
-                  std::uint64_t* n_outcomes, const std::uint64_t* x_masks,
-                  const std::uint64_t* z_masks, std::uint32_t n_terms, double* terms_out,
-                  double* seconds_out) {
+}  // extern "C"
+
+namespace {
+
+int run_engine(const menos::SimulationEngine& engine, std::uint32_t num_qubits, const mb2_op* ops,
+               std::uint32_t n_ops, double global_phase, int fuse_gates, std::uint32_t threads,
+               double* statevector, std::uint64_t shots, std::uint64_t seed, const std::uint32_t* targets,
+               std::uint32_t n_targets, std::uint32_t width, std::uint64_t* out_outcomes,
+               std::uint64_t* out_counts, std::uint64_t* n_outcomes, const std::uint64_t* x_masks,
+               const std::uint64_t* z_masks, std::uint32_t n_terms, double* terms_out, double* seconds_out) {
     try {
         std::vector<menos::Operation> v;
         v.reserve(n_ops);
@@ -270,7 +275,6 @@ int ref_run_dense(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_o
         req.observable = req.want_expectation ? &obs : nullptr;
         req.max_threads = threads == 0 ? menos::common::default_thread_count() : threads;
         req.fuse_gates = fuse_gates != 0;
-        menos::engines::dense::DenseEngine engine;
         const auto t0 = std::chrono::steady_clock::now();
         menos::EngineExecutionResult res = engine.execute(req);
         const auto t1 = std::chrono::steady_clock::now();
@@ -305,6 +309,44 @@ int ref_run_dense(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_o
         return -1;
     }
 }
+
+}  // namespace
+
+extern "C" {
+
+int ref_run_dense(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_ops,
+                  double global_phase, int fuse_gates, std::uint32_t threads,
+                  double* statevector, std::uint64_t shots, std::uint64_t seed,
+                  const std::uint32_t* targets, std::uint32_t n_targets, std::uint32_t width,
+                  std::uint64_t* out_outcomes, std::uint64_t* out_counts,
+                  std::uint64_t* n_outcomes, const std::uint64_t* x_masks,
+                  const std::uint64_t* z_masks, std::uint32_t n_terms, double* terms_out,
+                  double* seconds_out) {
+    const menos::engines::dense::DenseEngine engine;
+    return run_engine(engine, num_qubits, ops, n_ops, global_phase, fuse_gates, threads, statevector, shots, seed,
+                      targets, n_targets, width, out_outcomes, out_counts, n_outcomes, x_masks, z_masks, n_terms,
+                      terms_out, seconds_out);
+}
+
+#ifdef MENOS_REF_CUDA
+// CudaDenseEngine::execute (src/engines/dense_cuda/cuda_dense_engine.cpp:
+// 325-412) on the same request; arguments as ref_run_dense's.
+int ref_run_cuda(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_ops, double global_phase,
+                 int fuse_gates, std::uint32_t threads, double* statevector, std::uint64_t shots,
+                 std::uint64_t seed, const std::uint32_t* targets, std::uint32_t n_targets, std::uint32_t width,
+                 std::uint64_t* out_outcomes, std::uint64_t* out_counts, std::uint64_t* n_outcomes,
+                 const std::uint64_t* x_masks, const std::uint64_t* z_masks, std::uint32_t n_terms,
+                 double* terms_out, double* seconds_out) {
+    if (!menos::engines::dense_cuda::cuda_device_available()) {
+        g_error = "no CUDA device";
+        return -1;
+    }
+    const menos::engines::dense_cuda::CudaDenseEngine engine;
+    return run_engine(engine, num_qubits, ops, n_ops, global_phase, fuse_gates, threads, statevector, shots, seed,
+                      targets, n_targets, width, out_outcomes, out_counts, n_outcomes, x_masks, z_masks, n_terms,
+                      terms_out, seconds_out);
+}
+#endif
 
 // DensityMatrixEngine::execute on ops (src/engines/density_matrix/
 // density_matrix_engine.cpp): counts (capacity *n_outcomes, updated) and

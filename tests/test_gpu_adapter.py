@@ -204,3 +204,17 @@ def test_estimate_and_calibration_feed_the_time_model(harness):
         run = harness.execute(pyadapter.B200, circ, paulis=paulis)
         assert run["rc"] == 0, run["error"]
         assert 0.5 <= priced / run["seconds"] <= 2.0, (priced, run["seconds"])
+
+
+def test_serving_admissions_charge_the_memory_ledger(harness):
+    """The serving loop admits through the adapter's ServerLedger: every
+    request's device bytes are charged to the MemoryLedger while it runs
+    (Space::Device), the ledger's limit holds admission back, and every
+    charge is released at the end."""
+    qubits = [22] * 6 + [18] * 10 + [20] * 6
+    state22 = 16 << 22
+    limit = 3 * state22  # room for about two 22-qubit requests with their staging
+    r = harness.serve_with_ledger(qubits, 8, limit)
+    assert r["completed"] == len(qubits) and r["ok"] == len(qubits)
+    assert state22 < r["peak_device_bytes"] <= limit
+    assert r["live_device_bytes"] == 0

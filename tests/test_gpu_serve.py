@@ -164,3 +164,45 @@ print("BAD", bad)
     out = subprocess.run([sys.executable, "-c", code, root], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     assert "BAD 0" in out.stdout, out.stdout + out.stderr[-2000:]
+
+
+def test_admission_through_a_caller_ledger(ctx):
+    """mb2_server_set_ledger: a request is admitted only when the caller's
+    ledger takes its bytes; the bytes come back when it completes, so the
+    ledger's live total never passes its limit and ends at zero."""
+    import threading
+    from menos_b200 import workloads
+    from menos_b200.serve import Server
+    lock = threading.Lock()
+    book = {"live": 0, "peak": 0, "charges": 0, "refusals": 0}
+    limit = 3 * (16 << 20)  # about two 20-qubit states with staging
+
+    def charge(b):
+        with lock:
+            if book["live"] + b > limit:
+                book["refusals"] += 1
+                return False
+            book["live"] += b
+            book["charges"] += 1
+            book["peak"] = max(book["peak"], book["live"])
+            return True
+
+    def release(b):
+        with lock:
+            book["live"] -= b
+
+    srv = Server(ctx, 8 << 30, 8)
+    srv.set_ledger(charge, release)
+    n_req = 12
+    for i in range(n_req):
+        c = workloads.brick(20 if i % 2 else 16, 6, 100 + i)
+        srv.submit(c, "expectation", paulis=[(0, 1)], coefs=[1.0])
+    done = []
+    for _ in range(600):
+        done += srv.poll(100)
+        if len(done) == n_req:
+            break
+    srv.close()
+    assert len(done) == n_req and all(d["status"] == 0 for d in done)
+    assert book["charges"] == n_req and book["live"] == 0
+    assert 0 < book["peak"] <= limit
