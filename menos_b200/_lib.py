@@ -17,6 +17,7 @@ MB2_OK = 0
 ERRORS = {1: "invalid argument", 2: "resource exceeded", 3: "CUDA error", 4: "no sm_100 device",
           5: "timeout", 6: "unsupported", 7: "abandoned"}
 C128, C64 = 0, 1
+BATCH_MAX_TERMS = 64  # MB2_BATCH_MAX_TERMS
 
 
 class SweepOptions(C.Structure):
