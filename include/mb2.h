@@ -266,6 +266,32 @@ int mb2_dm_expectation(mb2_state* rho, uint32_t num_qubits, const uint64_t* x_ma
 int mb2_dm_sample(mb2_state* rho, uint32_t num_qubits, uint64_t shots, uint64_t seed, const uint32_t* targets,
                   uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes);
 
+/* The reference's sequential FP64 sum of |a_i|^2 over the state, bit for bit
+ * (the exact device chain of mb2_sample), e.g. to renormalise as the
+ * reference does (src/engines/trajectory/trajectory_engine.cpp:155-166). */
+int mb2_norm_exact(mb2_state* state, double* out);
+
+/* The reference's trajectory engine (src/engines/trajectory/
+ * trajectory_engine.cpp:424-494) on the device: `trajectories` pure-state
+ * runs of the n-qubit circuit, trajectory t drawing from a common::Rng seeded
+ * with SplitMix64 output t + 1 of `seed`.  Gates apply op by op; a channel
+ * (MB2_CHANNEL, 1..3 qubits) draws one uniform, picks the first Kraus
+ * operator whose cumulative Re Tr(K^dagger K rho_q) exceeds it (rho_q, the
+ * reduced density matrix, from the 4^k Pauli expectations on its qubits),
+ * applies it and renormalises by the exact sequential norm -- so each
+ * trajectory's state is bitwise the reference's whenever its branches are
+ * (they are unless a uniform falls within rounding of a branch boundary).
+ * Expectation (num_terms > 0; coefs: complex, 2 doubles each): term_means
+ * (2 * num_terms doubles, the mean of <P_t> over trajectories) and the
+ * standard error of sum_t coef_t <P_t>.  Counts (shots <= trajectories): one
+ * draw per trajectory t < shots, after its channel draws, by the exact walk;
+ * outcomes as mb2_sample's.  Readout errors are not carried. */
+int mb2_trajectories(mb2_context* ctx, uint32_t num_qubits, const mb2_op* ops, uint32_t num_ops,
+                     uint64_t trajectories, uint64_t seed, const uint64_t* x_masks, const uint64_t* z_masks,
+                     const double* coefs, uint32_t num_terms, double* term_means, double* standard_error,
+                     uint64_t shots, const uint32_t* targets, uint32_t num_targets, uint64_t* outcomes,
+                     uint64_t* counts, uint64_t* num_outcomes);
+
 /* ---- batched parameter sweep ------------------------------------------- */
 /* One circuit structure under many parameter bindings, in one device job:
  * every binding's state lives in one buffer (binding b at b * 2^n), the

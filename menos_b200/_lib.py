@@ -126,6 +126,10 @@ SIGNATURES = {
     "mb2_norm": (C.c_int, [_VP, C.POINTER(C.c_double)]),
     "mb2_normalize": (C.c_int, [_VP, C.POINTER(C.c_double)]),
     "mb2_sample": (C.c_int, [_VP, C.c_uint64, C.c_uint64, _VP, C.c_uint32, _VP, _VP, C.POINTER(C.c_uint64)]),
+    "mb2_norm_exact": (C.c_int, [_VP, C.POINTER(C.c_double)]),
+    "mb2_trajectories": (C.c_int, [_VP, C.c_uint32, _VP, C.c_uint32, C.c_uint64, C.c_uint64, _VP, _VP, _VP,
+                                   C.c_uint32, _VP, C.POINTER(C.c_double), C.c_uint64, _VP, C.c_uint32, _VP, _VP,
+                                   C.POINTER(C.c_uint64)]),
     "mb2_dm_apply_program": (C.c_int, [_VP, C.c_uint32, _VP, C.c_uint32]),
     "mb2_dm_expectation": (C.c_int, [_VP, C.c_uint32, _VP, _VP, C.c_uint32, _VP]),
     "mb2_dm_sample": (C.c_int, [_VP, C.c_uint32, C.c_uint64, C.c_uint64, _VP, C.c_uint32, _VP, _VP,

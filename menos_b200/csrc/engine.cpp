@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <bit>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -969,6 +970,232 @@ int mb2_dm_sample(mb2_state* rho, uint32_t n, uint64_t shots, uint64_t seed, con
     MB2_CUDA(rho->ctx, cudaMemcpyAsync(basis.data(), base + al_u, shots * 8, cudaMemcpyDeviceToHost, rho->stream));
     MB2_CUDA(rho->ctx, cudaStreamSynchronize(rho->stream));
     return histogram(rho, n, basis, targets, num_targets, outcomes, counts, num_outcomes);
+}
+
+int mb2_norm_exact(mb2_state* s, double* out) {
+    if (s == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    if (int e = ensure_scratch(s, mb2::sample_scratch_bytes(s->n, 0)); e != MB2_OK) return e;
+    const int rc = mb2::launch_exact_norm(s->amps, s->n, s->scratch, out, s->stream, s->precision);
+    if (rc != MB2_OK) return fail(s->ctx, rc, std::string("exact norm: ") + mb2::last_cuda_error_string());
+    return MB2_OK;
+}
+
+// ---- trajectories ----------------------------------------------------------
+// The reference's trajectory engine (src/engines/trajectory/
+// trajectory_engine.cpp:205-241,424-494) on the device.
+
+}  // extern "C"
+
+namespace {
+
+// SplitMix64 output t + 1 of the stream seeded with base_seed: the
+// trajectory's seed (trajectory_engine.cpp:319-323, src/common/splitmix64.h).
+uint64_t trajectory_seed(uint64_t base_seed, uint64_t t) {
+    uint64_t z = base_seed + t * 0x9E3779B97F4A7C15ULL + 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+double word_to_uniform(uint64_t w) { return static_cast<double>(w >> 11) * 0x1.0p-53; }
+
+struct TrajChannel {
+    std::vector<uint32_t> qubits;
+    std::vector<std::vector<mb2::Cd>> kraus;     // each dim x dim, row-major
+    std::vector<std::vector<mb2::Cd>> products;  // K^dagger K, as the reference forms them
+    std::vector<uint64_t> xs, zs;                // the 4^k Pauli strings on the channel's qubits
+};
+
+// K^dagger K (kraus_products, trajectory_engine.cpp:50-69).
+std::vector<mb2::Cd> kraus_product(const std::vector<mb2::Cd>& k, size_t dim) {
+    std::vector<mb2::Cd> m(dim * dim, mb2::Cd{0.0, 0.0});
+    for (size_t a = 0; a < dim; ++a)
+        for (size_t b = 0; b < dim; ++b) {
+            mb2::Cd sum{0.0, 0.0};
+            for (size_t r = 0; r < dim; ++r) sum += std::conj(k[r * dim + a]) * k[r * dim + b];
+            m[a * dim + b] = sum;
+        }
+    return m;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t num_ops, uint64_t trajectories,
+                     uint64_t seed, const uint64_t* x_masks, const uint64_t* z_masks, const double* coefs,
+                     uint32_t num_terms, double* term_means, double* standard_error, uint64_t shots,
+                     const uint32_t* targets, uint32_t num_targets, uint64_t* outcomes, uint64_t* counts,
+                     uint64_t* num_outcomes) {
+    if (ctx == nullptr || n < 1 || n > 34 || (ops == nullptr && num_ops != 0) || trajectories == 0)
+        return MB2_ERR_INVALID;
+    const bool want_exp = num_terms != 0;
+    const bool want_counts = shots != 0;
+    if (want_exp && (x_masks == nullptr || z_masks == nullptr || coefs == nullptr || term_means == nullptr))
+        return MB2_ERR_INVALID;
+    if (want_exp && trajectories < 2) return fail(ctx, MB2_ERR_INVALID, "an expectation needs at least 2 trajectories");
+    if (want_counts && (shots > trajectories || num_outcomes == nullptr || outcomes == nullptr || counts == nullptr))
+        return fail(ctx, MB2_ERR_INVALID, "more shots than trajectories");
+    for (uint32_t t = 0; t < num_targets; ++t)
+        if (targets[2 * t] >= n || targets[2 * t + 1] >= 64) return fail(ctx, MB2_ERR_INVALID, "measure target out of range");
+    // Segments: runs of gates (applied op by op, as the reference's
+    // apply_matrix per operation) and channels.
+    std::vector<std::vector<mb2_op>> gate_runs;
+    std::vector<TrajChannel> channels;
+    std::vector<std::pair<int, size_t>> steps;  // (0: gate run, 1: channel), index
+    try {
+        for (uint32_t i = 0; i < num_ops; ++i) {
+            const mb2_op& op = ops[i];
+            if (op.opcode == MB2_MEASURE) continue;
+            if (op.opcode != MB2_CHANNEL) {
+                if (steps.empty() || steps.back().first != 0) {
+                    steps.emplace_back(0, gate_runs.size());
+                    gate_runs.emplace_back();
+                }
+                gate_runs.back().push_back(op);
+                continue;
+            }
+            const uint32_t k = op.num_qubits;
+            if (k == 0 || k > 3 || op.matrix == nullptr || op.reserved == 0)
+                return fail(ctx, MB2_ERR_INVALID, "operation " + std::to_string(i) + ": channel of 1..3 qubits with Kraus operators");
+            const size_t dim = size_t{1} << k;
+            TrajChannel ch;
+            ch.qubits.assign(op.qubits, op.qubits + k);
+            for (uint32_t q : ch.qubits)
+                if (q >= n) return fail(ctx, MB2_ERR_INVALID, "operand out of range");
+            for (uint32_t t = 0; t < op.reserved; ++t) {
+                std::vector<mb2::Cd> km(dim * dim);
+                for (size_t e = 0; e < dim * dim; ++e)
+                    km[e] = mb2::Cd{op.matrix[2 * (t * dim * dim + e)], op.matrix[2 * (t * dim * dim + e) + 1]};
+                ch.products.push_back(kraus_product(km, dim));
+                ch.kraus.push_back(std::move(km));
+            }
+            for (uint64_t lx = 0; lx < dim; ++lx)
+                for (uint64_t lz = 0; lz < dim; ++lz) {
+                    uint64_t gx = 0, gz = 0;
+                    for (uint32_t j = 0; j < k; ++j) {
+                        if ((lx >> j) & 1u) gx |= uint64_t{1} << ch.qubits[j];
+                        if ((lz >> j) & 1u) gz |= uint64_t{1} << ch.qubits[j];
+                    }
+                    ch.xs.push_back(gx);
+                    ch.zs.push_back(gz);
+                }
+            steps.emplace_back(1, channels.size());
+            channels.push_back(std::move(ch));
+        }
+    } catch (const std::exception& e) {
+        return fail(ctx, MB2_ERR_INVALID, e.what());
+    }
+    mb2_state* st = nullptr;
+    if (int e = mb2_state_alloc(ctx, n, MB2_C128, ~uint64_t{0}, &st); e != MB2_OK) return e;
+    struct Free {
+        mb2_state* s;
+        ~Free() { mb2_state_free(s); }
+    } guard{st};
+    const mb2_sweep_options one_by_one{0, 0, 0, 0, 0, 0};
+    std::vector<mb2::Cd> term_sums(num_terms, mb2::Cd{0.0, 0.0});
+    std::vector<double> vals(2 * std::max<uint32_t>(num_terms, 1));
+    uint64_t count = 0;  // Welford (trajectory_engine.cpp:244-265)
+    mb2::Cd mean{0.0, 0.0};
+    double ssd = 0.0;
+    std::vector<uint64_t> shot_basis;
+    for (uint64_t t = 0; t < trajectories; ++t) {
+        std::mt19937_64 rng(trajectory_seed(seed, t));
+        if (int e = mb2_init(st, 0.0); e != MB2_OK) return e;  // |0..0>, no global phase
+        for (const auto& [kind, idx] : steps) {
+            if (kind == 0) {
+                const std::vector<mb2_op>& run = gate_runs[idx];
+                if (int e = mb2_apply_program(st, run.data(), static_cast<uint32_t>(run.size()), &one_by_one); e != MB2_OK)
+                    return e;
+                continue;
+            }
+            const TrajChannel& ch = channels[idx];
+            const uint32_t k = static_cast<uint32_t>(ch.qubits.size());
+            const size_t dim = size_t{1} << k;
+            // rho_q from its Pauli expectations: rho = 2^-k sum_P <P> P,
+            // P = i^{|x&z|} X^x Z^z in the channel's local basis.
+            std::vector<double> pv(2 * ch.xs.size());
+            if (int e = mb2_expectation(st, ch.xs.data(), ch.zs.data(), static_cast<uint32_t>(ch.xs.size()), pv.data());
+                e != MB2_OK)
+                return e;
+            std::vector<mb2::Cd> rho(dim * dim, mb2::Cd{0.0, 0.0});
+            const mb2::Cd ipow[4] = {{1.0, 0.0}, {0.0, 1.0}, {-1.0, 0.0}, {0.0, -1.0}};
+            size_t pi = 0;
+            for (uint64_t lx = 0; lx < dim; ++lx)
+                for (uint64_t lz = 0; lz < dim; ++lz, ++pi) {
+                    const mb2::Cd v{pv[2 * pi], pv[2 * pi + 1]};
+                    const mb2::Cd ph = ipow[std::popcount(lx & lz) & 3];
+                    for (uint64_t c = 0; c < dim; ++c) {
+                        const double sgn = (std::popcount(c & lz) & 1) ? -1.0 : 1.0;
+                        rho[(c ^ lx) * dim + c] += v * ph * sgn;
+                    }
+                }
+            for (mb2::Cd& r : rho) r /= static_cast<double>(dim);
+            // The branch: the first with cumulative p_i = Re Tr(M_i rho) above
+            // u, else the last with p_i > 0 (choose_branch, :123-152).
+            const double u = word_to_uniform(rng());
+            double cumulative = 0.0;
+            int64_t branch = -1, last_positive = -1;
+            for (size_t b = 0; b < ch.products.size() && branch < 0; ++b) {
+                double p = 0.0;
+                for (size_t a = 0; a < dim; ++a)
+                    for (size_t c = 0; c < dim; ++c) p += (ch.products[b][a * dim + c] * rho[c * dim + a]).real();
+                if (p > 0.0) {
+                    last_positive = static_cast<int64_t>(b);
+                    cumulative += p;
+                    if (u < cumulative) branch = static_cast<int64_t>(b);
+                }
+            }
+            if (branch < 0) branch = last_positive;
+            if (branch < 0) return fail(ctx, MB2_ERR_INVALID, "every Kraus branch has probability 0");
+            const std::vector<mb2::Cd>& km = ch.kraus[static_cast<size_t>(branch)];
+            if (int e = mb2_apply_matrix(st, reinterpret_cast<const double*>(km.data()), ch.qubits.data(), k); e != MB2_OK)
+                return e;
+            // psi /= ||psi|| with the reference's sequential norm (renormalize, :155-166).
+            double norm_sq = 0.0;
+            if (int e = mb2_norm_exact(st, &norm_sq); e != MB2_OK) return e;
+            if (!(norm_sq > 0.0)) return fail(ctx, MB2_ERR_INVALID, "a chosen Kraus branch annihilated the state");
+            const double scale = 1.0 / std::sqrt(norm_sq);
+            const double sm[8] = {scale, 0.0, 0.0, 0.0, 0.0, 0.0, scale, 0.0};
+            const uint32_t q0 = 0;
+            if (int e = mb2_apply_matrix(st, sm, &q0, 1); e != MB2_OK) return e;
+        }
+        if (want_exp) {
+            if (int e = mb2_expectation(st, x_masks, z_masks, num_terms, vals.data()); e != MB2_OK) return e;
+            mb2::Cd x{0.0, 0.0};
+            for (uint32_t i = 0; i < num_terms; ++i) {
+                const mb2::Cd v{vals[2 * i], vals[2 * i + 1]};
+                term_sums[i] += v;
+                x += mb2::Cd{coefs[2 * i], coefs[2 * i + 1]} * v;
+            }
+            ++count;
+            const mb2::Cd delta = x - mean;
+            mean += delta / static_cast<double>(count);
+            ssd += (std::conj(delta) * (x - mean)).real();
+        }
+        if (want_counts && t < shots) {
+            const double u = word_to_uniform(rng());
+            uint64_t b = 0;
+            if (int e = mb2_sample_basis(st, &u, 1, &b); e != MB2_OK) return e;
+            shot_basis.push_back(b);
+        }
+    }
+    if (want_exp) {
+        for (uint32_t i = 0; i < num_terms; ++i) {
+            term_sums[i] /= static_cast<double>(trajectories);
+            term_means[2 * i] = term_sums[i].real();
+            term_means[2 * i + 1] = term_sums[i].imag();
+        }
+        if (standard_error != nullptr) {
+            const double cnt = static_cast<double>(count);
+            *standard_error = std::sqrt(ssd / (cnt - 1.0) / cnt);
+        }
+    }
+    if (want_counts) {
+        std::sort(shot_basis.begin(), shot_basis.end());
+        return histogram(st, n, shot_basis, targets, num_targets, outcomes, counts, num_outcomes);
+    }
+    return MB2_OK;
 }
 
 int mb2_copy_out(mb2_state* s, void* host, uint64_t num_amplitudes) {

@@ -520,6 +520,56 @@ int launch_sample_t(const void* amps, uint32_t n, const double* dev_uniforms_sor
     return launch_status();
 }
 
+// The exact chain alone (steps A-D): the reference's sequential sum of
+// |a_i|^2 over the whole state is its final value, cstart[nchunks].
+template <typename A>
+int launch_exact_norm_t(const void* amps, uint32_t n, void* scratch, double* host_total, void* stream) {
+    const auto s = static_cast<cudaStream_t>(stream);
+    const auto* st = static_cast<const A*>(amps);
+    const uint64_t na = uint64_t{1} << n;
+    const uint32_t chunk = static_cast<uint32_t>(na < kSampleChunk ? na : kSampleChunk);
+    const uint64_t nchunks = na / chunk;
+    auto al = [](size_t b) { return (b + 255) & ~size_t{255}; };
+    auto* p = static_cast<unsigned char*>(scratch);
+    auto* sums = reinterpret_cast<double*>(p);
+    p += al(nchunks * 8);
+    auto* starts = reinterpret_cast<double*>(p);
+    p += al(nchunks * 8);
+    auto* cst = reinterpret_cast<double*>(p);
+    p += al((nchunks + 1) * 8);
+    auto* maps = reinterpret_cast<ChunkMap*>(p);
+    p += al(nchunks * sizeof(ChunkMap));
+    auto* seq = reinterpret_cast<unsigned char*>(p);
+    p += al(nchunks);
+    auto* excl = reinterpret_cast<SMap*>(p);
+    p += al(nchunks * sizeof(SMap));
+    auto* seg_total = reinterpret_cast<SMap*>(p);
+    p += al(nchunks * sizeof(SMap));
+    auto* direct = reinterpret_cast<unsigned char*>(p);
+    p += al(nchunks);
+    auto* seg_c = reinterpret_cast<double*>(p);
+    k_chunk_sums<<<static_cast<unsigned>(nchunks), kThreads, 0, s>>>(st, na, chunk, sums);
+    k_scan_sums<<<1, 1024, 0, s>>>(sums, nchunks, starts);
+    k_chunk_maps<<<static_cast<unsigned>(nchunks), kThreads, 0, s>>>(st, na, chunk, starts, sums, maps);
+    cudaMemsetAsync(direct, 0, nchunks, s);
+    k_seg_scan<<<1, 1024, 0, s>>>(maps, nchunks, excl, seg_total);
+    k_seg_chain<<<1, 32, 0, s>>>(st, na, chunk, nchunks, maps, seg_total, cst, seq, direct, seg_c);
+    k_seg_fill<<<static_cast<unsigned>((nchunks + kThreads - 1) / kThreads), kThreads, 0, s>>>(nchunks, maps, excl,
+                                                                                                direct, seg_c, cst,
+                                                                                                seq);
+    if (int rc = launch_status(); rc != MB2_OK) return rc;
+    if (cudaMemcpyAsync(host_total, cst + nchunks, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return record_cuda_error(static_cast<int>(cudaGetLastError()));
+    return MB2_OK;
+}
+
+int launch_exact_norm(const void* amps, uint32_t n, void* scratch, double* host_total, void* stream, int precision) {
+    note_launches(6);
+    return precision == MB2_C64 ? launch_exact_norm_t<float2>(amps, n, scratch, host_total, stream)
+                                : launch_exact_norm_t<double2>(amps, n, scratch, host_total, stream);
+}
+
 int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
                   uint64_t* dev_basis, void* stream, int precision) {
     note_launches(8);

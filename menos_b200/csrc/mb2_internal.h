@@ -340,6 +340,9 @@ constexpr uint32_t kMaxBatchTerms = MB2_BATCH_MAX_TERMS;
 // the s-th smallest uniform.
 constexpr uint32_t kSampleChunk = 4096;
 size_t sample_scratch_bytes(uint32_t n, uint64_t shots);
+// The reference's sequential FP64 sum of |a_i|^2 over the state, bit for bit
+// (the sampler's exact chain; scratch: sample_scratch_bytes(n, 0)); synchronises.
+int launch_exact_norm(const void* amps, uint32_t n, void* scratch, double* host_total, void* stream, int precision);
 int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
                   uint64_t* dev_basis, void* stream, int precision = MB2_C128);
 // complex64 precision path (kernels_c64.cu).

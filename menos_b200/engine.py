@@ -209,6 +209,12 @@ class DeviceState:
         self._chk(lib().mb2_normalize(self.h, C.byref(v)), "mb2_normalize")
         return v.value
 
+    def norm_exact(self) -> float:
+        """The reference's sequential sum of |a|^2, bit for bit."""
+        v = C.c_double()
+        self._chk(lib().mb2_norm_exact(self.h, C.byref(v)), "mb2_norm_exact")
+        return v.value
+
     def norm(self) -> float:
         v = C.c_double()
         self._chk(lib().mb2_norm(self.h, C.byref(v)), "mb2_norm")
@@ -238,6 +244,34 @@ class DeviceState:
 
     def synchronize(self) -> None:
         self._chk(lib().mb2_synchronize(self.h), "mb2_synchronize")
+
+
+def trajectories(ctx: Context, circ: Circuit, count: int, seed: int, paulis=(), coefs=None, shots: int = 0,
+                 targets=()) -> dict:
+    """mb2_trajectories: the reference's trajectory engine on the device.
+    Returns {"terms": complex means per Pauli term, "standard_error": of
+    sum coef_t <P_t> (coefs default 1), "counts": Counts or None}."""
+    arr, keep = to_mb2_ops(circ)
+    T = len(paulis)
+    xs = np.ascontiguousarray([int(p[0]) for p in paulis] or [0], dtype=np.uint64)
+    zs = np.ascontiguousarray([int(p[1]) for p in paulis] or [0], dtype=np.uint64)
+    cs = np.ascontiguousarray(np.asarray(coefs if coefs is not None else [1.0] * max(T, 1), np.complex128))
+    means = np.zeros(2 * max(T, 1), np.float64)
+    se = C.c_double(0.0)
+    t = np.ascontiguousarray(np.asarray(targets, np.uint32).ravel())
+    cap = max(int(shots), 1)
+    outc = np.zeros(cap, np.uint64)
+    cnt = np.zeros(cap, np.uint64)
+    nout = C.c_uint64(cap)
+    check(lib().mb2_trajectories(ctx.h, circ.num_qubits, arr, len(circ.ops), count, seed, xs.ctypes.data,
+                                 zs.ctypes.data, cs.view(np.float64).ctypes.data, T, means.ctypes.data,
+                                 C.byref(se), shots, t.ctypes.data if len(t) else None, len(t) // 2,
+                                 outc.ctypes.data, cnt.ctypes.data, C.byref(nout)), ctx.h, "mb2_trajectories")
+    del keep
+    d = nout.value if shots else 0
+    return {"terms": means[:2 * T].view(np.complex128).copy() if T else None,
+            "standard_error": se.value if T else None,
+            "counts": Counts(outc[:d].copy(), cnt[:d].copy()) if shots else None}
 
 
 class DensityMatrix:

@@ -253,6 +253,10 @@ class RefLib:
                                  C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         L.ref_run_dm.restype = C.c_int
+        L.ref_run_trajectories.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64,
+                                           C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_run_trajectories.restype = C.c_int
         L.ref_last_error.restype = C.c_char_p
         L.ref_default_threads.restype = C.c_uint32
         L.ref_kernel_isa.restype = C.c_int
@@ -377,6 +381,35 @@ class RefLib:
             "terms": terms[:2 * len(paulis)].view(np.complex128).copy() if paulis else None,
             "seconds": float(secs[0]),
         }
+
+    def run_trajectories(self, circ: Circuit, trajectories, seed, paulis=(), coefs=None, shots=0, targets=(),
+                         width=None):
+        """TrajectoryEngine::execute; returns dict(terms, standard_error, counts)."""
+        arr, keep = ops_struct_array(circ)
+        T = len(paulis)
+        xs = np.array([p[0] for p in paulis] or [0], np.uint64)
+        zs = np.array([p[1] for p in paulis] or [0], np.uint64)
+        cs = np.ascontiguousarray(np.asarray(coefs if coefs is not None else [1.0] * max(T, 1), np.complex128))
+        terms = np.zeros(2 * max(T, 1), np.float64)
+        se = np.zeros(1, np.float64)
+        t = np.asarray(targets, np.uint32).ravel()
+        if width is None:
+            width = int(max(t[1::2]) + 1) if len(t) else 0
+        cap = max(shots, 1)
+        outc = np.zeros(cap, np.uint64)
+        cnt = np.zeros(cap, np.uint64)
+        nout = np.array([cap], np.uint64)
+        rc = self.L.ref_run_trajectories(circ.num_qubits, C.addressof(arr), len(circ.ops), trajectories, seed,
+                                         xs.ctypes.data, zs.ctypes.data, cs.view(np.float64).ctypes.data, T,
+                                         terms.ctypes.data, se.ctypes.data, shots,
+                                         t.ctypes.data if len(t) else None, len(t) // 2, width,
+                                         outc.ctypes.data, cnt.ctypes.data, nout.ctypes.data)
+        assert rc == 0, self.L.ref_last_error()
+        del keep
+        d = int(nout[0]) if shots else 0
+        return {"terms": terms[:2 * T].view(np.complex128).copy() if T else None,
+                "standard_error": float(se[0]) if T else None,
+                "counts": {int(o): int(c) for o, c in zip(outc[:d], cnt[:d])}}
 
     def run_plan(self, circ, plan, threads=0) -> np.ndarray:
         """The dense engine's fused sweep over an explicit plan (order,

@@ -31,6 +31,7 @@
 #include "common/rng.h"
 #include "engines/dense/apply_matrix.h"
 #include "engines/density_matrix/density_matrix_engine.h"
+#include "engines/trajectory/trajectory_engine.h"
 #include "engines/dense/dense_engine.h"
 #ifdef MENOS_REF_CUDA
 #include "engines/dense_cuda/cuda_dense_engine.h"
@@ -411,6 +412,74 @@ int ref_run_dm(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_ops,
                 terms_out[2 * i] = (*res.expectation_terms)[i].real();
                 terms_out[2 * i + 1] = (*res.expectation_terms)[i].imag();
             }
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// TrajectoryEngine::execute on ops (src/engines/trajectory/
+// trajectory_engine.cpp:424-494): `trajectories` runs from `seed`; term
+// means (2 * n_terms doubles, coefficients `coefs` as complex pairs), the
+// standard error, and counts (capacity *n_outcomes, updated) when requested.
+int ref_run_trajectories(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_ops,
+                         std::uint64_t trajectories, std::uint64_t seed, const std::uint64_t* x_masks,
+                         const std::uint64_t* z_masks, const double* coefs, std::uint32_t n_terms, double* terms_out,
+                         double* standard_error, std::uint64_t shots, const std::uint32_t* targets,
+                         std::uint32_t n_targets, std::uint32_t width, std::uint64_t* out_outcomes,
+                         std::uint64_t* out_counts, std::uint64_t* n_outcomes) {
+    try {
+        std::vector<menos::Operation> v;
+        for (std::uint32_t i = 0; i < n_ops; ++i) {
+            v.push_back(to_operation(ops[i]));
+        }
+        std::vector<std::pair<menos::QubitId, menos::ClbitId>> t(n_targets);
+        for (std::uint32_t i = 0; i < n_targets; ++i) {
+            t[i] = {targets[2 * i], targets[2 * i + 1]};
+        }
+        menos::Observable obs;
+        for (std::uint32_t i = 0; i < n_terms; ++i) {
+            menos::PauliString p{num_qubits, {x_masks[i]}, {z_masks[i]}};
+            obs.terms.emplace_back(std::move(p), C{coefs[2 * i], coefs[2 * i + 1]});
+        }
+        menos::EngineExecutionRequest req{};
+        req.num_qubits = num_qubits;
+        req.operations = v;
+        req.want_statevector = false;
+        req.want_counts = shots > 0;
+        req.want_expectation = n_terms > 0;
+        req.shots = shots;
+        req.measure_targets = t;
+        req.bitstring_width = width;
+        req.seed = seed;
+        req.budget_bytes = ~std::uint64_t{0};
+        req.is_sole_region = true;
+        req.observable = req.want_expectation ? &obs : nullptr;
+        req.max_threads = 1;
+        req.trajectories = trajectories;
+        const menos::engines::trajectory::TrajectoryEngine engine;
+        menos::EngineExecutionResult res = engine.execute(req);
+        if (req.want_expectation) {
+            for (std::uint32_t i = 0; i < n_terms; ++i) {
+                terms_out[2 * i] = (*res.expectation_terms)[i].real();
+                terms_out[2 * i + 1] = (*res.expectation_terms)[i].imag();
+            }
+            *standard_error = res.expectation_standard_error.value_or(0.0);
+        }
+        if (req.want_counts) {
+            std::uint64_t i = 0;
+            for (const auto& [key, count] : *res.counts) {
+                if (i >= *n_outcomes) {
+                    g_error = "outcome capacity exceeded";
+                    return -1;
+                }
+                out_outcomes[i] = bits_of(key);
+                out_counts[i] = count;
+                ++i;
+            }
+            *n_outcomes = i;
         }
         return 0;
     } catch (const std::exception& e) {
