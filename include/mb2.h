@@ -100,6 +100,19 @@ int mb2_device_info(mb2_context* ctx, int* sm_count, uint64_t* total_bytes, uint
 int mb2_state_alloc(mb2_context* ctx, uint32_t num_qubits, int precision, uint64_t budget_bytes,
                     mb2_state** out);
 int mb2_state_free(mb2_state* state);
+/* A complex128 state that lives in pinned, mapped HOST memory (for states
+ * above the device's memory): every call above works on it unchanged -- the
+ * kernels read and write the host buffer over PCIe through its device alias,
+ * so results are bitwise those of a device-resident state, and each tiled
+ * pass streams the state once (sweeps default to the widest tile, for the
+ * fewest passes).  budget_bytes bounds the host buffer (MB2_ERR_RESOURCE
+ * before any allocation).  The reference records this tier as measured and
+ * not built (include/menos/menos.h:157, Tier::HostOffloaded); its disk tier
+ * streams a window of chunks per pass (src/engines/dense_tiered/
+ * chunked_executor.cpp).  mb2_state_host_ptr: the host buffer (2 * 2^n
+ * doubles), readable once the state's stream is idle (mb2_synchronize). */
+int mb2_state_alloc_host(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, mb2_state** out);
+int mb2_state_host_ptr(mb2_state* state, void** out);
 /* Replaces: kernels::cuda::initialize (src/kernels/cuda/dense_kernels.cu:273-286). */
 int mb2_init(mb2_state* state, double global_phase);
 /* Device pointer of the amplitudes (interleaved re/im), for in-process callers. */

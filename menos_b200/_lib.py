@@ -127,6 +127,8 @@ SIGNATURES = {
     "mb2_normalize": (C.c_int, [_VP, C.POINTER(C.c_double)]),
     "mb2_sample": (C.c_int, [_VP, C.c_uint64, C.c_uint64, _VP, C.c_uint32, _VP, _VP, C.POINTER(C.c_uint64)]),
     "mb2_norm_exact": (C.c_int, [_VP, C.POINTER(C.c_double)]),
+    "mb2_state_alloc_host": (C.c_int, [_VP, C.c_uint32, C.c_uint64, C.POINTER(_VP)]),
+    "mb2_state_host_ptr": (C.c_int, [_VP, C.POINTER(_VP)]),
     "mb2_trajectories": (C.c_int, [_VP, C.c_uint32, _VP, C.c_uint32, C.c_uint64, C.c_uint64, _VP, _VP, _VP,
                                    C.c_uint32, _VP, C.POINTER(C.c_double), C.c_uint64, _VP, C.c_uint32, _VP, _VP,
                                    C.POINTER(C.c_uint64)]),

@@ -44,6 +44,9 @@ struct mb2_state {
     bool owns_stream = true;
     void* scratch = nullptr;  // staging: program, matrices, masks, partials
     size_t scratch_bytes = 0;
+    // A host-resident state (mb2_state_alloc_host): the pinned, mapped host
+    // buffer, of which `amps` is the device's alias.
+    void* host_amps = nullptr;
     mb2_sweep_stats stats{};
 };
 
@@ -343,11 +346,55 @@ int mb2_state_alloc(mb2_context* ctx, uint32_t num_qubits, int precision, uint64
     return MB2_OK;
 }
 
+int mb2_state_alloc_host(mb2_context* ctx, uint32_t num_qubits, uint64_t budget_bytes, mb2_state** out) {
+    if (ctx == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    *out = nullptr;
+    if (num_qubits < 1 || num_qubits > 40) return fail(ctx, MB2_ERR_INVALID, "num_qubits must be 1..40");
+    const uint64_t bytes = (uint64_t{1} << num_qubits) * amp_bytes(MB2_C128);
+    if (bytes > budget_bytes)
+        return fail(ctx, MB2_ERR_RESOURCE,
+                    "host state needs " + std::to_string(bytes) + " bytes, budget is " + std::to_string(budget_bytes));
+    MB2_CUDA(ctx, cudaSetDevice(ctx->device));
+    void* host = nullptr;
+    cudaError_t e = cudaHostAlloc(&host, bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, MB2_ERR_RESOURCE, "cudaHostAlloc of " + std::to_string(bytes) + " bytes failed");
+    }
+    void* dev = nullptr;
+    e = cudaHostGetDevicePointer(&dev, host, 0);
+    if (e != cudaSuccess) {
+        cudaFreeHost(host);
+        return cuda_fail(ctx, e, "cudaHostGetDevicePointer");
+    }
+    auto* s = new mb2_state;
+    s->ctx = ctx;
+    s->n = num_qubits;
+    s->precision = MB2_C128;
+    e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cudaFreeHost(host);
+        delete s;
+        return cuda_fail(ctx, e, "cudaStreamCreate");
+    }
+    s->amps = dev;
+    s->host_amps = host;
+    *out = s;
+    return MB2_OK;
+}
+
+int mb2_state_host_ptr(mb2_state* s, void** out) {
+    if (s == nullptr || out == nullptr) return MB2_ERR_INVALID;
+    *out = s->host_amps;
+    return MB2_OK;
+}
+
 int mb2_state_free(mb2_state* s) {
     if (s == nullptr) return MB2_OK;
     if (s->scratch) cudaFreeAsync(s->scratch, s->stream);
-    cudaFreeAsync(s->amps, s->stream);
+    if (s->host_amps == nullptr) cudaFreeAsync(s->amps, s->stream);
     cudaStreamSynchronize(s->stream);
+    if (s->host_amps != nullptr) cudaFreeHost(s->host_amps);
     if (s->owns_stream) cudaStreamDestroy(s->stream);
     delete s;
     return MB2_OK;
@@ -408,8 +455,10 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     s->stats.blocks = blocks.size();
     if (blocks.empty()) return MB2_OK;
     const bool c64 = s->precision == MB2_C64;
-    uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : s->ctx->tile_c128.load(), s->n,
-                            blocks);
+    // A host-resident state streams over PCIe once per pass: the widest tile
+    // (fewest passes) unless asked otherwise.
+    const uint32_t dflt = s->host_amps != nullptr ? mb2::kMaxTileQubits : s->ctx->tile_c128.load();
+    uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : dflt, s->n, blocks);
     bool tc = false;
     if (c64) {
         // 8-byte amplitudes: up to 13-qubit tiles fit the same shared memory.
@@ -1201,7 +1250,8 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
 int mb2_copy_out(mb2_state* s, void* host, uint64_t num_amplitudes) {
     if (s == nullptr || host == nullptr) return MB2_ERR_INVALID;
     if (num_amplitudes > (uint64_t{1} << s->n)) return fail(s->ctx, MB2_ERR_INVALID, "copy beyond the state");
-    MB2_CUDA(s->ctx, cudaMemcpyAsync(host, s->amps, num_amplitudes * amp_bytes(s->precision), cudaMemcpyDeviceToHost,
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(host, s->amps, num_amplitudes * amp_bytes(s->precision),
+                                     s->host_amps != nullptr ? cudaMemcpyDefault : cudaMemcpyDeviceToHost,
                                      s->stream));
     MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
     return MB2_OK;
@@ -1210,7 +1260,8 @@ int mb2_copy_out(mb2_state* s, void* host, uint64_t num_amplitudes) {
 int mb2_copy_in(mb2_state* s, const void* host, uint64_t num_amplitudes) {
     if (s == nullptr || host == nullptr) return MB2_ERR_INVALID;
     if (num_amplitudes > (uint64_t{1} << s->n)) return fail(s->ctx, MB2_ERR_INVALID, "copy beyond the state");
-    MB2_CUDA(s->ctx, cudaMemcpyAsync(s->amps, host, num_amplitudes * amp_bytes(s->precision), cudaMemcpyHostToDevice,
+    MB2_CUDA(s->ctx, cudaMemcpyAsync(s->amps, host, num_amplitudes * amp_bytes(s->precision),
+                                     s->host_amps != nullptr ? cudaMemcpyDefault : cudaMemcpyHostToDevice,
                                      s->stream));
     MB2_CUDA(s->ctx, cudaStreamSynchronize(s->stream));
     return MB2_OK;

@@ -130,10 +130,19 @@ class DeviceState:
     """A statevector in device memory (reference: DeviceBuffer,
     src/kernels/cuda/device_buffer.h:25-55)."""
 
-    def __init__(self, ctx: Context, num_qubits: int, precision: int = C128, budget_bytes: int = 2 ** 64 - 1):
+    def __init__(self, ctx: Context, num_qubits: int, precision: int = C128, budget_bytes: int = 2 ** 64 - 1,
+                 host: bool = False):
+        """host=True: a complex128 state in pinned, mapped host memory
+        (mb2_state_alloc_host), for states above the device's memory."""
         h = C.c_void_p()
-        check(lib().mb2_state_alloc(ctx.h, num_qubits, precision, min(budget_bytes, 2 ** 64 - 1), C.byref(h)),
-              ctx.h, "mb2_state_alloc")
+        if host:
+            if precision != C128:
+                raise ValueError("host-resident states are complex128")
+            check(lib().mb2_state_alloc_host(ctx.h, num_qubits, min(budget_bytes, 2 ** 64 - 1), C.byref(h)),
+                  ctx.h, "mb2_state_alloc_host")
+        else:
+            check(lib().mb2_state_alloc(ctx.h, num_qubits, precision, min(budget_bytes, 2 ** 64 - 1), C.byref(h)),
+                  ctx.h, "mb2_state_alloc")
         self.ctx = ctx
         self.h = h
         self.n = num_qubits
