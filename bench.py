@@ -84,6 +84,8 @@ def parse():
     p.add_argument("--mode", default="job", choices=["job", "serve", "batch", "c64", "estimator", "host"])
     p.add_argument("--requests", type=int, default=600)
     p.add_argument("--load", default="4", help="serve: arrival rate / plain-loop capacity (comma list: a sweep)")
+    p.add_argument("--qubit-range", default="12,28", help="serve: request qubit counts, uniform in lo,hi")
+    p.add_argument("--slots", type=int, default=0, help="serve: concurrent requests (0: the server's default, 16)")
     p.add_argument("--bindings", type=int, default=4096)
     p.add_argument("--precision", default="c128", choices=["c128", "c64"], help="serve/batch: state precision")
     p.add_argument("--c64-kernel", default="auto", choices=["auto", "tensor", "simt"],
@@ -370,7 +372,13 @@ def main_serve(args, local):
     from menos_b200 import Context, DeviceState, workloads
     from menos_b200.serve import Server
     ctx = Context(local)
-    reqs = workloads.serving_stream(args.requests, 1.0, 20261201)
+    from menos_b200.circuit import PackedCircuit
+    nmin, nmax = (int(v) for v in args.qubit_range.split(","))
+    reqs = workloads.serving_stream(args.requests, 1.0, 20261201, nmin=nmin, nmax=nmax)
+    # Operations packed for the C ABI once, before any timed region, for
+    # both arms: the timed work is the engine's, not Python's conversion.
+    for r in reqs:
+        r["circuit"] = PackedCircuit(r["circuit"])
 
     def run_plain(r):
         st = DeviceState(ctx, r["circuit"].num_qubits)
@@ -409,7 +417,7 @@ def main_serve(args, local):
     prec = C64 if args.precision == "c64" else C128
 
     def serve(arrive):
-        srv = Server(ctx, budget_bytes=160 * 10**9)
+        srv = Server(ctx, budget_bytes=160 * 10**9, slots=args.slots)
         done, results, failed = {}, {}, {}
         tickets = {}
         t0 = time.perf_counter()
@@ -480,7 +488,7 @@ def main_serve(args, local):
         "results": {"burst_equals_live": mix_same, "counts_identical_to_plain_c128": counts_same,
                     "max_abs_dH_vs_plain_c128": worst_exp},
         "precision": args.precision,
-        "config": {"workload": "serving stream: qubits 12-28, depth 4-40 (U3/CZ brick or RY/RZ+CX), "
+        "config": {"workload": f"serving stream: qubits {nmin}-{nmax}, depth 4-40 (U3/CZ brick or RY/RZ+CX), "
                                f"4096 shots or <H> over 32 weighted Paulis, {args.precision}, budget 160 GB",
                    "seed": 20261201},
         "data": "synthetic (seeded requests)",

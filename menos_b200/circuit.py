@@ -84,8 +84,33 @@ class Circuit:
         return [(q, c) for c, q in sorted(by_clbit.items())]
 
 
-def to_mb2_ops(circ: Circuit):
+class PackedCircuit:
+    """A circuit with its operations packed once into the C ABI's mb2_op
+    array: every call that takes a Circuit takes it, without converting the
+    operations again (a Python loop over them, ~0.7 us an operation)."""
+
+    def __init__(self, circ: Circuit):
+        self.num_qubits = circ.num_qubits
+        self.num_clbits = getattr(circ, "num_clbits", 0)
+        self.global_phase = circ.global_phase
+        self.ops = list(circ.ops)
+        self._packed = _pack(self)
+
+    def __len__(self) -> int:
+        return len(self.ops)
+
+    def measure_targets(self):
+        return Circuit.measure_targets(self)
+
+
+def to_mb2_ops(circ):
     """Returns (array of MB2Op, keep-alive list of matrix buffers)."""
+    if isinstance(circ, PackedCircuit):
+        return circ._packed
+    return _pack(circ)
+
+
+def _pack(circ):
     n = len(circ.ops)
     arr = (MB2Op * max(n, 1))()
     keep = []

@@ -455,9 +455,11 @@ int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_op
     s->stats.blocks = blocks.size();
     if (blocks.empty()) return MB2_OK;
     const bool c64 = s->precision == MB2_C64;
-    // A host-resident state streams over PCIe once per pass: the widest tile
-    // (fewest passes) unless asked otherwise.
-    const uint32_t dflt = s->host_amps != nullptr ? mb2::kMaxTileQubits : s->ctx->tile_c128.load();
+    // The widest tile (fewest passes) unless asked otherwise for a
+    // host-resident state, which streams over PCIe once per pass, and for a
+    // small one (up to 16 qubits: a 12-qubit tile holds a whole 12-qubit
+    // state), whose passes are a few CTAs each and cost their launches.
+    const uint32_t dflt = s->host_amps != nullptr || s->n <= 16 ? mb2::kMaxTileQubits : s->ctx->tile_c128.load();
     uint32_t m = tile_width(o.tile_qubits > 0 ? static_cast<uint32_t>(o.tile_qubits) : dflt, s->n, blocks);
     bool tc = false;
     if (c64) {
@@ -745,7 +747,7 @@ std::vector<double> sorted_uniforms(uint64_t shots, uint64_t seed) {
 
 // The walk's basis states (non-decreasing) as counts of the measured
 // outcomes, ascending: mb2_sample's output.
-int histogram(mb2_state* s, uint32_t n, const std::vector<uint64_t>& basis, const uint32_t* targets,
+int histogram(mb2_context* ctx, uint32_t n, const std::vector<uint64_t>& basis, const uint32_t* targets,
               uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes) {
     const uint64_t shots = basis.size();
     // Outcomes through the measure targets, ascending, with counts.  The walk
@@ -792,7 +794,7 @@ int histogram(mb2_state* s, uint32_t n, const std::vector<uint64_t>& basis, cons
             counts[d - 1] += c;
             continue;
         }
-        if (d >= *num_outcomes) return fail(s->ctx, MB2_ERR_INVALID, "outcome capacity too small");
+        if (d >= *num_outcomes) return fail(ctx, MB2_ERR_INVALID, "outcome capacity too small");
         outcomes[d] = o;
         counts[d] = c;
         ++d;
@@ -802,6 +804,14 @@ int histogram(mb2_state* s, uint32_t n, const std::vector<uint64_t>& basis, cons
 }
 
 }  // namespace
+
+namespace mb2 {
+std::vector<double> sorted_reference_uniforms(uint64_t shots, uint64_t seed) { return sorted_uniforms(shots, seed); }
+int counts_of(mb2_context* ctx, uint32_t n, const std::vector<uint64_t>& basis, const uint32_t* targets,
+              uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes) {
+    return histogram(ctx, n, basis, targets, num_targets, outcomes, counts, num_outcomes);
+}
+}  // namespace mb2
 
 extern "C" {
 
@@ -818,7 +828,7 @@ int mb2_sample(mb2_state* s, uint64_t shots, uint64_t seed, const uint32_t* targ
     const std::vector<double> u = sorted_uniforms(shots, seed);
     std::vector<uint64_t> basis(shots);
     if (int e = walk_sorted(s, u, basis.data()); e != MB2_OK) return e;
-    return histogram(s, s->n, basis, targets, num_targets, outcomes, counts, num_outcomes);
+    return histogram(s->ctx, s->n, basis, targets, num_targets, outcomes, counts, num_outcomes);
 }
 
 int mb2_sample_basis(mb2_state* s, const double* uniforms, uint64_t n, uint64_t* basis_out) {
@@ -1018,7 +1028,7 @@ int mb2_dm_sample(mb2_state* rho, uint32_t n, uint64_t shots, uint64_t seed, con
     std::vector<uint64_t> basis(shots);
     MB2_CUDA(rho->ctx, cudaMemcpyAsync(basis.data(), base + al_u, shots * 8, cudaMemcpyDeviceToHost, rho->stream));
     MB2_CUDA(rho->ctx, cudaStreamSynchronize(rho->stream));
-    return histogram(rho, n, basis, targets, num_targets, outcomes, counts, num_outcomes);
+    return histogram(rho->ctx, n, basis, targets, num_targets, outcomes, counts, num_outcomes);
 }
 
 int mb2_norm_exact(mb2_state* s, double* out) {
@@ -1242,7 +1252,7 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
     }
     if (want_counts) {
         std::sort(shot_basis.begin(), shot_basis.end());
-        return histogram(st, n, shot_basis, targets, num_targets, outcomes, counts, num_outcomes);
+        return histogram(ctx, n, shot_basis, targets, num_targets, outcomes, counts, num_outcomes);
     }
     return MB2_OK;
 }

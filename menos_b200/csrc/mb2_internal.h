@@ -319,6 +319,46 @@ struct TileLaunch {
     size_t smem = 0;
     void* stream = nullptr;
 };
+// One state's pass in a launch of many (k_tile_pass_jobs): its CTAs are
+// [cta_begin, cta_begin + nctas); words and data in device memory.
+struct TileJob {
+    void* st;  // complex128 amplitudes
+    uint64_t smask, gmask, ntiles;
+    const uint32_t* words;
+    const double* sdata;
+    const double* gdata;
+    uint32_t n, nwords, nsdata, cta_begin, nctas, pad;
+};
+// Launches pass jobs[0..njobs) (host array `jobs`, copied to dev_jobs by the
+// caller beforehand) with tile width m, the full kernel variant; smem: the
+// largest job's dynamic shared memory.
+int launch_tile_jobs(const TileJob* dev_jobs, uint32_t njobs, uint32_t total_ctas, uint32_t m, size_t smem,
+                     void* stream);
+// The small-request batch's other steps (kernels_small.cu), one launch each
+// for every state: amplitude 0 of each zeroed state; a Pauli term per
+// (state, term) job (out: 2 doubles per job, <psi|P|psi>); the reference's
+// exact sampling walk per state (u sorted ascending, basis out).
+struct ExpectJob {
+    const void* st;
+    uint64_t x, z;
+    uint32_t n, pad;
+};
+struct WalkJob {
+    const void* st;
+    const double* u;
+    uint64_t* basis;
+    uint64_t shots;
+    uint32_t n, pad;
+};
+// The reference's sorted uniforms for `shots` draws from `seed` (common::Rng,
+// src/engines/dense/sample.cpp:36-42), and the outcomes through measure
+// targets of a non-decreasing basis list (mb2_sample's histogram).
+std::vector<double> sorted_reference_uniforms(uint64_t shots, uint64_t seed);
+int counts_of(mb2_context* ctx, uint32_t n, const std::vector<uint64_t>& basis, const uint32_t* targets,
+              uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes);
+int launch_init_jobs(void* base, const uint64_t* dev_offsets, const double* dev_vals, uint32_t count, void* stream);
+int launch_expect_jobs(const ExpectJob* dev_jobs, uint32_t count, double* dev_out, void* stream);
+int launch_walk_jobs(const WalkJob* dev_jobs, uint32_t count, void* stream);
 constexpr size_t kTileSmemMax = 227 * 1024;  // per block
 constexpr size_t kSmemPerSm = 228 * 1024;    // per SM (1 KiB of it reserved per resident block)
 int launch_tile_generic(TileLaunch& L);  // any tile width, 64-bit indices

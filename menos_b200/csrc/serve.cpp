@@ -26,6 +26,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <stdexcept>
 #include <thread>
 #include <vector>
 
@@ -61,9 +62,16 @@ struct Done {
 // state's staging buffer at its largest (the same layout and rounding the
 // engine's calls use), each allocation rounded up to the stream-ordered
 // pool's 2 MiB granularity.
+// Requests of 4..16 qubits run as part of a batch (run_small_batch) in
+// complex128, whatever precision they ask for: their states are a few CTAs'
+// work, so their cost is the launches and calls around them, which a batch
+// shares; complex128 costs them nothing more and is the reference's result.
+constexpr uint32_t kSmallMinQubits = 4, kSmallMaxQubits = 16, kSmallBatchMax = 64;
+bool small_request(const Request& r) { return r.n >= kSmallMinQubits && r.n <= kSmallMaxQubits; }
+
 uint64_t admission_bytes(const Request& r) {
     auto pool = [](uint64_t v) { return (v + (2ull << 20) - 1) & ~((2ull << 20) - 1); };
-    const uint64_t state = (uint64_t{1} << r.n) * (r.precision == MB2_C64 ? 8 : 16);
+    const uint64_t state = (uint64_t{1} << r.n) * (r.precision == MB2_C64 && !small_request(r) ? 8 : 16);
     const uint64_t staging =
         mb2::scratch_bound(r.n, r.ops.data(), static_cast<uint32_t>(r.ops.size()),
                            r.output == MB2_OUT_COUNTS ? r.shots : 0,
@@ -163,6 +171,258 @@ void run_request(mb2_server* s, cudaStream_t stream, Request& r, Done& d) {
     d.c.status = rc;
 }
 
+// Another pending small request that can be admitted now (no starvation
+// rule: the batch only gathers what is already waiting).
+bool pick_small(mb2_server* s, Request& out) {
+    for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
+        if (!small_request(*it)) continue;
+        if (!admit(s, it->bytes)) continue;
+        out = std::move(*it);
+        s->pending.erase(it);
+        s->held += out.bytes;
+        return true;
+    }
+    return false;
+}
+
+// Small requests together, each step one launch for all of them: the states
+// (complex128) in one allocation, zeroed with one memset and given their
+// initial phase by one launch; pass p of every request's tiled program in
+// one launch per tile width (k_tile_pass_jobs, a CTA per tile); every Pauli
+// term of every expectation request in one launch; every counts request's
+// exact walk in one launch; one upload and one download.  Each state's
+// arithmetic is that of mb2_apply_program (bitwise), its counts the same
+// walk over the same sorted uniforms as mb2_sample (identical), its terms a
+// fixed-order reduction (within 1e-12 of the reference).
+void run_small_batch(mb2_server* s, cudaStream_t stream, std::vector<Request>& batch, std::vector<Done>& dones) {
+    const size_t B = batch.size();
+    dones.assign(B, Done{});
+    for (size_t i = 0; i < B; ++i) dones[i].c.ticket = batch[i].ticket;
+    std::vector<mb2::TileProgram> progs(B);
+    std::vector<uint32_t> tile(B, 0);
+    std::vector<bool> ok(B, true);
+    for (size_t i = 0; i < B; ++i) {
+        const Request& r = batch[i];
+        try {
+            const std::vector<mb2::Block> blocks =
+                mb2::build_blocks(r.ops.data(), static_cast<uint32_t>(r.ops.size()), r.fuse != 0);
+            uint32_t m = std::min<uint32_t>(mb2::kMaxTileQubits, r.n);
+            for (const mb2::Block& b : blocks) m = std::max(m, b.k);
+            if (m > r.n) throw std::invalid_argument("a block wider than the state");
+            progs[i] = mb2::plan_tile_program(blocks, r.n, m, mb2::kDefaultFixedLow, nullptr, false);
+            mb2::encode_compact(progs[i]);
+            tile[i] = std::min(m, r.n);
+        } catch (const std::exception&) {
+            ok[i] = false;
+            dones[i].c.status = MB2_ERR_INVALID;
+        }
+    }
+    // Device layout: [uploaded: programs, job tables, init table, uniforms]
+    // [states] [written: terms, basis].
+    auto up = [](size_t v) { return (v + 255) & ~size_t{255}; };
+    size_t off = 0;
+    std::vector<size_t> w_off(B), d_off(B), g_off(B), u_off(B, 0), st_off(B), b_off(B, 0);
+    for (size_t i = 0; i < B; ++i) {
+        if (!ok[i]) continue;
+        w_off[i] = off;
+        off = up(off + progs[i].words.size() * 4);
+        d_off[i] = off;
+        off = up(off + progs[i].data.size() * 8);
+        g_off[i] = off;
+        off = up(off + progs[i].gdata.size() * 8);
+    }
+    // Tile jobs, grouped by (pass index, tile width).
+    struct Launch {
+        uint32_t m, count, ctas;
+        size_t off, smem;
+    };
+    std::vector<Launch> launches;
+    std::vector<mb2::TileJob> jobs;  // device pointers filled in after allocation
+    std::vector<size_t> job_req;     // job -> request
+    std::vector<uint32_t> job_pass;  // job -> pass index
+    size_t max_passes = 0;
+    for (size_t i = 0; i < B; ++i)
+        if (ok[i]) max_passes = std::max(max_passes, progs[i].passes.size());
+    for (size_t p = 0; p < max_passes; ++p) {
+        for (uint32_t m = mb2::kMinTileQubits; m <= mb2::kMaxTileQubits; ++m) {
+            Launch L{m, 0, 0, 0, 0};
+            const size_t first = jobs.size();
+            for (size_t i = 0; i < B; ++i) {
+                if (!ok[i] || tile[i] != m || p >= progs[i].passes.size()) continue;
+                const mb2::TilePass& tp = progs[i].passes[p];
+                mb2::TileJob J{};
+                J.smask = tp.smask;
+                J.gmask = tp.gmask;
+                J.ntiles = uint64_t{1} << (batch[i].n - tp.m);
+                J.n = batch[i].n;
+                J.nwords = tp.word_count;
+                J.nsdata = tp.sdata_count;
+                J.cta_begin = L.ctas;
+                J.nctas = static_cast<uint32_t>(J.ntiles);
+                L.ctas += J.nctas;
+                L.smem = std::max(L.smem, 2 * (size_t{1} << m) * 16 + size_t{tp.word_count} * 4 + size_t{tp.sdata_count} * 8);
+                jobs.push_back(J);
+                job_req.push_back(i);
+                job_pass.push_back(static_cast<uint32_t>(p));
+                ++L.count;
+            }
+            if (L.count == 0) continue;
+            L.off = first;  // job index for now
+            launches.push_back(L);
+        }
+    }
+    const size_t jobs_off = off;
+    off = up(off + jobs.size() * sizeof(mb2::TileJob));
+    const size_t init_off = off;
+    off = up(off + B * 8);
+    const size_t initv_off = off;
+    off = up(off + B * 16);
+    std::vector<mb2::ExpectJob> ejobs;
+    std::vector<size_t> e_first(B, 0);
+    std::vector<mb2::WalkJob> wjobs;
+    std::vector<std::vector<double>> uniforms(B);
+    for (size_t i = 0; i < B; ++i) {
+        if (!ok[i]) continue;
+        const Request& r = batch[i];
+        if (r.output == MB2_OUT_EXPECTATION) {
+            e_first[i] = ejobs.size();
+            for (size_t t = 0; t < r.xs.size(); ++t) ejobs.push_back(mb2::ExpectJob{nullptr, r.xs[t], r.zs[t], r.n, 0});
+        } else if (r.shots > 0) {
+            uniforms[i] = mb2::sorted_reference_uniforms(r.shots, r.seed);
+            u_off[i] = off;
+            off = up(off + r.shots * 8);
+        }
+    }
+    const size_t ejobs_off = off;
+    off = up(off + ejobs.size() * sizeof(mb2::ExpectJob));
+    size_t nwalk = 0;
+    for (size_t i = 0; i < B; ++i)
+        if (ok[i] && batch[i].output == MB2_OUT_COUNTS && batch[i].shots > 0) ++nwalk;
+    const size_t wjobs_off = off;
+    off = up(off + nwalk * sizeof(mb2::WalkJob));
+    const size_t upload_bytes = off;
+    const size_t states_off = off;
+    for (size_t i = 0; i < B; ++i) {
+        st_off[i] = off;
+        off = up(off + (ok[i] ? (size_t{16} << batch[i].n) : 0));
+    }
+    const size_t states_bytes = off - states_off;
+    const size_t eout_off = off;
+    off = up(off + ejobs.size() * 16);
+    const size_t basis_off = off;
+    for (size_t i = 0; i < B; ++i)
+        if (u_off[i] != 0 || (ok[i] && batch[i].output == MB2_OUT_COUNTS && batch[i].shots > 0)) {
+            b_off[i] = off;
+            off = up(off + batch[i].shots * 8);
+        }
+    const size_t total = off;
+    auto fail_all = [&](int rc) {
+        for (size_t i = 0; i < B; ++i)
+            if (dones[i].c.status == MB2_OK) dones[i].c.status = rc;
+    };
+    unsigned char* dev = nullptr;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&dev), total, stream) != cudaSuccess) {
+        cudaGetLastError();
+        fail_all(MB2_ERR_RESOURCE);
+        return;
+    }
+    std::vector<unsigned char> host(upload_bytes, 0);
+    for (size_t i = 0; i < B; ++i) {
+        if (!ok[i]) continue;
+        std::memcpy(host.data() + w_off[i], progs[i].words.data(), progs[i].words.size() * 4);
+        if (!progs[i].data.empty()) std::memcpy(host.data() + d_off[i], progs[i].data.data(), progs[i].data.size() * 8);
+        if (!progs[i].gdata.empty())
+            std::memcpy(host.data() + g_off[i], progs[i].gdata.data(), progs[i].gdata.size() * 8);
+        if (!uniforms[i].empty()) std::memcpy(host.data() + u_off[i], uniforms[i].data(), uniforms[i].size() * 8);
+    }
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        const size_t i = job_req[j];
+        const mb2::TilePass& tp = progs[i].passes[job_pass[j]];
+        jobs[j].st = dev + st_off[i];
+        jobs[j].words = reinterpret_cast<const uint32_t*>(dev + w_off[i]) + tp.word_begin;
+        jobs[j].sdata = reinterpret_cast<const double*>(dev + d_off[i]) + tp.sdata_begin;
+        jobs[j].gdata = reinterpret_cast<const double*>(dev + g_off[i]);
+    }
+    if (!jobs.empty()) std::memcpy(host.data() + jobs_off, jobs.data(), jobs.size() * sizeof(mb2::TileJob));
+    auto* init_offsets = reinterpret_cast<uint64_t*>(host.data() + init_off);
+    auto* init_vals = reinterpret_cast<double*>(host.data() + initv_off);
+    uint32_t ninit = 0;
+    for (size_t i = 0; i < B; ++i) {
+        if (!ok[i]) continue;
+        const mb2::Cd ph = mb2::initial_phase(batch[i].global_phase);
+        init_offsets[ninit] = (st_off[i] - states_off) / 16;
+        init_vals[2 * ninit] = ph.real();
+        init_vals[2 * ninit + 1] = ph.imag();
+        ++ninit;
+    }
+    for (size_t i = 0; i < B; ++i)
+        if (ok[i] && batch[i].output == MB2_OUT_EXPECTATION)
+            for (size_t t = 0; t < batch[i].xs.size(); ++t) ejobs[e_first[i] + t].st = dev + st_off[i];
+    if (!ejobs.empty()) std::memcpy(host.data() + ejobs_off, ejobs.data(), ejobs.size() * sizeof(mb2::ExpectJob));
+    for (size_t i = 0; i < B; ++i)
+        if (ok[i] && batch[i].output == MB2_OUT_COUNTS && batch[i].shots > 0)
+            wjobs.push_back(mb2::WalkJob{dev + st_off[i], reinterpret_cast<const double*>(dev + u_off[i]),
+                                         reinterpret_cast<uint64_t*>(dev + b_off[i]), batch[i].shots, batch[i].n, 0});
+    if (!wjobs.empty()) std::memcpy(host.data() + wjobs_off, wjobs.data(), wjobs.size() * sizeof(mb2::WalkJob));
+    int rc = MB2_OK;
+    if (cudaMemcpyAsync(dev, host.data(), upload_bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+        cudaMemsetAsync(dev + states_off, 0, states_bytes, stream) != cudaSuccess)
+        rc = mb2::record_cuda_error(static_cast<int>(cudaGetLastError()));
+    if (rc == MB2_OK)
+        rc = mb2::launch_init_jobs(dev + states_off, reinterpret_cast<const uint64_t*>(dev + init_off),
+                                   reinterpret_cast<const double*>(dev + initv_off), ninit, stream);
+    for (const Launch& L : launches) {
+        if (rc != MB2_OK) break;
+        rc = mb2::launch_tile_jobs(reinterpret_cast<const mb2::TileJob*>(dev + jobs_off) + L.off, L.count, L.ctas,
+                                   L.m, L.smem, stream);
+    }
+    if (rc == MB2_OK)
+        rc = mb2::launch_expect_jobs(reinterpret_cast<const mb2::ExpectJob*>(dev + ejobs_off),
+                                     static_cast<uint32_t>(ejobs.size()), reinterpret_cast<double*>(dev + eout_off),
+                                     stream);
+    if (rc == MB2_OK)
+        rc = mb2::launch_walk_jobs(reinterpret_cast<const mb2::WalkJob*>(dev + wjobs_off),
+                                   static_cast<uint32_t>(wjobs.size()), stream);
+    std::vector<double> eout(2 * ejobs.size());
+    std::vector<uint64_t> basis((total - basis_off) / 8);
+    if (rc == MB2_OK) {
+        if ((!eout.empty() && cudaMemcpyAsync(eout.data(), dev + eout_off, eout.size() * 8, cudaMemcpyDeviceToHost,
+                                              stream) != cudaSuccess) ||
+            (!basis.empty() && cudaMemcpyAsync(basis.data(), dev + basis_off, basis.size() * 8,
+                                               cudaMemcpyDeviceToHost, stream) != cudaSuccess) ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            rc = mb2::record_cuda_error(static_cast<int>(cudaGetLastError()));
+    }
+    cudaFreeAsync(dev, stream);
+    if (rc != MB2_OK) {
+        fail_all(rc);
+        return;
+    }
+    for (size_t i = 0; i < B; ++i) {
+        if (!ok[i]) continue;
+        const Request& r = batch[i];
+        Done& d = dones[i];
+        if (r.output == MB2_OUT_EXPECTATION) {
+            double total_h = 0.0;
+            for (size_t t = 0; t < r.xs.size(); ++t) total_h += r.coefs[t] * eout[2 * (e_first[i] + t)];
+            d.c.value = total_h;
+        } else if (r.shots > 0) {
+            const size_t first = (b_off[i] - basis_off) / 8;
+            const std::vector<uint64_t> bs(basis.begin() + static_cast<long>(first),
+                                           basis.begin() + static_cast<long>(first + r.shots));
+            d.outcomes.resize(r.shots);
+            d.counts.resize(r.shots);
+            uint64_t distinct = r.shots;
+            const int hr = mb2::counts_of(s->ctx, r.n, bs, r.targets.data(), static_cast<uint32_t>(r.targets.size() / 2),
+                                          d.outcomes.data(), d.counts.data(), &distinct);
+            d.outcomes.resize(hr == MB2_OK ? distinct : 0);
+            d.counts.resize(hr == MB2_OK ? distinct : 0);
+            d.c.num_outcomes = hr == MB2_OK ? distinct : 0;
+            d.c.status = hr;
+        }
+    }
+}
+
 void worker(mb2_server* s, uint32_t slot) {
     cudaSetDevice(mb2::context_device(s->ctx));
     for (;;) {
@@ -181,18 +441,37 @@ void worker(mb2_server* s, uint32_t slot) {
             admitted = Clock::now();
             ++s->in_flight;
         }
-        Done d;
-        d.c.ticket = r.ticket;
-        run_request(s, s->streams[slot], r, d);
+        std::vector<Request> batch;
+        batch.push_back(std::move(r));
+        if (small_request(batch[0])) {  // gather the small requests already waiting
+            std::lock_guard<std::mutex> lk(s->mu);
+            Request more;
+            while (batch.size() < kSmallBatchMax && pick_small(s, more)) {
+                batch.push_back(std::move(more));
+                ++s->in_flight;
+            }
+        }
+        std::vector<Done> dones;
+        if (small_request(batch[0])) {
+            run_small_batch(s, s->streams[slot], batch, dones);
+        } else {
+            dones.resize(1);
+            dones[0].c.ticket = batch[0].ticket;
+            run_request(s, s->streams[slot], batch[0], dones[0]);
+        }
         const auto finished = Clock::now();
-        d.c.queue_seconds = std::chrono::duration<double>(admitted - r.submitted).count();
-        d.c.latency_seconds = std::chrono::duration<double>(finished - r.submitted).count();
+        for (size_t i = 0; i < batch.size(); ++i) {
+            dones[i].c.queue_seconds = std::chrono::duration<double>(admitted - batch[i].submitted).count();
+            dones[i].c.latency_seconds = std::chrono::duration<double>(finished - batch[i].submitted).count();
+        }
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            s->held -= r.bytes;
-            if (s->ledger_release != nullptr) s->ledger_release(s->ledger_user, r.bytes);
-            --s->in_flight;
-            s->done.push_back(std::move(d));
+            for (size_t i = 0; i < batch.size(); ++i) {
+                s->held -= batch[i].bytes;
+                if (s->ledger_release != nullptr) s->ledger_release(s->ledger_user, batch[i].bytes);
+                --s->in_flight;
+                s->done.push_back(std::move(dones[i]));
+            }
         }
         s->cv_done.notify_all();
         s->cv_work.notify_all();  // memory freed: others may fit now

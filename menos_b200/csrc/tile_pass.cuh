@@ -428,12 +428,15 @@ __device__ __forceinline__ void compute_tile(double2* __restrict__ tile, const u
 // amplitudes.  A tile's base index is its number deposited on the bits
 // outside the tile (nmask); moving gridDim.x tiles on is the masked add
 // ((base | ~nmask) + step) & nmask, step = deposit(gridDim.x).
-template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
-__global__ void __launch_bounds__(MAXT, MINB)
-    k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask, uint64_t gmask,
-                const uint32_t* __restrict__ words, uint32_t nwords, const double* __restrict__ sdata,
-                uint32_t nsdata, const double* __restrict__ gdata, uint64_t ntiles, const double* __restrict__ pdata,
-                uint32_t pstride, uint32_t param_lo, uint32_t param_len, uint32_t bshift, uint32_t stages) {
+// The pass over this CTA's share of the tiles: tiles cta, cta + nctas, ...
+template <int MT, typename IDX, bool FULL>
+__device__ __forceinline__ void tile_pass_body(double2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask,
+                                               uint64_t gmask, const uint32_t* __restrict__ words, uint32_t nwords,
+                                               const double* __restrict__ sdata, uint32_t nsdata,
+                                               const double* __restrict__ gdata, uint64_t ntiles,
+                                               const double* __restrict__ pdata, uint32_t pstride, uint32_t param_lo,
+                                               uint32_t param_len, uint32_t bshift, uint32_t stages, uint32_t cta,
+                                               uint32_t nctas) {
     extern __shared__ double2 smem_tiles[];
     const uint32_t m = MT > 0 ? static_cast<uint32_t>(MT) : m_rt;
     const uint32_t tid = threadIdx.x;
@@ -468,7 +471,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
     const uint64_t nmask64 = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~smask;
     const IDX nmask = static_cast<IDX>(nmask64);
-    const IDX step = static_cast<IDX>(pdep64(gridDim.x, nmask64));
+    const IDX step = static_cast<IDX>(pdep64(nctas, nmask64));
     auto advance = [&](IDX b) -> IDX { return ((b | ~nmask) + step) & nmask; };
     // Amplitude (tid, j) of the canonical mapping: global index base +
     // off_lo + the register bits of j (disjoint bit sets, so + is |);
@@ -489,21 +492,21 @@ __global__ void __launch_bounds__(MAXT, MINB)
     // `stages` tile buffers: the tiles `stages - 1` ahead are in flight
     // while this one is computed (one commit group per tile, empty groups
     // past the end keep the count uniform).
-    uint64_t tp = blockIdx.x;  // next tile to prefetch
-    IDX pbase = static_cast<IDX>(pdep64(blockIdx.x, nmask64));
+    uint64_t tp = cta;  // next tile to prefetch
+    IDX pbase = static_cast<IDX>(pdep64(cta, nmask64));
     IDX cbase = pbase;  // base of the tile being computed
     for (uint32_t sg = 0; sg + 1 < stages; ++sg) {
         if (tp < ntiles) prefetch(pbase, smem_tiles + sg * tile_amps);
         else cp_async_commit();
-        tp += gridDim.x;
+        tp += nctas;
         pbase = advance(pbase);
     }
     uint32_t cur = 0, nxt = stages - 1;  // buffer of this tile, of the next prefetch
-    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (uint64_t t = cta; t < ntiles; t += nctas) {
         double2* tile = smem_tiles + cur * tile_amps;
         if (tp < ntiles) prefetch(pbase, smem_tiles + nxt * tile_amps);
         else cp_async_commit();
-        tp += gridDim.x;
+        tp += nctas;
         pbase = advance(pbase);
         cur = cur + 1 == stages ? 0u : cur + 1;
         nxt = nxt + 1 == stages ? 0u : nxt + 1;
@@ -533,6 +536,33 @@ __global__ void __launch_bounds__(MAXT, MINB)
         cbase = advance(cbase);
         __syncthreads();  // the buffer is the target of a later prefetch
     }
+}
+
+template <int MAXT, int MINB, int MT, typename IDX, bool FULL>
+__global__ void __launch_bounds__(MAXT, MINB)
+    k_tile_pass(double2* __restrict__ st, uint32_t n, uint32_t m_rt, uint64_t smask, uint64_t gmask,
+                const uint32_t* __restrict__ words, uint32_t nwords, const double* __restrict__ sdata,
+                uint32_t nsdata, const double* __restrict__ gdata, uint64_t ntiles, const double* __restrict__ pdata,
+                uint32_t pstride, uint32_t param_lo, uint32_t param_len, uint32_t bshift, uint32_t stages) {
+    tile_pass_body<MT, IDX, FULL>(st, n, m_rt, smask, gmask, words, nwords, sdata, nsdata, gdata, ntiles, pdata,
+                                  pstride, param_lo, param_len, bshift, stages, blockIdx.x, gridDim.x);
+}
+
+// Many states' passes in one launch (small states, one tile width): CTAs
+// [jobs[j].cta_begin, jobs[j + 1].cta_begin) run job j's pass over its state.
+template <int MAXT, int MT, bool FULL>
+__global__ void __launch_bounds__(MAXT, 1) k_tile_pass_jobs(const TileJob* __restrict__ jobs, uint32_t njobs,
+                                                           uint32_t m_rt) {
+    uint32_t lo = 0, hi = njobs;  // the last job whose cta_begin <= blockIdx.x
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (jobs[mid].cta_begin <= blockIdx.x) lo = mid;
+        else hi = mid;
+    }
+    const TileJob& J = jobs[lo];
+    tile_pass_body<MT, uint64_t, FULL>(static_cast<double2*>(J.st), J.n, m_rt, J.smask, J.gmask, J.words, J.nwords, J.sdata, J.nsdata,
+                                       J.gdata, J.ntiles, nullptr, 0, 0, 0, 0, 2, blockIdx.x - J.cta_begin,
+                                       J.nctas);
 }
 
 // Launches one instance; the shared-memory limit is raised once per instance.

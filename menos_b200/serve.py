@@ -10,7 +10,7 @@ import numpy as np
 from . import _lib
 from ._lib import OUT_COUNTS, OUT_EXPECTATION, Completion, Request, ServerOptions, check, lib
 from .circuit import Circuit, to_mb2_ops
-from .engine import Context
+from .engine import Context, Counts
 
 
 class Server:
@@ -50,7 +50,9 @@ class Server:
         return ticket.value
 
     def poll(self, timeout_ms: int = 100, capacity: int = 256):
-        """Completed requests as dicts (ticket, status, value, counts, queue_s, latency_s)."""
+        """Completed requests as dicts (ticket, status, value, counts, queue_s,
+        latency_s); counts as a Counts mapping over numpy arrays (copied out
+        of the completion before it is released, no per-outcome objects)."""
         buf = (Completion * capacity)()
         n = C.c_uint32()
         rc = lib().mb2_server_poll(self.h, buf, capacity, C.byref(n), timeout_ms)
@@ -59,7 +61,9 @@ class Server:
             c = buf[i]
             counts = None
             if c.num_outcomes:
-                counts = {int(c.outcomes[k]): int(c.counts[k]) for k in range(c.num_outcomes)}
+                k = int(c.num_outcomes)
+                counts = Counts(np.ctypeslib.as_array(c.outcomes, shape=(k,)).copy(),
+                                np.ctypeslib.as_array(c.counts, shape=(k,)).copy())
             out.append({"ticket": c.ticket, "status": c.status, "value": c.value, "counts": counts,
                         "queue_s": c.queue_seconds, "latency_s": c.latency_seconds})
             lib().mb2_server_release(self.h, c.ticket)
