@@ -170,3 +170,20 @@ def test_brick_schedule_pass_count():
     # runs of consecutive blocks (never reordered), diagonals reading qubits
     # outside the tile: ~160 passes instead of one per block (2260 blocks)
     assert passes < 200, passes
+
+
+def test_packed_circuit_is_the_same_op_array():
+    from menos_b200.circuit import PackedCircuit, to_mb2_ops
+    c = workloads.config_c2(n=10, depth=3)
+    c.unitary([1, 4], np.eye(4, dtype=np.complex128))
+    c.measure(2, 0)
+    p = PackedCircuit(c)
+    a, _ = to_mb2_ops(c)
+    b, _ = to_mb2_ops(p)
+    assert len(p) == len(c.ops) and p.num_qubits == c.num_qubits and p.global_phase == c.global_phase
+    assert p.measure_targets() == c.measure_targets()
+    for x, y in zip(a[:len(c.ops)], b[:len(c.ops)]):
+        assert (x.opcode, x.num_qubits, list(x.qubits), list(x.params), x.clbit) == \
+               (y.opcode, y.num_qubits, list(y.qubits), list(y.params), y.clbit)
+        assert bool(x.matrix) == bool(y.matrix)
+    assert to_mb2_ops(p)[0] is b  # packed once, reused
