@@ -129,19 +129,36 @@ __global__ void k_expectation_finish(const double* __restrict__ partials, uint32
 // dimension d.  A tile is a coset of V: 2^d chunks of 2^c contiguous
 // amplitudes (chunk k's high bits are rep ^ span[k]), so for every term the
 // partner m ^ x of each amplitude m is in the same tile, at tile index
-// L ^ dl with dl = (kx << c) | xl.  Each pair is visited once, from the
-// member whose bit hb (the highest bit of dl) is clear.
+// L ^ dl with dl = (kx << c) | xl.
 //
 // With s(m) = (-1)^popcount(z & m) and s(m ^ x) = s(m) (-1)^popcount(z & x),
 // the pair's share t s(m') + conj(t) s(m), t = conj(a_m) a_m', is
 // 2 s(m) Re t when popcount(z & x) is even and -2i s(m) Im t when it is odd,
-// so one real accumulator per term suffices.  s(m) splits over the parts of
-// m: the coset representative (one parity per term and coset), the chunk
-// (a per-term table over the 2^d chunks) and the low c bits.
+// so one real accumulator per term suffices; seen from the other member the
+// same pair gives the same s(m) Re t (or s(m) Im t), so a pair may equally be
+// visited once with weight 2 or from both members with weight 1.
+//
+// Thread r of the CTA owns tile amplitudes L = r | i << 8 (i < 2^(c+d-8),
+// four or eight), read into registers once per tile; per term it visits its
+// own amplitudes and reads only the partners from shared memory.  When dl
+// has a bit b >= 8 the visiting member is the one with bit b clear (half of
+// every thread's amplitudes, weight 2); otherwise every member visits
+// (weight 1).  s(m) is linear over XOR in the tile index apart from the
+// coset representative: s = parity(z_hi & rep) ^ sigma(r) ^ sigma(i << 8),
+// with sigma(L) = parity(z_lo & L) ^ parity(z_hi & span[L >> c]); the
+// thread's sigma(r) of every term is a register bit mask, sigma(i << 8) a
+// per-term byte.  Each term runs a body compiled for its (own count,
+// visiting bit, mode): its products are independent and summed as a
+// balanced tree before one add into the thread's accumulator of the term
+// (in shared memory, so the term loop needs no unrolling).
 // Partial sums go to fixed slots (term, CTA) and are added in CTA order by
 // the finish kernel.
 using GroupTerm = PauliGroupTerm;
 constexpr uint32_t kChunkWords = (1u << kPauliMaxSpan) / 32;
+constexpr uint32_t kOwnShift = 8;  // log2(kThreads): tile bits of the thread index
+constexpr uint32_t kMaxOwn = 1u << (kPauliTileQubits - kOwnShift);
+static_assert(kThreads == (1 << kOwnShift), "one thread per low tile index");
+static_assert(kPauliMinTileQubits >= kOwnShift + 1, "every thread owns at least two amplitudes");
 
 // cp.async of one amplitude (16 or 8 bytes), global -> shared.
 __device__ __forceinline__ void cp_async_amp(double2* smem, const double2* gmem) {
@@ -153,28 +170,60 @@ __device__ __forceinline__ void cp_async_amp(float2* smem, const float2* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
-// Per-group tables in shared memory: the span, each term's low/high parts
-// and mode, and the parity of z_hi & span[k] per chunk k.
+// Per-group tables in shared memory: the span, the parity of z_hi & span[k]
+// per chunk k, per term its partner offset, body, sigma(i << 8) bits and
+// high z bits, and every thread's accumulator of every term.
 struct GroupShared {
     uint64_t sspan[1u << kPauliMaxSpan];
     uint32_t cpar[kMaxGroupTerms][kChunkWords];  // parity of z_hi & span[k], bit k
     uint32_t tdl[kMaxGroupTerms], tzl[kMaxGroupTerms], tmode[kMaxGroupTerms];
+    uint32_t tcode[kMaxGroupTerms];  // the term's body (term_body)
+    uint32_t tsigi[kMaxGroupTerms];  // bit i: sigma(i << 8)
+    uint32_t tweight[kMaxGroupTerms];  // 2: each pair visited once; 1: from both members
     uint64_t tzh[kMaxGroupTerms];
+    double acc[kMaxGroupTerms][kThreads];
     double red[kThreads / 32];
 };
 
-__device__ __forceinline__ void group_setup(GroupShared& g, uint32_t c, uint32_t d, const uint64_t* __restrict__ span,
-                                            const GroupTerm* __restrict__ terms, uint32_t nterms) {
+// sigma(L): the sign parity of tile index L without the coset's part.
+__device__ __forceinline__ uint32_t group_sigma(const GroupShared& g, uint32_t t, uint32_t L, uint32_t c) {
+    const uint32_t k = L >> c;
+    return ((g.cpar[t][k >> 5] >> (k & 31u)) ^ static_cast<uint32_t>(__popc(g.tzl[t] & L))) & 1u;
+}
+
+// Term bodies: (own amplitudes, selector bit, mode).  Code = base of the
+// own count (0 for four, 7 for eight) + 0 for a Z string, else
+// 1 + 2 * (selector bit + 1) + (mode - 1), the selector bit -1 meaning every
+// member visits.
+__host__ __device__ constexpr uint32_t body_code(uint32_t own, int selb, uint32_t mode) {
+    return (own == 8 ? 7u : 0u) + (mode == 0 ? 0u : 1u + 2u * static_cast<uint32_t>(selb + 1) + (mode - 1));
+}
+
+// Fills the tables and clears the accumulators; returns this thread's
+// sigma(r) of every term (bit t).
+__device__ __forceinline__ uint32_t group_setup(GroupShared& g, uint32_t c, uint32_t d,
+                                                const uint64_t* __restrict__ span,
+                                                const GroupTerm* __restrict__ terms, uint32_t nterms) {
     const uint32_t nchunks = 1u << d;
+    const uint32_t own = 1u << (c + d - kOwnShift);
     for (uint32_t i = threadIdx.x; i < nchunks; i += kThreads) g.sspan[i] = span[i];
     for (uint32_t t = threadIdx.x; t < nterms; t += kThreads) {
         const GroupTerm T = terms[t];
-        g.tdl[t] = (T.kx << c) | T.xl;
+        const uint32_t dl = (T.kx << c) | T.xl;
+        g.tdl[t] = dl;
         g.tzl[t] = static_cast<uint32_t>(T.z & ((uint64_t{1} << c) - 1));
         g.tzh[t] = T.z >> c;
         // 0: a Z string (x = 0); 1: real pair sum; 2: imaginary pair sum
-        g.tmode[t] = T.x == 0 ? 0u : ((__popcll(T.x & T.z) & 1) ? 2u : 1u);
+        const uint32_t mode = T.x == 0 ? 0u : ((__popcll(T.x & T.z) & 1) ? 2u : 1u);
+        g.tmode[t] = mode;
+        // The visiting member of a pair: the one whose highest bit of dl
+        // among the register index bits is clear; none there: both visit.
+        const uint32_t hi = dl >> kOwnShift;
+        const int selb = hi == 0 ? -1 : 31 - __clz(hi);
+        g.tcode[t] = body_code(own, mode == 0 ? -1 : selb, mode);
+        g.tweight[t] = (mode != 0 && selb >= 0) ? 2u : 1u;
     }
+    for (uint32_t i = threadIdx.x; i < kMaxGroupTerms * kThreads; i += kThreads) (&g.acc[0][0])[i] = 0.0;
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < kMaxGroupTerms * kChunkWords; i += kThreads) {
         const uint32_t t = i / kChunkWords, w = i % kChunkWords;
@@ -185,82 +234,116 @@ __device__ __forceinline__ void group_setup(GroupShared& g, uint32_t c, uint32_t
         g.cpar[t][w] = bits;
     }
     __syncthreads();
+    for (uint32_t t = threadIdx.x; t < nterms; t += kThreads) {
+        uint32_t bits = 0;
+        for (uint32_t i = 0; i < own; ++i) bits |= group_sigma(g, t, i << kOwnShift, c) << i;
+        g.tsigi[t] = bits;
+    }
+    uint32_t sig = 0;
+    for (uint32_t t = 0; t < nterms; ++t) sig |= group_sigma(g, t, threadIdx.x, c) << t;
+    __syncthreads();
+    return sig;
 }
 
-// Adds one gathered coset tile (representative rep) to every term's two
-// accumulators.
-template <typename A>
-__device__ __forceinline__ void group_tile(const GroupShared& g, const A* __restrict__ cur, uint64_t rep, uint32_t c,
-                                           uint32_t tile_amps, uint32_t nterms, double (&acc0)[kMaxGroupTerms],
-                                           double (&acc1)[kMaxGroupTerms]) {
+// v with its sign flipped when f is 1 (an integer XOR: exact).
+__device__ __forceinline__ double flip_if(double v, uint32_t f) {
+    return __hiloint2double(__double2hiint(v) ^ static_cast<int>(f << 31), __double2loint(v));
+}
+
+// One term's share of this thread's own amplitudes in one tile, as a
+// balanced sum in a fixed order: OWN own amplitudes, SELB the register bit
+// that marks the non-visiting member (-1: all visit), MODE 0 (|a|^2),
+// 1 (Re conj(a) b) or 2 (Im conj(a) b); sg bit i: the sign of own
+// amplitude i.  Every branch is resolved at compile time.
+template <int OWN, int SELB, int MODE, typename A>
+__device__ __forceinline__ double term_body(const double2 (&a)[kMaxOwn], const A* __restrict__ cur, uint32_t r,
+                                            uint32_t dl, uint32_t sg) {
+    constexpr int NV = SELB < 0 ? OWN : OWN / 2;
+    constexpr int SB = SELB < 0 ? 0 : SELB;
+    double v[NV];
 #pragma unroll
-    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
-        if (t < nterms) {
-            const uint32_t dl = g.tdl[t], zl = g.tzl[t], mode = g.tmode[t];
-            const uint32_t rp = static_cast<uint32_t>(__popcll(g.tzh[t] & rep)) & 1u;
-            const uint32_t* cp = g.cpar[t];
-            if (mode == 0) {
-                for (uint32_t L = threadIdx.x; L < tile_amps; L += 2 * kThreads) {
-                    const uint32_t L1 = L + kThreads;
-                    const uint32_t k0 = L >> c, k1 = L1 >> c;
-                    const uint32_t n0 = rp ^ (cp[k0 >> 5] >> (k0 & 31)) ^ __popc(zl & L);
-                    const uint32_t n1 = rp ^ (cp[k1 >> 5] >> (k1 & 31)) ^ __popc(zl & L1);
-                    const double2 a0 = as_d2(cur[L]), a1 = as_d2(cur[L1]);
-                    const double p0 = __dadd_rn(__dmul_rn(a0.x, a0.x), __dmul_rn(a0.y, a0.y));
-                    const double p1 = __dadd_rn(__dmul_rn(a1.x, a1.x), __dmul_rn(a1.y, a1.y));
-                    acc0[t] = (n0 & 1) ? __dsub_rn(acc0[t], p0) : __dadd_rn(acc0[t], p0);
-                    acc1[t] = (n1 & 1) ? __dsub_rn(acc1[t], p1) : __dadd_rn(acc1[t], p1);
-                }
-            } else {
-                const uint32_t hb = 31 - __clz(dl);
-                const uint32_t below = (1u << hb) - 1;
-                for (uint32_t q = threadIdx.x; q < tile_amps / 2; q += 2 * kThreads) {
-                    const uint32_t q1 = q + kThreads;
-                    const uint32_t L0 = ((q & ~below) << 1) | (q & below);
-                    const uint32_t L1 = ((q1 & ~below) << 1) | (q1 & below);
-                    const uint32_t k0 = L0 >> c, k1 = L1 >> c;
-                    const uint32_t n0 = rp ^ (cp[k0 >> 5] >> (k0 & 31)) ^ __popc(zl & L0);
-                    const uint32_t n1 = rp ^ (cp[k1 >> 5] >> (k1 & 31)) ^ __popc(zl & L1);
-                    const double2 a0 = as_d2(cur[L0]), b0 = as_d2(cur[L0 ^ dl]);
-                    const double2 a1 = as_d2(cur[L1]), b1 = as_d2(cur[L1 ^ dl]);
-                    const double v0 = mode == 1 ? __dadd_rn(__dmul_rn(a0.x, b0.x), __dmul_rn(a0.y, b0.y))
-                                                : __dsub_rn(__dmul_rn(a0.x, b0.y), __dmul_rn(a0.y, b0.x));
-                    const double v1 = mode == 1 ? __dadd_rn(__dmul_rn(a1.x, b1.x), __dmul_rn(a1.y, b1.y))
-                                                : __dsub_rn(__dmul_rn(a1.x, b1.y), __dmul_rn(a1.y, b1.x));
-                    acc0[t] = (n0 & 1) ? __dsub_rn(acc0[t], v0) : __dadd_rn(acc0[t], v0);
-                    acc1[t] = (n1 & 1) ? __dsub_rn(acc1[t], v1) : __dadd_rn(acc1[t], v1);
-                }
-            }
+    for (int k = 0; k < NV; ++k) {
+        // The k-th visiting own amplitude: k with a zero inserted at SELB.
+        const int i = SELB < 0 ? k : (((k >> SB) << (SB + 1)) | (k & ((1 << SB) - 1)));
+        double x;
+        if constexpr (MODE == 0) {
+            x = __dadd_rn(__dmul_rn(a[i].x, a[i].x), __dmul_rn(a[i].y, a[i].y));
+        } else {
+            const double2 b = as_d2(cur[(r | (static_cast<uint32_t>(i) << kOwnShift)) ^ dl]);
+            x = MODE == 1 ? __dadd_rn(__dmul_rn(a[i].x, b.x), __dmul_rn(a[i].y, b.y))
+                          : __dsub_rn(__dmul_rn(a[i].x, b.y), __dmul_rn(a[i].y, b.x));
         }
+        v[k] = flip_if(x, (sg >> i) & 1u);
+    }
+#pragma unroll
+    for (int w = 1; w < NV; w <<= 1)
+#pragma unroll
+        for (int j = 0; j + w < NV; j += 2 * w) v[j] = __dadd_rn(v[j], v[j + w]);
+    return v[0];
+}
+
+// Adds one gathered coset tile (representative rep) to every term's
+// accumulator.  sig: this thread's sigma(r) bits (group_setup).
+template <typename A>
+__device__ __forceinline__ void group_tile(GroupShared& g, const A* __restrict__ cur, uint64_t rep,
+                                           uint32_t tile_amps, uint32_t nterms, uint32_t sig) {
+    const uint32_t r = threadIdx.x;
+    const uint32_t own = tile_amps >> kOwnShift;
+    double2 a[kMaxOwn];
+#pragma unroll
+    for (uint32_t i = 0; i < kMaxOwn; ++i)
+        a[i] = i < own ? as_d2(cur[r | (i << kOwnShift)]) : make_double2(0.0, 0.0);
+    for (uint32_t t = 0; t < nterms; ++t) {
+        // Bit i: the sign of own amplitude i.
+        const uint32_t s0 = (static_cast<uint32_t>(__popcll(g.tzh[t] & rep)) ^ (sig >> t)) & 1u;
+        const uint32_t sg = g.tsigi[t] ^ (0u - s0);
+        const uint32_t dl = g.tdl[t];
+        double v = 0.0;
+        switch (g.tcode[t]) {
+            case body_code(4, -1, 0): v = term_body<4, -1, 0>(a, cur, r, dl, sg); break;
+            case body_code(4, -1, 1): v = term_body<4, -1, 1>(a, cur, r, dl, sg); break;
+            case body_code(4, -1, 2): v = term_body<4, -1, 2>(a, cur, r, dl, sg); break;
+            case body_code(4, 0, 1): v = term_body<4, 0, 1>(a, cur, r, dl, sg); break;
+            case body_code(4, 0, 2): v = term_body<4, 0, 2>(a, cur, r, dl, sg); break;
+            case body_code(4, 1, 1): v = term_body<4, 1, 1>(a, cur, r, dl, sg); break;
+            case body_code(4, 1, 2): v = term_body<4, 1, 2>(a, cur, r, dl, sg); break;
+            case body_code(8, -1, 0): v = term_body<8, -1, 0>(a, cur, r, dl, sg); break;
+            case body_code(8, -1, 1): v = term_body<8, -1, 1>(a, cur, r, dl, sg); break;
+            case body_code(8, -1, 2): v = term_body<8, -1, 2>(a, cur, r, dl, sg); break;
+            case body_code(8, 0, 1): v = term_body<8, 0, 1>(a, cur, r, dl, sg); break;
+            case body_code(8, 0, 2): v = term_body<8, 0, 2>(a, cur, r, dl, sg); break;
+            case body_code(8, 1, 1): v = term_body<8, 1, 1>(a, cur, r, dl, sg); break;
+            case body_code(8, 1, 2): v = term_body<8, 1, 2>(a, cur, r, dl, sg); break;
+            case body_code(8, 2, 1): v = term_body<8, 2, 1>(a, cur, r, dl, sg); break;
+            case body_code(8, 2, 2): v = term_body<8, 2, 2>(a, cur, r, dl, sg); break;
+            default: break;
+        }
+        g.acc[t][r] = __dadd_rn(g.acc[t][r], v);
     }
 }
 
-// Per term: this CTA's sum in a fixed order (the two accumulators, lanes,
-// then warps), written to slot_of(t) as (re, im) of the pair sum before the
-// i^popcount(x & z) factor; the accumulators are cleared.
+// Per term: this CTA's sum in a fixed order (lanes, then warps), written to
+// slot_of(t) as (re, im) of the pair sum before the i^popcount(x & z)
+// factor, with the term's visit weight; the accumulators are cleared.
 template <typename SLOT>
 __device__ __forceinline__ void group_write(GroupShared& g, const GroupTerm* __restrict__ terms, uint32_t nterms,
-                                            double (&acc0)[kMaxGroupTerms], double (&acc1)[kMaxGroupTerms],
                                             SLOT slot_of) {
-#pragma unroll
-    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
-        if (t < nterms) {
-            double r = __dadd_rn(acc0[t], acc1[t]);
-            for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
-            __syncthreads();
-            if ((threadIdx.x & 31) == 0) g.red[threadIdx.x >> 5] = r;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double sum = 0.0;
-                for (int w = 0; w < kThreads / 32; ++w) sum += g.red[w];
-                double* p = slot_of(terms[t].out);
-                const uint32_t mode = g.tmode[t];
-                p[0] = mode == 0 ? sum : mode == 1 ? 2.0 * sum : 0.0;
-                p[1] = mode == 2 ? -2.0 * sum : 0.0;
-            }
+    for (uint32_t t = 0; t < nterms; ++t) {
+        double r = g.acc[t][threadIdx.x];
+        g.acc[t][threadIdx.x] = 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) g.red[threadIdx.x >> 5] = r;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sum = 0.0;
+            for (int w = 0; w < kThreads / 32; ++w) sum += g.red[w];
+            double* p = slot_of(terms[t].out);
+            const uint32_t mode = g.tmode[t];
+            const double w = static_cast<double>(g.tweight[t]);
+            p[0] = mode == 0 ? sum : mode == 1 ? w * sum : 0.0;
+            p[1] = mode == 2 ? -w * sum : 0.0;
         }
-        acc0[t] = 0.0;
-        acc1[t] = 0.0;
     }
 }
 
@@ -289,9 +372,7 @@ __device__ __forceinline__ void group_gather(const A* __restrict__ st, uint64_t 
 }
 
 // Cosets are processed with two shared-memory buffers: the next coset's
-// amplitudes are gathered with cp.async while this one is reduced.  Each
-// thread keeps two accumulators per term (alternate pairs) so consecutive
-// adds do not wait on each other.
+// amplitudes are gathered with cp.async while this one is reduced.
 template <typename A>
 __global__ void __launch_bounds__(kThreads, 2)
     k_pauli_group(const A* __restrict__ st, uint32_t c, uint32_t d, const uint64_t* __restrict__ span,
@@ -302,16 +383,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     const uint32_t tile_amps = 1u << (c + d);
     A* buf0 = reinterpret_cast<A*>(gsm);
     A* buf1 = buf0 + tile_amps;
-    group_setup(g, c, d, span, terms, nterms);
+    const uint32_t sig = group_setup(g, c, d, span, terms, nterms);
     // Moving gridDim.x cosets on is a masked add on the free bits.
     const uint64_t rstep = deposit_bits(gridDim.x, free_mask);
     auto advance = [&](uint64_t r) { return ((r | ~free_mask) + rstep) & free_mask; };
-    double acc0[kMaxGroupTerms], acc1[kMaxGroupTerms];
-#pragma unroll
-    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
-        acc0[t] = 0.0;
-        acc1[t] = 0.0;
-    }
     uint64_t rep = deposit_bits(blockIdx.x, free_mask);
     if (blockIdx.x < ncosets) group_gather(st, rep, buf0, g, c, tile_amps);
     A* cur = buf0;
@@ -322,7 +397,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         else asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         __syncthreads();
-        group_tile(g, cur, rep, c, tile_amps, nterms, acc0, acc1);
+        group_tile(g, cur, rep, tile_amps, nterms, sig);
         __syncthreads();  // this buffer is the target of the gather after next
         rep = rep_next;
         A* tmp = cur;
@@ -330,7 +405,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         nxt = tmp;
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    group_write(g, terms, nterms, acc0, acc1, [&](uint32_t out) {
+    group_write(g, terms, nterms, [&](uint32_t out) {
         return partials + 2 * (static_cast<uint64_t>(out) * gridDim.x + blockIdx.x);
     });
 }
@@ -351,7 +426,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const uint32_t tile_amps = 1u << (c + d);
     A* buf0 = reinterpret_cast<A*>(gsm);
     A* buf1 = buf0 + tile_amps;
-    group_setup(g, c, d, span, terms, nterms);
+    const uint32_t sig = group_setup(g, c, d, span, terms, nterms);
     const uint64_t ncosets = uint64_t{1} << (n - c - d);
     const uint32_t slot = blockIdx.x % per;
     const uint64_t b0 = blockIdx.x / per, bstep = gridDim.x / per;
@@ -360,14 +435,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     // item f = (binding b0 + (f / mine) * bstep, coset slot + (f % mine) * per).
     const uint64_t mine = ncosets > slot ? (ncosets - slot + per - 1) / per : 0;
     const uint64_t nb = (bindings - b0 + bstep - 1) / bstep;
-    double acc0[kMaxGroupTerms], acc1[kMaxGroupTerms];
-#pragma unroll
-    for (uint32_t t = 0; t < kMaxGroupTerms; ++t) {
-        acc0[t] = 0.0;
-        acc1[t] = 0.0;
-    }
     auto write = [&](uint64_t b) {
-        group_write(g, terms, nterms, acc0, acc1, [&](uint32_t out) {
+        group_write(g, terms, nterms, [&](uint32_t out) {
             return partials + 2 * ((static_cast<uint64_t>(out) * bindings + b) * per + slot);
         });
     };
@@ -395,7 +464,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         }
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
         __syncthreads();
-        group_tile(g, cur, rep, c, tile_amps, nterms, acc0, acc1);
+        group_tile(g, cur, rep, tile_amps, nterms, sig);
         __syncthreads();  // this buffer is the target of the gather after next
         if ((f + 1) % mine == 0) write(b);
         b = bn;
