@@ -12,13 +12,13 @@
 //   splits its row (32 floats, interleaved re/im) into FP16 high and low
 //   parts and stores both into tensor memory (TMEM lane =
 //   row within a 128-row block, two FP16 values per 32-bit column); one
-//   thread issues, per 128-row block, tcgen05.mma kind::f16 with A from
-//   tensor memory and B = 2^12 U's operand in shared memory (FP16 high parts
-//   over low parts, N = 64): A_hi x [B_hi; B_lo] into 64 FP32 accumulator columns,
-//   then A_lo x B_hi accumulated into the first 32 (two K-steps of 16 each);
-//   tcgen05.commit signals an mbarrier the issuing thread waits on; after a
-//   CTA barrier every thread reads its row back (tcgen05.ld), adds the two
-//   32-column halves, takes out the 2^12 and applies the phase's elementwise
+//   thread issues, per 128-row block, six tcgen05.mma kind::f16 (N = 32,
+//   two K-steps of 16 each) with A from tensor memory and B = 2^12 U's
+//   operand in shared memory (FP16 high parts over low parts):
+//   A_lo x B_hi, A_hi x B_lo, then A_hi x B_hi, all accumulated into one
+//   block of 32 FP32 columns; tcgen05.commit signals an mbarrier the issuing
+//   thread waits on; after a CTA barrier every thread reads its row back
+//   (one tcgen05.ld), takes out the 2^12 and applies the phase's elementwise
 //   diagonals on registers.
 //
 // Every wait on the tensor core is bounded: a wait that runs out sets the
@@ -125,12 +125,24 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 
 __device__ __forceinline__ uint32_t half2_bits(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 
-// tcgen05.mma kind::f16 instruction descriptors: D FP32 (bits 4-5 = 1),
+// tcgen05.mma kind::f16 instruction descriptor: D FP32 (bits 4-5 = 1),
 // A and B FP16 (bits 7-9, 10-12 = 0), both K-major, N >> 3 at bit 17,
-// M >> 4 at bit 24; M = 128 rows, N = 64 (the stacked high and low parts of
-// U's 32 output rows) or N = 32 (the high parts only).
-constexpr uint32_t kIdescN64 = (1u << 4) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// M >> 4 at bit 24; M = 128 rows, N = 32 (U's 32 real output rows: their
+// high parts at the operand's start, their low parts 2048 bytes on).
 constexpr uint32_t kIdescN32 = (1u << 4) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kLowPartBytes = 2048;  // 4 row groups of 512 bytes
+
+// Packed FP32 pairs (sm_100a f32x2): one instruction for both parts.
+__device__ __forceinline__ float2 sub_f32x2(float2 a, float2 b) {
+    uint64_t r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(*reinterpret_cast<uint64_t*>(&a)), "l"(*reinterpret_cast<uint64_t*>(&b)));
+    return *reinterpret_cast<float2*>(&r);
+}
+__device__ __forceinline__ float2 mul_f32x2(float2 a, float2 b) {
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(*reinterpret_cast<uint64_t*>(&a)), "l"(*reinterpret_cast<uint64_t*>(&b)));
+    return *reinterpret_cast<float2*>(&r);
+}
 // Shared-memory descriptor of B: start address >> 4 (bits 0-13), leading
 // (K) byte offset 128 >> 4 (bits 16-29), stride (N) byte offset 512 >> 4
 // (bits 32-45), descriptor version 1 (bits 46-47), no swizzle (bits 61-63 = 0).
@@ -174,7 +186,7 @@ __device__ __forceinline__ float pow2f(int e) { return __uint_as_float(static_ca
 // layout of tile_tc.cpp) at shared address b; the row is already scaled
 // into FP16's range (tile_scale_exp).  ROWS threads, ROWS / 128 row blocks;
 // TMEM columns: [0, 16 NB) high parts, [16 NB, 32 NB) low parts,
-// [32 NB, 96 NB) the products (64 per block).  All threads of the CTA call
+// [32 NB, 64 NB) the products (32 per block).  All threads of the CTA call
 // it; thread 0 issues the MMAs and waits for them.
 template <int ROWS>
 __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c) {
@@ -187,9 +199,8 @@ __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c)
 #pragma unroll
         for (int j = 0; j < kNA; ++j) {
             const __half2 h = __floats2half2_rn(a[j].x, a[j].y);
-            const float2 hf = __half22float2(h);
             hi[j] = half2_bits(h);
-            lo[j] = half2_bits(__floats2half2_rn(a[j].x - hf.x, a[j].y - hf.y));
+            lo[j] = half2_bits(__float22half2_rn(sub_f32x2(a[j], __half22float2(h))));
         }
         tmem_st16(c.tmem + lane + 16 * blk, hi);
         tmem_st16(c.tmem + lane + 16 * NB + 16 * blk, lo);
@@ -200,14 +211,18 @@ __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c)
     const bool abort = *c.abort != 0;
     if (!abort && tid == 0) {
         tc_fence_after();
-        const uint64_t d0 = b_desc(b), d1 = b_desc(b + 256);
+        const uint64_t bh0 = b_desc(b), bh1 = b_desc(b + 256);
+        const uint64_t bl0 = b_desc(b + kLowPartBytes), bl1 = b_desc(b + kLowPartBytes + 256);
 #pragma unroll
         for (uint32_t k = 0; k < NB; ++k) {
-            const uint32_t ah = c.tmem + 16 * k, al = c.tmem + 16 * NB + 16 * k, d = c.tmem + 32 * NB + 64 * k;
-            mma_f16(d, ah, d0, kIdescN64, 0);
-            mma_f16(d, ah + 8, d1, kIdescN64, 1);
-            mma_f16(d, al, d0, kIdescN32, 1);
-            mma_f16(d, al + 8, d1, kIdescN32, 1);
+            const uint32_t ah = c.tmem + 16 * k, al = c.tmem + 16 * NB + 16 * k, d = c.tmem + 32 * NB + 32 * k;
+            // The small products first, the high-by-high product last.
+            mma_f16(d, al, bh0, kIdescN32, 0);
+            mma_f16(d, al + 8, bh1, kIdescN32, 1);
+            mma_f16(d, ah, bl0, kIdescN32, 1);
+            mma_f16(d, ah + 8, bl1, kIdescN32, 1);
+            mma_f16(d, ah, bh0, kIdescN32, 1);
+            mma_f16(d, ah + 8, bh1, kIdescN32, 1);
         }
         mma_commit(c.bar);
         if (!mbar_wait(c.bar, c.parity)) {
@@ -219,15 +234,14 @@ __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c)
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    uint32_t v0[32], v1[32];
-    tmem_ld32(c.tmem + lane + 32 * NB + 64 * blk, v0);
-    tmem_ld32(c.tmem + lane + 32 * NB + 64 * blk + 32, v1);
+    uint32_t v[32];
+    tmem_ld32(c.tmem + lane + 32 * NB + 32 * blk, v);
     tmem_wait_ld();
     constexpr float kUnscale = static_cast<float>(1.0 / kTcOperandScale);
 #pragma unroll
     for (int j = 0; j < kNA; ++j)
-        a[j] = make_float2((__uint_as_float(v0[2 * j]) + __uint_as_float(v1[2 * j])) * kUnscale,
-                           (__uint_as_float(v0[2 * j + 1]) + __uint_as_float(v1[2 * j + 1])) * kUnscale);
+        a[j] = mul_f32x2(make_float2(__uint_as_float(v[2 * j]), __uint_as_float(v[2 * j + 1])),
+                         make_float2(kUnscale, kUnscale));
 }
 
 // Sets up TMEM (warp 0), the mbarrier and the abort flag; the caller's
