@@ -74,7 +74,10 @@ typedef struct mb2_op {
     uint32_t num_qubits;                 /* operands used in qubits[] */
     uint32_t qubits[MB2_MAX_OP_QUBITS];  /* operand j = matrix bit j */
     double params[3];                    /* gate parameters (RX/RY/RZ/P/CP/RZZ: 1, U: 3) */
-    const double* matrix;                /* MB2_UNITARY: 2*4^k doubles, row-major (re, im); else NULL */
+    const double* matrix;                /* MB2_UNITARY: 2*4^k doubles, row-major (re, im);
+                                            MB2_MEASURE: NULL, or its readout error as 4 doubles,
+                                            P(recorded r | true t) at 2t + r (the reference's
+                                            ReadoutError, include/menos/circuit.h:67-77); else NULL */
     uint32_t clbit;                      /* MB2_MEASURE: classical bit written */
     uint32_t reserved;
 } mb2_op;
@@ -272,12 +275,25 @@ int mb2_synchronize(mb2_state* state);
  * counts by the reference's sort-then-walk over rho's diagonal (identical
  * counts); outcomes as mb2_sample's.  n <= 15; channels of 1..5 qubits (4- and
  * 5-qubit ones run as 8- and 10-operand blocks from global memory).
- * MeasureOps carry no readout error across this ABI. */
+ * Readout errors: mb2_dm_sample_readout below. */
 int mb2_dm_apply_program(mb2_state* rho, uint32_t num_qubits, const mb2_op* ops, uint32_t num_ops);
 int mb2_dm_expectation(mb2_state* rho, uint32_t num_qubits, const uint64_t* x_masks, const uint64_t* z_masks,
                        uint32_t num_terms, double* out);
 int mb2_dm_sample(mb2_state* rho, uint32_t num_qubits, uint64_t shots, uint64_t seed, const uint32_t* targets,
                   uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes);
+/* mb2_dm_sample with the readout errors of the circuit's measurements: each
+ * target's error is that of the last MB2_MEASURE in ops writing its clbit
+ * (readout_targets, src/engines/noise/readout.cpp).  Without any, exactly
+ * mb2_dm_sample.  With some, the reference's per-shot draws
+ * (density_matrix_engine.cpp:378-390): from common::Rng(seed), one word per
+ * shot for the true outcome -- the first basis state whose sequential
+ * cumulative probability exceeds its uniform, found on the device -- then
+ * one word per readout-errored target in target order, the bit flipping
+ * when its uniform is below P(recorded != true | true) (apply_readout).
+ * Identical counts. */
+int mb2_dm_sample_readout(mb2_state* rho, uint32_t num_qubits, const mb2_op* ops, uint32_t num_ops, uint64_t shots,
+                          uint64_t seed, const uint32_t* targets, uint32_t num_targets, uint64_t* outcomes,
+                          uint64_t* counts, uint64_t* num_outcomes);
 
 /* The reference's sequential FP64 sum of |a_i|^2 over the state, bit for bit
  * (the exact device chain of mb2_sample), e.g. to renormalise as the
@@ -297,8 +313,10 @@ int mb2_norm_exact(mb2_state* state, double* out);
  * Expectation (num_terms > 0; coefs: complex, 2 doubles each): term_means
  * (2 * num_terms doubles, the mean of <P_t> over trajectories) and the
  * standard error of sum_t coef_t <P_t>.  Counts (shots <= trajectories): one
- * draw per trajectory t < shots, after its channel draws, by the exact walk;
- * outcomes as mb2_sample's.  Readout errors are not carried. */
+ * draw per trajectory t < shots, after its channel draws, by the exact walk,
+ * then one word per readout-errored target (the errors of the MB2_MEASURE
+ * ops, as mb2_dm_sample_readout; trajectory_engine.cpp:463-472); outcomes
+ * as mb2_sample's. */
 int mb2_trajectories(mb2_context* ctx, uint32_t num_qubits, const mb2_op* ops, uint32_t num_ops,
                      uint64_t trajectories, uint64_t seed, const uint64_t* x_masks, const uint64_t* z_masks,
                      const double* coefs, uint32_t num_terms, double* term_means, double* standard_error,

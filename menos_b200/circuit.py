@@ -66,8 +66,17 @@ class Circuit:
         self.ops.append((OP["channel"], qs, (), m, 0))
         return self
 
-    def measure(self, qubit: int, clbit: int) -> "Circuit":
-        self.ops.append((OP["measure"], (int(qubit),), (), None, int(clbit)))
+    def measure(self, qubit: int, clbit: int, readout=None) -> "Circuit":
+        """readout: the measurement's readout error, P(recorded r | true t)
+        as a 2x2 array [t][r] (or its 4 entries in that order), as the
+        reference's ReadoutError; the density-matrix and trajectory samplers
+        record the bit through it."""
+        m = None
+        if readout is not None:
+            m = np.ascontiguousarray(np.asarray(readout, dtype=np.float64).ravel())
+            if m.size != 4 or not np.all((m >= 0.0) & (m <= 1.0)):
+                raise ValueError("a readout error is 4 probabilities P(recorded r | true t) at 2t + r")
+        self.ops.append((OP["measure"], (int(qubit),), (), m, int(clbit)))
         self.num_clbits = max(self.num_clbits, int(clbit) + 1)
         return self
 

@@ -1058,6 +1058,72 @@ uint64_t trajectory_seed(uint64_t base_seed, uint64_t t) {
 
 double word_to_uniform(uint64_t w) { return static_cast<double>(w >> 11) * 0x1.0p-53; }
 
+// A measure target's readout error (the reference's ReadoutTarget,
+// src/engines/noise/readout.h): its clbit and P(recorded r | true t) at 2t + r.
+struct Readout {
+    uint32_t clbit;
+    double a[4];
+};
+
+// readout_targets (src/engines/noise/readout.cpp): per measure target, in
+// target order, the readout error of the last MB2_MEASURE writing its clbit,
+// when that measurement has one.
+std::vector<Readout> readout_targets(const mb2_op* ops, uint32_t num_ops, const uint32_t* targets,
+                                     uint32_t num_targets) {
+    std::vector<Readout> out;
+    for (uint32_t t = 0; t < num_targets; ++t) {
+        const uint32_t clbit = targets[2 * t + 1];
+        const double* err = nullptr;
+        for (uint32_t i = 0; i < num_ops; ++i)
+            if (ops[i].opcode == MB2_MEASURE && ops[i].clbit == clbit) err = ops[i].matrix;
+        if (err != nullptr) out.push_back(Readout{clbit, {err[0], err[1], err[2], err[3]}});
+    }
+    return out;
+}
+
+bool readouts_valid(const std::vector<Readout>& rs) {
+    for (const Readout& r : rs)
+        for (double v : r.a)
+            if (!(v >= 0.0 && v <= 1.0)) return false;
+    return true;
+}
+
+// apply_readout: one uniform per readout-errored target, in order; the bit
+// flips when the uniform is below P(recorded != true | true).
+void apply_readout(uint64_t& outcome, const std::vector<Readout>& rs, std::mt19937_64& rng) {
+    for (const Readout& r : rs) {
+        const bool truth = ((outcome >> r.clbit) & 1u) != 0;
+        const double flip = truth ? r.a[2] : r.a[1];
+        if (word_to_uniform(rng()) < flip) outcome ^= uint64_t{1} << r.clbit;
+    }
+}
+
+// The outcome word of a basis index: bit clbit set when the target's qubit is.
+uint64_t outcome_word(uint64_t basis, const uint32_t* targets, uint32_t num_targets) {
+    uint64_t o = 0;
+    for (uint32_t t = 0; t < num_targets; ++t)
+        if ((basis >> targets[2 * t]) & 1u) o |= uint64_t{1} << targets[2 * t + 1];
+    return o;
+}
+
+// Ascending distinct outcomes with their counts.
+int histogram_words(mb2_context* ctx, std::vector<uint64_t> words, uint64_t* outcomes, uint64_t* counts,
+                    uint64_t* num_outcomes) {
+    std::sort(words.begin(), words.end());
+    uint64_t d = 0;
+    for (size_t i = 0; i < words.size();) {
+        size_t j = i + 1;
+        while (j < words.size() && words[j] == words[i]) ++j;
+        if (d >= *num_outcomes) return fail(ctx, MB2_ERR_INVALID, "outcome capacity too small");
+        outcomes[d] = words[i];
+        counts[d] = j - i;
+        ++d;
+        i = j;
+    }
+    *num_outcomes = d;
+    return MB2_OK;
+}
+
 struct TrajChannel {
     std::vector<uint32_t> qubits;
     std::vector<std::vector<mb2::Cd>> kraus;     // each dim x dim, row-major
@@ -1145,6 +1211,9 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
     } catch (const std::exception& e) {
         return fail(ctx, MB2_ERR_INVALID, e.what());
     }
+    const std::vector<Readout> readouts =
+        want_counts ? readout_targets(ops, num_ops, targets, num_targets) : std::vector<Readout>{};
+    if (!readouts_valid(readouts)) return fail(ctx, MB2_ERR_INVALID, "readout error entries must lie in [0, 1]");
     mb2_state* st = nullptr;
     if (int e = mb2_state_alloc(ctx, n, MB2_C128, ~uint64_t{0}, &st); e != MB2_OK) return e;
     struct Free {
@@ -1157,7 +1226,7 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
     uint64_t count = 0;  // Welford (trajectory_engine.cpp:244-265)
     mb2::Cd mean{0.0, 0.0};
     double ssd = 0.0;
-    std::vector<uint64_t> shot_basis;
+    std::vector<uint64_t> shot_words;
     for (uint64_t t = 0; t < trajectories; ++t) {
         std::mt19937_64 rng(trajectory_seed(seed, t));
         if (int e = mb2_init(st, 0.0); e != MB2_OK) return e;  // |0..0>, no global phase
@@ -1233,10 +1302,14 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
             ssd += (std::conj(delta) * (x - mean)).real();
         }
         if (want_counts && t < shots) {
+            // One word for the shot, then one per readout-errored target
+            // (trajectory_engine.cpp:465-471).
             const double u = word_to_uniform(rng());
             uint64_t b = 0;
             if (int e = mb2_sample_basis(st, &u, 1, &b); e != MB2_OK) return e;
-            shot_basis.push_back(b);
+            uint64_t o = outcome_word(b, targets, num_targets);
+            apply_readout(o, readouts, rng);
+            shot_words.push_back(o);
         }
     }
     if (want_exp) {
@@ -1250,11 +1323,65 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
             *standard_error = std::sqrt(ssd / (cnt - 1.0) / cnt);
         }
     }
-    if (want_counts) {
-        std::sort(shot_basis.begin(), shot_basis.end());
-        return histogram(ctx, n, shot_basis, targets, num_targets, outcomes, counts, num_outcomes);
-    }
+    if (want_counts) return histogram_words(ctx, std::move(shot_words), outcomes, counts, num_outcomes);
     return MB2_OK;
+}
+
+int mb2_dm_sample_readout(mb2_state* rho, uint32_t n, const mb2_op* ops, uint32_t num_ops, uint64_t shots,
+                          uint64_t seed, const uint32_t* targets, uint32_t num_targets, uint64_t* outcomes,
+                          uint64_t* counts, uint64_t* num_outcomes) {
+    if (int e = check_rho(rho, n); e != MB2_OK) return e;
+    if (num_outcomes == nullptr || (ops == nullptr && num_ops != 0) || (targets == nullptr && num_targets != 0))
+        return MB2_ERR_INVALID;
+    for (uint32_t t = 0; t < num_targets; ++t)
+        if (targets[2 * t] >= n || targets[2 * t + 1] >= 64)
+            return fail(rho->ctx, MB2_ERR_INVALID, "measure target out of range");
+    const std::vector<Readout> rs = readout_targets(ops, num_ops, targets, num_targets);
+    if (rs.empty()) return mb2_dm_sample(rho, n, shots, seed, targets, num_targets, outcomes, counts, num_outcomes);
+    if (!readouts_valid(rs)) return fail(rho->ctx, MB2_ERR_INVALID, "readout error entries must lie in [0, 1]");
+    if (shots == 0) {
+        *num_outcomes = 0;
+        return MB2_OK;
+    }
+    if (outcomes == nullptr || counts == nullptr) return MB2_ERR_INVALID;
+    // Per shot, from one generator: the outcome's word, then one word per
+    // readout-errored target (density_matrix_engine.cpp:378-390).
+    const size_t R = rs.size();
+    std::mt19937_64 rng(seed);
+    std::vector<std::pair<double, uint64_t>> draw(shots);  // (uniform, shot)
+    std::vector<uint64_t> flip_words(shots * R);
+    for (uint64_t i = 0; i < shots; ++i) {
+        draw[i] = {word_to_uniform(rng()), i};
+        for (size_t r = 0; r < R; ++r) flip_words[i * R + r] = rng();
+    }
+    // Each shot's basis state is the first whose sequential cumulative
+    // probability exceeds its uniform (CumulativeDistribution::sample_one):
+    // the device walk takes the uniforms sorted.
+    std::sort(draw.begin(), draw.end());
+    std::vector<double> u(shots);
+    for (uint64_t i = 0; i < shots; ++i) u[i] = draw[i].first;
+    const size_t al_u = (shots * 8 + 255) & ~size_t{255};
+    if (int e = ensure_scratch(rho, 2 * al_u); e != MB2_OK) return e;
+    auto* base = static_cast<unsigned char*>(rho->scratch);
+    MB2_CUDA(rho->ctx, cudaMemcpyAsync(base, u.data(), shots * 8, cudaMemcpyHostToDevice, rho->stream));
+    const int rc = mb2::launch_dm_walk(rho->amps, n, reinterpret_cast<const double*>(base), shots,
+                                       reinterpret_cast<uint64_t*>(base + al_u), rho->stream);
+    if (rc != MB2_OK) return fail(rho->ctx, rc, std::string("walk launch: ") + mb2::last_cuda_error_string());
+    std::vector<uint64_t> basis(shots);
+    MB2_CUDA(rho->ctx, cudaMemcpyAsync(basis.data(), base + al_u, shots * 8, cudaMemcpyDeviceToHost, rho->stream));
+    MB2_CUDA(rho->ctx, cudaStreamSynchronize(rho->stream));
+    std::vector<uint64_t> words(shots);
+    for (uint64_t i = 0; i < shots; ++i) {
+        const uint64_t shot = draw[i].second;
+        uint64_t o = outcome_word(basis[i], targets, num_targets);
+        for (size_t r = 0; r < R; ++r) {
+            const bool truth = ((o >> rs[r].clbit) & 1u) != 0;
+            if (word_to_uniform(flip_words[shot * R + r]) < (truth ? rs[r].a[2] : rs[r].a[1]))
+                o ^= uint64_t{1} << rs[r].clbit;
+        }
+        words[i] = o;
+    }
+    return histogram_words(rho->ctx, std::move(words), outcomes, counts, num_outcomes);
 }
 
 int mb2_copy_out(mb2_state* s, void* host, uint64_t num_amplitudes) {

@@ -321,15 +321,26 @@ class DensityMatrix:
                                            out.ctypes.data), "mb2_dm_expectation")
         return out.view(np.complex128).copy()
 
-    def sample(self, shots: int, seed: int, targets) -> "Counts":
+    def sample(self, shots: int, seed: int, targets, circuit: Circuit | None = None) -> "Counts":
+        """Counts of rho's diagonal (the reference's samplers).  circuit:
+        the measurements whose readout errors record the bits (the last
+        measurement of each target's clbit, mb2_dm_sample_readout)."""
         t = np.ascontiguousarray(np.asarray(targets, np.uint32).ravel())
         cap = max(int(shots), 1)
         outc = np.zeros(cap, np.uint64)
         cnt = np.zeros(cap, np.uint64)
         nout = C.c_uint64(cap)
-        self._chk(lib().mb2_dm_sample(self.state.h, self.n, shots, seed, t.ctypes.data if len(t) else None,
-                                      len(t) // 2, outc.ctypes.data, cnt.ctypes.data, C.byref(nout)),
-                  "mb2_dm_sample")
+        if circuit is not None:
+            arr, keep = to_mb2_ops(circuit)
+            self._chk(lib().mb2_dm_sample_readout(self.state.h, self.n, arr, len(circuit.ops), shots, seed,
+                                                  t.ctypes.data if len(t) else None, len(t) // 2,
+                                                  outc.ctypes.data, cnt.ctypes.data, C.byref(nout)),
+                      "mb2_dm_sample_readout")
+            del keep
+        else:
+            self._chk(lib().mb2_dm_sample(self.state.h, self.n, shots, seed, t.ctypes.data if len(t) else None,
+                                          len(t) // 2, outc.ctypes.data, cnt.ctypes.data, C.byref(nout)),
+                      "mb2_dm_sample")
         d = nout.value
         return Counts(outc[:d].copy(), cnt[:d].copy())
 

@@ -57,8 +57,10 @@ class Circuit:
         self.ops.append((OP["unitary"], tuple(int(q) for q in qubits), (), m, 0))
         return self
 
-    def measure(self, qubit: int, clbit: int):
-        self.ops.append((OP["measure"], (int(qubit),), (), None, int(clbit)))
+    def measure(self, qubit: int, clbit: int, readout=None):
+        """readout: P(recorded r | true t) at 2t + r (the reference's ReadoutError)."""
+        m = None if readout is None else np.ascontiguousarray(np.asarray(readout, np.float64).ravel())
+        self.ops.append((OP["measure"], (int(qubit),), (), m, int(clbit)))
         return self
 
     def channel(self, qubits, kraus):
@@ -86,7 +88,7 @@ def arrays(circ):
         nq[i] = len(qs)
         qubits[6 * i:6 * i + len(qs)] = qs
         params[3 * i:3 * i + len(ps)] = ps
-        if m is not None:
+        if m is not None and oc != OP["measure"]:  # a measurement's readout error is not a matrix here
             mats.append(m.view(np.float64).ravel())
     matrices = np.ascontiguousarray(np.concatenate(mats)) if mats else np.zeros(1, np.float64)
     return n, opcode, nq, qubits, params, matrices

@@ -63,7 +63,11 @@ std::span<const C> as_cspan(const double* p, std::uint64_t n) {
 
 menos::Operation to_operation(const mb2_op& op) {
     if (op.opcode == MB2_MEASURE) {
-        return menos::MeasureOp{op.qubits[0], op.clbit};
+        menos::MeasureOp m{op.qubits[0], op.clbit};
+        if (op.matrix != nullptr) {
+            m.readout_error = menos::ReadoutError{{op.matrix[0], op.matrix[1], op.matrix[2], op.matrix[3]}};
+        }
+        return m;
     }
     std::vector<menos::QubitId> qubits(op.qubits, op.qubits + op.num_qubits);
     if (op.opcode == MB2_CHANNEL) {

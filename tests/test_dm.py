@@ -216,6 +216,95 @@ def test_reference_dm_counts_follow_the_diagonal(ref):
         assert abs(cnt / shots - p[key]) < 5 * np.sqrt(p[key] / shots) + 1e-3
 
 
+def with_readout_measures(circs, n, rng):
+    """Appends measurements of every qubit q into clbit n-1-q to each circuit,
+    most with a readout error; clbit n-1 is written twice and the later
+    measurement (the one that counts) carries none when n > 1."""
+    errs = {}
+    for q in range(n):
+        if q == 0 and n > 1:
+            errs[q] = None
+        else:
+            e0, e1 = float(rng.uniform(0.02, 0.3)), float(rng.uniform(0.02, 0.3))
+            errs[q] = [1.0 - e0, e0, e1, 1.0 - e1]
+    for c in circs:
+        if n > 1:
+            c.measure(0, n - 1, readout=[0.5, 0.5, 0.5, 0.5])  # overwritten below
+        for q in range(n):
+            c.measure(q, n - 1 - q, readout=errs[q])
+    return [(q, n - 1 - q) for q in range(n)]
+
+
+def restated_readout_counts(ref, circ, shots, seed, targets):
+    """The reference's density-matrix counts with readout errors
+    (density_matrix_engine.cpp:378-390, src/engines/noise/readout.cpp):
+    per shot, one uniform for the true outcome -- the first basis state
+    whose sequential cumulative probability exceeds it -- then one per
+    readout-errored target, the bit flipping when the uniform is below
+    P(recorded != true | true)."""
+    import bisect
+    n = circ.num_qubits
+    vec = reference_rho_vector(ref, circ)
+    cum, acc = [], 0.0
+    for x in range(1 << n):
+        acc += vec[x | (x << n)].real
+        cum.append(acc)
+    readouts = []
+    for _q, cl in targets:
+        err = None
+        for oc, _qs, _ps, m, c2 in circ.ops:
+            if oc == pyoracle.OP["measure"] and c2 == cl:
+                err = m
+        if err is not None:
+            readouts.append((cl, err))
+    u = iter(ref.uniforms(seed, shots * (1 + len(readouts))))
+    counts = {}
+    for _ in range(shots):
+        idx = min(bisect.bisect_right(cum, next(u)), len(cum) - 1)
+        o = 0
+        for q, cl in targets:
+            if (idx >> q) & 1:
+                o |= 1 << cl
+        for cl, a in readouts:
+            truth = (o >> cl) & 1
+            if next(u) < (a[2] if truth else a[1]):
+                o ^= 1 << cl
+        counts[o] = counts.get(o, 0) + 1
+    return counts
+
+
+@pytest.mark.parametrize("n", [1, 3])
+def test_reference_readout_counts_follow_the_restated_rule(ref, n):
+    rng = np.random.default_rng(400 + n)
+    c, _ = noisy_circuit(n, 24, rng)
+    targets = with_readout_measures([c], n, rng)
+    for seed in (3, 4):
+        want = ref.run_dm(c, threads=1, shots=3000, seed=seed, targets=targets)["counts"]
+        assert restated_readout_counts(ref, c, 3000, seed, targets) == want
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 3, 6])
+def test_device_readout_counts_are_the_reference(ctx, ref, n):
+    from menos_b200 import DensityMatrix
+    rng = np.random.default_rng(500 + n)
+    c, d = noisy_circuit(n, 40, rng)
+    targets = with_readout_measures([c, d], n, rng)
+    rho = DensityMatrix(ctx, n)
+    rho.init()
+    rho.apply(d)
+    for seed in (5, 6):
+        got = rho.sample(40000, seed, targets, circuit=d).to_dict()
+        assert got == ref.run_dm(c, threads=1, shots=40000, seed=seed, targets=targets)["counts"]
+    # Measurements without readout errors: the plain sampler's counts.
+    plain = [(q, q) for q in range(n)]
+    d2 = type(d)(n)
+    d2.ops = [op for op in d.ops if op[0] != pyoracle.OP["measure"]]
+    for q in range(n):
+        d2.measure(q, q)
+    assert rho.sample(5000, 9, plain, circuit=d2).to_dict() == rho.sample(5000, 9, plain).to_dict()
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [1, 3, 6, 9])
 def test_device_rho_is_bitwise_the_reference(ctx, ref, n):

@@ -127,6 +127,24 @@ def test_device_trajectories_match_the_reference(ctx, ref, n):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [2, 7])
+def test_device_trajectory_readout_counts_are_the_reference(ctx, ref, n):
+    """Readout errors on the measurements: after each shot's word, one per
+    readout-errored target (trajectory_engine.cpp:465-471)."""
+    from menos_b200 import Circuit
+    from menos_b200.engine import trajectories
+    from test_dm import with_readout_measures
+    c = pure_noise_circuit(n, 30, 40 + n, widest=2)
+    d = Circuit(n)
+    d.ops = list(c.ops)
+    targets = with_readout_measures([c, d], n, np.random.default_rng(n))
+    count = shots = 160
+    got = trajectories(ctx, d, count, 77, shots=shots, targets=targets)
+    want = ref.run_trajectories(c, count, 77, shots=shots, targets=targets)
+    assert got["counts"].to_dict() == want["counts"]
+
+
+@pytest.mark.gpu
 def test_device_exact_norm_is_the_sequential_sum(ctx):
     from menos_b200 import DeviceState, workloads
     n = 18
