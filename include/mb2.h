@@ -295,6 +295,14 @@ int mb2_dm_sample_readout(mb2_state* rho, uint32_t num_qubits, const mb2_op* ops
                           uint64_t seed, const uint32_t* targets, uint32_t num_targets, uint64_t* outcomes,
                           uint64_t* counts, uint64_t* num_outcomes);
 
+/* For each uniform (any order, each in [0, 1)), the basis state whose
+ * sequential cumulative probability over rho's diagonal first exceeds it
+ * (CumulativeDistribution::sample_one on the diagonal,
+ * src/engines/dense/cumulative_distribution.cpp:83-92): the draws of a
+ * Factorized region's density-matrix sampler.  Synchronous. */
+int mb2_dm_sample_basis(mb2_state* rho, uint32_t num_qubits, const double* uniforms, uint64_t count,
+                        uint64_t* basis);
+
 /* The reference's sequential FP64 sum of |a_i|^2 over the state, bit for bit
  * (the exact device chain of mb2_sample), e.g. to renormalise as the
  * reference does (src/engines/trajectory/trajectory_engine.cpp:155-166). */
@@ -322,6 +330,19 @@ int mb2_trajectories(mb2_context* ctx, uint32_t num_qubits, const mb2_op* ops, u
                      const double* coefs, uint32_t num_terms, double* term_means, double* standard_error,
                      uint64_t shots, const uint32_t* targets, uint32_t num_targets, uint64_t* outcomes,
                      uint64_t* counts, uint64_t* num_outcomes);
+/* mb2_trajectories with the reference's execution monitor: boundary(user,
+ * crossed) is called with the reference's count of safe boundaries crossed
+ * (one after every operation of every trajectory, one after each
+ * trajectory's outputs; trajectory_engine.cpp:171-181) at the end of each
+ * run of gates, each channel and each trajectory; a nonzero return abandons
+ * with MB2_ERR_ABANDONED.  A monitor that abandons at count c stops here at
+ * the first such point at or past c. */
+int mb2_trajectories_monitored(mb2_context* ctx, uint32_t num_qubits, const mb2_op* ops, uint32_t num_ops,
+                               uint64_t trajectories, uint64_t seed, const uint64_t* x_masks,
+                               const uint64_t* z_masks, const double* coefs, uint32_t num_terms, double* term_means,
+                               double* standard_error, uint64_t shots, const uint32_t* targets,
+                               uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes,
+                               mb2_boundary_fn boundary, void* user);
 
 /* ---- batched parameter sweep ------------------------------------------- */
 /* One circuit structure under many parameter bindings, in one device job:

@@ -138,6 +138,10 @@ SIGNATURES = {
                                 C.POINTER(C.c_uint64)]),
     "mb2_dm_sample_readout": (C.c_int, [_VP, C.c_uint32, _VP, C.c_uint32, C.c_uint64, C.c_uint64, _VP, C.c_uint32,
                                         _VP, _VP, C.POINTER(C.c_uint64)]),
+    "mb2_dm_sample_basis": (C.c_int, [_VP, C.c_uint32, _VP, C.c_uint64, _VP]),
+    "mb2_trajectories_monitored": (C.c_int, [_VP, C.c_uint32, _VP, C.c_uint32, C.c_uint64, C.c_uint64, _VP, _VP,
+                                             _VP, C.c_uint32, _VP, C.POINTER(C.c_double), C.c_uint64, _VP,
+                                             C.c_uint32, _VP, _VP, C.POINTER(C.c_uint64), _VP, _VP]),
     "mb2_sample_basis": (C.c_int, [_VP, _VP, C.c_uint64, _VP]),
     "mb2_debug_tc_probe": (C.c_int, [_VP, _VP, _VP, _VP]),
     "mb2_fusion_plan": (C.c_int, [C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions), _VP, _VP, _VP, _VP,

@@ -1152,6 +1152,17 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
                      uint32_t num_terms, double* term_means, double* standard_error, uint64_t shots,
                      const uint32_t* targets, uint32_t num_targets, uint64_t* outcomes, uint64_t* counts,
                      uint64_t* num_outcomes) {
+    return mb2_trajectories_monitored(ctx, n, ops, num_ops, trajectories, seed, x_masks, z_masks, coefs, num_terms,
+                                      term_means, standard_error, shots, targets, num_targets, outcomes, counts,
+                                      num_outcomes, nullptr, nullptr);
+}
+
+int mb2_trajectories_monitored(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t num_ops,
+                               uint64_t trajectories, uint64_t seed, const uint64_t* x_masks,
+                               const uint64_t* z_masks, const double* coefs, uint32_t num_terms, double* term_means,
+                               double* standard_error, uint64_t shots, const uint32_t* targets,
+                               uint32_t num_targets, uint64_t* outcomes, uint64_t* counts, uint64_t* num_outcomes,
+                               mb2_boundary_fn boundary, void* user) {
     if (ctx == nullptr || n < 1 || n > 34 || (ops == nullptr && num_ops != 0) || trajectories == 0)
         return MB2_ERR_INVALID;
     const bool want_exp = num_terms != 0;
@@ -1168,6 +1179,7 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
     std::vector<std::vector<mb2_op>> gate_runs;
     std::vector<TrajChannel> channels;
     std::vector<std::pair<int, size_t>> steps;  // (0: gate run, 1: channel), index
+    std::vector<uint64_t> step_end;             // operations done once the step is (measurements included)
     try {
         for (uint32_t i = 0; i < num_ops; ++i) {
             const mb2_op& op = ops[i];
@@ -1175,9 +1187,11 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
             if (op.opcode != MB2_CHANNEL) {
                 if (steps.empty() || steps.back().first != 0) {
                     steps.emplace_back(0, gate_runs.size());
+                    step_end.push_back(0);
                     gate_runs.emplace_back();
                 }
                 gate_runs.back().push_back(op);
+                step_end.back() = i + 1;
                 continue;
             }
             const uint32_t k = op.num_qubits;
@@ -1206,6 +1220,7 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
                     ch.zs.push_back(gz);
                 }
             steps.emplace_back(1, channels.size());
+            step_end.push_back(i + 1);
             channels.push_back(std::move(ch));
         }
     } catch (const std::exception& e) {
@@ -1227,10 +1242,21 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
     mb2::Cd mean{0.0, 0.0};
     double ssd = 0.0;
     std::vector<uint64_t> shot_words;
+    // The reference's safe boundaries (trajectory_engine.cpp:171-181,216,
+    // 473): one after every operation of every trajectory and one after each
+    // trajectory's outputs, counted across trajectories; the monitor is asked
+    // at the end of each step here, with the count the reference has there.
+    const uint64_t per_trajectory = uint64_t{num_ops} + 1;
+    auto cross = [&](uint64_t crossed) {
+        return boundary == nullptr || boundary(user, crossed) == 0;
+    };
     for (uint64_t t = 0; t < trajectories; ++t) {
         std::mt19937_64 rng(trajectory_seed(seed, t));
         if (int e = mb2_init(st, 0.0); e != MB2_OK) return e;  // |0..0>, no global phase
-        for (const auto& [kind, idx] : steps) {
+        for (size_t si = 0; si < steps.size(); ++si) {
+            if (si > 0 && !cross(t * per_trajectory + step_end[si - 1]))
+                return fail(ctx, MB2_ERR_ABANDONED, "abandoned at a safe boundary");
+            const auto& [kind, idx] = steps[si];
             if (kind == 0) {
                 const std::vector<mb2_op>& run = gate_runs[idx];
                 if (int e = mb2_apply_program(st, run.data(), static_cast<uint32_t>(run.size()), &one_by_one); e != MB2_OK)
@@ -1311,6 +1337,8 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
             apply_readout(o, readouts, rng);
             shot_words.push_back(o);
         }
+        if ((!steps.empty() && !cross(t * per_trajectory + num_ops)) || !cross((t + 1) * per_trajectory))
+            return fail(ctx, MB2_ERR_ABANDONED, "abandoned at a safe boundary");
     }
     if (want_exp) {
         for (uint32_t i = 0; i < num_terms; ++i) {
@@ -1324,6 +1352,32 @@ int mb2_trajectories(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t n
         }
     }
     if (want_counts) return histogram_words(ctx, std::move(shot_words), outcomes, counts, num_outcomes);
+    return MB2_OK;
+}
+
+int mb2_dm_sample_basis(mb2_state* rho, uint32_t n, const double* uniforms, uint64_t count, uint64_t* basis) {
+    if (int e = check_rho(rho, n); e != MB2_OK) return e;
+    if (count == 0) return MB2_OK;
+    if (uniforms == nullptr || basis == nullptr) return MB2_ERR_INVALID;
+    std::vector<std::pair<double, uint64_t>> draw(count);
+    for (uint64_t i = 0; i < count; ++i) {
+        if (!(uniforms[i] >= 0.0 && uniforms[i] < 1.0)) return fail(rho->ctx, MB2_ERR_INVALID, "a uniform outside [0, 1)");
+        draw[i] = {uniforms[i], i};
+    }
+    std::sort(draw.begin(), draw.end());
+    std::vector<double> u(count);
+    for (uint64_t i = 0; i < count; ++i) u[i] = draw[i].first;
+    const size_t al_u = (count * 8 + 255) & ~size_t{255};
+    if (int e = ensure_scratch(rho, 2 * al_u); e != MB2_OK) return e;
+    auto* base = static_cast<unsigned char*>(rho->scratch);
+    MB2_CUDA(rho->ctx, cudaMemcpyAsync(base, u.data(), count * 8, cudaMemcpyHostToDevice, rho->stream));
+    const int rc = mb2::launch_dm_walk(rho->amps, n, reinterpret_cast<const double*>(base), count,
+                                       reinterpret_cast<uint64_t*>(base + al_u), rho->stream);
+    if (rc != MB2_OK) return fail(rho->ctx, rc, std::string("walk launch: ") + mb2::last_cuda_error_string());
+    std::vector<uint64_t> sorted(count);
+    MB2_CUDA(rho->ctx, cudaMemcpyAsync(sorted.data(), base + al_u, count * 8, cudaMemcpyDeviceToHost, rho->stream));
+    MB2_CUDA(rho->ctx, cudaStreamSynchronize(rho->stream));
+    for (uint64_t i = 0; i < count; ++i) basis[draw[i].second] = sorted[i];
     return MB2_OK;
 }
 

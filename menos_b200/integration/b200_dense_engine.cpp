@@ -209,6 +209,8 @@ private:
 
 bool b200_device_available() { return context() != nullptr; }
 
+mb2_context* b200_context() { return context(); }
+
 // The figures the planner's CUDA time model reads
 // (src/plan/planner.cpp:415-433, plan::CudaCalibration), measured on this
 // engine: a work unit is one amplitude of one state pass, priced at the

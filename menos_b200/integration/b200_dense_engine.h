@@ -18,6 +18,9 @@ namespace menos::engines::dense_b200 {
 const SimulationEngine& b200_dense_engine();
 // True when a device is usable (the registration's guard).
 bool b200_device_available();
+// The process's context on device 0 (opened on first use; NULL without a
+// device), shared by every engine of this binding.
+mb2_context* b200_context();
 // The hardware profile's CUDA figures, measured on this engine (in place of
 // plan::measure_cuda_calibration, src/plan/cuda_calibration.cpp:42-153).
 plan::CudaCalibration measure_b200_calibration();

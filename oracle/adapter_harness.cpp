@@ -1,9 +1,11 @@
 // adapter_harness.cpp -- TEST INFRASTRUCTURE, not product code.
 //
 // Drives the reference-side binding (menos_b200/integration/
-// b200_dense_engine.cpp, the menos::SimulationEngine the reference would
-// register) and the reference's own CPU DenseEngine
-// (src/engines/dense/dense_engine.cpp:333-400) through one request shape, so
+// b200_dense_engine.cpp and b200_noisy_engines.cpp, the
+// menos::SimulationEngines the reference would register) and the
+// reference's own CPU engines (DenseEngine, src/engines/dense/
+// dense_engine.cpp:333-400; DensityMatrixEngine; TrajectoryEngine) through
+// one request shape, so
 // tests can run the reference's CPU/CUDA differential cases
 // (tests/api/cpu_cuda_differential_test.cpp:132-421) against the adapter
 // itself.  oracle/Makefile links it with the adapter, the reference's CPU
@@ -40,14 +42,30 @@
 #include "../include/mb2.h"
 
 #include "../menos_b200/integration/b200_dense_engine.h"
+#include "../menos_b200/integration/b200_noisy_engines.h"
+#include "engines/density_matrix/density_matrix_engine.h"
+#include "engines/trajectory/trajectory_engine.h"
 
 namespace {
 
 using C = std::complex<double>;
 
 menos::Operation to_operation(const mb2_op& op) {
-    if (op.opcode == MB2_MEASURE) return menos::MeasureOp{op.qubits[0], op.clbit};
+    if (op.opcode == MB2_MEASURE) {
+        menos::MeasureOp m{op.qubits[0], op.clbit};
+        if (op.matrix != nullptr)
+            m.readout_error = menos::ReadoutError{{op.matrix[0], op.matrix[1], op.matrix[2], op.matrix[3]}};
+        return m;
+    }
     std::vector<menos::QubitId> qubits(op.qubits, op.qubits + op.num_qubits);
+    if (op.opcode == MB2_CHANNEL) {
+        const std::size_t entries = std::size_t{1} << (2 * op.num_qubits);
+        std::vector<std::vector<C>> kraus(op.reserved, std::vector<C>(entries));
+        for (std::size_t t = 0; t < op.reserved; ++t)
+            for (std::size_t i = 0; i < entries; ++i)
+                kraus[t][i] = C{op.matrix[2 * (t * entries + i)], op.matrix[2 * (t * entries + i) + 1]};
+        return menos::ChannelOp{std::move(qubits), std::move(kraus)};
+    }
     if (op.opcode == MB2_UNITARY) {
         const std::size_t dim = std::size_t{1} << op.num_qubits;
         std::vector<C> m(dim * dim);
@@ -81,10 +99,21 @@ private:
     std::int64_t at_;
 };
 
+// 0/1: the reference's CPU DenseEngine / the dense binding; 2/3: the
+// reference's DensityMatrixEngine / its binding; 4/5: the reference's
+// TrajectoryEngine / its binding.
 const menos::SimulationEngine& engine_of(int which) {
     static const menos::engines::dense::DenseEngine cpu;
-    if (which == 0) return cpu;
-    return menos::engines::dense_b200::b200_dense_engine();
+    static const menos::engines::density_matrix::DensityMatrixEngine dm;
+    static const menos::engines::trajectory::TrajectoryEngine traj;
+    switch (which) {
+        case 0: return cpu;
+        case 2: return dm;
+        case 3: return menos::engines::dense_b200::b200_density_matrix_engine();
+        case 4: return traj;
+        case 5: return menos::engines::dense_b200::b200_trajectory_engine();
+        default: return menos::engines::dense_b200::b200_dense_engine();
+    }
 }
 
 void set_error(char* err, std::size_t len, const char* what) {
@@ -112,6 +141,8 @@ typedef struct ah_request {
     const std::uint64_t* z_masks;
     std::uint32_t num_terms, reserved2;
     std::int64_t abandon_at;
+    std::uint64_t trajectories;   // the trajectory engines' count
+    const double* coefs;          // complex coefficient per term (2 doubles), or NULL for 1
 } ah_request;
 
 typedef struct ah_result {
@@ -127,6 +158,8 @@ typedef struct ah_result {
     std::uint64_t actual_bytes, peak_host, peak_device, monitor_calls;
     std::int32_t has_statevector, has_counts, has_sampler, has_expectation;
     double seconds;               // wall time of execute()
+    double standard_error;        // the result's expectation_standard_error, or -1
+    std::int32_t statistical, reserved;
 } ah_result;
 
 // 0 ok; 1 ResourceExceeded; 2 InternalError (the monitor's abandon included);
@@ -144,7 +177,8 @@ int ah_execute(int which, const ah_request* rq, ah_result* res, char* err, std::
             p.num_qubits = rq->num_qubits;
             p.x_words.assign(1, rq->x_masks[t]);
             p.z_words.assign(1, rq->z_masks[t]);
-            obs.terms.emplace_back(std::move(p), C{1.0, 0.0});
+            const C coef = rq->coefs != nullptr ? C{rq->coefs[2 * t], rq->coefs[2 * t + 1]} : C{1.0, 0.0};
+            obs.terms.emplace_back(std::move(p), coef);
         }
         CountingMonitor monitor(rq->abandon_at);
         menos::EngineExecutionRequest request{
@@ -163,6 +197,7 @@ int ah_execute(int which, const ah_request* rq, ah_result* res, char* err, std::
             .observable = rq->want_expectation ? &obs : nullptr,
         };
         request.fuse_gates = rq->fuse_gates != 0;
+        request.trajectories = rq->trajectories;
         if (rq->abandon_at >= 0) request.monitor = &monitor;
         menos::common::MemoryLedger ledger;
         {
@@ -197,6 +232,8 @@ int ah_execute(int which, const ah_request* rq, ah_result* res, char* err, std::
                 for (std::uint64_t i = 0; i < res->draws && i < res->capacity; ++i)
                     res->drawn[i] = bits_of(r.counts_sampler->sample_one(rng));
             }
+            res->statistical = r.statistical ? 1 : 0;
+            res->standard_error = r.expectation_standard_error.value_or(-1.0);
             res->has_expectation = r.expectation_terms.has_value();
             if (r.expectation_terms && res->expectation)
                 std::memcpy(res->expectation, r.expectation_terms->data(), r.expectation_terms->size() * sizeof(C));
@@ -242,6 +279,7 @@ int ah_estimate(int which, const ah_request* rq, std::uint64_t* out, char* reaso
         request.bitstring_width = rq->bitstring_width;
         request.is_sole_region = rq->is_sole_region != 0;
         request.fuse_gates = rq->fuse_gates != 0;
+        request.trajectories = rq->trajectories;
         const menos::CostEstimate e = engine_of(which).estimate(request);
         out[0] = e.feasible;
         out[1] = e.estimated_peak_bytes;
@@ -250,7 +288,8 @@ int ah_estimate(int which, const ah_request* rq, std::uint64_t* out, char* reaso
         out[4] = e.device.host_to_device_bytes;
         out[5] = e.device.device_to_host_bytes;
         out[6] = e.device.kernel_launches;
-        out[7] = static_cast<std::uint64_t>(e.time.counts[static_cast<std::size_t>(menos::Engine::Dense)][0]);
+        const menos::Engine id = engine_of(which).engine_id();
+        out[7] = static_cast<std::uint64_t>(e.time.counts[static_cast<std::size_t>(id)][0]);
         set_error(reason, len, e.infeasible_reason.c_str());
         return 0;
     } catch (const std::exception& e) {

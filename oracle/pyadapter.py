@@ -20,6 +20,10 @@ ADAPTER_SO = os.path.join(HERE, "_ref", "libmenos_adapter.so")
 
 REFERENCE_CPU = 0   # engines::dense::DenseEngine
 B200 = 1            # engines::dense_b200::B200DenseEngine (the adapter)
+REFERENCE_DM = 2    # engines::density_matrix::DensityMatrixEngine
+B200_DM = 3         # engines::dense_b200::b200_density_matrix_engine()
+REFERENCE_TRAJ = 4  # engines::trajectory::TrajectoryEngine
+B200_TRAJ = 5       # engines::dense_b200::b200_trajectory_engine()
 
 OK, RESOURCE_EXCEEDED, INTERNAL_ERROR, OTHER = 0, 1, 2, 3
 
@@ -31,7 +35,8 @@ class _Request(C.Structure):
                 ("shots", C.c_uint64), ("seed", C.c_uint64), ("targets", C.c_void_p),
                 ("num_targets", C.c_uint32), ("bitstring_width", C.c_uint32), ("global_phase", C.c_double),
                 ("budget_bytes", C.c_uint64), ("x_masks", C.c_void_p), ("z_masks", C.c_void_p),
-                ("num_terms", C.c_uint32), ("reserved2", C.c_uint32), ("abandon_at", C.c_int64)]
+                ("num_terms", C.c_uint32), ("reserved2", C.c_uint32), ("abandon_at", C.c_int64),
+                ("trajectories", C.c_uint64), ("coefs", C.c_void_p)]
 
 
 class _Result(C.Structure):
@@ -40,7 +45,8 @@ class _Result(C.Structure):
                 ("draws", C.c_uint64), ("draw_seed", C.c_uint64), ("drawn", C.c_void_p),
                 ("actual_bytes", C.c_uint64), ("peak_host", C.c_uint64), ("peak_device", C.c_uint64),
                 ("monitor_calls", C.c_uint64), ("has_statevector", C.c_int32), ("has_counts", C.c_int32),
-                ("has_sampler", C.c_int32), ("has_expectation", C.c_int32), ("seconds", C.c_double)]
+                ("has_sampler", C.c_int32), ("has_expectation", C.c_int32), ("seconds", C.c_double),
+                ("standard_error", C.c_double), ("statistical", C.c_int32), ("reserved", C.c_int32)]
 
 
 class AdapterHarness:
@@ -56,7 +62,8 @@ class AdapterHarness:
         self.L.ah_serve_with_ledger.restype = C.c_int
 
     def _request(self, circ, keep, *, fuse=True, statevector=False, shots=0, seed=0, targets=(), width=None,
-                 sole=True, paulis=(), global_phase=None, budget=1 << 40, abandon_at=-1):
+                 sole=True, paulis=(), global_phase=None, budget=1 << 40, abandon_at=-1, trajectories=0,
+                 coefs=None):
         arr, mats = ops_struct_array(circ)
         keep += [arr, mats]
         t = np.ascontiguousarray(np.asarray(targets, np.uint32).ravel())
@@ -86,6 +93,11 @@ class AdapterHarness:
         rq.z_masks = zs.ctypes.data
         rq.num_terms = len(paulis)
         rq.abandon_at = abandon_at
+        rq.trajectories = trajectories
+        if coefs is not None:
+            cs = np.ascontiguousarray(np.asarray(coefs, np.complex128))
+            keep.append(cs)
+            rq.coefs = cs.ctypes.data
         return rq
 
     def execute(self, engine: int, circ, *, draws: int = 0, draw_seed: int = 0, **kw) -> dict:
@@ -124,6 +136,8 @@ class AdapterHarness:
             "peak_device": int(res.peak_device),
             "monitor_calls": int(res.monitor_calls),
             "seconds": float(res.seconds),
+            "standard_error": float(res.standard_error) if res.standard_error >= 0 else None,
+            "statistical": bool(res.statistical),
         }
 
     def estimate(self, engine: int, circ, **kw) -> dict:
