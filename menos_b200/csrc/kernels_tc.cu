@@ -16,10 +16,10 @@
 //   two K-steps of 16 each) with A from tensor memory and B = 2^12 U's
 //   operand in shared memory (FP16 high parts over low parts):
 //   A_lo x B_hi, A_hi x B_lo, then A_hi x B_hi, all accumulated into one
-//   block of 32 FP32 columns; tcgen05.commit signals an mbarrier the issuing
-//   thread waits on; after a CTA barrier every thread reads its row back
-//   (one tcgen05.ld), takes out the 2^12 and applies the phase's elementwise
-//   diagonals on registers.
+//   block of 32 FP32 columns; tcgen05.commit signals an mbarrier that every
+//   thread waits on; each thread then reads its row back (one tcgen05.ld),
+//   takes out the 2^12 and applies the phase's elementwise diagonals on
+//   registers.
 //
 // Every wait on the tensor core is bounded: a wait that runs out sets the
 // caller's error word, the CTA stops issuing work, frees its tensor memory
@@ -187,7 +187,7 @@ __device__ __forceinline__ float pow2f(int e) { return __uint_as_float(static_ca
 // into FP16's range (tile_scale_exp).  ROWS threads, ROWS / 128 row blocks;
 // TMEM columns: [0, 16 NB) high parts, [16 NB, 32 NB) low parts,
 // [32 NB, 64 NB) the products (32 per block).  All threads of the CTA call
-// it; thread 0 issues the MMAs and waits for them.
+// it; thread 0 issues the MMAs, every thread waits for them on the mbarrier.
 template <int ROWS>
 __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c) {
     constexpr uint32_t NB = ROWS / 128;
@@ -225,14 +225,16 @@ __device__ __forceinline__ void tc_apply(float2 (&a)[kNA], uint32_t b, TcCtx& c)
             mma_f16(d, ah + 8, bh1, kIdescN32, 1);
         }
         mma_commit(c.bar);
+    }
+    // Every thread waits on the MMAs' mbarrier itself (no CTA barrier): its
+    // phase completes when the products are in tensor memory.
+    if (!abort) {
         if (!mbar_wait(c.bar, c.parity)) {
             *c.abort = 1;
             atomicExch(c.err, 1);
         }
+        c.parity ^= 1u;
     }
-    if (!abort) c.parity ^= 1u;
-    tc_fence_before();
-    __syncthreads();
     tc_fence_after();
     uint32_t v[32];
     tmem_ld32(c.tmem + lane + 32 * NB + 32 * blk, v);
