@@ -158,6 +158,28 @@ typedef struct mb2_sweep_options {
  * 337-355).  opts may be NULL (defaults: reference fusion on, autotuned tile). */
 int mb2_apply_program(mb2_state* state, const mb2_op* ops, uint32_t num_ops,
                       const mb2_sweep_options* opts);
+/* A host-resident state (mb2_state_alloc_host) swept through device
+ * windows, the reference's chunked tier on the device's copy engines
+ * (src/engines/dense_tiered/pass_plan.h, chunked_executor.cpp): the state is
+ * 2^(n-L) chunks of 2^L amplitudes (L = chunk_qubits; 0: chosen as the
+ * reference's choose_pass_plan does, pass_plan.cpp:123-150, from 2^24
+ * amplitudes up -- below that from 2^min(16, W)); a window of 2^W amplitudes
+ * (W = window_qubits, 4..n) holds the 2^g chunks of g <= W - L global qubits;
+ * passes are the reference's greedy rule over the fusion plan's blocks
+ * (pass_plan.cpp:43-121).  Each window is copied in, swept by the tiled
+ * kernels with its blocks' operands remapped, and copied back; two device
+ * windows on two streams let one window's copies overlap the other's sweep.
+ * Bitwise the device-resident result.  Device memory: two windows (2 * 16 *
+ * 2^W bytes, MB2_ERR_RESOURCE when they do not fit).  mb2_sweep_stats:
+ * passes = window passes, launches = tile-pass launches.  A block with more
+ * than W - L operands at or above L: MB2_ERR_INVALID.  Synchronous. */
+int mb2_apply_program_windowed(mb2_state* state, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
+                               uint32_t window_qubits, uint32_t chunk_qubits);
+/* The window plan mb2_apply_program_windowed runs, on the host: out =
+ * [L, W, passes, then per pass its global mask (bit g - L per global qubit
+ * g), first block, end block]; *out_words in: capacity, out: words. */
+int mb2_window_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
+                    uint32_t window_qubits, uint32_t chunk_qubits, uint64_t* out, uint64_t* out_words);
 /* As mb2_apply_program, calling `boundary(user, blocks_done)` on the host
  * after each pass has completed on the device: the state is then complete
  * and consistent, the reference's safe boundary (ExecutionMonitor::

@@ -139,6 +139,10 @@ SIGNATURES = {
     "mb2_dm_sample_readout": (C.c_int, [_VP, C.c_uint32, _VP, C.c_uint32, C.c_uint64, C.c_uint64, _VP, C.c_uint32,
                                         _VP, _VP, C.POINTER(C.c_uint64)]),
     "mb2_dm_sample_basis": (C.c_int, [_VP, C.c_uint32, _VP, C.c_uint64, _VP]),
+    "mb2_apply_program_windowed": (C.c_int, [_VP, C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions), C.c_uint32,
+                                             C.c_uint32]),
+    "mb2_window_plan": (C.c_int, [C.POINTER(MB2Op), C.c_uint32, C.POINTER(SweepOptions), C.c_uint32, C.c_uint32,
+                                  C.c_uint32, _VP, C.POINTER(C.c_uint64)]),
     "mb2_trajectories_monitored": (C.c_int, [_VP, C.c_uint32, _VP, C.c_uint32, C.c_uint64, C.c_uint64, _VP, _VP,
                                              _VP, C.c_uint32, _VP, C.POINTER(C.c_double), C.c_uint64, _VP,
                                              C.c_uint32, _VP, _VP, C.POINTER(C.c_uint64), _VP, _VP]),

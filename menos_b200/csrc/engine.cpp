@@ -559,6 +559,276 @@ int mb2_apply_program(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const m
     return mb2_apply_program_monitored(s, ops, num_ops, opts, nullptr, nullptr);
 }
 
+}  // extern "C"
+
+// ---- host-resident states streamed through device windows -------------------
+// The reference's chunked tier (src/engines/dense_tiered/pass_plan.h): a state
+// of n qubits is 2^(n-L) chunks of 2^L amplitudes (local qubits 0..L-1,
+// global qubits L..n-1); a window of 2^W amplitudes holds the 2^g chunks of
+// any g <= W - L global qubits G, whose slot bits L..L+g-1 stand for G in
+// increasing order, so a block on local qubits and qubits of G runs on the
+// window with its operands remapped, and multiplies every amplitude by the
+// same entries in the same order as on the whole state.
+namespace {
+
+struct WindowPass {
+    uint64_t global_mask;  // bit g - L for each global qubit g in G
+    size_t first, end;     // blocks [first, end)
+};
+struct WindowPlan {
+    uint32_t chunk_qubits = 0, window_qubits = 0;
+    std::vector<WindowPass> passes;
+    bool too_small = false;
+};
+
+// The greedy rule of build_pass_plan (pass_plan.cpp:43-121) over the fusion
+// plan's blocks: a pass opens with the first block's global operands as G
+// and absorbs each following block while G stays within W - L qubits.
+WindowPlan window_plan(const std::vector<mb2::Block>& blocks, uint32_t L, uint32_t W) {
+    WindowPlan p;
+    p.chunk_qubits = L;
+    p.window_qubits = W;
+    const int wg = static_cast<int>(W - L);
+    bool open = false;
+    uint64_t group = 0;
+    size_t first = 0;
+    for (size_t i = 0; i < blocks.size(); ++i) {
+        uint64_t mask = 0;
+        for (uint32_t j = 0; j < blocks[i].k; ++j)
+            if (blocks[i].q[j] >= L) mask |= uint64_t{1} << (blocks[i].q[j] - L);
+        if (std::popcount(mask) > wg) p.too_small = true;
+        if (!open) {
+            open = true;
+            group = mask;
+            continue;
+        }
+        const uint64_t merged = group | mask;
+        if (std::popcount(merged) <= wg) {
+            group = merged;
+        } else {
+            p.passes.push_back(WindowPass{group, first, i});
+            first = i;
+            group = mask;
+        }
+    }
+    if (open) p.passes.push_back(WindowPass{group, first, blocks.size()});
+    return p;
+}
+
+// Smallest chunk the automatic choice takes: 2^16 amplitudes (1 MiB a copy).
+constexpr uint32_t kMinWindowChunkQubits = 16;
+
+// The chunk size as choose_pass_plan picks it (pass_plan.cpp:123-150): the
+// fewest passes, the larger chunk on a tie, among chunks from 2^24
+// amplitudes up to the window, smaller ones only when none of those fits the
+// blocks -- except that for a window of at most 2^24 the search starts
+// below at 2^min(16, W) rather than at one amplitude (a device copy of less
+// than 1 MiB costs more in calls than it saves in passes), and no chunk is
+// below the tile kernels' 2^4.  W >= 4.
+WindowPlan choose_window_plan(const std::vector<mb2::Block>& blocks, uint32_t W) {
+    const uint32_t lowest = W > 24 ? 24u : std::min(W, kMinWindowChunkQubits);
+    WindowPlan best;
+    best.too_small = true;
+    for (uint32_t L = W;; --L) {
+        if (L < lowest && !best.too_small) break;
+        WindowPlan p = window_plan(blocks, L, W);
+        if (!p.too_small && (best.too_small || p.passes.size() < best.passes.size())) best = std::move(p);
+        if (L <= mb2::kMinTileQubits) break;
+    }
+    return best;
+}
+
+uint64_t pdep_host(uint64_t v, uint64_t mask) {
+    uint64_t r = 0;
+    for (uint64_t m = mask; m != 0; m &= m - 1) {
+        if (v & 1u) r |= m & (~m + 1);
+        v >>= 1;
+    }
+    return r;
+}
+
+// The blocks of a fusion plan, validated against n qubits.
+int window_blocks(mb2_context* ctx, uint32_t n, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
+                  std::vector<mb2::Block>& blocks) {
+    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
+    if (opts != nullptr) o = *opts;
+    for (uint32_t i = 0; i < num_ops; ++i) {
+        if (ops[i].opcode == MB2_MEASURE) continue;
+        if (ops[i].num_qubits == 0 || ops[i].num_qubits > MB2_MAX_OP_QUBITS)
+            return fail(ctx, MB2_ERR_INVALID, "operation " + std::to_string(i) + ": operand count");
+        for (uint32_t j = 0; j < ops[i].num_qubits; ++j)
+            if (ops[i].qubits[j] >= n) return fail(ctx, MB2_ERR_INVALID, "operation " + std::to_string(i) + ": operand out of range");
+    }
+    try {
+        blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0, static_cast<uint32_t>(o.fusion_width));
+    } catch (const std::exception& e) {
+        return fail(ctx, MB2_ERR_INVALID, e.what());
+    }
+    return MB2_OK;
+}
+
+int plan_windows(mb2_context* ctx, const std::vector<mb2::Block>& blocks, uint32_t n, uint32_t W, uint32_t L,
+                 WindowPlan& plan) {
+    if (W < mb2::kMinTileQubits || W > n) return fail(ctx, MB2_ERR_INVALID, "the window holds 4..n qubits");
+    if (L != 0 && (L < mb2::kMinTileQubits || L > W))
+        return fail(ctx, MB2_ERR_INVALID, "a chunk holds 4..window qubits (0: chosen)");
+    plan = L != 0 ? window_plan(blocks, L, W) : choose_window_plan(blocks, W);
+    if (plan.too_small)
+        return fail(ctx, MB2_ERR_INVALID, "a block has more operands above the chunk than the window holds");
+    return MB2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mb2_window_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
+                    uint32_t window_qubits, uint32_t chunk_qubits, uint64_t* out, uint64_t* out_words) {
+    if ((ops == nullptr && num_ops != 0) || out_words == nullptr || num_qubits < 1 || num_qubits > 40)
+        return MB2_ERR_INVALID;
+    std::vector<mb2::Block> blocks;
+    if (int e = window_blocks(nullptr, num_qubits, ops, num_ops, opts, blocks); e != MB2_OK) return e;
+    WindowPlan plan;
+    if (int e = plan_windows(nullptr, blocks, num_qubits, window_qubits, chunk_qubits, plan); e != MB2_OK) return e;
+    std::vector<uint64_t> w{plan.chunk_qubits, plan.window_qubits, plan.passes.size()};
+    for (const WindowPass& p : plan.passes) {
+        w.push_back(p.global_mask);
+        w.push_back(p.first);
+        w.push_back(p.end);
+    }
+    const uint64_t cap = *out_words;
+    *out_words = w.size();
+    if (out == nullptr || cap < w.size()) return MB2_ERR_INVALID;
+    std::copy(w.begin(), w.end(), out);
+    return MB2_OK;
+}
+
+int mb2_apply_program_windowed(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
+                               uint32_t window_qubits, uint32_t chunk_qubits) {
+    if (s == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
+    mb2_context* ctx = s->ctx;
+    if (s->host_amps == nullptr) return fail(ctx, MB2_ERR_INVALID, "windowed sweeps take a host-resident state");
+    if (s->precision != MB2_C128) return fail(ctx, MB2_ERR_UNSUPPORTED, "windowed sweeps: complex128 states only");
+    const uint32_t n = s->n;
+    std::vector<mb2::Block> blocks;
+    if (int e = window_blocks(ctx, n, ops, num_ops, opts, blocks); e != MB2_OK) return e;
+    s->stats = mb2_sweep_stats{};
+    s->stats.blocks = blocks.size();
+    if (blocks.empty()) return MB2_OK;
+    WindowPlan plan;
+    if (int e = plan_windows(ctx, blocks, n, window_qubits, chunk_qubits, plan); e != MB2_OK) return e;
+    const uint32_t L = plan.chunk_qubits, W = plan.window_qubits;
+    MB2_CUDA(ctx, cudaSetDevice(ctx->device));
+    // Whatever the state's own stream wrote (initialisation, earlier calls
+    // through the mapped alias) lands before the copies read the host buffer.
+    MB2_CUDA(ctx, cudaStreamSynchronize(s->stream));
+    // Two windows, each with its stream: a window's copies in, sweep and
+    // copies out are ordered on its stream, and the two streams overlap, so
+    // one window's copies run while the other is swept.
+    const size_t win_bytes = (size_t{1} << W) * 16;
+    size_t free_bytes = 0, total_bytes = 0;
+    MB2_CUDA(ctx, cudaMemGetInfo(&free_bytes, &total_bytes));
+    if (2 * win_bytes + (size_t{64} << 20) > free_bytes)
+        return fail(ctx, MB2_ERR_RESOURCE, "two windows of " + std::to_string(win_bytes) + " bytes do not fit the device");
+    struct Res {
+        cudaStream_t st[2] = {nullptr, nullptr};
+        void* win[2] = {nullptr, nullptr};
+        void* prog = nullptr;
+        ~Res() {
+            for (cudaStream_t t : st)
+                if (t != nullptr) cudaStreamSynchronize(t);
+            for (void* p : win)
+                if (p != nullptr) cudaFree(p);
+            if (prog != nullptr) cudaFree(prog);
+            for (cudaStream_t t : st)
+                if (t != nullptr) cudaStreamDestroy(t);
+        }
+    } r;
+    size_t prog_bytes = 0;
+    for (int b = 0; b < 2; ++b) {
+        MB2_CUDA(ctx, cudaStreamCreateWithFlags(&r.st[b], cudaStreamNonBlocking));
+        MB2_CUDA(ctx, cudaMalloc(&r.win[b], win_bytes));
+    }
+    auto* host = static_cast<unsigned char*>(s->host_amps);
+    const uint64_t global_bits = n - L;
+    const uint64_t all_globals = global_bits >= 64 ? ~uint64_t{0} : (uint64_t{1} << global_bits) - 1;
+    for (const WindowPass& wp : plan.passes) {
+        const uint32_t g = static_cast<uint32_t>(std::popcount(wp.global_mask));
+        const uint32_t n_eff = L + g;
+        // The pass's blocks on window qubits: local qubits stay, global
+        // qubit L + b becomes L + (its rank among G).
+        std::vector<mb2::Block> local(blocks.begin() + static_cast<std::ptrdiff_t>(wp.first),
+                                      blocks.begin() + static_cast<std::ptrdiff_t>(wp.end));
+        for (mb2::Block& b : local)
+            for (uint32_t j = 0; j < b.k; ++j)
+                if (b.q[j] >= L) {
+                    const uint32_t bit = b.q[j] - L;
+                    b.q[j] = L + static_cast<uint32_t>(std::popcount(wp.global_mask & ((uint64_t{1} << bit) - 1)));
+                }
+        const uint32_t dflt = n_eff <= 16 ? mb2::kMaxTileQubits : ctx->tile_c128.load();
+        const uint32_t m = std::min(tile_width(dflt, n_eff, local), n_eff);
+        mb2::TileProgram prog;
+        try {
+            prog = mb2::plan_tile_program(local, n_eff, m);
+        } catch (const std::exception& e) {
+            return fail(ctx, MB2_ERR_INVALID, e.what());
+        }
+        const size_t ibytes = prog.words.size() * sizeof(uint32_t);
+        const size_t dbytes = prog.data.size() * sizeof(double);
+        const size_t gbytes = prog.gdata.size() * sizeof(double);
+        const size_t doff = (ibytes + 255) & ~size_t{255};
+        const size_t goff = (doff + dbytes + 255) & ~size_t{255};
+        const size_t need = goff + gbytes + 256;
+        if (need > prog_bytes) {
+            if (r.prog != nullptr) MB2_CUDA(ctx, cudaFree(r.prog));
+            r.prog = nullptr;
+            MB2_CUDA(ctx, cudaMalloc(&r.prog, need));
+            prog_bytes = need;
+        }
+        std::vector<unsigned char> staged(need, 0);
+        std::memcpy(staged.data(), prog.words.data(), ibytes);
+        if (dbytes) std::memcpy(staged.data() + doff, prog.data.data(), dbytes);
+        if (gbytes) std::memcpy(staged.data() + goff, prog.gdata.data(), gbytes);
+        // Both streams are idle here (the previous pass ended with a sync).
+        MB2_CUDA(ctx, cudaMemcpy(r.prog, staged.data(), need, cudaMemcpyHostToDevice));
+        auto* pbase = static_cast<unsigned char*>(r.prog);
+        const auto* dev_words = reinterpret_cast<const uint32_t*>(pbase);
+        const auto* dev_sdata = reinterpret_cast<const double*>(pbase + doff);
+        const auto* dev_gdata = reinterpret_cast<const double*>(pbase + goff);
+        // Chunks whose slots follow each other and whose host addresses do too
+        // (the lowest global qubits, when G holds them) move in one copy.
+        const uint32_t run = static_cast<uint32_t>(std::countr_one(wp.global_mask));
+        const size_t copy_bytes = (size_t{1} << (L + run)) * 16;
+        const uint64_t other = all_globals & ~wp.global_mask;
+        const uint64_t groups = uint64_t{1} << (global_bits - g);
+        for (uint64_t grp = 0; grp < groups; ++grp) {
+            const int b = static_cast<int>(grp & 1u);
+            auto* win = static_cast<unsigned char*>(r.win[b]);
+            const uint64_t base_chunk = pdep_host(grp, other);
+            for (uint64_t slot = 0; slot < (uint64_t{1} << g); slot += uint64_t{1} << run) {
+                const uint64_t chunk = base_chunk | pdep_host(slot, wp.global_mask);
+                MB2_CUDA(ctx, cudaMemcpyAsync(win + ((slot << L) * 16), host + ((chunk << L) * 16), copy_bytes,
+                                              cudaMemcpyHostToDevice, r.st[b]));
+            }
+            for (const mb2::TilePass& pass : prog.passes) {
+                const int rc = mb2::launch_tile_pass(win, n_eff, pass, dev_words, dev_sdata, dev_gdata, ctx->sm_count,
+                                                     r.st[b]);
+                if (rc != MB2_OK) return fail(ctx, rc, std::string("tile pass launch: ") + mb2::last_cuda_error_string());
+                s->stats.launches += 1;
+            }
+            for (uint64_t slot = 0; slot < (uint64_t{1} << g); slot += uint64_t{1} << run) {
+                const uint64_t chunk = base_chunk | pdep_host(slot, wp.global_mask);
+                MB2_CUDA(ctx, cudaMemcpyAsync(host + ((chunk << L) * 16), win + ((slot << L) * 16), copy_bytes,
+                                              cudaMemcpyDeviceToHost, r.st[b]));
+            }
+        }
+        MB2_CUDA(ctx, cudaStreamSynchronize(r.st[0]));
+        MB2_CUDA(ctx, cudaStreamSynchronize(r.st[1]));
+        s->stats.passes += 1;
+    }
+    return MB2_OK;
+}
+
 int mb2_fusion_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t* order,
                     uint32_t* block_begin, uint32_t* block_qubits, uint32_t* qubits_begin, uint64_t* num_blocks,
                     uint64_t* num_block_qubits) {

@@ -196,6 +196,20 @@ class DeviceState:
         del keep
         return self.stats()
 
+    def apply_program_windowed(self, circ: Circuit, window_qubits: int, chunk_qubits: int = 0,
+                               fuse_gates: bool = True) -> SweepStats:
+        """A host-resident state swept through device windows of
+        2^window_qubits amplitudes (mb2_apply_program_windowed: the
+        reference's chunked tier on the copy engines; chunk_qubits 0 chooses
+        the chunk as the reference does).  stats.passes counts window
+        passes."""
+        arr, keep = to_mb2_ops(circ)
+        opts = SweepOptions(1 if fuse_gates else 0, 0, 0, 0, 0, 0)
+        self._chk(lib().mb2_apply_program_windowed(self.h, arr, len(circ.ops), C.byref(opts), window_qubits,
+                                                   chunk_qubits), "mb2_apply_program_windowed")
+        del keep
+        return self.stats()
+
     def stats(self) -> SweepStats:
         s = SweepStats()
         self._chk(lib().mb2_last_sweep_stats(self.h, C.byref(s)), "stats")

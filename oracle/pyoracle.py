@@ -259,6 +259,9 @@ class RefLib:
                                            C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint64,
                                            C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_run_trajectories.restype = C.c_int
+        L.ref_pass_plan.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                    C.c_uint64]
+        L.ref_pass_plan.restype = C.c_int64
         L.ref_last_error.restype = C.c_char_p
         L.ref_default_threads.restype = C.c_uint32
         L.ref_kernel_isa.restype = C.c_int
@@ -383,6 +386,19 @@ class RefLib:
             "terms": terms[:2 * len(paulis)].view(np.complex128).copy() if paulis else None,
             "seconds": float(secs[0]),
         }
+
+    def pass_plan(self, circ: Circuit, chunk_qubits: int, window_qubits: int):
+        """The chunked tier's pass plan over the circuit's fusion plan
+        (build_pass_plan, or choose_pass_plan for chunk_qubits 0):
+        (chunk_qubits, window_too_small, [(global_mask, first, end), ...])."""
+        arr, keep = ops_struct_array(circ)
+        out = np.zeros(1 << 20, np.uint64)
+        k = self.L.ref_pass_plan(circ.num_qubits, C.addressof(arr), len(circ.ops), chunk_qubits, window_qubits,
+                                 out.ctypes.data, out.size)
+        assert k >= 0, self.L.ref_last_error()
+        del keep
+        w = [int(v) for v in out[:k]]
+        return w[0], bool(w[1]), [tuple(w[3 + 3 * i:6 + 3 * i]) for i in range(w[2])]
 
     def run_trajectories(self, circ: Circuit, trajectories, seed, paulis=(), coefs=None, shots=0, targets=(),
                          width=None):

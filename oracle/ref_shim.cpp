@@ -19,6 +19,7 @@
 //                               engine's apply_matrix, for a plan given as ir::FusionPlan's
 //                               arrays (src/engines/dense/dense_engine.cpp:100-112)
 #include <algorithm>
+#include <optional>
 #include <chrono>
 #include <complex>
 #include <cstdint>
@@ -38,6 +39,7 @@
 #endif
 #include "engines/dense/fused_block.h"
 #include "engines/dense/sample.h"
+#include "engines/dense_tiered/pass_plan.h"
 #include "ir/fuse_gates.h"
 #include "ir/gate_table.h"
 #include "kernels/cpu/dense_kernel_table.h"
@@ -523,6 +525,46 @@ int ref_run_plan(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_op
 
 std::uint32_t ref_default_threads() {
     return menos::common::default_thread_count();
+}
+
+// The chunked tier's pass plan over the fusion plan of ops
+// (src/engines/dense_tiered/pass_plan.cpp:43-150): build_pass_plan with
+// chunk_qubits > 0, else choose_pass_plan (no chunk pair needed).  out:
+// [chunk_qubits, window_too_small, passes, then per pass global_mask, first,
+// end]; returns the words written, or -1.
+std::int64_t ref_pass_plan(std::uint32_t num_qubits, const mb2_op* ops, std::uint32_t n_ops,
+                           std::uint32_t chunk_qubits, std::uint32_t window_qubits, std::uint64_t* out,
+                           std::uint64_t cap) {
+    try {
+        std::vector<menos::Operation> v;
+        for (std::uint32_t i = 0; i < n_ops; ++i) v.push_back(to_operation(ops[i]));
+        const menos::ir::FusionPlan fusion = menos::ir::plan_fusion(v);
+        std::optional<menos::engines::dense_tiered::PassPlan> plan;
+        if (chunk_qubits > 0) {
+            plan = menos::engines::dense_tiered::build_pass_plan(v, num_qubits, chunk_qubits, window_qubits, &fusion);
+        } else {
+            plan = menos::engines::dense_tiered::choose_pass_plan(v, num_qubits, window_qubits, false, &fusion);
+        }
+        if (!plan.has_value()) {
+            g_error = "no chunk size fits";
+            return -1;
+        }
+        std::vector<std::uint64_t> w{plan->chunk_qubits, plan->window_too_small ? 1u : 0u, plan->passes.size()};
+        for (const auto& p : plan->passes) {
+            w.push_back(p.global_mask);
+            w.push_back(p.first_operation);
+            w.push_back(p.end_operation);
+        }
+        if (w.size() > cap) {
+            g_error = "capacity";
+            return -1;
+        }
+        std::copy(w.begin(), w.end(), out);
+        return static_cast<std::int64_t>(w.size());
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
 }
 
 int ref_kernel_isa() {
