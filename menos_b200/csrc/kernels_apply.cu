@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(256) k_apply_diag(double2* __restrict__ st, ui
 // The generic k-operand kernel (dense_kernels.cpp:465-524), cooperative per
 // CTA: a batch of groups is gathered into shared memory, each thread then
 // forms whole outputs (sum over `in` in increasing order) and stores them.
-// Dynamic shared memory: the matrix (dim^2) then the batch (kGenBatch amps).
+// Dynamic shared memory: the matrix (dim^2, transposed) then the batch (kGenBatch amps).
 constexpr uint32_t kGenBatch = 1024;
 __global__ void __launch_bounds__(256) k_apply_generic(double2* __restrict__ st, uint32_t n, uint32_t k,
                                                        uint32_t q0, uint32_t q1, uint32_t q2, uint32_t q3,
@@ -115,10 +115,24 @@ __global__ void __launch_bounds__(256) k_apply_generic(double2* __restrict__ st,
     double2* mat = smem;
     double2* buf = smem + dim * dim;
     const uint32_t q[6] = {q0, q1, q2, q3, q4, q5};
-    uint64_t opmask = 0;
-    for (uint32_t j = 0; j < k; ++j) opmask |= uint64_t{1} << q[j];
-    const uint64_t rest = ((n >= 64) ? ~uint64_t{0} : ((uint64_t{1} << n) - 1)) & ~opmask;
-    for (uint32_t i = threadIdx.x; i < dim * dim; i += blockDim.x) mat[i] = matrix[i];
+    // The operands in increasing order: a group's base index is its number
+    // with a zero bit inserted at each of them, lowest first (k steps, not
+    // one per free qubit).
+    uint32_t qs[6] = {q0, q1, q2, q3, q4, q5};
+    for (uint32_t a = 1; a < k; ++a)
+        for (uint32_t b = a; b > 0 && qs[b - 1] > qs[b]; --b) {
+            const uint32_t t = qs[b];
+            qs[b] = qs[b - 1];
+            qs[b - 1] = t;
+        }
+    auto group_base = [&](uint64_t g) {
+        for (uint32_t j = 0; j < k; ++j) g = insert_zero(g, qs[j]);
+        return g;
+    };
+    // Transposed in shared memory (mat[in * dim + out]): the lanes of a
+    // quarter-warp form consecutive outputs, so their reads of one input's
+    // column are contiguous instead of dim entries apart (one bank).
+    for (uint32_t i = threadIdx.x; i < dim * dim; i += blockDim.x) mat[(i % dim) * dim + i / dim] = matrix[i];
     const uint64_t ngroups = (uint64_t{1} << n) >> k;
     const uint32_t per_batch = kGenBatch >> k;  // groups per batch (k <= 6 -> >= 16)
     const uint64_t nbatches = (ngroups + per_batch - 1) / per_batch;
@@ -129,7 +143,7 @@ __global__ void __launch_bounds__(256) k_apply_generic(double2* __restrict__ st,
             const uint64_t g = bt * per_batch + (s >> k);
             if (g >= ngroups) continue;
             const uint32_t local = s & (dim - 1);
-            uint64_t idx = pdep64(g, rest);
+            uint64_t idx = group_base(g);
             for (uint32_t j = 0; j < k; ++j)
                 if ((local >> j) & 1u) idx |= uint64_t{1} << q[j];
             buf[s] = st[idx];
@@ -140,9 +154,9 @@ __global__ void __launch_bounds__(256) k_apply_generic(double2* __restrict__ st,
             if (g >= ngroups) continue;
             const uint32_t out = s & (dim - 1);
             const double2* grp = buf + (s & ~(dim - 1));
-            double2 acc = cmul(mat[out * dim].x, mat[out * dim].y, grp[0]);
-            for (uint32_t in = 1; in < dim; ++in) acc = cadd(acc, cmul(mat[out * dim + in].x, mat[out * dim + in].y, grp[in]));
-            uint64_t idx = pdep64(g, rest);
+            double2 acc = cmul(mat[out].x, mat[out].y, grp[0]);
+            for (uint32_t in = 1; in < dim; ++in) acc = cadd(acc, cmul(mat[in * dim + out].x, mat[in * dim + out].y, grp[in]));
+            uint64_t idx = group_base(g);
             for (uint32_t j = 0; j < k; ++j)
                 if ((out >> j) & 1u) idx |= uint64_t{1} << q[j];
             st[idx] = canon(acc);
