@@ -373,6 +373,15 @@ __device__ __forceinline__ uint64_t count_below(const double* __restrict__ u, ui
     return lo;
 }
 
+// Each chunk boundary's shot index: bounds[j] = the uniforms below
+// cstart[j] (j = 0..nchunks), one thread per boundary, so the searches'
+// dependent loads overlap across the grid.
+__global__ void k_shot_bounds(const double* __restrict__ cstart, uint64_t nchunks, const double* __restrict__ u,
+                              uint64_t shots, uint64_t* __restrict__ bounds) {
+    const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j <= nchunks) bounds[j] = count_below(u, shots, cstart[j]);
+}
+
 // Step E: per chunk, the exact running sums of its elements, then each of
 // its shots placed on the first element whose sum exceeds the uniform.
 template <typename A>
@@ -380,20 +389,14 @@ __global__ void __launch_bounds__(kThreads) k_assign(const A* __restrict__ st, u
                                                      uint32_t chunk, const ChunkMap* __restrict__ maps,
                                                      const double* __restrict__ cstart,
                                                      const unsigned char* __restrict__ seq,
-                                                     const double* __restrict__ u, uint64_t shots,
+                                                     const double* __restrict__ u, const uint64_t* __restrict__ bounds,
                                                      uint64_t* __restrict__ basis) {
     __shared__ double cs[kSampleChunk];
-    __shared__ uint64_t s_lo, s_hi;
     const uint64_t j = blockIdx.x;
     const uint64_t base = j * chunk;
-    const double c0 = cstart[j], c1 = cstart[j + 1];
-    if (threadIdx.x == 0) {
-        s_lo = count_below(u, shots, c0);
-        s_hi = count_below(u, shots, c1);
-    }
-    __syncthreads();
-    const uint64_t lo = s_lo, hi = s_hi;
-    if (lo >= hi) return;
+    const double c0 = cstart[j];
+    const uint64_t lo = bounds[j], hi = bounds[j + 1];
+    if (lo >= hi) return;  // (uniform over the CTA)
     if (seq[j]) {
         // The reference's own adds, in order.
         for (uint32_t i = threadIdx.x; i < chunk; i += kThreads) cs[i] = (base + i < n_amps) ? prob(st[base + i]) : 0.0;
@@ -421,18 +424,39 @@ __global__ void __launch_bounds__(kThreads) k_assign(const A* __restrict__ st, u
             p[i] = (my + i < n_amps) ? prob(st[my + i]) : 0.0;
             acc = compose(acc, element_map(p[i], m.e));
         }
-        runs[threadIdx.x] = acc;
+        // The runs' maps composed in thread order (exact integer maps, so
+        // any grouping gives the same result): an inclusive scan within
+        // each warp by shuffles, the warps' totals in order, then each
+        // thread's exclusive prefix.
+        const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+        PMap inc = acc;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            PMap prev;
+            prev.inc0 = __shfl_up_sync(0xffffffffu, inc.inc0, o);
+            prev.inc1 = __shfl_up_sync(0xffffffffu, inc.inc1, o);
+            prev.par0 = __shfl_up_sync(0xffffffffu, inc.par0, o);
+            prev.par1 = __shfl_up_sync(0xffffffffu, inc.par1, o);
+            if (lane >= o) inc = compose(prev, inc);
+        }
+        if (lane == 31) runs[warp] = inc;
         __syncthreads();
         if (threadIdx.x == 0) {
             PMap run{0, 0, 0, 1};
-            for (int t = 0; t < kThreads; ++t) {
-                const PMap v = runs[t];
-                runs[t] = run;
+            for (uint32_t w = 0; w < kThreads / 32; ++w) {
+                const PMap v = runs[w];
+                runs[w] = run;
                 run = compose(run, v);
             }
         }
         __syncthreads();
-        const PMap before = runs[threadIdx.x];
+        PMap ex;  // this thread's runs before it within the warp
+        ex.inc0 = __shfl_up_sync(0xffffffffu, inc.inc0, 1);
+        ex.inc1 = __shfl_up_sync(0xffffffffu, inc.inc1, 1);
+        ex.par0 = __shfl_up_sync(0xffffffffu, inc.par0, 1);
+        ex.par1 = __shfl_up_sync(0xffffffffu, inc.par1, 1);
+        if (lane == 0) ex = PMap{0, 0, 0, 1};
+        const PMap before = compose(runs[warp], ex);
         int par = static_cast<int>(M0 & 1);
         long long M = M0 + (par ? before.inc1 : before.inc0);
         par = static_cast<int>(M & 1);
@@ -458,12 +482,9 @@ __global__ void __launch_bounds__(kThreads) k_assign(const A* __restrict__ st, u
 }
 
 // Shots at or past the final sum go to the last basis state.
-__global__ void k_leftover(const double* __restrict__ cstart, uint64_t nchunks, const double* __restrict__ u,
-                           uint64_t shots, uint64_t last, uint64_t* __restrict__ basis) {
-    __shared__ uint64_t s_from;
-    if (threadIdx.x == 0) s_from = count_below(u, shots, cstart[nchunks]);
-    __syncthreads();
-    for (uint64_t s = s_from + threadIdx.x; s < shots; s += blockDim.x) basis[s] = last;
+__global__ void k_leftover(const uint64_t* __restrict__ bounds, uint64_t nchunks, uint64_t shots, uint64_t last,
+                           uint64_t* __restrict__ basis) {
+    for (uint64_t s = bounds[nchunks] + threadIdx.x; s < shots; s += blockDim.x) basis[s] = last;
 }
 
 }  // namespace
@@ -475,7 +496,7 @@ size_t sample_scratch_bytes(uint32_t n, uint64_t shots) {
     auto al = [](size_t b) { return (b + 255) & ~size_t{255}; };
     (void)shots;
     return 2 * al(nchunks * 8) + al((nchunks + 1) * 8) + al(nchunks * sizeof(ChunkMap)) + al(nchunks) +
-           2 * al(nchunks * sizeof(SMap)) + al(nchunks) + al(nchunks * 8);
+           2 * al(nchunks * sizeof(SMap)) + al(nchunks) + al(nchunks * 8) + al((nchunks + 1) * 8);
 }
 
 template <typename A>
@@ -505,6 +526,8 @@ int launch_sample_t(const void* amps, uint32_t n, const double* dev_uniforms_sor
     auto* direct = reinterpret_cast<unsigned char*>(p);
     p += al(nchunks);
     auto* seg_c = reinterpret_cast<double*>(p);
+    p += al(nchunks * 8);
+    auto* bounds = reinterpret_cast<uint64_t*>(p);
     k_chunk_sums<<<static_cast<unsigned>(nchunks), kThreads, 0, s>>>(st, na, chunk, sums);
     k_scan_sums<<<1, 1024, 0, s>>>(sums, nchunks, starts);
     k_chunk_maps<<<static_cast<unsigned>(nchunks), kThreads, 0, s>>>(st, na, chunk, starts, sums, maps);
@@ -514,9 +537,11 @@ int launch_sample_t(const void* amps, uint32_t n, const double* dev_uniforms_sor
     k_seg_fill<<<static_cast<unsigned>((nchunks + kThreads - 1) / kThreads), kThreads, 0, s>>>(nchunks, maps, excl,
                                                                                                 direct, seg_c, cst,
                                                                                                 seq);
+    k_shot_bounds<<<static_cast<unsigned>((nchunks + 1 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+        cst, nchunks, dev_uniforms_sorted, shots, bounds);
     k_assign<<<static_cast<unsigned>(nchunks), kThreads, 0, s>>>(st, na, chunk, maps, cst, seq,
-                                                                 dev_uniforms_sorted, shots, dev_basis);
-    k_leftover<<<1, 256, 0, s>>>(cst, nchunks, dev_uniforms_sorted, shots, na - 1, dev_basis);
+                                                                 dev_uniforms_sorted, bounds, dev_basis);
+    k_leftover<<<1, 256, 0, s>>>(bounds, nchunks, shots, na - 1, dev_basis);
     return launch_status();
 }
 
@@ -572,7 +597,7 @@ int launch_exact_norm(const void* amps, uint32_t n, void* scratch, double* host_
 
 int launch_sample(const void* amps, uint32_t n, const double* dev_uniforms_sorted, uint64_t shots, void* scratch,
                   uint64_t* dev_basis, void* stream, int precision) {
-    note_launches(8);
+    note_launches(9);
     return precision == MB2_C64
                ? launch_sample_t<float2>(amps, n, dev_uniforms_sorted, shots, scratch, dev_basis, stream)
                : launch_sample_t<double2>(amps, n, dev_uniforms_sorted, shots, scratch, dev_basis, stream);
