@@ -168,8 +168,11 @@ int mb2_apply_program(mb2_state* state, const mb2_op* ops, uint32_t num_ops,
  * passes are the reference's greedy rule over the fusion plan's blocks
  * (pass_plan.cpp:43-121).  Each window is copied in, swept by the tiled
  * kernels with its blocks' operands remapped, and copied back; two device
- * windows on two streams let one window's copies overlap the other's sweep.
- * Bitwise the device-resident result.  Device memory: two windows (2 * 16 *
+ * windows on two streams let one window's copies overlap the other's sweep,
+ * and with no barrier between passes (a group's copies in wait only for the
+ * copies that last wrote its own chunks back) the copies run on across pass
+ * boundaries.  At most 2^24 chunks (L >= n - 24).  Bitwise the
+ * device-resident result.  Device memory: two windows (2 * 16 *
  * 2^W bytes, MB2_ERR_RESOURCE when they do not fit).  mb2_sweep_stats:
  * passes = window passes, launches = tile-pass launches.  A block with more
  * than W - L operands at or above L: MB2_ERR_INVALID.  Synchronous. */

@@ -718,13 +718,16 @@ int mb2_apply_program_windowed(mb2_state* s, const mb2_op* ops, uint32_t num_ops
     WindowPlan plan;
     if (int e = plan_windows(ctx, blocks, n, window_qubits, chunk_qubits, plan); e != MB2_OK) return e;
     const uint32_t L = plan.chunk_qubits, W = plan.window_qubits;
+    // Chunk bookkeeping is one entry per chunk: at most 2^24 of them.
+    if (n - L > 24) return fail(ctx, MB2_ERR_INVALID, "chunks of at least 2^(n - 24) amplitudes");
     MB2_CUDA(ctx, cudaSetDevice(ctx->device));
     // Whatever the state's own stream wrote (initialisation, earlier calls
     // through the mapped alias) lands before the copies read the host buffer.
     MB2_CUDA(ctx, cudaStreamSynchronize(s->stream));
     // Two windows, each with its stream: a window's copies in, sweep and
     // copies out are ordered on its stream, and the two streams overlap, so
-    // one window's copies run while the other is swept.
+    // one window's copies run while the other is swept.  Groups alternate
+    // between them across passes.
     const size_t win_bytes = (size_t{1} << W) * 16;
     size_t free_bytes = 0, total_bytes = 0;
     MB2_CUDA(ctx, cudaMemGetInfo(&free_bytes, &total_bytes));
@@ -734,9 +737,11 @@ int mb2_apply_program_windowed(mb2_state* s, const mb2_op* ops, uint32_t num_ops
         cudaStream_t st[2] = {nullptr, nullptr};
         void* win[2] = {nullptr, nullptr};
         void* prog = nullptr;
+        std::vector<cudaEvent_t> events;
         ~Res() {
             for (cudaStream_t t : st)
                 if (t != nullptr) cudaStreamSynchronize(t);
+            for (cudaEvent_t e : events) cudaEventDestroy(e);
             for (void* p : win)
                 if (p != nullptr) cudaFree(p);
             if (prog != nullptr) cudaFree(prog);
@@ -744,19 +749,22 @@ int mb2_apply_program_windowed(mb2_state* s, const mb2_op* ops, uint32_t num_ops
                 if (t != nullptr) cudaStreamDestroy(t);
         }
     } r;
-    size_t prog_bytes = 0;
     for (int b = 0; b < 2; ++b) {
         MB2_CUDA(ctx, cudaStreamCreateWithFlags(&r.st[b], cudaStreamNonBlocking));
         MB2_CUDA(ctx, cudaMalloc(&r.win[b], win_bytes));
     }
-    auto* host = static_cast<unsigned char*>(s->host_amps);
-    const uint64_t global_bits = n - L;
-    const uint64_t all_globals = global_bits >= 64 ? ~uint64_t{0} : (uint64_t{1} << global_bits) - 1;
-    for (const WindowPass& wp : plan.passes) {
-        const uint32_t g = static_cast<uint32_t>(std::popcount(wp.global_mask));
-        const uint32_t n_eff = L + g;
-        // The pass's blocks on window qubits: local qubits stay, global
-        // qubit L + b becomes L + (its rank among G).
+    // Every pass's tiled program, planned on its window qubits (local qubits
+    // stay, global qubit L + b becomes L + its rank among G) and uploaded once.
+    struct PassProg {
+        mb2::TileProgram prog;
+        uint32_t n_eff = 0;
+        size_t off = 0, doff = 0, goff = 0;
+    };
+    std::vector<PassProg> progs(plan.passes.size());
+    size_t total = 0;
+    for (size_t pi = 0; pi < plan.passes.size(); ++pi) {
+        const WindowPass& wp = plan.passes[pi];
+        const uint32_t n_eff = L + static_cast<uint32_t>(std::popcount(wp.global_mask));
         std::vector<mb2::Block> local(blocks.begin() + static_cast<std::ptrdiff_t>(wp.first),
                                       blocks.begin() + static_cast<std::ptrdiff_t>(wp.end));
         for (mb2::Block& b : local)
@@ -767,65 +775,93 @@ int mb2_apply_program_windowed(mb2_state* s, const mb2_op* ops, uint32_t num_ops
                 }
         const uint32_t dflt = n_eff <= 16 ? mb2::kMaxTileQubits : ctx->tile_c128.load();
         const uint32_t m = std::min(tile_width(dflt, n_eff, local), n_eff);
-        mb2::TileProgram prog;
+        PassProg& pp = progs[pi];
         try {
-            prog = mb2::plan_tile_program(local, n_eff, m);
+            pp.prog = mb2::plan_tile_program(local, n_eff, m);
         } catch (const std::exception& e) {
             return fail(ctx, MB2_ERR_INVALID, e.what());
         }
-        const size_t ibytes = prog.words.size() * sizeof(uint32_t);
-        const size_t dbytes = prog.data.size() * sizeof(double);
-        const size_t gbytes = prog.gdata.size() * sizeof(double);
-        const size_t doff = (ibytes + 255) & ~size_t{255};
-        const size_t goff = (doff + dbytes + 255) & ~size_t{255};
-        const size_t need = goff + gbytes + 256;
-        if (need > prog_bytes) {
-            if (r.prog != nullptr) MB2_CUDA(ctx, cudaFree(r.prog));
-            r.prog = nullptr;
-            MB2_CUDA(ctx, cudaMalloc(&r.prog, need));
-            prog_bytes = need;
+        pp.n_eff = n_eff;
+        pp.off = total;
+        pp.doff = total + ((pp.prog.words.size() * sizeof(uint32_t) + 255) & ~size_t{255});
+        pp.goff = pp.doff + ((pp.prog.data.size() * sizeof(double) + 255) & ~size_t{255});
+        total = pp.goff + ((pp.prog.gdata.size() * sizeof(double) + 255) & ~size_t{255}) + 256;
+    }
+    {
+        std::vector<unsigned char> staged(total, 0);
+        for (const PassProg& pp : progs) {
+            std::memcpy(staged.data() + pp.off, pp.prog.words.data(), pp.prog.words.size() * sizeof(uint32_t));
+            if (!pp.prog.data.empty())
+                std::memcpy(staged.data() + pp.doff, pp.prog.data.data(), pp.prog.data.size() * sizeof(double));
+            if (!pp.prog.gdata.empty())
+                std::memcpy(staged.data() + pp.goff, pp.prog.gdata.data(), pp.prog.gdata.size() * sizeof(double));
         }
-        std::vector<unsigned char> staged(need, 0);
-        std::memcpy(staged.data(), prog.words.data(), ibytes);
-        if (dbytes) std::memcpy(staged.data() + doff, prog.data.data(), dbytes);
-        if (gbytes) std::memcpy(staged.data() + goff, prog.gdata.data(), gbytes);
-        // Both streams are idle here (the previous pass ended with a sync).
-        MB2_CUDA(ctx, cudaMemcpy(r.prog, staged.data(), need, cudaMemcpyHostToDevice));
-        auto* pbase = static_cast<unsigned char*>(r.prog);
-        const auto* dev_words = reinterpret_cast<const uint32_t*>(pbase);
-        const auto* dev_sdata = reinterpret_cast<const double*>(pbase + doff);
-        const auto* dev_gdata = reinterpret_cast<const double*>(pbase + goff);
+        MB2_CUDA(ctx, cudaMalloc(&r.prog, total));
+        MB2_CUDA(ctx, cudaMemcpy(r.prog, staged.data(), total, cudaMemcpyHostToDevice));
+    }
+    auto* pbase = static_cast<unsigned char*>(r.prog);
+    auto* host = static_cast<unsigned char*>(s->host_amps);
+    const uint64_t global_bits = n - L;
+    const uint64_t all_globals = global_bits >= 64 ? ~uint64_t{0} : (uint64_t{1} << global_bits) - 1;
+    // No barrier between passes: each chunk remembers the event recorded
+    // after the copy that last wrote it back, and a group's copies in wait on
+    // the events of the chunks it reads (which are the chunks it writes), so
+    // a group starts as soon as its own chunks are home and the two copy
+    // directions stay busy across pass boundaries.
+    std::vector<cudaEvent_t> last_writer(size_t{1} << global_bits, nullptr);
+    uint64_t turn = 0;  // alternates the windows across groups and passes
+    std::vector<cudaEvent_t> waits;
+    for (size_t pi = 0; pi < plan.passes.size(); ++pi) {
+        const WindowPass& wp = plan.passes[pi];
+        const PassProg& pp = progs[pi];
+        const uint32_t g = static_cast<uint32_t>(std::popcount(wp.global_mask));
+        const auto* dev_words = reinterpret_cast<const uint32_t*>(pbase + pp.off);
+        const auto* dev_sdata = reinterpret_cast<const double*>(pbase + pp.doff);
+        const auto* dev_gdata = reinterpret_cast<const double*>(pbase + pp.goff);
         // Chunks whose slots follow each other and whose host addresses do too
         // (the lowest global qubits, when G holds them) move in one copy.
         const uint32_t run = static_cast<uint32_t>(std::countr_one(wp.global_mask));
         const size_t copy_bytes = (size_t{1} << (L + run)) * 16;
         const uint64_t other = all_globals & ~wp.global_mask;
         const uint64_t groups = uint64_t{1} << (global_bits - g);
-        for (uint64_t grp = 0; grp < groups; ++grp) {
-            const int b = static_cast<int>(grp & 1u);
+        for (uint64_t grp = 0; grp < groups; ++grp, ++turn) {
+            const int b = static_cast<int>(turn & 1u);
+            cudaStream_t st = r.st[b];
             auto* win = static_cast<unsigned char*>(r.win[b]);
             const uint64_t base_chunk = pdep_host(grp, other);
+            waits.clear();
+            for (uint64_t slot = 0; slot < (uint64_t{1} << g); ++slot) {
+                const cudaEvent_t e = last_writer[base_chunk | pdep_host(slot, wp.global_mask)];
+                if (e != nullptr && std::find(waits.begin(), waits.end(), e) == waits.end()) waits.push_back(e);
+            }
+            for (cudaEvent_t e : waits) MB2_CUDA(ctx, cudaStreamWaitEvent(st, e, 0));
             for (uint64_t slot = 0; slot < (uint64_t{1} << g); slot += uint64_t{1} << run) {
                 const uint64_t chunk = base_chunk | pdep_host(slot, wp.global_mask);
                 MB2_CUDA(ctx, cudaMemcpyAsync(win + ((slot << L) * 16), host + ((chunk << L) * 16), copy_bytes,
-                                              cudaMemcpyHostToDevice, r.st[b]));
+                                              cudaMemcpyHostToDevice, st));
             }
-            for (const mb2::TilePass& pass : prog.passes) {
-                const int rc = mb2::launch_tile_pass(win, n_eff, pass, dev_words, dev_sdata, dev_gdata, ctx->sm_count,
-                                                     r.st[b]);
+            for (const mb2::TilePass& pass : pp.prog.passes) {
+                const int rc = mb2::launch_tile_pass(win, pp.n_eff, pass, dev_words, dev_sdata, dev_gdata,
+                                                     ctx->sm_count, st);
                 if (rc != MB2_OK) return fail(ctx, rc, std::string("tile pass launch: ") + mb2::last_cuda_error_string());
                 s->stats.launches += 1;
             }
             for (uint64_t slot = 0; slot < (uint64_t{1} << g); slot += uint64_t{1} << run) {
                 const uint64_t chunk = base_chunk | pdep_host(slot, wp.global_mask);
                 MB2_CUDA(ctx, cudaMemcpyAsync(host + ((chunk << L) * 16), win + ((slot << L) * 16), copy_bytes,
-                                              cudaMemcpyDeviceToHost, r.st[b]));
+                                              cudaMemcpyDeviceToHost, st));
             }
+            cudaEvent_t done = nullptr;
+            MB2_CUDA(ctx, cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+            r.events.push_back(done);
+            MB2_CUDA(ctx, cudaEventRecord(done, st));
+            for (uint64_t slot = 0; slot < (uint64_t{1} << g); ++slot)
+                last_writer[base_chunk | pdep_host(slot, wp.global_mask)] = done;
         }
-        MB2_CUDA(ctx, cudaStreamSynchronize(r.st[0]));
-        MB2_CUDA(ctx, cudaStreamSynchronize(r.st[1]));
         s->stats.passes += 1;
     }
+    MB2_CUDA(ctx, cudaStreamSynchronize(r.st[0]));
+    MB2_CUDA(ctx, cudaStreamSynchronize(r.st[1]));
     return MB2_OK;
 }
 
