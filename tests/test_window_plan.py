@@ -58,3 +58,21 @@ def test_chunk_choice_is_the_reference(ref, name, make, n, window):
     c = make(n)
     L, _too_small, passes = ref.pass_plan(as_oracle(c), 0, window)
     assert window_plan(c, window, 0) == (L, passes)
+
+
+def test_small_windows_keep_chunks_of_at_least_2_16(ref):
+    """Windows of at most 2^24 amplitudes: the same rule (fewest passes,
+    larger chunk on a tie) searched from the window down to 2^min(16, W)
+    only (the reference goes on down to one amplitude), smaller chunks only
+    when none of those fits."""
+    n = 22
+    c = workloads.config_c2(n=n, depth=6)
+    for window in (18, 20):
+        L, passes = window_plan(c, window, 0)
+        assert 16 <= L <= window
+        best = min((len(window_plan(c, window, l)[1]), -l) for l in range(16, window + 1)
+                   if window_plan(c, window, l) is not None)
+        assert (len(passes), -L) == best
+    # A window too narrow for chunks of 2^16 still finds a plan below it.
+    L, passes = window_plan(c, 12, 0)
+    assert L < 12 and passes
