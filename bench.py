@@ -336,7 +336,10 @@ def main():
                      "traffic_source": "ncu dram__bytes_read+write of one pass at 28 qubits, scaled by the "
                                        "state size (profiles/k_tile_pass_c2_28q_ncu_full.md)",
                      "peak_source": peak_src,
-                     "algorithmic_bytes_per_launch": 2 * state_bytes},
+                     "algorithmic_bytes_per_launch": 2 * state_bytes,
+                     # Blocks x one state pass each / sweep time: what the multi-gate
+                     # passes buy; reported beside `achieved`, never as the fraction.
+                     "gate_equivalent_gbs": round(int(stats.blocks) * 2 * state_bytes / (sweep_avg * 1e-3) / 1e9, 1)},
         "fp64": {"kernel": "k_tile_pass", "achieved_ops_per_s": round(stats.fp64_ops_per_amp * (1 << n) /
                                                                      (sweep_avg * 1e-3), 1),
                  "peak_ops_per_s": round(fp64_peak, 1), "peak_source": "measured (mb2_probe_rates)",
