@@ -18,8 +18,9 @@
  * The complex64 precision path (MB2_C64 states) runs the same tiled sweep with
  * gate matrices composed in FP64: each phase's gates on its four register
  * qubits compose into one 16x16 complex matrix applied on the tcgen05 tensor
- * cores as a split-precision GEMM (TF32 high and low parts of both operands,
- * FP32 accumulation), or, per option, gate by gate with FP32 fused
+ * cores as a split-precision GEMM (FP16 high and low parts of both operands
+ * after a power-of-two scaling of each tile, the products lo*hi, hi*lo and
+ * hi*hi, FP32 accumulation), or, per option, gate by gate with FP32 fused
  * multiply-adds; norms, expectations and sampling probabilities accumulate
  * in FP64.
  *
@@ -556,7 +557,8 @@ int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
 /* The complex64 tensor-core step alone, on the context's device: 256 rows of
  * 16 complex64 amplitudes (rows: 256 * 32 floats, interleaved) times the
  * 16x16 complex matrix (row-major, interleaved doubles) as the tile pass
- * applies a phase -- split-TF32 operands, FP32 accumulation -- into out
+ * applies a phase -- the rows scaled by a power of two, split-FP16
+ * operands, FP32 accumulation, the scale taken out again -- into out
  * (256 * 32 floats): out_row = matrix * in_row.  Lets tests check the
  * tensor-memory and operand layouts in isolation.  Has no counterpart in the
  * reference. */

@@ -189,7 +189,7 @@ constexpr uint32_t kPhase = 200;
 constexpr uint32_t kPhaseWords = 29;
 constexpr uint32_t kSmem = 201;  // aux = k; extra words: tile positions, gdata offset (doubles)
 // Tensor-core pass: apply the pass's composed phase matrix number aux (its
-// split-TF32 operands staged in shared memory) to the registers' amplitudes.
+// split-FP16 operands staged in shared memory) to the registers' amplitudes.
 constexpr uint32_t kMma = 202;
 // A sign monomial word: bits 0-15 the register slots j (of 16) whose
 // register-bit factors are all 1 (0xffff: no register factor), bits 16-31

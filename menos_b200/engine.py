@@ -72,7 +72,7 @@ class Context:
 
     def tc_probe(self, rows: np.ndarray, matrix: np.ndarray) -> np.ndarray:
         """The tensor-core step alone (mb2_debug_tc_probe): rows (256 x 16
-        complex64) times matrix^T (16 x 16 complex), split-TF32 on tcgen05."""
+        complex64) times matrix^T (16 x 16 complex), split-FP16 on tcgen05."""
         r = np.ascontiguousarray(np.asarray(rows, np.complex64).reshape(256, 16))
         m = np.ascontiguousarray(np.asarray(matrix, np.complex128).reshape(16, 16))
         out = np.zeros((256, 16), np.complex64)

@@ -1,9 +1,9 @@
-"""The complex64 tensor-core path (tcgen05, split-TF32 operands, FP32
-accumulation) on the GPU.
+"""The complex64 tensor-core path (tcgen05 kind::f16, split-FP16 operands,
+FP32 accumulation) on the GPU.
 
 * The tensor-core step alone (mb2_debug_tc_probe): 256 rows of 16 complex
   amplitudes times a 16x16 complex matrix equal the FP64 product within the
-  split's precision (about 2^-21 relative per operand), for random
+  split's precision (about 2^-21 of the largest amplitude), for random
   unitaries, the identity and a permutation -- which pins the tensor-memory
   and shared-memory operand layouts.
 * Whole sweeps: the tensor-core passes against the complex128 path (itself
@@ -41,7 +41,7 @@ def test_tc_probe_matches_fp64_product(ctx):
 
 def test_tc_probe_row_and_column_placement(ctx):
     # One nonzero amplitude per row, a matrix with one nonzero per row: every
-    # output lands where the layout says, exactly (products of TF32 values).
+    # output lands where the layout says, exactly (every value is exact in FP16).
     rows = np.zeros((256, 16), np.complex64)
     for r in range(256):
         rows[r, r % 16] = (r + 1) + 0.5j * (r % 7)
