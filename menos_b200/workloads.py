@@ -105,6 +105,36 @@ def hea(n: int, layers: int, seed: int, circ: Circuit | None = None) -> Circuit:
     return c
 
 
+CROSSOVER_LAYERS = 6
+
+
+def crossover(n: int, circ: Circuit | None = None) -> Circuit:
+    """The chunked tier's crossover family (benchmarks/crossover_circuit.h:
+    make_crossover_circuit): per layer H on every qubit, T on qubit 0, then
+    CX on neighbour pairs starting at qubit layer % 2; six layers."""
+    c = circ if circ is not None else Circuit(n)
+    for layer in range(CROSSOVER_LAYERS):
+        for q in range(n):
+            c.gate("h", [q])
+        c.gate("t", [0])
+        for q in range(layer % 2, n - 1, 2):
+            c.gate("cx", [q, q + 1])
+    return c
+
+
+def ladder(n: int, circ: Circuit | None = None) -> Circuit:
+    """The chunked tier's ladder family (tests/engines/dense_tiered/
+    pass_plan_test.cpp: ladder): per layer H on every qubit, then the CX
+    chain q -> q + 1; six layers."""
+    c = circ if circ is not None else Circuit(n)
+    for _ in range(CROSSOVER_LAYERS):
+        for q in range(n):
+            c.gate("h", [q])
+        for q in range(n - 1):
+            c.gate("cx", [q, q + 1])
+    return c
+
+
 def hea_bindings(n: int, layers: int, count: int, seed: int):
     """`count` parameter rows for hea(n, layers): per layer and qubit RY(theta)
     then RZ(phi), angles in [-pi, pi) from mt19937_64(seed), in op order."""
