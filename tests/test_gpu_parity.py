@@ -13,7 +13,7 @@ from menos_b200.engine import C64 as MB2_C64, C128 as MB2_C128
 from menos_b200._lib import MB2Error, ResourceExceeded
 from menos_b200.circuit import OP, Circuit
 from test_host import as_oracle_circuit
-from test_oracle_pin import bits_equal, rand_state, rand_unitary, random_circuit
+from test_oracle_pin import Y_CONVENTION, bits_equal, rand_state, rand_unitary, random_circuit
 
 pytestmark = pytest.mark.gpu
 
@@ -186,6 +186,17 @@ def test_expectation_y_convention(ctx):
     st.copy_in(np.array([1, 1j], np.complex128) / np.sqrt(2))
     v = st.expectation([(1, 1), (1, 0), (0, 1)])
     assert abs(v[0] - 1.0) < 1e-15 and abs(v[1]) < 1e-15 and abs(v[2]) < 1e-15
+    # The reference's circuits for the same convention, through the sweep.
+    for n, gates, terms in Y_CONVENTION:
+        c = Circuit(n)
+        for name, qs in gates:
+            c.gate(name, qs)
+        st = DeviceState(ctx, n)
+        st.init(0.0)
+        st.apply_program(c)
+        got = st.expectation([(x, z) for x, z, _ in terms])
+        for (x, z, want), g in zip(terms, got):
+            assert abs(g - want) <= EXP_TOL, (n, x, z, g)
 
 
 def test_sampling_identical_counts(ctx, oracle):
@@ -204,6 +215,13 @@ def test_sampling_golden_plus_state(ctx):
     st = DeviceState(ctx, 1)
     st.copy_in(np.array([1, 1], np.complex128) / np.sqrt(2.0))
     assert st.sample(20, 42, [(0, 0)]) == {0: 9, 1: 11}
+    # tests/engines/dense/sample_test.cpp:39-83: zero shots give no counts;
+    # basis bits reach clbits through the targets (|q1=1, q0=0>, q0 -> c1,
+    # q1 -> c0: outcome 1).
+    assert st.sample(0, 1, [(0, 0)]) == {}
+    st2 = DeviceState(ctx, 2)
+    st2.copy_in(np.array([0, 0, 1, 0], np.complex128))
+    assert st2.sample(10, 1, [(0, 1), (1, 0)]) == {1: 10}
 
 
 def test_engine_execute_matches_reference(ctx, ref):

@@ -42,6 +42,52 @@ def test_golden_counts_seed42_plus_state(oracle):
     assert oracle.sample(plus, 20, 42, [(0, 0)]) == {0: 9, 1: 11}
 
 
+def test_sampler_known_answers(oracle):
+    # tests/engines/dense/sample_test.cpp:39-83: zero shots give no counts;
+    # the same seed gives the same counts; every shot is counted; basis bits
+    # reach clbits through the targets (|q1=1, q0=0>, q0 -> c1, q1 -> c0:
+    # outcome 1).
+    plus = np.array([1, 1], np.complex128) / np.sqrt(2.0)
+    assert oracle.sample(plus, 0, 1, [(0, 0)]) == {}
+    assert oracle.sample(plus, 1000, 2024, [(0, 0)]) == oracle.sample(plus, 1000, 2024, [(0, 0)])
+    assert sum(oracle.sample(plus, 12345, 9, [(0, 0)]).values()) == 12345
+    basis2 = np.array([0, 0, 1, 0], np.complex128)
+    assert oracle.sample(basis2, 10, 1, [(0, 1), (1, 0)]) == {1: 10}
+
+
+def test_sampler_chi_square(oracle):
+    # tests/engines/dense/sample_test.cpp:99-127: 1e5 shots of probabilities
+    # 0.1..0.4 at seed 31415 stay below the chi-square critical value for
+    # three degrees of freedom at 0.001 (16.2662).
+    p = np.array([0.1, 0.2, 0.3, 0.4])
+    counts = oracle.sample(np.sqrt(p).astype(np.complex128), 100000, 31415, [(0, 0), (1, 1)])
+    obs = np.array([counts.get(k, 0) for k in range(4)], float)
+    assert float(np.sum((obs - p * 1e5) ** 2 / (p * 1e5))) < 16.2662
+
+
+# tests/engines/dense/dense_engine_test.cpp:279-330, Y = i X Z (Qiskit's
+# convention): (qubits, gates, [(x mask, z mask, <P>)]) for S H|0>,
+# S(0) CX(0,1) H(0)|00> and the product (S H|0>)(H|0>)(S H|0>).
+Y_CONVENTION = [
+    (1, [("h", [0]), ("s", [0])], [(1, 1, 1.0), (1, 0, 0.0), (0, 1, 0.0)]),
+    (2, [("h", [0]), ("cx", [0, 1]), ("s", [0])],
+     [(0b11, 0b10, 1.0), (0b11, 0b01, 1.0), (0b00, 0b11, 1.0), (0b11, 0b11, 0.0), (0b11, 0b00, 0.0)]),
+    (3, [("h", [0]), ("s", [0]), ("h", [1]), ("h", [2]), ("s", [2])],
+     [(0b001, 0b001, 1.0), (0b010, 0b010, 0.0), (0b100, 0b100, 1.0), (0b101, 0b101, 1.0),
+      (0b011, 0b011, 0.0), (0b001, 0b000, 0.0), (0b000, 0b001, 0.0)]),
+]
+
+
+def test_y_convention_known_answers(oracle):
+    for n, gates, terms in Y_CONVENTION:
+        c = Circuit(n)
+        for name, qs in gates:
+            c.gate(name, qs)
+        s = oracle.run(c)
+        for x, z, want in terms:
+            assert abs(oracle.expectation(s, x, z) - want) <= 1e-12, (n, x, z)
+
+
 def test_golden_fixtures(oracle):
     g = golden()
     for case in g["uniforms"]:
