@@ -372,6 +372,8 @@ private:
         if (auto reason = ir::first_noise_reason(*request.operations); reason.has_value())
             return CostEstimate{false, 0, 0, *reason, {}};
         if (request.num_qubits > 34) return CostEstimate{false, 0, 0, "more than 34 qubits on one B200", {}};
+        if (request.num_qubits == 0)
+            return CostEstimate{false, 0, 0, "a region of no qubits (one amplitude) is not worth a device", {}};
         Ops ops = to_mb2(*request.operations);
         const uint32_t n = request.num_qubits;
         mb2_sweep_options o{request.fuse_gates ? 1 : 0, 0, 0, 0};
