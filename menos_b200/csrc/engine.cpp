@@ -437,7 +437,7 @@ int mb2_apply_matrix_generic(mb2_state* s, const double* matrix, const uint32_t*
 int mb2_apply_program_monitored(mb2_state* s, const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts,
                                 mb2_boundary_fn boundary, void* user) {
     if (s == nullptr || (ops == nullptr && num_ops != 0)) return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     for (uint32_t i = 0; i < num_ops; ++i) {
         if (ops[i].opcode == MB2_MEASURE) continue;
@@ -895,7 +895,7 @@ int mb2_fusion_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options
 int mb2_estimate_sweep(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t num_qubits,
                        mb2_sweep_estimate* out) {
     if (out == nullptr || (ops == nullptr && num_ops != 0) || num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     *out = mb2_sweep_estimate{};
     try {
@@ -1775,7 +1775,7 @@ int mb2_debug_run_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
     if ((ops == nullptr && num_ops != 0) || num_qubits < 1 || num_qubits > 40 || (state != nullptr && num_qubits > 28) ||
         (precision != MB2_C128 && precision != MB2_C64))
         return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     try {
         const std::vector<mb2::Block> blocks = mb2::build_blocks(ops, num_ops, o.fuse_gates != 0, static_cast<uint32_t>(o.fusion_width));
@@ -1859,7 +1859,7 @@ int mb2_debug_schedule(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_opti
     if (precision != MB2_C128 && precision != MB2_C64) return MB2_ERR_INVALID;
     const bool c64 = precision == MB2_C64;
     if (num_qubits < 1 || num_qubits > 40) return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     std::vector<mb2::Block> blocks;
     std::vector<uint32_t> order, order_pass;
@@ -1937,7 +1937,7 @@ std::vector<mb2_op> probe_brick(uint32_t n, uint32_t layers) {
 }
 
 int time_sweep(mb2_state* st, const std::vector<mb2_op>& ops, uint32_t tile, double* ms, int32_t fuse = 1) {
-    mb2_sweep_options o{fuse, 0, static_cast<int32_t>(tile), 0};
+    mb2_sweep_options o{fuse, 0, static_cast<int32_t>(tile), 0, 0, 0};
     if (int e = mb2_init(st, 0.0); e != MB2_OK) return e;
     if (int e = mb2_apply_program(st, ops.data(), static_cast<uint32_t>(ops.size()), &o); e != MB2_OK) return e;
     cudaEvent_t a = nullptr, b = nullptr;
@@ -2082,7 +2082,7 @@ int mb2_estimate_sweep_time(mb2_context* ctx, const mb2_op* ops, uint32_t num_op
     if (ctx == nullptr || seconds == nullptr || (ops == nullptr && num_ops != 0) || num_qubits < 1 ||
         num_qubits > 40 || (precision != MB2_C128 && precision != MB2_C64))
         return MB2_ERR_INVALID;
-    mb2_sweep_options o{1, 0, 0, 0};
+    mb2_sweep_options o{1, 0, 0, 0, 0, 0};
     if (opts != nullptr) o = *opts;
     mb2_tuning t;
     {

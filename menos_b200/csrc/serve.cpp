@@ -135,7 +135,7 @@ void run_request(mb2_server* s, cudaStream_t stream, Request& r, Done& d) {
     int rc = mb2::state_on_stream(s->ctx, r.n, ~uint64_t{0}, stream, &st, r.precision);
     if (rc == MB2_OK) rc = mb2_init(st, r.global_phase);
     if (rc == MB2_OK) {
-        mb2_sweep_options o{r.fuse, 0, 0, 0};
+        mb2_sweep_options o{r.fuse, 0, 0, 0, 0, 0};
         rc = mb2_apply_program(st, r.ops.data(), static_cast<uint32_t>(r.ops.size()), &o);
     }
     // A complex64 state is renormalised in FP64 (its norm drifts by FP32

@@ -298,7 +298,7 @@ public:
         check(mb2_state_alloc(context(), request.num_qubits, MB2_C128, free_bytes, &st.s), "state");
         st.charge = common::MemoryLedger::Charge(state_bytes, common::MemoryLedger::Space::Device);
         check(mb2_init(st.s, request.global_phase), "init");
-        mb2_sweep_options o{request.fuse_gates ? 1 : 0, 0, 0, 0};
+        mb2_sweep_options o{request.fuse_gates ? 1 : 0, 0, 0, 0, 0, 0};
         if (request.monitor != nullptr) {
             MonitorBridge bridge{request.monitor, nullptr};
             const int rc = mb2_apply_program_monitored(st.s, ops.ops.data(), static_cast<uint32_t>(ops.ops.size()),
@@ -376,7 +376,7 @@ private:
             return CostEstimate{false, 0, 0, "a region of no qubits (one amplitude) is not worth a device", {}};
         Ops ops = to_mb2(*request.operations);
         const uint32_t n = request.num_qubits;
-        mb2_sweep_options o{request.fuse_gates ? 1 : 0, 0, 0, 0};
+        mb2_sweep_options o{request.fuse_gates ? 1 : 0, 0, 0, 0, 0, 0};
         mb2_sweep_estimate e{};
         if (mb2_estimate_sweep(ops.ops.data(), static_cast<uint32_t>(ops.ops.size()), &o, n, &e) != MB2_OK)
             return CostEstimate{false, 0, 0, "dense_b200: operations rejected", {}};
