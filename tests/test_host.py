@@ -51,6 +51,36 @@ def test_gate_table_bitwise(oracle, opcode):
         assert bits_equal(out[:2 * ref.size], ref.view(np.float64).ravel())
 
 
+def gate(name, params=()):
+    p = np.zeros(3)
+    p[:len(params)] = params
+    out = np.zeros(128, np.float64)
+    assert _lib.lib().mb2_gate_matrix(OP[name], p.ctypes.data, out.ctypes.data, 128) == 0
+    k = 3 if name == "ccx" else (2 if name in ("cx", "cz", "swap", "cp", "rzz") else 1)
+    d = 1 << k
+    return out[:2 * d * d].view(np.complex128).reshape(d, d)
+
+
+def test_gate_table_known_answers():
+    # tests/ir/gate_table_test.cpp:105-190.  RZZ(t) is diagonal with
+    # e^{-it/2} on |00>, |11> and e^{it/2} on |01>, |10>, and equals
+    # CX RZ(t) CX (RZ on operand 1, CX flipping bit 1 when bit 0 is set).
+    t = 0.83
+    rzz = gate("rzz", [t])
+    want = np.diag([np.exp(-0.5j * t), np.exp(0.5j * t), np.exp(0.5j * t), np.exp(-0.5j * t)])
+    assert np.max(np.abs(rzz - want)) <= 1e-15
+    rz = gate("rz", [t])
+    for i in range(4):
+        flipped = i ^ 2 if i & 1 else i
+        assert abs(rzz[i, i] - rz[(flipped >> 1) & 1, (flipped >> 1) & 1]) <= 1e-15
+    # RZ is not P: they differ by a global phase.
+    assert abs(gate("rz", [1.234])[0, 0] - gate("p", [1.234])[0, 0]) > 1e-6
+    # CX operands are (control, target) = (bit 0, bit 1): |control set> at
+    # local index 1 goes to index 3.
+    cx = gate("cx")
+    assert cx[3, 1] == 1.0 and cx[1, 1] == 0.0
+
+
 def test_gate_table_rejects_non_gates():
     out = np.zeros(128, np.float64)
     assert _lib.lib().mb2_gate_matrix(OP["unitary"], None, out.ctypes.data, 128) == 1
