@@ -164,6 +164,59 @@ def test_reference_dm_engine_matches_numpy(ref, n):
     assert np.max(np.abs(vec.reshape(dim, dim).T - rho)) < 1e-12
 
 
+def test_restatement_known_answers(oracle):
+    """The closed forms of the reference's own density-matrix tests
+    (tests/engines/density_matrix/density_matrix_engine_test.cpp:132-227)
+    on the numpy restatement: no reference build needed."""
+    def trace(circ, x, z):
+        return np.trace(pauli_matrix(circ.num_qubits, x, z) @ numpy_rho(circ, oracle.gate_matrix))
+
+    def close(a, b):
+        return abs(a - b) < 1e-12
+
+    # An empty circuit is |00><00|.
+    empty = pyoracle.Circuit(2)
+    assert all(close(trace(empty, 0, z), 1.0) for z in range(4))
+    assert all(close(trace(empty, x, z), 0.0) for x in range(1, 4) for z in range(4))
+    # Depolarizing with p = 0.3: <Z> = 0.7 on |0>, <X> = 0.7 on |+>.
+    zero = pyoracle.Circuit(1)
+    zero.channel((0,), depolarizing(0.3))
+    assert close(trace(zero, 0, 1), 0.7) and close(trace(zero, 1, 0), 0.0) and close(trace(zero, 0, 0), 1.0)
+    plus = pyoracle.Circuit(1)
+    plus.gate("h", [0])
+    plus.channel((0,), depolarizing(0.3))
+    assert close(trace(plus, 1, 0), 0.7)
+    # Amplitude damping with gamma = 0.25 on |1>: <Z> = 2 gamma - 1.
+    one = pyoracle.Circuit(1)
+    one.gate("x", [0])
+    one.channel((0,), amplitude_damping(0.25))
+    assert close(trace(one, 0, 1), -0.5)
+    # A one-operator channel whose operator is CX's matrix is the CX gate.
+    as_gate = pyoracle.Circuit(2)
+    as_gate.gate("h", [0]).gate("ry", [1], [0.4]).gate("cx", [0, 1])
+    as_channel = pyoracle.Circuit(2)
+    as_channel.gate("h", [0]).gate("ry", [1], [0.4])
+    as_channel.channel((0, 1), oracle.gate_matrix(pyoracle.OP["cx"], ())[None])
+    # A two-qubit channel K (x) I on operands (1, 0) is K on qubit 1.
+    one_q = amplitude_damping(0.4)
+    two_q = np.zeros((2, 4, 4), np.complex128)
+    for i, k in enumerate(one_q):
+        for r in range(4):
+            for c in range(4):
+                if r >> 1 == c >> 1:
+                    two_q[i, r, c] = k[r & 1, c & 1]
+    single = pyoracle.Circuit(2)
+    single.gate("x", [1]).gate("h", [0])
+    single.channel((1,), one_q)
+    wide = pyoracle.Circuit(2)
+    wide.gate("x", [1]).gate("h", [0])
+    wide.channel((1, 0), two_q)
+    for x in range(4):
+        for z in range(4):
+            assert close(trace(as_channel, x, z), trace(as_gate, x, z))
+            assert close(trace(wide, x, z), trace(single, x, z))
+
+
 def test_restated_sequence_is_bitwise_the_reference_engine(ref):
     """The reference engine's traces (trace_with_pauli: a sequential sum,
     density_matrix_engine.cpp:182-197) recomputed on reference_rho_vector
