@@ -337,6 +337,7 @@ def main():
                                        "state size (profiles/k_tile_pass_c2_28q_ncu_full.md)",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": 2 * state_bytes,
+                     "blocks_per_launch": round(int(stats.blocks) / max(1, passes), 2),
                      # Blocks x one state pass each / sweep time: what the multi-gate
                      # passes buy; reported beside `achieved`, never as the fraction.
                      "gate_equivalent_gbs": round(int(stats.blocks) * 2 * state_bytes / (sweep_avg * 1e-3) / 1e9, 1)},
