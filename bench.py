@@ -236,6 +236,8 @@ def main():
     import torch
     from menos_b200 import Context, DeviceState, workloads
     from menos_b200.circuit import to_mb2_ops
+    from menos_b200._lib import SweepEstimate, SweepOptions, lib
+    import ctypes as C
 
     torch.cuda.set_device(local)
     n = args.qubits
@@ -303,11 +305,20 @@ def main():
     dist_barrier(dist)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        res = eng.execute(req)
+        eng.execute(req)
     e2e_s = dist_max(dist, time.perf_counter() - t0)
+    # The copies one execute() makes (the circuit is planned on the host and
+    # only its encoded program crosses): the tiled program, the Pauli terms'
+    # X and Z masks and the sampler's sorted uniforms in; the terms' values
+    # and each shot's basis index out.  The expectation's group tables (a
+    # few KB) are not counted.
     arr, _keep = to_mb2_ops(circ)
-    h2d = len(circ.ops) * 80 + sum(m.nbytes for (_o, _q, _p, m, _c) in circ.ops if m is not None) + 16 * len(paulis)
-    d2h = 16 * (len(paulis) + 1) + 16 * len(res.counts)
+    est = SweepEstimate()
+    rc_est = lib().mb2_estimate_sweep(arr, len(circ.ops), C.byref(SweepOptions(1, 0, args.tile, 0, 0, args.fusion)),
+                                      n, C.byref(est))
+    n_terms = len(paulis) + 1
+    h2d = int(est.h2d_bytes) + 16 * n_terms + 8 * args.shots if rc_est == 0 else None
+    d2h = 16 * n_terms + 8 * args.shots
 
     passes = int(stats.passes)
     sweep_avg = statistics.median(sweep_ms)
