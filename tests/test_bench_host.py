@@ -62,3 +62,32 @@ def test_percentile():
     assert bench.percentile([], 50) is None
     xs = [5, 1, 4, 2, 3]
     assert bench.percentile(xs, 0) == 1 and bench.percentile(xs, 50) == 3 and bench.percentile(xs, 100) == 5
+
+
+def _run_reference(env_extra):
+    import json
+    import subprocess
+    import sys
+    env = dict(os.environ, **env_extra)
+    r = subprocess.run([sys.executable, os.path.join(os.path.dirname(bench.__file__), "bench.py"), "--impl",
+                        "reference", "--qubits", "16", "--steps", "1", "--warmup", "3", "--no-reference-gpu"],
+                       capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    return lines
+
+
+def test_reference_arm_line(ref):
+    """The reference arm on the host cores (oracle/_ref): one JSON line with
+    the contract's keys; its e2e moves no bytes."""
+    (line,) = _run_reference({})
+    assert line["impl"] == "reference" and line["unit"] == "circuits/s" and line["value"] > 0
+    assert line["higher_is_better"] is True and line["n_gpus"] == 1
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": "circuits/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_other_ranks_do_no_work(ref):
+    assert _run_reference({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []
