@@ -190,3 +190,27 @@ def test_reference_passes_partition_the_blocks_in_order():
             assert passes and passes[0][1] == 0 and passes[-1][2] == len(c.ops)
             for a, b in zip(passes, passes[1:]):
                 assert b[1] == a[2] and b[1] < b[2]
+
+
+def test_argument_refusals_and_capacity():
+    c = workloads.crossover(12)
+    arr, keep = to_mb2_ops(c)
+    opts = SweepOptions(0, 0, 0, 0, 0, 0)
+    out = (C.c_uint64 * 64)()
+
+    def call(n, window, chunk, cap):
+        nw = C.c_uint64(cap)
+        rc = lib().mb2_window_plan(arr, len(c.ops), C.byref(opts), n, window, chunk, out, C.byref(nw))
+        return rc, nw.value
+
+    assert call(12, 3, 0, 64)[0] != 0          # a window below 2^4 amplitudes
+    assert call(12, 13, 0, 64)[0] != 0         # a window above the state
+    assert call(12, 10, 11, 64)[0] != 0        # a chunk above the window
+    assert call(12, 10, 3, 64)[0] != 0         # a chunk below 2^4 amplitudes
+    assert call(41, 12, 0, 64)[0] != 0         # more than 40 qubits
+    assert call(12, 12, 0, 64) == (0, 3 + 3 * 1)  # the whole state: one pass
+    rc, need = call(12, 10, 8, 0)              # capacity 0: refused, size reported
+    assert rc != 0 and need > 3
+    out = (C.c_uint64 * need)()
+    assert call(12, 10, 8, need) == (0, need)
+    del keep
