@@ -199,8 +199,10 @@ int mb2_apply_program_monitored(mb2_state* state, const mb2_op* ops, uint32_t nu
  * block_qubits[qubits_begin[b] .. qubits_begin[b+1]) (ascending; empty for a
  * MeasureOp barrier).  Handing it to the reference's block sweep
  * (engines::dense::apply_blocks) reproduces this engine's complex128 state
- * bit for bit.  Capacities in, sizes out: *num_blocks (blocks), *num_order
- * (entries of order, = num_ops), *num_block_qubits.  Host only. */
+ * bit for bit.  order holds num_ops entries; capacities in, sizes out:
+ * *num_blocks (blocks: block_begin and qubits_begin hold one entry more)
+ * and *num_block_qubits (entries of block_qubits); MB2_ERR_INVALID with
+ * the sizes set when a capacity is short.  Host only. */
 int mb2_fusion_plan(const mb2_op* ops, uint32_t num_ops, const mb2_sweep_options* opts, uint32_t* order,
                     uint32_t* block_begin, uint32_t* block_qubits, uint32_t* qubits_begin, uint64_t* num_blocks,
                     uint64_t* num_block_qubits);

@@ -81,3 +81,31 @@ def test_an_operand_beyond_63_qubits_is_refused():
     # :216-219
     with pytest.raises(MB2Error):
         fusion_plan(Circuit(65).gate("h", [64]))
+
+
+def test_fusion_plan_size_query():
+    """Capacities in, sizes out: a short capacity is refused with the sizes
+    set; block_begin and qubits_begin hold one entry more than the blocks."""
+    import ctypes as C
+
+    from menos_b200._lib import SweepOptions, lib
+    from menos_b200.circuit import to_mb2_ops
+    c = Circuit(3).gate("h", [0]).gate("cx", [0, 1]).gate("h", [2])
+    arr, keep = to_mb2_ops(c)
+    nb, nq = C.c_uint64(0), C.c_uint64(0)
+    opts = SweepOptions(1, 0, 0, 0, 0, 0)
+    order = np.zeros(3, np.uint32)
+    bb = np.zeros(1, np.uint32)
+    qb = np.zeros(1, np.uint32)
+    bq = np.zeros(1, np.uint32)
+    rc = lib().mb2_fusion_plan(arr, 3, C.byref(opts), order.ctypes.data, bb.ctypes.data, bq.ctypes.data,
+                               qb.ctypes.data, C.byref(nb), C.byref(nq))
+    assert rc != 0 and (nb.value, nq.value) == (2, 3)
+    bb = np.zeros(nb.value + 1, np.uint32)
+    qb = np.zeros(nb.value + 1, np.uint32)
+    bq = np.zeros(nq.value, np.uint32)
+    rc = lib().mb2_fusion_plan(arr, 3, C.byref(opts), order.ctypes.data, bb.ctypes.data, bq.ctypes.data,
+                               qb.ctypes.data, C.byref(nb), C.byref(nq))
+    del keep
+    assert rc == 0
+    assert (order.tolist(), bb.tolist(), bq.tolist(), qb.tolist()) == ([0, 1, 2], [0, 2, 3], [0, 1, 2], [0, 2, 3])
