@@ -86,6 +86,18 @@ def pure_noise_circuit(n, depth, seed, widest=2):
     return c
 
 
+def test_trajectory_seed_is_the_matching_splitmix64_output():
+    """tests/engines/trajectory/trajectory_engine_test.cpp:67-73: trajectory
+    t's seed is output t of one SplitMix64 stream seeded with the job's
+    seed (state += 0x9E3779B97F4A7C15, then the published output mix)."""
+    state = 0xDEADBEEF
+    for t in range(8):
+        state = (state + 0x9E3779B97F4A7C15) & MASK64
+        z = ((state ^ (state >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK64
+        assert trajectory_seed(0xDEADBEEF, t) == z ^ (z >> 31)
+
+
 def test_restatement_is_bitwise_the_reference_engine(ref):
     n = 5
     c = pure_noise_circuit(n, 30, 1)
